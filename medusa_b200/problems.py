@@ -1,0 +1,241 @@
+"""Problem setups: the host-side counterpart of the reference's problems/init_*.c hooks.
+
+Each function returns a :class:`Problem`: the grid, the physics switches that the
+reference fixes at compile time (setups/*.mk -> build.h) and reads from its input.*
+files, and the initial primitive state of the interior zones in the reference's zone
+order (i-major: ``ic[(i*n2 + j), :]`` holds rho, u (internal energy density), v1, v2, v3,
+with v^d the contravariant coordinate velocities).
+
+The setups follow the reference files they cite but use the sizes, parameters and
+initial conditions of the workloads this library is measured on (Sod 1024 zones,
+Kelvin-Helmholtz 2048^2, ensembles of 1-D spherical Sod/Noh/Sedov problems).  All
+random numbers come from splitmix64 (Steele, Lea & Flood 2014) on a caller-given seed,
+so the same seed gives the same bits on every host.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+# geometry ids (decs.h:669-671)
+CARTESIAN = 0
+SPHERICAL = 1
+# EOS ids (decs.h:674-675)
+GAMMA_LAW = 0
+POLYTROPIC = 1
+# boundary kinds (decs.h:64-69)
+OUTFLOW = 0
+REFLECT = 1
+EXTRAP = 2
+PERIODIC = 3
+PROB = 4
+SPHERICAL_ORIGIN = 5
+# problem-specific PROB boundary hooks
+PROB_NONE = 0
+PROB_NOH = 1
+
+NG = 2
+NPRIM = 5
+
+
+@dataclasses.dataclass
+class Problem:
+    """A hydro problem: grid, physics switches, run controls and initial state."""
+    name: str
+    ndim: int
+    geom: int
+    n: tuple                      # (n1, n2, n3) interior zones
+    startx: tuple                 # coordinate of the lower edge of zone 0 per direction
+    dx: tuple                     # coordinate spacing per direction
+    gam: float
+    ic: np.ndarray                # [n1*n2*n3, 5] float64, i-major
+    Kpoly: float = 1.0
+    eos: int = GAMMA_LAW
+    bc_lo: tuple = (OUTFLOW, OUTFLOW, OUTFLOW)
+    bc_hi: tuple = (OUTFLOW, OUTFLOW, OUTFLOW)
+    prob_kind: int = PROB_NONE
+    cfl: float = 0.9              # io.c:5018 default
+    dt_init_safety: float = 0.1   # io.c:5036
+    dt_grow_safety: float = 1.1   # io.c:5035
+    initial_dt: float = 1.0e100   # io.c:5063
+    dtmax: float = 1.0e200        # io.c:5037
+    dtmin: float = 1.0e-200       # io.c:5038
+    tmax: float = 1.0e100
+    rtrans: float = 1.0
+    hydro_interp_order: int = 3   # io.c:5055
+    nsteps: Optional[int] = None  # fixed step count for the workload, if any
+
+    @property
+    def ncell(self) -> int:
+        return int(self.n[0] * self.n[1] * self.n[2])
+
+    def copy(self, **kw) -> "Problem":
+        d = dataclasses.asdict(self)
+        d["ic"] = self.ic.copy()
+        d.update(kw)
+        return Problem(**d)
+
+
+# ----------------------------------------------------------------------------- PRNG
+_MASK = np.uint64(0xFFFFFFFFFFFFFFFF)
+
+
+def splitmix64(seed: int, count: int) -> np.ndarray:
+    """First ``count`` outputs of splitmix64 seeded with ``seed`` (uint64)."""
+    with np.errstate(over="ignore"):
+        idx = np.arange(1, count + 1, dtype=np.uint64)
+        z = np.uint64(seed & 0xFFFFFFFFFFFFFFFF) + idx * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def uniform01(seed: int, count: int) -> np.ndarray:
+    """Uniform doubles in [0,1) from the top 53 bits of splitmix64."""
+    return (splitmix64(seed, count) >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+# ----------------------------------------------------------------------------- setups
+def sod(n1: int = 1024, cfl: float = 0.8, tmax: float = 0.2) -> Problem:
+    """Sod shock tube, problems/init_sod.c:31-99 (Toro test 1 states, gamma=1.4)."""
+    gam = 1.4
+    dx = 1.0 / n1
+    rhol, el, ul = 1.0, 1.0 / (gam - 1.0), 0.0
+    rhor, er, ur = 0.125, 0.1 / (gam - 1.0), 0.0
+    ic = np.zeros((n1, NPRIM))
+    for ii in range(n1):
+        xl = ii * dx
+        xr = xl + dx
+        if xr < 0.5:
+            ic[ii] = (rhol, el, ul, 0.0, 0.0)
+        elif xl < 0.5:
+            wl = (0.5 - xl) / dx
+            wr = (xr - 0.5) / dx
+            ic[ii] = (rhol * wl + rhor * wr, el * wl + er * wr, ul * wl + ur * wr, 0.0, 0.0)
+        else:
+            ic[ii] = (rhor, er, ur, 0.0, 0.0)
+    return Problem(name="sod1d_%d" % n1, ndim=1, geom=CARTESIAN, n=(n1, 1, 1),
+                   startx=(0.0, 0.0, 0.0), dx=(dx, 1.0, 1.0), gam=gam, ic=ic,
+                   bc_lo=(OUTFLOW,) * 3, bc_hi=(OUTFLOW,) * 3, cfl=cfl, tmax=tmax)
+
+
+def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240601,
+                     cfl: float = 0.8, nsteps: int = 200) -> Problem:
+    """2-D Kelvin-Helmholtz on the periodic unit square (the structure of
+    problems/init_kh.c:23-89 with the shear-layer state of the measured workload):
+    rho=2, v_x=+0.5 where |y-0.5|<0.25, else rho=1, v_x=-0.5; p=2.5; gamma=5/3;
+    v_y = 0.01 sin(4 pi x); uniform noise of amplitude 1e-3 on v_x and v_y."""
+    n2 = n1 if n2 is None else n2
+    gam = 5.0 / 3.0
+    dx0, dx1 = 1.0 / n1, 1.0 / n2
+    x = (np.arange(n1) + 0.5) * dx0
+    y = (np.arange(n2) + 0.5) * dx1
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    inner = np.abs(Y - 0.5) < 0.25
+    rho = np.where(inner, 2.0, 1.0)
+    vx = np.where(inner, 0.5, -0.5)
+    vy = 0.01 * np.sin(4.0 * math.pi * X)
+    noise = uniform01(seed, 2 * n1 * n2).reshape(2, n1, n2)
+    vx = vx + (2.0 * noise[0] - 1.0) * 1.0e-3
+    vy = vy + (2.0 * noise[1] - 1.0) * 1.0e-3
+    ic = np.zeros((n1 * n2, NPRIM))
+    ic[:, 0] = rho.ravel()
+    ic[:, 1] = 2.5 / (gam - 1.0)
+    ic[:, 2] = vx.ravel()
+    ic[:, 3] = vy.ravel()
+    return Problem(name="kh2d_%dx%d" % (n1, n2), ndim=2, geom=CARTESIAN, n=(n1, n2, 1),
+                   startx=(0.0, 0.0, 0.0), dx=(dx0, dx1, 1.0), gam=gam, ic=ic,
+                   bc_lo=(PERIODIC, PERIODIC, PERIODIC), bc_hi=(PERIODIC, PERIODIC, PERIODIC),
+                   cfl=cfl, nsteps=nsteps)
+
+
+def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
+                 p_ratio: float = 100.0, r0: float = 0.5, cfl: float = 0.8,
+                 tmax: float = 1.0e100) -> Problem:
+    """1-D spherical problem on r in [0,1] (uniform radius), SPHERICAL_ORIGIN inner
+    boundary (bc.c:776-803).
+
+    kind='sod'   : rho, p = rho_ratio, p_ratio inside r<r0; 1, 1 outside; at rest;
+                   OUTFLOW outer boundary.
+    kind='sedov' : rho=1; p = p_ratio inside r<r0 (a small blast radius), the ambient p is 1e-5;
+                   OUTFLOW outer boundary.
+    kind='noh'   : problems/init_spherical_noh.c:14-61: rho=1, u=1e-6/(gam-1), v^r=-1;
+                   PROB outer boundary with the Noh inflow (init_spherical_noh.c:63-79).
+    """
+    dx = 1.0 / n1
+    rc = (np.arange(n1) + 0.5) * dx
+    ic = np.zeros((n1, NPRIM))
+    bc_hi = OUTFLOW
+    prob_kind = PROB_NONE
+    if kind == "sod":
+        inside = rc < r0
+        rho = np.where(inside, rho_ratio, 1.0)
+        p = np.where(inside, p_ratio, 1.0)
+        ic[:, 0] = rho
+        ic[:, 1] = p / (gam - 1.0)
+    elif kind == "sedov":
+        inside = rc < r0
+        p_amb = 1.0e-5
+        ic[:, 0] = 1.0
+        ic[:, 1] = np.where(inside, p_amb * p_ratio, p_amb) / (gam - 1.0)
+    elif kind == "noh":
+        ic[:, 0] = 1.0
+        ic[:, 1] = 1.0e-6 / (gam - 1.0)
+        ic[:, 2] = -1.0   # vr / scale[0][0], scale[0][0] = 1 for a uniform radius
+        bc_hi = PROB
+        prob_kind = PROB_NOH
+    else:
+        raise ValueError("unknown 1-D spherical problem kind %r" % kind)
+    return Problem(name="sph1d_%s_%d" % (kind, n1), ndim=1, geom=SPHERICAL, n=(n1, 1, 1),
+                   startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
+                   bc_lo=(SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW), bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
+                   prob_kind=prob_kind, cfl=cfl, tmax=tmax)
+
+
+def ensemble_1d(count: int = 2048, seed: int = 7, nmin: int = 128, nmax: int = 8192,
+                cfl: float = 0.8) -> list:
+    """Ensemble of independent 1-D spherical problems: zone counts log-uniform in
+    [nmin, nmax], kinds Sod/Noh/Sedov, density ratio log-uniform in [2, 100], pressure
+    ratio log-uniform in [2, 1e4], gamma drawn from {4/3, 1.4, 5/3}."""
+    u = uniform01(seed, 5 * count).reshape(count, 5)
+    out = []
+    gams = (4.0 / 3.0, 1.4, 5.0 / 3.0)
+    kinds = ("sod", "noh", "sedov")
+    for m in range(count):
+        n1 = int(round(math.exp(math.log(nmin) + u[m, 0] * (math.log(nmax) - math.log(nmin)))))
+        n1 = max(nmin, min(nmax, n1))
+        kind = kinds[min(2, int(u[m, 1] * 3))]
+        rr = math.exp(math.log(2.0) + u[m, 2] * (math.log(100.0) - math.log(2.0)))
+        pr = math.exp(math.log(2.0) + u[m, 3] * (math.log(1.0e4) - math.log(2.0)))
+        gam = gams[min(2, int(u[m, 4] * 3))]
+        r0 = 0.5 if kind == "sod" else 0.05
+        pb = spherical_1d(kind, n1, gam, rho_ratio=rr, p_ratio=pr, r0=r0, cfl=cfl)
+        pb.name = "ens%04d_%s" % (m, pb.name)
+        out.append(pb)
+    return out
+
+
+def blast_2d(n1: int = 64, n2: Optional[int] = None, p_in: float = 10.0, p_out: float = 0.01,
+             radius: float = 0.1, bc: int = REFLECT, cfl: float = 0.8) -> Problem:
+    """2-D Cartesian blast wave on the unit square (in the spirit of
+    problems/init_sedov_cart.c): rho=1 at rest, p=p_in inside a circle of the given
+    radius around (0.5, 0.5), p_out outside; the strong shock exercises the shock flags
+    and the HLLE switch of step.c:711-755."""
+    n2 = n1 if n2 is None else n2
+    gam = 1.4
+    dx0, dx1 = 1.0 / n1, 1.0 / n2
+    x = (np.arange(n1) + 0.5) * dx0
+    y = (np.arange(n2) + 0.5) * dx1
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    r = np.sqrt((X - 0.5) ** 2 + (Y - 0.5) ** 2)
+    p = np.where(r < radius, p_in, p_out)
+    ic = np.zeros((n1 * n2, NPRIM))
+    ic[:, 0] = 1.0
+    ic[:, 1] = (p / (gam - 1.0)).ravel()
+    return Problem(name="blast2d_%dx%d" % (n1, n2), ndim=2, geom=CARTESIAN, n=(n1, n2, 1),
+                   startx=(0.0, 0.0, 0.0), dx=(dx0, dx1, 1.0), gam=gam, ic=ic,
+                   bc_lo=(bc, bc, bc), bc_hi=(bc, bc, bc), cfl=cfl)

@@ -1,0 +1,126 @@
+"""Build recipe for oracle/_ref: the reference's own hydro sweep, compiled UNMODIFIED
+from the reference tree, around the glue in oracle/refshim/.
+
+TEST INFRASTRUCTURE ONLY.  Nothing under medusa_b200/ imports, links or runs what
+this script builds.  The reference's Makefile is not used: this recipe writes the
+build.h that Makefile:157-212 would write (same DEFS list) for each configuration
+and compiles the hot-path sources directly with gcc.  Outputs go only into
+oracle/_ref/ (git-ignored; it travels with the working tree to a GPU host).
+
+Two binaries per configuration:
+  ref_<cfg>        parity build, -O2 -fno-fast-math -ffp-contract=off
+  reffast_<cfg>    the reference's own flags (Makefile:14), used as the timed CPU baseline
+
+Usage: python oracle/build_ref.py [--ref-root DIR] [--force]
+"""
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+OUT = os.path.join(HERE, "_ref")
+SHIM = os.path.join(HERE, "refshim")
+DEFAULT_REF_ROOT = "/root/reference"
+
+# hot-path sources compiled unmodified (SURVEY-verified link set minus main.c/io.c)
+REF_SOURCES = ["array.c", "mpi.c", "utils.c", "step.c", "geometry.c", "rad_fluid.c",
+               "fluid.c", "riemann.c", "reconstruct.c", "bc.c", "eos.c", "timer.c",
+               "quadrupole.c", "tracer.c"]
+
+BASE_DEFS = dict(USE_MPI="FALSE", USE_OMP="FALSE", USE_GPU="FALSE", EOS="GAMMA_LAW",
+                 GRAV="NO_GRAV", GR_MONOPOLE="FALSE", PN_POTENTIAL="FALSE",
+                 USE_EXT_SRC="FALSE", USE_AUX_SRC="FALSE", DO_HYDRO="TRUE",
+                 PRINT_OPAC_DATA="FALSE", DO_RADIATION="FALSE", PHOTON="FALSE",
+                 NEUTRINO="FALSE", PERTURB="NONE", DO_ROTATION="FALSE",
+                 ENFORCE_FLOORS="FALSE", OUTPUT_PRECISION="DOUBLE", DO_TIMING="FALSE",
+                 DEBUG="FALSE", POLAR_AVG="FALSE", USE_FORTRAN_CODE="FALSE",
+                 USE_EXP_INTERP="FALSE", RAD_CLOSURE="M1", USE_LARGER_STEP="FALSE",
+                 USE_LINEAR_ALLOCATION="TRUE", INEL_DT_CONTROL="FALSE")
+DEF_ORDER = ["NDIM", "USE_MPI", "USE_OMP", "USE_GPU", "GEOM", "EOS", "GRAV", "GR_MONOPOLE",
+             "PN_POTENTIAL", "USE_EXT_SRC", "USE_AUX_SRC", "DO_HYDRO", "PRINT_OPAC_DATA",
+             "DO_RADIATION", "PHOTON", "NEUTRINO", "PERTURB", "DO_ROTATION",
+             "ENFORCE_FLOORS", "DENDRITIC_GRID", "OUTPUT_PRECISION", "DO_TIMING", "DEBUG",
+             "POLAR_AVG", "USE_FORTRAN_CODE", "USE_EXP_INTERP", "RAD_CLOSURE",
+             "USE_LARGER_STEP", "USE_LINEAR_ALLOCATION", "INEL_DT_CONTROL", "RCOORD",
+             "THCOORD"]
+
+CONFIGS = {
+    # 1-D Cartesian (Sod shock tube)
+    "cart1d": dict(NDIM="1", GEOM="CARTESIAN", DENDRITIC_GRID="FALSE",
+                   RCOORD="UNIFORM", THCOORD="UNIFORM"),
+    # 2-D Cartesian (Kelvin-Helmholtz)
+    "cart2d": dict(NDIM="2", GEOM="CARTESIAN", DENDRITIC_GRID="FALSE",
+                   RCOORD="UNIFORM", THCOORD="UNIFORM"),
+    # 1-D spherical, uniform radius (ensemble members: Sod/Noh/Sedov type)
+    "sph1d": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                  RCOORD="UNIFORM", THCOORD="UNIFORM"),
+}
+
+PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]
+FAST_FLAGS = ["-O3", "-ffast-math", "-ftree-vectorize", "-fpeel-loops"]
+
+
+def write_build_h(path, defs):
+    lines = ["#ifndef BUILD_H_", "#define BUILD_H_", "", '#include "enumerators.h"', ""]
+    for k in DEF_ORDER:
+        lines.append("#define %s %s" % (k, defs[k]))
+    lines.append("")
+    lines.append('#define BUILD_STRING "medusa_b200 oracle/_ref build\\n"')
+    lines.append("#endif // BUILD_H_")
+    lines.append("")
+    text = "\n".join(lines)
+    if os.path.exists(path) and open(path).read() == text:
+        return
+    with open(path, "w") as f:
+        f.write(text)
+
+
+def build_config(name, cfg, ref_root, force=False):
+    defs = dict(BASE_DEFS)
+    defs.update(cfg)
+    cdir = os.path.join(OUT, name)
+    os.makedirs(cdir, exist_ok=True)
+    write_build_h(os.path.join(cdir, "build.h"), defs)
+    srcs = [os.path.join(ref_root, s) for s in REF_SOURCES]
+    if defs["GEOM"] == "SPHERICAL":
+        srcs.append(os.path.join(ref_root, "metrics", "metric_spherical_general.c"))
+    else:
+        srcs.append(os.path.join(SHIM, "metric_cartesian_current.c"))
+    srcs += [os.path.join(SHIM, "ref_harness.c"), os.path.join(SHIM, "ref_main.c")]
+    deps = srcs + [os.path.join(cdir, "build.h"), os.path.abspath(__file__)]
+    built = []
+    for exe, flags in (("ref_" + name, PARITY_FLAGS), ("reffast_" + name, FAST_FLAGS)):
+        target = os.path.join(OUT, exe)
+        if (not force and os.path.exists(target)
+                and os.path.getmtime(target) >= max(os.path.getmtime(d) for d in deps)):
+            built.append(target)
+            continue
+        cmd = (["gcc", "-std=gnu99", "-w"] + flags +
+               ["-I" + cdir, "-I" + ref_root, "-include", "limits.h", "-o", target] + srcs + ["-lm"])
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+            raise RuntimeError("oracle/_ref build failed for %s" % exe)
+        built.append(target)
+    return built
+
+
+def build(ref_root=DEFAULT_REF_ROOT, force=False):
+    """Build every configuration; returns the list of binaries.  Needs the reference tree."""
+    if not os.path.isdir(ref_root):
+        raise FileNotFoundError("reference tree not found at %s" % ref_root)
+    os.makedirs(OUT, exist_ok=True)
+    out = []
+    for name, cfg in CONFIGS.items():
+        out += build_config(name, cfg, ref_root, force)
+    return out
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref-root", default=DEFAULT_REF_ROOT)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    for p in build(a.ref_root, a.force):
+        print(p)

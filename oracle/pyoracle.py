@@ -1,0 +1,202 @@
+"""Python access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+- :func:`build_oracle` compiles oracle/hydro_oracle.c (the plain-C restatement of the
+  reference sweep) into oracle/_build/liboracle.so with -O2 -fno-fast-math
+  -ffp-contract=off, the flags under which it reproduces the reference bit for bit.
+- :class:`Oracle` drives that library through ctypes.
+- :func:`run_reference` runs the reference itself (built unmodified by
+  oracle/build_ref.py into oracle/_ref/) on the same problem in a subprocess.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD_DIR = os.path.join(HERE, "_build")
+LIB_PATH = os.path.join(BUILD_DIR, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+SRC = os.path.join(HERE, "hydro_oracle.c")
+ORACLE_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]
+
+
+class Params(ctypes.Structure):
+    """Field order of ref_params (oracle/refshim/ref_harness.c) and orc_params."""
+    _fields_ = [("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int),
+                ("startx", ctypes.c_double * 3), ("dx", ctypes.c_double * 3),
+                ("gam", ctypes.c_double), ("Kpoly", ctypes.c_double),
+                ("eos_kind", ctypes.c_int),
+                ("bc_lo", ctypes.c_int * 3), ("bc_hi", ctypes.c_int * 3),
+                ("prob_kind", ctypes.c_int),
+                ("cfl", ctypes.c_double),
+                ("dt_init_safety", ctypes.c_double), ("dt_grow_safety", ctypes.c_double),
+                ("initial_dt", ctypes.c_double), ("dtmax", ctypes.c_double),
+                ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
+                ("rtrans", ctypes.c_double), ("hydro_interp_order", ctypes.c_int)]
+
+
+def params_of(pb) -> Params:
+    p = Params()
+    p.n1, p.n2, p.n3 = pb.n
+    for d in range(3):
+        p.startx[d] = pb.startx[d]
+        p.dx[d] = pb.dx[d]
+        p.bc_lo[d] = pb.bc_lo[d]
+        p.bc_hi[d] = pb.bc_hi[d]
+    p.gam, p.Kpoly, p.eos_kind, p.prob_kind = pb.gam, pb.Kpoly, pb.eos, pb.prob_kind
+    p.cfl = pb.cfl
+    p.dt_init_safety, p.dt_grow_safety = pb.dt_init_safety, pb.dt_grow_safety
+    p.initial_dt, p.dtmax, p.dtmin, p.tmax = pb.initial_dt, pb.dtmax, pb.dtmin, pb.tmax
+    p.rtrans = pb.rtrans
+    p.hydro_interp_order = pb.hydro_interp_order
+    return p
+
+
+def build_oracle(force: bool = False) -> str:
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    if (not force and os.path.exists(LIB_PATH)
+            and os.path.getmtime(LIB_PATH) >= os.path.getmtime(SRC)):
+        return LIB_PATH
+    cmd = ["gcc", "-std=gnu99", "-shared", "-fPIC"] + ORACLE_FLAGS + ["-o", LIB_PATH, SRC, "-lm"]
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build_oracle()
+        L = ctypes.CDLL(LIB_PATH)
+        L.orc_create.restype = ctypes.c_void_p
+        L.orc_create.argtypes = [ctypes.POINTER(Params), ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_advance_one.restype = ctypes.c_double
+        L.orc_advance_one.argtypes = [ctypes.c_void_p]
+        L.orc_estimate_dt.restype = ctypes.c_double
+        L.orc_estimate_dt.argtypes = [ctypes.c_void_p]
+        L.orc_step.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.orc_get_t.restype = ctypes.c_double
+        L.orc_get_t.argtypes = [ctypes.c_void_p]
+        L.orc_get_min_dt.restype = ctypes.c_double
+        L.orc_get_min_dt.argtypes = [ctypes.c_void_p]
+        L.orc_get_istep.argtypes = [ctypes.c_void_p]
+        L.orc_get_interior.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_set_interior.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_get_moments0.argtypes = [ctypes.c_void_p] * 4
+        L.orc_get_geom.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """One problem advanced by the CPU restatement."""
+
+    def __init__(self, pb):
+        self.pb = pb
+        self._prm = params_of(pb)
+        ic = np.ascontiguousarray(pb.ic, dtype=np.float64)
+        self._h = lib().orc_create(ctypes.byref(self._prm), pb.ndim, pb.geom, ic.ctypes.data)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def advance(self, nsteps: int = 1):
+        """Run nsteps passes of the reference time loop; returns the list of dt used."""
+        return [lib().orc_advance_one(self._h) for _ in range(nsteps)]
+
+    def estimate_dt(self) -> float:
+        return lib().orc_estimate_dt(self._h)
+
+    def step(self, dt: float):
+        lib().orc_step(self._h, dt)
+
+    @property
+    def t(self) -> float:
+        return lib().orc_get_t(self._h)
+
+    @property
+    def min_dt(self) -> float:
+        return lib().orc_get_min_dt(self._h)
+
+    def state(self):
+        prim = np.zeros((self.pb.ncell, 5))
+        eos = np.zeros((self.pb.ncell, 5))
+        lib().orc_get_interior(self._h, prim.ctypes.data, eos.ctypes.data)
+        return prim, eos
+
+    def set_state(self, prim):
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        lib().orc_set_interior(self._h, prim.ctypes.data)
+
+    def moments0(self):
+        n = self.pb.n[0] + 4
+        a, b, g = np.zeros(n), np.zeros(n), np.zeros(n)
+        lib().orc_get_moments0(self._h, a.ctypes.data, b.ctypes.data, g.ctypes.data)
+        return a, b, g
+
+    def geom(self, i: int, j: int = 0):
+        out = np.zeros(64)
+        lib().orc_get_geom(self._h, i, j, out.ctypes.data)
+        return out
+
+
+# ----------------------------------------------------------------------------- reference
+def ref_config(pb) -> str:
+    if pb.geom == 0:
+        return "cart%dd" % pb.ndim
+    return "sph%dd" % pb.ndim
+
+
+def ref_available(pb, fast: bool = False) -> bool:
+    exe = os.path.join(REF_DIR, ("reffast_" if fast else "ref_") + ref_config(pb))
+    return os.path.exists(exe)
+
+
+def _write_input(pb, path):
+    prm = params_of(pb)
+    with open(path, "wb") as f:
+        f.write(bytes(prm))
+        f.write(np.ascontiguousarray(pb.ic, dtype=np.float64).tobytes())
+
+
+def run_reference(pb, nsteps: int, every: int = 1):
+    """Run the unmodified reference for nsteps; returns a list of snapshots
+    (istep, t, dt_used, min_dt, prim[ncell,5]) including the initial state."""
+    exe = os.path.join(REF_DIR, "ref_" + ref_config(pb))
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        _write_input(pb, fin)
+        subprocess.run([exe, "run", fin, fout, str(nsteps), str(every)], check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        raw = np.fromfile(fout, dtype=np.float64)
+    rec = 4 + 5 * pb.ncell
+    raw = raw.reshape(-1, rec)
+    return [(int(r[0]), r[1], r[2], r[3], r[4:].reshape(pb.ncell, 5).copy()) for r in raw]
+
+
+def time_reference(pb, warmup: int, steps: int, fast: bool = True) -> dict:
+    """Time the reference's own build (its Makefile flags when fast=True) in a
+    subprocess; returns zone_updates_per_s, seconds, steps, cells."""
+    exe = os.path.join(REF_DIR, ("reffast_" if fast else "ref_") + ref_config(pb))
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        _write_input(pb, fin)
+        r = subprocess.run([exe, "time", fin, str(warmup), str(steps)], check=True,
+                           capture_output=True, text=True)
+    out = {}
+    for tok in r.stdout.split():
+        k, v = tok.split("=")
+        out[k] = float(v)
+    return out
