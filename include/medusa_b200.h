@@ -1,0 +1,150 @@
+/*
+ * medusa_b200 -- C ABI of the B200 hydrodynamic sweep.
+ *
+ * This is the drop-in boundary for the reference's hot path.  The reference's time
+ * loop (main.c:206-313) calls three functions with global state:
+ *
+ *   void estimate_dt(void);   step.c:163-203   (declared decs.h:756)
+ *   void step(void);          step.c:28-129    (declared decs.h:755)
+ *   void update_cpu(void);    step.c:16-24     (declared decs.h:754)
+ *
+ * and establishes device residency in the upload block main.c:129-165.  The entry
+ * points below replace those with handle-based calls: one handle (a "solver") holds
+ * one or more independent problems of the same dimensionality that advance together.
+ * All arguments are plain C types; no call allocates on behalf of the caller except
+ * mdg_create (device state) and none calls exit().  Every call returns an MDG_*
+ * status; the reference's own error codes (decs.h:89-98) map onto the same values.
+ *
+ * Semantics follow the reference exactly: the primitive state (rho, internal energy
+ * density u, contravariant velocities v1 v2 v3) lives on the device between calls; one
+ * mdg_step is one pass of the main.c time loop: estimate_dt() + the dt safety/clip
+ * rules of main.c:228-251 + the two-stage step() + t += dt.
+ */
+#ifndef MEDUSA_B200_H_
+#define MEDUSA_B200_H_
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes: same numbering as decs.h:89-98 */
+#define MDG_OK             0
+#define MDG_ERR_INVALID    1
+#define MDG_ERR_INDEX      2
+#define MDG_ERR_NOTFOUND   3
+#define MDG_ERR_IO         4
+#define MDG_ERR_NOTIMPL    5
+#define MDG_ERR_OUTOFMEM   6
+#define MDG_ERR_PARFILE    7
+#define MDG_ERR_LOGICAL    8
+#define MDG_ERR_INTERNAL   9
+#define MDG_ERR_CUDA       10   /* a CUDA runtime call failed; see mdg_last_error_message */
+#define MDG_ERR_NONFINITE  11   /* a non-finite time step was produced (dt < dtmin, main.c:229) */
+
+/* geometry (decs.h:669-671), EOS (decs.h:674-675), boundary kinds (decs.h:64-69) */
+#define MDG_CARTESIAN 0
+#define MDG_SPHERICAL 1
+#define MDG_GAMMA_LAW 0
+#define MDG_POLYTROPIC 1
+#define MDG_BC_OUTFLOW 0
+#define MDG_BC_REFLECT 1
+#define MDG_BC_EXTRAP 2
+#define MDG_BC_PERIODIC 3
+#define MDG_BC_PROB 4
+#define MDG_BC_SPHERICAL_ORIGIN 5
+/* PROB boundary hooks restated on the device (the reference's prob_bounds callbacks) */
+#define MDG_PROB_NONE 0
+#define MDG_PROB_NOH 1   /* problems/init_spherical_noh.c:63-79 */
+
+/* arithmetic of the sweep */
+#define MDG_PREC_FP64 0   /* plain: FP64 throughout, the reference's operation order */
+#define MDG_PREC_MIXED 1  /* FP32 reconstruction/limiting/Riemann, FP64 accumulation,
+                             sources, geometry and dt */
+
+/*
+ * One problem.  Replaces the compile-time switches of setup.mk/build.h (NDIM, GEOM,
+ * EOS; Makefile:157-212), the run-time keys of the input.* file that the sweep reads
+ * (io.c:4979-5785: n1 n2 n3 cfl dt_init_safety dt_grow_safety initial_dt dtmax dtmin
+ * tmax hydro_interp_order) and what the problem hooks set (init_grid: startx, dx;
+ * init_problem: gam/Kpoly, bc[]; prob_bounds).  The geometry tables that the
+ * reference builds in init_geometry() (geometry.c:4-63) are rebuilt from these fields
+ * by the library, bit-identically.
+ */
+typedef struct mdg_problem_desc {
+  int ndim;                 /* 1 or 2 */
+  int geom;                 /* MDG_CARTESIAN (1-D, 2-D) or MDG_SPHERICAL (1-D) */
+  int eos;                  /* MDG_GAMMA_LAW or MDG_POLYTROPIC */
+  int n1, n2, n3;           /* interior zones; n2 = n3 = 1 in 1-D */
+  double startx[3];         /* lower coordinate edge of zone 0 */
+  double dx[3];             /* coordinate spacing */
+  double gam;               /* adiabatic index */
+  double Kpoly;             /* polytropic constant (MDG_POLYTROPIC) */
+  int bc_lo[3], bc_hi[3];   /* boundary kind per direction */
+  int prob_kind;            /* MDG_PROB_* used by MDG_BC_PROB boundaries */
+  double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
+  int hydro_interp_order;   /* 1, 2 (linear) or 3 (parabolic) */
+} mdg_problem_desc;
+
+typedef struct mdg_solver mdg_solver;   /* opaque */
+
+/* Create a solver for nprob problems (all of the same ndim) and allocate their
+ * device state.  Replaces the allocation + upload block main.c:129-165.
+ * precision: MDG_PREC_FP64 or MDG_PREC_MIXED.  device: CUDA ordinal. */
+int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int device,
+               mdg_solver **out);
+
+/* Copy the interior primitive state of problem `prob` to the device, from host memory
+ * laid out [zone][5] in the reference's zone order (ZLOOP: i-major, then j), and reset
+ * its time to t=0, istep=0 (main.c:172-176, 180-182). */
+int mdg_upload_state(mdg_solver *s, int prob, const double *prim);
+
+/* The next time step of every problem as estimate_dt() + main.c:239-251 would produce
+ * it; written to dt_out[nprob] (may be NULL).  Idempotent until the next mdg_step. */
+int mdg_estimate_dt(mdg_solver *s, double *dt_out);
+
+/* Advance every problem by nsteps passes of the main.c time loop.  Asynchronous with
+ * respect to the host (work is queued on the solver's stream). */
+int mdg_step(mdg_solver *s, int nsteps);
+
+/* update_cpu() equivalent: copy problem `prob`'s interior primitives ([zone][5]) and,
+ * if eos != NULL, its EOS record ([zone][5]: PRESS, CS, TEMP, ENT(=0), GAMMA; the EOS
+ * of the most recent stage state, as the reference's sim_eos holds) to host memory. */
+int mdg_download_state(mdg_solver *s, int prob, double *prim, double *eos);
+
+/* Time bookkeeping of problem `prob` after all queued work: t, the dt of the last
+ * step and the step count. */
+int mdg_get_time(mdg_solver *s, int prob, double *t, double *dt_last, int *istep);
+
+/* The CUDA stream all work of this solver is queued on (a cudaStream_t). */
+int mdg_get_stream(mdg_solver *s, void **stream);
+
+/* Wait for all queued work; returns the first asynchronous error, if any. */
+int mdg_synchronize(mdg_solver *s);
+
+/* Free the solver and its device memory. */
+int mdg_destroy(mdg_solver *s);
+
+/* Static description of a status code, and the message of the last failure in this
+ * thread (a CUDA error string or the validation that failed). */
+const char *mdg_error_string(int code);
+const char *mdg_last_error_message(void);
+
+/* Per-kernel timers, the counterpart of the reference's TIMER_START/TIMER_STOP
+ * instrumentation (decs.h:717-746, timer.c) and its timing.csv (io.c:51-108).  With
+ * timing enabled every queued launch is bracketed by CUDA events and each mdg_step
+ * waits for its step to finish; ms[k] and calls[k] accumulate per timer k: */
+#define MDG_TIMER_DT        0   /* estimate_dt + main.c dt rules */
+#define MDG_TIMER_STAGE0    1   /* first RK stage (fused sweep) */
+#define MDG_TIMER_STAGE1    2   /* second RK stage (fused sweep) */
+#define MDG_TIMER_FINISH    3   /* t += dt bookkeeping */
+#define MDG_NTIMERS         4
+int mdg_set_timing(mdg_solver *s, int enable);
+int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
+
+/* Library version as major*10000 + minor*100 + patch. */
+int mdg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MEDUSA_B200_H_ */

@@ -1,0 +1,423 @@
+// C ABI of medusa_b200 (include/medusa_b200.h): solver lifetime, state transfer and the
+// per-step launch sequence.
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "mdg_internal.h"
+#include "mdg_kernels.cuh"
+
+namespace mdg {
+void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
+void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area0, double &area1);
+}
+
+using namespace mdg;
+
+struct mdg_solver {
+  int device = 0;
+  int ndim = 1;
+  int nprob = 0;
+  int precision = MDG_PREC_FP64;
+  cudaStream_t stream = nullptr;
+  std::vector<mdg_problem_desc> descs;
+  std::vector<ProbDev> hprobs;
+  ProbDev *d_probs = nullptr;
+  ProbTime *d_times = nullptr;
+  Tile *d_tiles = nullptr;
+  int ntiles = 0;
+  double *d_rc0 = nullptr, *d_rc1 = nullptr, *d_geo = nullptr;
+  Tables tb{};
+  double *d_state = nullptr;      // 10 arrays: P (5) then PH (5)
+  StateSoA P{}, PH{};
+  int64_t ncell_total = 0;
+  unsigned char *d_shock0 = nullptr;
+  double *d_stage = nullptr;      // AoS staging buffer, 5 doubles per zone of the largest problem
+  int64_t max_cells = 0;
+  int *d_err = nullptr;
+  bool timing = false;
+  cudaEvent_t ev[MDG_NTIMERS][2] = {};
+  double tms[MDG_NTIMERS] = {0, 0, 0, 0};
+  long long tcalls[MDG_NTIMERS] = {0, 0, 0, 0};
+};
+
+static thread_local std::string g_msg;
+
+static int fail(int code, const std::string &msg)
+{
+  g_msg = msg;
+  return code;
+}
+
+#define CK(call)                                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                         \
+      return fail(MDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+static int validate(const mdg_problem_desc &d, int ndim0, std::string &why)
+{
+  char buf[256];
+  auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
+  if (d.ndim != 1 && d.ndim != 2) return bad("ndim must be 1 or 2");
+  if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
+  if (d.n1 < 2 || d.n1 > (1 << 28)) return bad("n1 out of range [2, 2^28]");
+  if (d.ndim == 2 && (d.n2 < 2 || (int64_t)d.n1 * d.n2 > (int64_t)1 << 31)) return bad("n2 out of range");
+  if (d.eos != MDG_GAMMA_LAW && d.eos != MDG_POLYTROPIC) return bad("eos must be gamma-law or polytrope");
+  if (d.hydro_interp_order < 1 || d.hydro_interp_order > 3) return bad("hydro_interp_order must be 1, 2 or 3");
+  if (!(d.dx[0] > 0.0) || (d.ndim == 2 && !(d.dx[1] > 0.0))) return bad("dx must be positive");
+  if (!(d.gam > 1.0)) return bad("gam must exceed 1");
+  if (!(d.cfl > 0.0)) return bad("cfl must be positive");
+  if (d.ndim == 1) {
+    if (d.geom != MDG_CARTESIAN && d.geom != MDG_SPHERICAL) return bad("1-D geometry must be Cartesian or spherical");
+    int lo = d.bc_lo[0], hi = d.bc_hi[0];
+    bool lo_ok = lo == MDG_BC_OUTFLOW || lo == MDG_BC_REFLECT || lo == MDG_BC_EXTRAP || lo == MDG_BC_PERIODIC ||
+                 (lo == MDG_BC_PROB && d.geom == MDG_SPHERICAL && d.prob_kind == MDG_PROB_NOH) ||
+                 (lo == MDG_BC_SPHERICAL_ORIGIN && d.geom == MDG_SPHERICAL);
+    bool hi_ok = hi == MDG_BC_OUTFLOW || hi == MDG_BC_REFLECT || hi == MDG_BC_EXTRAP || hi == MDG_BC_PERIODIC ||
+                 (hi == MDG_BC_PROB && d.geom == MDG_SPHERICAL && d.prob_kind == MDG_PROB_NOH);
+    if (!lo_ok || !hi_ok) {
+      snprintf(buf, sizeof buf, "unsupported 1-D boundary kinds lo=%d hi=%d for geom=%d", lo, hi, d.geom);
+      why = buf;
+      return MDG_ERR_NOTIMPL;
+    }
+    if ((lo == MDG_BC_PERIODIC) != (hi == MDG_BC_PERIODIC)) return bad("periodic boundaries must be paired");
+    if (d.geom == MDG_SPHERICAL && (d.startx[0] != d.startx[0])) return bad("bad startx");
+  } else {
+    if (d.geom != MDG_CARTESIAN) {
+      why = "2-D grids are Cartesian in this version";
+      return MDG_ERR_NOTIMPL;
+    }
+    for (int dir = 0; dir < 2; dir++) {
+      int lo = d.bc_lo[dir], hi = d.bc_hi[dir];
+      auto ok = [&](int k) {
+        return k == MDG_BC_OUTFLOW || k == MDG_BC_REFLECT || k == MDG_BC_PERIODIC || (dir == 0 && k == MDG_BC_EXTRAP);
+      };
+      if (!ok(lo) || !ok(hi)) {
+        snprintf(buf, sizeof buf, "unsupported 2-D boundary kinds in direction %d: lo=%d hi=%d", dir, lo, hi);
+        why = buf;
+        return MDG_ERR_NOTIMPL;
+      }
+      if ((lo == MDG_BC_PERIODIC) != (hi == MDG_BC_PERIODIC)) return bad("periodic boundaries must be paired");
+    }
+  }
+  return MDG_OK;
+}
+
+static void free_all(mdg_solver *s)
+{
+  if (!s) return;
+  for (int k = 0; k < MDG_NTIMERS; k++)
+    for (int e = 0; e < 2; e++)
+      if (s->ev[k][e]) cudaEventDestroy(s->ev[k][e]);
+  cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles);
+  cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
+  cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_stage); cudaFree(s->d_err);
+  if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+extern "C" {
+
+int mdg_version(void) { return 100; }
+
+const char *mdg_error_string(int code)
+{
+  switch (code) {
+    case MDG_OK: return "ok";
+    case MDG_ERR_INVALID: return "invalid argument";
+    case MDG_ERR_INDEX: return "index out of range";
+    case MDG_ERR_NOTFOUND: return "not found";
+    case MDG_ERR_IO: return "i/o error";
+    case MDG_ERR_NOTIMPL: return "not implemented";
+    case MDG_ERR_OUTOFMEM: return "out of device memory";
+    case MDG_ERR_PARFILE: return "parameter error";
+    case MDG_ERR_LOGICAL: return "logical error";
+    case MDG_ERR_INTERNAL: return "internal error";
+    case MDG_ERR_CUDA: return "CUDA runtime error";
+    case MDG_ERR_NONFINITE: return "time step dropped below dtmin";
+    default: return "unknown status";
+  }
+}
+
+const char *mdg_last_error_message(void) { return g_msg.c_str(); }
+
+int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int device, mdg_solver **out)
+{
+  if (!descs || nprob <= 0 || !out) return fail(MDG_ERR_INVALID, "descs/nprob/out");
+  if (precision != MDG_PREC_FP64) return fail(MDG_ERR_NOTIMPL, "only MDG_PREC_FP64 is built into this solver entry point");
+  *out = nullptr;
+  const int ndim = descs[0].ndim;
+  for (int m = 0; m < nprob; m++) {
+    std::string why;
+    int rc = validate(descs[m], ndim, why);
+    if (rc != MDG_OK) return fail(rc, "problem " + std::to_string(m) + ": " + why);
+  }
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MDG_ERR_INVALID, "device ordinal out of range");
+  CK(cudaSetDevice(device));
+
+  mdg_solver *s = new mdg_solver();
+  s->device = device;
+  s->ndim = ndim;
+  s->nprob = nprob;
+  s->precision = precision;
+  s->descs.assign(descs, descs + nprob);
+
+  // layout: state offsets, table offsets, tiles
+  std::vector<Tile> tiles;
+  int64_t cell = 0, rc0 = 0, rc1 = 0, sh = 0;
+  for (int m = 0; m < nprob; m++) {
+    const mdg_problem_desc &d = descs[m];
+    ProbDev P;
+    memset(&P, 0, sizeof P);
+    P.ndim = d.ndim; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
+    P.n1 = d.n1; P.n2 = (d.ndim > 1) ? d.n2 : 1;
+    P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0]; P.bc_lo1 = d.bc_lo[1]; P.bc_hi1 = d.bc_hi[1];
+    P.prob_kind = d.prob_kind;
+    P.has_src = (d.geom == MDG_SPHERICAL);
+    P.cell_off = cell;
+    P.geo_off = rc0;
+    P.rc1_off = rc1;
+    P.sh_off = sh;
+    P.gam = d.gam; P.Kpoly = d.Kpoly;
+    P.dx0 = d.dx[0]; P.dx1 = d.dx[1];
+    if (d.ndim == 2) cartesian_2d_constants(d, P.vol, P.area0, P.area1);
+    P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
+    P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
+    s->hprobs.push_back(P);
+    const int64_t nc = (int64_t)P.n1 * P.n2;
+    if (nc > s->max_cells) s->max_cells = nc;
+    cell += nc;
+    rc0 += P.n1 + 2 * NG;
+    if (d.ndim == 2) {
+      rc1 += P.n2 + 2 * NG;
+      sh += (int64_t)(P.n1 + 3) * P.n2;
+      for (int i0 = 0; i0 < P.n1; i0 += TI2)
+        for (int j0 = 0; j0 < P.n2; j0 += TJ2) tiles.push_back(Tile{m, i0, j0, 0});
+    } else {
+      for (int i0 = 0; i0 < P.n1; i0 += TILE1) tiles.push_back(Tile{m, i0, 0, 0});
+    }
+  }
+  s->ncell_total = cell;
+  s->ntiles = (int)tiles.size();
+
+  // host tables
+  std::vector<double> h_rc0((size_t)RC_NFIELDS * rc0), h_rc1, h_geo;
+  if (ndim == 2) h_rc1.assign((size_t)RC_NFIELDS * rc1, 0.0);
+  else h_geo.assign((size_t)GF_NFIELDS * rc0, 0.0);
+  for (int m = 0; m < nprob; m++) {
+    build_recon_table(descs[m], 0, h_rc0.data(), rc0, s->hprobs[m].geo_off);
+    if (ndim == 2) build_recon_table(descs[m], 1, h_rc1.data(), rc1, s->hprobs[m].rc1_off);
+    else build_geo_1d(descs[m], h_geo.data(), rc0, s->hprobs[m].geo_off);
+  }
+
+  auto cleanup_fail = [&](int code) { free_all(s); delete s; return code; };
+#define CKC(call)                                                                     \
+  do {                                                                                \
+    cudaError_t e_ = (call);                                                          \
+    if (e_ != cudaSuccess) {                                                          \
+      fail(e_ == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA,         \
+           std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+      return cleanup_fail(e_ == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA); \
+    }                                                                                 \
+  } while (0)
+
+  CKC(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  CKC(cudaMalloc(&s->d_probs, sizeof(ProbDev) * nprob));
+  CKC(cudaMalloc(&s->d_times, sizeof(ProbTime) * nprob));
+  CKC(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->ntiles));
+  CKC(cudaMalloc(&s->d_rc0, sizeof(double) * h_rc0.size()));
+  if (ndim == 2) CKC(cudaMalloc(&s->d_rc1, sizeof(double) * h_rc1.size()));
+  else CKC(cudaMalloc(&s->d_geo, sizeof(double) * h_geo.size()));
+  CKC(cudaMalloc(&s->d_state, sizeof(double) * 2 * NPRIM * cell));
+  CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
+  CKC(cudaMalloc(&s->d_err, sizeof(int)));
+  if (ndim == 2) CKC(cudaMalloc(&s->d_shock0, sh > 0 ? sh : 1));
+
+  CKC(cudaMemcpy(s->d_probs, s->hprobs.data(), sizeof(ProbDev) * nprob, cudaMemcpyHostToDevice));
+  CKC(cudaMemcpy(s->d_tiles, tiles.data(), sizeof(Tile) * s->ntiles, cudaMemcpyHostToDevice));
+  CKC(cudaMemcpy(s->d_rc0, h_rc0.data(), sizeof(double) * h_rc0.size(), cudaMemcpyHostToDevice));
+  if (ndim == 2) CKC(cudaMemcpy(s->d_rc1, h_rc1.data(), sizeof(double) * h_rc1.size(), cudaMemcpyHostToDevice));
+  else CKC(cudaMemcpy(s->d_geo, h_geo.data(), sizeof(double) * h_geo.size(), cudaMemcpyHostToDevice));
+  CKC(cudaMemset(s->d_state, 0, sizeof(double) * 2 * NPRIM * cell));
+  CKC(cudaMemset(s->d_err, 0, sizeof(int)));
+  if (ndim == 2) CKC(cudaMemset(s->d_shock0, 0, sh > 0 ? sh : 1));
+  CKC(cudaMemset(s->d_times, 0, sizeof(ProbTime) * nprob));
+  for (int v = 0; v < NPRIM; v++) {
+    s->P.v[v] = s->d_state + (int64_t)v * cell;
+    s->PH.v[v] = s->d_state + (int64_t)(NPRIM + v) * cell;
+  }
+  s->tb.rc0 = s->d_rc0; s->tb.rc0_stride = rc0;
+  s->tb.rc1 = s->d_rc1; s->tb.rc1_stride = rc1;
+  s->tb.geo = s->d_geo; s->tb.geo_stride = rc0;
+#undef CKC
+  *out = s;
+  return MDG_OK;
+}
+
+int mdg_upload_state(mdg_solver *s, int prob, const double *prim)
+{
+  if (!s || !prim) return fail(MDG_ERR_INVALID, "solver/prim");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  CK(cudaSetDevice(s->device));
+  const ProbDev &P = s->hprobs[prob];
+  const int64_t n = (int64_t)P.n1 * P.n2;
+  CK(cudaMemcpyAsync(s->d_stage, prim, sizeof(double) * NPRIM * n, cudaMemcpyHostToDevice, s->stream));
+  launch_aos_to_soa(s->d_stage, s->P, P.cell_off, n, s->stream);
+  launch_reset_time(s->d_times, prob, s->stream);
+  launch_initial_estimate_one(s->d_probs, s->d_times, prob, n, s->tb, s->P, s->stream);
+  CK(cudaGetLastError());
+  return MDG_OK;
+}
+
+static int queue_steps(mdg_solver *s, int nsteps)
+{
+  auto mark = [&](int k, int e) { if (s->timing) cudaEventRecord(s->ev[k][e], s->stream); };
+  for (int k = 0; k < nsteps; k++) {
+    mark(MDG_TIMER_DT, 0);
+    launch_dt_finalize(s->d_probs, s->d_times, s->nprob, s->d_err, s->stream);
+    mark(MDG_TIMER_DT, 1);
+    mark(MDG_TIMER_STAGE0, 0);
+    if (s->ndim == 1)
+      launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
+    else
+      launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->d_shock0, s->stream);
+    mark(MDG_TIMER_STAGE0, 1);
+    mark(MDG_TIMER_STAGE1, 0);
+    if (s->ndim == 1)
+      launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
+    else
+      launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->d_shock0, s->stream);
+    mark(MDG_TIMER_STAGE1, 1);
+    mark(MDG_TIMER_FINISH, 0);
+    launch_finish(s->d_times, s->nprob, s->stream);
+    mark(MDG_TIMER_FINISH, 1);
+    if (s->timing) {
+      CK(cudaStreamSynchronize(s->stream));
+      for (int t = 0; t < MDG_NTIMERS; t++) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, s->ev[t][0], s->ev[t][1]));
+        s->tms[t] += ms;
+        s->tcalls[t] += 1;
+      }
+    }
+  }
+  CK(cudaGetLastError());
+  return MDG_OK;
+}
+
+int mdg_estimate_dt(mdg_solver *s, double *dt_out)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  CK(cudaSetDevice(s->device));
+  launch_dt_finalize(s->d_probs, s->d_times, s->nprob, s->d_err, s->stream);
+  CK(cudaGetLastError());
+  if (dt_out) {
+    std::vector<ProbTime> T(s->nprob);
+    CK(cudaMemcpyAsync(T.data(), s->d_times, sizeof(ProbTime) * s->nprob, cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    for (int m = 0; m < s->nprob; m++) dt_out[m] = T[m].dt;
+  }
+  return MDG_OK;
+}
+
+int mdg_step(mdg_solver *s, int nsteps)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  if (nsteps < 0) return fail(MDG_ERR_INVALID, "nsteps < 0");
+  CK(cudaSetDevice(s->device));
+  return queue_steps(s, nsteps);
+}
+
+int mdg_download_state(mdg_solver *s, int prob, double *prim, double *eos)
+{
+  if (!s || !prim) return fail(MDG_ERR_INVALID, "solver/prim");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  CK(cudaSetDevice(s->device));
+  const ProbDev &P = s->hprobs[prob];
+  const int64_t n = (int64_t)P.n1 * P.n2;
+  launch_soa_to_aos(s->P, P.cell_off, n, s->d_stage, s->stream);
+  CK(cudaMemcpyAsync(prim, s->d_stage, sizeof(double) * NPRIM * n, cudaMemcpyDeviceToHost, s->stream));
+  if (eos) {
+    ProbTime T;
+    CK(cudaMemcpyAsync(&T, s->d_times + prob, sizeof(ProbTime), cudaMemcpyDeviceToHost, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    // the reference's sim_eos holds the EOS of the last stage state (update_eos(sim_ph))
+    launch_eos_aos_m(T.istep > 0 ? s->PH : s->P, s->d_probs, prob, P.cell_off, n, s->d_stage, s->stream);
+    CK(cudaMemcpyAsync(eos, s->d_stage, sizeof(double) * NPRIM * n, cudaMemcpyDeviceToHost, s->stream));
+  }
+  CK(cudaStreamSynchronize(s->stream));
+  CK(cudaGetLastError());
+  return MDG_OK;
+}
+
+int mdg_get_time(mdg_solver *s, int prob, double *t, double *dt_last, int *istep)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  CK(cudaSetDevice(s->device));
+  ProbTime T;
+  CK(cudaMemcpyAsync(&T, s->d_times + prob, sizeof(ProbTime), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  if (t) *t = T.t;
+  if (dt_last) *dt_last = T.dt;
+  if (istep) *istep = T.istep;
+  return MDG_OK;
+}
+
+int mdg_get_stream(mdg_solver *s, void **stream)
+{
+  if (!s || !stream) return fail(MDG_ERR_INVALID, "solver/stream");
+  *stream = (void *)s->stream;
+  return MDG_OK;
+}
+
+int mdg_synchronize(mdg_solver *s)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize(s->stream));
+  int err = 0;
+  CK(cudaMemcpy(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (err) return fail(err, "a time step estimate dropped below dtmin");
+  return MDG_OK;
+}
+
+int mdg_set_timing(mdg_solver *s, int enable)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  CK(cudaSetDevice(s->device));
+  if (enable && !s->ev[0][0]) {
+    for (int k = 0; k < MDG_NTIMERS; k++)
+      for (int e = 0; e < 2; e++) CK(cudaEventCreate(&s->ev[k][e]));
+  }
+  s->timing = enable != 0;
+  for (int k = 0; k < MDG_NTIMERS; k++) { s->tms[k] = 0.0; s->tcalls[k] = 0; }
+  return MDG_OK;
+}
+
+int mdg_get_timers(mdg_solver *s, double *ms, long long *calls)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  for (int k = 0; k < MDG_NTIMERS; k++) {
+    if (ms) ms[k] = s->tms[k];
+    if (calls) calls[k] = s->tcalls[k];
+  }
+  return MDG_OK;
+}
+
+int mdg_destroy(mdg_solver *s)
+{
+  if (!s) return MDG_OK;
+  cudaSetDevice(s->device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_all(s);
+  delete s;
+  return MDG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,223 @@
+// Host-side geometry tables of the sweep, rebuilt from the problem description exactly
+// as the reference's init_geometry() builds them (geometry.c:4-63), and reduced to the
+// per-index tables the kernels read.
+//
+//   Cartesian: metrics/metric_cartesian.c:47-55 (volume moments), 127-295 (volume,
+//              area, gcov, gcon, scale; conn = 0)
+//   Spherical, 1-D, uniform radius (RCOORD=UNIFORM, THCOORD=UNIFORM):
+//              metrics/metric_spherical_general.c:149-243 (maps), 558-568 (moments),
+//              708-740 (volume), 745-779 (area), 820-930 (conn), 941-1051 (gcov, gcon,
+//              scale); Romberg integration as utils.c:16-62.
+//
+// Compiled with -ffp-contract=off so that every product and sum rounds as in the
+// reference's CPU build.
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "mdg_internal.h"
+#include "../../include/medusa_b200.h"
+
+namespace mdg {
+
+// ----------------------------------------------------------------- Romberg (utils.c:16-62)
+static double rtrap(double x0, double x1, int rstage, double (*f)(double))
+{
+  unsigned long long nseg = 1ULL << rstage, i;
+  double dx = (x1 - x0) / nseg, sum = 0.0;
+  if (rstage == 0) return 0.5 * dx * ((*f)(x0) + (*f)(x1));
+  for (i = 0; i < (1ULL << (rstage - 1)); i++) sum += (*f)(x0 + (2 * i + 1) * dx);
+  return dx * sum;
+}
+
+static double romb(double x0, double x1, double (*f)(double))
+{
+  double rvec[16], R0, R1;
+  unsigned long long fm;
+  rvec[0] = rtrap(x0, x1, 0, f);
+  for (int rstage = 1; rstage <= 15; rstage++) {
+    R0 = rvec[0];
+    rvec[0] = 0.5 * R0 + rtrap(x0, x1, rstage, f);
+    for (int m = 1; m <= rstage; m++) {
+      fm = 1ULL << (2 * m);
+      R1 = rvec[m];
+      rvec[m] = 1.0 / (fm - 1) * (fm * rvec[m - 1] - R0);
+      R0 = R1;
+    }
+    if (std::fabs((rvec[rstage] - rvec[rstage - 1]) / rvec[rstage]) < 1.e-15 ||
+        (rstage > 2 && std::fabs(rvec[rstage]) < 1.e-15))
+      return rvec[rstage];
+  }
+  return rvec[15];
+}
+
+// uniform-radius / uniform-theta maps and the integrands of the spherical metric
+static double r_of_x(double x) { return std::fabs(x); }
+static double dr_dx(double) { return 1.0; }
+static double d2r_dx2(double) { return 0.0; }
+static double th_of_x(double x)
+{
+  if (x < -1.0) x = -2.0 - x;
+  if (x > 1.0) x = 2.0 - x;
+  return 0.5 * M_PI * (x + 1.0);
+}
+static double dth_dx(double) { return 0.5 * M_PI; }
+static double d2th_dx2(double) { return 0.0; }
+static double f_r2dr_dx(double x) { return std::pow(r_of_x(x), 2) * dr_dx(x); }
+static double f_xr1g(double x) { return x * std::pow(r_of_x(x), 2) * dr_dx(x); }
+static double f_xr2g(double x) { return x * x * std::pow(r_of_x(x), 2) * dr_dx(x); }
+static double f_r2d2r_dx2(double x) { return std::pow(r_of_x(x), 2) * d2r_dx2(x); }
+static double f_r3(double x) { return std::pow(r_of_x(x), 3); }
+static double f_r2dr_dx3(double x) { return std::pow(r_of_x(x), 2) * std::pow(dr_dx(x), 3); }
+static double f_rdr_dx2(double x) { return r_of_x(x) * std::pow(dr_dx(x), 2); }
+static double f_sthdth_dx(double x) { return std::sin(th_of_x(x)) * dth_dx(x); }
+static double f_sthdth_dx3(double x) { return std::sin(th_of_x(x)) * std::pow(dth_dx(x), 3); }
+static double f_sth3dth_dx(double x) { return std::pow(std::sin(th_of_x(x)), 3) * dth_dx(x); }
+static double f_sthd2th_dx2(double x) { return std::sin(th_of_x(x)) * d2th_dx2(x); }
+static double f_cthdth_dx2(double x) { return std::cos(th_of_x(x)) * std::pow(dth_dx(x), 2); }
+
+// Volume moments alpha/beta/Gamma of direction d over i in [-NG, n+NG), stored at i+NG.
+void build_moments(const mdg_problem_desc &d, int dir, std::vector<double> &al,
+                   std::vector<double> &be, std::vector<double> &ga)
+{
+  const int n = (dir == 0) ? d.n1 : (dir == 1 ? d.n2 : d.n3);
+  al.assign(n + 2 * NG, 0.0); be.assign(n + 2 * NG, 0.0); ga.assign(n + 2 * NG, 0.0);
+  for (int i = -NG; i < n + NG; i++) {
+    if (d.geom == MDG_CARTESIAN) {
+      double x0 = d.startx[dir] + i * d.dx[dir], x1 = x0 + d.dx[dir];
+      al[i + NG] = (x1 * x1 * x1 - x0 * x0 * x0) / 3.0;
+      be[i + NG] = (x1 * x1 - x0 * x0) / 2.0;
+      ga[i + NG] = d.dx[dir];
+    } else {
+      double x0 = d.startx[0] + i * d.dx[0], x1 = d.startx[0] + (i + 1) * d.dx[0];
+      ga[i + NG] = romb(x0, x1, f_r2dr_dx);
+      be[i + NG] = romb(x0, x1, f_xr1g);
+      al[i + NG] = romb(x0, x1, f_xr2g);
+    }
+  }
+}
+
+// Reconstruction coefficient table (RC_NFIELDS x stride, starting at column `off`) for the
+// zones of direction dir: zone i at column off+i+NG, i in [-NG, n+NG).
+void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off)
+{
+  std::vector<double> al, be, ga;
+  build_moments(d, dir, al, be, ga);
+  const int n = (dir == 0) ? d.n1 : d.n2;
+  for (int i = -NG; i < n + NG; i++) {
+    int im = (i - 1 < -NG) ? -NG : i - 1, ip = (i + 1 >= n + NG) ? n + NG - 1 : i + 1;
+    double am = al[im + NG], a0 = al[i + NG], ap = al[ip + NG];
+    double bm = be[im + NG], b0 = be[i + NG], bp = be[ip + NG];
+    double gm = ga[im + NG], g0 = ga[i + NG], gp = ga[ip + NG];
+    // zone edges as prim_to_fluxesN forms them: startx + index*dx (step.c:509,736)
+    double xl = d.startx[dir] + i * d.dx[dir];
+    double xr = d.startx[dir] + (i + 1) * d.dx[dir];
+    double a0b1g2 = am * b0 * gp, a0b2g1 = am * bp * g0, a1b0g2 = a0 * bm * gp;
+    double a1b2g0 = a0 * bp * gm, a2b0g1 = ap * bm * g0, a2b1g0 = ap * b0 * gm;
+    double den1 = 1.0 / (a0b1g2 + a1b2g0 + a2b0g1 - a0b2g1 - a1b0g2 - a2b1g0);
+    double den2 = (xl - xr) * (a0 + g0 * xl * xr - b0 * (xl + xr));
+    den2 = 1.0 / den2;
+    double xm = bm / gm, xp = bp / gp, xc = b0 / g0;
+    double v[RC_NFIELDS];
+    v[RC_AM] = am; v[RC_A0] = a0; v[RC_AP] = ap;
+    v[RC_BM] = bm; v[RC_B0] = b0; v[RC_BP] = bp;
+    v[RC_GM] = gm; v[RC_G0] = g0; v[RC_GP] = gp;
+    v[RC_XL] = xl; v[RC_XR] = xr;
+    v[RC_DEN1] = den1; v[RC_DEN2] = den2;
+    v[RC_XLR] = xl - xr;
+    v[RC_XL2] = xl * xl; v[RC_XR2] = xr * xr;
+    v[RC_XMID] = 0.5 * (xl + xr);
+    v[RC_DMR] = a0 + xr * (g0 * xr - 2.0 * b0);
+    v[RC_DML] = a0 + xl * (g0 * xl - 2.0 * b0);
+    v[RC_LSM] = xc - 0.5 * (xl + xm);
+    v[RC_LSP] = 0.5 * (xr + xp) - xc;
+    v[RC_LSC] = xp - xm;
+    for (int f = 0; f < RC_NFIELDS; f++) tab[f * stride + off + i + NG] = v[f];
+  }
+}
+
+// Face and zone geometry of a 1-D problem (GF_NFIELDS x stride, starting at column off).
+void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off)
+{
+  const int n1 = d.n1;
+  auto put = [&](int f, int i, double v) { tab[f * stride + off + i + NG] = v; };
+  for (int i = -NG; i < n1 + NG; i++)
+    for (int f = 0; f < GF_NFIELDS; f++) put(f, i, 0.0);
+  if (d.geom == MDG_CARTESIAN) {
+    for (int i = -NG; i < n1 + NG; i++) {
+      double vol = 1.0;
+      vol *= d.dx[0];
+      double area = 1.0;
+      area *= d.dx[0];
+      area /= d.dx[0];
+      put(GF_VOL, i, vol);
+      put(GF_AREA, i, (i >= 0 && i <= n1) ? area : 0.0);
+      put(GF_FSCALE, i, 1.0);
+      put(GF_FG0, i, 1.0); put(GF_FG1, i, 1.0); put(GF_FG2, i, 1.0);
+      put(GF_G0, i, 1.0); put(GF_G1, i, 1.0); put(GF_G2, i, 1.0);
+      put(GF_GC0, i, 1.0); put(GF_GC1, i, 1.0); put(GF_GC2, i, 1.0);
+      put(GF_S00, i, 1.0);
+    }
+    return;
+  }
+  // spherical 1-D: x1 in [-1,1], dx[1] = 2, dx[2] = 2 pi (init_coords)
+  const double x1lo = -1.0, x1hi = 1.0, dph = 2.0 * M_PI;
+  double vthf = romb(x1lo, x1hi, f_sthdth_dx);
+  double th_sthdth_dx3 = romb(x1lo, x1hi, f_sthdth_dx3);
+  double th_sth3dth_dx = romb(x1lo, x1hi, f_sth3dth_dx);
+  double th_sthd2th_dx2 = romb(x1lo, x1hi, f_sthd2th_dx2);
+  double th_cthdth_dx2 = romb(x1lo, x1hi, f_cthdth_dx2);
+  for (int i = -NG; i < n1 + NG; i++) {
+    double x0lo = d.startx[0] + i * d.dx[0], x0hi = d.startx[0] + (i + 1) * d.dx[0];
+    double r2dr_int = romb(x0lo, x0hi, f_r2dr_dx);
+    double vrf = r2dr_int;
+    double rint_r2dr_dx3 = romb(x0lo, x0hi, f_r2dr_dx3);
+    put(GF_VOL, i, r2dr_int * vthf * 1 * dph);
+    put(GF_AREA, i, (i >= 0 && i <= n1) ? f_r2dr_dx(x0lo) * vthf * (1 * dph) : 0.0);
+    double g00 = rint_r2dr_dx3 / vrf;
+    double g01 = std::fabs(0.2 * (std::pow(r_of_x(x0hi), 5) - std::pow(r_of_x(x0lo), 5)) / vrf * th_sthdth_dx3 / vthf);
+    double g02 = std::fabs(0.2 * (std::pow(r_of_x(x0hi), 5) - std::pow(r_of_x(x0lo), 5)) / vrf * th_sth3dth_dx / vthf);
+    double g10 = std::pow(dr_dx(x0lo), 2);
+    double g11 = std::pow(r_of_x(x0lo), 2) * th_sthdth_dx3 / vthf;
+    double g12 = std::pow(r_of_x(x0lo), 2) * th_sth3dth_dx / vthf;
+    put(GF_G0, i, g00); put(GF_G1, i, g01); put(GF_G2, i, g02);
+    put(GF_FG0, i, g10); put(GF_FG1, i, g11); put(GF_FG2, i, g12);
+    put(GF_GC0, i, (std::fabs(g00) > 1.0e-50) ? 1.0 / g00 : 0.0);
+    put(GF_GC1, i, (std::fabs(g01) > 1.0e-50) ? 1.0 / g01 : 0.0);
+    put(GF_GC2, i, (std::fabs(g02) > 1.0e-50) ? 1.0 / g02 : 0.0);
+    put(GF_S00, i, std::sqrt(g00));
+    put(GF_FSCALE, i, std::sqrt(g10));
+    if (i >= 0 && i < n1) {
+      double c[3][3][3];
+      std::memset(c, 0, sizeof c);
+      double rint_r2d2r_dx2 = romb(x0lo, x0hi, f_r2d2r_dx2);
+      double rint_r3 = romb(x0lo, x0hi, f_r3);
+      double rint_rdr_dx2 = romb(x0lo, x0hi, f_rdr_dx2);
+      double vr = romb(x0lo, x0lo + d.dx[0], f_r2dr_dx);
+      c[0][0][0] = rint_r2d2r_dx2 / vr;
+      c[0][1][1] = -(rint_r3 / vr) * (th_sthdth_dx3 / vthf);
+      c[1][0][1] = rint_rdr_dx2 / vr;
+      c[1][1][0] = c[1][0][1];
+      c[2][0][2] = c[1][0][1];
+      c[2][2][0] = c[2][0][2];
+      c[2][1][2] = th_cthdth_dx2 / vthf;
+      c[2][2][1] = c[2][1][2];
+      c[0][2][2] = -c[2][2][0] * g02 / g00;
+      c[1][2][2] = -c[2][2][1] * g02 / g01;
+      c[1][1][1] = th_sthd2th_dx2 / vthf;
+      for (int l = 0; l < 3; l++)
+        for (int m = 0; m < 3; m++)
+          for (int nn = 0; nn < 3; nn++) put(GF_CONN + (l * 9 + m * 3 + nn), i, c[l][m][nn]);
+    }
+  }
+}
+
+// Cartesian 2-D constants: volume = dx0*dx1, area[loc] = (dx0*dx1)/dx[loc]
+// (metric_cartesian.c:127-189, loop order of init_volume/init_area).
+void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area0, double &area1)
+{
+  vol = 1.0; vol *= d.dx[0]; vol *= d.dx[1];
+  area0 = 1.0; area0 *= d.dx[0]; area0 *= d.dx[1]; area0 /= d.dx[0];
+  area1 = 1.0; area1 *= d.dx[0]; area1 *= d.dx[1]; area1 /= d.dx[1];
+}
+
+}  // namespace mdg

@@ -1,0 +1,93 @@
+// Internal data structures shared by the host code (mdg_capi.cu, mdg_geometry.cpp) and
+// the sweep kernels.  Not part of the public ABI.
+#pragma once
+#include <stdint.h>
+#include "../../include/medusa_b200.h"
+
+#ifdef __CUDACC__
+#define MDG_HD __host__ __device__
+#else
+#define MDG_HD
+#endif
+
+namespace mdg {
+
+constexpr int NG = 2;       // ghost layers (decs.h:61)
+constexpr int NPRIM = 5;    // rho, u, v1, v2, v3 (decs.h:57)
+enum { RHO = 0, UU = 1, U1 = 2, U2 = 3, U3 = 4 };
+enum { BC_OUTFLOW = 0, BC_REFLECT = 1, BC_EXTRAP = 2, BC_PERIODIC = 3, BC_PROB = 4,
+       BC_SPHERICAL_ORIGIN = 5 };
+
+// Per-zone reconstruction coefficients along one direction: the geometry-only
+// sub-expressions of para_recon (reconstruct.c:151-157,174-175) and lin_recon
+// (reconstruct.c:100-104), precomputed on the host in the reference's operation order.
+enum ReconField {
+  RC_AM, RC_A0, RC_AP,        // alpha[i-1], alpha[i], alpha[i+1]
+  RC_BM, RC_B0, RC_BP,        // beta
+  RC_GM, RC_G0, RC_GP,        // Gamma
+  RC_XL, RC_XR,               // x[i], x[i+1] (zone edges)
+  RC_DEN1,                    // 1/(a0b1g2 + a1b2g0 + a2b0g1 - a0b2g1 - a1b0g2 - a2b1g0)
+  RC_DEN2,                    // 1/((x[i]-x[i+1])*(alpha[i] + Gamma[i]x[i]x[i+1] - beta[i](x[i]+x[i+1])))
+  RC_XLR,                     // x[i]-x[i+1]
+  RC_XL2, RC_XR2,             // SQR(x[i]), SQR(x[i+1])
+  RC_XMID,                    // 0.5*(x[i]+x[i+1])
+  RC_DMR, RC_DML,             // alpha + xhi*(Gamma*xhi - 2 beta), alpha + xlo*(Gamma*xlo - 2 beta)
+  RC_LSM, RC_LSP, RC_LSC,     // lin_recon denominators x0-0.5(x[i]+xm), 0.5(x[i+1]+xp)-x0, xp-xm
+  RC_NFIELDS
+};
+
+// Per-face and per-zone geometry of 1-D problems (one record per index i+NG).
+enum GeoField {
+  GF_AREA,                    // face i: area[0]
+  GF_FSCALE,                  // face i: scale[1][0]
+  GF_FG0, GF_FG1, GF_FG2,     // face i: gcov[1][0..2]
+  GF_VOL,                     // zone i: volume
+  GF_G0, GF_G1, GF_G2,        // zone i: gcov[0][0..2]
+  GF_GC0, GF_GC1, GF_GC2,     // zone i: gcon[0..2]
+  GF_S00,                     // zone i: scale[0][0]
+  GF_CONN,                    // zone i: conn[l][m][n], 27 consecutive fields
+  GF_NFIELDS = GF_CONN + 27
+};
+
+// Device-side description of one problem.
+struct ProbDev {
+  int ndim, geom, eos, interp_order;
+  int n1, n2;
+  int bc_lo0, bc_hi0, bc_lo1, bc_hi1;
+  int prob_kind;
+  int has_src;              // spherical: geometric source terms are computed
+  int64_t cell_off;         // first zone of this problem in the state arrays
+  int64_t geo_off;          // first record (i=-NG) in the 1-D geometry tables
+  int64_t rc1_off;          // first record (j=-NG) of the direction-1 recon table (2-D)
+  int64_t sh_off;           // first byte of the first-stage shock bits (2-D)
+  double gam, Kpoly;
+  double dx0, dx1;
+  double area0, area1, vol; // Cartesian 2-D constants
+  double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
+};
+
+// Time bookkeeping of one problem, resident on the device.
+struct ProbTime {
+  double t;          // time of the state
+  double dt;         // dt of the step in progress / last step
+  double dtold;      // main.c dtold
+  double t_bc1;      // t + dt: time seen by the second-stage boundaries (bc.c:721)
+  double t_next;     // ((t + dt) - dt) + dt, the reference's t after the step
+  unsigned long long minacc;   // order-preserving encoding of the running min_dt
+  int istep;
+  int dt_ready;      // dt of the next step already finalized
+};
+
+// Order-preserving map from double to uint64 so atomicMin on the integer is a min on
+// the double (negative values and infinities included).
+MDG_HD inline unsigned long long dbl_to_ord(double x) {
+  union { double d; unsigned long long u; } c; c.d = x;
+  return (c.u & 0x8000000000000000ULL) ? ~c.u : (c.u | 0x8000000000000000ULL);
+}
+MDG_HD inline double ord_to_dbl(unsigned long long u) {
+  union { double d; unsigned long long u; } c;
+  c.u = (u & 0x8000000000000000ULL) ? (u & 0x7FFFFFFFFFFFFFFFULL) : ~u;
+  return c.d;
+}
+
+}  // namespace mdg

@@ -1,0 +1,47 @@
+// Shared declarations of the sweep kernels and their launch helpers.
+#pragma once
+#include <cuda_runtime.h>
+#include "mdg_internal.h"
+
+namespace mdg {
+
+// Structure-of-arrays state of all problems of a solver: v[var][zone], zones of problem m
+// at [cell_off, cell_off + n1*n2), i-major, no ghost storage (boundaries are applied on
+// the fly as index maps).
+struct StateSoA { double *v[NPRIM]; };
+
+struct Tables {
+  const double *rc0;     // direction-0 reconstruction table, RC_NFIELDS x rc0_stride
+  int64_t rc0_stride;
+  const double *rc1;     // direction-1 reconstruction table (2-D)
+  int64_t rc1_stride;
+  const double *geo;     // 1-D face/zone geometry, GF_NFIELDS x geo_stride
+  int64_t geo_stride;
+};
+
+// One work tile: problem, first output row i0, first output column j0 (2-D).
+struct Tile { int prob; int i0; int j0; int pad; };
+
+constexpr int NT1 = 128;          // threads per 1-D tile (126 output zones)
+constexpr int TILE1 = NT1 - 2;
+constexpr int NT2 = 128;          // threads per 2-D tile (126 output columns)
+constexpr int TJ2 = NT2 - 2;
+constexpr int TI2 = 32;           // output rows per 2-D tile
+
+void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
+                    const Tables &tb, StateSoA stage_state, StateSoA state_n, StateSoA out,
+                    cudaStream_t st);
+void launch_stage2d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
+                    const Tables &tb, StateSoA stage_state, StateSoA state_n, StateSoA out,
+                    unsigned char *shock0, cudaStream_t st);
+void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st);
+void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
+void launch_reset_time(ProbTime *times, int m, cudaStream_t st);
+void launch_initial_estimate_one(const ProbDev *probs, ProbTime *times, int m, int64_t ncell,
+                                 const Tables &tb, StateSoA s, cudaStream_t st);
+void launch_aos_to_soa(const double *aos, StateSoA s, int64_t off, int64_t n, cudaStream_t st);
+void launch_soa_to_aos(StateSoA s, int64_t off, int64_t n, double *aos, cudaStream_t st);
+void launch_eos_aos_m(StateSoA s, const ProbDev *probs, int m, int64_t off, int64_t n, double *aos,
+                      cudaStream_t st);
+
+}  // namespace mdg

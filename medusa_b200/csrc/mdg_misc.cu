@@ -1,0 +1,162 @@
+// Small kernels around the sweep: time-step control (estimate_dt + main.c rules), time
+// bookkeeping, the first estimate before step 0, and AoS <-> SoA staging of the state.
+#include "mdg_hydro.cuh"
+#include "mdg_kernels.cuh"
+
+namespace mdg {
+
+// estimate_dt() (step.c:192-198) applied to the accumulated minimum, then the safety,
+// growth and end-time rules of main.c:239-251.  One thread per problem.
+__global__ void dt_finalize_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, int nprob,
+                                   int *err)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nprob) return;
+  ProbTime T = times[m];
+  if (T.dt_ready) return;
+  const ProbDev &P = probs[m];
+  double min_dt = ord_to_dbl(T.minacc);
+  if (T.istep == 0) min_dt = tmin(min_dt, P.initial_dt);
+  min_dt = tmin(min_dt, P.dtmax);
+  min_dt *= P.cfl;
+  // main.c:229-238 aborts the run when the estimate drops below dtmin; here the
+  // condition is recorded for the host (mdg_synchronize returns MDG_ERR_NONFINITE)
+  if (!(min_dt >= P.dtmin)) atomicExch(err, MDG_ERR_NONFINITE);
+  double dt = min_dt;
+  if (T.istep == 0) dt *= P.dt_init_safety;
+  else dt = tmin(T.dtold * P.dt_grow_safety, dt);
+  T.dtold = dt;
+  if (T.t + 1 * dt > P.tmax) dt = 1.000000001 * (P.tmax - T.t) / 1;
+  if (dt < P.dtmin) dt = P.dtmin;
+  T.dt = dt;
+  T.t_bc1 = T.t + dt;                  // reset_boundaries_gpu: t += dt (bc.c:721)
+  T.t_next = (T.t_bc1 - dt) + dt;      // ... t -= dt (bc.c:1418), then main.c:263 t += dt
+  T.minacc = dbl_to_ord(1.0e100);      // step.c:49
+  T.dt_ready = 1;
+  times[m] = T;
+}
+
+__global__ void finish_kernel(ProbTime *__restrict__ times, int nprob)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nprob) return;
+  times[m].t = times[m].t_next;
+  times[m].istep += 1;
+  times[m].dt_ready = 0;
+}
+
+// First estimate_dt() of a problem (step.c:171-187 with firstc): zone terms of the
+// initial state with its own EOS (main.c:180-182 fills sim_eos from sim_p).
+__global__ void initial_estimate_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, int m,
+                                        Tables tb, StateSoA s)
+{
+  __shared__ double sred[32];
+  const ProbDev &P = probs[m];
+  const int64_t ncell = (int64_t)P.n1 * P.n2;
+  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double lmin = 1.0e300;
+  if (z < ncell) {
+    const int64_t c = P.cell_off + z;
+    const double rho = s.v[RHO][c], uu = s.v[UU][c];
+    const double press = eos_press(P.eos, P.gam, P.Kpoly, rho, uu);
+    const double cs = sqrt(P.gam * press / rho);
+    double local_dt = 0.0;
+    if (P.ndim == 1) {
+      const double s00 = __ldg(tb.geo + GF_S00 * tb.geo_stride + P.geo_off + z + NG);
+      local_dt += (fabs(s.v[U1][c]) + cs / s00) / P.dx0;
+      lmin = tmin(lmin, 1.0 / local_dt);
+    } else {
+      local_dt += (fabs(s.v[U1][c]) + cs) / P.dx0;
+      lmin = tmin(lmin, 1.0 / local_dt);
+      local_dt += (fabs(s.v[U2][c]) + cs) / P.dx1;
+      lmin = tmin(lmin, 1.0 / local_dt);
+    }
+  }
+  block_min_to(lmin, &times[m].minacc, sred);
+}
+
+__global__ void reset_time_kernel(ProbTime *times, int m)
+{
+  ProbTime T;
+  T.t = 0.0; T.dt = 0.0; T.dtold = 1.0e100; T.t_bc1 = 0.0; T.t_next = 0.0;
+  T.minacc = dbl_to_ord(1.0e100);
+  T.istep = 0; T.dt_ready = 0;
+  times[m] = T;
+}
+
+__global__ void aos_to_soa_kernel(const double *__restrict__ aos, StateSoA s, int64_t off, int64_t n)
+{
+  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) s.v[v][off + z] = aos[z * NPRIM + v];
+}
+
+__global__ void soa_to_aos_kernel(StateSoA s, int64_t off, int64_t n, double *__restrict__ aos)
+{
+  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) aos[z * NPRIM + v] = s.v[v][off + z];
+}
+
+// EOS record of each zone (PRESS, CS, TEMP, ENT, GAMMA), eos_gamma.c:45-58 / eos_poly.c:56-69
+__global__ void eos_aos_kernel(StateSoA s, const ProbDev *__restrict__ probs, int m, int64_t off, int64_t n,
+                               double *__restrict__ aos)
+{
+  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  const ProbDev &P = probs[m];
+  const double rho = s.v[RHO][off + z], uu = s.v[UU][off + z];
+  const double press = eos_press(P.eos, P.gam, P.Kpoly, rho, uu);
+  const double cs = sqrt(P.gam * press / rho);
+  const double kb = 1.3806488e-16, mp = 1.67262158e-24, me = 9.10938291e-28;
+  const double tp = (P.eos == 0) ? press / (2.0 * rho * kb) * (mp + me) : press / (rho * kb) * mp;
+  aos[z * 5 + 0] = press;
+  aos[z * 5 + 1] = cs;
+  aos[z * 5 + 2] = tp;
+  aos[z * 5 + 3] = 0.0;
+  aos[z * 5 + 4] = P.gam;
+}
+
+void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st)
+{
+  dt_finalize_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(probs, times, nprob, err);
+}
+
+void launch_finish(ProbTime *times, int nprob, cudaStream_t st)
+{
+  finish_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(times, nprob);
+}
+
+void launch_reset_time(ProbTime *times, int m, cudaStream_t st)
+{
+  reset_time_kernel<<<1, 1, 0, st>>>(times, m);
+}
+
+void launch_initial_estimate_one(const ProbDev *probs, ProbTime *times, int m, int64_t ncell,
+                                 const Tables &tb, StateSoA s, cudaStream_t st)
+{
+  const int nb = (int)((ncell + 255) / 256);
+  initial_estimate_kernel<<<nb, 256, 0, st>>>(probs, times, m, tb, s);
+}
+
+void launch_aos_to_soa(const double *aos, StateSoA s, int64_t off, int64_t n, cudaStream_t st)
+{
+  if (n <= 0) return;
+  aos_to_soa_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(aos, s, off, n);
+}
+
+void launch_soa_to_aos(StateSoA s, int64_t off, int64_t n, double *aos, cudaStream_t st)
+{
+  if (n <= 0) return;
+  soa_to_aos_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s, off, n, aos);
+}
+
+void launch_eos_aos_m(StateSoA s, const ProbDev *probs, int m, int64_t off, int64_t n, double *aos, cudaStream_t st)
+{
+  if (n <= 0) return;
+  eos_aos_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(s, probs, m, off, n, aos);
+}
+
+}  // namespace mdg

@@ -1,0 +1,236 @@
+// Fused 1-D RK stage kernel (plain FP64).
+//
+// One CTA advances one tile of TILE1 = 126 zones of one problem through a whole RK
+// stage: it stages the 130-zone pencil (tile + 2 ghost zones each side) in shared
+// memory, reconstructs every zone ONCE (the reference reconstructs each zone twice,
+// once per adjacent face: step.c:501-547), solves the 127 face Riemann problems, and
+// applies push() (step.c:380-470) to its 126 zones.  Boundary zones are never stored:
+// they are produced on load by the boundary kinds of reset_boundaries_gpu (bc.c:705-1422)
+// as index maps.  The CFL minimum (face terms step.c:560, source terms step.c:393, and in
+// the second stage the zone terms of the next estimate_dt, step.c:177-187) is reduced
+// per CTA with warp shuffles and folded into the problem's accumulator with one atomic.
+//
+// Many problems of different sizes are advanced by one launch: the grid is a list of
+// (problem, tile) work items.
+#include "mdg_hydro.cuh"
+#include "mdg_kernels.cuh"
+
+namespace mdg {
+
+// Noh inflow boundary, problems/init_spherical_noh.c:63-79 (ijk_to_r of
+// metric_spherical_general.c:483-496: r = r(beta0/Gamma0), rhat0 = dr/dx = 1).
+__device__ __forceinline__ void prob_bounds_noh(double gam, double b0, double g0, double t, double *w)
+{
+  double x = b0 / g0;
+  double r = fabs(x);
+  w[RHO] = 1.;
+  w[UU] = 1.e-6 / (gam - 1.);
+  w[U1] = -1. / 1.0;
+  w[U2] = 0.;
+  w[U3] = 0.;
+  w[RHO] += t / r;
+  w[RHO] *= w[RHO];
+}
+
+// Zone i (may be a ghost, i in [-NG, n1+NG)) of a 1-D problem: 5 primitives + pressure.
+__device__ __forceinline__ void load_cell_1d(const ProbDev &P, const StateSoA &s, const double *__restrict__ rc,
+                                             int64_t rcs, int i, double t_bc, double *w)
+{
+  const int n = P.n1;
+  const int64_t base = P.cell_off;
+  if (i < -NG) i = -NG;
+  if (i > n + NG - 1) i = n + NG - 1;
+  auto rd = [&](int k, double *o) {
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) o[v] = s.v[v][base + k];
+  };
+  if (i >= 0 && i < n) {
+    rd(i, w);
+  } else if (i < 0) {
+    switch (P.bc_lo0) {
+      case BC_REFLECT: rd(-1 - i, w); w[U1] *= -1.0; break;
+      case BC_SPHERICAL_ORIGIN: rd(-1 - i, w); w[U1] *= -1.0; w[U3] *= -1.0; break;
+      case BC_PERIODIC: rd(i + n, w); break;
+      case BC_EXTRAP: {
+        double a[NPRIM], b[NPRIM];
+        rd(0, a); rd(1, b);
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) w[v] = a[v] + i * (b[v] - a[v]);
+      } break;
+      case BC_PROB:
+        prob_bounds_noh(P.gam, __ldg(rc + RC_B0 * rcs + P.geo_off + i + NG),
+                        __ldg(rc + RC_G0 * rcs + P.geo_off + i + NG), t_bc, w);
+        break;
+      default: rd(0, w); break;   // OUTFLOW
+    }
+  } else {
+    switch (P.bc_hi0) {
+      case BC_REFLECT: rd(2 * n - i - 1, w); w[U1] *= -1.0; break;
+      case BC_PERIODIC: rd(i - n, w); break;
+      case BC_EXTRAP: {
+        double a[NPRIM], b[NPRIM];
+        rd(n - 1, a); rd(n - 2, b);
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) w[v] = a[v] + (i - n + 1) * (a[v] - b[v]);
+      } break;
+      case BC_PROB:
+        prob_bounds_noh(P.gam, __ldg(rc + RC_B0 * rcs + P.geo_off + i + NG),
+                        __ldg(rc + RC_G0 * rcs + P.geo_off + i + NG), t_bc, w);
+        break;
+      default: rd(n - 1, w); break;   // OUTFLOW
+    }
+  }
+  w[5] = eos_press(P.eos, P.gam, P.Kpoly, w[RHO], w[UU]);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(NT1)
+stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+               const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA sn, StateSoA out)
+{
+  __shared__ double sv[6][NT1 + 2];     // stage-state pencil: 5 primitives + pressure
+  __shared__ double sar[6][NT1];        // right face values of each reconstructed zone
+  __shared__ double sfl[NPRIM][NT1];    // face fluxes
+  __shared__ double sred[32];
+
+  const Tile tile = tiles[blockIdx.x];
+  const ProbDev &P = probs[tile.prob];
+  const double dt = times[tile.prob].dt;
+  const double t_bc = STAGE ? times[tile.prob].t_bc1 : times[tile.prob].t;
+  const int t = threadIdx.x;
+  const int n1 = P.n1;
+  const int z = tile.i0 - 1 + t;           // zone reconstructed by this thread
+  const double *rc = tb.rc0;
+  const int64_t rcs = tb.rc0_stride;
+  const double *geo = tb.geo;
+  const int64_t gs = tb.geo_stride;
+
+  double w[6];
+  load_cell_1d(P, sst, rc, rcs, z, t_bc, w);
+#pragma unroll
+  for (int v = 0; v < 6; v++) sv[v][t + 1] = w[v];
+  if (t == 0) {
+    double w2[6];
+    load_cell_1d(P, sst, rc, rcs, tile.i0 - 2, t_bc, w2);
+#pragma unroll
+    for (int v = 0; v < 6; v++) sv[v][0] = w2[v];
+  }
+  if (t == NT1 - 1) {
+    double w2[6];
+    load_cell_1d(P, sst, rc, rcs, tile.i0 + NT1 - 1, t_bc, w2);
+#pragma unroll
+    for (int v = 0; v < 6; v++) sv[v][NT1 + 1] = w2[v];
+  }
+  __syncthreads();
+
+  // reconstruct zone z once (interp(), reconstruct.c:225-279); Gamma is the constant
+  // adiabatic index, which every order reconstructs to itself.
+  double al[7], ar[7];
+  {
+    Rc<double> g;
+    int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
+    load_rc(g, rc, rcs, P.geo_off + zc + NG);
+#pragma unroll
+    for (int v = 0; v < 6; v++) recon_zone<double>(P.interp_order, sv[v][t], sv[v][t + 1], sv[v][t + 2], g, al[v], ar[v]);
+    al[6] = P.gam; ar[6] = P.gam;
+  }
+#pragma unroll
+  for (int v = 0; v < 6; v++) sar[v][t] = ar[v];
+  __syncthreads();
+
+  double lmin = 1.0e300;
+  // face z: between zones z-1 and z (pl = right state of z-1, pr = left state of z)
+  const bool face_ok = (t >= 1) && (z >= 0) && (z <= n1);
+  if (t >= 1) {
+    double pl[7], flux[NPRIM], sig;
+#pragma unroll
+    for (int v = 0; v < 6; v++) pl[v] = sar[v][t - 1];
+    pl[6] = P.gam;
+    FaceGeom<double> fg;
+    int zf = z < 0 ? 0 : (z > n1 ? n1 : z);
+    const int64_t gi = P.geo_off + zf + NG;
+    fg.area = __ldg(geo + GF_AREA * gs + gi);
+    fg.scale = __ldg(geo + GF_FSCALE * gs + gi);
+    fg.g0 = __ldg(geo + GF_FG0 * gs + gi);
+    fg.g1 = __ldg(geo + GF_FG1 * gs + gi);
+    fg.g2 = __ldg(geo + GF_FG2 * gs + gi);
+    riemann_hllc<0, double>(pl, al, fg, flux, sig);
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) sfl[v][t] = flux[v];
+    if (face_ok) lmin = tmin(lmin, P.dx0 / fabs(sig));
+  }
+  __syncthreads();
+
+  // push() for zone z (step.c:380-470)
+  if (t >= 1 && t <= NT1 - 2 && z >= 0 && z < n1) {
+    const int64_t gi = P.geo_off + z + NG;
+    const int64_t cell = P.cell_off + z;
+    double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM], divF[NPRIM], pf[NPRIM];
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) ph[v] = sv[v][t + 1];
+    if (STAGE == 0) {
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
+    }
+    const double gc0 = __ldg(geo + GF_G0 * gs + gi), gc1 = __ldg(geo + GF_G1 * gs + gi),
+                 gc2 = __ldg(geo + GF_G2 * gs + gi);
+    // geometric source terms from the stage state (rad_fluid.c:164-192, fluid.c:56-73)
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+    if (P.has_src) {
+      const double press = sv[5][t + 1];
+      double vcov[3] = {gc0 * ph[U1], gc1 * ph[U2], gc2 * ph[U3]};
+      double T[3][3];
+#pragma unroll
+      for (int l = 0; l < 3; l++) {
+#pragma unroll
+        for (int m = 0; m < 3; m++) T[l][m] = ph[RHO] * ph[U1 + m] * vcov[l];
+        T[l][l] += press;
+      }
+#pragma unroll
+      for (int l = 0; l < 3; l++)
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+          for (int n = 0; n < 3; n++)
+            src[U1 + m] += T[l][n] * __ldg(geo + (GF_CONN + l * 9 + m * 3 + n) * gs + gi);
+    }
+    p_to_u(pn, u, gc0, gc1, gc2);
+    p_to_u(ph, uh, gc0, gc1, gc2);
+    lmin = tmin(lmin, dt_source_control(pn, u, src));
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) { divF[v] = 0.0; divF[v] += sfl[v][t + 1]; divF[v] -= sfl[v][t]; }
+    const double vol = __ldg(geo + GF_VOL * gs + gi);
+    const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) {
+      double ddt = divF[v] / vol - src[v];
+      u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
+    }
+    u_to_p(u, pf, __ldg(geo + GF_GC0 * gs + gi), __ldg(geo + GF_GC1 * gs + gi), __ldg(geo + GF_GC2 * gs + gi));
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+    if (STAGE == 1) {
+      // zone term of the next estimate_dt (step.c:177-187): velocity of the new state,
+      // sound speed of the stage state (sim_eos was last filled from sim_ph)
+      const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
+      double local_dt = 0.0;
+      local_dt += (fabs(pf[U1]) + cs / __ldg(geo + GF_S00 * gs + gi)) / P.dx0;
+      lmin = tmin(lmin, 1.0 / local_dt);
+    }
+  }
+  block_min_to(lmin, &times[tile.prob].minacc, sred);
+}
+
+void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
+                    const Tables &tb, StateSoA sst, StateSoA sn, StateSoA out, cudaStream_t st)
+{
+  if (ntiles <= 0) return;
+  if (stage == 0) stage1d_kernel<0><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out);
+  else stage1d_kernel<1><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out);
+}
+
+}  // namespace mdg

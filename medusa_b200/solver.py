@@ -1,0 +1,203 @@
+"""Host-side mirror of the reference's hot-path interface over the C ABI.
+
+The reference drives its sweep with three global-state calls from main.c
+(estimate_dt(), step(), update_cpu(); decs.h:754-757).  :class:`Solver` holds one or more
+problems resident on the GPU and exposes the same operations:
+
+=====================  ===================================================
+reference              medusa_b200
+=====================  ===================================================
+main.c:129-165 upload  ``Solver(problems)`` + ``upload()`` (mdg_create/mdg_upload_state)
+estimate_dt()          ``estimate_dt()``  (mdg_estimate_dt)
+step(); t += dt        ``step(n)``        (mdg_step)
+update_cpu()           ``update_cpu(m)``  (mdg_download_state)
+=====================  ===================================================
+
+Every call goes through libmedusa_b200.so; there is no CPU fallback.  If the library is
+missing or the GPU is unavailable the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Sequence
+
+import numpy as np
+
+from . import problems as _pb
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libmedusa_b200.so")
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+
+class MdgError(RuntimeError):
+    """A non-zero status from the C ABI."""
+
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__("%s failed with status %d: %s" % (where, code, msg))
+        self.code = code
+
+
+class ProblemDesc(ctypes.Structure):
+    """mdg_problem_desc of include/medusa_b200.h."""
+    _fields_ = [("ndim", ctypes.c_int), ("geom", ctypes.c_int), ("eos", ctypes.c_int),
+                ("n1", ctypes.c_int), ("n2", ctypes.c_int), ("n3", ctypes.c_int),
+                ("startx", ctypes.c_double * 3), ("dx", ctypes.c_double * 3),
+                ("gam", ctypes.c_double), ("Kpoly", ctypes.c_double),
+                ("bc_lo", ctypes.c_int * 3), ("bc_hi", ctypes.c_int * 3),
+                ("prob_kind", ctypes.c_int),
+                ("cfl", ctypes.c_double), ("dt_init_safety", ctypes.c_double),
+                ("dt_grow_safety", ctypes.c_double), ("initial_dt", ctypes.c_double),
+                ("dtmax", ctypes.c_double), ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
+                ("hydro_interp_order", ctypes.c_int)]
+
+
+def desc_of(pb: "_pb.Problem") -> ProblemDesc:
+    d = ProblemDesc()
+    d.ndim, d.geom, d.eos = pb.ndim, pb.geom, pb.eos
+    d.n1, d.n2, d.n3 = pb.n
+    for k in range(3):
+        d.startx[k] = pb.startx[k]
+        d.dx[k] = pb.dx[k]
+        d.bc_lo[k] = pb.bc_lo[k]
+        d.bc_hi[k] = pb.bc_hi[k]
+    d.gam, d.Kpoly, d.prob_kind = pb.gam, pb.Kpoly, pb.prob_kind
+    d.cfl, d.dt_init_safety, d.dt_grow_safety = pb.cfl, pb.dt_init_safety, pb.dt_grow_safety
+    d.initial_dt, d.dtmax, d.dtmin, d.tmax = pb.initial_dt, pb.dtmax, pb.dtmin, pb.tmax
+    d.hydro_interp_order = pb.hydro_interp_order
+    return d
+
+
+_lib = None
+
+
+def library(path: str = _LIB_PATH) -> ctypes.CDLL:
+    """Load libmedusa_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError("libmedusa_b200.so not built (run python -m medusa_b200.build): %s" % path)
+    L = ctypes.CDLL(path)
+    vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    L.mdg_create.argtypes = [ctypes.POINTER(ProblemDesc), i, i, i, ctypes.POINTER(vp)]
+    L.mdg_upload_state.argtypes = [vp, i, vp]
+    L.mdg_estimate_dt.argtypes = [vp, vp]
+    L.mdg_step.argtypes = [vp, i]
+    L.mdg_download_state.argtypes = [vp, i, vp, vp]
+    L.mdg_get_time.argtypes = [vp, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(i)]
+    L.mdg_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.mdg_synchronize.argtypes = [vp]
+    L.mdg_destroy.argtypes = [vp]
+    L.mdg_error_string.restype = ctypes.c_char_p
+    L.mdg_error_string.argtypes = [i]
+    L.mdg_last_error_message.restype = ctypes.c_char_p
+    L.mdg_version.restype = i
+    L.mdg_set_timing.argtypes = [vp, i]
+    L.mdg_get_timers.argtypes = [vp, vp, vp]
+    for name in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step", "mdg_download_state",
+                 "mdg_get_time", "mdg_get_stream", "mdg_synchronize", "mdg_destroy", "mdg_set_timing",
+                 "mdg_get_timers"):
+        getattr(L, name).restype = i
+    _lib = L
+    return L
+
+
+def _check(rc: int, where: str):
+    if rc != 0:
+        L = library()
+        raise MdgError(rc, where, (L.mdg_last_error_message() or b"").decode())
+
+
+class Solver:
+    """Problems resident on one GPU, advanced together."""
+
+    def __init__(self, problems: Sequence["_pb.Problem"], precision: int = PREC_FP64, device: int = 0,
+                 upload: bool = True):
+        if isinstance(problems, _pb.Problem):
+            problems = [problems]
+        self.problems = list(problems)
+        L = library()
+        arr = (ProblemDesc * len(self.problems))(*[desc_of(p) for p in self.problems])
+        h = ctypes.c_void_p()
+        _check(L.mdg_create(arr, len(self.problems), precision, device, ctypes.byref(h)), "mdg_create")
+        self._h = h
+        if upload:
+            for m, p in enumerate(self.problems):
+                self.upload(m, p.ic)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().mdg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # --- the reference's operations
+    def upload(self, m: int, prim: np.ndarray):
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        if prim.shape != (self.problems[m].ncell, 5):
+            raise ValueError("state of problem %d must have shape (%d, 5)" % (m, self.problems[m].ncell))
+        _check(library().mdg_upload_state(self._h, m, prim.ctypes.data), "mdg_upload_state")
+
+    def upload_ptr(self, m: int, host_ptr: int):
+        """Upload from a raw host pointer (e.g. pinned memory) laid out [zone][5]."""
+        _check(library().mdg_upload_state(self._h, m, ctypes.c_void_p(host_ptr)), "mdg_upload_state")
+
+    def estimate_dt(self) -> np.ndarray:
+        out = np.zeros(len(self.problems))
+        _check(library().mdg_estimate_dt(self._h, out.ctypes.data), "mdg_estimate_dt")
+        return out
+
+    def step(self, nsteps: int = 1):
+        _check(library().mdg_step(self._h, int(nsteps)), "mdg_step")
+
+    def update_cpu(self, m: int = 0, with_eos: bool = False):
+        n = self.problems[m].ncell
+        prim = np.empty((n, 5))
+        eos = np.empty((n, 5)) if with_eos else None
+        _check(library().mdg_download_state(self._h, m, prim.ctypes.data,
+                                            eos.ctypes.data if with_eos else None), "mdg_download_state")
+        return (prim, eos) if with_eos else prim
+
+    def download_ptr(self, m: int, host_ptr: int):
+        _check(library().mdg_download_state(self._h, m, ctypes.c_void_p(host_ptr), None), "mdg_download_state")
+
+    def time(self, m: int = 0):
+        t, dt = ctypes.c_double(), ctypes.c_double()
+        ist = ctypes.c_int()
+        _check(library().mdg_get_time(self._h, m, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(ist)),
+               "mdg_get_time")
+        return t.value, dt.value, ist.value
+
+    def synchronize(self):
+        _check(library().mdg_synchronize(self._h), "mdg_synchronize")
+
+    TIMER_NAMES = ("estimate_dt", "stage0", "stage1", "finish")
+
+    def set_timing(self, enable: bool = True):
+        _check(library().mdg_set_timing(self._h, int(bool(enable))), "mdg_set_timing")
+
+    def timers(self) -> dict:
+        ms = np.zeros(4)
+        calls = np.zeros(4, dtype=np.int64)
+        _check(library().mdg_get_timers(self._h, ms.ctypes.data, calls.ctypes.data), "mdg_get_timers")
+        return {n: (float(ms[k]), int(calls[k])) for k, n in enumerate(self.TIMER_NAMES)}
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        _check(library().mdg_get_stream(self._h, ctypes.byref(s)), "mdg_get_stream")
+        return s.value or 0

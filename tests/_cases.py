@@ -1,0 +1,31 @@
+"""Shared test cases: the golden fixture set and helpers to compare states."""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+
+import make_golden  # noqa: E402
+
+GOLDEN_DIR = os.path.join(HERE, "golden")
+
+
+def golden_cases():
+    return make_golden.cases()
+
+
+def load_golden(name):
+    return np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
+
+
+def max_rel_diff(a, b, floor=1.0e-300):
+    """max |a-b| / max(|a|,|b|) over entries, treating +0 and -0 as equal."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    num = np.abs(a - b)
+    den = np.maximum(np.maximum(np.abs(a), np.abs(b)), floor)
+    r = num / den
+    r[num == 0] = 0.0
+    return float(r.max()) if r.size else 0.0

@@ -1,0 +1,63 @@
+"""The C ABI library without a GPU: it loads, exports every entry point that
+include/medusa_b200.h declares, and rejects bad input before touching the device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from medusa_b200 import problems as P
+from medusa_b200 import solver as S
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "medusa_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(mdg_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_the_abi():
+    names = declared_functions()
+    for required in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step",
+                     "mdg_download_state", "mdg_destroy"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    L = S.library()
+    for name in declared_functions():
+        assert hasattr(L, name), name
+
+
+def test_error_strings_and_version():
+    L = S.library()
+    for code in range(0, 12):
+        assert L.mdg_error_string(code)
+    assert L.mdg_version() >= 100
+
+
+@pytest.mark.parametrize("mutate,code", [
+    (dict(ndim=3), 1),
+    (dict(hydro_interp_order=4), 1),
+    (dict(gam=1.0), 1),
+    (dict(bc_lo=(P.SPHERICAL_ORIGIN, 0, 0)), 5),      # spherical origin on a Cartesian grid
+    (dict(bc_lo=(P.PERIODIC, 0, 0)), 1),              # unpaired periodic boundary
+])
+def test_create_rejects_invalid_descriptions(mutate, code):
+    pb = P.sod(64).copy(**mutate)
+    arr = (S.ProblemDesc * 1)(S.desc_of(pb))
+    h = ctypes.c_void_p()
+    rc = S.library().mdg_create(arr, 1, 0, 0, ctypes.byref(h))
+    assert rc == code
+    assert not h.value
+    assert S.library().mdg_last_error_message()
+
+
+def test_null_handles_are_rejected():
+    L = S.library()
+    assert L.mdg_step(None, 1) == 1
+    assert L.mdg_synchronize(None) == 1
+    assert L.mdg_destroy(None) == 0

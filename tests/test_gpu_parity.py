@@ -1,0 +1,118 @@
+"""GPU parity: the CUDA sweep through the C ABI against the reference's golden fixtures
+and the CPU oracle.
+
+Tolerance: 1e-12 relative per entry (the bar the plain FP64 sweep is held to).  The
+FP64 kernels keep the reference's operation order without contraction, so almost every
+case is in fact bit-exact; the tolerance covers pow() in the two-rarefaction wave-speed
+branch, where CUDA's and the host libm's results may differ in the last place.
+"""
+import numpy as np
+import pytest
+
+from medusa_b200 import problems as P
+from medusa_b200.solver import Solver, MdgError
+from oracle import pyoracle
+from tests._cases import golden_cases, load_golden, max_rel_diff
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1.0e-12
+CASES = golden_cases()
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gpu_matches_reference_fixture(name):
+    pb, n = CASES[name]
+    g = load_golden(name)
+    with Solver(pb) as s:
+        s.step(n)
+        s.synchronize()
+        prim = s.update_cpu(0)
+        t, dt, istep = s.time(0)
+    assert istep == n
+    assert max_rel_diff(prim, g["prim"]) <= TOL
+    assert abs(t - float(g["t"])) <= TOL * abs(float(g["t"]))
+    assert abs(dt - float(g["dt"])) <= TOL * abs(float(g["dt"]))
+
+
+def test_gpu_first_dt_matches_oracle():
+    pb = P.spherical_1d("sedov", 300, 1.4, p_ratio=1.0e4, r0=0.05)
+    o = pyoracle.Oracle(pb)
+    dt0 = o.advance(1)[0]
+    with Solver(pb) as s:
+        dt = s.estimate_dt()[0]
+        s.step(1)
+        s.synchronize()
+        assert s.time(0)[1] == dt
+    assert abs(dt - dt0) <= TOL * dt0
+
+
+def test_gpu_eos_download_matches_oracle():
+    pb = P.blast_2d(40, 48, bc=P.REFLECT)
+    o = pyoracle.Oracle(pb)
+    o.advance(5)
+    with Solver(pb) as s:
+        s.step(5)
+        prim, eos = s.update_cpu(0, with_eos=True)
+    oprim, oeos = o.state()
+    assert max_rel_diff(prim, oprim) <= TOL
+    # PRESS, CS, TEMP, GAMMA of the last stage state (ENT is not filled by the gamma law)
+    for k in (0, 1, 2, 4):
+        assert max_rel_diff(eos[:, k], oeos[:, k]) <= TOL
+
+
+def test_kh_full_size_per_step_parity():
+    """Kelvin-Helmholtz 2048^2 (the measured workload): two steps from the same initial
+    state on the GPU and on the oracle."""
+    pb = P.kelvin_helmholtz(2048)
+    o = pyoracle.Oracle(pb)
+    with Solver(pb) as s:
+        for k in range(2):
+            o.advance(1)
+            s.step(1)
+            prim = s.update_cpu(0)
+            oprim, _ = o.state()
+            assert max_rel_diff(prim, oprim) <= TOL, "step %d" % (k + 1)
+            assert s.time(0)[0] == o.t
+
+
+def test_kh_full_size_mass_conservation():
+    """Periodic box: total mass sum(rho*V) is conserved to round-off (flux differences
+    telescope), over 20 steps at full size."""
+    pb = P.kelvin_helmholtz(2048)
+    m0 = pb.ic[:, 0].sum()
+    with Solver(pb) as s:
+        s.step(20)
+        prim = s.update_cpu(0)
+    assert np.all(np.isfinite(prim))
+    assert abs(prim[:, 0].sum() - m0) <= 1.0e-12 * m0
+
+
+def test_batched_ensemble_equals_one_at_a_time_and_oracle():
+    ens = P.ensemble_1d(24, seed=3, nmin=128, nmax=1500)
+    n = 30
+    with Solver(ens) as s:
+        s.step(n)
+        batched = [s.update_cpu(m) for m in range(len(ens))]
+        times = [s.time(m) for m in range(len(ens))]
+    for m, pb in enumerate(ens):
+        with Solver(pb) as s1:
+            s1.step(n)
+            alone = s1.update_cpu(0)
+            assert s1.time(0) == times[m]
+        assert np.array_equal(alone, batched[m]), pb.name
+        o = pyoracle.Oracle(pb)
+        o.advance(n)
+        oprim, _ = o.state()
+        assert max_rel_diff(batched[m], oprim) <= TOL, pb.name
+        assert abs(times[m][0] - o.t) <= TOL * o.t
+
+
+def test_upload_rejects_bad_index_and_shape():
+    pb = P.sod(64)
+    with Solver(pb) as s:
+        with pytest.raises(MdgError) as e:
+            s.upload_ptr(3, pb.ic.ctypes.data)
+        assert e.value.code == 2
+        with pytest.raises(ValueError):
+            s.upload(0, pb.ic[:10])
