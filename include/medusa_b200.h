@@ -141,6 +141,33 @@ const char *mdg_last_error_message(void);
 int mdg_set_timing(mdg_solver *s, int enable);
 int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
 
+/*
+ * No counterpart in the reference.  A 1-D advance that allocates nothing, for callers
+ * that cannot call cudaMalloc: hosts whose device memory is owned by their own pool
+ * allocator, real-time loops that cannot afford cudaMalloc's implicit synchronisation,
+ * embeddings that must not grow their device footprint after start-up.
+ *
+ * Advances one 1-D problem (desc->ndim == 1, desc->n1 <= MDG_NOALLOC_MAX_ZONES) by
+ * nsteps passes of the reference time loop, exactly as mdg_create + mdg_upload_state +
+ * mdg_step would, starting from t = 0.  prim_in and prim_out are DEVICE pointers owned
+ * by the caller, laid out [var][zone] (5 x n1 doubles; they may be the same buffer);
+ * work is queued on `stream` (a cudaStream_t, 0 for the legacy default stream).  If
+ * t_out/dt_out are non-NULL the call waits for the stream and returns the final time
+ * and the last dt there.
+ *
+ * Everything else the sweep needs lives in one file-scope device array of fixed size
+ * (about 4.4 MB, held by every GPU that loads this library until exit).  Rules:
+ *   - n1 > MDG_NOALLOC_MAX_ZONES is rejected with MDG_ERR_OUTOFMEM (does not fit);
+ *   - the first call on a device performs the device set-up (it looks up the array's
+ *     device address); make that first call before any stream capture;
+ *   - all calls share the array: calls whose work overlaps on the GPU race;
+ *   - the array keeps the last call's contents; each call re-initialises what it uses.
+ * Calls no cudaMalloc, cudaFree or other allocating routine.
+ */
+#define MDG_NOALLOC_MAX_ZONES 8192
+int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double *prim_in, double *prim_out,
+                           int nsteps, void *stream, double *t_out, double *dt_out);
+
 /* Library version as major*10000 + minor*100 + patch. */
 int mdg_version(void);
 

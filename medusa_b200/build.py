@@ -22,7 +22,8 @@ LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libmedusa_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["mdg_capi.cu", "mdg_sweep1d.cu", "mdg_sweep2d.cu", "mdg_misc.cu", "mdg_geometry.cpp"]
+SOURCES = ["mdg_capi.cu", "mdg_sweep1d.cu", "mdg_sweep2d.cu", "mdg_misc.cu", "mdg_geometry.cpp",
+           "mdg_noalloc.cu"]
 HEADERS = ["mdg_internal.h", "mdg_hydro.cuh", "mdg_kernels.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

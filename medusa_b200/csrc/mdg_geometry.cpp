@@ -221,3 +221,64 @@ void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area
 }
 
 }  // namespace mdg
+
+namespace mdg {
+
+// Non-allocating variants for callers that provide every buffer: the same moments and
+// reconstruction table as build_moments/build_recon_table above, written into caller
+// memory (al/be/ga hold n+2*NG entries each).
+void build_moments_into(const mdg_problem_desc &d, int dir, double *al, double *be, double *ga)
+{
+  const int n = (dir == 0) ? d.n1 : (dir == 1 ? d.n2 : d.n3);
+  for (int i = -NG; i < n + NG; i++) {
+    if (d.geom == MDG_CARTESIAN) {
+      double x0 = d.startx[dir] + i * d.dx[dir], x1 = x0 + d.dx[dir];
+      al[i + NG] = (x1 * x1 * x1 - x0 * x0 * x0) / 3.0;
+      be[i + NG] = (x1 * x1 - x0 * x0) / 2.0;
+      ga[i + NG] = d.dx[dir];
+    } else {
+      double x0 = d.startx[0] + i * d.dx[0], x1 = d.startx[0] + (i + 1) * d.dx[0];
+      ga[i + NG] = romb(x0, x1, f_r2dr_dx);
+      be[i + NG] = romb(x0, x1, f_xr1g);
+      al[i + NG] = romb(x0, x1, f_xr2g);
+    }
+  }
+}
+
+void build_recon_table_into(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off,
+                            double *al, double *be, double *ga)
+{
+  build_moments_into(d, dir, al, be, ga);
+  const int n = (dir == 0) ? d.n1 : d.n2;
+  for (int i = -NG; i < n + NG; i++) {
+    int im = (i - 1 < -NG) ? -NG : i - 1, ip = (i + 1 >= n + NG) ? n + NG - 1 : i + 1;
+    double am = al[im + NG], a0 = al[i + NG], ap = al[ip + NG];
+    double bm = be[im + NG], b0 = be[i + NG], bp = be[ip + NG];
+    double gm = ga[im + NG], g0 = ga[i + NG], gp = ga[ip + NG];
+    double xl = d.startx[dir] + i * d.dx[dir];
+    double xr = d.startx[dir] + (i + 1) * d.dx[dir];
+    double a0b1g2 = am * b0 * gp, a0b2g1 = am * bp * g0, a1b0g2 = a0 * bm * gp;
+    double a1b2g0 = a0 * bp * gm, a2b0g1 = ap * bm * g0, a2b1g0 = ap * b0 * gm;
+    double den1 = 1.0 / (a0b1g2 + a1b2g0 + a2b0g1 - a0b2g1 - a1b0g2 - a2b1g0);
+    double den2 = (xl - xr) * (a0 + g0 * xl * xr - b0 * (xl + xr));
+    den2 = 1.0 / den2;
+    double xm = bm / gm, xp = bp / gp, xc = b0 / g0;
+    double v[RC_NFIELDS];
+    v[RC_AM] = am; v[RC_A0] = a0; v[RC_AP] = ap;
+    v[RC_BM] = bm; v[RC_B0] = b0; v[RC_BP] = bp;
+    v[RC_GM] = gm; v[RC_G0] = g0; v[RC_GP] = gp;
+    v[RC_XL] = xl; v[RC_XR] = xr;
+    v[RC_DEN1] = den1; v[RC_DEN2] = den2;
+    v[RC_XLR] = xl - xr;
+    v[RC_XL2] = xl * xl; v[RC_XR2] = xr * xr;
+    v[RC_XMID] = 0.5 * (xl + xr);
+    v[RC_DMR] = a0 + xr * (g0 * xr - 2.0 * b0);
+    v[RC_DML] = a0 + xl * (g0 * xl - 2.0 * b0);
+    v[RC_LSM] = xc - 0.5 * (xl + xm);
+    v[RC_LSP] = 0.5 * (xr + xp) - xc;
+    v[RC_LSC] = xp - xm;
+    for (int f = 0; f < RC_NFIELDS; f++) tab[f * stride + off + i + NG] = v[f];
+  }
+}
+
+}  // namespace mdg

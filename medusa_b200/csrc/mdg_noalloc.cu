@@ -1,0 +1,200 @@
+// mdg_advance_1d_noalloc: the 1-D sweep for callers that cannot allocate device memory.
+//
+// Who needs this: code that runs where cudaMalloc is not available or not allowed --
+// a host that has handed all device memory to its own pool allocator and forbids other
+// allocations, a real-time or interrupt-driven control loop in which cudaMalloc's
+// implicit device synchronisation and unbounded latency are unacceptable, or an
+// embedding that must not grow the process's device footprint after start-up.  Such a
+// caller owns its input and output buffers; everything else the sweep needs between its
+// kernels (the RK stage state, the geometry tables, the per-problem time and CFL
+// accumulators, the tile list) lives in ONE file-scope device array below, which every
+// GPU that loads this library holds until the process exits.
+//
+// Limits and rules (also stated in include/medusa_b200.h):
+//  * one 1-D problem per call, at most MDG_NOALLOC_MAX_ZONES zones, plain FP64;
+//  * the scratch array is shared by every call in the process: calls whose work overlaps
+//    on the GPU (different streams, different host threads) race and corrupt each other;
+//  * the first call on a device resolves the array's device address with
+//    cudaGetSymbolAddress (device set-up); make that first call before any stream capture;
+//  * the array keeps the previous call's contents: each call re-initialises everything it
+//    reads (time record, error flag, tables, tile list) before use.
+// This entry point calls no cudaMalloc, cudaFree or other allocating library routine.
+#include <cuda_runtime.h>
+#include <cstring>
+#include <mutex>
+#include "mdg_internal.h"
+#include "mdg_kernels.cuh"
+
+namespace mdg {
+void build_recon_table_into(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off,
+                            double *al, double *be, double *ga);
+void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+}
+
+using namespace mdg;
+
+namespace {
+
+constexpr int64_t NMAX = MDG_NOALLOC_MAX_ZONES;
+constexpr int64_t NCOL = NMAX + 2 * NG;                    // table columns (zones + ghosts)
+constexpr int64_t MAX_TILES = (NMAX + TILE1 - 1) / TILE1;
+
+// byte layout of the scratch array (every block 256-byte aligned)
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+constexpr size_t OFF_PH = 0;                                                  // stage state [5][NMAX]
+constexpr size_t OFF_RC = align256(OFF_PH + sizeof(double) * NPRIM * NMAX);   // RC_NFIELDS x NCOL
+constexpr size_t OFF_GEO = align256(OFF_RC + sizeof(double) * RC_NFIELDS * NCOL);  // GF_NFIELDS x NCOL
+constexpr size_t OFF_PROB = align256(OFF_GEO + sizeof(double) * GF_NFIELDS * NCOL);
+constexpr size_t OFF_TIME = align256(OFF_PROB + sizeof(ProbDev));
+constexpr size_t OFF_TILES = align256(OFF_TIME + sizeof(ProbTime));
+constexpr size_t OFF_ERR = align256(OFF_TILES + sizeof(Tile) * MAX_TILES);
+constexpr size_t SCRATCH_BYTES = align256(OFF_ERR + sizeof(int));
+
+}  // namespace
+
+// The scratch: ~4.4 MB per device for MDG_NOALLOC_MAX_ZONES = 8192.
+static __device__ __align__(256) unsigned char mdg_noalloc_scratch[SCRATCH_BYTES];
+
+namespace {
+
+constexpr int MAX_DEVICES = 64;
+unsigned char *g_scratch[MAX_DEVICES] = {nullptr};
+std::mutex g_setup_mutex;
+
+// Host staging of the tables (host memory reserved at load time, not allocated per call).
+double h_rc[RC_NFIELDS * NCOL];
+double h_geo[GF_NFIELDS * NCOL];
+Tile h_tiles[MAX_TILES];
+double h_al[NCOL], h_be[NCOL], h_ga[NCOL];
+// Failures are reported by status code only (the message text documents the cause).
+int fail(int code, const char *why)
+{
+  (void)why;
+  return code;
+}
+
+int check_desc(const mdg_problem_desc &d)
+{
+  if (d.ndim != 1) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: ndim must be 1");
+  if (d.n1 < 2) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: n1 must be at least 2");
+  if (d.n1 > NMAX)
+    return fail(MDG_ERR_OUTOFMEM, "mdg_advance_1d_noalloc: n1 exceeds MDG_NOALLOC_MAX_ZONES: does not fit the scratch");
+  if (d.geom != MDG_CARTESIAN && d.geom != MDG_SPHERICAL) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: geom");
+  if (d.eos != MDG_GAMMA_LAW && d.eos != MDG_POLYTROPIC) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: eos");
+  if (d.hydro_interp_order < 1 || d.hydro_interp_order > 3)
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: hydro_interp_order");
+  if (!(d.dx[0] > 0.0) || !(d.gam > 1.0) || !(d.cfl > 0.0))
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: dx, gam or cfl");
+  const int lo = d.bc_lo[0], hi = d.bc_hi[0];
+  const bool sph = d.geom == MDG_SPHERICAL, noh = d.prob_kind == MDG_PROB_NOH;
+  const bool lo_ok = lo == MDG_BC_OUTFLOW || lo == MDG_BC_REFLECT || lo == MDG_BC_EXTRAP ||
+                     lo == MDG_BC_PERIODIC || (lo == MDG_BC_PROB && sph && noh) ||
+                     (lo == MDG_BC_SPHERICAL_ORIGIN && sph);
+  const bool hi_ok = hi == MDG_BC_OUTFLOW || hi == MDG_BC_REFLECT || hi == MDG_BC_EXTRAP ||
+                     hi == MDG_BC_PERIODIC || (hi == MDG_BC_PROB && sph && noh);
+  if (!lo_ok || !hi_ok) return fail(MDG_ERR_NOTIMPL, "mdg_advance_1d_noalloc: boundary kinds");
+  if ((lo == MDG_BC_PERIODIC) != (hi == MDG_BC_PERIODIC))
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: periodic boundaries must be paired");
+  return MDG_OK;
+}
+
+// Device set-up, once per device, with that device current.
+int scratch_of_current_device(unsigned char **out)
+{
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return fail(MDG_ERR_CUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= MAX_DEVICES) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: device ordinal");
+  std::lock_guard<std::mutex> lk(g_setup_mutex);
+  if (!g_scratch[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, mdg_noalloc_scratch);
+    if (e != cudaSuccess || !p) return fail(MDG_ERR_CUDA, "cudaGetSymbolAddress(mdg_noalloc_scratch) failed");
+    g_scratch[dev] = static_cast<unsigned char *>(p);
+  }
+  *out = g_scratch[dev];
+  return MDG_OK;
+}
+
+}  // namespace
+
+extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double *prim_in, double *prim_out,
+                                      int nsteps, void *stream, double *t_out, double *dt_out)
+{
+  if (!desc || !prim_in || !prim_out) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: null argument");
+  if (nsteps < 0) return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: nsteps < 0");
+  int rc = check_desc(*desc);
+  if (rc != MDG_OK) return rc;
+  unsigned char *base = nullptr;
+  rc = scratch_of_current_device(&base);
+  if (rc != MDG_OK) return rc;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const mdg_problem_desc &d = *desc;
+  const int n1 = d.n1;
+
+  // problem record, tables and tiles (host staging, copied into the scratch)
+  ProbDev P;
+  memset(&P, 0, sizeof P);
+  P.ndim = 1; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
+  P.n1 = n1; P.n2 = 1;
+  P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0];
+  P.prob_kind = d.prob_kind;
+  P.has_src = (d.geom == MDG_SPHERICAL);
+  P.cell_off = 0; P.geo_off = 0;
+  P.gam = d.gam; P.Kpoly = d.Kpoly; P.dx0 = d.dx[0]; P.dx1 = d.dx[1];
+  P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
+  P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
+  const int64_t ncol = n1 + 2 * NG;
+  build_recon_table_into(d, 0, h_rc, ncol, 0, h_al, h_be, h_ga);
+  build_geo_1d(d, h_geo, ncol, 0);
+  int ntiles = 0;
+  for (int i0 = 0; i0 < n1; i0 += TILE1) h_tiles[ntiles++] = Tile{0, i0, 0, 0};
+
+  double *ph = reinterpret_cast<double *>(base + OFF_PH);
+  double *rcd = reinterpret_cast<double *>(base + OFF_RC);
+  double *geo = reinterpret_cast<double *>(base + OFF_GEO);
+  ProbDev *probs = reinterpret_cast<ProbDev *>(base + OFF_PROB);
+  ProbTime *times = reinterpret_cast<ProbTime *>(base + OFF_TIME);
+  Tile *tiles = reinterpret_cast<Tile *>(base + OFF_TILES);
+  int *err = reinterpret_cast<int *>(base + OFF_ERR);
+
+#define CKN(call)                                                            \
+  do {                                                                       \
+    cudaError_t e_ = (call);                                                 \
+    if (e_ != cudaSuccess) return fail(MDG_ERR_CUDA, cudaGetErrorString(e_)); \
+  } while (0)
+  CKN(cudaMemcpyAsync(rcd, h_rc, sizeof(double) * RC_NFIELDS * ncol, cudaMemcpyHostToDevice, st));
+  CKN(cudaMemcpyAsync(geo, h_geo, sizeof(double) * GF_NFIELDS * ncol, cudaMemcpyHostToDevice, st));
+  CKN(cudaMemcpyAsync(probs, &P, sizeof P, cudaMemcpyHostToDevice, st));
+  CKN(cudaMemcpyAsync(tiles, h_tiles, sizeof(Tile) * ntiles, cudaMemcpyHostToDevice, st));
+  CKN(cudaMemsetAsync(err, 0, sizeof(int), st));        // the error flag must start at zero
+  if (prim_out != prim_in)
+    CKN(cudaMemcpyAsync(prim_out, prim_in, sizeof(double) * NPRIM * n1, cudaMemcpyDeviceToDevice, st));
+  // the host staging above is reused by the next call: wait until the copies have landed
+  CKN(cudaStreamSynchronize(st));
+
+  Tables tb{};
+  tb.rc0 = rcd; tb.rc0_stride = ncol;
+  tb.geo = geo; tb.geo_stride = ncol;
+  StateSoA S{}, PH{};
+  for (int v = 0; v < NPRIM; v++) { S.v[v] = prim_out + (int64_t)v * n1; PH.v[v] = ph + (int64_t)v * n1; }
+
+  launch_reset_time(times, 0, st);
+  launch_initial_estimate_one(probs, times, 0, n1, tb, S, st);
+  for (int k = 0; k < nsteps; k++) {
+    launch_dt_finalize(probs, times, 1, err, st);
+    launch_stage1d(0, probs, times, tiles, ntiles, tb, S, S, PH, st);
+    launch_stage1d(1, probs, times, tiles, ntiles, tb, PH, S, S, st);
+    launch_finish(times, 1, st);
+  }
+  CKN(cudaGetLastError());
+  if (t_out || dt_out) {
+    ProbTime T;
+    CKN(cudaMemcpyAsync(&T, times, sizeof T, cudaMemcpyDeviceToHost, st));
+    CKN(cudaStreamSynchronize(st));
+    if (t_out) *t_out = T.t;
+    if (dt_out) *dt_out = T.dt;
+  }
+#undef CKN
+  return MDG_OK;
+}
