@@ -28,6 +28,9 @@ struct mdg_solver {
   ProbTime *d_times = nullptr;
   Tile *d_tiles = nullptr;
   int ntiles = 0;
+  int ntx = 0, nty = 0;           // 2-D: direction-0 tiles first, then direction-1 tiles
+  StateSoA ACC{};                 // 2-D: direction-0 part of the flux difference
+  unsigned char *d_shock1 = nullptr;
   double *d_rc0 = nullptr, *d_rc1 = nullptr, *d_geo = nullptr;
   Tables tb{};
   double *d_state = nullptr;      // 10 arrays: P (5) then PH (5)
@@ -115,7 +118,7 @@ static void free_all(mdg_solver *s)
       if (s->ev[k][e]) cudaEventDestroy(s->ev[k][e]);
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles);
   cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
-  cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_stage); cudaFree(s->d_err);
+  cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -168,7 +171,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   s->descs.assign(descs, descs + nprob);
 
   // layout: state offsets, table offsets, tiles
-  std::vector<Tile> tiles;
+  std::vector<Tile> tiles, ytiles;
   int64_t cell = 0, rc0 = 0, rc1 = 0, sh = 0;
   for (int m = 0; m < nprob; m++) {
     const mdg_problem_desc &d = descs[m];
@@ -196,14 +199,20 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (d.ndim == 2) {
       rc1 += P.n2 + 2 * NG;
       sh += (int64_t)(P.n1 + 3) * P.n2;
-      for (int i0 = 0; i0 < P.n1; i0 += TI2)
-        for (int j0 = 0; j0 < P.n2; j0 += TJ2) tiles.push_back(Tile{m, i0, j0, 0});
+      for (int i0 = 0; i0 < P.n1; i0 += TIX2)
+        for (int j0 = 0; j0 < P.n2; j0 += NTX2) tiles.push_back(Tile{m, i0, j0, 0});
+      for (int i0 = 0; i0 < P.n1; i0 += TIY2)
+        for (int j0 = 0; j0 < P.n2; j0 += TJY2) ytiles.push_back(Tile{m, i0, j0, 0});
     } else {
       for (int i0 = 0; i0 < P.n1; i0 += TILE1) tiles.push_back(Tile{m, i0, 0, 0});
     }
   }
   s->ncell_total = cell;
+  s->ntx = (int)tiles.size();
+  s->nty = (int)ytiles.size();
+  tiles.insert(tiles.end(), ytiles.begin(), ytiles.end());
   s->ntiles = (int)tiles.size();
+  const int nstate = (ndim == 2) ? 3 : 2;   // P, PH (+ ACC in 2-D)
 
   // host tables
   std::vector<double> h_rc0((size_t)RC_NFIELDS * rc0), h_rc1, h_geo;
@@ -233,23 +242,26 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMalloc(&s->d_rc0, sizeof(double) * h_rc0.size()));
   if (ndim == 2) CKC(cudaMalloc(&s->d_rc1, sizeof(double) * h_rc1.size()));
   else CKC(cudaMalloc(&s->d_geo, sizeof(double) * h_geo.size()));
-  CKC(cudaMalloc(&s->d_state, sizeof(double) * 2 * NPRIM * cell));
+  CKC(cudaMalloc(&s->d_state, sizeof(double) * nstate * NPRIM * cell));
   CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
   CKC(cudaMalloc(&s->d_err, sizeof(int)));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock0, sh > 0 ? sh : 1));
+  if (ndim == 2) CKC(cudaMalloc(&s->d_shock1, sh > 0 ? sh : 1));
 
   CKC(cudaMemcpy(s->d_probs, s->hprobs.data(), sizeof(ProbDev) * nprob, cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(s->d_tiles, tiles.data(), sizeof(Tile) * s->ntiles, cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(s->d_rc0, h_rc0.data(), sizeof(double) * h_rc0.size(), cudaMemcpyHostToDevice));
   if (ndim == 2) CKC(cudaMemcpy(s->d_rc1, h_rc1.data(), sizeof(double) * h_rc1.size(), cudaMemcpyHostToDevice));
   else CKC(cudaMemcpy(s->d_geo, h_geo.data(), sizeof(double) * h_geo.size(), cudaMemcpyHostToDevice));
-  CKC(cudaMemset(s->d_state, 0, sizeof(double) * 2 * NPRIM * cell));
+  CKC(cudaMemset(s->d_state, 0, sizeof(double) * nstate * NPRIM * cell));
   CKC(cudaMemset(s->d_err, 0, sizeof(int)));
   if (ndim == 2) CKC(cudaMemset(s->d_shock0, 0, sh > 0 ? sh : 1));
+  if (ndim == 2) CKC(cudaMemset(s->d_shock1, 0, sh > 0 ? sh : 1));
   CKC(cudaMemset(s->d_times, 0, sizeof(ProbTime) * nprob));
   for (int v = 0; v < NPRIM; v++) {
     s->P.v[v] = s->d_state + (int64_t)v * cell;
     s->PH.v[v] = s->d_state + (int64_t)(NPRIM + v) * cell;
+    if (ndim == 2) s->ACC.v[v] = s->d_state + (int64_t)(2 * NPRIM + v) * cell;
   }
   s->tb.rc0 = s->d_rc0; s->tb.rc0_stride = rc0;
   s->tb.rc1 = s->d_rc1; s->tb.rc1_stride = rc1;
@@ -285,13 +297,15 @@ static int queue_steps(mdg_solver *s, int nsteps)
     if (s->ndim == 1)
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
     else
-      launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->d_shock0, s->stream);
+      launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
+                     s->P, s->P, s->ACC, s->PH, s->d_shock0, s->d_shock1, s->stream);
     mark(MDG_TIMER_STAGE0, 1);
     mark(MDG_TIMER_STAGE1, 0);
     if (s->ndim == 1)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     else
-      launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->d_shock0, s->stream);
+      launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
+                     s->PH, s->P, s->ACC, s->P, s->d_shock0, s->d_shock1, s->stream);
     mark(MDG_TIMER_STAGE1, 1);
     mark(MDG_TIMER_FINISH, 0);
     launch_finish(s->d_times, s->nprob, s->stream);

@@ -19,89 +19,88 @@ template <typename T> __device__ __forceinline__ T tmin(T a, T b) { return (a < 
 template <typename T> __device__ __forceinline__ T tmax(T a, T b) { return (a > b) ? a : b; }
 template <typename T> __device__ __forceinline__ T tsign(T a) { return (a < T(0)) ? T(-1) : T(1); }
 
-// Reconstruction coefficients of one zone (the geometry of para_recon/lin_recon).
-template <typename T>
-struct Rc {
-  T am, a0, ap, bm, b0, bp, gm, g0, gp;
-  T xl, xr, den1, den2, xlr, xl2, xr2, xmid, dmr, dml, lsm, lsp, lsc;
+// Read access to the reconstruction coefficients of one zone (the geometry-only
+// sub-expressions of para_recon/lin_recon, field f at p[f*stride]).  Fields are read when
+// used, so the 22 coefficients never occupy registers all at once; LDG selects the
+// read-only global path (tables in HBM) or plain loads (tables staged in shared memory).
+template <typename T, bool LDG>
+struct RcView {
+  const double *p;
+  int64_t stride;
+  __device__ __forceinline__ T operator()(int f) const
+  {
+    return LDG ? T(__ldg(p + f * stride)) : T(p[f * stride]);
+  }
 };
-
-template <typename T>
-__device__ __forceinline__ void load_rc(Rc<T> &r, const double *__restrict__ tab, int64_t stride, int64_t idx)
-{
-  r.am = T(__ldg(tab + RC_AM * stride + idx)); r.a0 = T(__ldg(tab + RC_A0 * stride + idx));
-  r.ap = T(__ldg(tab + RC_AP * stride + idx));
-  r.bm = T(__ldg(tab + RC_BM * stride + idx)); r.b0 = T(__ldg(tab + RC_B0 * stride + idx));
-  r.bp = T(__ldg(tab + RC_BP * stride + idx));
-  r.gm = T(__ldg(tab + RC_GM * stride + idx)); r.g0 = T(__ldg(tab + RC_G0 * stride + idx));
-  r.gp = T(__ldg(tab + RC_GP * stride + idx));
-  r.xl = T(__ldg(tab + RC_XL * stride + idx)); r.xr = T(__ldg(tab + RC_XR * stride + idx));
-  r.den1 = T(__ldg(tab + RC_DEN1 * stride + idx)); r.den2 = T(__ldg(tab + RC_DEN2 * stride + idx));
-  r.xlr = T(__ldg(tab + RC_XLR * stride + idx));
-  r.xl2 = T(__ldg(tab + RC_XL2 * stride + idx)); r.xr2 = T(__ldg(tab + RC_XR2 * stride + idx));
-  r.xmid = T(__ldg(tab + RC_XMID * stride + idx));
-  r.dmr = T(__ldg(tab + RC_DMR * stride + idx)); r.dml = T(__ldg(tab + RC_DML * stride + idx));
-  r.lsm = T(__ldg(tab + RC_LSM * stride + idx)); r.lsp = T(__ldg(tab + RC_LSP * stride + idx));
-  r.lsc = T(__ldg(tab + RC_LSC * stride + idx));
-}
 
 // para_recon for one zone (reconstruct.c:142-201): am/a0/ap are the zone averages at
 // i-1, i, i+1; returns the left (al) and right (ar) face values of zone i.
-template <typename T>
-__device__ __forceinline__ void para_recon_zone(T am_v, T a, T ap_v, const Rc<T> &g, T &al, T &ar)
+//
+// Control flow is arranged for the SIMT machine without changing any result: the
+// extremum test (reconstruct.c:145) only skips the work when every active lane of the
+// warp is at an extremum; otherwise all lanes compute and extremum lanes select a[i] at
+// the end, so the six variables of a zone run as independent instruction streams.  The
+// two "move the zero" cases (reconstruct.c:190-200) share one code path.
+template <typename T, typename G>
+__device__ __forceinline__ void para_recon_zone(T am_v, T a, T ap_v, const G &g, T &al, T &ar)
 {
   T dqm = a - am_v;
   T dqp = ap_v - a;
-  if (dqm * dqp <= T(0)) { al = a; ar = a; return; }
+  const bool flat = (dqm * dqp <= T(0));
+  if (__all_sync(__activemask(), flat)) { al = a; ar = a; return; }
   T dqc = ap_v - am_v;
-  T A = (dqm * g.bp * g.gm * g.g0 + g.gp * (dqp * g.bm * g.g0 - dqc * g.b0 * g.gm)) * g.den1;
-  T B = -(dqm * g.ap * g.gm * g.g0 + g.gp * (dqp * g.am * g.g0 - dqc * g.a0 * g.gm)) * g.den1;
-  T C = a - (g.a0 * A + g.b0 * B) / g.g0;
-  T l = g.xl * (A * g.xl + B) + C;
-  T r = g.xr * (A * g.xr + B) + C;
+  T A = (dqm * g(RC_BP) * g(RC_GM) * g(RC_G0) + g(RC_GP) * (dqp * g(RC_BM) * g(RC_G0) - dqc * g(RC_B0) * g(RC_GM))) * g(RC_DEN1);
+  T B = -(dqm * g(RC_AP) * g(RC_GM) * g(RC_G0) + g(RC_GP) * (dqp * g(RC_AM) * g(RC_G0) - dqc * g(RC_A0) * g(RC_GM))) * g(RC_DEN1);
+  T C = a - (g(RC_A0) * A + g(RC_B0) * B) / g(RC_G0);
+  const T xl = g(RC_XL), xr = g(RC_XR);
+  T l = xl * (A * xl + B) + C;
+  T r = xr * (A * xr + B) + C;
   T mean = T(0.75) * am_v + T(0.25) * a;
   T mask = (a - l) * (l - mean);
   l = (mask < T(0)) ? mean : l;
   mean = T(0.75) * ap_v + T(0.25) * a;
   mask = (mean - r) * (r - a);
   r = (mask < T(0)) ? mean : r;
-  A = (g.b0 * (r - l) + g.g0 * (a * g.xlr - r * g.xl + l * g.xr)) * g.den2;
-  B = (g.a0 * (l - r) + g.g0 * (r - a) * g.xl2 + g.g0 * (a - l) * g.xr2) * g.den2;
+  A = (g(RC_B0) * (r - l) + g(RC_G0) * (a * g(RC_XLR) - r * xl + l * xr)) * g(RC_DEN2);
+  B = (g(RC_A0) * (l - r) + g(RC_G0) * (r - a) * g(RC_XL2) + g(RC_G0) * (a - l) * g(RC_XR2)) * g(RC_DEN2);
   T xzero = -B / (T(2) * A + T(1.0e-16));
   if (isinf(xzero) || isnan(xzero)) xzero = T(-1.0e-200);
-  if (xzero > g.xl && xzero < g.xr) {
-    if (xzero > g.xmid) {
-      A = g.g0 * (a - r) / g.dmr;
-      B = T(-2.0) * A * g.xr;
-      C = a - (g.a0 * A + g.b0 * B) / g.g0;
-      l = g.xl * (A * g.xl + B) + C;
-    } else {
-      A = g.g0 * (a - l) / g.dml;
-      B = T(-2.0) * A * g.xl;
-      C = a - (g.a0 * A + g.b0 * B) / g.g0;
-      r = g.xr * (A * g.xr + B) + C;
+  const bool inside = !flat && (xzero > xl && xzero < xr);
+  if (__any_sync(__activemask(), inside)) {
+    // move the zero to the right edge (replace al) or to the left edge (replace ar)
+    const bool right = xzero > g(RC_XMID);
+    const T e = right ? r : l;
+    const T xe = right ? xr : xl;
+    const T xo = right ? xl : xr;
+    A = g(RC_G0) * (a - e) / (right ? g(RC_DMR) : g(RC_DML));
+    B = T(-2.0) * A * xe;
+    C = a - (g(RC_A0) * A + g(RC_B0) * B) / g(RC_G0);
+    const T val = xo * (A * xo + B) + C;
+    if (inside) {
+      if (right) l = val;
+      else r = val;
     }
   }
-  al = l;
-  ar = r;
+  al = flat ? a : l;
+  ar = flat ? a : r;
 }
 
 // lin_recon for one zone (reconstruct.c:99-121)
-template <typename T>
-__device__ __forceinline__ void lin_recon_zone(T am_v, T a, T ap_v, const Rc<T> &g, T &al, T &ar)
+template <typename T, typename G>
+__device__ __forceinline__ void lin_recon_zone(T am_v, T a, T ap_v, const G &g, T &al, T &ar)
 {
-  T sm = (a - am_v) / g.lsm;
-  T sp = (ap_v - a) / g.lsp;
+  T sm = (a - am_v) / g(RC_LSM);
+  T sp = (ap_v - a) / g(RC_LSP);
   if (sm * sp <= T(0)) { al = a; ar = a; return; }
-  T sc = (ap_v - am_v) / g.lsc;
+  T sc = (ap_v - am_v) / g(RC_LSC);
   T A = tsign(sc) * tmin(tmin(fabs(sm), fabs(sp)), fabs(sc));
-  T B = a - A * g.b0 / g.g0;
-  al = A * g.xl + B;
-  ar = A * g.xr + B;
+  T B = a - A * g(RC_B0) / g(RC_G0);
+  al = A * g(RC_XL) + B;
+  ar = A * g(RC_XR) + B;
 }
 
-template <typename T>
-__device__ __forceinline__ void recon_zone(int order, T am_v, T a, T ap_v, const Rc<T> &g, T &al, T &ar)
+template <typename T, typename G>
+__device__ __forceinline__ void recon_zone(int order, T am_v, T a, T ap_v, const G &g, T &al, T &ar)
 {
   if (order == 3) para_recon_zone(am_v, a, ap_v, g, al, ar);
   else if (order == 2) lin_recon_zone(am_v, a, ap_v, g, al, ar);
@@ -112,15 +111,48 @@ __device__ __forceinline__ void recon_zone(int order, T am_v, T a, T ap_v, const
 template <typename T>
 struct FaceGeom { T area, scale; T g0, g1, g2; };
 
+// Metric factors: with UNIT (Cartesian grids: gcov = scale = 1) the multiplications and
+// divisions by 1.0 are dropped; x*1.0 == x and x/1.0 == x exactly, so results are unchanged.
+template <bool UNIT, typename T> __device__ __forceinline__ T gmul(T g, T x) { return UNIT ? x : g * x; }
+template <bool UNIT, typename T> __device__ __forceinline__ T gdiv(T x, T s) { return UNIT ? x : x / s; }
+
+// Adiabatic-index constants of the wave-speed estimate.  Every cell carries Gamma = gam
+// (gamma-law and polytrope), so these sub-expressions of riemann.c are constants;
+// computed here with the reference's own operation order they are bit-identical.
+template <typename T>
+struct GamConst {
+  T g;      // Gamma
+  T cq;     // (Gamma+1)/(2 Gamma)        riemann.c:389-390
+  T gp1;    // Gamma+1                    riemann.c:413-414
+  T cb;     // (Gamma-1)/(Gamma+1)        riemann.c:415-416
+  T ce;     // (Gamma_avg-1)/(2 Gamma_avg), Gamma_avg = 0.5(Gamma+Gamma) = Gamma   riemann.c:400
+  T gm1;    // Gamma-1
+  T cx;     // 2 Gamma/(Gamma-1)          riemann.c:402
+};
+template <typename T>
+__device__ __forceinline__ GamConst<T> gam_const(T G)
+{
+  GamConst<T> c;
+  T Gavg = T(0.5) * (G + G);
+  c.g = G;
+  c.cq = (G + T(1)) / (T(2) * G);
+  c.gp1 = G + T(1);
+  c.cb = (G - T(1)) / (G + T(1));
+  c.ce = (Gavg - T(1)) / (T(2) * Gavg);
+  c.gm1 = G - T(1);
+  c.cx = T(2) * G / (G - T(1));
+  return c;
+}
+
 // Wave-speed estimate shared by HLLC and HLLE (riemann.c:368-429 / 210-303).
-// w[0..4] primitives, w[5] pressure, w[6] Gamma.
+// w[0..4] primitives, w[5] pressure (w[6], Gamma, equals gc.g).
 template <typename T>
 __device__ __forceinline__ void wave_speeds(const T *pl, const T *pr, T u_l, T u_r, bool hlle,
-                                            T &sl, T &sr, T &ss, T &p_s, int &isshock)
+                                            const GamConst<T> &gc, T &sl, T &sr, T &ss, T &p_s, int &isshock)
 {
-  const T p_l = pl[5], p_r = pr[5], G_l = pl[6], G_r = pr[6];
-  T cs_l = sqrt(G_l * p_l / pl[RHO]);
-  T cs_r = sqrt(G_r * p_r / pr[RHO]);
+  const T p_l = pl[5], p_r = pr[5], G = gc.g;
+  T cs_l = sqrt(G * p_l / pl[RHO]);
+  T cs_r = sqrt(G * p_r / pr[RHO]);
   T p_max, p_min;
   if (p_l > p_r) { p_max = p_l; p_min = p_r; } else { p_max = p_r; p_min = p_l; }
   T pratio = p_max / p_min;
@@ -133,25 +165,26 @@ __device__ __forceinline__ void wave_speeds(const T *pl, const T *pr, T u_l, T u
     // primitive-variable estimate kept
   } else if (p_s < p_min) {
     // two rarefactions (Toro 9.35-9.36)
-    T G_avg = T(0.5) * (G_l + G_r);
-    T plr = pow(p_l / p_r, (G_avg - T(1)) / (T(2) * G_avg));
-    T s0 = (plr * u_l / cs_l + u_r / cs_r + T(2) * (plr - T(1)) / (G_avg - T(1))) / (plr / cs_l + T(1) / cs_r);
-    p_s = T(0.5) * (p_l * pow(T(1) + (G_l - T(1)) / (T(2) * cs_l) * (u_l - s0), T(2) * G_l / (G_l - T(1)))
-                  + p_r * pow(T(1) + (G_r - T(1)) / (T(2) * cs_r) * (s0 - u_r), T(2) * G_r / (G_r - T(1))));
+    T plr = pow(p_l / p_r, gc.ce);
+    T s0 = (plr * u_l / cs_l + u_r / cs_r + T(2) * (plr - T(1)) / gc.gm1) / (plr / cs_l + T(1) / cs_r);
+    p_s = T(0.5) * (p_l * pow(T(1) + gc.gm1 / (T(2) * cs_l) * (u_l - s0), gc.cx)
+                  + p_r * pow(T(1) + gc.gm1 / (T(2) * cs_r) * (s0 - u_r), gc.cx));
     p_s = tmax(p_s, T(0));
   } else {
     // two shocks (Toro 9.42-9.43)
-    T a_l = T(2) / ((G_l + T(1)) * pl[RHO]);
-    T a_r = T(2) / ((G_r + T(1)) * pr[RHO]);
-    T b_l = (G_l - T(1)) / (G_l + T(1)) * p_l;
-    T b_r = (G_r - T(1)) / (G_r + T(1)) * p_r;
+    T a_l = T(2) / (gc.gp1 * pl[RHO]);
+    T a_r = T(2) / (gc.gp1 * pr[RHO]);
+    T b_l = gc.cb * p_l;
+    T b_r = gc.cb * p_r;
     T g_l = sqrt(a_l / (p_s + b_l));
     T g_r = sqrt(a_r / (p_s + b_r));
     p_s = (g_l * p_l + g_r * p_r - (u_r - u_l)) / (g_l + g_r);
     p_s = tmax(p_s, T(0));
   }
-  T q_l = (p_s <= p_l) ? T(1) : sqrt(T(1) + (G_l + T(1)) / (T(2) * G_l) * (p_s / p_l - T(1)));
-  T q_r = (p_s <= p_r) ? T(1) : sqrt(T(1) + (G_r + T(1)) / (T(2) * G_r) * (p_s / p_r - T(1)));
+  // q = 1 when p_s <= p, else sqrt(1 + (G+1)/(2G) (p_s/p - 1)); sqrt(1) == 1 exactly, so
+  // the square root is taken unconditionally on the selected argument (no branch)
+  T q_l = sqrt((p_s <= p_l) ? T(1) : T(1) + gc.cq * (p_s / p_l - T(1)));
+  T q_r = sqrt((p_s <= p_r) ? T(1) : T(1) + gc.cq * (p_s / p_r - T(1)));
   sl = u_l - cs_l * q_l;
   sr = u_r + cs_r * q_r;
   ss = (p_r - p_l + pl[RHO] * u_l * (sl - u_l) - pr[RHO] * u_r * (sr - u_r))
@@ -159,10 +192,10 @@ __device__ __forceinline__ void wave_speeds(const T *pl, const T *pr, T u_l, T u
 }
 
 // p_uflux (riemann.c:4-37) for direction DIR
-template <int DIR, typename T>
+template <int DIR, bool UNIT, typename T>
 __device__ __forceinline__ void p_uflux(const T *p, const FaceGeom<T> &g, T press, T *u, T *f)
 {
-  T vc0 = g.g0 * p[U1], vc1 = g.g1 * p[U2], vc2 = g.g2 * p[U3];
+  T vc0 = gmul<UNIT>(g.g0, p[U1]), vc1 = gmul<UNIT>(g.g1, p[U2]), vc2 = gmul<UNIT>(g.g2, p[U3]);
   T v = p[U1 + DIR];
   u[RHO] = p[RHO];
   T vsq = T(0);
@@ -177,10 +210,10 @@ __device__ __forceinline__ void p_uflux(const T *p, const FaceGeom<T> &g, T pres
 }
 
 // pflux (riemann.c:39-62)
-template <int DIR, typename T>
+template <int DIR, bool UNIT, typename T>
 __device__ __forceinline__ void pflux(const T *p, T press, const FaceGeom<T> &g, T *f)
 {
-  T vc0 = g.g0 * p[U1], vc1 = g.g1 * p[U2], vc2 = g.g2 * p[U3];
+  T vc0 = gmul<UNIT>(g.g0, p[U1]), vc1 = gmul<UNIT>(g.g1, p[U2]), vc2 = gmul<UNIT>(g.g2, p[U3]);
   T v = p[U1 + DIR];
   T area = g.area;
   f[RHO] = area * p[RHO] * v;
@@ -194,8 +227,9 @@ __device__ __forceinline__ void pflux(const T *p, T press, const FaceGeom<T> &g,
 
 // riemann_flux_HLLC (riemann.c:328-499); returns isshock, writes flux[5] and the signal
 // speed used by the CFL reduction.
-template <int DIR, typename T>
-__device__ __forceinline__ int riemann_hllc(const T *pl, const T *pr, const FaceGeom<T> &g, T *flux, T &sig)
+template <int DIR, bool UNIT, typename T>
+__device__ __forceinline__ int riemann_hllc(const T *pl, const T *pr, const FaceGeom<T> &g, const GamConst<T> &gc,
+                                            T *flux, T &sig)
 {
   int isshock = 0;
   if (g.area < T(1.0e-16)) {
@@ -205,32 +239,32 @@ __device__ __forceinline__ int riemann_hllc(const T *pl, const T *pr, const Face
     return isshock;
   }
   const T sc = g.scale;
-  T u_l = pl[U1 + DIR] * sc;
-  T u_r = pr[U1 + DIR] * sc;
+  T u_l = gmul<UNIT>(sc, pl[U1 + DIR]);
+  T u_r = gmul<UNIT>(sc, pr[U1 + DIR]);
   T sl, sr, ss, p_s;
-  wave_speeds<T>(pl, pr, u_l, u_r, false, sl, sr, ss, p_s, isshock);
+  wave_speeds<T>(pl, pr, u_l, u_r, false, gc, sl, sr, ss, p_s, isshock);
   if (ss > sr) sr = T(1.001) * ss;
   if (ss < sl) sl = T(1.001) * ss;
-  sig = tmax(fabs(sl), fabs(sr)) / sc;
-  if (sl > T(0)) { pflux<DIR, T>(pl, pl[5], g, flux); return isshock; }
-  if (sr < T(0)) { pflux<DIR, T>(pr, pr[5], g, flux); return isshock; }
-  T u[NPRIM], fx[NPRIM], Us[NPRIM], slr;
-  if (ss > T(0)) {
-    p_uflux<DIR, T>(pl, g, pl[5], u, fx);
-    Us[0] = pl[RHO] * (sl - u_l) / (sl - ss);
-    Us[UU] = (u[UU] * (sl - u_l) - pl[5] * u_l + p_s * ss) / (sl - ss);
-    Us[U1] = pl[U1]; Us[U2] = pl[U2]; Us[U3] = pl[U3];
-    Us[U1 + DIR] = ss / sc;
-    slr = sl / sc;
-  } else {
-    p_uflux<DIR, T>(pr, g, pr[5], u, fx);
-    Us[0] = pr[RHO] * (sr - u_r) / (sr - ss);
-    Us[UU] = (u[UU] * (u_r - sr) + pr[5] * u_r - p_s * ss) / (ss - sr);
-    Us[U1] = pr[U1]; Us[U2] = pr[U2]; Us[U3] = pr[U3];
-    Us[U1 + DIR] = ss / sc;
-    slr = sr / sc;
-  }
-  T vc0 = g.g0 * Us[U1], vc1 = g.g1 * Us[U2], vc2 = g.g2 * Us[U3];
+  sig = gdiv<UNIT>(tmax(fabs(sl), fabs(sr)), sc);
+  if (sl > T(0)) { pflux<DIR, UNIT, T>(pl, pl[5], g, flux); return isshock; }
+  if (sr < T(0)) { pflux<DIR, UNIT, T>(pr, pr[5], g, flux); return isshock; }
+  // Star state of the upwind side k (k = left if ss > 0, riemann.c:453-491).  The
+  // right-side formula of the reference, (E(u_r - s_r) + p_r u_r - p_s ss)/(ss - s_r), is
+  // the left-side formula with every sum and difference negated; round-to-nearest is
+  // symmetric under negation, so one code path gives bit-identical results for both sides.
+  T u[NPRIM], fx[NPRIM], Us[NPRIM], pk[6];
+  const bool left = ss > T(0);
+#pragma unroll
+  for (int v = 0; v < 6; v++) pk[v] = left ? pl[v] : pr[v];
+  const T sk = left ? sl : sr;
+  const T uk = left ? u_l : u_r;
+  p_uflux<DIR, UNIT, T>(pk, g, pk[5], u, fx);
+  Us[0] = pk[RHO] * (sk - uk) / (sk - ss);
+  Us[UU] = (u[UU] * (sk - uk) - pk[5] * uk + p_s * ss) / (sk - ss);
+  Us[U1] = pk[U1]; Us[U2] = pk[U2]; Us[U3] = pk[U3];
+  Us[U1 + DIR] = gdiv<UNIT>(ss, sc);
+  const T slr = gdiv<UNIT>(sk, sc);
+  T vc0 = gmul<UNIT>(g.g0, Us[U1]), vc1 = gmul<UNIT>(g.g1, Us[U2]), vc2 = gmul<UNIT>(g.g2, Us[U3]);
   Us[U1] = vc0 * Us[0]; Us[U2] = vc1 * Us[0]; Us[U3] = vc2 * Us[0];
 #pragma unroll
   for (int v = 0; v < NPRIM; v++) flux[v] = g.area * (fx[v] + slr * (Us[v] - u[v]));
@@ -238,8 +272,9 @@ __device__ __forceinline__ int riemann_hllc(const T *pl, const T *pr, const Face
 }
 
 // riemann_flux_HLLE (riemann.c:178-325)
-template <int DIR, typename T>
-__device__ __forceinline__ void riemann_hlle(const T *pl, const T *pr, const FaceGeom<T> &g, T *flux, T &sig)
+template <int DIR, bool UNIT, typename T>
+__device__ __forceinline__ void riemann_hlle(const T *pl, const T *pr, const FaceGeom<T> &g, const GamConst<T> &gc,
+                                             T *flux, T &sig)
 {
   if (g.area < T(1.0e-16)) {
     sig = T(1.0e-200);
@@ -248,16 +283,16 @@ __device__ __forceinline__ void riemann_hlle(const T *pl, const T *pr, const Fac
     return;
   }
   const T sc = g.scale;
-  T u_l = pl[U1 + DIR] * sc;
-  T u_r = pr[U1 + DIR] * sc;
+  T u_l = gmul<UNIT>(sc, pl[U1 + DIR]);
+  T u_r = gmul<UNIT>(sc, pr[U1 + DIR]);
   T sl, sr, ss, p_s;
   int isshock;
-  wave_speeds<T>(pl, pr, u_l, u_r, true, sl, sr, ss, p_s, isshock);
+  wave_speeds<T>(pl, pr, u_l, u_r, true, gc, sl, sr, ss, p_s, isshock);
   T ul[NPRIM], ur[NPRIM], fl[NPRIM], fr[NPRIM];
-  p_uflux<DIR, T>(pl, g, pl[5], ul, fl);
-  p_uflux<DIR, T>(pr, g, pr[5], ur, fr);
-  T cmax = tmax(sr / sc, T(0));
-  T cmin = fabs(tmin(sl / sc, T(0)));
+  p_uflux<DIR, UNIT, T>(pl, g, pl[5], ul, fl);
+  p_uflux<DIR, UNIT, T>(pr, g, pr[5], ur, fr);
+  T cmax = tmax(gdiv<UNIT>(sr, sc), T(0));
+  T cmin = fabs(tmin(gdiv<UNIT>(sl, sc), T(0)));
   sig = tmax(cmax, cmin);
 #pragma unroll
   for (int v = 0; v < NPRIM; v++)
@@ -300,6 +335,26 @@ __device__ __forceinline__ double dt_source_control(const double *p, const doubl
   local_dt = 100 * alpha * p[UU] / (fabs(fabs(s[1]) - fabs(momterm)) + 1.0e-16);
   mdt = tmin(mdt, local_dt);
   return mdt;
+}
+
+// The CFL reduction without a division per term.  Correctly rounded division is
+// monotone, so for a fixed c > 0:  min_k fl(x_k / c) == fl(min_k x_k / c)  and, for
+// y_k >= 0,  min_k fl(c / y_k) == fl(c / max_k y_k).  The face terms dx/|sig| and the zone
+// terms 1/local_dt are therefore reduced as maxima of their denominators, and with zero
+// source terms (Cartesian grids) dt_source_control's three terms share the denominator
+// |0| + 1e-16 and are reduced on their numerators.  The results are bit-identical.
+__device__ __forceinline__ double src_dt_numerator_min(const double *p, const double *u)
+{
+  const double alpha = 0.02;
+  double m = alpha * u[0];
+  m = tmin(m, alpha * u[1]);
+  m = tmin(m, 100 * alpha * p[UU]);
+  return m;
+}
+// dt_source_control's minimum over zones with zero sources, from the numerator minimum
+__device__ __forceinline__ double src_dt_from_numerator(double nmin)
+{
+  return tmin(1.0e100, nmin / (fabs(0.0) + 1.0e-16));
 }
 
 // gamma-law / polytrope pressure (eos_gamma.c:7, eos_poly.c:7)

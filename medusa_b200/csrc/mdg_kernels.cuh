@@ -24,16 +24,31 @@ struct Tile { int prob; int i0; int j0; int pad; };
 
 constexpr int NT1 = 128;          // threads per 1-D tile (126 output zones)
 constexpr int TILE1 = NT1 - 2;
-constexpr int NT2 = 128;          // threads per 2-D tile (126 output columns)
-constexpr int TJ2 = NT2 - 2;
-constexpr int TI2 = 32;           // output rows per 2-D tile
+// 2-D tile shapes and occupancy targets (compile-time tunables)
+#ifndef MDG_TIX2
+#define MDG_TIX2 32
+#endif
+#ifndef MDG_TIY2
+#define MDG_TIY2 16
+#endif
+#ifndef MDG_XMINB
+#define MDG_XMINB 4
+#endif
+#ifndef MDG_YMINB
+#define MDG_YMINB 4
+#endif
+constexpr int NTX2 = 128;         // threads (= columns) per direction-0 tile
+constexpr int TIX2 = MDG_TIX2;    // rows per direction-0 tile
+constexpr int NTY2 = 128;         // threads per direction-1 tile (126 output columns)
+constexpr int TJY2 = NTY2 - 2;
+constexpr int TIY2 = MDG_TIY2;    // rows per direction-1 tile
 
 void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
                     const Tables &tb, StateSoA stage_state, StateSoA state_n, StateSoA out,
                     cudaStream_t st);
-void launch_stage2d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
-                    const Tables &tb, StateSoA stage_state, StateSoA state_n, StateSoA out,
-                    unsigned char *shock0, cudaStream_t st);
+void launch_stage2d(int stage, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
+                    const Tile *ytiles, int nyt, const Tables &tb, StateSoA stage_state, StateSoA state_n,
+                    StateSoA acc, StateSoA out, unsigned char *shock0, unsigned char *shock1, cudaStream_t st);
 void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st);
 void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
 void launch_reset_time(ProbTime *times, int m, cudaStream_t st);

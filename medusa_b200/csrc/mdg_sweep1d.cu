@@ -127,9 +127,8 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   // adiabatic index, which every order reconstructs to itself.
   double al[7], ar[7];
   {
-    Rc<double> g;
     int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
-    load_rc(g, rc, rcs, P.geo_off + zc + NG);
+    const RcView<double, true> g{rc + P.geo_off + zc + NG, rcs};
 #pragma unroll
     for (int v = 0; v < 6; v++) recon_zone<double>(P.interp_order, sv[v][t], sv[v][t + 1], sv[v][t + 2], g, al[v], ar[v]);
     al[6] = P.gam; ar[6] = P.gam;
@@ -139,6 +138,8 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   __syncthreads();
 
   double lmin = 1.0e300;
+  double smax = 0.0, nmin = 1.0e300, lmax = 0.0;
+  const GamConst<double> gc = gam_const(P.gam);
   // face z: between zones z-1 and z (pl = right state of z-1, pr = left state of z)
   const bool face_ok = (t >= 1) && (z >= 0) && (z <= n1);
   if (t >= 1) {
@@ -154,10 +155,10 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     fg.g0 = __ldg(geo + GF_FG0 * gs + gi);
     fg.g1 = __ldg(geo + GF_FG1 * gs + gi);
     fg.g2 = __ldg(geo + GF_FG2 * gs + gi);
-    riemann_hllc<0, double>(pl, al, fg, flux, sig);
+    riemann_hllc<0, false, double>(pl, al, fg, gc, flux, sig);
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) sfl[v][t] = flux[v];
-    if (face_ok) lmin = tmin(lmin, P.dx0 / fabs(sig));
+    if (face_ok) smax = tmax(smax, fabs(sig));
   }
   __syncthreads();
 
@@ -200,7 +201,8 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     }
     p_to_u(pn, u, gc0, gc1, gc2);
     p_to_u(ph, uh, gc0, gc1, gc2);
-    lmin = tmin(lmin, dt_source_control(pn, u, src));
+    if (P.has_src) lmin = tmin(lmin, dt_source_control(pn, u, src));
+    else nmin = tmin(nmin, src_dt_numerator_min(pn, u));   // zero sources: shared denominator
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) { divF[v] = 0.0; divF[v] += sfl[v][t + 1]; divF[v] -= sfl[v][t]; }
     const double vol = __ldg(geo + GF_VOL * gs + gi);
@@ -219,9 +221,14 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
       double local_dt = 0.0;
       local_dt += (fabs(pf[U1]) + cs / __ldg(geo + GF_S00 * gs + gi)) / P.dx0;
-      lmin = tmin(lmin, 1.0 / local_dt);
+      lmax = tmax(lmax, local_dt);
     }
   }
+  // min of dx/|sig| over faces, of the zero-source limits and of 1/local_dt, each taken
+  // on its numerator or denominator (monotone division, see src_dt_numerator_min)
+  lmin = tmin(lmin, P.dx0 / smax);
+  lmin = tmin(lmin, src_dt_from_numerator(nmin));
+  if (STAGE == 1) lmin = tmin(lmin, 1.0 / lmax);
   block_min_to(lmin, &times[tile.prob].minacc, sred);
 }
 
