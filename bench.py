@@ -1,25 +1,44 @@
-"""Benchmark: plain FP64 hydro sweep on the 2-D Kelvin-Helmholtz workload.
+"""Benchmark of the hydro sweep: zone-updates/s, batched mixed precision vs plain FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ensemble|kh2048] [--no-cpu-baseline]
 
-Workload: Kelvin-Helmholtz on the periodic unit square, 2048 x 2048 zones, gamma = 5/3,
-CFL 0.8 (seeded synthetic initial state, medusa_b200.problems.kelvin_helmholtz).  A step
-is one full RK2 step of the reference time loop (estimate_dt + both stages + t += dt);
-the metric is zone-updates/s (zones x steps / seconds), whole job over all ranks.
+A step is one full RK2 step of the reference time loop (estimate_dt + both stages +
+t += dt) of every problem of the workload; the metric is zone-updates/s (zones x steps /
+seconds), whole job over all ranks.
+
+Workload "ensemble" (default): 2048 independent 1-D spherical problems, zone counts
+log-uniform in [128, 8192] (4.0 M zones), Sod/Noh/Sedov initial states with seeded
+density and pressure ratios and gamma in {4/3, 1.4, 5/3}
+(medusa_b200.problems.ensemble_1d, seed 7 + rank).  The headline runs them all in one
+solver with the mixed-precision sweep (FP32 reconstruction/Riemann, FP64 state, fluxes,
+sources, update and dt), launch shape chosen by the autotuner, each step's launches
+replayed from a CUDA graph.  Beside it, measured in the same run:
+  - the same ensemble batched through the plain FP64 sweep;
+  - the plain FP64 sweep run one problem at a time (a sample of 64 problems, each in its
+    own solver, back to back), the baseline of the >= 3x target;
+  - accuracy of the mixed result against the plain FP64 result at the same physical time:
+    volume-weighted relative L1 of density and internal energy, mass and total-energy
+    differences (compensated sums), per problem kind; beside it the FP64 result's own
+    sensitivity floor (the same FP64 run with its CFL number scaled by 1 + 1e-7) and, for
+    the Noh problems, the FP64 path's L1 error against the analytic solution.
+Workload "kh2048": 2-D Kelvin-Helmholtz 2048 x 2048, plain FP64, gamma 5/3, CFL 0.8.
 
 - value:  device time of K steps with the state resident in HBM, CUDA events on the
           solver's stream, barrier + synchronize on both sides, max over ranks.  The
-          state (2 x 168 MB) exceeds the 126 MB L2, so no L2 flush is needed.
-- e2e:    the same metric through the public API with host buffers: upload of the
-          initial state from pinned memory, K steps, download of the final state to
+          ensemble state (2 x 160 MB) and the KH state (2 x 168 MB) exceed the 126 MB L2,
+          so no L2 flush is needed.
+- e2e:    the same metric through the public API with host buffers: upload of every
+          initial state from pinned memory, K steps, download of every final state to
           pinned memory, all inside the timed region.
 - roofline: the dominant kernel (second RK stage) against the measured HBM copy
-          bandwidth; algorithmic bytes per zone-update B_alg(2-D) = 440 B, of which the
-          second stage accounts for 240 B.
+          bandwidth; algorithmic bytes per zone-update B_alg = 240 NDIM - 40
+          (1-D 200 B, 2-D 440 B), of which the second stage accounts for 120 B (1-D) /
+          240 B (2-D).
 - cpu_baseline: the reference's own CPU build (its Makefile flags) on a bounded sample
-          of the same workload, rank 0 only.
-With --gpus N > 1 (torchrun), every rank runs an independent replica (the single-grid
-sweep does not shard: replicas only).
+          of the same workload (ensemble: problem-parallel over the host's cores).
+With --gpus N > 1 (torchrun) every rank runs its own workload (ensemble: seed 7 + rank;
+KH: a replica); there is no collective on the data path.
 --impl reference times the reference's CPU implementation instead (rank 0 only).
 """
 import argparse
@@ -35,8 +54,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NX = 2048
-B_ALG_STEP = 440.0          # bytes per zone-update, 2-D (240*NDIM - 40)
-B_ALG_STAGE1 = 240.0        # second-stage share: read state, accumulators and base state
+ENSEMBLE_COUNT = 2048
+ENSEMBLE_SEED = 7
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -49,12 +68,11 @@ def read_peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
-def read_profile_traffic():
-    """Per-launch DRAM traffic of the second-stage kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "stage2d_kh2048_ncu.md")
+def read_profile_value(name, key):
+    """A number recorded as '<key> <value>' in a committed ncu summary under profiles/."""
     try:
-        for line in open(path):
-            if line.startswith("TRAFFIC_PER_LAUNCH_STAGE1_BYTES"):
+        for line in open(os.path.join(ROOT, "profiles", name)):
+            if line.startswith(key + " "):
                 return float(line.split()[1])
     except Exception:
         pass
@@ -122,13 +140,117 @@ def dist_setup():
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=None)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=None)
         return world, rank, local, dist
     return 1, 0, 0, None
 
 
-def cpu_baseline_reference(pb_full, steps=2):
+class Ctx:
+    """Rank bookkeeping: barrier and max over ranks of a device time."""
+
+    def __init__(self, world, rank, local, dist):
+        self.world, self.rank, self.local, self.dist = world, rank, local, dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_ms(self, ms):
+        if self.dist is None:
+            return ms
+        import torch
+        tt = torch.tensor([ms], device="cuda")
+        self.dist.all_reduce(tt, op=self.dist.ReduceOp.MAX)
+        return float(tt.item())
+
+
+def timed_steps(ctx, solver, K, sample_clocks=False):
+    """Device time (ms, max over ranks) of K steps on the solver's stream."""
+    import torch
+    stream = torch.cuda.ExternalStream(solver.stream, device=ctx.local)
+    sampler = ClockSampler(ctx.local) if sample_clocks else None
+    if sampler:
+        sampler.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    solver.step(K)
+    e1.record(stream)
+    e1.synchronize()
+    solver.synchronize()
+    ctx.barrier()
+    clocks = sampler.stop() if sampler else None
+    return ctx.max_ms(e0.elapsed_time(e1)), clocks
+
+
+def stage_times(solver, nsteps):
+    """Per-step device time of each RK stage from the library's event timers."""
+    solver.set_timing(True)
+    solver.step(nsteps)
+    solver.synchronize()
+    tm = solver.timers()
+    solver.set_timing(False)
+    return ({k: tm[k][0] / max(1, tm[k][1]) for k in ("stage0", "stage1", "estimate_dt", "finish")})
+
+
+def run_to_times(ctx, problems, t_end, precision, nsteps, cfg):
+    """A solver over `problems` whose end times are t_end, stepped until every problem
+    has reached its end time (a problem that reaches it stays there: dt = dtmin);
+    returns (solver, steps beyond nsteps, largest relative time mismatch)."""
+    from medusa_b200.solver import Solver
+    s = Solver([pb.copy(tmax=te) for pb, te in zip(problems, t_end)], precision=precision, device=ctx.local)
+    if cfg:
+        s.set_launch_config(**cfg)
+    s.step(nsteps)
+    extra = 0
+    while True:
+        t_now = [s.time(m)[0] for m in range(len(problems))]
+        if all(tn >= te * (1.0 - 1.0e-12) for tn, te in zip(t_now, t_end)) or extra >= 20 * nsteps:
+            break
+        s.step(20)
+        extra += 20
+    return s, extra, max(abs(tn - te) / te for tn, te in zip(t_now, t_end))
+
+
+def e2e_run(ctx, make_solver, problems, K, W):
+    """Upload every state from pinned host memory, K steps, download every state, all in
+    the timed region; returns (ms, h2d bytes, d2h bytes)."""
+    import numpy as np
+    import torch
+    offs = np.cumsum([0] + [p.ncell for p in problems])
+    host = np.concatenate([np.ascontiguousarray(p.ic, dtype=np.float64) for p in problems])
+    h_in = torch.from_numpy(host).pin_memory()
+    h_out = torch.empty_like(h_in).pin_memory()
+    s = make_solver(upload=False)
+    stream = torch.cuda.ExternalStream(s.stream, device=ctx.local)
+    row = 5 * 8
+    for m in range(len(problems)):
+        s.upload_ptr(m, h_in.data_ptr() + int(offs[m]) * row)
+    s.step(W)
+    s.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    ctx.barrier()
+    torch.cuda.synchronize()
+    f0.record(stream)
+    for m in range(len(problems)):
+        s.upload_ptr(m, h_in.data_ptr() + int(offs[m]) * row)
+    s.step(K)
+    for m in range(len(problems)):
+        s.download_ptr(m, h_out.data_ptr() + int(offs[m]) * row)
+    f1.record(stream)
+    f1.synchronize()
+    ctx.barrier()
+    ms = ctx.max_ms(f0.elapsed_time(f1))
+    s.close()
+    nbytes = int(offs[-1]) * row
+    return ms, nbytes, nbytes
+
+
+# ----------------------------------------------------------------------------- CPU side
+def cpu_baseline_kh(pb_full, steps=2):
     """Reference CPU build (Makefile flags) on a bounded sample: `steps` RK2 steps of the
     full grid, single core (the reference's hot path has no host threading)."""
     from oracle import pyoracle
@@ -138,7 +260,6 @@ def cpu_baseline_reference(pb_full, steps=2):
                 "kind": "reference",
                 "sample": "%d RK2 steps of the %dx%d grid, reference build with its own flags "
                           "(-O3 -ffast-math), 1 core, %.1f s" % (steps, NX, NX, r["seconds"])}
-    # the oracle restatement when the reference build is not present
     o = pyoracle.Oracle(pb_full)
     t0 = time.perf_counter()
     o.advance(1)
@@ -147,150 +268,306 @@ def cpu_baseline_reference(pb_full, steps=2):
             "sample": "1 RK2 step of the %dx%d grid, CPU oracle, 1 core, %.1f s" % (NX, NX, el)}
 
 
-def run_reference_arm(args, world, rank):
+def cpu_baseline_ensemble(problems, every=8, steps=50, warm=2):
+    """The reference CPU build on every `every`-th problem of the ensemble, `steps` timed
+    RK2 steps each, as independent single-threaded processes over all host cores (the
+    reference has no host threading on this path; problem-parallel is its best use of
+    the host).  Rate = timed zone-updates / (summed timed seconds / processes), i.e.
+    perfect packing of the processes (the reference's best case)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import pyoracle
+    sample = problems[::every]
+    procs = os.cpu_count() or 1
+    if pyoracle.ref_available(sample[0], fast=True):
+        kind = "reference"
+
+        def job(pb):
+            r = pyoracle.time_reference(pb, warm, steps, fast=True)
+            return r["cells"] * r["steps"], r["seconds"]
+    else:
+        kind = "port"
+
+        def job(pb):
+            o = pyoracle.Oracle(pb)
+            o.advance(warm)
+            t0 = time.perf_counter()
+            o.advance(steps)
+            return pb.ncell * steps, time.perf_counter() - t0
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=procs) as ex:
+        res = list(ex.map(job, sample))
+    wall = time.perf_counter() - t0
+    zu = sum(r[0] for r in res)
+    busy = sum(r[1] for r in res)
+    return {"value": zu / (busy / procs), "unit": "zone-updates/s", "cores": procs, "kind": kind,
+            "sample": "%d of the %d problems (every %dth), %d timed RK2 steps each after %d warm-up, "
+                      "%d concurrent single-threaded processes, %s build%s; %.1f s wall"
+                      % (len(sample), len(problems), every, steps, warm, procs, kind,
+                         " with its own flags (-O3 -ffast-math)" if kind == "reference" else "", wall)}
+
+
+def run_reference_arm(args, ctx):
     from medusa_b200 import problems as P
-    if rank != 0:
+    if ctx.rank != 0:
         return
-    pb = P.kelvin_helmholtz(NX)
-    cb = cpu_baseline_reference(pb, steps=max(1, min(args.steps, 2)))
-    line = {"metric": "zone-updates/s", "value": cb["value"], "unit": "zone-updates/s", "n_gpus": world,
+    if args.workload == "kh2048":
+        pb = P.kelvin_helmholtz(NX)
+        cb = cpu_baseline_kh(pb, steps=max(1, min(args.steps, 2)))
+        config = {"workload": "kelvin_helmholtz_2d_%dx%d_fp64" % (NX, NX), "global_batch": 1,
+                  "seq_len": NX * NX, "parallelism": "replicas", "l2": "inputs larger than L2"}
+        dtype = "f64"
+    else:
+        probs = P.ensemble_1d(ENSEMBLE_COUNT, seed=ENSEMBLE_SEED)
+        cb = cpu_baseline_ensemble(probs)
+        config = ensemble_config(probs, 1)
+        dtype = "f64"
+    line = {"metric": "zone-updates/s", "value": cb["value"], "unit": "zone-updates/s", "n_gpus": ctx.world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "impl": "reference",
-            "config": {"workload": "kelvin_helmholtz_2d_%dx%d_fp64" % (NX, NX), "global_batch": 1,
-                       "seq_len": NX * NX, "parallelism": "replicas", "l2": "inputs larger than L2"},
-            "cpu_baseline": cb,
+            "vs_baseline": None, "dtype": dtype, "data": "synthetic", "impl": "reference",
+            "config": config, "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- workloads
+def ensemble_config(problems, world):
+    ncell = sum(p.ncell for p in problems)
+    return {"workload": "ensemble_1d_spherical_%d_problems_128_8192_zones" % len(problems),
+            "global_batch": world * len(problems), "seq_len": ncell,
+            "parallelism": "problem-parallel, no collective" if world > 1 else "single",
+            "kinds": "Sod/Noh/Sedov, rho ratio 2-100, p ratio 2-1e4, gamma 4/3|1.4|5/3",
+            "l2": "inputs larger than L2 (state 2 x %.0f MB)" % (ncell * 40 / 1e6)}
+
+
+def run_ensemble(args, ctx):
+    import numpy as np
+    from medusa_b200 import analytic as A
+    from medusa_b200 import problems as P
+    from medusa_b200.solver import PREC_FP64, PREC_MIXED, Solver
+
+    K, W = args.steps, args.warmup
+    probs = P.ensemble_1d(ENSEMBLE_COUNT, seed=ENSEMBLE_SEED + ctx.rank)
+    ncell = sum(p.ncell for p in probs)
+    NT = 10   # timer-instrumented steps (roofline)
+
+    # ---- headline: batched mixed precision, autotuned, CUDA graphs
+    mix = Solver(probs, precision=PREC_MIXED, device=ctx.local)
+    tuned, tune_ms = mix.autotune(trial_steps=10)
+    mix.step(W)
+    mix.synchronize()
+    ms_mix, clocks = timed_steps(ctx, mix, K, sample_clocks=True)
+    value = ctx.world * ncell * K / (ms_mix / 1e3)
+    st_mix = stage_times(mix, NT)
+
+    # ---- the same ensemble batched through the plain FP64 sweep (same step count)
+    f64 = Solver(probs, precision=PREC_FP64, device=ctx.local)
+    f64.step(W)
+    f64.synchronize()
+    ms_f64, _ = timed_steps(ctx, f64, K)
+    st_f64 = stage_times(f64, NT)
+
+    mix.close()
+
+    # ---- accuracy at equal physical time: each problem's time after W + K + NT plain FP64
+    # steps is its end time for a fresh mixed run (whose last step lands on it) and for a
+    # plain FP64 run with the CFL number scaled by 1 + 1e-7, the FP64 result's own
+    # sensitivity to a perturbation at FP32 resolution
+    t_end = [f64.time(m)[0] for m in range(len(probs))]
+    acc, extra, t_mis = run_to_times(ctx, probs, t_end, PREC_MIXED, W + K + NT, tuned)
+    ref2, _, _ = run_to_times(ctx, [pb.copy(cfl=pb.cfl * (1.0 + 1.0e-7)) for pb in probs], t_end, PREC_FP64,
+                              W + K + NT, None)
+    kinds = ("sod", "noh", "sedov")
+    st = {k: {"l1_rho": [], "l1_u": [], "floor_rho": [], "mass": [], "energy": [], "trunc": []} for k in kinds}
+    mm, em = acc.conserved_totals()
+    mf, ef = f64.conserved_totals()
+    for m, pb in enumerate(probs):
+        a = acc.update_cpu(m)
+        b = f64.update_cpu(m)
+        c = ref2.update_cpu(m)
+        w = A.spherical_volumes(pb.n[0])
+        d = st[[k for k in kinds if "_" + k + "_" in pb.name][0]]
+        d["l1_rho"].append(A.l1_rel(a[:, 0], b[:, 0], w))
+        d["l1_u"].append(A.l1_rel(a[:, 1], b[:, 1], w))
+        d["floor_rho"].append(A.l1_rel(c[:, 0], b[:, 0], w))
+        d["mass"].append(abs(mm[m] - mf[m]) / abs(mf[m]))
+        d["energy"].append(abs(em[m] - ef[m]) / abs(ef[m]))
+        if "noh" in pb.name:
+            r = (np.arange(pb.n[0]) + 0.5) * pb.dx[0]
+            d["trunc"].append(A.l1_rel(b[:, 0], A.noh_spherical(r, t_end[m], pb.gam)[:, 0], w))
+    acc.close()
+    ref2.close()
+    f64.close()
+
+    def mm_(v):
+        v = np.asarray(v, dtype=np.float64)
+        return {"median": float(np.median(v)), "max": float(np.max(v))} if v.size else None
+
+    accuracy = {"compared_at": "equal physical time: each problem's time after %d plain FP64 steps "
+                               "(mixed: %d + %d steps, last step landing on that time; max relative time "
+                               "mismatch %.1e)" % (W + K + NT, W + K + NT, extra, t_mis),
+                "fp64_floor": "plain FP64 with CFL x (1 + 1e-7), same end times"}
+    for k in kinds:
+        d = st[k]
+        e = {"count": len(d["l1_rho"]), "l1_rho_mixed_vs_fp64": mm_(d["l1_rho"]),
+             "l1_u_mixed_vs_fp64": mm_(d["l1_u"]), "l1_rho_fp64_floor": mm_(d["floor_rho"]),
+             "mass_drift_vs_fp64": mm_(d["mass"]), "energy_drift_vs_fp64": mm_(d["energy"])}
+        if d["trunc"]:
+            e["l1_rho_fp64_vs_analytic"] = mm_(d["trunc"])
+            e["mixed_over_truncation"] = mm_(np.asarray(d["l1_rho"]) / np.asarray(d["trunc"]))
+            e["fp64_floor_over_truncation"] = mm_(np.asarray(d["floor_rho"]) / np.asarray(d["trunc"]))
+        accuracy[k] = e
+
+    # ---- one problem at a time through the plain FP64 sweep (every 32nd problem)
+    import torch
+    sample = probs[::32]
+    K1 = min(K, 100)
+    ms_one, zu_one = 0.0, 0
+    for pb in sample:
+        s = Solver(pb, precision=PREC_FP64, device=ctx.local)
+        s.step(W)
+        s.synchronize()
+        stream = torch.cuda.ExternalStream(s.stream, device=ctx.local)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.step(K1)
+        e1.record(stream)
+        e1.synchronize()
+        ms_one += e0.elapsed_time(e1)
+        zu_one += pb.ncell * K1
+        s.close()
+    one_rate = zu_one / (ms_one / 1e3)
+
+    # ---- e2e through the public API with host buffers
+    def make(upload):
+        s = Solver(probs, precision=PREC_MIXED, device=ctx.local, upload=upload)
+        s.set_launch_config(**tuned)
+        return s
+    ms_e2e, h2d, d2h = e2e_run(ctx, make, probs, K, W)
+    e2e = ctx.world * ncell * K / (ms_e2e / 1e3)
+
+    if ctx.rank != 0:
+        return
+    peak, peak_kind = read_peaks()
+    b_stage1 = 120.0   # 1-D second stage: read stage state + base state, write new state
+    achieved = b_stage1 * ncell / (st_mix["stage1"] / 1e3) / 1e9
+    traffic = read_profile_value("stage1d_mixed_ensemble_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+        "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms_mix / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": dict(ensemble_config(probs, ctx.world),
+                       precision="mixed: FP32 reconstruction/limiting/Riemann, FP64 state/fluxes/"
+                                 "sources/update/dt",
+                       launch=tuned, autotune_ms_per_step=tune_ms),
+        "gpu_launches": 4 * K,
+        "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / K,
+                "d2h_bytes_per_step": d2h / K,
+                "timed": "upload of all %d initial states (pinned H2D) + %d steps + download of all "
+                         "final states (pinned D2H)" % (len(probs), K),
+                "ms": ms_e2e},
+        "comparison": {
+            "fp64_batched": {"value": ctx.world * ncell * K / (ms_f64 / 1e3), "ms_per_step": ms_f64 / K,
+                             "stage_ms": st_f64},
+            "fp64_one_at_a_time": {"value": one_rate, "sample": "%d problems (every 32nd), %d steps "
+                                                                "each, one solver at a time" % (len(sample), K1)},
+            "mixed_over_fp64_one_at_a_time": value / (ctx.world * one_rate),
+            "mixed_over_fp64_batched": ms_f64 / ms_mix,
+        },
+        "accuracy": accuracy,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "stage1d_mixed_kernel<%d,1> (second RK stage)" % tuned["threads"],
+                     "kernel_ms": st_mix["stage1"], "stage0_ms": st_mix["stage0"],
+                     "algorithmic_bytes_per_zone": b_stage1,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_ensemble(probs)
+    print(json.dumps(line), flush=True)
+
+
+def run_kh(args, ctx):
+    import medusa_b200
+    from medusa_b200 import problems as P
+
+    K, W = args.steps, args.warmup
+    pb = P.kelvin_helmholtz(NX)
+    ncell = pb.ncell
+    s = medusa_b200.Solver(pb, device=ctx.local)
+    s.step(W)
+    s.synchronize()
+    ms, clocks = timed_steps(ctx, s, K, sample_clocks=True)
+    value = ctx.world * ncell * K / (ms / 1e3)
+    st = stage_times(s, min(K, 20))
+    s.close()
+    ms_e2e, h2d, d2h = e2e_run(ctx, lambda upload: medusa_b200.Solver(pb, device=ctx.local, upload=upload),
+                               [pb], K, W)
+    e2e = ctx.world * ncell * K / (ms_e2e / 1e3)
+    if ctx.rank != 0:
+        return
+    peak, peak_kind = read_peaks()
+    b_stage1 = 240.0
+    achieved = b_stage1 * ncell / (st["stage1"] / 1e3) / 1e9
+    traffic = read_profile_value("stage2d_kh2048_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+        "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "kelvin_helmholtz_2d_%dx%d_fp64" % (NX, NX), "global_batch": ctx.world,
+                   "seq_len": ncell, "parallelism": "replicas" if ctx.world > 1 else "single",
+                   "precision": "plain FP64 (reference operation order)",
+                   "l2": "inputs larger than L2 (state 2 x 168 MB)"},
+        "gpu_launches": 6 * K,
+        "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / K,
+                "d2h_bytes_per_step": d2h / K,
+                "timed": "upload initial state (pinned H2D) + %d steps + download state (pinned D2H)" % K,
+                "ms": ms_e2e},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "second RK stage (xsweep2d_kernel<1> + ysweep2d_kernel<1>)",
+                     "kernel_ms": st["stage1"], "stage0_ms": st["stage0"],
+                     "algorithmic_bytes_per_zone": b_stage1,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_kh(pb)
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
+    if args.steps is None:
+        args.steps = 1000 if args.workload == "ensemble" else 200
 
-    world, rank, local, dist = dist_setup()
-    if args.impl == "reference":
-        run_reference_arm(args, world, rank)
-        if dist is not None:
-            dist.destroy_process_group()
-        return
-
-    import numpy as np
-    import torch
-    import medusa_b200
-    from medusa_b200 import problems as P
-
-    torch.cuda.set_device(local)
-    pb = P.kelvin_helmholtz(NX)
-    ncell = pb.ncell
-    K, W = args.steps, args.warmup
-
-    s = medusa_b200.Solver(pb, device=local)
-    stream = torch.cuda.ExternalStream(s.stream, device=local)
-    s.step(W)
-    s.synchronize()
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    # ---- value: K steps, state resident in HBM
-    sampler = ClockSampler(local)
-    sampler.start()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    s.step(K)
-    e1.record(stream)
-    e1.synchronize()
-    s.synchronize()
-    barrier()
-    clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if dist is not None:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = world * ncell * K / (ms / 1e3)
-
-    # ---- per-kernel timers (roofline of the dominant kernel)
-    s.set_timing(True)
-    nt = min(K, 20)
-    s.step(nt)
-    s.synchronize()
-    tm = s.timers()
-    s.set_timing(False)
-    st0 = tm["stage0"][0] / max(1, tm["stage0"][1])
-    st1 = tm["stage1"][0] / max(1, tm["stage1"][1])
-    peak, peak_kind = read_peaks()
-    achieved = B_ALG_STAGE1 * ncell / (st1 / 1e3) / 1e9
-    traffic = read_profile_traffic()
-
-    # ---- e2e: pinned host buffers, upload + K steps + download in the timed region
-    h_in = torch.from_numpy(np.ascontiguousarray(pb.ic)).pin_memory()
-    h_out = torch.empty_like(h_in).pin_memory()
-    s2 = medusa_b200.Solver(pb, device=local, upload=False)
-    stream2 = torch.cuda.ExternalStream(s2.stream, device=local)
-    s2.upload_ptr(0, h_in.data_ptr())
-    s2.step(W)
-    s2.synchronize()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    f0.record(stream2)
-    s2.upload_ptr(0, h_in.data_ptr())
-    s2.step(K)
-    s2.download_ptr(0, h_out.data_ptr())
-    f1.record(stream2)
-    f1.synchronize()
-    barrier()
-    ms_e2e = f0.elapsed_time(f1)
-    if dist is not None:
-        tt = torch.tensor([ms_e2e], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_e2e = float(tt.item())
-    e2e = world * ncell * K / (ms_e2e / 1e3)
-    nbytes = ncell * 5 * 8
-    s2.close()
-    s.close()
-
-    if rank == 0:
-        line = {
-            "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
-            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "kelvin_helmholtz_2d_%dx%d_fp64" % (NX, NX), "global_batch": world,
-                       "seq_len": ncell, "parallelism": "replicas" if world > 1 else "single",
-                       "precision": "plain FP64 (reference operation order)",
-                       "l2": "inputs larger than L2 (state 2 x 168 MB)"},
-            "gpu_launches": 4 * K,
-            "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": nbytes / K,
-                    "d2h_bytes_per_step": nbytes / K,
-                    "timed": "upload initial state (pinned H2D) + %d steps + download state (pinned D2H)" % K,
-                    "ms": ms_e2e},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "stage2d_kernel<1> (second RK stage)",
-                         "kernel_ms": st1, "stage0_ms": st0,
-                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
-            "clocks": clocks,
-        }
-        if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline_reference(pb)
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.destroy_process_group()
+    ctx = Ctx(*dist_setup())
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ctx)
+            return
+        import torch
+        torch.cuda.set_device(ctx.local)
+        if args.workload == "ensemble":
+            run_ensemble(args, ctx)
+        else:
+            run_kh(args, ctx)
+    finally:
+        if ctx.dist is not None:
+            ctx.dist.destroy_process_group()
 
 
 if __name__ == "__main__":

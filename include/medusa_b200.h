@@ -63,12 +63,12 @@ extern "C" {
 
 /*
  * One problem.  Replaces the compile-time switches of setup.mk/build.h (NDIM, GEOM,
- * EOS; Makefile:157-212), the run-time keys of the input.* file that the sweep reads
- * (io.c:4979-5785: n1 n2 n3 cfl dt_init_safety dt_grow_safety initial_dt dtmax dtmin
- * tmax hydro_interp_order) and what the problem hooks set (init_grid: startx, dx;
- * init_problem: gam/Kpoly, bc[]; prob_bounds).  The geometry tables that the
- * reference builds in init_geometry() (geometry.c:4-63) are rebuilt from these fields
- * by the library, bit-identically.
+ * EOS, ENFORCE_FLOORS; Makefile:157-212), the run-time keys of the input.* file that
+ * the sweep reads (io.c:4979-5785: n1 n2 n3 cfl dt_init_safety dt_grow_safety
+ * initial_dt dtmax dtmin tmax hydro_interp_order) and what the problem hooks set
+ * (init_grid: startx, dx; init_problem: gam/Kpoly, bc[], rho_floor/e_floor;
+ * prob_bounds).  The geometry tables that the reference builds in init_geometry()
+ * (geometry.c:4-63) are rebuilt from these fields by the library, bit-identically.
  */
 typedef struct mdg_problem_desc {
   int ndim;                 /* 1 or 2 */
@@ -83,6 +83,8 @@ typedef struct mdg_problem_desc {
   int prob_kind;            /* MDG_PROB_* used by MDG_BC_PROB boundaries */
   double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
   int hydro_interp_order;   /* 1, 2 (linear) or 3 (parabolic) */
+  int enforce_floors;       /* the ENFORCE_FLOORS build switch (fluid.c:43-46): 0 or 1 */
+  double rho_floor, e_floor;/* floors set by the problem hook (io.c:5081-5082 defaults -1) */
 } mdg_problem_desc;
 
 typedef struct mdg_solver mdg_solver;   /* opaque */
@@ -140,6 +142,37 @@ const char *mdg_last_error_message(void);
 #define MDG_NTIMERS         4
 int mdg_set_timing(mdg_solver *s, int enable);
 int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
+
+/*
+ * No counterpart in the reference (its launch shapes are compile-time constants).
+ * Launch shape of a solver's step sequence:
+ *   threads          mixed 1-D sweep: threads per CTA, 64, 128 or 256; a tile holds
+ *                    threads-2 zones (the FP64 sweeps ignore it: 128);
+ *   ctas_per_sm      mixed 1-D sweep: 0 = one CTA per tile; k > 0 = k persistent CTAs
+ *                    per SM that pull (problem, tile) items from a device work queue;
+ *   steps_per_graph  steps captured in one CUDA graph and replayed by mdg_step
+ *                    (0 = direct launches; timing enabled always launches directly).
+ */
+typedef struct mdg_launch_config {
+  int threads;
+  int ctas_per_sm;
+  int steps_per_graph;
+} mdg_launch_config;
+int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg);
+int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg);
+
+/* Time every admissible (threads, ctas_per_sm) of the mixed sweep over trial_steps
+ * steps of the solver's own problems, keep the fastest and restore the state, times
+ * and error flag as they were.  best/ms_per_step may be NULL.  MDG_ERR_NOTIMPL for FP64
+ * solvers, whose shapes are fixed. */
+int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double *ms_per_step);
+
+/* Conserved totals of every problem after all queued work: mass[m] = sum rho dV and
+ * energy[m] = sum (rho v.v/2 + u) dV over the interior zones, each summed in FP64 with
+ * compensated (Neumaier) summation.  The integrands of calculate_total_mass and
+ * calculate_total_energy (utils.c:2337-2361, 2581-2612; without the gravitational
+ * term), which the reference sums in plain serial order. */
+int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy);
 
 /*
  * No counterpart in the reference.  A 1-D advance that allocates nothing, for callers

@@ -1,0 +1,147 @@
+"""Analytic solutions and error norms used to state the accuracy of a run.
+
+* :func:`exact_riemann` - the exact solution of the 1-D Riemann problem of a gamma-law gas
+  (Godunov's exact solver as described in Toro, "Riemann Solvers and Numerical Methods for
+  Fluid Dynamics", 3rd ed., ch. 4: Newton iteration on the star pressure, then sampling);
+  the analytic answer of the Sod shock tube (problems/init_sod.c).
+* :func:`noh_spherical` - the spherical Noh implosion (Noh 1987, J. Comput. Phys. 72, 78):
+  a shock moving out at D = (gamma-1) v0 / 2 behind which the gas is at rest with density
+  rho0 ((gamma+1)/(gamma-1))^3 and specific internal energy v0^2/2; ahead of it the inflow
+  is compressed geometrically, rho = rho0 (1 + v0 t / r)^2
+  (problems/init_spherical_noh.c:63-79 drives the outer boundary with that inflow).
+* :func:`l1_rel` - volume-weighted relative L1 distance, sum |a-b| dV / sum |b| dV.
+
+Primitive states follow the library's layout: rho, u (internal energy density), v1, v2, v3.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+
+def _pressure_function(p, rk, pk, ck, gam):
+    """Toro's f_K(p) and its derivative for one side K of the Riemann problem."""
+    if p > pk:   # shock
+        A = 2.0 / ((gam + 1.0) * rk)
+        B = (gam - 1.0) / (gam + 1.0) * pk
+        q = math.sqrt(A / (p + B))
+        return (p - pk) * q, q * (1.0 - 0.5 * (p - pk) / (B + p))
+    # rarefaction
+    e = (gam - 1.0) / (2.0 * gam)
+    f = 2.0 * ck / (gam - 1.0) * ((p / pk) ** e - 1.0)
+    return f, (p / pk) ** (-(gam + 1.0) / (2.0 * gam)) / (rk * ck)
+
+
+def exact_riemann(left, right, gam: float, x: np.ndarray, t: float, x0: float = 0.5):
+    """Exact solution (rho, v, p) at points x and time t > 0 of the Riemann problem with
+    left/right states (rho, v, p) separated at x0."""
+    rl, ul, pl = left
+    rr, ur, pr = right
+    cl, cr = math.sqrt(gam * pl / rl), math.sqrt(gam * pr / rr)
+    # star pressure: Newton iteration from the two-rarefaction guess
+    e = (gam - 1.0) / (2.0 * gam)
+    p = ((cl + cr - 0.5 * (gam - 1.0) * (ur - ul)) / (cl / pl ** e + cr / pr ** e)) ** (1.0 / e)
+    p = max(p, 1.0e-12)
+    for _ in range(100):
+        fl, dl = _pressure_function(p, rl, pl, cl, gam)
+        fr, dr = _pressure_function(p, rr, pr, cr, gam)
+        pn = p - (fl + fr + ur - ul) / (dl + dr)
+        pn = max(pn, 1.0e-14)
+        done = abs(pn - p) < 1.0e-15 * (pn + p)
+        p = pn
+        if done:
+            break
+    fl, _ = _pressure_function(p, rl, pl, cl, gam)
+    fr, _ = _pressure_function(p, rr, pr, cr, gam)
+    us = 0.5 * (ul + ur) + 0.5 * (fr - fl)
+    gm, gp = gam - 1.0, gam + 1.0
+    s = (np.asarray(x, dtype=np.float64) - x0) / t
+    rho, vel, pre = np.empty_like(s), np.empty_like(s), np.empty_like(s)
+    for k, sk in enumerate(s):
+        if sk <= us:   # left of the contact
+            if p > pl:
+                sh = ul - cl * math.sqrt(gp / (2 * gam) * p / pl + gm / (2 * gam))
+                if sk <= sh:
+                    rho[k], vel[k], pre[k] = rl, ul, pl
+                else:
+                    rho[k] = rl * (p / pl + gm / gp) / (gm / gp * p / pl + 1.0)
+                    vel[k], pre[k] = us, p
+            else:
+                shl = ul - cl
+                cs = cl * (p / pl) ** e
+                stl = us - cs
+                if sk <= shl:
+                    rho[k], vel[k], pre[k] = rl, ul, pl
+                elif sk > stl:
+                    rho[k], vel[k], pre[k] = rl * (p / pl) ** (1.0 / gam), us, p
+                else:
+                    c = 2.0 / gp * (cl + gm / 2.0 * (ul - sk))
+                    vel[k] = 2.0 / gp * (cl + gm / 2.0 * ul + sk)
+                    rho[k] = rl * (c / cl) ** (2.0 / gm)
+                    pre[k] = pl * (c / cl) ** (2.0 * gam / gm)
+        else:          # right of the contact
+            if p > pr:
+                sh = ur + cr * math.sqrt(gp / (2 * gam) * p / pr + gm / (2 * gam))
+                if sk >= sh:
+                    rho[k], vel[k], pre[k] = rr, ur, pr
+                else:
+                    rho[k] = rr * (p / pr + gm / gp) / (gm / gp * p / pr + 1.0)
+                    vel[k], pre[k] = us, p
+            else:
+                shr = ur + cr
+                cs = cr * (p / pr) ** e
+                stl = us + cs
+                if sk >= shr:
+                    rho[k], vel[k], pre[k] = rr, ur, pr
+                elif sk < stl:
+                    rho[k], vel[k], pre[k] = rr * (p / pr) ** (1.0 / gam), us, p
+                else:
+                    c = 2.0 / gp * (cr - gm / 2.0 * (ur - sk))
+                    vel[k] = 2.0 / gp * (-cr + gm / 2.0 * ur + sk)
+                    rho[k] = rr * (c / cr) ** (2.0 / gm)
+                    pre[k] = pr * (c / cr) ** (2.0 * gam / gm)
+    return rho, vel, pre
+
+
+def sod_exact_state(n1: int, t: float, gam: float = 1.4) -> np.ndarray:
+    """Zone-centre samples [n1, 5] of the exact Sod solution (left 1, 0, 1; right 0.125,
+    0, 0.1; interface at 0.5) on [0, 1]."""
+    x = (np.arange(n1) + 0.5) / n1
+    rho, v, p = exact_riemann((1.0, 0.0, 1.0), (0.125, 0.0, 0.1), gam, x, t, 0.5)
+    out = np.zeros((n1, 5))
+    out[:, 0], out[:, 1], out[:, 2] = rho, p / (gam - 1.0), v
+    return out
+
+
+def noh_spherical(r: np.ndarray, t: float, gam: float, v0: float = 1.0, rho0: float = 1.0,
+                  u0: float = 1.0e-6) -> np.ndarray:
+    """Spherical Noh solution [len(r), 5] at radii r and time t (inflow speed v0, upstream
+    density rho0 and internal energy density u0/(gam-1) at t=0)."""
+    r = np.asarray(r, dtype=np.float64)
+    rs = 0.5 * (gam - 1.0) * v0 * t
+    out = np.zeros((r.size, 5))
+    inside = r < rs
+    rho_in = rho0 * ((gam + 1.0) / (gam - 1.0)) ** 3
+    rho_out = rho0 * (1.0 + v0 * t / np.maximum(r, 1.0e-300)) ** 2
+    out[:, 0] = np.where(inside, rho_in, rho_out)
+    # behind the shock: specific internal energy v0^2/2; ahead: adiabatic compression
+    u_out = u0 / (gam - 1.0) * (rho_out / rho0) ** gam
+    out[:, 1] = np.where(inside, rho_in * 0.5 * v0 * v0, u_out)
+    out[:, 2] = np.where(inside, 0.0, -v0)
+    return out
+
+
+def spherical_volumes(n1: int, r_lo: float = 0.0, r_hi: float = 1.0) -> np.ndarray:
+    """Zone volumes (up to the constant 4 pi / 3) of a uniform radial grid."""
+    e = np.linspace(r_lo, r_hi, n1 + 1)
+    return e[1:] ** 3 - e[:-1] ** 3
+
+
+def l1_rel(a: np.ndarray, b: np.ndarray, w=None) -> float:
+    """sum |a - b| w / sum |b| w (w = zone volumes; uniform if None)."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    w = np.ones_like(b) if w is None else np.asarray(w, dtype=np.float64)
+    den = float(np.sum(np.abs(b) * w))
+    return float(np.sum(np.abs(a - b) * w)) / (den if den > 0.0 else 1.0)

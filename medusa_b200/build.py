@@ -5,7 +5,8 @@
 Produces medusa_b200/_lib/libmedusa_b200.so (exports exactly the mdg_* entry points of
 include/medusa_b200.h).  The FP64 sweep translation units are compiled with
 -fmad=false and the host code with -ffp-contract=off: no multiply-add contraction, so
-every product and sum rounds as in the reference's CPU build.
+every product and sum rounds as in the reference's CPU build.  The mixed-precision
+sweep (mdg_sweep1d_mixed.cu) is compiled with -use_fast_math instead.
 """
 from __future__ import annotations
 
@@ -22,9 +23,13 @@ LIBDIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(LIBDIR, "libmedusa_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["mdg_capi.cu", "mdg_sweep1d.cu", "mdg_sweep2d.cu", "mdg_misc.cu", "mdg_geometry.cpp",
-           "mdg_noalloc.cu"]
-HEADERS = ["mdg_internal.h", "mdg_hydro.cuh", "mdg_kernels.cuh"]
+SOURCES = ["mdg_capi.cu", "mdg_sweep1d.cu", "mdg_sweep1d_mixed.cu", "mdg_sweep2d.cu", "mdg_misc.cu",
+           "mdg_geometry.cpp", "mdg_noalloc.cu"]
+HEADERS = ["mdg_internal.h", "mdg_hydro.cuh", "mdg_kernels.cuh", "mdg_load1d.cuh"]
+# The mixed-precision sweep: fast FP32 division/square root and multiply-add contraction
+# (its FP64 parts are not required to round like the reference's).
+MIXED_FLAGS = ["-use_fast_math"]
+FLAGS = {"mdg_sweep1d_mixed.cu": MIXED_FLAGS}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -54,7 +59,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
         if not force and _newer(obj, [sp] + hdrs + [os.path.abspath(__file__)]):
             continue
-        cmd = [nvcc(), "-c", sp, "-o", obj, "-std=c++17", "-O3", "-lineinfo", "-fmad=false",
+        fp = FLAGS.get(src, ["-fmad=false"])
+        cmd = [nvcc(), "-c", sp, "-o", obj, "-std=c++17", "-O3", "-lineinfo"] + fp + [
                "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-I", INCLUDE] + ARCH
         if verbose:
             cmd += ["-Xptxas", "-v"]

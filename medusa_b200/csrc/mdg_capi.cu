@@ -12,6 +12,8 @@ namespace mdg {
 void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
 void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area0, double &area1);
+void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
+int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
 }
 
 using namespace mdg;
@@ -40,6 +42,17 @@ struct mdg_solver {
   double *d_stage = nullptr;      // AoS staging buffer, 5 doubles per zone of the largest problem
   int64_t max_cells = 0;
   int *d_err = nullptr;
+  // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
+  float *d_mx = nullptr;
+  WorkQueue *d_queue = nullptr;
+  Tile *d_mtiles = nullptr;
+  int mtiles_cap = 0, nmtiles = 0;
+  int num_sms = 0;
+  mdg_launch_config cfg{128, 0, 10};
+  // CUDA graph of cfg.steps_per_graph steps (rebuilt when the launch shape changes)
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  double *d_totals = nullptr;
   bool timing = false;
   cudaEvent_t ev[MDG_NTIMERS][2] = {};
   double tms[MDG_NTIMERS] = {0, 0, 0, 0};
@@ -74,6 +87,7 @@ static int validate(const mdg_problem_desc &d, int ndim0, std::string &why)
   if (!(d.dx[0] > 0.0) || (d.ndim == 2 && !(d.dx[1] > 0.0))) return bad("dx must be positive");
   if (!(d.gam > 1.0)) return bad("gam must exceed 1");
   if (!(d.cfl > 0.0)) return bad("cfl must be positive");
+  if (d.enforce_floors != 0 && d.enforce_floors != 1) return bad("enforce_floors must be 0 or 1");
   if (d.ndim == 1) {
     if (d.geom != MDG_CARTESIAN && d.geom != MDG_SPHERICAL) return bad("1-D geometry must be Cartesian or spherical");
     int lo = d.bc_lo[0], hi = d.bc_hi[0];
@@ -110,6 +124,41 @@ static int validate(const mdg_problem_desc &d, int ndim0, std::string &why)
   return MDG_OK;
 }
 
+// Tile list of the mixed sweep for nt threads per CTA (tiles of nt-2 zones) and the work
+// queue's item count.  Caller has synchronized the solver's stream.
+static int build_mixed_tiles(mdg_solver *s, int nt)
+{
+  const int tl = nt - 2;
+  std::vector<Tile> t;
+  for (int m = 0; m < s->nprob; m++)
+    for (int i0 = 0; i0 < s->hprobs[m].n1; i0 += tl) t.push_back(Tile{m, i0, 0, 0});
+  if ((int)t.size() > s->mtiles_cap) {
+    cudaFree(s->d_mtiles);
+    s->d_mtiles = nullptr;
+    s->mtiles_cap = 0;
+    cudaError_t e = cudaMalloc(&s->d_mtiles, sizeof(Tile) * t.size());
+    if (e != cudaSuccess) return fail(MDG_ERR_OUTOFMEM, std::string("tile list: ") + cudaGetErrorString(e));
+    s->mtiles_cap = (int)t.size();
+  }
+  CK(cudaMemcpy(s->d_mtiles, t.data(), sizeof(Tile) * t.size(), cudaMemcpyHostToDevice));
+  WorkQueue q{{0u, 0u}, (int)t.size(), 0};
+  CK(cudaMemcpy(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice));
+  s->nmtiles = (int)t.size();
+  return MDG_OK;
+}
+
+// CTAs of one mixed-sweep launch: one per tile, or ctas_per_sm persistent CTAs per SM
+// (bounded by the occupancy of the kernel and by the number of tiles)
+static int mixed_grid(const mdg_solver *s)
+{
+  if (s->cfg.ctas_per_sm <= 0) return s->nmtiles;
+  int k = mixed_max_ctas_per_sm(s->cfg.threads);
+  if (k <= 0) k = 1;
+  if (s->cfg.ctas_per_sm < k) k = s->cfg.ctas_per_sm;
+  const int64_t g = (int64_t)k * s->num_sms;
+  return (int)(g < s->nmtiles ? g : s->nmtiles);
+}
+
 static void free_all(mdg_solver *s)
 {
   if (!s) return;
@@ -119,6 +168,8 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles);
   cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
   cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
+  cudaFree(s->d_mx); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals);
+  if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -150,13 +201,16 @@ const char *mdg_last_error_message(void) { return g_msg.c_str(); }
 int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int device, mdg_solver **out)
 {
   if (!descs || nprob <= 0 || !out) return fail(MDG_ERR_INVALID, "descs/nprob/out");
-  if (precision != MDG_PREC_FP64) return fail(MDG_ERR_NOTIMPL, "only MDG_PREC_FP64 is built into this solver entry point");
+  if (precision != MDG_PREC_FP64 && precision != MDG_PREC_MIXED) return fail(MDG_ERR_INVALID, "precision");
   *out = nullptr;
   const int ndim = descs[0].ndim;
   for (int m = 0; m < nprob; m++) {
     std::string why;
     int rc = validate(descs[m], ndim, why);
     if (rc != MDG_OK) return fail(rc, "problem " + std::to_string(m) + ": " + why);
+    if (precision == MDG_PREC_MIXED && (descs[m].ndim != 1 || descs[m].hydro_interp_order != 3))
+      return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
+                                       ": the mixed-precision sweep is built for 1-D parabolic reconstruction");
   }
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
@@ -191,6 +245,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (d.ndim == 2) cartesian_2d_constants(d, P.vol, P.area0, P.area1);
     P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
     P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
+    P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
     s->hprobs.push_back(P);
     const int64_t nc = (int64_t)P.n1 * P.n2;
     if (nc > s->max_cells) s->max_cells = nc;
@@ -218,10 +273,17 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   std::vector<double> h_rc0((size_t)RC_NFIELDS * rc0), h_rc1, h_geo;
   if (ndim == 2) h_rc1.assign((size_t)RC_NFIELDS * rc1, 0.0);
   else h_geo.assign((size_t)GF_NFIELDS * rc0, 0.0);
+  std::vector<float> h_mx;
+  if (precision == MDG_PREC_MIXED) h_mx.assign((size_t)MX_NFIELDS * rc0, 0.0f);
   for (int m = 0; m < nprob; m++) {
     build_recon_table(descs[m], 0, h_rc0.data(), rc0, s->hprobs[m].geo_off);
-    if (ndim == 2) build_recon_table(descs[m], 1, h_rc1.data(), rc1, s->hprobs[m].rc1_off);
-    else build_geo_1d(descs[m], h_geo.data(), rc0, s->hprobs[m].geo_off);
+    if (ndim == 2) {
+      build_recon_table(descs[m], 1, h_rc1.data(), rc1, s->hprobs[m].rc1_off);
+    } else {
+      build_geo_1d(descs[m], h_geo.data(), rc0, s->hprobs[m].geo_off);
+      s->hprobs[m].sparse_conn = conn_is_sparse(h_geo.data(), rc0, s->hprobs[m].geo_off, descs[m].n1 + 2 * NG);
+    }
+    if (precision == MDG_PREC_MIXED) build_mixed_table(descs[m], 0, h_mx.data(), rc0, s->hprobs[m].geo_off);
   }
 
   auto cleanup_fail = [&](int code) { free_all(s); delete s; return code; };
@@ -245,6 +307,14 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMalloc(&s->d_state, sizeof(double) * nstate * NPRIM * cell));
   CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
   CKC(cudaMalloc(&s->d_err, sizeof(int)));
+  CKC(cudaMalloc(&s->d_totals, sizeof(double) * 2 * nprob));
+  CKC(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
+  CKC(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
+  if (precision == MDG_PREC_MIXED) {
+    CKC(cudaMalloc(&s->d_mx, sizeof(float) * h_mx.size()));
+    CKC(cudaMemcpy(s->d_mx, h_mx.data(), sizeof(float) * h_mx.size(), cudaMemcpyHostToDevice));
+  }
+  CKC(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock0, sh > 0 ? sh : 1));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock1, sh > 0 ? sh : 1));
 
@@ -266,7 +336,12 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   s->tb.rc0 = s->d_rc0; s->tb.rc0_stride = rc0;
   s->tb.rc1 = s->d_rc1; s->tb.rc1_stride = rc1;
   s->tb.geo = s->d_geo; s->tb.geo_stride = rc0;
+  s->tb.mx = s->d_mx;
 #undef CKC
+  if (precision == MDG_PREC_MIXED) {
+    int rc = build_mixed_tiles(s, s->cfg.threads);
+    if (rc != MDG_OK) { free_all(s); delete s; return rc; }
+  }
   *out = s;
   return MDG_OK;
 }
@@ -289,19 +364,28 @@ int mdg_upload_state(mdg_solver *s, int prob, const double *prim)
 static int queue_steps(mdg_solver *s, int nsteps)
 {
   auto mark = [&](int k, int e) { if (s->timing) cudaEventRecord(s->ev[k][e], s->stream); };
+  const bool mixed = s->precision == MDG_PREC_MIXED;
+  const int mgrid = mixed ? mixed_grid(s) : 0;
+  const bool queue = s->cfg.ctas_per_sm > 0;
   for (int k = 0; k < nsteps; k++) {
     mark(MDG_TIMER_DT, 0);
     launch_dt_finalize(s->d_probs, s->d_times, s->nprob, s->d_err, s->stream);
     mark(MDG_TIMER_DT, 1);
     mark(MDG_TIMER_STAGE0, 0);
-    if (s->ndim == 1)
+    if (mixed)
+      launch_stage1d_mixed(0, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
+                           s->tb, s->P, s->P, s->PH, s->stream);
+    else if (s->ndim == 1)
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
     else
       launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
                      s->P, s->P, s->ACC, s->PH, s->d_shock0, s->d_shock1, s->stream);
     mark(MDG_TIMER_STAGE0, 1);
     mark(MDG_TIMER_STAGE1, 0);
-    if (s->ndim == 1)
+    if (mixed)
+      launch_stage1d_mixed(1, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
+                           s->tb, s->PH, s->P, s->P, s->stream);
+    else if (s->ndim == 1)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     else
       launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
@@ -339,12 +423,179 @@ int mdg_estimate_dt(mdg_solver *s, double *dt_out)
   return MDG_OK;
 }
 
+// Capture cfg.steps_per_graph steps of the launch sequence into a CUDA graph (once per
+// launch shape).  Every kernel argument is fixed for the solver's life; what changes from
+// step to step (dt, times, the work queue) lives in device memory.
+static int ensure_graph(mdg_solver *s)
+{
+  const int k = s->cfg.steps_per_graph;
+  if (s->graph && s->graph_steps == k) return MDG_OK;
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = queue_steps(s, k);
+  const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (rc != MDG_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) {
+    s->graph = nullptr;
+    return fail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+  }
+  s->graph_steps = k;
+  return MDG_OK;
+}
+
+static void drop_graph(mdg_solver *s)
+{
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  s->graph = nullptr;
+  s->graph_steps = 0;
+}
+
 int mdg_step(mdg_solver *s, int nsteps)
 {
   if (!s) return fail(MDG_ERR_INVALID, "solver");
   if (nsteps < 0) return fail(MDG_ERR_INVALID, "nsteps < 0");
   CK(cudaSetDevice(s->device));
-  return queue_steps(s, nsteps);
+  const int k = s->cfg.steps_per_graph;
+  if (s->timing || k <= 0 || nsteps < k) return queue_steps(s, nsteps);
+  int rc = ensure_graph(s);
+  if (rc != MDG_OK) return rc;
+  for (int g = 0; g < nsteps / k; g++) CK(cudaGraphLaunch(s->graph, s->stream));
+  return queue_steps(s, nsteps % k);
+}
+
+int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg)
+{
+  if (!s || !cfg) return fail(MDG_ERR_INVALID, "solver/cfg");
+  *cfg = s->cfg;
+  return MDG_OK;
+}
+
+int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
+{
+  if (!s || !cfg) return fail(MDG_ERR_INVALID, "solver/cfg");
+  if (cfg->threads != 64 && cfg->threads != 128 && cfg->threads != 256)
+    return fail(MDG_ERR_INVALID, "threads must be 64, 128 or 256");
+  if (cfg->ctas_per_sm < 0 || cfg->ctas_per_sm > 64) return fail(MDG_ERR_INVALID, "ctas_per_sm out of [0, 64]");
+  if (cfg->steps_per_graph < 0 || cfg->steps_per_graph > 10000)
+    return fail(MDG_ERR_INVALID, "steps_per_graph out of [0, 10000]");
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize(s->stream));
+  const bool reshape = cfg->threads != s->cfg.threads;
+  if (reshape && s->precision == MDG_PREC_MIXED) {
+    int rc = build_mixed_tiles(s, cfg->threads);
+    if (rc != MDG_OK) return rc;
+  } else if (s->precision == MDG_PREC_MIXED) {
+    WorkQueue q{{0u, 0u}, s->nmtiles, 0};
+    CK(cudaMemcpy(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice));
+  }
+  if (reshape || cfg->ctas_per_sm != s->cfg.ctas_per_sm || cfg->steps_per_graph != s->cfg.steps_per_graph)
+    drop_graph(s);
+  s->cfg = *cfg;
+  return MDG_OK;
+}
+
+int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double *ms_per_step)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  if (trial_steps < 1) return fail(MDG_ERR_INVALID, "trial_steps < 1");
+  if (s->precision != MDG_PREC_MIXED)
+    return fail(MDG_ERR_NOTIMPL, "the FP64 sweeps have fixed launch shapes");
+  CK(cudaSetDevice(s->device));
+  CK(cudaStreamSynchronize(s->stream));
+  // the trials advance the state: keep a copy of everything a step changes
+  const size_t sbytes = sizeof(double) * 2 * NPRIM * s->ncell_total;
+  double *bk = nullptr;
+  ProbTime *bt = nullptr;
+  int berr = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = MDG_OK;
+  auto restore = [&]() -> int {
+    CK(cudaMemcpyAsync(s->d_state, bk, sbytes, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->d_times, bt, sizeof(ProbTime) * s->nprob, cudaMemcpyDeviceToDevice, s->stream));
+    CK(cudaMemcpyAsync(s->d_err, &berr, sizeof(int), cudaMemcpyHostToDevice, s->stream));
+    CK(cudaStreamSynchronize(s->stream));
+    return MDG_OK;
+  };
+  const mdg_launch_config orig = s->cfg;
+  mdg_launch_config bestc = orig;
+  double bestms = 1.0e300;
+  do {
+    if (cudaMalloc(&bk, sbytes) != cudaSuccess || cudaMalloc(&bt, sizeof(ProbTime) * s->nprob) != cudaSuccess) {
+      rc = fail(MDG_ERR_OUTOFMEM, "autotune: no room for the state copy");
+      break;
+    }
+    if (cudaMemcpy(bk, s->d_state, sbytes, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+        cudaMemcpy(bt, s->d_times, sizeof(ProbTime) * s->nprob, cudaMemcpyDeviceToDevice) != cudaSuccess ||
+        cudaMemcpy(&berr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+      rc = fail(MDG_ERR_CUDA, "autotune: set-up");
+      break;
+    }
+    const int threads[3] = {64, 128, 256};
+    const int ctas[9] = {0, 1, 2, 3, 4, 6, 8, 12, 16};
+    const int k = orig.steps_per_graph;
+    const int steps = (k > 0) ? ((trial_steps + k - 1) / k) * k : trial_steps;
+    for (int ti = 0; ti < 3 && rc == MDG_OK; ti++) {
+      const int occ = mixed_max_ctas_per_sm(threads[ti]);
+      for (int ci = 0; ci < 9 && rc == MDG_OK; ci++) {
+        if (ctas[ci] > occ) continue;
+        mdg_launch_config c{threads[ti], ctas[ci], k};
+        if ((rc = mdg_set_launch_config(s, &c)) != MDG_OK) break;
+        if ((rc = restore()) != MDG_OK) break;
+        if ((rc = mdg_step(s, k > 0 ? k : 1)) != MDG_OK) break;   // warm-up (and graph capture)
+        float ms = 0.f;
+        cudaError_t ce = cudaEventRecord(e0, s->stream);
+        if (ce == cudaSuccess && (rc = mdg_step(s, steps)) != MDG_OK) break;
+        if (ce == cudaSuccess) ce = cudaEventRecord(e1, s->stream);
+        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+        if (ce != cudaSuccess) {
+          rc = fail(MDG_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(ce));
+          break;
+        }
+        const double per = ms / steps;
+        if (per < bestms) { bestms = per; bestc = c; }
+      }
+    }
+    if (rc == MDG_OK) rc = mdg_set_launch_config(s, &bestc);
+    else mdg_set_launch_config(s, &orig);
+    const int rc2 = restore();
+    if (rc == MDG_OK) rc = rc2;
+  } while (0);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(bk);
+  cudaFree(bt);
+  if (rc != MDG_OK) return rc;
+  if (best) *best = bestc;
+  if (ms_per_step) *ms_per_step = bestms;
+  return MDG_OK;
+}
+
+int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  CK(cudaSetDevice(s->device));
+  launch_conserved_totals(s->d_probs, s->nprob, s->tb, s->P, s->d_totals, s->stream);
+  CK(cudaGetLastError());
+  std::vector<double> h(2 * (size_t)s->nprob);
+  CK(cudaMemcpyAsync(h.data(), s->d_totals, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  for (int m = 0; m < s->nprob; m++) {
+    if (mass) mass[m] = h[2 * m];
+    if (energy) energy[m] = h[2 * m + 1];
+  }
+  return MDG_OK;
 }
 
 int mdg_download_state(mdg_solver *s, int prob, double *prim, double *eos)

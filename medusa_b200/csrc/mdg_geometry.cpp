@@ -282,3 +282,63 @@ void build_recon_table_into(const mdg_problem_desc &d, int dir, double *tab, int
 }
 
 }  // namespace mdg
+
+namespace mdg {
+
+// FP32 reconstruction weights (MX_* fields, see mdg_internal.h) of direction dir, zone i
+// at column off+i+NG, computed in FP64 from the volume moments.
+void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off)
+{
+  std::vector<double> al, be, ga;
+  build_moments(d, dir, al, be, ga);
+  const int n = (dir == 0) ? d.n1 : d.n2;
+  for (int i = -NG; i < n + NG; i++) {
+    int im = (i - 1 < -NG) ? -NG : i - 1, ip = (i + 1 >= n + NG) ? n + NG - 1 : i + 1;
+    double am = al[im + NG], a0 = al[i + NG], ap = al[ip + NG];
+    double bm = be[im + NG], b0 = be[i + NG], bp = be[ip + NG];
+    double gm = ga[im + NG], g0 = ga[i + NG], gp = ga[ip + NG];
+    double xl = d.startx[dir] + i * d.dx[dir];
+    double xr = d.startx[dir] + (i + 1) * d.dx[dir];
+    double den1 = 1.0 / (am * b0 * gp + a0 * bp * gm + ap * bm * g0 - am * bp * g0 - a0 * bm * gp - ap * b0 * gm);
+    double kAm = (bp * gm * g0 - gp * b0 * gm) * den1, kAp = (gp * bm * g0 - gp * b0 * gm) * den1;
+    double kBm = -(ap * gm * g0 - gp * a0 * gm) * den1, kBp = -(gp * am * g0 - gp * a0 * gm) * den1;
+    double cl2 = xl * xl - a0 / g0, cl1 = xl - b0 / g0, cr2 = xr * xr - a0 / g0, cr1 = xr - b0 / g0;
+    double den2 = 1.0 / ((xl - xr) * (a0 + g0 * xl * xr - b0 * (xl + xr)));
+    double eAl = (g0 * xr - b0) * den2, eAr = (b0 - g0 * xl) * den2;
+    double eBl = (a0 - g0 * xr * xr) * den2, eBr = (g0 * xl * xl - a0) * den2;
+    double dmr = a0 + xr * (g0 * xr - 2.0 * b0), dml = a0 + xl * (g0 * xl - 2.0 * b0);
+    double v[MX_NFIELDS];
+    v[MX_WLM] = kAm * cl2 + kBm * cl1;
+    v[MX_WLP] = kAp * cl2 + kBp * cl1;
+    v[MX_WRM] = kAm * cr2 + kBm * cr1;
+    v[MX_WRP] = kAp * cr2 + kBp * cr1;
+    v[MX_EAL] = eAl;
+    v[MX_EAR] = eAr;
+    v[MX_EBL] = eBl + 2.0 * xl * eAl;
+    v[MX_EBR] = eBr + 2.0 * xl * eAr;
+    v[MX_DXZ] = xr - xl;
+    v[MX_MR] = (-g0 / dmr) * (cl2 - 2.0 * xr * cl1);
+    v[MX_ML] = (-g0 / dml) * (cr2 - 2.0 * xl * cr1);
+    for (int f = 0; f < MX_NFIELDS; f++) tab[f * stride + off + i + NG] = (float)v[f];
+  }
+}
+
+}  // namespace mdg
+
+namespace mdg {
+
+// 1 when every connection coefficient outside SPARSE_CONN is exactly zero in the nrec
+// records of a 1-D geometry table starting at column off.
+int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec)
+{
+  bool keep[27] = {};
+  for (int k = 0; k < NSPARSE_CONN; k++) keep[SPARSE_CONN[k]] = true;
+  for (int k = 0; k < 27; k++) {
+    if (keep[k]) continue;
+    for (int i = 0; i < nrec; i++)
+      if (tab[(GF_CONN + k) * stride + off + i] != 0.0) return 0;
+  }
+  return 1;
+}
+
+}  // namespace mdg

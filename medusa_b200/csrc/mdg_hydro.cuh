@@ -311,8 +311,11 @@ __device__ __forceinline__ void p_to_u(const double *p, double *u, double g0, do
   u[UU] = 0.5 * u[RHO] * vsq + p[UU];
 }
 
-// hydro_u_to_p (fluid.c:27-53, ENFORCE_FLOORS off); u is modified as in the reference
-__device__ __forceinline__ void u_to_p(double *u, double *p, double gc0, double gc1, double gc2)
+// hydro_u_to_p (fluid.c:27-53); u is modified as in the reference.  With floors (the
+// ENFORCE_FLOORS build, fluid.c:43-46) density and internal energy are clamped from below
+// with the reference's MAX (decs.h:628) after the velocities are formed.
+__device__ __forceinline__ void u_to_p(double *u, double *p, double gc0, double gc1, double gc2,
+                                       bool floors = false, double rho_floor = 0.0, double e_floor = 0.0)
 {
   p[RHO] = u[RHO];
   u[U1] /= u[RHO]; u[U2] /= u[RHO]; u[U3] /= u[RHO];
@@ -320,6 +323,10 @@ __device__ __forceinline__ void u_to_p(double *u, double *p, double gc0, double 
   double vsq = 0.0;
   vsq += u[U1] * p[U1]; vsq += u[U2] * p[U2]; vsq += u[U3] * p[U3];
   p[UU] = u[UU] - 0.5 * p[RHO] * vsq;
+  if (floors) {
+    p[RHO] = (p[RHO] > rho_floor) ? p[RHO] : rho_floor;
+    p[UU] = (p[UU] > e_floor) ? p[UU] : e_floor;
+  }
 }
 
 // dt_source_control (step.c:205-223)

@@ -36,6 +36,18 @@ enum ReconField {
   RC_NFIELDS
 };
 
+// FP32 reconstruction weights of one zone for the mixed-precision sweep: para_recon
+// rewritten on the differences dqm = a[i]-a[i-1], dqp = a[i+1]-a[i] (the same parabola,
+// well conditioned in FP32), with the geometry folded into weights computed in FP64:
+//   al - a = WLM dqm + WLP dqp,  ar - a = WRM dqm + WRP dqp          (reconstruct.c:151-163)
+//   second fit  A2 = EAL dl + EAR dr,  B2' = EBL dl + EBR dr  (x measured from x[i]),
+//   extremum at s = -B2'/(2 A2), inside when 0 < s < DXZ, "right" when s > DXZ/2;
+//   moved faces  al = a + MR dr,  ar = a + ML dl                      (reconstruct.c:174-200)
+enum MixField {
+  MX_WLM, MX_WLP, MX_WRM, MX_WRP, MX_EAL, MX_EAR, MX_EBL, MX_EBR, MX_DXZ, MX_MR, MX_ML,
+  MX_NFIELDS
+};
+
 // Per-face and per-zone geometry of 1-D problems (one record per index i+NG).
 enum GeoField {
   GF_AREA,                    // face i: area[0]
@@ -49,6 +61,12 @@ enum GeoField {
   GF_NFIELDS = GF_CONN + 27
 };
 
+// The connection coefficients conn[l][m][n] (index l*9+m*3+n) that the 1-D spherical
+// metric can make non-zero; with every other entry exactly 0.0 the source sum over these
+// nine alone, in the same order, is bit-identical to the full 27-term sum.
+constexpr int NSPARSE_CONN = 9;
+constexpr int SPARSE_CONN[NSPARSE_CONN] = {4, 8, 10, 12, 17, 20, 23, 24, 25};
+
 // Device-side description of one problem.
 struct ProbDev {
   int ndim, geom, eos, interp_order;
@@ -56,6 +74,8 @@ struct ProbDev {
   int bc_lo0, bc_hi0, bc_lo1, bc_hi1;
   int prob_kind;
   int has_src;              // spherical: geometric source terms are computed
+  int sparse_conn;          // 1-D: only the 9 connection coefficients of SPARSE_CONN are non-zero
+  int floors;               // ENFORCE_FLOORS: u_to_p clamps rho and u to the floors below
   int64_t cell_off;         // first zone of this problem in the state arrays
   int64_t geo_off;          // first record (i=-NG) in the 1-D geometry tables
   int64_t rc1_off;          // first record (j=-NG) of the direction-1 recon table (2-D)
@@ -64,6 +84,7 @@ struct ProbDev {
   double dx0, dx1;
   double area0, area1, vol; // Cartesian 2-D constants
   double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
+  double rho_floor, e_floor;
 };
 
 // Time bookkeeping of one problem, resident on the device.

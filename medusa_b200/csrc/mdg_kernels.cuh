@@ -17,7 +17,13 @@ struct Tables {
   int64_t rc1_stride;
   const double *geo;     // 1-D face/zone geometry, GF_NFIELDS x geo_stride
   int64_t geo_stride;
+  const float *mx;       // 1-D FP32 reconstruction weights (mixed precision), MX_NFIELDS x geo_stride
 };
+
+// Device work queue of the persistent mixed-precision sweep: one head counter per RK
+// stage (each stage resets the other's head, so a step needs no reset launch) and the
+// number of (problem, tile) items in the tile list.
+struct WorkQueue { unsigned int head[2]; int ntiles; int pad; };
 
 // One work tile: problem, first output row i0, first output column j0 (2-D).
 struct Tile { int prob; int i0; int j0; int pad; };
@@ -49,6 +55,14 @@ void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile
 void launch_stage2d(int stage, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
                     const Tile *ytiles, int nyt, const Tables &tb, StateSoA stage_state, StateSoA state_n,
                     StateSoA acc, StateSoA out, unsigned char *shock0, unsigned char *shock1, cudaStream_t st);
+// Mixed-precision 1-D stage: nt threads per CTA (tile = nt-2 zones), grid CTAs; with
+// use_queue the CTAs are persistent and pull tiles from q, else CTA b takes tile b.
+void launch_stage1d_mixed(int stage, int nt, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
+                          const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA stage_state,
+                          StateSoA state_n, StateSoA out, cudaStream_t st);
+int mixed_max_ctas_per_sm(int nt);
+void launch_conserved_totals(const ProbDev *probs, int nprob, const Tables &tb, StateSoA s, double *out,
+                             cudaStream_t st);
 void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st);
 void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
 void launch_reset_time(ProbTime *times, int m, cudaStream_t st);

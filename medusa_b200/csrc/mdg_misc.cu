@@ -119,6 +119,65 @@ __global__ void eos_aos_kernel(StateSoA s, const ProbDev *__restrict__ probs, in
   aos[z * 5 + 4] = P.gam;
 }
 
+// Neumaier's compensated summation: s + c carries the sum of the added terms with an
+// error independent of their number (to first order).
+__device__ __forceinline__ void neumaier_add(double &s, double &c, double x)
+{
+  const double t = s + x;
+  if (fabs(s) >= fabs(x)) c += (s - t) + x;
+  else c += (x - t) + s;
+  s = t;
+}
+
+// Mass and total energy of each problem (one CTA per problem): the integrands of
+// calculate_total_mass / calculate_total_energy (utils.c:2337-2361, 2581-2612) summed
+// with compensation per thread and then over the threads in a fixed order.
+__global__ void conserved_totals_kernel(const ProbDev *__restrict__ probs, Tables tb, StateSoA s,
+                                        double *__restrict__ out)
+{
+  __shared__ double sh[4][256];
+  const int m = blockIdx.x;
+  const int t = threadIdx.x;
+  const ProbDev &P = probs[m];
+  const int64_t n = (int64_t)P.n1 * P.n2;
+  double ms = 0.0, mc = 0.0, es = 0.0, ec = 0.0;
+  for (int64_t z = t; z < n; z += blockDim.x) {
+    const int64_t c = P.cell_off + z;
+    double p[NPRIM], u[NPRIM];
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) p[v] = s.v[v][c];
+    double vol = P.vol, g0 = 1.0, g1 = 1.0, g2 = 1.0;
+    if (P.ndim == 1) {
+      const int64_t gi = P.geo_off + z + NG;
+      vol = tb.geo[GF_VOL * tb.geo_stride + gi];
+      g0 = tb.geo[GF_G0 * tb.geo_stride + gi];
+      g1 = tb.geo[GF_G1 * tb.geo_stride + gi];
+      g2 = tb.geo[GF_G2 * tb.geo_stride + gi];
+    }
+    p_to_u(p, u, g0, g1, g2);
+    neumaier_add(ms, mc, p[RHO] * vol);
+    neumaier_add(es, ec, u[UU] * vol);
+  }
+  sh[0][t] = ms; sh[1][t] = mc; sh[2][t] = es; sh[3][t] = ec;
+  __syncthreads();
+  if (t == 0) {
+    double S = 0.0, C = 0.0, E = 0.0, D = 0.0;
+    for (int k = 0; k < (int)blockDim.x; k++) {
+      neumaier_add(S, C, sh[0][k]); C += sh[1][k];
+      neumaier_add(E, D, sh[2][k]); D += sh[3][k];
+    }
+    out[2 * m] = S + C;
+    out[2 * m + 1] = E + D;
+  }
+}
+
+void launch_conserved_totals(const ProbDev *probs, int nprob, const Tables &tb, StateSoA s, double *out,
+                             cudaStream_t st)
+{
+  if (nprob <= 0) return;
+  conserved_totals_kernel<<<nprob, 256, 0, st>>>(probs, tb, s, out);
+}
+
 void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st)
 {
   dt_finalize_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(probs, times, nprob, err);

@@ -29,6 +29,7 @@ namespace mdg {
 void build_recon_table_into(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off,
                             double *al, double *be, double *ga);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
 }
 
 using namespace mdg;
@@ -144,9 +145,11 @@ extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double
   P.gam = d.gam; P.Kpoly = d.Kpoly; P.dx0 = d.dx[0]; P.dx1 = d.dx[1];
   P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
   P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
+  P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
   const int64_t ncol = n1 + 2 * NG;
   build_recon_table_into(d, 0, h_rc, ncol, 0, h_al, h_be, h_ga);
   build_geo_1d(d, h_geo, ncol, 0);
+  P.sparse_conn = conn_is_sparse(h_geo, ncol, 0, (int)ncol);
   int ntiles = 0;
   for (int i0 = 0; i0 < n1; i0 += TILE1) h_tiles[ntiles++] = Tile{0, i0, 0, 0};
 

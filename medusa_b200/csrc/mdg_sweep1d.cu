@@ -14,74 +14,9 @@
 // (problem, tile) work items.
 #include "mdg_hydro.cuh"
 #include "mdg_kernels.cuh"
+#include "mdg_load1d.cuh"
 
 namespace mdg {
-
-// Noh inflow boundary, problems/init_spherical_noh.c:63-79 (ijk_to_r of
-// metric_spherical_general.c:483-496: r = r(beta0/Gamma0), rhat0 = dr/dx = 1).
-__device__ __forceinline__ void prob_bounds_noh(double gam, double b0, double g0, double t, double *w)
-{
-  double x = b0 / g0;
-  double r = fabs(x);
-  w[RHO] = 1.;
-  w[UU] = 1.e-6 / (gam - 1.);
-  w[U1] = -1. / 1.0;
-  w[U2] = 0.;
-  w[U3] = 0.;
-  w[RHO] += t / r;
-  w[RHO] *= w[RHO];
-}
-
-// Zone i (may be a ghost, i in [-NG, n1+NG)) of a 1-D problem: 5 primitives + pressure.
-__device__ __forceinline__ void load_cell_1d(const ProbDev &P, const StateSoA &s, const double *__restrict__ rc,
-                                             int64_t rcs, int i, double t_bc, double *w)
-{
-  const int n = P.n1;
-  const int64_t base = P.cell_off;
-  if (i < -NG) i = -NG;
-  if (i > n + NG - 1) i = n + NG - 1;
-  auto rd = [&](int k, double *o) {
-#pragma unroll
-    for (int v = 0; v < NPRIM; v++) o[v] = s.v[v][base + k];
-  };
-  if (i >= 0 && i < n) {
-    rd(i, w);
-  } else if (i < 0) {
-    switch (P.bc_lo0) {
-      case BC_REFLECT: rd(-1 - i, w); w[U1] *= -1.0; break;
-      case BC_SPHERICAL_ORIGIN: rd(-1 - i, w); w[U1] *= -1.0; w[U3] *= -1.0; break;
-      case BC_PERIODIC: rd(i + n, w); break;
-      case BC_EXTRAP: {
-        double a[NPRIM], b[NPRIM];
-        rd(0, a); rd(1, b);
-#pragma unroll
-        for (int v = 0; v < NPRIM; v++) w[v] = a[v] + i * (b[v] - a[v]);
-      } break;
-      case BC_PROB:
-        prob_bounds_noh(P.gam, __ldg(rc + RC_B0 * rcs + P.geo_off + i + NG),
-                        __ldg(rc + RC_G0 * rcs + P.geo_off + i + NG), t_bc, w);
-        break;
-      default: rd(0, w); break;   // OUTFLOW
-    }
-  } else {
-    switch (P.bc_hi0) {
-      case BC_REFLECT: rd(2 * n - i - 1, w); w[U1] *= -1.0; break;
-      case BC_PERIODIC: rd(i - n, w); break;
-      case BC_EXTRAP: {
-        double a[NPRIM], b[NPRIM];
-        rd(n - 1, a); rd(n - 2, b);
-#pragma unroll
-        for (int v = 0; v < NPRIM; v++) w[v] = a[v] + (i - n + 1) * (a[v] - b[v]);
-      } break;
-      case BC_PROB:
-        prob_bounds_noh(P.gam, __ldg(rc + RC_B0 * rcs + P.geo_off + i + NG),
-                        __ldg(rc + RC_G0 * rcs + P.geo_off + i + NG), t_bc, w);
-        break;
-      default: rd(n - 1, w); break;   // OUTFLOW
-    }
-  }
-  w[5] = eos_press(P.eos, P.gam, P.Kpoly, w[RHO], w[UU]);
-}
 
 template <int STAGE>
 __global__ void __launch_bounds__(NT1)
@@ -179,25 +114,11 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     const double gc0 = __ldg(geo + GF_G0 * gs + gi), gc1 = __ldg(geo + GF_G1 * gs + gi),
                  gc2 = __ldg(geo + GF_G2 * gs + gi);
     // geometric source terms from the stage state (rad_fluid.c:164-192, fluid.c:56-73)
-#pragma unroll
-    for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
     if (P.has_src) {
-      const double press = sv[5][t + 1];
-      double vcov[3] = {gc0 * ph[U1], gc1 * ph[U2], gc2 * ph[U3]};
-      double T[3][3];
+      geo_sources_1d(geo, gs, gi, P.sparse_conn != 0, ph, sv[5][t + 1], gc0, gc1, gc2, src);
+    } else {
 #pragma unroll
-      for (int l = 0; l < 3; l++) {
-#pragma unroll
-        for (int m = 0; m < 3; m++) T[l][m] = ph[RHO] * ph[U1 + m] * vcov[l];
-        T[l][l] += press;
-      }
-#pragma unroll
-      for (int l = 0; l < 3; l++)
-#pragma unroll
-        for (int m = 0; m < 3; m++)
-#pragma unroll
-          for (int n = 0; n < 3; n++)
-            src[U1 + m] += T[l][n] * __ldg(geo + (GF_CONN + l * 9 + m * 3 + n) * gs + gi);
+      for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
     }
     p_to_u(pn, u, gc0, gc1, gc2);
     p_to_u(ph, uh, gc0, gc1, gc2);
@@ -212,7 +133,8 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       double ddt = divF[v] / vol - src[v];
       u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
     }
-    u_to_p(u, pf, __ldg(geo + GF_GC0 * gs + gi), __ldg(geo + GF_GC1 * gs + gi), __ldg(geo + GF_GC2 * gs + gi));
+    u_to_p(u, pf, __ldg(geo + GF_GC0 * gs + gi), __ldg(geo + GF_GC1 * gs + gi), __ldg(geo + GF_GC2 * gs + gi),
+           P.floors != 0, P.rho_floor, P.e_floor);
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
     if (STAGE == 1) {

@@ -1,0 +1,374 @@
+// Mixed-precision batched 1-D RK stage kernel.
+//
+// The batched ensemble path: many independent 1-D problems of different sizes advance
+// together, one launch per RK stage.  In persistent mode the grid is a fixed number of
+// CTAs (chosen by the autotuner) that pull (problem, tile) work items from a device work
+// queue (an atomic counter over the tile list, whose length is read from device memory,
+// so a captured CUDA graph serves any batch composition); otherwise CTA b takes tile b.
+//
+// Precision split:
+//  * FP32: reconstruction and limiting (para_recon on the differences dqm, dqp with the
+//    geometry folded into FP64-computed weights, MixField), the wave speeds and the
+//    star-state increments U* - U of the HLLC solver (faces where FP32 cannot resolve
+//    the internal energy of the colder side are re-solved in FP64, MIX_COND_MAX);
+//  * FP64: the state, the face states a + da, the upwind physical flux, area and volume
+//    factors, the geometric source terms, the conserved-variable update and the dt
+//    reduction.
+// Each FP64 face flux is used once with each sign, so the flux differences conserve mass
+// and energy to FP64 round-off.
+//
+// This translation unit is compiled with fast FP32 math (approximate FP32 division and
+// square root); FP64 division and square root stay IEEE.
+#include "mdg_hydro.cuh"
+#include "mdg_kernels.cuh"
+#include "mdg_load1d.cuh"
+
+namespace mdg {
+
+// FP32 reconstruction weights of one zone
+struct MixW { float wlm, wlp, wrm, wrp, eal, ear, ebl, ebr, dxz, mr, ml; };
+
+__device__ __forceinline__ MixW load_mixw(const float *__restrict__ w, int64_t st)
+{
+  MixW m;
+  m.wlm = __ldg(w + MX_WLM * st); m.wlp = __ldg(w + MX_WLP * st);
+  m.wrm = __ldg(w + MX_WRM * st); m.wrp = __ldg(w + MX_WRP * st);
+  m.eal = __ldg(w + MX_EAL * st); m.ear = __ldg(w + MX_EAR * st);
+  m.ebl = __ldg(w + MX_EBL * st); m.ebr = __ldg(w + MX_EBR * st);
+  m.dxz = __ldg(w + MX_DXZ * st); m.mr = __ldg(w + MX_MR * st); m.ml = __ldg(w + MX_ML * st);
+  return m;
+}
+
+// para_recon of one variable in difference form (reconstruct.c:142-201): returns the face
+// offsets dl = al - a and dr = ar - a.
+__device__ __forceinline__ void mixed_recon(float dqm, float dqp, const MixW &w, float &dl, float &dr)
+{
+  if (dqm * dqp <= 0.0f) { dl = 0.0f; dr = 0.0f; return; }
+  float l = w.wlm * dqm + w.wlp * dqp;
+  float r = w.wrm * dqm + w.wrp * dqp;
+  // face values limited to the range of the neighbouring means (reconstruct.c:165-171)
+  if ((-l) * (l + 0.75f * dqm) < 0.0f) l = -0.75f * dqm;
+  if ((0.75f * dqp - r) * r < 0.0f) r = 0.75f * dqp;
+  // re-fit and move an interior extremum to the nearer edge (reconstruct.c:174-200)
+  const float A2 = w.eal * l + w.ear * r;
+  const float B2 = w.ebl * l + w.ebr * r;
+  const float s = -B2 / (2.0f * A2);
+  if (s > 0.0f && s < w.dxz) {
+    if (s > 0.5f * w.dxz) l = r * w.mr;
+    else r = l * w.ml;
+  }
+  dl = l;
+  dr = r;
+}
+
+// A subsonic face is ill-conditioned in FP32 when max(rho u^2 + p) over its two states
+// exceeds MIX_COND_MAX times the smaller pressure.  FP32 face states and star-state
+// increments carry absolute errors of about 6e-8 (rho u^2 + p) (times the jump, for the
+// face states); where the colder side's internal energy is a tiny fraction of that
+// (strong shocks into cold or hypersonic gas) the error would swamp it -- it can drive the
+// internal energy negative, and through dt_source_control's internal-energy term it
+// steers dt.  Such faces are recomputed in FP64: both face states and the Riemann solve.
+// Supersonic faces take the upwind FP64 flux of the FP32-reconstructed face state, whose
+// error leaves the upwind zone's internal energy unchanged to first order.
+#ifndef MDG_MIX_COND_MAX
+#define MDG_MIX_COND_MAX 1000.0f
+#endif
+constexpr float MIX_COND_MAX = MDG_MIX_COND_MAX;
+
+// HLLC (riemann.c:328-499) with FP32 wave speeds and star-state increments and an FP64
+// upwind flux; pl/pr: FP64 face states (rho, u, v1, v2, v3, p).  Returns false, with no
+// flux written, for an ill-conditioned subsonic face (see MIX_COND_MAX).
+__device__ __forceinline__ bool riemann_hllc_mixed(const double *pl, const double *pr, const FaceGeom<double> &g,
+                                                   const GamConst<float> &gc, double *flux, float &sig)
+{
+  if (g.area < 1.0e-16) {
+    sig = 1.0e-30f;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) flux[v] = 0.0;
+    return true;
+  }
+  const float sc = (float)g.scale;
+  float plf[6], prf[6];
+#pragma unroll
+  for (int v = 0; v < 6; v++) { plf[v] = (float)pl[v]; prf[v] = (float)pr[v]; }
+  const float u_l = plf[U1] * sc, u_r = prf[U1] * sc;
+  float sl, sr, ss, p_s;
+  int isshock;
+  wave_speeds<float>(plf, prf, u_l, u_r, false, gc, sl, sr, ss, p_s, isshock);
+  if (ss > sr) sr = 1.001f * ss;
+  if (ss < sl) sl = 1.001f * ss;
+  sig = fmaxf(fabsf(sl), fabsf(sr)) / sc;
+  if (sl > 0.0f) { pflux<0, false, double>(pl, pl[5], g, flux); return true; }
+  if (sr < 0.0f) { pflux<0, false, double>(pr, pr[5], g, flux); return true; }
+  const float emax = fmaxf(plf[RHO] * u_l * u_l + plf[5], prf[RHO] * u_r * u_r + prf[5]);
+  if (!(emax <= MIX_COND_MAX * fminf(plf[5], prf[5]))) return false;
+  const bool left = ss > 0.0f;
+  double pk[6];
+#pragma unroll
+  for (int v = 0; v < 6; v++) pk[v] = left ? pl[v] : pr[v];
+  const float sk = left ? sl : sr, uk = left ? u_l : u_r;
+  double u[NPRIM], fx[NPRIM];
+  p_uflux<0, false, double>(pk, g, pk[5], u, fx);
+  // U* - U of the upwind side in a form where nothing cancels in FP32:
+  //   rho* - rho = rho (ss-uk)/(sk-ss),  E* - E = (E (ss-uk) + p* ss - p uk)/(sk-ss)
+  const float rk = left ? plf[RHO] : prf[RHO];
+  const float pkf = left ? plf[5] : prf[5];
+  const float inv = 1.0f / (sk - ss);
+  const float dU0 = rk * (ss - uk) * inv;
+  const float dUE = ((float)u[UU] * (ss - uk) + p_s * ss - pkf * uk) * inv;
+  double dU[NPRIM];
+  dU[RHO] = (double)dU0;
+  dU[UU] = (double)dUE;
+  dU[U1] = g.g0 * (double)(((ss - uk) * rk + ss * dU0) / sc);   // normal component
+  dU[U2] = g.g1 * pk[U2] * (double)dU0;
+  dU[U3] = g.g2 * pk[U3] * (double)dU0;
+  const double slr = (double)(sk / sc);
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) flux[v] = g.area * (fx[v] + slr * dU[v]);
+  return true;
+}
+
+// FP64 re-solve of an ill-conditioned face (MIX_COND_MAX), out of line so that its
+// register demand does not raise the common path's.  c = &sv[0][k] holds the stencil of
+// the face (zones z-2 .. z+1 at c[v*cs + 0..3]); both face states are reconstructed in FP64
+// (right face of zone z-1, left face of zone z; reconstruct.c:142-201), the FP64 solver
+// writes flux[v * fs] and the signal speed is returned.
+__device__ __noinline__ float face_fp64(const double *c, int cs, const double *rc_zm, const double *rc_z,
+                                        int64_t rcs, double gam, double area, double scale, double g0,
+                                        double g1, double g2, double *flux, int fs)
+{
+  double xs[12];
+  const RcView<double, true> gm{rc_zm, rcs};
+  const RcView<double, true> gz{rc_z, rcs};
+#pragma unroll 1
+  for (int v = 0; v < 6; v++) {
+    const double *q = c + v * cs;
+    double lo, hi;
+    para_recon_zone<double>(q[0], q[1], q[2], gm, lo, hi);
+    xs[v] = hi;
+    para_recon_zone<double>(q[1], q[2], q[3], gz, lo, hi);
+    xs[6 + v] = lo;
+  }
+  FaceGeom<double> fg;
+  fg.area = area; fg.scale = scale; fg.g0 = g0; fg.g1 = g1; fg.g2 = g2;
+  double f[NPRIM], sig64;
+  riemann_hllc<0, false, double>(xs, xs + 6, fg, gam_const<double>(gam), f, sig64);
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) flux[v * fs] = f[v];
+  return (float)sig64;
+}
+
+// dt_source_control (step.c:205-223) with one division: the three ratios a_k/b_k have
+// positive denominators, so the smallest is selected by cross-multiplication.
+__device__ __forceinline__ double dt_source_control_1div(const double *p, const double *u, const double *s)
+{
+  const double alpha = 0.02;
+  double num = alpha * u[0], den = fabs(s[0]) + 1.0e-16;
+  const double n1 = alpha * u[1], d1 = fabs(s[1]) + 1.0e-16;
+  if (n1 * den < num * d1) { num = n1; den = d1; }
+  const double momterm = p[U1] * s[U1] + p[U2] * s[U2] + p[U3] * s[U3];
+  const double n2 = 100 * alpha * p[UU], d2 = fabs(fabs(s[1]) - fabs(momterm)) + 1.0e-16;
+  if (n2 * den < num * d2) { num = n2; den = d2; }
+  return fmin(1.0e100, num / den);
+}
+
+template <int NT, int STAGE>
+__global__ void __launch_bounds__(NT)
+stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                     const Tile *__restrict__ tiles, WorkQueue *__restrict__ q, bool use_queue,
+                     Tables tb, StateSoA sst, StateSoA sn, StateSoA out)
+{
+  __shared__ double sv[6][NT + 2];     // stage-state pencil: 5 primitives + pressure
+  __shared__ double sar[6][NT];        // right face values of each reconstructed zone
+  __shared__ double sfl[NPRIM][NT];    // face fluxes
+  __shared__ double sred[32];
+  __shared__ int s_item;
+  const int t = threadIdx.x;
+  const double *rc = tb.rc0;
+  const int64_t rcs = tb.rc0_stride;
+  const double *geo = tb.geo;
+  const int64_t gs = tb.geo_stride;
+  const int ntiles = q->ntiles;
+
+  int item;
+  if (use_queue) {
+    // the other stage's counter is idle while this kernel runs: reset it for its next launch
+    if (blockIdx.x == 0 && t == 0) q->head[1 - STAGE] = 0u;
+    if (t == 0) s_item = (int)atomicAdd(&q->head[STAGE], 1u);
+    __syncthreads();
+    item = s_item;
+  } else {
+    item = blockIdx.x;
+  }
+
+  while (item < ntiles) {
+    const Tile tile = tiles[item];
+    const ProbDev &P = probs[tile.prob];
+    const double dt = times[tile.prob].dt;
+    const double t_bc = STAGE ? times[tile.prob].t_bc1 : times[tile.prob].t;
+    const int n1 = P.n1;
+    const int z = tile.i0 - 1 + t;
+
+    {
+      double w[6];
+      load_cell_1d(P, sst, rc, rcs, z, t_bc, w);
+#pragma unroll
+      for (int v = 0; v < 6; v++) sv[v][t + 1] = w[v];
+      if (t == 0) {
+        load_cell_1d(P, sst, rc, rcs, tile.i0 - 2, t_bc, w);
+#pragma unroll
+        for (int v = 0; v < 6; v++) sv[v][0] = w[v];
+      }
+      if (t == NT - 1) {
+        load_cell_1d(P, sst, rc, rcs, tile.i0 + NT - 1, t_bc, w);
+#pragma unroll
+        for (int v = 0; v < 6; v++) sv[v][NT + 1] = w[v];
+      }
+    }
+    __syncthreads();
+    // fetch the next work item while this one is processed (read after later barriers)
+    if (use_queue && t == 0) s_item = (int)atomicAdd(&q->head[STAGE], 1u);
+
+    // FP32 reconstruction of zone z; FP64 face values a + da
+    double al[6];
+    {
+      const int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
+      const MixW w = load_mixw(tb.mx + P.geo_off + zc + NG, gs);
+#pragma unroll
+      for (int v = 0; v < 6; v++) {
+        const double a = sv[v][t + 1];
+        float dl, dr;
+        mixed_recon((float)(a - sv[v][t]), (float)(sv[v][t + 2] - a), w, dl, dr);
+        al[v] = a + (double)dl;
+        sar[v][t] = a + (double)dr;
+      }
+    }
+    __syncthreads();
+
+    double lmin = 1.0e300, lmax = 0.0;
+    float smax = 0.0f;
+    if (t >= 1) {
+      double pl[6], flux[NPRIM];
+      float sig;
+#pragma unroll
+      for (int v = 0; v < 6; v++) pl[v] = sar[v][t - 1];
+      const int zf = z < 0 ? 0 : (z > n1 ? n1 : z);
+      const int64_t gi = P.geo_off + zf + NG;
+      FaceGeom<double> fg;
+      fg.area = __ldg(geo + GF_AREA * gs + gi);
+      fg.scale = __ldg(geo + GF_FSCALE * gs + gi);
+      fg.g0 = __ldg(geo + GF_FG0 * gs + gi);
+      fg.g1 = __ldg(geo + GF_FG1 * gs + gi);
+      fg.g2 = __ldg(geo + GF_FG2 * gs + gi);
+      const GamConst<float> gc = gam_const<float>((float)P.gam);
+      if (riemann_hllc_mixed(pl, al, fg, gc, flux, sig)) {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) sfl[v][t] = flux[v];
+      } else {
+        const int zm = z - 1 < -1 ? -1 : (z - 1 > n1 ? n1 : z - 1);
+        const int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
+        sig = face_fp64(&sv[0][t - 1], NT + 2, rc + P.geo_off + zm + NG, rc + P.geo_off + zc + NG, rcs, P.gam,
+                        fg.area, fg.scale, fg.g0, fg.g1, fg.g2, &sfl[0][t], NT);
+      }
+      if (z >= 0 && z <= n1) smax = fmaxf(smax, sig);
+    }
+    __syncthreads();
+
+    // push() for zone z in FP64 (step.c:380-470)
+    if (t >= 1 && t <= NT - 2 && z >= 0 && z < n1) {
+      const int64_t gi = P.geo_off + z + NG;
+      const int64_t cell = P.cell_off + z;
+      double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM];
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) ph[v] = sv[v][t + 1];
+      if (STAGE == 0) {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
+      } else {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
+      }
+      const double gc0 = __ldg(geo + GF_G0 * gs + gi), gc1 = __ldg(geo + GF_G1 * gs + gi),
+                   gc2 = __ldg(geo + GF_G2 * gs + gi);
+      if (P.has_src) {
+        geo_sources_1d(geo, gs, gi, P.sparse_conn != 0, ph, sv[5][t + 1], gc0, gc1, gc2, src);
+      } else {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+      }
+      p_to_u(pn, u, gc0, gc1, gc2);
+      p_to_u(ph, uh, gc0, gc1, gc2);
+      lmin = dt_source_control_1div(pn, u, src);
+      const double ivol = 1.0 / __ldg(geo + GF_VOL * gs + gi);
+      const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) {
+        const double ddt = (sfl[v][t + 1] - sfl[v][t]) * ivol - src[v];
+        u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
+      }
+      // hydro_u_to_p (fluid.c:27-53) with one division
+      double pf[NPRIM];
+      const double irho = 1.0 / u[RHO];
+      const double w1 = u[U1] * irho, w2 = u[U2] * irho, w3 = u[U3] * irho;
+      pf[RHO] = u[RHO];
+      pf[U1] = __ldg(geo + GF_GC0 * gs + gi) * w1;
+      pf[U2] = __ldg(geo + GF_GC1 * gs + gi) * w2;
+      pf[U3] = __ldg(geo + GF_GC2 * gs + gi) * w3;
+      pf[UU] = u[UU] - 0.5 * pf[RHO] * (w1 * pf[U1] + w2 * pf[U2] + w3 * pf[U3]);
+      if (P.floors) {   // ENFORCE_FLOORS, fluid.c:43-46
+        pf[RHO] = fmax(pf[RHO], P.rho_floor);
+        pf[UU] = fmax(pf[UU], P.e_floor);
+      }
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+      if (STAGE == 1) {
+        // zone term of the next estimate_dt (step.c:177-187)
+        const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
+        lmax = (fabs(pf[U1]) + cs / __ldg(geo + GF_S00 * gs + gi)) / P.dx0;
+      }
+    }
+    lmin = fmin(lmin, P.dx0 / (double)smax);
+    if (STAGE == 1) lmin = fmin(lmin, 1.0 / lmax);
+    block_min_to(lmin, &times[tile.prob].minacc, sred);
+    if (!use_queue) break;
+    __syncthreads();
+    item = s_item;
+  }
+}
+
+template <int NT>
+static void launch_mixed_nt(int stage, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
+                            const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA sst, StateSoA sn,
+                            StateSoA out, cudaStream_t st)
+{
+  if (stage == 0)
+    stage1d_mixed_kernel<NT, 0><<<grid, NT, 0, st>>>(probs, times, tiles, q, use_queue, tb, sst, sn, out);
+  else
+    stage1d_mixed_kernel<NT, 1><<<grid, NT, 0, st>>>(probs, times, tiles, q, use_queue, tb, sst, sn, out);
+}
+
+void launch_stage1d_mixed(int stage, int nt, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
+                          const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA sst, StateSoA sn,
+                          StateSoA out, cudaStream_t st)
+{
+  if (grid <= 0) return;
+  switch (nt) {
+    case 64: launch_mixed_nt<64>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
+    case 256: launch_mixed_nt<256>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
+    default: launch_mixed_nt<128>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
+  }
+}
+
+int mixed_max_ctas_per_sm(int nt)
+{
+  int n = 0;
+  cudaError_t e;
+  switch (nt) {
+    case 64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<64, 1>, 64, 0); break;
+    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<256, 1>, 256, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<128, 1>, 128, 0); break;
+  }
+  return e == cudaSuccess ? n : 0;
+}
+
+}  // namespace mdg

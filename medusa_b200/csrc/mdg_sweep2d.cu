@@ -349,7 +349,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
         double ddt = divF / P.vol - src[v];
         u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
       }
-      u_to_p(u, pf, 1.0, 1.0, 1.0);
+      u_to_p(u, pf, 1.0, 1.0, 1.0, P.floors != 0, P.rho_floor, P.e_floor);
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
       if (STAGE == 1) {

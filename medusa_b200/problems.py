@@ -66,6 +66,9 @@ class Problem:
     tmax: float = 1.0e100
     rtrans: float = 1.0
     hydro_interp_order: int = 3   # io.c:5055
+    enforce_floors: int = 0       # ENFORCE_FLOORS build switch (fluid.c:43-46)
+    rho_floor: float = -1.0       # io.c:5082 default; problem hooks set their own
+    e_floor: float = -1.0         # io.c:5081
     nsteps: Optional[int] = None  # fixed step count for the workload, if any
 
     @property
@@ -123,6 +126,27 @@ def sod(n1: int = 1024, cfl: float = 0.8, tmax: float = 0.2) -> Problem:
                    bc_lo=(OUTFLOW,) * 3, bc_hi=(OUTFLOW,) * 3, cfl=cfl, tmax=tmax)
 
 
+def double_rarefaction(n1: int = 256, v: float = 2.0, cfl: float = 0.8, tmax: float = 0.15,
+                       rho_floor: float = 1.0e-8, e_floor: float = 1.0e-8) -> Problem:
+    """Two rarefactions running apart (problems/init_double_rare.c): rho=1, p=0.4, v=-v
+    left of x=0.5 and +v right of it (the hook uses v=2), gamma=1.4, with the hook's floors
+    rho 1e-8, e 1e-8 enforced (ENFORCE_FLOORS).  For v above 2 c/(gamma-1) = 3.74 the
+    rarefactions open a vacuum and the centre zones approach the floors (raise them to
+    make the clamp act)."""
+    gam = 1.4
+    dx = 1.0 / n1
+    ic = np.zeros((n1, NPRIM))
+    xr = (np.arange(n1) + 1) * dx
+    left = xr < 0.5 + 1.0e-6
+    ic[:, 0] = 1.0
+    ic[:, 1] = 0.4 / (gam - 1.0)
+    ic[:, 2] = np.where(left, -v, v)
+    return Problem(name="double_rare1d_%d" % n1 if v == 2.0 else "double_rare1d_v%g_%d" % (v, n1), ndim=1, geom=CARTESIAN, n=(n1, 1, 1),
+                   startx=(0.0, 0.0, 0.0), dx=(dx, 1.0, 1.0), gam=gam, ic=ic,
+                   bc_lo=(OUTFLOW,) * 3, bc_hi=(OUTFLOW,) * 3, cfl=cfl, tmax=tmax,
+                   enforce_floors=1, rho_floor=rho_floor, e_floor=e_floor)
+
+
 def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240601,
                      cfl: float = 0.8, nsteps: int = 200) -> Problem:
     """2-D Kelvin-Helmholtz on the periodic unit square (the structure of
@@ -155,7 +179,7 @@ def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240
 
 def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                  p_ratio: float = 100.0, r0: float = 0.5, cfl: float = 0.8,
-                 tmax: float = 1.0e100) -> Problem:
+                 tmax: float = 1.0e100, floors: bool = True) -> Problem:
     """1-D spherical problem on r in [0,1] (uniform radius), SPHERICAL_ORIGIN inner
     boundary (bc.c:776-803).
 
@@ -164,13 +188,16 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
     kind='sedov' : rho=1; p = p_ratio inside r<r0 (a small blast radius), the ambient p is 1e-5;
                    OUTFLOW outer boundary.
     kind='noh'   : problems/init_spherical_noh.c:14-61: rho=1, u=1e-6/(gam-1), v^r=-1;
-                   PROB outer boundary with the Noh inflow (init_spherical_noh.c:63-79).
+                   PROB outer boundary with the Noh inflow (init_spherical_noh.c:63-79);
+                   the hook's floors rho 1e-6, e 1e-7/(gam-1) (init_spherical_noh.c:22-23),
+                   enforced (ENFORCE_FLOORS) unless floors=False.
     """
     dx = 1.0 / n1
     rc = (np.arange(n1) + 0.5) * dx
     ic = np.zeros((n1, NPRIM))
     bc_hi = OUTFLOW
     prob_kind = PROB_NONE
+    fl = dict()
     if kind == "sod":
         inside = rc < r0
         rho = np.where(inside, rho_ratio, 1.0)
@@ -188,12 +215,14 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
         ic[:, 2] = -1.0   # vr / scale[0][0], scale[0][0] = 1 for a uniform radius
         bc_hi = PROB
         prob_kind = PROB_NOH
+        if floors:
+            fl = dict(enforce_floors=1, rho_floor=1.0e-6, e_floor=1.0e-7 / (gam - 1.0))
     else:
         raise ValueError("unknown 1-D spherical problem kind %r" % kind)
     return Problem(name="sph1d_%s_%d" % (kind, n1), ndim=1, geom=SPHERICAL, n=(n1, 1, 1),
                    startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
                    bc_lo=(SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW), bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
-                   prob_kind=prob_kind, cfl=cfl, tmax=tmax)
+                   prob_kind=prob_kind, cfl=cfl, tmax=tmax, **fl)
 
 
 def ensemble_1d(count: int = 2048, seed: int = 7, nmin: int = 128, nmax: int = 8192,

@@ -40,6 +40,14 @@ class MdgError(RuntimeError):
         self.code = code
 
 
+class LaunchConfig(ctypes.Structure):
+    """mdg_launch_config of include/medusa_b200.h."""
+    _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("steps_per_graph", ctypes.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"threads": self.threads, "ctas_per_sm": self.ctas_per_sm, "steps_per_graph": self.steps_per_graph}
+
+
 class ProblemDesc(ctypes.Structure):
     """mdg_problem_desc of include/medusa_b200.h."""
     _fields_ = [("ndim", ctypes.c_int), ("geom", ctypes.c_int), ("eos", ctypes.c_int),
@@ -51,7 +59,8 @@ class ProblemDesc(ctypes.Structure):
                 ("cfl", ctypes.c_double), ("dt_init_safety", ctypes.c_double),
                 ("dt_grow_safety", ctypes.c_double), ("initial_dt", ctypes.c_double),
                 ("dtmax", ctypes.c_double), ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
-                ("hydro_interp_order", ctypes.c_int)]
+                ("hydro_interp_order", ctypes.c_int),
+                ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double), ("e_floor", ctypes.c_double)]
 
 
 def desc_of(pb: "_pb.Problem") -> ProblemDesc:
@@ -67,6 +76,7 @@ def desc_of(pb: "_pb.Problem") -> ProblemDesc:
     d.cfl, d.dt_init_safety, d.dt_grow_safety = pb.cfl, pb.dt_init_safety, pb.dt_grow_safety
     d.initial_dt, d.dtmax, d.dtmin, d.tmax = pb.initial_dt, pb.dtmax, pb.dtmin, pb.tmax
     d.hydro_interp_order = pb.hydro_interp_order
+    d.enforce_floors, d.rho_floor, d.e_floor = int(pb.enforce_floors), pb.rho_floor, pb.e_floor
     return d
 
 
@@ -97,9 +107,14 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_version.restype = i
     L.mdg_set_timing.argtypes = [vp, i]
     L.mdg_get_timers.argtypes = [vp, vp, vp]
+    L.mdg_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.mdg_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.mdg_autotune.argtypes = [vp, i, ctypes.POINTER(LaunchConfig), ctypes.POINTER(d)]
+    L.mdg_conserved_totals.argtypes = [vp, vp, vp]
     for name in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step", "mdg_download_state",
                  "mdg_get_time", "mdg_get_stream", "mdg_synchronize", "mdg_destroy", "mdg_set_timing",
-                 "mdg_get_timers"):
+                 "mdg_get_timers", "mdg_get_launch_config", "mdg_set_launch_config", "mdg_autotune",
+                 "mdg_conserved_totals"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -195,6 +210,34 @@ class Solver:
         calls = np.zeros(4, dtype=np.int64)
         _check(library().mdg_get_timers(self._h, ms.ctypes.data, calls.ctypes.data), "mdg_get_timers")
         return {n: (float(ms[k]), int(calls[k])) for k, n in enumerate(self.TIMER_NAMES)}
+
+    # --- launch shape, autotuning and conservation diagnostics
+    def launch_config(self) -> dict:
+        c = LaunchConfig()
+        _check(library().mdg_get_launch_config(self._h, ctypes.byref(c)), "mdg_get_launch_config")
+        return c.as_dict()
+
+    def set_launch_config(self, threads: int = None, ctas_per_sm: int = None, steps_per_graph: int = None):
+        cur = self.launch_config()
+        c = LaunchConfig(cur["threads"] if threads is None else threads,
+                         cur["ctas_per_sm"] if ctas_per_sm is None else ctas_per_sm,
+                         cur["steps_per_graph"] if steps_per_graph is None else steps_per_graph)
+        _check(library().mdg_set_launch_config(self._h, ctypes.byref(c)), "mdg_set_launch_config")
+
+    def autotune(self, trial_steps: int = 5):
+        """Pick the fastest launch shape of the mixed sweep; returns (config, ms per step)."""
+        c = LaunchConfig()
+        ms = ctypes.c_double()
+        _check(library().mdg_autotune(self._h, int(trial_steps), ctypes.byref(c), ctypes.byref(ms)), "mdg_autotune")
+        return c.as_dict(), ms.value
+
+    def conserved_totals(self):
+        """(mass, energy) arrays over the problems, compensated FP64 sums on the device."""
+        n = len(self.problems)
+        mass, energy = np.zeros(n), np.zeros(n)
+        _check(library().mdg_conserved_totals(self._h, mass.ctypes.data, energy.ctypes.data),
+               "mdg_conserved_totals")
+        return mass, energy
 
     @property
     def stream(self) -> int:

@@ -55,6 +55,12 @@ CONFIGS = {
     # 1-D spherical, uniform radius (ensemble members: Sod/Noh/Sedov type)
     "sph1d": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
                   RCOORD="UNIFORM", THCOORD="UNIFORM"),
+    # the same with the ENFORCE_FLOORS switch on (problems that set rho_floor/e_floor:
+    # Noh, double rarefaction)
+    "cart1d_floors": dict(NDIM="1", GEOM="CARTESIAN", DENDRITIC_GRID="FALSE",
+                          RCOORD="UNIFORM", THCOORD="UNIFORM", ENFORCE_FLOORS="TRUE"),
+    "sph1d_floors": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                         RCOORD="UNIFORM", THCOORD="UNIFORM", ENFORCE_FLOORS="TRUE"),
 }
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]

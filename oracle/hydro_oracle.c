@@ -89,6 +89,8 @@ typedef struct {
   double tmax;
   double rtrans;
   int hydro_interp_order;
+  int enforce_floors;
+  double rho_floor, e_floor;
 } orc_params;
 
 typedef struct {
@@ -767,8 +769,8 @@ static void p_to_u(const double *pv, double *u, const double *gcov)
   u[UU] = 0.5*u[RHO]*vsq + pv[UU];
 }
 
-/* fluid.c:27-53 (ENFORCE_FLOORS off) */
-static void u_to_p(double *u, double *pv, const double *gcon)
+/* fluid.c:27-53; the floors of fluid.c:43-46 when the ENFORCE_FLOORS switch is on */
+static void u_to_p(double *u, double *pv, const double *gcon, const orc_params *P)
 {
   double vsq = 0.0;
   int dd;
@@ -777,6 +779,10 @@ static void u_to_p(double *u, double *pv, const double *gcon)
   for (dd=0; dd<3; dd++) pv[U1+dd] = gcon[dd]*u[U1+dd];
   for (dd=0; dd<3; dd++) vsq += u[U1+dd]*pv[U1+dd];
   pv[UU] = u[UU] - 0.5*pv[RHO]*vsq;
+  if (P->enforce_floors) {
+    pv[RHO] = MAX(pv[RHO], P->rho_floor);
+    pv[UU] = MAX(pv[UU], P->e_floor);
+  }
 }
 
 /* step.c:205-223 */
@@ -821,7 +827,7 @@ static void push(orc_t *o, double dtpush, double *const *p, double *const *ph, d
         double ddt = divF[v]/g->volume - s[v];
         u[v] = pfact*u[v] + phfact*uh[v] - ffact*dtpush * ddt;
       }
-      u_to_p(u, out, g->gcon);
+      u_to_p(u, out, g->gcon, &o->prm);
       for (v=0; v<NPRIM; v++) pf[v][c] = out[v];
     }
   }

@@ -38,7 +38,9 @@ class Params(ctypes.Structure):
                 ("dt_init_safety", ctypes.c_double), ("dt_grow_safety", ctypes.c_double),
                 ("initial_dt", ctypes.c_double), ("dtmax", ctypes.c_double),
                 ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
-                ("rtrans", ctypes.c_double), ("hydro_interp_order", ctypes.c_int)]
+                ("rtrans", ctypes.c_double), ("hydro_interp_order", ctypes.c_int),
+                ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double),
+                ("e_floor", ctypes.c_double)]
 
 
 def params_of(pb) -> Params:
@@ -55,6 +57,9 @@ def params_of(pb) -> Params:
     p.initial_dt, p.dtmax, p.dtmin, p.tmax = pb.initial_dt, pb.dtmax, pb.dtmin, pb.tmax
     p.rtrans = pb.rtrans
     p.hydro_interp_order = pb.hydro_interp_order
+    p.enforce_floors = int(getattr(pb, "enforce_floors", 0))
+    p.rho_floor = getattr(pb, "rho_floor", -1.0)
+    p.e_floor = getattr(pb, "e_floor", -1.0)
     return p
 
 
@@ -154,9 +159,10 @@ class Oracle:
 
 # ----------------------------------------------------------------------------- reference
 def ref_config(pb) -> str:
-    if pb.geom == 0:
-        return "cart%dd" % pb.ndim
-    return "sph%dd" % pb.ndim
+    """The oracle/_ref build of a problem: its geometry and dimension, and whether the
+    ENFORCE_FLOORS switch is compiled in."""
+    name = ("cart%dd" if pb.geom == 0 else "sph%dd") % pb.ndim
+    return name + ("_floors" if getattr(pb, "enforce_floors", 0) else "")
 
 
 def ref_available(pb, fast: bool = False) -> bool:

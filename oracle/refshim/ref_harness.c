@@ -42,6 +42,8 @@ typedef struct {
   double tmax;
   double rtrans;
   int hydro_interp_order;
+  int enforce_floors;  /* must match the ENFORCE_FLOORS of the build */
+  double rho_floor, e_floor;
 } ref_params;
 
 static ref_params g_prm;
@@ -170,6 +172,11 @@ REF_API int ref_init(const ref_params *prm, const double *ic)
   tmax = prm->tmax;
   ncomp = 0;
   hydro_interp_order = prm->hydro_interp_order;
+  if (prm->enforce_floors != (ENFORCE_FLOORS == TRUE)) {
+    fprintf(stderr, "ref_harness: enforce_floors=%d but this build has ENFORCE_FLOORS=%d\n",
+            prm->enforce_floors, (int)(ENFORCE_FLOORS == TRUE));
+    exit(3);
+  }
   rad_interp_order = 2;
   dt_dump = 1.0e100;
   dt_pdump = dt_dump;
@@ -179,8 +186,8 @@ REF_API int ref_init(const ref_params *prm, const double *ic)
   nstep_analysis = 100;
   nstep_timing = INT_MAX;
   max_steps = 2147483647;
-  e_floor = -1.0;
-  rho_floor = -1.0;
+  e_floor = prm->e_floor;       /* io.c:5081-5082 defaults are -1; problem hooks set their own */
+  rho_floor = prm->rho_floor;
   detect_tbounce = 0;
   dump_hdf = 0;
 #if (NDIM==1)

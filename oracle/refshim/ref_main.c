@@ -32,6 +32,8 @@ typedef struct {
   double tmax;
   double rtrans;
   int hydro_interp_order;
+  int enforce_floors;
+  double rho_floor, e_floor;
 } ref_params;
 
 int ref_init(const ref_params *prm, const double *ic);

@@ -27,6 +27,8 @@ def cases():
         "sod1d_1024": (P.sod(1024), 60),
         "sph1d_sod_128": (P.spherical_1d("sod", 128, 1.4, rho_ratio=8.0, p_ratio=50.0), 80),
         "sph1d_noh_200": (P.spherical_1d("noh", 200, 5.0 / 3.0), 100),
+        "sph1d_noh_nofloor_160": (P.spherical_1d("noh", 160, 1.4, floors=False), 90),
+        "double_rare1d_v6_floors_200": (P.double_rarefaction(200, v=6.0, rho_floor=1.0e-2, e_floor=5.0e-3), 80),
         "sph1d_sedov_256": (P.spherical_1d("sedov", 256, 1.4, p_ratio=1.0e4, r0=0.05), 100),
         "sph1d_sod_poly_lin_96": (P.spherical_1d("sod", 96, 4.0 / 3.0, rho_ratio=20.0)
                                   .copy(eos=P.POLYTROPIC, Kpoly=1.0, hydro_interp_order=2), 60),

@@ -61,3 +61,31 @@ def test_null_handles_are_rejected():
     assert L.mdg_step(None, 1) == 1
     assert L.mdg_synchronize(None) == 1
     assert L.mdg_destroy(None) == 0
+
+
+@pytest.mark.parametrize("pb", [P.kelvin_helmholtz(16, 16, nsteps=1), P.sod(64).copy(hydro_interp_order=2)],
+                         ids=["2d", "linear"])
+def test_mixed_precision_scope_is_checked_before_any_device_work(pb):
+    """The mixed sweep is built for 1-D parabolic reconstruction: other problems are
+    refused with MDG_ERR_NOTIMPL (validation runs before any CUDA call)."""
+    arr = (S.ProblemDesc * 1)(S.desc_of(pb))
+    h = ctypes.c_void_p()
+    rc = S.library().mdg_create(arr, 1, S.PREC_MIXED, 0, ctypes.byref(h))
+    assert rc == 5
+    assert not h.value
+    assert b"mixed" in S.library().mdg_last_error_message()
+
+
+def test_unknown_precision_is_rejected():
+    arr = (S.ProblemDesc * 1)(S.desc_of(P.sod(64)))
+    h = ctypes.c_void_p()
+    assert S.library().mdg_create(arr, 1, 7, 0, ctypes.byref(h)) == 1
+
+
+def test_launch_config_calls_reject_null_solver():
+    L = S.library()
+    c = S.LaunchConfig(128, 0, 10)
+    assert L.mdg_get_launch_config(None, ctypes.byref(c)) == 1
+    assert L.mdg_set_launch_config(None, ctypes.byref(c)) == 1
+    assert L.mdg_autotune(None, 3, None, None) == 1
+    assert L.mdg_conserved_totals(None, None, None) == 1

@@ -18,6 +18,7 @@ def _cases():
     out.append(P.blast_2d(24, 30, bc=P.PERIODIC))
     out.append(P.blast_2d(30, 24, bc=P.OUTFLOW).copy(bc_lo=(P.EXTRAP, P.OUTFLOW, 0), bc_hi=(P.EXTRAP, P.REFLECT, 0)))
     out.append(P.kelvin_helmholtz(32, 24, seed=3))
+    out.append(P.double_rarefaction(150, v=6.0, rho_floor=1.0e-2, e_floor=5.0e-3))
     return out
 
 
