@@ -318,7 +318,7 @@ def run_reference_arm(args, ctx):
                   "seq_len": NX * NX, "parallelism": "replicas", "l2": "inputs larger than L2"}
         dtype = "f64"
     else:
-        probs = P.ensemble_1d(ENSEMBLE_COUNT, seed=ENSEMBLE_SEED)
+        probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED)
         cb = cpu_baseline_ensemble(probs)
         config = ensemble_config(probs, 1)
         dtype = "f64"
@@ -348,13 +348,18 @@ def run_ensemble(args, ctx):
     from medusa_b200.solver import PREC_FP64, PREC_MIXED, Solver
 
     K, W = args.steps, args.warmup
-    probs = P.ensemble_1d(ENSEMBLE_COUNT, seed=ENSEMBLE_SEED + ctx.rank)
+    probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED + ctx.rank)
     ncell = sum(p.ncell for p in probs)
     NT = 10   # timer-instrumented steps (roofline)
 
     # ---- headline: batched mixed precision, autotuned, CUDA graphs
     mix = Solver(probs, precision=PREC_MIXED, device=ctx.local)
-    tuned, tune_ms = mix.autotune(trial_steps=10)
+    if args.launch:
+        th, cps = (int(x) for x in args.launch.split(","))
+        mix.set_launch_config(threads=th, ctas_per_sm=cps)
+        tuned, tune_ms = mix.launch_config(), None
+    else:
+        tuned, tune_ms = mix.autotune(trial_steps=10)
     mix.step(W)
     mix.synchronize()
     ms_mix, clocks = timed_steps(ctx, mix, K, sample_clocks=True)
@@ -549,6 +554,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE_COUNT,
+                    help="ensemble: number of problems (a smaller ensemble for profiling runs)")
+    ap.add_argument("--launch", default=None,
+                    help="ensemble: fixed mixed-sweep launch shape 'threads,ctas_per_sm' instead of the autotuner")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.steps is None:

@@ -14,6 +14,7 @@ void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_
 void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area0, double &area1);
 void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
+void spherical_1d_constants(double &area_k, double &th1, double &th2, double &tc);
 }
 
 using namespace mdg;
@@ -211,6 +212,9 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (precision == MDG_PREC_MIXED && (descs[m].ndim != 1 || descs[m].hydro_interp_order != 3))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep is built for 1-D parabolic reconstruction");
+    if (precision == MDG_PREC_MIXED && descs[m].geom == MDG_SPHERICAL && !(descs[m].startx[0] >= 0.0))
+      return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
+                                       ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
   }
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
@@ -246,6 +250,8 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
     P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
     P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
+    P.x0 = d.startx[0];
+    if (d.ndim == 1 && d.geom == MDG_SPHERICAL) spherical_1d_constants(P.gk_area, P.gk_th1, P.gk_th2, P.gk_tc);
     s->hprobs.push_back(P);
     const int64_t nc = (int64_t)P.n1 * P.n2;
     if (nc > s->max_cells) s->max_cells = nc;

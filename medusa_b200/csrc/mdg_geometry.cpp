@@ -342,3 +342,22 @@ int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec)
 }
 
 }  // namespace mdg
+
+namespace mdg {
+
+// Angular constants of the 1-D spherical metric (theta integrated over [0, pi], phi over
+// 2 pi; metric_spherical_general.c:708-930): area/volume factor vthf*dph, and the
+// theta averages th_sthdth_dx3/vthf, th_sth3dth_dx/vthf, th_cthdth_dx2/vthf that scale
+// gcov[.][1], gcov[.][2] and conn[2][1][2].  With them every per-zone quantity of the
+// uniform-radius grid is a polynomial in the zone's edge radii (see the mixed sweep).
+void spherical_1d_constants(double &area_k, double &th1, double &th2, double &tc)
+{
+  const double x1lo = -1.0, x1hi = 1.0, dph = 2.0 * M_PI;
+  const double vthf = romb(x1lo, x1hi, f_sthdth_dx);
+  area_k = vthf * 1 * dph;
+  th1 = romb(x1lo, x1hi, f_sthdth_dx3) / vthf;
+  th2 = romb(x1lo, x1hi, f_sth3dth_dx) / vthf;
+  tc = romb(x1lo, x1hi, f_cthdth_dx2) / vthf;
+}
+
+}  // namespace mdg

@@ -85,6 +85,9 @@ struct ProbDev {
   double area0, area1, vol; // Cartesian 2-D constants
   double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
   double rho_floor, e_floor;
+  // 1-D geometry in closed form (mixed-precision sweep): lower edge of zone 0 and the
+  // angular integrals of the 1-D spherical metric (spherical_1d_constants)
+  double x0, gk_area, gk_th1, gk_th2, gk_tc;
 };
 
 // Time bookkeeping of one problem, resident on the device.
