@@ -201,6 +201,68 @@ int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy);
 int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double *prim_in, double *prim_out,
                            int nsteps, void *stream, double *t_out, double *dt_out);
 
+/*
+ * Solve server.  No counterpart in the reference, whose executable advances one problem
+ * per process.  A server keeps 1-D problems resident on one GPU and advances every
+ * admitted problem together, batching their uneven grids into the same stage launches
+ * (for MDG_PREC_MIXED: persistent CTAs fed from a device work queue, each round of
+ * steps_per_round steps replayed from one CUDA graph).  A request is a problem
+ * description, its initial state ([zone][5], as mdg_upload_state) and its end time
+ * desc->tmax; it runs the main.c time loop until t >= tmax and is then retired.
+ *
+ * Admission is by device-memory footprint: the arenas are sized once from hbm_bytes, and
+ * a queued request is admitted between rounds when a slot and a contiguous range of
+ * n1 + 4 zone units are free (requests that do not fit yet wait; smaller ones behind them
+ * may go first).  A finished problem's state is left unchanged by later rounds, so every
+ * result is the same whatever else shares the GPU and whenever it is collected.
+ *
+ * The request loop runs either on a thread of the server (mdg_server_start/stop), while
+ * other threads submit, poll and collect, or in the caller's thread (mdg_server_run).
+ */
+typedef struct mdg_server mdg_server;   /* opaque */
+typedef struct mdg_server_config {
+  int device;               /* CUDA ordinal */
+  int precision;            /* MDG_PREC_MIXED or MDG_PREC_FP64 */
+  long long hbm_bytes;      /* device memory for resident problems: the admission budget */
+  int max_problems;         /* resident problems at most */
+  int max_zones;            /* largest n1 a request may have */
+  int steps_per_round;      /* steps between two scheduling points */
+  int threads;              /* mixed sweep: threads per CTA, 64, 128 or 256 */
+  int ctas_per_sm;          /* mixed sweep: persistent CTAs per SM (0: as many as fit) */
+} mdg_server_config;
+
+#define MDG_REQ_QUEUED  0
+#define MDG_REQ_RUNNING 1
+#define MDG_REQ_DONE    2
+#define MDG_REQ_FAILED  3   /* its time step dropped below dtmin (main.c:229-238) */
+
+typedef struct mdg_server_stats {
+  long long submitted, completed, failed, queued, running, rounds;
+  double zone_updates;      /* sum over finished requests of n1 x steps */
+  double device_seconds;    /* device time of the step rounds */
+  double latency_p50, latency_p99;   /* seconds from submission to completion */
+  double wait_p50, wait_p99;         /* seconds from submission to admission */
+  double hbm_capacity, hbm_in_use;   /* bytes of the arenas, bytes held by resident problems */
+} mdg_server_stats;
+
+int mdg_server_create(const mdg_server_config *cfg, mdg_server **out);
+/* Queue a 1-D request (thread-safe); *id identifies it in the calls below. */
+int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double *prim, long long *id);
+/* Run `rounds` scheduling rounds in the calling thread (rounds <= 0: until nothing is
+ * queued or running); *active = problems resident after the last round. */
+int mdg_server_run(mdg_server *s, int rounds, int *active);
+/* Run the request loop on a thread of the server / stop it (returns the loop's error). */
+int mdg_server_start(mdg_server *s);
+int mdg_server_stop(mdg_server *s);
+int mdg_server_poll(mdg_server *s, long long id, int *status);
+/* Wait up to timeout_s seconds for a request to finish (its status in *status). */
+int mdg_server_wait(mdg_server *s, long long id, double timeout_s, int *status);
+/* Copy a finished request's final state ([zone][5]), time, step count and seconds from
+ * submission to completion, and forget the request. */
+int mdg_server_result(mdg_server *s, long long id, double *prim, double *t, int *istep, double *latency_s);
+int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st);
+int mdg_server_destroy(mdg_server *s);
+
 /* Library version as major*10000 + minor*100 + patch. */
 int mdg_version(void);
 

@@ -6,6 +6,6 @@
 - ``medusa_b200.build``: in-tree nvcc build of libmedusa_b200.so for sm_100a.
 """
 from . import problems  # noqa: F401
-from .solver import Solver, MdgError, PREC_FP64, PREC_MIXED, library  # noqa: F401
+from .solver import Solver, Server, MdgError, PREC_FP64, PREC_MIXED, library  # noqa: F401
 
-__all__ = ["problems", "Solver", "MdgError", "PREC_FP64", "PREC_MIXED", "library"]
+__all__ = ["problems", "Solver", "Server", "MdgError", "PREC_FP64", "PREC_MIXED", "library"]

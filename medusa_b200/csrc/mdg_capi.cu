@@ -75,7 +75,14 @@ static int fail(int code, const std::string &msg)
       return fail(MDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-static int validate(const mdg_problem_desc &d, int ndim0, std::string &why)
+namespace mdg {
+int report_error(int code, const std::string &msg) { return fail(code, msg); }
+int validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why);
+void make_probdev(const mdg_problem_desc &d, ProbDev &P);
+}
+
+// Checks of one problem description (shared with the solve server).
+int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
 {
   char buf[256];
   auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
@@ -160,6 +167,25 @@ static int mixed_grid(const mdg_solver *s)
   return (int)(g < s->nmtiles ? g : s->nmtiles);
 }
 
+// Device record of one problem from its description (offsets left at zero).
+void mdg::make_probdev(const mdg_problem_desc &d, ProbDev &P)
+{
+  memset(&P, 0, sizeof P);
+  P.ndim = d.ndim; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
+  P.n1 = d.n1; P.n2 = (d.ndim > 1) ? d.n2 : 1;
+  P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0]; P.bc_lo1 = d.bc_lo[1]; P.bc_hi1 = d.bc_hi[1];
+  P.prob_kind = d.prob_kind;
+  P.has_src = (d.geom == MDG_SPHERICAL);
+  P.gam = d.gam; P.Kpoly = d.Kpoly;
+  P.dx0 = d.dx[0]; P.dx1 = d.dx[1];
+  if (d.ndim == 2) cartesian_2d_constants(d, P.vol, P.area0, P.area1);
+  P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
+  P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
+  P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
+  P.x0 = d.startx[0];
+  if (d.ndim == 1 && d.geom == MDG_SPHERICAL) spherical_1d_constants(P.gk_area, P.gk_th1, P.gk_th2, P.gk_tc);
+}
+
 static void free_all(mdg_solver *s)
 {
   if (!s) return;
@@ -207,7 +233,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   const int ndim = descs[0].ndim;
   for (int m = 0; m < nprob; m++) {
     std::string why;
-    int rc = validate(descs[m], ndim, why);
+    int rc = validate_desc(descs[m], ndim, why);
     if (rc != MDG_OK) return fail(rc, "problem " + std::to_string(m) + ": " + why);
     if (precision == MDG_PREC_MIXED && (descs[m].ndim != 1 || descs[m].hydro_interp_order != 3))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
@@ -234,24 +260,11 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   for (int m = 0; m < nprob; m++) {
     const mdg_problem_desc &d = descs[m];
     ProbDev P;
-    memset(&P, 0, sizeof P);
-    P.ndim = d.ndim; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
-    P.n1 = d.n1; P.n2 = (d.ndim > 1) ? d.n2 : 1;
-    P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0]; P.bc_lo1 = d.bc_lo[1]; P.bc_hi1 = d.bc_hi[1];
-    P.prob_kind = d.prob_kind;
-    P.has_src = (d.geom == MDG_SPHERICAL);
+    make_probdev(d, P);
     P.cell_off = cell;
     P.geo_off = rc0;
     P.rc1_off = rc1;
     P.sh_off = sh;
-    P.gam = d.gam; P.Kpoly = d.Kpoly;
-    P.dx0 = d.dx[0]; P.dx1 = d.dx[1];
-    if (d.ndim == 2) cartesian_2d_constants(d, P.vol, P.area0, P.area1);
-    P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
-    P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
-    P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
-    P.x0 = d.startx[0];
-    if (d.ndim == 1 && d.geom == MDG_SPHERICAL) spherical_1d_constants(P.gk_area, P.gk_th1, P.gk_th2, P.gk_tc);
     s->hprobs.push_back(P);
     const int64_t nc = (int64_t)P.n1 * P.n2;
     if (nc > s->max_cells) s->max_cells = nc;

@@ -100,6 +100,8 @@ struct ProbTime {
   unsigned long long minacc;   // order-preserving encoding of the running min_dt
   int istep;
   int dt_ready;      // dt of the next step already finalized
+  int done;          // t >= tmax: the main.c loop (main.c:206) has ended; steps leave it unchanged
+  int err;           // MDG_ERR_NONFINITE once its estimate dropped below dtmin (main.c:229-238)
 };
 
 // Order-preserving map from double to uint64 so atomicMin on the integer is a min on

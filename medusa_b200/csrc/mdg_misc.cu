@@ -15,13 +15,24 @@ __global__ void dt_finalize_kernel(const ProbDev *__restrict__ probs, ProbTime *
   ProbTime T = times[m];
   if (T.dt_ready) return;
   const ProbDev &P = probs[m];
+  // the reference's time loop runs while t < tmax (main.c:206); past it nothing changes
+  // (an empty slot of a solve server has tmax = 0 and is done from the start)
+  if (!(T.t < P.tmax)) {
+    T.done = 1;
+    T.dt_ready = 1;
+    times[m] = T;
+    return;
+  }
   double min_dt = ord_to_dbl(T.minacc);
   if (T.istep == 0) min_dt = tmin(min_dt, P.initial_dt);
   min_dt = tmin(min_dt, P.dtmax);
   min_dt *= P.cfl;
   // main.c:229-238 aborts the run when the estimate drops below dtmin; here the
   // condition is recorded for the host (mdg_synchronize returns MDG_ERR_NONFINITE)
-  if (!(min_dt >= P.dtmin)) atomicExch(err, MDG_ERR_NONFINITE);
+  if (!(min_dt >= P.dtmin)) {
+    atomicExch(err, MDG_ERR_NONFINITE);
+    T.err = MDG_ERR_NONFINITE;
+  }
   double dt = min_dt;
   if (T.istep == 0) dt *= P.dt_init_safety;
   else dt = tmin(T.dtold * P.dt_grow_safety, dt);
@@ -40,8 +51,10 @@ __global__ void finish_kernel(ProbTime *__restrict__ times, int nprob)
 {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= nprob) return;
-  times[m].t = times[m].t_next;
-  times[m].istep += 1;
+  if (!times[m].done) {
+    times[m].t = times[m].t_next;
+    times[m].istep += 1;
+  }
   times[m].dt_ready = 0;
 }
 
@@ -80,7 +93,7 @@ __global__ void reset_time_kernel(ProbTime *times, int m)
   ProbTime T;
   T.t = 0.0; T.dt = 0.0; T.dtold = 1.0e100; T.t_bc1 = 0.0; T.t_next = 0.0;
   T.minacc = dbl_to_ord(1.0e100);
-  T.istep = 0; T.dt_ready = 0;
+  T.istep = 0; T.dt_ready = 0; T.done = 0; T.err = 0;
   times[m] = T;
 }
 

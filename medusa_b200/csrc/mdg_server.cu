@@ -1,0 +1,625 @@
+// Solve server: a request loop that keeps 1-D problems resident on one GPU and advances
+// every admitted problem together (continuous batching).
+//
+// No counterpart in the reference, whose executable advances one problem per process
+// through the main.c time loop (main.c:206-313).  Each request here is such a run: a
+// problem description, its initial state and its end time (desc.tmax); the loop steps it
+// with exactly the main.c rules until t >= tmax, after which the stage kernels leave it
+// untouched (ProbTime::done), so a result does not depend on when it is collected nor on
+// the other problems in the batch.
+//
+// Device memory is one set of arenas sized at creation from an HBM budget: state (P, PH),
+// the reconstruction and geometry tables and the FP32 weights, all indexed by zone units.
+// A request is admitted when a slot and a contiguous range of n1 + 2*NG units are free
+// (first fit, coalescing on release): the HBM footprint is the admission test.  Between
+// rounds of steps_per_round steps the loop admits queued requests (back-filling smaller
+// ones when the oldest does not fit), rebuilds the (problem, tile) list, runs the round --
+// for the mixed sweep one CUDA graph of persistent, work-queue fed stage launches, whose
+// arguments never change because the tile count lives in device memory -- and retires
+// the problems that reached their end time.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+#include "mdg_internal.h"
+#include "mdg_kernels.cuh"
+
+namespace mdg {
+int report_error(int code, const std::string &msg);
+int validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why);
+void make_probdev(const mdg_problem_desc &d, ProbDev &P);
+void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
+void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
+int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
+}
+
+using namespace mdg;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// failures are reported like the solver's: the message is read by mdg_last_error_message
+int sfail(int code, const std::string &msg) { return report_error(code, msg); }
+
+#define SCK(call)                                                                      \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return sfail(e_ == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA,  \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));                \
+  } while (0)
+
+// First-fit allocator over [0, cap) with coalescing of released ranges.
+class RangeAlloc {
+ public:
+  void reset(int64_t cap)
+  {
+    free_.clear();
+    if (cap > 0) free_[0] = cap;
+  }
+  int64_t alloc(int64_t n)
+  {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < n) continue;
+      const int64_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > n) free_[off + n] = len - n;
+      return off;
+    }
+    return -1;
+  }
+  void release(int64_t off, int64_t n)
+  {
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+ private:
+  std::map<int64_t, int64_t> free_;
+};
+
+struct Request {
+  long long id = 0;
+  mdg_problem_desc desc{};
+  std::vector<double> ic;       // [zone][5]
+  std::vector<double> result;   // [zone][5] once finished
+  int status = MDG_REQ_QUEUED;
+  int err = MDG_OK;
+  int slot = -1;
+  int64_t seg = -1, units = 0;
+  double t = 0.0;
+  int istep = 0;
+  Clock::time_point t_submit, t_admit, t_done;
+};
+
+double seconds(Clock::time_point a, Clock::time_point b)
+{
+  return std::chrono::duration<double>(b - a).count();
+}
+
+}  // namespace
+
+struct mdg_server {
+  mdg_server_config cfg{};
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  int64_t units = 0;
+  int max_probs = 0, max_tiles = 0, tile_len = 0;
+  ProbDev *d_probs = nullptr;
+  ProbTime *d_times = nullptr;
+  Tile *d_tiles = nullptr;
+  WorkQueue *d_queue = nullptr;
+  int *d_err = nullptr;
+  double *d_state = nullptr, *d_rc0 = nullptr, *d_geo = nullptr, *d_stage = nullptr;
+  float *d_mx = nullptr;
+  StateSoA P{}, PH{};
+  Tables tb{};
+  ProbTime *h_times = nullptr;   // pinned
+  std::vector<Request *> slots;
+  RangeAlloc alloc;
+  int64_t units_in_use = 0;
+  int ntiles = 0;
+  bool tiles_dirty = true;
+  cudaGraphExec_t graph = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // requests
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<Request *> queue;
+  std::unordered_map<long long, Request *> reqs;
+  long long next_id = 1;
+  long long submitted = 0;
+  // loop
+  std::mutex loop_mu;
+  std::thread th;
+  std::atomic<bool> running{false};
+  int loop_rc = MDG_OK;
+  std::string loop_msg;
+  // statistics of finished requests
+  long long completed = 0, failed = 0, rounds = 0;
+  double zone_updates = 0.0, device_ms = 0.0;
+  std::vector<double> latency, wait;
+};
+
+namespace {
+
+void free_server(mdg_server *s)
+{
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles); cudaFree(s->d_queue); cudaFree(s->d_err);
+  cudaFree(s->d_state); cudaFree(s->d_rc0); cudaFree(s->d_geo); cudaFree(s->d_stage); cudaFree(s->d_mx);
+  if (s->h_times) cudaFreeHost(s->h_times);
+  if (s->stream) cudaStreamDestroy(s->stream);
+  for (auto &kv : s->reqs) delete kv.second;
+}
+
+// bytes of device memory per zone unit: state P and PH, RC and GF tables, FP32 weights
+int64_t bytes_per_unit(int precision)
+{
+  return 2 * NPRIM * 8 + RC_NFIELDS * 8 + GF_NFIELDS * 8 + (precision == MDG_PREC_MIXED ? MX_NFIELDS * 4 : 0);
+}
+
+int persistent_grid(const mdg_server *s)
+{
+  int k = mixed_max_ctas_per_sm(s->cfg.threads);
+  if (k <= 0) k = 1;
+  if (s->cfg.ctas_per_sm > 0 && s->cfg.ctas_per_sm < k) k = s->cfg.ctas_per_sm;
+  return k * s->num_sms;
+}
+
+void queue_round(mdg_server *s, int nsteps)
+{
+  const bool mixed = s->cfg.precision == MDG_PREC_MIXED;
+  const int grid = mixed ? persistent_grid(s) : 0;
+  for (int k = 0; k < nsteps; k++) {
+    launch_dt_finalize(s->d_probs, s->d_times, s->max_probs, s->d_err, s->stream);
+    if (mixed) {
+      launch_stage1d_mixed(0, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
+                           s->P, s->P, s->PH, s->stream);
+      launch_stage1d_mixed(1, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
+                           s->PH, s->P, s->P, s->stream);
+    } else {
+      launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
+      launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
+    }
+    launch_finish(s->d_times, s->max_probs, s->stream);
+  }
+}
+
+// Upload tables, record, state and time of request r into slot r->slot, units r->seg...
+int admit(mdg_server *s, Request *r)
+{
+  const mdg_problem_desc &d = r->desc;
+  const int64_t w = r->units, seg = r->seg;
+  std::vector<double> rc((size_t)RC_NFIELDS * w, 0.0), geo((size_t)GF_NFIELDS * w, 0.0);
+  build_recon_table(d, 0, rc.data(), w, 0);
+  build_geo_1d(d, geo.data(), w, 0);
+  ProbDev P;
+  make_probdev(d, P);
+  P.cell_off = seg;
+  P.geo_off = seg;
+  P.sparse_conn = conn_is_sparse(geo.data(), w, 0, (int)w);
+  const size_t pitch = sizeof(double) * s->units;
+  SCK(cudaMemcpy2DAsync(s->d_rc0 + seg, pitch, rc.data(), sizeof(double) * w, sizeof(double) * w, RC_NFIELDS,
+                        cudaMemcpyHostToDevice, s->stream));
+  SCK(cudaMemcpy2DAsync(s->d_geo + seg, pitch, geo.data(), sizeof(double) * w, sizeof(double) * w, GF_NFIELDS,
+                        cudaMemcpyHostToDevice, s->stream));
+  if (s->cfg.precision == MDG_PREC_MIXED) {
+    std::vector<float> mx((size_t)MX_NFIELDS * w, 0.0f);
+    build_mixed_table(d, 0, mx.data(), w, 0);
+    SCK(cudaMemcpy2DAsync(s->d_mx + seg, sizeof(float) * s->units, mx.data(), sizeof(float) * w, sizeof(float) * w,
+                          MX_NFIELDS, cudaMemcpyHostToDevice, s->stream));
+  }
+  SCK(cudaMemcpyAsync(s->d_probs + r->slot, &P, sizeof P, cudaMemcpyHostToDevice, s->stream));
+  SCK(cudaMemcpyAsync(s->d_stage, r->ic.data(), sizeof(double) * NPRIM * d.n1, cudaMemcpyHostToDevice, s->stream));
+  launch_aos_to_soa(s->d_stage, s->P, seg, d.n1, s->stream);
+  launch_reset_time(s->d_times, r->slot, s->stream);
+  launch_initial_estimate_one(s->d_probs, s->d_times, r->slot, d.n1, s->tb, s->P, s->stream);
+  // the host sources above are stack/heap buffers: wait before they go out of scope
+  SCK(cudaStreamSynchronize(s->stream));
+  SCK(cudaGetLastError());
+  return MDG_OK;
+}
+
+int retire(mdg_server *s, Request *r, const ProbTime &T)
+{
+  const int n = r->desc.n1;
+  r->result.resize((size_t)NPRIM * n);
+  launch_soa_to_aos(s->P, r->seg, n, s->d_stage, s->stream);
+  SCK(cudaMemcpyAsync(r->result.data(), s->d_stage, sizeof(double) * NPRIM * n, cudaMemcpyDeviceToHost, s->stream));
+  SCK(cudaStreamSynchronize(s->stream));
+  r->t = T.t;
+  r->istep = T.istep;
+  r->err = T.err;
+  r->t_done = Clock::now();
+  s->slots[r->slot] = nullptr;
+  s->alloc.release(r->seg, r->units);
+  s->units_in_use -= r->units;
+  r->slot = -1;
+  s->tiles_dirty = true;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->status = T.err ? MDG_REQ_FAILED : MDG_REQ_DONE;
+    if (T.err) s->failed++;
+    else s->completed++;
+    s->zone_updates += (double)n * T.istep;
+    s->latency.push_back(seconds(r->t_submit, r->t_done));
+    s->wait.push_back(seconds(r->t_submit, r->t_admit));
+  }
+  s->cv.notify_all();
+  return MDG_OK;
+}
+
+// One scheduling round: admit, rebuild the tile list, step, retire.
+int round_once(mdg_server *s, int *active_out)
+{
+  std::lock_guard<std::mutex> lk(s->loop_mu);
+  SCK(cudaSetDevice(s->cfg.device));
+  // 1. admission (back-filling: a request that does not fit does not block smaller ones)
+  std::vector<Request *> adm;
+  {
+    std::lock_guard<std::mutex> ql(s->mu);
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+      Request *r = *it;
+      int slot = -1;
+      for (int k = 0; k < s->max_probs; k++)
+        if (!s->slots[k]) { slot = k; break; }
+      if (slot < 0) break;
+      const int64_t seg = s->alloc.alloc(r->units);
+      if (seg < 0) { ++it; continue; }
+      r->slot = slot;
+      r->seg = seg;
+      s->slots[slot] = r;
+      s->units_in_use += r->units;
+      r->status = MDG_REQ_RUNNING;
+      r->t_admit = Clock::now();
+      adm.push_back(r);
+      it = s->queue.erase(it);
+    }
+  }
+  for (Request *r : adm) {
+    int rc = admit(s, r);
+    if (rc != MDG_OK) return rc;
+    s->tiles_dirty = true;
+  }
+  // 2. the (problem, tile) list of the resident problems
+  int active = 0;
+  for (int k = 0; k < s->max_probs; k++) active += s->slots[k] != nullptr;
+  if (s->tiles_dirty) {
+    std::vector<Tile> tl;
+    for (int k = 0; k < s->max_probs; k++) {
+      if (!s->slots[k]) continue;
+      for (int i0 = 0; i0 < s->slots[k]->desc.n1; i0 += s->tile_len) tl.push_back(Tile{k, i0, 0, 0});
+    }
+    if ((int)tl.size() > s->max_tiles) return sfail(MDG_ERR_INTERNAL, "tile list exceeds its capacity");
+    if (!tl.empty())
+      SCK(cudaMemcpyAsync(s->d_tiles, tl.data(), sizeof(Tile) * tl.size(), cudaMemcpyHostToDevice, s->stream));
+    WorkQueue q{{0u, 0u}, (int)tl.size(), 0};
+    SCK(cudaMemcpyAsync(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaStreamSynchronize(s->stream));
+    s->ntiles = (int)tl.size();
+    s->tiles_dirty = false;
+  }
+  // 3. the round of steps
+  if (active > 0) {
+    const int K = s->cfg.steps_per_round;
+    SCK(cudaEventRecord(s->ev0, s->stream));
+    if (s->cfg.precision == MDG_PREC_MIXED) {
+      if (!s->graph) {
+        cudaGraph_t g = nullptr;
+        SCK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        queue_round(s, K);
+        const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (e != cudaSuccess) return sfail(MDG_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+          s->graph = nullptr;
+          return sfail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
+        }
+      }
+      SCK(cudaGraphLaunch(s->graph, s->stream));
+    } else {
+      queue_round(s, K);
+    }
+    SCK(cudaEventRecord(s->ev1, s->stream));
+    SCK(cudaGetLastError());
+  }
+  // 4. retire the problems that reached their end time (or failed)
+  SCK(cudaMemcpyAsync(s->h_times, s->d_times, sizeof(ProbTime) * s->max_probs, cudaMemcpyDeviceToHost, s->stream));
+  SCK(cudaStreamSynchronize(s->stream));
+  if (active > 0) {
+    float ms = 0.f;
+    SCK(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    s->device_ms += ms;
+    s->rounds++;
+  }
+  for (int k = 0; k < s->max_probs; k++) {
+    Request *r = s->slots[k];
+    if (!r) continue;
+    const ProbTime &T = s->h_times[k];
+    if (T.done || T.err) {
+      int rc = retire(s, r, T);
+      if (rc != MDG_OK) return rc;
+      active--;
+    }
+  }
+  if (active_out) *active_out = active;
+  return MDG_OK;
+}
+
+void loop_main(mdg_server *s)
+{
+  while (s->running.load()) {
+    int active = 0;
+    const int rc = round_once(s, &active);
+    if (rc != MDG_OK) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      s->loop_rc = rc;
+      s->loop_msg = mdg_last_error_message();
+      s->running = false;
+      s->cv.notify_all();
+      return;
+    }
+    if (active == 0) {
+      std::unique_lock<std::mutex> lk(s->mu);
+      if (s->queue.empty())
+        s->cv.wait_for(lk, std::chrono::milliseconds(1), [&] { return !s->queue.empty() || !s->running.load(); });
+    }
+  }
+}
+
+double percentile(std::vector<double> v, double q)
+{
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const double pos = q * (v.size() - 1);
+  const size_t i = (size_t)pos;
+  const double f = pos - i;
+  return (i + 1 < v.size()) ? v[i] * (1.0 - f) + v[i + 1] * f : v[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
+{
+  if (!cfg || !out) return sfail(MDG_ERR_INVALID, "cfg/out");
+  *out = nullptr;
+  const mdg_server_config &c = *cfg;
+  if (c.precision != MDG_PREC_FP64 && c.precision != MDG_PREC_MIXED) return sfail(MDG_ERR_INVALID, "precision");
+  if (c.max_problems < 1 || c.max_problems > (1 << 20)) return sfail(MDG_ERR_INVALID, "max_problems out of [1, 2^20]");
+  if (c.max_zones < 8 || c.max_zones > (1 << 26)) return sfail(MDG_ERR_INVALID, "max_zones out of [8, 2^26]");
+  if (c.steps_per_round < 1 || c.steps_per_round > 100000) return sfail(MDG_ERR_INVALID, "steps_per_round out of [1, 1e5]");
+  if (c.precision == MDG_PREC_MIXED && c.threads != 64 && c.threads != 128 && c.threads != 256)
+    return sfail(MDG_ERR_INVALID, "threads must be 64, 128 or 256");
+  const int64_t bpu = bytes_per_unit(c.precision);
+  const int64_t units = c.hbm_bytes / bpu;
+  if (units < c.max_zones + 2 * NG) return sfail(MDG_ERR_INVALID, "hbm_bytes too small for one problem of max_zones");
+  int ndev = 0;
+  SCK(cudaGetDeviceCount(&ndev));
+  if (c.device < 0 || c.device >= ndev) return sfail(MDG_ERR_INVALID, "device ordinal out of range");
+  SCK(cudaSetDevice(c.device));
+  mdg_server *s = new mdg_server();
+  s->cfg = c;
+  s->units = units;
+  s->max_probs = c.max_problems;
+  s->tile_len = (c.precision == MDG_PREC_MIXED) ? c.threads - 2 : TILE1;
+  s->max_tiles = (int)(units / s->tile_len + c.max_problems + 1);
+  s->slots.assign(c.max_problems, nullptr);
+  s->alloc.reset(units);
+  auto bail = [&](int rc) { free_server(s); delete s; return rc; };
+#define SCKB(call)                                                                         \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess)                                                                 \
+      return bail(sfail(e_ == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA, \
+                        std::string(#call) + ": " + cudaGetErrorString(e_)));              \
+  } while (0)
+  SCKB(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, c.device));
+  SCKB(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  SCKB(cudaEventCreate(&s->ev0));
+  SCKB(cudaEventCreate(&s->ev1));
+  SCKB(cudaMalloc(&s->d_probs, sizeof(ProbDev) * s->max_probs));
+  SCKB(cudaMalloc(&s->d_times, sizeof(ProbTime) * s->max_probs));
+  SCKB(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->max_tiles));
+  SCKB(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
+  SCKB(cudaMalloc(&s->d_err, sizeof(int)));
+  SCKB(cudaMalloc(&s->d_state, sizeof(double) * 2 * NPRIM * units));
+  SCKB(cudaMalloc(&s->d_rc0, sizeof(double) * RC_NFIELDS * units));
+  SCKB(cudaMalloc(&s->d_geo, sizeof(double) * GF_NFIELDS * units));
+  SCKB(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * c.max_zones));
+  if (c.precision == MDG_PREC_MIXED) SCKB(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * units));
+  SCKB(cudaMallocHost(&s->h_times, sizeof(ProbTime) * s->max_probs));
+  // empty slots: a zero record has tmax = 0, so the time loop treats it as finished
+  SCKB(cudaMemset(s->d_probs, 0, sizeof(ProbDev) * s->max_probs));
+  SCKB(cudaMemset(s->d_times, 0, sizeof(ProbTime) * s->max_probs));
+  SCKB(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
+  SCKB(cudaMemset(s->d_err, 0, sizeof(int)));
+  SCKB(cudaMemset(s->d_state, 0, sizeof(double) * 2 * NPRIM * units));
+#undef SCKB
+  for (int v = 0; v < NPRIM; v++) {
+    s->P.v[v] = s->d_state + (int64_t)v * units;
+    s->PH.v[v] = s->d_state + (int64_t)(NPRIM + v) * units;
+  }
+  s->tb.rc0 = s->d_rc0; s->tb.rc0_stride = units;
+  s->tb.geo = s->d_geo; s->tb.geo_stride = units;
+  s->tb.mx = s->d_mx;
+  *out = s;
+  return MDG_OK;
+}
+
+int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double *prim, long long *id)
+{
+  if (!s || !desc || !prim) return sfail(MDG_ERR_INVALID, "server/desc/prim");
+  std::string why;
+  int rc = validate_desc(*desc, 1, why);
+  if (rc != MDG_OK) return sfail(rc, "request: " + why);
+  if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
+    return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
+  if (desc->n1 > s->cfg.max_zones) return sfail(MDG_ERR_OUTOFMEM, "request: n1 exceeds the server's max_zones");
+  if (s->cfg.precision == MDG_PREC_MIXED) {
+    if (desc->hydro_interp_order != 3)
+      return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep is built for parabolic reconstruction");
+    if (desc->geom == MDG_SPHERICAL && !(desc->startx[0] >= 0.0))
+      return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep needs a spherical grid starting at r >= 0");
+  }
+  Request *r = new Request();
+  r->desc = *desc;
+  r->ic.assign(prim, prim + (size_t)NPRIM * desc->n1);
+  r->units = desc->n1 + 2 * NG;
+  r->t_submit = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    s->reqs[r->id] = r;
+    s->queue.push_back(r);
+    s->submitted++;
+  }
+  s->cv.notify_all();
+  if (id) *id = r->id;
+  return MDG_OK;
+}
+
+int mdg_server_run(mdg_server *s, int rounds, int *active)
+{
+  if (!s) return sfail(MDG_ERR_INVALID, "server");
+  if (s->running.load()) return sfail(MDG_ERR_LOGICAL, "the request loop is running on its own thread");
+  int act = 0;
+  for (int k = 0; rounds <= 0 || k < rounds; k++) {
+    int rc = round_once(s, &act);
+    if (rc != MDG_OK) return rc;
+    if (rounds <= 0) {
+      std::lock_guard<std::mutex> lk(s->mu);
+      if (act == 0 && s->queue.empty()) break;
+    }
+  }
+  if (active) *active = act;
+  return MDG_OK;
+}
+
+int mdg_server_start(mdg_server *s)
+{
+  if (!s) return sfail(MDG_ERR_INVALID, "server");
+  if (s->running.load()) return MDG_OK;
+  s->loop_rc = MDG_OK;
+  s->running = true;
+  s->th = std::thread(loop_main, s);
+  return MDG_OK;
+}
+
+int mdg_server_stop(mdg_server *s)
+{
+  if (!s) return sfail(MDG_ERR_INVALID, "server");
+  s->running = false;
+  s->cv.notify_all();
+  if (s->th.joinable()) s->th.join();
+  if (s->loop_rc != MDG_OK) return sfail(s->loop_rc, "request loop: " + s->loop_msg);
+  return MDG_OK;
+}
+
+int mdg_server_poll(mdg_server *s, long long id, int *status)
+{
+  if (!s || !status) return sfail(MDG_ERR_INVALID, "server/status");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return sfail(MDG_ERR_NOTFOUND, "no such request");
+  *status = it->second->status;
+  return MDG_OK;
+}
+
+int mdg_server_wait(mdg_server *s, long long id, double timeout_s, int *status)
+{
+  if (!s) return sfail(MDG_ERR_INVALID, "server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return sfail(MDG_ERR_NOTFOUND, "no such request");
+  Request *r = it->second;
+  const auto until = Clock::now() + std::chrono::duration<double>(timeout_s > 0 ? timeout_s : 0.0);
+  s->cv.wait_until(lk, until, [&] {
+    return r->status == MDG_REQ_DONE || r->status == MDG_REQ_FAILED || !s->running.load();
+  });
+  if (status) *status = r->status;
+  return MDG_OK;
+}
+
+int mdg_server_result(mdg_server *s, long long id, double *prim, double *t, int *istep, double *latency_s)
+{
+  if (!s) return sfail(MDG_ERR_INVALID, "server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(id);
+  if (it == s->reqs.end()) return sfail(MDG_ERR_NOTFOUND, "no such request");
+  Request *r = it->second;
+  if (r->status != MDG_REQ_DONE && r->status != MDG_REQ_FAILED)
+    return sfail(MDG_ERR_LOGICAL, "request has not finished");
+  if (prim) std::memcpy(prim, r->result.data(), sizeof(double) * r->result.size());
+  if (t) *t = r->t;
+  if (istep) *istep = r->istep;
+  if (latency_s) *latency_s = seconds(r->t_submit, r->t_done);
+  const int err = r->err;
+  s->reqs.erase(it);
+  delete r;
+  return err ? sfail(err, "request stopped: time step dropped below dtmin") : MDG_OK;
+}
+
+int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st)
+{
+  if (!s || !st) return sfail(MDG_ERR_INVALID, "server/stats");
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(st, 0, sizeof *st);
+  st->submitted = s->submitted;
+  st->completed = s->completed;
+  st->failed = s->failed;
+  st->queued = (long long)s->queue.size();
+  long long running = 0;
+  for (auto &kv : s->reqs) running += kv.second->status == MDG_REQ_RUNNING;
+  st->running = running;
+  st->rounds = s->rounds;
+  st->zone_updates = s->zone_updates;
+  st->device_seconds = s->device_ms * 1e-3;
+  st->latency_p50 = percentile(s->latency, 0.50);
+  st->latency_p99 = percentile(s->latency, 0.99);
+  st->wait_p50 = percentile(s->wait, 0.50);
+  st->wait_p99 = percentile(s->wait, 0.99);
+  const int64_t bpu = bytes_per_unit(s->cfg.precision);
+  st->hbm_capacity = (double)s->units * bpu;
+  st->hbm_in_use = (double)s->units_in_use * bpu;
+  return MDG_OK;
+}
+
+int mdg_server_destroy(mdg_server *s)
+{
+  if (!s) return MDG_OK;
+  mdg_server_stop(s);
+  cudaSetDevice(s->cfg.device);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_server(s);
+  delete s;
+  return MDG_OK;
+}
+
+}  // extern "C"

@@ -29,6 +29,7 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   __shared__ double sred[32];
 
   const Tile tile = tiles[blockIdx.x];
+  if (times[tile.prob].done) return;   // past tmax: the time loop has ended (CTA-uniform)
   const ProbDev &P = probs[tile.prob];
   const double dt = times[tile.prob].dt;
   const double t_bc = STAGE ? times[tile.prob].t_bc1 : times[tile.prob].t;

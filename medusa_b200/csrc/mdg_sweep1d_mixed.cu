@@ -289,6 +289,14 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
 
   while (item < ntiles) {
     const Tile tile = tiles[item];
+    if (times[tile.prob].done) {       // past tmax: the time loop has ended (CTA-uniform)
+      if (!use_queue) break;
+      __syncthreads();                  // every thread has read the current s_item
+      if (t == 0) s_item = (int)atomicAdd(&q->head[STAGE], 1u);
+      __syncthreads();
+      item = s_item;
+      continue;
+    }
     const ProbDev &P = probs[tile.prob];
     const double dt = times[tile.prob].dt;
     const double t_bc = STAGE ? times[tile.prob].t_bc1 : times[tile.prob].t;

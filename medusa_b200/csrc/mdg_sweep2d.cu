@@ -124,6 +124,7 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   __shared__ double xrc[RC_NFIELDS][TIX2 + 2];
   __shared__ double sred[32];
   const Tile tile = tiles[blockIdx.x];
+  if (times[tile.prob].done) return;   // past tmax: the time loop has ended (CTA-uniform)
   const ProbDev &P = probs[tile.prob];
   const int n1 = P.n1, n2 = P.n2;
   const int t = threadIdx.x;
@@ -238,6 +239,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   __shared__ double sred[32];
 
   const Tile tile = tiles[blockIdx.x];
+  if (times[tile.prob].done) return;   // past tmax: the time loop has ended (CTA-uniform)
   const ProbDev &P = probs[tile.prob];
   const double dt = times[tile.prob].dt;
   const int t = threadIdx.x;

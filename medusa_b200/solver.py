@@ -48,6 +48,23 @@ class LaunchConfig(ctypes.Structure):
         return {"threads": self.threads, "ctas_per_sm": self.ctas_per_sm, "steps_per_graph": self.steps_per_graph}
 
 
+class ServerConfig(ctypes.Structure):
+    """mdg_server_config of include/medusa_b200.h."""
+    _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("hbm_bytes", ctypes.c_longlong),
+                ("max_problems", ctypes.c_int), ("max_zones", ctypes.c_int), ("steps_per_round", ctypes.c_int),
+                ("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    """mdg_server_stats of include/medusa_b200.h."""
+    _fields_ = [(n, ctypes.c_longlong) for n in ("submitted", "completed", "failed", "queued", "running", "rounds")] + \
+               [(n, ctypes.c_double) for n in ("zone_updates", "device_seconds", "latency_p50", "latency_p99",
+                                                "wait_p50", "wait_p99", "hbm_capacity", "hbm_in_use")]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 class ProblemDesc(ctypes.Structure):
     """mdg_problem_desc of include/medusa_b200.h."""
     _fields_ = [("ndim", ctypes.c_int), ("geom", ctypes.c_int), ("eos", ctypes.c_int),
@@ -111,10 +128,23 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     L.mdg_autotune.argtypes = [vp, i, ctypes.POINTER(LaunchConfig), ctypes.POINTER(d)]
     L.mdg_conserved_totals.argtypes = [vp, vp, vp]
+    ll = ctypes.c_longlong
+    L.mdg_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+    L.mdg_server_submit.argtypes = [vp, ctypes.POINTER(ProblemDesc), vp, ctypes.POINTER(ll)]
+    L.mdg_server_run.argtypes = [vp, i, ctypes.POINTER(i)]
+    L.mdg_server_start.argtypes = [vp]
+    L.mdg_server_stop.argtypes = [vp]
+    L.mdg_server_poll.argtypes = [vp, ll, ctypes.POINTER(i)]
+    L.mdg_server_wait.argtypes = [vp, ll, d, ctypes.POINTER(i)]
+    L.mdg_server_result.argtypes = [vp, ll, vp, ctypes.POINTER(d), ctypes.POINTER(i), ctypes.POINTER(d)]
+    L.mdg_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+    L.mdg_server_destroy.argtypes = [vp]
     for name in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step", "mdg_download_state",
                  "mdg_get_time", "mdg_get_stream", "mdg_synchronize", "mdg_destroy", "mdg_set_timing",
                  "mdg_get_timers", "mdg_get_launch_config", "mdg_set_launch_config", "mdg_autotune",
-                 "mdg_conserved_totals"):
+                 "mdg_conserved_totals", "mdg_server_create", "mdg_server_submit", "mdg_server_run",
+                 "mdg_server_start", "mdg_server_stop", "mdg_server_poll", "mdg_server_wait", "mdg_server_result",
+                 "mdg_server_get_stats", "mdg_server_destroy"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -244,3 +274,86 @@ class Solver:
         s = ctypes.c_void_p()
         _check(library().mdg_get_stream(self._h, ctypes.byref(s)), "mdg_get_stream")
         return s.value or 0
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
+class Server:
+    """Solve server (mdg_server_*): 1-D problems resident on one GPU, admitted by their
+    device-memory footprint and advanced together; each request runs to its end time
+    (the problem's tmax)."""
+
+    def __init__(self, precision: int = PREC_MIXED, device: int = 0, hbm_bytes: int = 2 << 30,
+                 max_problems: int = 4096, max_zones: int = 16384, steps_per_round: int = 20,
+                 threads: int = 64, ctas_per_sm: int = 0):
+        L = library()
+        c = ServerConfig(device, precision, int(hbm_bytes), max_problems, max_zones, steps_per_round, threads,
+                         ctas_per_sm)
+        h = ctypes.c_void_p()
+        _check(L.mdg_server_create(ctypes.byref(c), ctypes.byref(h)), "mdg_server_create")
+        self._h = h
+        self._n = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().mdg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def submit(self, pb: "_pb.Problem") -> int:
+        ic = np.ascontiguousarray(pb.ic, dtype=np.float64)
+        d = desc_of(pb)
+        rid = ctypes.c_longlong()
+        _check(library().mdg_server_submit(self._h, ctypes.byref(d), ic.ctypes.data, ctypes.byref(rid)),
+               "mdg_server_submit")
+        self._n[rid.value] = pb.ncell
+        return rid.value
+
+    def run(self, rounds: int = 0) -> int:
+        act = ctypes.c_int()
+        _check(library().mdg_server_run(self._h, int(rounds), ctypes.byref(act)), "mdg_server_run")
+        return act.value
+
+    def start(self):
+        _check(library().mdg_server_start(self._h), "mdg_server_start")
+
+    def stop(self):
+        _check(library().mdg_server_stop(self._h), "mdg_server_stop")
+
+    def poll(self, rid: int) -> int:
+        st = ctypes.c_int()
+        _check(library().mdg_server_poll(self._h, rid, ctypes.byref(st)), "mdg_server_poll")
+        return st.value
+
+    def wait(self, rid: int, timeout: float = 60.0) -> int:
+        st = ctypes.c_int()
+        _check(library().mdg_server_wait(self._h, rid, float(timeout), ctypes.byref(st)), "mdg_server_wait")
+        return st.value
+
+    def result(self, rid: int):
+        """(final state [zone][5], t, steps, seconds from submission to completion)."""
+        prim = np.empty((self._n[rid], 5))
+        t, lat = ctypes.c_double(), ctypes.c_double()
+        ist = ctypes.c_int()
+        _check(library().mdg_server_result(self._h, rid, prim.ctypes.data, ctypes.byref(t), ctypes.byref(ist),
+                                           ctypes.byref(lat)), "mdg_server_result")
+        del self._n[rid]
+        return prim, t.value, ist.value, lat.value
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(library().mdg_server_get_stats(self._h, ctypes.byref(st)), "mdg_server_get_stats")
+        return st.as_dict()
+

@@ -89,3 +89,24 @@ def test_launch_config_calls_reject_null_solver():
     assert L.mdg_set_launch_config(None, ctypes.byref(c)) == 1
     assert L.mdg_autotune(None, 3, None, None) == 1
     assert L.mdg_conserved_totals(None, None, None) == 1
+
+
+@pytest.mark.parametrize("field,value", [("precision", 7), ("max_problems", 0), ("max_zones", 2),
+                                         ("steps_per_round", 0), ("threads", 96), ("hbm_bytes", 1000)])
+def test_server_config_is_checked_before_any_device_work(field, value):
+    c = S.ServerConfig(0, S.PREC_MIXED, 1 << 30, 64, 4096, 10, 64, 0)
+    setattr(c, field, value)
+    h = ctypes.c_void_p()
+    assert S.library().mdg_server_create(ctypes.byref(c), ctypes.byref(h)) == 1
+    assert not h.value
+    assert S.library().mdg_last_error_message()
+
+
+def test_server_calls_reject_null_handle():
+    L = S.library()
+    st = ctypes.c_int()
+    assert L.mdg_server_poll(None, 1, ctypes.byref(st)) == 1
+    assert L.mdg_server_run(None, 1, None) == 1
+    assert L.mdg_server_start(None) == 1
+    assert L.mdg_server_stop(None) == 1
+    assert L.mdg_server_destroy(None) == 0

@@ -1,0 +1,157 @@
+"""The solve server (mdg_server_*): requests run to their end time, results equal the
+solver's, each result is the same alone and in a mix, and admission respects the
+device-memory budget.
+
+Equality here is bit-for-bit: the stage kernels do the same arithmetic for a zone whatever
+else is in the batch, and a problem that has reached its end time is left unchanged by
+later rounds (the main.c loop has ended for it), so neither the company of other problems
+nor the round at which a result is collected can change it.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+from medusa_b200 import problems as P
+from medusa_b200.solver import (PREC_FP64, PREC_MIXED, REQ_DONE, REQ_QUEUED, REQ_RUNNING, MdgError, Server,
+                                Solver)
+
+pytestmark = pytest.mark.gpu
+
+
+def _req(kind, n1, gam, t_end, **kw):
+    return P.spherical_1d(kind, n1, gam, **kw).copy(tmax=t_end)
+
+
+def _mix():
+    """A handful of requests of different kinds, sizes and end times."""
+    return [
+        _req("sod", 300, 1.4, 0.05, rho_ratio=10.0, p_ratio=100.0),
+        _req("noh", 200, 5.0 / 3.0, 0.08),
+        _req("sedov", 420, 1.4, 0.02, p_ratio=1.0e4, r0=0.05),
+        _req("sod", 150, 4.0 / 3.0, 0.03, rho_ratio=3.0, p_ratio=20.0),
+        _req("sedov", 700, 5.0 / 3.0, 0.015, p_ratio=3.0e3, r0=0.08),
+        _req("noh", 333, 1.4, 0.05),
+    ]
+
+
+def _solver_result(pb, precision):
+    """The same run through the solver: step until the time loop has ended."""
+    with Solver(pb, precision=precision) as s:
+        for _ in range(2000):
+            s.step(25)
+            t, _, ist = s.time(0)
+            if t >= pb.tmax:
+                break
+        s.step(5)   # further steps must change nothing
+        s.synchronize()
+        return s.update_cpu(0), s.time(0)
+
+
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_server_results_equal_solver(precision):
+    reqs = _mix()
+    with Server(precision=precision, hbm_bytes=256 << 20, max_problems=16, max_zones=4096,
+                steps_per_round=17) as srv:
+        ids = [srv.submit(pb) for pb in reqs]
+        assert srv.run(0) == 0
+        st = srv.stats()
+        assert st["completed"] == len(reqs) and st["failed"] == 0 and st["queued"] == 0
+        for rid, pb in zip(ids, reqs):
+            assert srv.poll(rid) == REQ_DONE
+            prim, t, ist, lat = srv.result(rid)
+            ref, (rt, _, rist) = _solver_result(pb, precision)
+            assert t >= pb.tmax and t == rt and ist == rist
+            assert np.array_equal(prim, ref)
+            assert lat > 0.0
+
+
+def test_server_result_same_alone_and_in_mix():
+    """Continuous batching: a request's result does not depend on what else is resident,
+    nor on when the others arrive."""
+    reqs = _mix()
+    target = reqs[2]
+    with Server(precision=PREC_MIXED, hbm_bytes=256 << 20, max_problems=16, max_zones=4096,
+                steps_per_round=13) as srv:
+        rid = srv.submit(target)
+        srv.run(0)
+        alone = srv.result(rid)
+    with Server(precision=PREC_MIXED, hbm_bytes=256 << 20, max_problems=16, max_zones=4096,
+                steps_per_round=13) as srv:
+        others = [srv.submit(pb) for pb in reqs[:2]]
+        srv.run(3)                       # the target arrives while two others run
+        rid = srv.submit(target)
+        srv.run(2)
+        late = [srv.submit(pb) for pb in reqs[3:]]   # and more arrive while it runs
+        srv.run(0)
+        mixed = srv.result(rid)
+        for r in others + late:
+            srv.result(r)
+    assert np.array_equal(alone[0], mixed[0])
+    assert alone[1] == mixed[1] and alone[2] == mixed[2]
+
+
+def test_server_admission_respects_memory_budget():
+    """With room for about two problems at a time, the rest wait in the queue and are
+    admitted as earlier ones finish; no more memory is ever held than the budget."""
+    reqs = [_req("sod", 1000, 1.4, 0.02 + 0.002 * k, rho_ratio=5.0, p_ratio=40.0) for k in range(6)]
+    bpu = 2 * 5 * 8 + 22 * 8 + 40 * 8 + 11 * 4
+    budget = bpu * (2 * 1004 + 500)
+    with Server(precision=PREC_MIXED, hbm_bytes=budget, max_problems=8, max_zones=1000,
+                steps_per_round=10) as srv:
+        ids = [srv.submit(pb) for pb in reqs]
+        srv.run(1)
+        st = [srv.poll(r) for r in ids]
+        assert st.count(REQ_RUNNING) == 2 and st.count(REQ_QUEUED) == 4
+        peak = 0.0
+        for _ in range(10000):
+            act = srv.run(1)
+            s = srv.stats()
+            peak = max(peak, s["hbm_in_use"])
+            assert s["hbm_in_use"] <= s["hbm_capacity"]
+            if act == 0 and s["queued"] == 0:
+                break
+        assert srv.stats()["completed"] == len(reqs)
+        assert 0 < peak <= budget
+        for r in ids:
+            srv.result(r)
+
+
+def test_server_request_loop_thread():
+    """The loop on the server's own thread while this thread submits and collects."""
+    reqs = _mix()
+    with Server(precision=PREC_MIXED, hbm_bytes=256 << 20, max_problems=16, max_zones=4096,
+                steps_per_round=20) as srv:
+        srv.start()
+        got = {}
+
+        def client(pbs):
+            for pb in pbs:
+                got[srv.submit(pb)] = pb
+
+        th = threading.Thread(target=client, args=(reqs,))
+        th.start()
+        th.join()
+        for rid in list(got):
+            assert srv.wait(rid, timeout=120.0) == REQ_DONE
+        srv.stop()
+        s = srv.stats()
+        assert s["completed"] == len(reqs) and s["latency_p99"] >= s["latency_p50"] > 0.0
+        for rid, pb in got.items():
+            prim, t, ist, lat = srv.result(rid)
+            assert np.all(np.isfinite(prim)) and t >= pb.tmax
+
+
+@pytest.mark.parametrize("bad,code", [
+    (dict(tmax=1.0e100), 1),                 # no end time
+    (dict(n=(5000, 1, 1)), 6),               # larger than max_zones
+    (dict(hydro_interp_order=2), 5),         # the mixed sweep is parabolic only
+])
+def test_server_rejects_requests(bad, code):
+    pb = _req("sod", 100, 1.4, 0.01).copy(**bad)
+    if "n" in bad:
+        pb = pb.copy(ic=np.tile(pb.ic[:1], (bad["n"][0], 1)), dx=(1.0 / bad["n"][0], 2.0, 2.0 * np.pi))
+    with Server(precision=PREC_MIXED, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
+        with pytest.raises(MdgError) as e:
+            srv.submit(pb)
+        assert e.value.code == code
