@@ -317,6 +317,12 @@ def run_reference_arm(args, ctx):
         config = {"workload": "kelvin_helmholtz_2d_%dx%d_fp64" % (NX, NX), "global_batch": 1,
                   "seq_len": NX * NX, "parallelism": "replicas", "l2": "inputs larger than L2"}
         dtype = "f64"
+    elif args.workload == "server":
+        from medusa_b200 import loadgen
+        probs = loadgen.request_stream(args.server_requests, seed=11)
+        cb = cpu_baseline_ensemble(probs)
+        config = {"workload": "server_stream_1d_spherical_256_8192_zones", "requests": len(probs)}
+        dtype = "f64"
     else:
         probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED)
         cb = cpu_baseline_ensemble(probs)
@@ -546,13 +552,80 @@ def run_kh(args, ctx):
     print(json.dumps(line), flush=True)
 
 
+def run_server(args, ctx):
+    """Solve-server stream: seeded 1-D spherical requests (Sod/Noh/Sedov, 256-8192 zones,
+    each to its end time) submitted with Poisson arrivals at a swept rate to a running
+    server, mixed precision and plain FP64; throughput and p50/p99 time-to-solution."""
+    import math
+    from medusa_b200 import loadgen
+    from medusa_b200.solver import PREC_FP64, PREC_MIXED, Server
+
+    rates = [float(r) for r in args.server_rates.split(",")]
+    reqs = loadgen.request_stream(args.server_requests, seed=11 + ctx.rank)
+    spr = 20
+    sweep = {}
+    best = {}
+    for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64)):
+        sweep[name] = []
+        srv = Server(precision=prec, device=ctx.local, hbm_bytes=24 << 30, max_problems=16384, max_zones=8192,
+                     steps_per_round=spr, threads=64, ctas_per_sm=12)
+        srv.start()
+        # warm-up: graph capture and first admissions
+        loadgen.drive(srv, reqs[:32], math.inf)
+        for rate in rates:
+            n = len(reqs) if math.isinf(rate) else int(min(len(reqs), max(200, rate * args.server_seconds)))
+            ctx.barrier()
+            r = loadgen.drive(srv, reqs[:n], rate)
+            sweep[name].append(r)
+        st = srv.stats()
+        srv.stop()
+        srv.close()
+        best[name] = max(sweep[name], key=lambda r: r["zone_updates_per_s"])
+        best[name]["device_seconds_total"] = st["device_seconds"]
+        best[name]["rounds_total"] = st["rounds"]
+    if ctx.rank != 0:
+        return
+    peak, peak_kind = read_peaks()
+    m = best["mixed"]
+    zu_dev = m["zone_updates_per_s"]
+    value = ctx.world * m["zone_updates_per_s"]
+    h2d = sum(pb.ncell for pb in reqs[:m["requests"]]) * 40
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": ctx.world,
+        "steps": spr, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "server_stream_1d_spherical_256_8192_zones",
+                   "requests": len(reqs), "rates_req_per_s": args.server_rates,
+                   "mix": "1-D spherical Sod/Noh/Sedov to their end times (the 1-D part of the request mix)",
+                   "steps_per_round": spr, "parallelism": "single" if ctx.world == 1 else "independent servers"},
+        "p50_s": m["latency_p50_s"], "p99_s": m["latency_p99_s"],
+        "sweep": sweep,
+        "fp64_best_zone_updates_per_s": best["fp64"]["zone_updates_per_s"],
+        "mixed_over_fp64": m["zone_updates_per_s"] / best["fp64"]["zone_updates_per_s"],
+        "gpu_launches": 4 * spr * m["rounds_total"],
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / max(1, m["rounds_total"]),
+                "d2h_bytes_per_step": h2d / max(1, m["rounds_total"]),
+                "timed": "submission of every request from host memory to the return of every final state"},
+        "roofline": {"bound": "hbm", "achieved": 200.0 * zu_dev / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": 200.0 * zu_dev / 1e9 / peak, "traffic": None,
+                     "note": "whole-stream rate x 200 B/zone-update (1-D B_alg), wall clock",
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048", "server"])
+    ap.add_argument("--server-requests", type=int, default=6000)
+    ap.add_argument("--server-rates", default="1000,4000,16000,inf",
+                    help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
+    ap.add_argument("--server-seconds", type=float, default=3.0,
+                    help="server: length of the arrival window at each finite rate")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE_COUNT,
                     help="ensemble: number of problems (a smaller ensemble for profiling runs)")
@@ -572,6 +645,8 @@ def main():
         torch.cuda.set_device(ctx.local)
         if args.workload == "ensemble":
             run_ensemble(args, ctx)
+        elif args.workload == "server":
+            run_server(args, ctx)
         else:
             run_kh(args, ctx)
     finally:

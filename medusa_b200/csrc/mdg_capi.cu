@@ -288,13 +288,15 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   s->ntiles = (int)tiles.size();
   const int nstate = (ndim == 2) ? 3 : 2;   // P, PH (+ ACC in 2-D)
 
-  // host tables
-  std::vector<double> h_rc0((size_t)RC_NFIELDS * rc0), h_rc1, h_geo;
+  // host tables of the FP64 sweeps (Romberg moments, bit-identical to the reference's);
+  // the mixed sweep's tables are built on the device from closed-form moments below
+  const bool dev_tables = precision == MDG_PREC_MIXED;
+  const size_t n_rc0 = (size_t)RC_NFIELDS * rc0, n_geo = (ndim == 2) ? 0 : (size_t)GF_NFIELDS * rc0;
+  std::vector<double> h_rc0, h_rc1, h_geo;
+  if (!dev_tables) h_rc0.assign(n_rc0, 0.0);
   if (ndim == 2) h_rc1.assign((size_t)RC_NFIELDS * rc1, 0.0);
-  else h_geo.assign((size_t)GF_NFIELDS * rc0, 0.0);
-  std::vector<float> h_mx;
-  if (precision == MDG_PREC_MIXED) h_mx.assign((size_t)MX_NFIELDS * rc0, 0.0f);
-  for (int m = 0; m < nprob; m++) {
+  else if (!dev_tables) h_geo.assign(n_geo, 0.0);
+  for (int m = 0; m < nprob && !dev_tables; m++) {
     build_recon_table(descs[m], 0, h_rc0.data(), rc0, s->hprobs[m].geo_off);
     if (ndim == 2) {
       build_recon_table(descs[m], 1, h_rc1.data(), rc1, s->hprobs[m].rc1_off);
@@ -302,7 +304,6 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
       build_geo_1d(descs[m], h_geo.data(), rc0, s->hprobs[m].geo_off);
       s->hprobs[m].sparse_conn = conn_is_sparse(h_geo.data(), rc0, s->hprobs[m].geo_off, descs[m].n1 + 2 * NG);
     }
-    if (precision == MDG_PREC_MIXED) build_mixed_table(descs[m], 0, h_mx.data(), rc0, s->hprobs[m].geo_off);
   }
 
   auto cleanup_fail = [&](int code) { free_all(s); delete s; return code; };
@@ -320,28 +321,32 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMalloc(&s->d_probs, sizeof(ProbDev) * nprob));
   CKC(cudaMalloc(&s->d_times, sizeof(ProbTime) * nprob));
   CKC(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->ntiles));
-  CKC(cudaMalloc(&s->d_rc0, sizeof(double) * h_rc0.size()));
+  CKC(cudaMalloc(&s->d_rc0, sizeof(double) * n_rc0));
   if (ndim == 2) CKC(cudaMalloc(&s->d_rc1, sizeof(double) * h_rc1.size()));
-  else CKC(cudaMalloc(&s->d_geo, sizeof(double) * h_geo.size()));
+  else CKC(cudaMalloc(&s->d_geo, sizeof(double) * n_geo));
   CKC(cudaMalloc(&s->d_state, sizeof(double) * nstate * NPRIM * cell));
   CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
   CKC(cudaMalloc(&s->d_err, sizeof(int)));
   CKC(cudaMalloc(&s->d_totals, sizeof(double) * 2 * nprob));
   CKC(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
   CKC(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
-  if (precision == MDG_PREC_MIXED) {
-    CKC(cudaMalloc(&s->d_mx, sizeof(float) * h_mx.size()));
-    CKC(cudaMemcpy(s->d_mx, h_mx.data(), sizeof(float) * h_mx.size(), cudaMemcpyHostToDevice));
-  }
+  if (precision == MDG_PREC_MIXED) CKC(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * rc0));
   CKC(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock0, sh > 0 ? sh : 1));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock1, sh > 0 ? sh : 1));
 
   CKC(cudaMemcpy(s->d_probs, s->hprobs.data(), sizeof(ProbDev) * nprob, cudaMemcpyHostToDevice));
   CKC(cudaMemcpy(s->d_tiles, tiles.data(), sizeof(Tile) * s->ntiles, cudaMemcpyHostToDevice));
-  CKC(cudaMemcpy(s->d_rc0, h_rc0.data(), sizeof(double) * h_rc0.size(), cudaMemcpyHostToDevice));
+  if (dev_tables) {
+    for (int m = 0; m < nprob; m++)
+      launch_build_tables_1d(s->d_probs, m, descs[m].n1, s->d_rc0, s->d_geo, s->d_mx, rc0, s->stream);
+    CKC(cudaGetLastError());
+    CKC(cudaStreamSynchronize(s->stream));
+  } else {
+    CKC(cudaMemcpy(s->d_rc0, h_rc0.data(), sizeof(double) * n_rc0, cudaMemcpyHostToDevice));
+    if (ndim != 2) CKC(cudaMemcpy(s->d_geo, h_geo.data(), sizeof(double) * n_geo, cudaMemcpyHostToDevice));
+  }
   if (ndim == 2) CKC(cudaMemcpy(s->d_rc1, h_rc1.data(), sizeof(double) * h_rc1.size(), cudaMemcpyHostToDevice));
-  else CKC(cudaMemcpy(s->d_geo, h_geo.data(), sizeof(double) * h_geo.size(), cudaMemcpyHostToDevice));
   CKC(cudaMemset(s->d_state, 0, sizeof(double) * nstate * NPRIM * cell));
   CKC(cudaMemset(s->d_err, 0, sizeof(int)));
   if (ndim == 2) CKC(cudaMemset(s->d_shock0, 0, sh > 0 ? sh : 1));

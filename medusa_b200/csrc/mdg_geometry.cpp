@@ -15,6 +15,7 @@
 #include <cstring>
 #include <vector>
 #include "mdg_internal.h"
+#include "mdg_tables.cuh"
 #include "../../include/medusa_b200.h"
 
 namespace mdg {
@@ -111,26 +112,8 @@ void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t 
     // zone edges as prim_to_fluxesN forms them: startx + index*dx (step.c:509,736)
     double xl = d.startx[dir] + i * d.dx[dir];
     double xr = d.startx[dir] + (i + 1) * d.dx[dir];
-    double a0b1g2 = am * b0 * gp, a0b2g1 = am * bp * g0, a1b0g2 = a0 * bm * gp;
-    double a1b2g0 = a0 * bp * gm, a2b0g1 = ap * bm * g0, a2b1g0 = ap * b0 * gm;
-    double den1 = 1.0 / (a0b1g2 + a1b2g0 + a2b0g1 - a0b2g1 - a1b0g2 - a2b1g0);
-    double den2 = (xl - xr) * (a0 + g0 * xl * xr - b0 * (xl + xr));
-    den2 = 1.0 / den2;
-    double xm = bm / gm, xp = bp / gp, xc = b0 / g0;
     double v[RC_NFIELDS];
-    v[RC_AM] = am; v[RC_A0] = a0; v[RC_AP] = ap;
-    v[RC_BM] = bm; v[RC_B0] = b0; v[RC_BP] = bp;
-    v[RC_GM] = gm; v[RC_G0] = g0; v[RC_GP] = gp;
-    v[RC_XL] = xl; v[RC_XR] = xr;
-    v[RC_DEN1] = den1; v[RC_DEN2] = den2;
-    v[RC_XLR] = xl - xr;
-    v[RC_XL2] = xl * xl; v[RC_XR2] = xr * xr;
-    v[RC_XMID] = 0.5 * (xl + xr);
-    v[RC_DMR] = a0 + xr * (g0 * xr - 2.0 * b0);
-    v[RC_DML] = a0 + xl * (g0 * xl - 2.0 * b0);
-    v[RC_LSM] = xc - 0.5 * (xl + xm);
-    v[RC_LSP] = 0.5 * (xr + xp) - xc;
-    v[RC_LSC] = xp - xm;
+    rc_fields(am, a0, ap, bm, b0, bp, gm, g0, gp, xl, xr, v);
     for (int f = 0; f < RC_NFIELDS; f++) tab[f * stride + off + i + NG] = v[f];
   }
 }
@@ -257,26 +240,8 @@ void build_recon_table_into(const mdg_problem_desc &d, int dir, double *tab, int
     double gm = ga[im + NG], g0 = ga[i + NG], gp = ga[ip + NG];
     double xl = d.startx[dir] + i * d.dx[dir];
     double xr = d.startx[dir] + (i + 1) * d.dx[dir];
-    double a0b1g2 = am * b0 * gp, a0b2g1 = am * bp * g0, a1b0g2 = a0 * bm * gp;
-    double a1b2g0 = a0 * bp * gm, a2b0g1 = ap * bm * g0, a2b1g0 = ap * b0 * gm;
-    double den1 = 1.0 / (a0b1g2 + a1b2g0 + a2b0g1 - a0b2g1 - a1b0g2 - a2b1g0);
-    double den2 = (xl - xr) * (a0 + g0 * xl * xr - b0 * (xl + xr));
-    den2 = 1.0 / den2;
-    double xm = bm / gm, xp = bp / gp, xc = b0 / g0;
     double v[RC_NFIELDS];
-    v[RC_AM] = am; v[RC_A0] = a0; v[RC_AP] = ap;
-    v[RC_BM] = bm; v[RC_B0] = b0; v[RC_BP] = bp;
-    v[RC_GM] = gm; v[RC_G0] = g0; v[RC_GP] = gp;
-    v[RC_XL] = xl; v[RC_XR] = xr;
-    v[RC_DEN1] = den1; v[RC_DEN2] = den2;
-    v[RC_XLR] = xl - xr;
-    v[RC_XL2] = xl * xl; v[RC_XR2] = xr * xr;
-    v[RC_XMID] = 0.5 * (xl + xr);
-    v[RC_DMR] = a0 + xr * (g0 * xr - 2.0 * b0);
-    v[RC_DML] = a0 + xl * (g0 * xl - 2.0 * b0);
-    v[RC_LSM] = xc - 0.5 * (xl + xm);
-    v[RC_LSP] = 0.5 * (xr + xp) - xc;
-    v[RC_LSC] = xp - xm;
+    rc_fields(am, a0, ap, bm, b0, bp, gm, g0, gp, xl, xr, v);
     for (int f = 0; f < RC_NFIELDS; f++) tab[f * stride + off + i + NG] = v[f];
   }
 }
@@ -299,27 +264,9 @@ void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t s
     double gm = ga[im + NG], g0 = ga[i + NG], gp = ga[ip + NG];
     double xl = d.startx[dir] + i * d.dx[dir];
     double xr = d.startx[dir] + (i + 1) * d.dx[dir];
-    double den1 = 1.0 / (am * b0 * gp + a0 * bp * gm + ap * bm * g0 - am * bp * g0 - a0 * bm * gp - ap * b0 * gm);
-    double kAm = (bp * gm * g0 - gp * b0 * gm) * den1, kAp = (gp * bm * g0 - gp * b0 * gm) * den1;
-    double kBm = -(ap * gm * g0 - gp * a0 * gm) * den1, kBp = -(gp * am * g0 - gp * a0 * gm) * den1;
-    double cl2 = xl * xl - a0 / g0, cl1 = xl - b0 / g0, cr2 = xr * xr - a0 / g0, cr1 = xr - b0 / g0;
-    double den2 = 1.0 / ((xl - xr) * (a0 + g0 * xl * xr - b0 * (xl + xr)));
-    double eAl = (g0 * xr - b0) * den2, eAr = (b0 - g0 * xl) * den2;
-    double eBl = (a0 - g0 * xr * xr) * den2, eBr = (g0 * xl * xl - a0) * den2;
-    double dmr = a0 + xr * (g0 * xr - 2.0 * b0), dml = a0 + xl * (g0 * xl - 2.0 * b0);
-    double v[MX_NFIELDS];
-    v[MX_WLM] = kAm * cl2 + kBm * cl1;
-    v[MX_WLP] = kAp * cl2 + kBp * cl1;
-    v[MX_WRM] = kAm * cr2 + kBm * cr1;
-    v[MX_WRP] = kAp * cr2 + kBp * cr1;
-    v[MX_EAL] = eAl;
-    v[MX_EAR] = eAr;
-    v[MX_EBL] = eBl + 2.0 * xl * eAl;
-    v[MX_EBR] = eBr + 2.0 * xl * eAr;
-    v[MX_DXZ] = xr - xl;
-    v[MX_MR] = (-g0 / dmr) * (cl2 - 2.0 * xr * cl1);
-    v[MX_ML] = (-g0 / dml) * (cr2 - 2.0 * xl * cr1);
-    for (int f = 0; f < MX_NFIELDS; f++) tab[f * stride + off + i + NG] = (float)v[f];
+    float v[MX_NFIELDS];
+    mx_fields(am, a0, ap, bm, b0, bp, gm, g0, gp, xl, xr, v);
+    for (int f = 0; f < MX_NFIELDS; f++) tab[f * stride + off + i + NG] = v[f];
   }
 }
 

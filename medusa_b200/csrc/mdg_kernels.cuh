@@ -63,6 +63,10 @@ void launch_stage1d_mixed(int stage, int nt, int grid, bool use_queue, const Pro
 int mixed_max_ctas_per_sm(int nt);
 void launch_conserved_totals(const ProbDev *probs, int nprob, const Tables &tb, StateSoA s, double *out,
                              cudaStream_t st);
+// Reconstruction, geometry and FP32-weight tables of 1-D problem m, built on the device
+// from closed-form moments (the mixed-precision sweep's tables), at columns geo_off..+n1+3.
+void launch_build_tables_1d(const ProbDev *probs, int m, int n1, double *rc, double *geo, float *mx,
+                            int64_t stride, cudaStream_t st);
 void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st);
 void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
 void launch_reset_time(ProbTime *times, int m, cudaStream_t st);

@@ -10,6 +10,8 @@
 //
 // Device memory is one set of arenas sized at creation from an HBM budget: state (P, PH),
 // the reconstruction and geometry tables and the FP32 weights, all indexed by zone units.
+// The mixed sweep's tables are built on the device at admission (mdg_tables.cu); the FP64
+// sweep's, which must be the reference's Romberg values, in the submitting thread.
 // A request is admitted when a slot and a contiguous range of n1 + 2*NG units are free
 // (first fit, coalescing on release): the HBM footprint is the admission test.  Between
 // rounds of steps_per_round steps the loop admits queued requests (back-filling smaller
@@ -39,7 +41,6 @@ int validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why);
 void make_probdev(const mdg_problem_desc &d, ProbDev &P);
 void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
-void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
 }
 
@@ -104,6 +105,8 @@ struct Request {
   mdg_problem_desc desc{};
   std::vector<double> ic;       // [zone][5]
   std::vector<double> result;   // [zone][5] once finished
+  std::vector<double> rc, geo;  // FP64 sweep: the reference's tables, built at submission
+  int sparse = 0;
   int status = MDG_REQ_QUEUED;
   int err = MDG_OK;
   int slot = -1;
@@ -136,6 +139,8 @@ struct mdg_server {
   StateSoA P{}, PH{};
   Tables tb{};
   ProbTime *h_times = nullptr;   // pinned
+  double *h_ret = nullptr;       // pinned return buffer of finished states
+  size_t ret_cap = 0;
   std::vector<Request *> slots;
   RangeAlloc alloc;
   int64_t units_in_use = 0;
@@ -172,6 +177,7 @@ void free_server(mdg_server *s)
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles); cudaFree(s->d_queue); cudaFree(s->d_err);
   cudaFree(s->d_state); cudaFree(s->d_rc0); cudaFree(s->d_geo); cudaFree(s->d_stage); cudaFree(s->d_mx);
   if (s->h_times) cudaFreeHost(s->h_times);
+  if (s->h_ret) cudaFreeHost(s->h_ret);
   if (s->stream) cudaStreamDestroy(s->stream);
   for (auto &kv : s->reqs) delete kv.second;
 }
@@ -214,53 +220,72 @@ int admit(mdg_server *s, Request *r)
 {
   const mdg_problem_desc &d = r->desc;
   const int64_t w = r->units, seg = r->seg;
-  std::vector<double> rc((size_t)RC_NFIELDS * w, 0.0), geo((size_t)GF_NFIELDS * w, 0.0);
-  build_recon_table(d, 0, rc.data(), w, 0);
-  build_geo_1d(d, geo.data(), w, 0);
   ProbDev P;
   make_probdev(d, P);
   P.cell_off = seg;
   P.geo_off = seg;
-  P.sparse_conn = conn_is_sparse(geo.data(), w, 0, (int)w);
-  const size_t pitch = sizeof(double) * s->units;
-  SCK(cudaMemcpy2DAsync(s->d_rc0 + seg, pitch, rc.data(), sizeof(double) * w, sizeof(double) * w, RC_NFIELDS,
-                        cudaMemcpyHostToDevice, s->stream));
-  SCK(cudaMemcpy2DAsync(s->d_geo + seg, pitch, geo.data(), sizeof(double) * w, sizeof(double) * w, GF_NFIELDS,
-                        cudaMemcpyHostToDevice, s->stream));
-  if (s->cfg.precision == MDG_PREC_MIXED) {
-    std::vector<float> mx((size_t)MX_NFIELDS * w, 0.0f);
-    build_mixed_table(d, 0, mx.data(), w, 0);
-    SCK(cudaMemcpy2DAsync(s->d_mx + seg, sizeof(float) * s->units, mx.data(), sizeof(float) * w, sizeof(float) * w,
-                          MX_NFIELDS, cudaMemcpyHostToDevice, s->stream));
-  }
+  P.sparse_conn = r->sparse;
+  // stream-ordered copies from pageable memory return once the source has been staged,
+  // so nothing here waits for the device
   SCK(cudaMemcpyAsync(s->d_probs + r->slot, &P, sizeof P, cudaMemcpyHostToDevice, s->stream));
+  if (s->cfg.precision == MDG_PREC_MIXED) {
+    launch_build_tables_1d(s->d_probs, r->slot, d.n1, s->d_rc0, s->d_geo, s->d_mx, s->units, s->stream);
+  } else {
+    const size_t pitch = sizeof(double) * s->units;
+    SCK(cudaMemcpy2DAsync(s->d_rc0 + seg, pitch, r->rc.data(), sizeof(double) * w, sizeof(double) * w, RC_NFIELDS,
+                          cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaMemcpy2DAsync(s->d_geo + seg, pitch, r->geo.data(), sizeof(double) * w, sizeof(double) * w,
+                          GF_NFIELDS, cudaMemcpyHostToDevice, s->stream));
+  }
   SCK(cudaMemcpyAsync(s->d_stage, r->ic.data(), sizeof(double) * NPRIM * d.n1, cudaMemcpyHostToDevice, s->stream));
   launch_aos_to_soa(s->d_stage, s->P, seg, d.n1, s->stream);
   launch_reset_time(s->d_times, r->slot, s->stream);
   launch_initial_estimate_one(s->d_probs, s->d_times, r->slot, d.n1, s->tb, s->P, s->stream);
-  // the host sources above are stack/heap buffers: wait before they go out of scope
-  SCK(cudaStreamSynchronize(s->stream));
   SCK(cudaGetLastError());
   return MDG_OK;
 }
 
-int retire(mdg_server *s, Request *r, const ProbTime &T)
+// Retire the finished problems of a round: one strided copy of each state (5 rows of n1
+// doubles) into the pinned return buffer, one wait, then the [zone][5] results.
+int retire_all(mdg_server *s, const std::vector<int> &fin)
 {
-  const int n = r->desc.n1;
-  r->result.resize((size_t)NPRIM * n);
-  launch_soa_to_aos(s->P, r->seg, n, s->d_stage, s->stream);
-  SCK(cudaMemcpyAsync(r->result.data(), s->d_stage, sizeof(double) * NPRIM * n, cudaMemcpyDeviceToHost, s->stream));
+  if (fin.empty()) return MDG_OK;
+  size_t need = 0;
+  for (int k : fin) need += (size_t)NPRIM * s->slots[k]->desc.n1;
+  if (need > s->ret_cap) {
+    if (s->h_ret) cudaFreeHost(s->h_ret);
+    s->h_ret = nullptr;
+    s->ret_cap = 0;
+    SCK(cudaMallocHost(&s->h_ret, sizeof(double) * need));
+    s->ret_cap = need;
+  }
+  size_t off = 0;
+  for (int k : fin) {
+    Request *r = s->slots[k];
+    const int n = r->desc.n1;
+    SCK(cudaMemcpy2DAsync(s->h_ret + off, sizeof(double) * n, s->P.v[0] + r->seg, sizeof(double) * s->units,
+                          sizeof(double) * n, NPRIM, cudaMemcpyDeviceToHost, s->stream));
+    off += (size_t)NPRIM * n;
+  }
   SCK(cudaStreamSynchronize(s->stream));
-  r->t = T.t;
-  r->istep = T.istep;
-  r->err = T.err;
-  r->t_done = Clock::now();
-  s->slots[r->slot] = nullptr;
-  s->alloc.release(r->seg, r->units);
-  s->units_in_use -= r->units;
-  r->slot = -1;
-  s->tiles_dirty = true;
-  {
+  const Clock::time_point now = Clock::now();
+  off = 0;
+  for (int k : fin) {
+    Request *r = s->slots[k];
+    const ProbTime &T = s->h_times[k];
+    const int n = r->desc.n1;
+    r->result.resize((size_t)NPRIM * n);
+    for (int z = 0; z < n; z++)
+      for (int v = 0; v < NPRIM; v++) r->result[(size_t)z * NPRIM + v] = s->h_ret[off + (size_t)v * n + z];
+    off += (size_t)NPRIM * n;
+    r->t = T.t;
+    r->istep = T.istep;
+    r->err = T.err;
+    r->t_done = now;
+    s->slots[k] = nullptr;
+    s->alloc.release(r->seg, r->units);
+    s->units_in_use -= r->units;
+    r->slot = -1;
     std::lock_guard<std::mutex> lk(s->mu);
     r->status = T.err ? MDG_REQ_FAILED : MDG_REQ_DONE;
     if (T.err) s->failed++;
@@ -269,6 +294,7 @@ int retire(mdg_server *s, Request *r, const ProbTime &T)
     s->latency.push_back(seconds(r->t_submit, r->t_done));
     s->wait.push_back(seconds(r->t_submit, r->t_admit));
   }
+  s->tiles_dirty = true;
   s->cv.notify_all();
   return MDG_OK;
 }
@@ -319,7 +345,6 @@ int round_once(mdg_server *s, int *active_out)
       SCK(cudaMemcpyAsync(s->d_tiles, tl.data(), sizeof(Tile) * tl.size(), cudaMemcpyHostToDevice, s->stream));
     WorkQueue q{{0u, 0u}, (int)tl.size(), 0};
     SCK(cudaMemcpyAsync(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, s->stream));
-    SCK(cudaStreamSynchronize(s->stream));
     s->ntiles = (int)tl.size();
     s->tiles_dirty = false;
   }
@@ -357,16 +382,12 @@ int round_once(mdg_server *s, int *active_out)
     s->device_ms += ms;
     s->rounds++;
   }
-  for (int k = 0; k < s->max_probs; k++) {
-    Request *r = s->slots[k];
-    if (!r) continue;
-    const ProbTime &T = s->h_times[k];
-    if (T.done || T.err) {
-      int rc = retire(s, r, T);
-      if (rc != MDG_OK) return rc;
-      active--;
-    }
-  }
+  std::vector<int> fin;
+  for (int k = 0; k < s->max_probs; k++)
+    if (s->slots[k] && (s->h_times[k].done || s->h_times[k].err)) fin.push_back(k);
+  int rc = retire_all(s, fin);
+  if (rc != MDG_OK) return rc;
+  active -= (int)fin.size();
   if (active_out) *active_out = active;
   return MDG_OK;
 }
@@ -492,6 +513,15 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
   r->desc = *desc;
   r->ic.assign(prim, prim + (size_t)NPRIM * desc->n1);
   r->units = desc->n1 + 2 * NG;
+  if (s->cfg.precision == MDG_PREC_FP64) {
+    // the reference's Romberg tables, built here in the submitting thread so that the
+    // request loop does not spend its time on them
+    r->rc.assign((size_t)RC_NFIELDS * r->units, 0.0);
+    r->geo.assign((size_t)GF_NFIELDS * r->units, 0.0);
+    build_recon_table(r->desc, 0, r->rc.data(), r->units, 0);
+    build_geo_1d(r->desc, r->geo.data(), r->units, 0);
+    r->sparse = conn_is_sparse(r->geo.data(), r->units, 0, (int)r->units);
+  }
   r->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(s->mu);
