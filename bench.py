@@ -524,7 +524,7 @@ def run_kh(args, ctx):
     peak, peak_kind = read_peaks()
     b_stage1 = 240.0
     achieved = b_stage1 * ncell / (st["stage1"] / 1e3) / 1e9
-    traffic = read_profile_value("stage2d_kh2048_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
+    traffic = read_profile_value("sweep2d_kh2048_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
     line = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
         "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms / K,

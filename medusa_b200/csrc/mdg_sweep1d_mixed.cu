@@ -252,11 +252,12 @@ __device__ __forceinline__ double dt_source_control_1div(const double *p, const 
 }
 
 // Resident 64-thread-equivalents per SM the register allocation is bounded for (0: none).
-// The kernel waits mostly on global loads (state pencils, FP32 weights); 12 x 64 threads
-// per SM (80 registers, a few spilled bytes on the rare FP64 face path) ran the 2048-problem
-// ensemble 1.23x faster than the unbounded 114-register build (8 x 64 threads per SM).
+// The kernel waits mostly on global loads (state pencils, FP32 weights), so occupancy
+// pays: on the 2048-problem ensemble 16 x 64 threads per SM (64 registers, a few spilled
+// bytes) ran 1.18x faster than 12 x 64 (80 registers) and 1.41x faster than the unbounded
+// 114-register build (8 x 64); 20 x 64 (48 registers) was slower again (spills).
 #ifndef MDG_MIX_MINB64
-#define MDG_MIX_MINB64 12
+#define MDG_MIX_MINB64 16
 #endif
 
 template <int NT, int STAGE>
