@@ -100,6 +100,13 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
  * its time to t=0, istep=0 (main.c:172-176, 180-182). */
 int mdg_upload_state(mdg_solver *s, int prob, const double *prim);
 
+/* mdg_upload_state / mdg_download_state for every problem at once (one copy and a few
+ * launches instead of several per problem): prim holds the problems' states one after
+ * the other in problem order, each [zone][5].  The first call allocates a staging buffer
+ * of the whole state on the device. */
+int mdg_upload_all(mdg_solver *s, const double *prim);
+int mdg_download_all(mdg_solver *s, double *prim);
+
 /* The next time step of every problem as estimate_dt() + main.c:239-251 would produce
  * it; written to dt_out[nprob] (may be NULL).  Idempotent until the next mdg_step. */
 int mdg_estimate_dt(mdg_solver *s, double *dt_out);

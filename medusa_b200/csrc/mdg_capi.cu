@@ -41,6 +41,7 @@ struct mdg_solver {
   int64_t ncell_total = 0;
   unsigned char *d_shock0 = nullptr;
   double *d_stage = nullptr;      // AoS staging buffer, 5 doubles per zone of the largest problem
+  double *d_stage_all = nullptr;  // AoS staging of every problem (mdg_upload_all / mdg_download_all)
   int64_t max_cells = 0;
   int *d_err = nullptr;
   // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
@@ -195,7 +196,7 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles);
   cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
   cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
-  cudaFree(s->d_mx); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals);
+  cudaFree(s->d_mx); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
@@ -381,6 +382,41 @@ int mdg_upload_state(mdg_solver *s, int prob, const double *prim)
   launch_aos_to_soa(s->d_stage, s->P, P.cell_off, n, s->stream);
   launch_reset_time(s->d_times, prob, s->stream);
   launch_initial_estimate_one(s->d_probs, s->d_times, prob, n, s->tb, s->P, s->stream);
+  CK(cudaGetLastError());
+  return MDG_OK;
+}
+
+static int stage_all(mdg_solver *s)
+{
+  if (!s->d_stage_all) CK(cudaMalloc(&s->d_stage_all, sizeof(double) * NPRIM * s->ncell_total));
+  return MDG_OK;
+}
+
+int mdg_upload_all(mdg_solver *s, const double *prim)
+{
+  if (!s || !prim) return fail(MDG_ERR_INVALID, "solver/prim");
+  CK(cudaSetDevice(s->device));
+  int rc = stage_all(s);
+  if (rc != MDG_OK) return rc;
+  CK(cudaMemcpyAsync(s->d_stage_all, prim, sizeof(double) * NPRIM * s->ncell_total, cudaMemcpyHostToDevice,
+                     s->stream));
+  launch_aos_to_soa(s->d_stage_all, s->P, 0, s->ncell_total, s->stream);
+  launch_reset_time_all(s->d_times, s->nprob, s->stream);
+  launch_initial_estimate_all(s->d_probs, s->d_times, s->nprob, s->max_cells, s->tb, s->P, s->stream);
+  CK(cudaGetLastError());
+  return MDG_OK;
+}
+
+int mdg_download_all(mdg_solver *s, double *prim)
+{
+  if (!s || !prim) return fail(MDG_ERR_INVALID, "solver/prim");
+  CK(cudaSetDevice(s->device));
+  int rc = stage_all(s);
+  if (rc != MDG_OK) return rc;
+  launch_soa_to_aos(s->P, 0, s->ncell_total, s->d_stage_all, s->stream);
+  CK(cudaMemcpyAsync(prim, s->d_stage_all, sizeof(double) * NPRIM * s->ncell_total, cudaMemcpyDeviceToHost,
+                     s->stream));
+  CK(cudaStreamSynchronize(s->stream));
   CK(cudaGetLastError());
   return MDG_OK;
 }

@@ -72,6 +72,9 @@ void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
 void launch_reset_time(ProbTime *times, int m, cudaStream_t st);
 void launch_initial_estimate_one(const ProbDev *probs, ProbTime *times, int m, int64_t ncell,
                                  const Tables &tb, StateSoA s, cudaStream_t st);
+void launch_reset_time_all(ProbTime *times, int nprob, cudaStream_t st);
+void launch_initial_estimate_all(const ProbDev *probs, ProbTime *times, int nprob, int64_t max_cells,
+                                 const Tables &tb, StateSoA s, cudaStream_t st);
 void launch_aos_to_soa(const double *aos, StateSoA s, int64_t off, int64_t n, cudaStream_t st);
 void launch_soa_to_aos(StateSoA s, int64_t off, int64_t n, double *aos, cudaStream_t st);
 void launch_eos_aos_m(StateSoA s, const ProbDev *probs, int m, int64_t off, int64_t n, double *aos,

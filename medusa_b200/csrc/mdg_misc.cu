@@ -60,8 +60,9 @@ __global__ void finish_kernel(ProbTime *__restrict__ times, int nprob)
 
 // First estimate_dt() of a problem (step.c:171-187 with firstc): zone terms of the
 // initial state with its own EOS (main.c:180-182 fills sim_eos from sim_p).
-__global__ void initial_estimate_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, int m,
-                                        Tables tb, StateSoA s)
+__device__ __forceinline__ void initial_estimate_block(const ProbDev *__restrict__ probs,
+                                                      ProbTime *__restrict__ times, int m, const Tables &tb,
+                                                      const StateSoA &s)
 {
   __shared__ double sred[32];
   const ProbDev &P = probs[m];
@@ -86,6 +87,34 @@ __global__ void initial_estimate_kernel(const ProbDev *__restrict__ probs, ProbT
     }
   }
   block_min_to(lmin, &times[m].minacc, sred);
+}
+
+__global__ void initial_estimate_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, int m,
+                                        Tables tb, StateSoA s)
+{
+  initial_estimate_block(probs, times, m, tb, s);
+}
+
+// The same for problems m0 .. m0+gridDim.y-1 at once (blocks beyond a problem's zones
+// return as a whole, before any barrier).
+__global__ void initial_estimate_many_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                                             int m0, Tables tb, StateSoA s)
+{
+  const int m = m0 + blockIdx.y;
+  const ProbDev &P = probs[m];
+  if ((int64_t)blockIdx.x * blockDim.x >= (int64_t)P.n1 * P.n2) return;
+  initial_estimate_block(probs, times, m, tb, s);
+}
+
+__global__ void reset_time_all_kernel(ProbTime *times, int nprob)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nprob) return;
+  ProbTime T;
+  T.t = 0.0; T.dt = 0.0; T.dtold = 1.0e100; T.t_bc1 = 0.0; T.t_next = 0.0;
+  T.minacc = dbl_to_ord(1.0e100);
+  T.istep = 0; T.dt_ready = 0; T.done = 0; T.err = 0;
+  times[m] = T;
 }
 
 __global__ void reset_time_kernel(ProbTime *times, int m)
@@ -211,6 +240,21 @@ void launch_initial_estimate_one(const ProbDev *probs, ProbTime *times, int m, i
 {
   const int nb = (int)((ncell + 255) / 256);
   initial_estimate_kernel<<<nb, 256, 0, st>>>(probs, times, m, tb, s);
+}
+
+void launch_reset_time_all(ProbTime *times, int nprob, cudaStream_t st)
+{
+  if (nprob > 0) reset_time_all_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(times, nprob);
+}
+
+void launch_initial_estimate_all(const ProbDev *probs, ProbTime *times, int nprob, int64_t max_cells,
+                                 const Tables &tb, StateSoA s, cudaStream_t st)
+{
+  const unsigned nb = (unsigned)((max_cells + 255) / 256);
+  for (int m0 = 0; m0 < nprob; m0 += 65535) {
+    const int k = (nprob - m0 < 65535) ? nprob - m0 : 65535;
+    initial_estimate_many_kernel<<<dim3(nb, k), 256, 0, st>>>(probs, times, m0, tb, s);
+  }
 }
 
 void launch_aos_to_soa(const double *aos, StateSoA s, int64_t off, int64_t n, cudaStream_t st)

@@ -128,6 +128,8 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     L.mdg_autotune.argtypes = [vp, i, ctypes.POINTER(LaunchConfig), ctypes.POINTER(d)]
     L.mdg_conserved_totals.argtypes = [vp, vp, vp]
+    L.mdg_upload_all.argtypes = [vp, vp]
+    L.mdg_download_all.argtypes = [vp, vp]
     ll = ctypes.c_longlong
     L.mdg_server_create.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
     L.mdg_server_submit.argtypes = [vp, ctypes.POINTER(ProblemDesc), vp, ctypes.POINTER(ll)]
@@ -142,7 +144,7 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     for name in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step", "mdg_download_state",
                  "mdg_get_time", "mdg_get_stream", "mdg_synchronize", "mdg_destroy", "mdg_set_timing",
                  "mdg_get_timers", "mdg_get_launch_config", "mdg_set_launch_config", "mdg_autotune",
-                 "mdg_conserved_totals", "mdg_server_create", "mdg_server_submit", "mdg_server_run",
+                 "mdg_conserved_totals", "mdg_upload_all", "mdg_download_all", "mdg_server_create", "mdg_server_submit", "mdg_server_run",
                  "mdg_server_start", "mdg_server_stop", "mdg_server_poll", "mdg_server_wait", "mdg_server_result",
                  "mdg_server_get_stats", "mdg_server_destroy"):
         getattr(L, name).restype = i
@@ -200,6 +202,25 @@ class Solver:
     def upload_ptr(self, m: int, host_ptr: int):
         """Upload from a raw host pointer (e.g. pinned memory) laid out [zone][5]."""
         _check(library().mdg_upload_state(self._h, m, ctypes.c_void_p(host_ptr)), "mdg_upload_state")
+
+    def upload_all_ptr(self, host_ptr: int):
+        """Upload every problem's state from one host buffer (problems back to back, each
+        [zone][5], e.g. pinned memory)."""
+        _check(library().mdg_upload_all(self._h, ctypes.c_void_p(host_ptr)), "mdg_upload_all")
+
+    def download_all_ptr(self, host_ptr: int):
+        _check(library().mdg_download_all(self._h, ctypes.c_void_p(host_ptr)), "mdg_download_all")
+
+    def download_all(self) -> list:
+        """Every problem's state as a list of [zone][5] arrays."""
+        n = [p.ncell for p in self.problems]
+        buf = np.empty((sum(n), 5))
+        self.download_all_ptr(buf.ctypes.data)
+        out, o = [], 0
+        for k in n:
+            out.append(buf[o:o + k])
+            o += k
+        return out
 
     def estimate_dt(self) -> np.ndarray:
         out = np.zeros(len(self.problems))
