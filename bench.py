@@ -226,8 +226,7 @@ def e2e_run(ctx, make_solver, problems, K, W):
     s = make_solver(upload=False)
     stream = torch.cuda.ExternalStream(s.stream, device=ctx.local)
     row = 5 * 8
-    for m in range(len(problems)):
-        s.upload_ptr(m, h_in.data_ptr() + int(offs[m]) * row)
+    s.upload_all_ptr(h_in.data_ptr())
     s.step(W)
     s.synchronize()
     f0 = torch.cuda.Event(enable_timing=True)
@@ -235,11 +234,9 @@ def e2e_run(ctx, make_solver, problems, K, W):
     ctx.barrier()
     torch.cuda.synchronize()
     f0.record(stream)
-    for m in range(len(problems)):
-        s.upload_ptr(m, h_in.data_ptr() + int(offs[m]) * row)
+    s.upload_all_ptr(h_in.data_ptr())     # every problem's state in one copy
     s.step(K)
-    for m in range(len(problems)):
-        s.download_ptr(m, h_out.data_ptr() + int(offs[m]) * row)
+    s.download_all_ptr(h_out.data_ptr())
     f1.record(stream)
     f1.synchronize()
     ctx.barrier()

@@ -85,6 +85,8 @@ typedef struct mdg_problem_desc {
   int hydro_interp_order;   /* 1, 2 (linear) or 3 (parabolic) */
   int enforce_floors;       /* the ENFORCE_FLOORS build switch (fluid.c:43-46): 0 or 1 */
   double rho_floor, e_floor;/* floors set by the problem hook (io.c:5081-5082 defaults -1) */
+  double grav[3];           /* fixed contravariant gravitational acceleration g0 (the GRAV=FIXED_GRAV
+                               build, gravity.c:38-64; init_rt.c:57-59); all zero: NO_GRAV */
 } mdg_problem_desc;
 
 typedef struct mdg_solver mdg_solver;   /* opaque */

@@ -183,6 +183,8 @@ void mdg::make_probdev(const mdg_problem_desc &d, ProbDev &P)
   P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
   P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
   P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
+  P.grav[0] = d.grav[0]; P.grav[1] = d.grav[1]; P.grav[2] = d.grav[2];
+  P.grav_on = (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0);
   P.x0 = d.startx[0];
   if (d.ndim == 1 && d.geom == MDG_SPHERICAL) spherical_1d_constants(P.gk_area, P.gk_th1, P.gk_th2, P.gk_tc);
 }

@@ -329,6 +329,22 @@ __device__ __forceinline__ void u_to_p(double *u, double *p, double gc0, double 
   }
 }
 
+// fixed_gravity (gravity.c:38-64) added to the sources of a zone: src[ETOT] += rho
+// geom_dot(v, g0, gcov) (geometry.c:65-73, over all three components) and
+// src[P1+d] += rho g0[d] gcov[d] for the grid's directions d < ndim.
+__device__ __forceinline__ void add_fixed_gravity(const double *p, const double *g, double gc0, double gc1,
+                                                  double gc2, int ndim, double *src)
+{
+  double vsq = 0.0;
+  vsq += p[U1] * g[0] * gc0;
+  vsq += p[U2] * g[1] * gc1;
+  vsq += p[U3] * g[2] * gc2;
+  src[UU] += p[RHO] * vsq;
+  src[U1] += p[RHO] * g[0] * gc0;
+  if (ndim > 1) src[U2] += p[RHO] * g[1] * gc1;
+  if (ndim > 2) src[U3] += p[RHO] * g[2] * gc2;
+}
+
 // dt_source_control (step.c:205-223)
 __device__ __forceinline__ double dt_source_control(const double *p, const double *u, const double *s)
 {

@@ -76,6 +76,7 @@ struct ProbDev {
   int has_src;              // spherical: geometric source terms are computed
   int sparse_conn;          // 1-D: only the 9 connection coefficients of SPARSE_CONN are non-zero
   int floors;               // ENFORCE_FLOORS: u_to_p clamps rho and u to the floors below
+  int grav_on;              // GRAV=FIXED_GRAV: the fixed acceleration grav[] is applied
   int64_t cell_off;         // first zone of this problem in the state arrays
   int64_t geo_off;          // first record (i=-NG) in the 1-D geometry tables
   int64_t rc1_off;          // first record (j=-NG) of the direction-1 recon table (2-D)
@@ -85,6 +86,7 @@ struct ProbDev {
   double area0, area1, vol; // Cartesian 2-D constants
   double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
   double rho_floor, e_floor;
+  double grav[3];           // contravariant g0
   // 1-D geometry in closed form (mixed-precision sweep): lower edge of zone 0 and the
   // angular integrals of the 1-D spherical metric (spherical_1d_constants)
   double x0, gk_area, gk_th1, gk_th2, gk_tc;

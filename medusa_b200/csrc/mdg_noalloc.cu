@@ -146,6 +146,8 @@ extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double
   P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
   P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
   P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
+  P.grav[0] = d.grav[0]; P.grav[1] = d.grav[1]; P.grav[2] = d.grav[2];
+  P.grav_on = (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0);
   const int64_t ncol = n1 + 2 * NG;
   build_recon_table_into(d, 0, h_rc, ncol, 0, h_al, h_be, h_ga);
   build_geo_1d(d, h_geo, ncol, 0);

@@ -121,9 +121,10 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
     }
+    if (P.grav_on) add_fixed_gravity(ph, P.grav, gc0, gc1, gc2, 1, src);
     p_to_u(pn, u, gc0, gc1, gc2);
     p_to_u(ph, uh, gc0, gc1, gc2);
-    if (P.has_src) lmin = tmin(lmin, dt_source_control(pn, u, src));
+    if (P.has_src || P.grav_on) lmin = tmin(lmin, dt_source_control(pn, u, src));
     else nmin = tmin(nmin, src_dt_numerator_min(pn, u));   // zero sources: shared denominator
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) { divF[v] = 0.0; divF[v] += sfl[v][t + 1]; divF[v] -= sfl[v][t]; }

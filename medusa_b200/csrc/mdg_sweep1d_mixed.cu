@@ -383,6 +383,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
 #pragma unroll
         for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
       }
+      if (P.grav_on) add_fixed_gravity(ph, P.grav, 1.0, zg.g1, zg.g2, 1, src);
       p_to_u(pn, u, 1.0, zg.g1, zg.g2);
       p_to_u(ph, uh, 1.0, zg.g1, zg.g2);
       lmin = dt_source_control_1div(pn, u, src);

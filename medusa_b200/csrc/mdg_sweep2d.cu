@@ -257,6 +257,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   const int iend = min(tile.i0 + TIY2, n1);
   double smax = 0.0;      // max |signal speed| of this thread's faces
   double nmin = 1.0e300;  // min numerator of the source-term limits (zero sources)
+  double lsrc = 1.0e300;  // min source-term limit (fixed gravity)
   double lmax = 0.0;      // max local_dt of the next estimate_dt's zone terms
   {
     const int jc = jx < -1 ? -1 : (jx > n2 ? n2 : jx);
@@ -332,7 +333,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     // push() of zone (r, jx), step.c:380-470 (Cartesian: no sources, unit metric)
     if (out_col) {
       double ph[NPRIM], u[NPRIM], uh[NPRIM], pf[NPRIM];
-      const double src[NPRIM] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      double src[NPRIM] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) ph[v] = sv[v][t + 1];
       if (STAGE == 0) {
@@ -341,7 +342,13 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       }
       p_to_u(pn, u, 1.0, 1.0, 1.0);
       p_to_u(ph, uh, 1.0, 1.0, 1.0);
-      nmin = tmin(nmin, src_dt_numerator_min(pn, u));   // dt_source_control, step.c:393
+      if (P.grav_on) {
+        // sources of the stage state: fixed gravity (the Cartesian geometric ones are 0)
+        add_fixed_gravity(ph, P.grav, 1.0, 1.0, 1.0, 2, src);
+        lsrc = tmin(lsrc, dt_source_control(pn, u, src));
+      } else {
+        nmin = tmin(nmin, src_dt_numerator_min(pn, u));   // dt_source_control, step.c:393
+      }
       const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) {
@@ -368,6 +375,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     }
   }
   double lmin = tmin(1 * P.dx1 / smax, src_dt_from_numerator(nmin));
+  lmin = tmin(lmin, lsrc);
   if (STAGE == 1) lmin = tmin(lmin, 1.0 / lmax);
   block_min_to(lmin, &times[tile.prob].minacc, sred);
 }

@@ -69,6 +69,7 @@ class Problem:
     enforce_floors: int = 0       # ENFORCE_FLOORS build switch (fluid.c:43-46)
     rho_floor: float = -1.0       # io.c:5082 default; problem hooks set their own
     e_floor: float = -1.0         # io.c:5081
+    grav: tuple = (0.0, 0.0, 0.0) # fixed gravitational acceleration g0 (GRAV=FIXED_GRAV when non-zero)
     nsteps: Optional[int] = None  # fixed step count for the workload, if any
 
     @property
@@ -145,6 +146,36 @@ def double_rarefaction(n1: int = 256, v: float = 2.0, cfl: float = 0.8, tmax: fl
                    startx=(0.0, 0.0, 0.0), dx=(dx, 1.0, 1.0), gam=gam, ic=ic,
                    bc_lo=(OUTFLOW,) * 3, bc_hi=(OUTFLOW,) * 3, cfl=cfl, tmax=tmax,
                    enforce_floors=1, rho_floor=rho_floor, e_floor=e_floor)
+
+
+def rayleigh_taylor_2d(n1: int = 128, n2: Optional[int] = None, g: float = -0.1, seed: int = 20240602,
+                       noise: float = 0.01, cfl: float = 0.8, nsteps: Optional[int] = None,
+                       tmax: float = 1.0e100) -> Problem:
+    """2-D Rayleigh-Taylor with fixed gravity (the structure of problems/init_rt.c:26-125,
+    GRAV=FIXED_GRAV): box [0, 0.5] x [0, 1], periodic in x and reflecting in y, heavy fluid
+    (rho 2) over light (rho 1) at y = 0.5, hydrostatic pressure from p = 10/7 + 1/4 at
+    y = 0 under g = (0, g), gamma = 1.4; the interface is seeded with velocity noise of
+    amplitude `noise` in v_y (uniform in [-noise, noise], splitmix64 on `seed`)."""
+    n2 = 2 * n1 if n2 is None else n2
+    gam = 1.4
+    dx0, dx1 = 0.5 / n1, 1.0 / n2
+    x = (np.arange(n1) + 0.5) * dx0
+    y = (np.arange(n2) + 0.5) * dx1
+    X, Y = np.meshgrid(x, y, indexing="ij")
+    rhotop, rhobot, pbase = 2.0, 1.0, 10.0 / 7.0 + 1.0 / 4.0
+    top = Y >= 0.5
+    rho = np.where(top, rhotop, rhobot)
+    p = np.where(top, pbase + rhobot * g * 0.5 + rhotop * g * (Y - 0.5), pbase + rhobot * g * Y)
+    u = uniform01(seed, n1 * n2).reshape(n1, n2)
+    vy = noise * (2.0 * u - 1.0) * np.exp(-((Y - 0.5) / 0.05) ** 2)
+    ic = np.zeros((n1 * n2, NPRIM))
+    ic[:, 0] = rho.ravel()
+    ic[:, 1] = (p / (gam - 1.0)).ravel()
+    ic[:, 3] = vy.ravel()
+    return Problem(name="rt2d_%dx%d" % (n1, n2), ndim=2, geom=CARTESIAN, n=(n1, n2, 1),
+                   startx=(0.0, 0.0, 0.0), dx=(dx0, dx1, 1.0), gam=gam, ic=ic,
+                   bc_lo=(PERIODIC, REFLECT, PERIODIC), bc_hi=(PERIODIC, REFLECT, PERIODIC),
+                   cfl=cfl, nsteps=nsteps, tmax=tmax, grav=(0.0, g, 0.0))
 
 
 def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240601,

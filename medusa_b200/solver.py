@@ -77,7 +77,8 @@ class ProblemDesc(ctypes.Structure):
                 ("dt_grow_safety", ctypes.c_double), ("initial_dt", ctypes.c_double),
                 ("dtmax", ctypes.c_double), ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
                 ("hydro_interp_order", ctypes.c_int),
-                ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double), ("e_floor", ctypes.c_double)]
+                ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double), ("e_floor", ctypes.c_double),
+                ("grav", ctypes.c_double * 3)]
 
 
 def desc_of(pb: "_pb.Problem") -> ProblemDesc:
@@ -94,6 +95,8 @@ def desc_of(pb: "_pb.Problem") -> ProblemDesc:
     d.initial_dt, d.dtmax, d.dtmin, d.tmax = pb.initial_dt, pb.dtmax, pb.dtmin, pb.tmax
     d.hydro_interp_order = pb.hydro_interp_order
     d.enforce_floors, d.rho_floor, d.e_floor = int(pb.enforce_floors), pb.rho_floor, pb.e_floor
+    for k in range(3):
+        d.grav[k] = pb.grav[k]
     return d
 
 

@@ -61,6 +61,15 @@ CONFIGS = {
                           RCOORD="UNIFORM", THCOORD="UNIFORM", ENFORCE_FLOORS="TRUE"),
     "sph1d_floors": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
                          RCOORD="UNIFORM", THCOORD="UNIFORM", ENFORCE_FLOORS="TRUE"),
+    # 2-D Cartesian with the fixed gravitational acceleration of GRAV=FIXED_GRAV
+    # (Rayleigh-Taylor, problems/init_rt.c; setups/rt_2d.mk)
+    "cart2d_grav": dict(NDIM="2", GEOM="CARTESIAN", DENDRITIC_GRID="FALSE",
+                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
+    # the same acceleration on 1-D Cartesian and spherical grids
+    "cart1d_grav": dict(NDIM="1", GEOM="CARTESIAN", DENDRITIC_GRID="FALSE",
+                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
+    "sph1d_grav": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                       RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
 }
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]
@@ -89,6 +98,8 @@ def build_config(name, cfg, ref_root, force=False):
     os.makedirs(cdir, exist_ok=True)
     write_build_h(os.path.join(cdir, "build.h"), defs)
     srcs = [os.path.join(ref_root, s) for s in REF_SOURCES]
+    if defs["GRAV"] != "NO_GRAV":
+        srcs.append(os.path.join(ref_root, "gravity.c"))
     if defs["GEOM"] == "SPHERICAL":
         srcs.append(os.path.join(ref_root, "metrics", "metric_spherical_general.c"))
     else:

@@ -91,6 +91,7 @@ typedef struct {
   int hydro_interp_order;
   int enforce_floors;
   double rho_floor, e_floor;
+  double grav[3];
 } orc_params;
 
 typedef struct {
@@ -117,6 +118,7 @@ typedef struct {
   int istep;
   int interp_order;
   int est_first;
+  int grav_on;            /* GRAV=FIXED_GRAV: a non-zero fixed acceleration */
 } orc_t;
 
 static inline int C(const orc_t *o, int i, int j) { return (i+NG)*o->s2 + (o->ndim > 1 ? j+NG : j); }
@@ -744,16 +746,24 @@ static void geom_src(const orc_t *o, double *const *p)
     for (int j=0; j<jh; j++) {
       int c = C(o,i,j), v, l, m, n;
       for (v=0; v<NPRIM; v++) o->src[v][c] = 0;
-      if (o->geom != 1) continue;
       const orc_geom *g = &o->g[c];
-      double T[3][3], vcov[3];
-      for (l=0; l<3; l++) vcov[l] = g->gcov[0][l]*p[U1+l][c];
-      for (l=0; l<3; l++) {
-        for (m=0; m<3; m++) T[l][m] = p[RHO][c]*p[U1+m][c]*vcov[l];
-        T[l][l] += o->eos[PRESS][c];
+      if (o->geom == 1) {
+        double T[3][3], vcov[3];
+        for (l=0; l<3; l++) vcov[l] = g->gcov[0][l]*p[U1+l][c];
+        for (l=0; l<3; l++) {
+          for (m=0; m<3; m++) T[l][m] = p[RHO][c]*p[U1+m][c]*vcov[l];
+          T[l][l] += o->eos[PRESS][c];
+        }
+        for (l=0; l<3; l++) for (m=0; m<3; m++) for (n=0; n<3; n++)
+          o->src[U1+m][c] += T[l][n]*g->conn[l][m][n];
       }
-      for (l=0; l<3; l++) for (m=0; m<3; m++) for (n=0; n<3; n++)
-        o->src[U1+m][c] += T[l][n]*g->conn[l][m][n];
+      if (o->grav_on) {
+        /* fixed_gravity (gravity.c:38-64): g0 is contravariant; geom_dot (geometry.c:65-73) */
+        double vsq = 0.0;
+        for (l=0; l<3; l++) vsq += p[U1+l][c]*o->prm.grav[l]*g->gcov[0][l];
+        o->src[UU][c] += p[RHO][c]*vsq;
+        for (l=0; l<o->ndim; l++) o->src[U1+l][c] += p[RHO][c]*o->prm.grav[l]*g->gcov[0][l];
+      }
     }
   }
 }
@@ -934,6 +944,7 @@ orc_t *orc_create(const orc_params *prm, int ndim, int geom, const double *ic)
   o->beta1 = calloc(o->n2 + 2*NG, sizeof(double));
   o->Gamma1 = calloc(o->n2 + 2*NG, sizeof(double));
   o->interp_order = prm->hydro_interp_order;
+  o->grav_on = (prm->grav[0] != 0.0 || prm->grav[1] != 0.0 || prm->grav[2] != 0.0);
   o->est_first = 1;
   o->dtold = 1.0e100;
   init_geometry(o);

@@ -40,7 +40,7 @@ class Params(ctypes.Structure):
                 ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
                 ("rtrans", ctypes.c_double), ("hydro_interp_order", ctypes.c_int),
                 ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double),
-                ("e_floor", ctypes.c_double)]
+                ("e_floor", ctypes.c_double), ("grav", ctypes.c_double * 3)]
 
 
 def params_of(pb) -> Params:
@@ -60,6 +60,8 @@ def params_of(pb) -> Params:
     p.enforce_floors = int(getattr(pb, "enforce_floors", 0))
     p.rho_floor = getattr(pb, "rho_floor", -1.0)
     p.e_floor = getattr(pb, "e_floor", -1.0)
+    for d in range(3):
+        p.grav[d] = getattr(pb, "grav", (0.0, 0.0, 0.0))[d]
     return p
 
 
@@ -162,6 +164,8 @@ def ref_config(pb) -> str:
     """The oracle/_ref build of a problem: its geometry and dimension, and whether the
     ENFORCE_FLOORS switch is compiled in."""
     name = ("cart%dd" if pb.geom == 0 else "sph%dd") % pb.ndim
+    if any(g != 0.0 for g in getattr(pb, "grav", (0.0, 0.0, 0.0))):
+        name += "_grav"
     return name + ("_floors" if getattr(pb, "enforce_floors", 0) else "")
 
 

@@ -44,6 +44,7 @@ typedef struct {
   int hydro_interp_order;
   int enforce_floors;  /* must match the ENFORCE_FLOORS of the build */
   double rho_floor, e_floor;
+  double grav[3];     /* fixed gravitational acceleration g0 (GRAV=FIXED_GRAV builds) */
 } ref_params;
 
 static ref_params g_prm;
@@ -172,6 +173,9 @@ REF_API int ref_init(const ref_params *prm, const double *ic)
   tmax = prm->tmax;
   ncomp = 0;
   hydro_interp_order = prm->hydro_interp_order;
+#if (GRAV == FIXED_GRAV)
+  g0[0] = prm->grav[0]; g0[1] = prm->grav[1]; g0[2] = prm->grav[2];   /* init_rt.c:57-59 */
+#endif
   if (prm->enforce_floors != (ENFORCE_FLOORS == TRUE)) {
     fprintf(stderr, "ref_harness: enforce_floors=%d but this build has ENFORCE_FLOORS=%d\n",
             prm->enforce_floors, (int)(ENFORCE_FLOORS == TRUE));

@@ -34,6 +34,7 @@ typedef struct {
   int hydro_interp_order;
   int enforce_floors;
   double rho_floor, e_floor;
+  double grav[3];
 } ref_params;
 
 int ref_init(const ref_params *prm, const double *ic);

@@ -36,6 +36,7 @@ def cases():
         "kh2d_48x40": (P.kelvin_helmholtz(48, 40, seed=11), 25),
         "blast2d_40x48_reflect": (P.blast_2d(40, 48, bc=P.REFLECT), 40),
         "blast2d_44x36_outflow": (P.blast_2d(44, 36, bc=P.OUTFLOW), 40),
+        "rt2d_32x64_grav": (P.rayleigh_taylor_2d(32, 64, g=-0.5, noise=0.05), 40),
     }
 
 

@@ -36,6 +36,7 @@ def _cases():
         "sph_noh_256": (P.spherical_1d("noh", 256, 5.0 / 3.0), 300),
         "sph_sedov_256": (P.spherical_1d("sedov", 256, 1.4, p_ratio=1.0e4, r0=0.05), 200),
         "sph_sod_384_g43": (P.spherical_1d("sod", 384, 4.0 / 3.0, rho_ratio=50.0, p_ratio=3.0e3), 250),
+        "grav_sod1d_512": (P.sod(512, tmax=0.2).copy(grav=(-0.8, 0.0, 0.0), name="grav_sod1d_512"), 200),
     }
 
 

@@ -19,6 +19,9 @@ def _cases():
     out.append(P.blast_2d(30, 24, bc=P.OUTFLOW).copy(bc_lo=(P.EXTRAP, P.OUTFLOW, 0), bc_hi=(P.EXTRAP, P.REFLECT, 0)))
     out.append(P.kelvin_helmholtz(32, 24, seed=3))
     out.append(P.double_rarefaction(150, v=6.0, rho_floor=1.0e-2, e_floor=5.0e-3))
+    out.append(P.rayleigh_taylor_2d(24, 40, g=-0.3, noise=0.05))
+    out.append(P.sod(160).copy(grav=(-0.9, 0.0, 0.0), name="sod_grav"))
+    out.append(P.spherical_1d("sod", 120, 1.4).copy(grav=(-0.4, 0.0, 0.0), name="sph_sod_grav"))
     return out
 
 
