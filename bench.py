@@ -265,12 +265,13 @@ def cpu_baseline_kh(pb_full, steps=2):
             "sample": "1 RK2 step of the %dx%d grid, CPU oracle, 1 core, %.1f s" % (NX, NX, el)}
 
 
-def cpu_baseline_ensemble(problems, every=8, steps=50, warm=2):
+def cpu_baseline_ensemble(problems, every=8, steps=50, warm=2, zu_cap=2.0e6):
     """The reference CPU build on every `every`-th problem of the ensemble, `steps` timed
-    RK2 steps each, as independent single-threaded processes over all host cores (the
-    reference has no host threading on this path; problem-parallel is its best use of
-    the host).  Rate = timed zone-updates / (summed timed seconds / processes), i.e.
-    perfect packing of the processes (the reference's best case)."""
+    RK2 steps each (fewer for large 2-D grids: at most zu_cap zone-updates, at least 2
+    steps), as independent single-threaded processes over all host cores (the reference
+    has no host threading on this path; problem-parallel is its best use of the host).
+    Rate = timed zone-updates / (summed timed seconds / processes), i.e. perfect packing
+    of the processes (the reference's best case)."""
     from concurrent.futures import ThreadPoolExecutor
 
     from oracle import pyoracle
@@ -280,17 +281,18 @@ def cpu_baseline_ensemble(problems, every=8, steps=50, warm=2):
         kind = "reference"
 
         def job(pb):
-            r = pyoracle.time_reference(pb, warm, steps, fast=True)
+            r = pyoracle.time_reference(pb, warm, max(2, min(steps, int(zu_cap / pb.ncell))), fast=True)
             return r["cells"] * r["steps"], r["seconds"]
     else:
         kind = "port"
 
         def job(pb):
+            n = max(2, min(steps, int(zu_cap / pb.ncell)))
             o = pyoracle.Oracle(pb)
             o.advance(warm)
             t0 = time.perf_counter()
-            o.advance(steps)
-            return pb.ncell * steps, time.perf_counter() - t0
+            o.advance(n)
+            return pb.ncell * n, time.perf_counter() - t0
     t0 = time.perf_counter()
     with ThreadPoolExecutor(max_workers=procs) as ex:
         res = list(ex.map(job, sample))
@@ -298,9 +300,10 @@ def cpu_baseline_ensemble(problems, every=8, steps=50, warm=2):
     zu = sum(r[0] for r in res)
     busy = sum(r[1] for r in res)
     return {"value": zu / (busy / procs), "unit": "zone-updates/s", "cores": procs, "kind": kind,
-            "sample": "%d of the %d problems (every %dth), %d timed RK2 steps each after %d warm-up, "
+            "sample": "%d of the %d problems (every %dth), %d timed RK2 steps each (at most %.0e zone-updates) "
+                      "after %d warm-up, "
                       "%d concurrent single-threaded processes, %s build%s; %.1f s wall"
-                      % (len(sample), len(problems), every, steps, warm, procs, kind,
+                      % (len(sample), len(problems), every, steps, zu_cap, warm, procs, kind,
                          " with its own flags (-O3 -ffast-math)" if kind == "reference" else "", wall)}
 
 
@@ -316,9 +319,9 @@ def run_reference_arm(args, ctx):
         dtype = "f64"
     elif args.workload == "server":
         from medusa_b200 import loadgen
-        probs = loadgen.request_stream(args.server_requests, seed=11)
+        probs = loadgen.request_stream(args.server_requests, seed=11, frac_2d=args.server_frac_2d)
         cb = cpu_baseline_ensemble(probs)
-        config = {"workload": "server_stream_1d_spherical_256_8192_zones", "requests": len(probs)}
+        config = {"workload": server_workload_name(args), "requests": len(probs)}
         dtype = "f64"
     else:
         probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED)
@@ -549,23 +552,34 @@ def run_kh(args, ctx):
     print(json.dumps(line), flush=True)
 
 
+def server_workload_name(args):
+    if args.server_frac_2d > 0.0:
+        return "server_stream_1d_spherical_256_8192_and_%d%%_2d_cartesian_128sq_1024sq" % round(
+            100 * args.server_frac_2d)
+    return "server_stream_1d_spherical_256_8192_zones"
+
+
 def run_server(args, ctx):
-    """Solve-server stream: seeded 1-D spherical requests (Sod/Noh/Sedov, 256-8192 zones,
-    each to its end time) submitted with Poisson arrivals at a swept rate to a running
-    server, mixed precision and plain FP64; throughput and p50/p99 time-to-solution."""
+    """Solve-server stream: seeded 1-D spherical requests (Sod/Noh/Sedov, 256-8192 zones)
+    and, with --server-frac-2d, 2-D Cartesian ones (Kelvin-Helmholtz / Rayleigh-Taylor,
+    128^2-1024^2 zones), each to its end time, submitted with Poisson arrivals at a swept
+    rate to a running server, mixed precision and plain FP64; throughput and p50/p99
+    time-to-solution."""
     import math
     from medusa_b200 import loadgen
     from medusa_b200.solver import PREC_FP64, PREC_MIXED, Server
 
     rates = [float(r) for r in args.server_rates.split(",")]
-    reqs = loadgen.request_stream(args.server_requests, seed=11 + ctx.rank)
+    reqs = loadgen.request_stream(args.server_requests, seed=11 + ctx.rank, frac_2d=args.server_frac_2d)
     spr = 20
     sweep = {}
     best = {}
+    two_d = args.server_frac_2d > 0.0
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64)):
         sweep[name] = []
         srv = Server(precision=prec, device=ctx.local, hbm_bytes=24 << 30, max_problems=16384, max_zones=8192,
-                     steps_per_round=spr, threads=64, ctas_per_sm=12)
+                     steps_per_round=spr, threads=64, ctas_per_sm=12,
+                     hbm_bytes_2d=(32 << 30) if two_d else 0, max_cells_2d=(1 << 20) + 4096)
         srv.start()
         # warm-up: graph capture and first admissions
         loadgen.drive(srv, reqs[:32], math.inf)
@@ -580,6 +594,7 @@ def run_server(args, ctx):
         best[name] = max(sweep[name], key=lambda r: r["zone_updates_per_s"])
         best[name]["device_seconds_total"] = st["device_seconds"]
         best[name]["rounds_total"] = st["rounds"]
+        best[name]["kernel_launches_total"] = st["kernel_launches"]
     if ctx.rank != 0:
         return
     peak, peak_kind = read_peaks()
@@ -591,15 +606,18 @@ def run_server(args, ctx):
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": ctx.world,
         "steps": spr, "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-        "config": {"workload": "server_stream_1d_spherical_256_8192_zones",
+        "config": {"workload": server_workload_name(args),
                    "requests": len(reqs), "rates_req_per_s": args.server_rates,
-                   "mix": "1-D spherical Sod/Noh/Sedov to their end times (the 1-D part of the request mix)",
+                   "mix": ("1-D spherical Sod/Noh/Sedov and %d%% 2-D Cartesian KH/RT (FP64 split sweep in both "
+                           "server precisions) to their end times; the 3-D share is left out (no 3-D sweep)"
+                           % round(100 * args.server_frac_2d)) if two_d else
+                          "1-D spherical Sod/Noh/Sedov to their end times (the 1-D part of the request mix)",
                    "steps_per_round": spr, "parallelism": "single" if ctx.world == 1 else "independent servers"},
         "p50_s": m["latency_p50_s"], "p99_s": m["latency_p99_s"],
         "sweep": sweep,
         "fp64_best_zone_updates_per_s": best["fp64"]["zone_updates_per_s"],
         "mixed_over_fp64": m["zone_updates_per_s"] / best["fp64"]["zone_updates_per_s"],
-        "gpu_launches": 4 * spr * m["rounds_total"],
+        "gpu_launches": m["kernel_launches_total"],
         "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / max(1, m["rounds_total"]),
                 "d2h_bytes_per_step": h2d / max(1, m["rounds_total"]),
                 "timed": "submission of every request from host memory to the return of every final state"},
@@ -621,6 +639,9 @@ def main():
     ap.add_argument("--server-requests", type=int, default=6000)
     ap.add_argument("--server-rates", default="1000,4000,16000,inf",
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
+    ap.add_argument("--server-frac-2d", type=float, default=0.0,
+                    help="server: fraction of 2-D Cartesian requests (0.263 = the 70:25 share of 1-D and 2-D "
+                         "requests of the mixed stream)")
     ap.add_argument("--server-seconds", type=float, default=3.0,
                     help="server: length of the arrival window at each finite rate")
     ap.add_argument("--no-cpu-baseline", action="store_true")

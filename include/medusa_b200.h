@@ -212,18 +212,22 @@ int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double *prim_in, 
 
 /*
  * Solve server.  No counterpart in the reference, whose executable advances one problem
- * per process.  A server keeps 1-D problems resident on one GPU and advances every
- * admitted problem together, batching their uneven grids into the same stage launches
- * (for MDG_PREC_MIXED: persistent CTAs fed from a device work queue, each round of
- * steps_per_round steps replayed from one CUDA graph).  A request is a problem
- * description, its initial state ([zone][5], as mdg_upload_state) and its end time
- * desc->tmax; it runs the main.c time loop until t >= tmax and is then retired.
+ * per process.  A server keeps 1-D and 2-D problems resident on one GPU and advances
+ * every admitted problem together, batching their uneven grids into the same stage
+ * launches (1-D, for MDG_PREC_MIXED: persistent CTAs fed from a device work queue, each
+ * round of steps_per_round steps replayed from one CUDA graph; 2-D: the plain FP64 split
+ * sweep in either precision, on a second stream that runs beside the 1-D launches).  A
+ * request is a problem description, its initial state ([zone][5], as mdg_upload_state)
+ * and its end time desc->tmax; it runs the main.c time loop until t >= tmax and is then
+ * retired.
  *
- * Admission is by device-memory footprint: the arenas are sized once from hbm_bytes, and
- * a queued request is admitted between rounds when a slot and a contiguous range of
- * n1 + 4 zone units are free (requests that do not fit yet wait; smaller ones behind them
- * may go first).  A finished problem's state is left unchanged by later rounds, so every
- * result is the same whatever else shares the GPU and whenever it is collected.
+ * Admission is by device-memory footprint: the arenas are sized once from hbm_bytes
+ * (1-D states and every request's tables) and hbm_bytes_2d (2-D states), and a queued
+ * request is admitted between rounds when a slot and contiguous ranges of n1 + 4 zone
+ * units (2-D: n1 + n2 + 8 table units and (n1 + 3) x n2 cells) are free (requests that do
+ * not fit yet wait; smaller ones behind them may go first).  A finished problem's state
+ * is left unchanged by later rounds, so every result is the same whatever else shares
+ * the GPU and whenever it is collected.
  *
  * The request loop runs either on a thread of the server (mdg_server_start/stop), while
  * other threads submit, poll and collect, or in the caller's thread (mdg_server_run).
@@ -238,6 +242,8 @@ typedef struct mdg_server_config {
   int steps_per_round;      /* steps between two scheduling points */
   int threads;              /* mixed sweep: threads per CTA, 64, 128 or 256 */
   int ctas_per_sm;          /* mixed sweep: persistent CTAs per SM (0: as many as fit) */
+  long long hbm_bytes_2d;   /* device memory for resident 2-D states (0: 2-D requests refused) */
+  int max_cells_2d;         /* largest n1 x n2 a 2-D request may have */
 } mdg_server_config;
 
 #define MDG_REQ_QUEUED  0
@@ -247,15 +253,16 @@ typedef struct mdg_server_config {
 
 typedef struct mdg_server_stats {
   long long submitted, completed, failed, queued, running, rounds;
-  double zone_updates;      /* sum over finished requests of n1 x steps */
+  double zone_updates;      /* sum over finished requests of zones (n1 or n1 x n2) x steps */
   double device_seconds;    /* device time of the step rounds */
   double latency_p50, latency_p99;   /* seconds from submission to completion */
   double wait_p50, wait_p99;         /* seconds from submission to admission */
   double hbm_capacity, hbm_in_use;   /* bytes of the arenas, bytes held by resident problems */
+  long long kernel_launches;         /* this library's kernels launched (graph replays included) */
 } mdg_server_stats;
 
 int mdg_server_create(const mdg_server_config *cfg, mdg_server **out);
-/* Queue a 1-D request (thread-safe); *id identifies it in the calls below. */
+/* Queue a 1-D or 2-D request (thread-safe); *id identifies it in the calls below. */
 int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double *prim, long long *id);
 /* Run `rounds` scheduling rounds in the calling thread (rounds <= 0: until nothing is
  * queued or running); *active = problems resident after the last round. */

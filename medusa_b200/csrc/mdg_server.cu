@@ -1,5 +1,5 @@
-// Solve server: a request loop that keeps 1-D problems resident on one GPU and advances
-// every admitted problem together (continuous batching).
+// Solve server: a request loop that keeps 1-D and 2-D problems resident on one GPU and
+// advances every admitted problem together (continuous batching).
 //
 // No counterpart in the reference, whose executable advances one problem per process
 // through the main.c time loop (main.c:206-313).  Each request here is such a run: a
@@ -8,17 +8,24 @@
 // untouched (ProbTime::done), so a result does not depend on when it is collected nor on
 // the other problems in the batch.
 //
-// Device memory is one set of arenas sized at creation from an HBM budget: state (P, PH),
-// the reconstruction and geometry tables and the FP32 weights, all indexed by zone units.
-// The mixed sweep's tables are built on the device at admission (mdg_tables.cu); the FP64
-// sweep's, which must be the reference's Romberg values, in the submitting thread.
-// A request is admitted when a slot and a contiguous range of n1 + 2*NG units are free
-// (first fit, coalescing on release): the HBM footprint is the admission test.  Between
-// rounds of steps_per_round steps the loop admits queued requests (back-filling smaller
-// ones when the oldest does not fit), rebuilds the (problem, tile) list, runs the round --
-// for the mixed sweep one CUDA graph of persistent, work-queue fed stage launches, whose
-// arguments never change because the tile count lives in device memory -- and retires
-// the problems that reached their end time.
+// Device memory is two sets of arenas sized at creation from HBM budgets.  The unit arena
+// holds the 1-D states (P, PH), the reconstruction and geometry tables and the FP32
+// weights, all indexed by zone units; 2-D requests keep their two reconstruction tables
+// there too (n1 + 2*NG units of direction 0, then n2 + 2*NG of direction 1).  The cell
+// arena holds the 2-D states (P, PH and the direction-0 accumulator) and the two shock-bit
+// arrays, indexed by cells.  The mixed 1-D sweep's tables are built on the device at
+// admission (mdg_tables.cu); the FP64 sweeps', which must be the reference's Romberg
+// values, in the submitting thread.  A request is admitted when a slot and contiguous
+// ranges of both arenas are free (first fit, coalescing on release): the HBM footprint
+// is the admission test.  Between rounds of steps_per_round steps the loop admits queued
+// requests (back-filling smaller ones when the oldest does not fit), rebuilds the
+// (problem, tile) lists, runs the round and retires the problems that reached their end
+// time.  A round is, per step, the dt reduction, the two RK stages of the 1-D lane on the
+// main stream and of the 2-D lane (plain FP64 split sweep) on a second stream forked
+// from it, and the time update after both lanes joined.  For the mixed 1-D sweep the
+// round is one CUDA graph: the persistent, work-queue fed stage launches never change
+// their arguments because the tile count lives in device memory; the graph is captured
+// again only when the 2-D tile counts change.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <atomic>
@@ -105,12 +112,14 @@ struct Request {
   mdg_problem_desc desc{};
   std::vector<double> ic;       // [zone][5]
   std::vector<double> result;   // [zone][5] once finished
-  std::vector<double> rc, geo;  // FP64 sweep: the reference's tables, built at submission
+  std::vector<double> rc, geo;  // FP64 sweeps: the reference's tables, built at submission
   int sparse = 0;
   int status = MDG_REQ_QUEUED;
   int err = MDG_OK;
   int slot = -1;
-  int64_t seg = -1, units = 0;
+  int64_t seg = -1, units = 0;  // range of the unit arena
+  int64_t seg2 = -1, cells = 0; // range of the cell arena (2-D)
+  int64_t ncell = 0;            // zones of the problem
   double t = 0.0;
   int istep = 0;
   Clock::time_point t_submit, t_admit, t_done;
@@ -146,6 +155,18 @@ struct mdg_server {
   int64_t units_in_use = 0;
   int ntiles = 0;
   bool tiles_dirty = true;
+  // 2-D lane: cell arena, shock bits, tile lists (x tiles then y tiles), second stream
+  int64_t cells = 0;
+  RangeAlloc alloc2;
+  int64_t cells_in_use = 0;
+  double *d_state2 = nullptr;
+  unsigned char *d_shock0 = nullptr, *d_shock1 = nullptr;
+  StateSoA P2{}, PH2{}, ACC2{};
+  Tile *d_tiles2 = nullptr;
+  int tiles2_cap = 0, ntx2 = 0, nty2 = 0;
+  cudaStream_t stream2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  int graph_ntx2 = -1, graph_nty2 = -1;   // 2-D tile counts the graph was captured with
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // requests
@@ -163,6 +184,7 @@ struct mdg_server {
   std::string loop_msg;
   // statistics of finished requests
   long long completed = 0, failed = 0, rounds = 0;
+  std::atomic<long long> launches{0};
   double zone_updates = 0.0, device_ms = 0.0;
   std::vector<double> latency, wait;
 };
@@ -174,10 +196,14 @@ void free_server(mdg_server *s)
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  if (s->ev_join) cudaEventDestroy(s->ev_join);
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles); cudaFree(s->d_queue); cudaFree(s->d_err);
   cudaFree(s->d_state); cudaFree(s->d_rc0); cudaFree(s->d_geo); cudaFree(s->d_stage); cudaFree(s->d_mx);
+  cudaFree(s->d_state2); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_tiles2);
   if (s->h_times) cudaFreeHost(s->h_times);
   if (s->h_ret) cudaFreeHost(s->h_ret);
+  if (s->stream2) cudaStreamDestroy(s->stream2);
   if (s->stream) cudaStreamDestroy(s->stream);
   for (auto &kv : s->reqs) delete kv.second;
 }
@@ -188,6 +214,23 @@ int64_t bytes_per_unit(int precision)
   return 2 * NPRIM * 8 + RC_NFIELDS * 8 + GF_NFIELDS * 8 + (precision == MDG_PREC_MIXED ? MX_NFIELDS * 4 : 0);
 }
 
+// bytes per cell of the 2-D arena: state P, PH and accumulator, two shock bytes
+int64_t bytes_per_cell_2d() { return 3 * NPRIM * 8 + 2; }
+
+// Unit-arena and cell-arena footprints of a request: the 1-D state and tables, or the
+// two 2-D reconstruction tables and the 2-D state with its shock bits ((n1 + 3) x n2
+// bytes each: the face count of set_shock_flag, as in the solver's layout).
+void footprint(const mdg_problem_desc &d, int64_t &units, int64_t &cells)
+{
+  if (d.ndim == 2) {
+    units = (int64_t)d.n1 + 2 * NG + d.n2 + 2 * NG;
+    cells = (int64_t)(d.n1 + 3) * d.n2;
+  } else {
+    units = (int64_t)d.n1 + 2 * NG;
+    cells = 0;
+  }
+}
+
 int persistent_grid(const mdg_server *s)
 {
   int k = mixed_max_ctas_per_sm(s->cfg.threads);
@@ -196,12 +239,17 @@ int persistent_grid(const mdg_server *s)
   return k * s->num_sms;
 }
 
-void queue_round(mdg_server *s, int nsteps)
+int queue_round(mdg_server *s, int nsteps)
 {
   const bool mixed = s->cfg.precision == MDG_PREC_MIXED;
   const int grid = mixed ? persistent_grid(s) : 0;
+  const bool lane2 = s->ntx2 > 0;
   for (int k = 0; k < nsteps; k++) {
     launch_dt_finalize(s->d_probs, s->d_times, s->max_probs, s->d_err, s->stream);
+    if (lane2) {
+      SCK(cudaEventRecord(s->ev_fork, s->stream));
+      SCK(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
+    }
     if (mixed) {
       launch_stage1d_mixed(0, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
                            s->P, s->P, s->PH, s->stream);
@@ -211,8 +259,17 @@ void queue_round(mdg_server *s, int nsteps)
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     }
+    if (lane2) {
+      launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+                     s->P2, s->P2, s->ACC2, s->PH2, s->d_shock0, s->d_shock1, s->stream2);
+      launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+                     s->PH2, s->P2, s->ACC2, s->P2, s->d_shock0, s->d_shock1, s->stream2);
+      SCK(cudaEventRecord(s->ev_join, s->stream2));
+      SCK(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+    }
     launch_finish(s->d_times, s->max_probs, s->stream);
   }
+  return MDG_OK;
 }
 
 // Upload tables, record, state and time of request r into slot r->slot, units r->seg...
@@ -225,9 +282,30 @@ int admit(mdg_server *s, Request *r)
   P.cell_off = seg;
   P.geo_off = seg;
   P.sparse_conn = r->sparse;
+  if (d.ndim == 2) {
+    P.cell_off = r->seg2;
+    P.rc1_off = seg + d.n1 + 2 * NG;
+    P.sh_off = r->seg2;
+  }
   // stream-ordered copies from pageable memory return once the source has been staged,
   // so nothing here waits for the device
   SCK(cudaMemcpyAsync(s->d_probs + r->slot, &P, sizeof P, cudaMemcpyHostToDevice, s->stream));
+  if (d.ndim == 2) {
+    // both reconstruction tables in one copy; the shock bits start zero-filled, as the
+    // reference's calloc'd flag arrays (utils.c:164-174)
+    SCK(cudaMemcpy2DAsync(s->d_rc0 + seg, sizeof(double) * s->units, r->rc.data(), sizeof(double) * w,
+                          sizeof(double) * w, RC_NFIELDS, cudaMemcpyHostToDevice, s->stream));
+    SCK(cudaMemsetAsync(s->d_shock0 + r->seg2, 0, r->cells, s->stream));
+    SCK(cudaMemsetAsync(s->d_shock1 + r->seg2, 0, r->cells, s->stream));
+    SCK(cudaMemcpyAsync(s->d_stage, r->ic.data(), sizeof(double) * NPRIM * r->ncell, cudaMemcpyHostToDevice,
+                        s->stream));
+    launch_aos_to_soa(s->d_stage, s->P2, r->seg2, r->ncell, s->stream);
+    launch_reset_time(s->d_times, r->slot, s->stream);
+    launch_initial_estimate_one(s->d_probs, s->d_times, r->slot, r->ncell, s->tb, s->P2, s->stream);
+    SCK(cudaGetLastError());
+    s->launches += 3;
+    return MDG_OK;
+  }
   if (s->cfg.precision == MDG_PREC_MIXED) {
     launch_build_tables_1d(s->d_probs, r->slot, d.n1, s->d_rc0, s->d_geo, s->d_mx, s->units, s->stream);
   } else {
@@ -242,16 +320,18 @@ int admit(mdg_server *s, Request *r)
   launch_reset_time(s->d_times, r->slot, s->stream);
   launch_initial_estimate_one(s->d_probs, s->d_times, r->slot, d.n1, s->tb, s->P, s->stream);
   SCK(cudaGetLastError());
+  s->launches += (s->cfg.precision == MDG_PREC_MIXED) ? 4 : 3;
   return MDG_OK;
 }
 
-// Retire the finished problems of a round: one strided copy of each state (5 rows of n1
-// doubles) into the pinned return buffer, one wait, then the [zone][5] results.
+// Retire the finished problems of a round: one strided copy of each state (5 rows of
+// n1 or n1 x n2 doubles) into the pinned return buffer, one wait, then the [zone][5]
+// results.
 int retire_all(mdg_server *s, const std::vector<int> &fin)
 {
   if (fin.empty()) return MDG_OK;
   size_t need = 0;
-  for (int k : fin) need += (size_t)NPRIM * s->slots[k]->desc.n1;
+  for (int k : fin) need += (size_t)NPRIM * s->slots[k]->ncell;
   if (need > s->ret_cap) {
     if (s->h_ret) cudaFreeHost(s->h_ret);
     s->h_ret = nullptr;
@@ -262,9 +342,12 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
   size_t off = 0;
   for (int k : fin) {
     Request *r = s->slots[k];
-    const int n = r->desc.n1;
-    SCK(cudaMemcpy2DAsync(s->h_ret + off, sizeof(double) * n, s->P.v[0] + r->seg, sizeof(double) * s->units,
-                          sizeof(double) * n, NPRIM, cudaMemcpyDeviceToHost, s->stream));
+    const int64_t n = r->ncell;
+    const bool two = r->desc.ndim == 2;
+    const double *src = two ? s->P2.v[0] + r->seg2 : s->P.v[0] + r->seg;
+    const size_t pitch = sizeof(double) * (two ? s->cells : s->units);
+    SCK(cudaMemcpy2DAsync(s->h_ret + off, sizeof(double) * n, src, pitch, sizeof(double) * n, NPRIM,
+                          cudaMemcpyDeviceToHost, s->stream));
     off += (size_t)NPRIM * n;
   }
   SCK(cudaStreamSynchronize(s->stream));
@@ -273,9 +356,9 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
   for (int k : fin) {
     Request *r = s->slots[k];
     const ProbTime &T = s->h_times[k];
-    const int n = r->desc.n1;
+    const int64_t n = r->ncell;
     r->result.resize((size_t)NPRIM * n);
-    for (int z = 0; z < n; z++)
+    for (int64_t z = 0; z < n; z++)
       for (int v = 0; v < NPRIM; v++) r->result[(size_t)z * NPRIM + v] = s->h_ret[off + (size_t)v * n + z];
     off += (size_t)NPRIM * n;
     r->t = T.t;
@@ -285,6 +368,10 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
     s->slots[k] = nullptr;
     s->alloc.release(r->seg, r->units);
     s->units_in_use -= r->units;
+    if (r->cells > 0) {
+      s->alloc2.release(r->seg2, r->cells);
+      s->cells_in_use -= r->cells;
+    }
     r->slot = -1;
     std::lock_guard<std::mutex> lk(s->mu);
     r->status = T.err ? MDG_REQ_FAILED : MDG_REQ_DONE;
@@ -316,8 +403,19 @@ int round_once(mdg_server *s, int *active_out)
       if (slot < 0) break;
       const int64_t seg = s->alloc.alloc(r->units);
       if (seg < 0) { ++it; continue; }
+      int64_t seg2 = -1;
+      if (r->cells > 0) {
+        seg2 = s->alloc2.alloc(r->cells);
+        if (seg2 < 0) {
+          s->alloc.release(seg, r->units);
+          ++it;
+          continue;
+        }
+        s->cells_in_use += r->cells;
+      }
       r->slot = slot;
       r->seg = seg;
+      r->seg2 = seg2;
       s->slots[slot] = r;
       s->units_in_use += r->units;
       r->status = MDG_REQ_RUNNING;
@@ -335,10 +433,20 @@ int round_once(mdg_server *s, int *active_out)
   int active = 0;
   for (int k = 0; k < s->max_probs; k++) active += s->slots[k] != nullptr;
   if (s->tiles_dirty) {
-    std::vector<Tile> tl;
+    std::vector<Tile> tl, xt, yt;
     for (int k = 0; k < s->max_probs; k++) {
-      if (!s->slots[k]) continue;
-      for (int i0 = 0; i0 < s->slots[k]->desc.n1; i0 += s->tile_len) tl.push_back(Tile{k, i0, 0, 0});
+      const Request *r = s->slots[k];
+      if (!r) continue;
+      if (r->desc.ndim == 2) {
+        // the solver's 2-D tiling: direction-0 tiles of TIX2 rows x NTX2 columns,
+        // direction-1 tiles of TIY2 rows x TJY2 columns
+        for (int i0 = 0; i0 < r->desc.n1; i0 += TIX2)
+          for (int j0 = 0; j0 < r->desc.n2; j0 += NTX2) xt.push_back(Tile{k, i0, j0, 0});
+        for (int i0 = 0; i0 < r->desc.n1; i0 += TIY2)
+          for (int j0 = 0; j0 < r->desc.n2; j0 += TJY2) yt.push_back(Tile{k, i0, j0, 0});
+      } else {
+        for (int i0 = 0; i0 < r->desc.n1; i0 += s->tile_len) tl.push_back(Tile{k, i0, 0, 0});
+      }
     }
     if ((int)tl.size() > s->max_tiles) return sfail(MDG_ERR_INTERNAL, "tile list exceeds its capacity");
     if (!tl.empty())
@@ -346,6 +454,22 @@ int round_once(mdg_server *s, int *active_out)
     WorkQueue q{{0u, 0u}, (int)tl.size(), 0};
     SCK(cudaMemcpyAsync(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, s->stream));
     s->ntiles = (int)tl.size();
+    const int n2d = (int)(xt.size() + yt.size());
+    if (n2d > s->tiles2_cap) {
+      // grow the 2-D tile list (the previous round has ended: round_once waits for it)
+      const int cap = std::max(n2d, 2 * s->tiles2_cap + 1024);
+      cudaFree(s->d_tiles2);
+      s->d_tiles2 = nullptr;
+      s->tiles2_cap = 0;
+      SCK(cudaMalloc(&s->d_tiles2, sizeof(Tile) * cap));
+      s->tiles2_cap = cap;
+      s->graph_ntx2 = -1;   // the graph holds the old list's address
+    }
+    xt.insert(xt.end(), yt.begin(), yt.end());
+    if (!xt.empty())
+      SCK(cudaMemcpyAsync(s->d_tiles2, xt.data(), sizeof(Tile) * xt.size(), cudaMemcpyHostToDevice, s->stream));
+    s->ntx2 = n2d > 0 ? n2d - (int)yt.size() : 0;
+    s->nty2 = (int)yt.size();
     s->tiles_dirty = false;
   }
   // 3. the round of steps
@@ -353,11 +477,19 @@ int round_once(mdg_server *s, int *active_out)
     const int K = s->cfg.steps_per_round;
     SCK(cudaEventRecord(s->ev0, s->stream));
     if (s->cfg.precision == MDG_PREC_MIXED) {
+      if (s->graph && (s->graph_ntx2 != s->ntx2 || s->graph_nty2 != s->nty2)) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+      }
       if (!s->graph) {
         cudaGraph_t g = nullptr;
         SCK(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        queue_round(s, K);
+        const int qrc = queue_round(s, K);
         const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+        if (qrc != MDG_OK) {
+          if (g) cudaGraphDestroy(g);
+          return qrc;
+        }
         if (e != cudaSuccess) return sfail(MDG_ERR_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
         const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
         cudaGraphDestroy(g);
@@ -365,13 +497,18 @@ int round_once(mdg_server *s, int *active_out)
           s->graph = nullptr;
           return sfail(MDG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ei));
         }
+        s->graph_ntx2 = s->ntx2;
+        s->graph_nty2 = s->nty2;
       }
       SCK(cudaGraphLaunch(s->graph, s->stream));
     } else {
-      queue_round(s, K);
+      const int qrc = queue_round(s, K);
+      if (qrc != MDG_OK) return qrc;
     }
     SCK(cudaEventRecord(s->ev1, s->stream));
     SCK(cudaGetLastError());
+    // per step: dt reduction, two 1-D stages, time update; four 2-D direction sweeps
+    s->launches += (long long)K * (4 + (s->ntx2 > 0 ? 4 : 0));
   }
   // 4. retire the problems that reached their end time (or failed)
   SCK(cudaMemcpyAsync(s->h_times, s->d_times, sizeof(ProbTime) * s->max_probs, cudaMemcpyDeviceToHost, s->stream));
@@ -441,6 +578,14 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   const int64_t bpu = bytes_per_unit(c.precision);
   const int64_t units = c.hbm_bytes / bpu;
   if (units < c.max_zones + 2 * NG) return sfail(MDG_ERR_INVALID, "hbm_bytes too small for one problem of max_zones");
+  if (c.hbm_bytes_2d < 0) return sfail(MDG_ERR_INVALID, "hbm_bytes_2d must not be negative");
+  const int64_t cells = c.hbm_bytes_2d / bytes_per_cell_2d();
+  if (cells > 0) {
+    if (c.max_cells_2d < 4 || c.max_cells_2d > (1 << 30))
+      return sfail(MDG_ERR_INVALID, "max_cells_2d out of [4, 2^30]");
+    if (cells < 2 * (int64_t)c.max_cells_2d)
+      return sfail(MDG_ERR_INVALID, "hbm_bytes_2d too small for one 2-D problem of max_cells_2d");
+  }
   int ndev = 0;
   SCK(cudaGetDeviceCount(&ndev));
   if (c.device < 0 || c.device >= ndev) return sfail(MDG_ERR_INVALID, "device ordinal out of range");
@@ -453,6 +598,8 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   s->max_tiles = (int)(units / s->tile_len + c.max_problems + 1);
   s->slots.assign(c.max_problems, nullptr);
   s->alloc.reset(units);
+  s->cells = cells;
+  s->alloc2.reset(cells);
   auto bail = [&](int rc) { free_server(s); delete s; return rc; };
 #define SCKB(call)                                                                         \
   do {                                                                                     \
@@ -463,8 +610,11 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   } while (0)
   SCKB(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, c.device));
   SCKB(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  SCKB(cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
   SCKB(cudaEventCreate(&s->ev0));
   SCKB(cudaEventCreate(&s->ev1));
+  SCKB(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  SCKB(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
   SCKB(cudaMalloc(&s->d_probs, sizeof(ProbDev) * s->max_probs));
   SCKB(cudaMalloc(&s->d_times, sizeof(ProbTime) * s->max_probs));
   SCKB(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->max_tiles));
@@ -473,8 +623,14 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   SCKB(cudaMalloc(&s->d_state, sizeof(double) * 2 * NPRIM * units));
   SCKB(cudaMalloc(&s->d_rc0, sizeof(double) * RC_NFIELDS * units));
   SCKB(cudaMalloc(&s->d_geo, sizeof(double) * GF_NFIELDS * units));
-  SCKB(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * c.max_zones));
+  SCKB(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * std::max<int64_t>(c.max_zones, cells > 0 ? c.max_cells_2d : 0)));
   if (c.precision == MDG_PREC_MIXED) SCKB(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * units));
+  if (cells > 0) {
+    SCKB(cudaMalloc(&s->d_state2, sizeof(double) * 3 * NPRIM * cells));
+    SCKB(cudaMalloc(&s->d_shock0, cells));
+    SCKB(cudaMalloc(&s->d_shock1, cells));
+    SCKB(cudaMemset(s->d_state2, 0, sizeof(double) * 3 * NPRIM * cells));
+  }
   SCKB(cudaMallocHost(&s->h_times, sizeof(ProbTime) * s->max_probs));
   // empty slots: a zero record has tmax = 0, so the time loop treats it as finished
   SCKB(cudaMemset(s->d_probs, 0, sizeof(ProbDev) * s->max_probs));
@@ -487,7 +643,14 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
     s->P.v[v] = s->d_state + (int64_t)v * units;
     s->PH.v[v] = s->d_state + (int64_t)(NPRIM + v) * units;
   }
+  for (int v = 0; v < NPRIM && cells > 0; v++) {
+    s->P2.v[v] = s->d_state2 + (int64_t)v * cells;
+    s->PH2.v[v] = s->d_state2 + (int64_t)(NPRIM + v) * cells;
+    s->ACC2.v[v] = s->d_state2 + (int64_t)(2 * NPRIM + v) * cells;
+  }
+  // a 2-D problem's direction-1 table sits in the same arena, after its direction-0 one
   s->tb.rc0 = s->d_rc0; s->tb.rc0_stride = units;
+  s->tb.rc1 = s->d_rc0; s->tb.rc1_stride = units;
   s->tb.geo = s->d_geo; s->tb.geo_stride = units;
   s->tb.mx = s->d_mx;
   *out = s;
@@ -498,12 +661,21 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
 {
   if (!s || !desc || !prim) return sfail(MDG_ERR_INVALID, "server/desc/prim");
   std::string why;
-  int rc = validate_desc(*desc, 1, why);
+  const int ndim = desc->ndim == 2 ? 2 : 1;
+  int rc = validate_desc(*desc, ndim, why);
   if (rc != MDG_OK) return sfail(rc, "request: " + why);
   if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
     return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
-  if (desc->n1 > s->cfg.max_zones) return sfail(MDG_ERR_OUTOFMEM, "request: n1 exceeds the server's max_zones");
-  if (s->cfg.precision == MDG_PREC_MIXED) {
+  if (ndim == 2) {
+    if (s->cells == 0) return sfail(MDG_ERR_NOTIMPL, "request: the server was created without a 2-D arena");
+    if ((int64_t)desc->n1 * desc->n2 > s->cfg.max_cells_2d)
+      return sfail(MDG_ERR_OUTOFMEM, "request: n1 x n2 exceeds the server's max_cells_2d");
+    if ((int64_t)desc->n1 + desc->n2 + 4 * NG > s->units)
+      return sfail(MDG_ERR_OUTOFMEM, "request: its tables exceed the unit arena");
+  } else if (desc->n1 > s->cfg.max_zones) {
+    return sfail(MDG_ERR_OUTOFMEM, "request: n1 exceeds the server's max_zones");
+  }
+  if (s->cfg.precision == MDG_PREC_MIXED && ndim == 1) {
     if (desc->hydro_interp_order != 3)
       return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep is built for parabolic reconstruction");
     if (desc->geom == MDG_SPHERICAL && !(desc->startx[0] >= 0.0))
@@ -511,9 +683,16 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
   }
   Request *r = new Request();
   r->desc = *desc;
-  r->ic.assign(prim, prim + (size_t)NPRIM * desc->n1);
-  r->units = desc->n1 + 2 * NG;
-  if (s->cfg.precision == MDG_PREC_FP64) {
+  r->ncell = (int64_t)desc->n1 * (ndim == 2 ? desc->n2 : 1);
+  r->ic.assign(prim, prim + (size_t)NPRIM * r->ncell);
+  footprint(*desc, r->units, r->cells);
+  if (ndim == 2) {
+    // the reference's Romberg tables of both directions, side by side: direction 0 at
+    // columns 0 .. n1+2NG-1, direction 1 after it
+    r->rc.assign((size_t)RC_NFIELDS * r->units, 0.0);
+    build_recon_table(r->desc, 0, r->rc.data(), r->units, 0);
+    build_recon_table(r->desc, 1, r->rc.data(), r->units, desc->n1 + 2 * NG);
+  } else if (s->cfg.precision == MDG_PREC_FP64) {
     // the reference's Romberg tables, built here in the submitting thread so that the
     // request loop does not spend its time on them
     r->rc.assign((size_t)RC_NFIELDS * r->units, 0.0);
@@ -636,8 +815,9 @@ int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st)
   st->wait_p50 = percentile(s->wait, 0.50);
   st->wait_p99 = percentile(s->wait, 0.99);
   const int64_t bpu = bytes_per_unit(s->cfg.precision);
-  st->hbm_capacity = (double)s->units * bpu;
-  st->hbm_in_use = (double)s->units_in_use * bpu;
+  st->hbm_capacity = (double)s->units * bpu + (double)s->cells * bytes_per_cell_2d();
+  st->hbm_in_use = (double)s->units_in_use * bpu + (double)s->cells_in_use * bytes_per_cell_2d();
+  st->kernel_launches = s->launches.load();
   return MDG_OK;
 }
 

@@ -52,14 +52,16 @@ class ServerConfig(ctypes.Structure):
     """mdg_server_config of include/medusa_b200.h."""
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("hbm_bytes", ctypes.c_longlong),
                 ("max_problems", ctypes.c_int), ("max_zones", ctypes.c_int), ("steps_per_round", ctypes.c_int),
-                ("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int)]
+                ("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("hbm_bytes_2d", ctypes.c_longlong), ("max_cells_2d", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):
     """mdg_server_stats of include/medusa_b200.h."""
     _fields_ = [(n, ctypes.c_longlong) for n in ("submitted", "completed", "failed", "queued", "running", "rounds")] + \
                [(n, ctypes.c_double) for n in ("zone_updates", "device_seconds", "latency_p50", "latency_p99",
-                                                "wait_p50", "wait_p99", "hbm_capacity", "hbm_in_use")]
+                                                "wait_p50", "wait_p99", "hbm_capacity", "hbm_in_use")] + \
+               [("kernel_launches", ctypes.c_longlong)]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -304,16 +306,16 @@ REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 
 class Server:
-    """Solve server (mdg_server_*): 1-D problems resident on one GPU, admitted by their
-    device-memory footprint and advanced together; each request runs to its end time
-    (the problem's tmax)."""
+    """Solve server (mdg_server_*): 1-D and 2-D problems resident on one GPU, admitted by
+    their device-memory footprint and advanced together; each request runs to its end
+    time (the problem's tmax).  2-D requests need hbm_bytes_2d > 0."""
 
     def __init__(self, precision: int = PREC_MIXED, device: int = 0, hbm_bytes: int = 2 << 30,
                  max_problems: int = 4096, max_zones: int = 16384, steps_per_round: int = 20,
-                 threads: int = 64, ctas_per_sm: int = 0):
+                 threads: int = 64, ctas_per_sm: int = 0, hbm_bytes_2d: int = 0, max_cells_2d: int = 1 << 20):
         L = library()
         c = ServerConfig(device, precision, int(hbm_bytes), max_problems, max_zones, steps_per_round, threads,
-                         ctas_per_sm)
+                         ctas_per_sm, int(hbm_bytes_2d), int(max_cells_2d))
         h = ctypes.c_void_p()
         _check(L.mdg_server_create(ctypes.byref(c), ctypes.byref(h)), "mdg_server_create")
         self._h = h

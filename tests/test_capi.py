@@ -92,7 +92,8 @@ def test_launch_config_calls_reject_null_solver():
 
 
 @pytest.mark.parametrize("field,value", [("precision", 7), ("max_problems", 0), ("max_zones", 2),
-                                         ("steps_per_round", 0), ("threads", 96), ("hbm_bytes", 1000)])
+                                         ("steps_per_round", 0), ("threads", 96), ("hbm_bytes", 1000),
+                                         ("hbm_bytes_2d", -1), ("hbm_bytes_2d", 1 << 20)])
 def test_server_config_is_checked_before_any_device_work(field, value):
     c = S.ServerConfig(0, S.PREC_MIXED, 1 << 30, 64, 4096, 10, 64, 0)
     setattr(c, field, value)

@@ -142,6 +142,78 @@ def test_server_request_loop_thread():
             assert np.all(np.isfinite(prim)) and t >= pb.tmax
 
 
+def _mix_2d():
+    """2-D requests: Kelvin-Helmholtz and Rayleigh-Taylor of uneven sizes and end times."""
+    return [
+        P.kelvin_helmholtz(64, 48, seed=5).copy(tmax=0.03, name="kh64x48"),
+        P.rayleigh_taylor_2d(40, 72, g=-0.5, noise=0.05).copy(tmax=0.05, name="rt40x72"),
+        P.kelvin_helmholtz(96, 130, seed=9).copy(tmax=0.02, name="kh96x130"),
+        P.rayleigh_taylor_2d(33, 66, g=-0.1, noise=0.02).copy(tmax=0.04, name="rt33x66"),
+    ]
+
+
+def _server_2d(precision, spr=11):
+    return Server(precision=precision, hbm_bytes=256 << 20, max_problems=32, max_zones=4096,
+                  steps_per_round=spr, hbm_bytes_2d=64 << 20, max_cells_2d=1 << 16)
+
+
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_server_2d_requests_equal_solver(precision):
+    """2-D requests run on the FP64 split sweep beside the 1-D lane; each result is the
+    solver's FP64 run of the same problem, bit for bit, also with 1-D requests resident."""
+    reqs2 = _mix_2d()
+    reqs1 = _mix()[:3]
+    with _server_2d(precision) as srv:
+        ids2 = [srv.submit(pb) for pb in reqs2]
+        ids1 = [srv.submit(pb) for pb in reqs1]
+        assert srv.run(0) == 0
+        assert srv.stats()["completed"] == len(reqs1) + len(reqs2)
+        for rid, pb in zip(ids2, reqs2):
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_result(pb, PREC_FP64)
+            assert t >= pb.tmax and t == rt and ist == rist, pb.name
+            assert np.array_equal(prim, ref), pb.name
+        for rid, pb in zip(ids1, reqs1):
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_result(pb, precision)
+            assert t == rt and ist == rist
+            assert np.array_equal(prim, ref)
+
+
+def test_server_2d_slot_reuse_and_graph_recapture():
+    """2-D requests arriving and leaving between rounds (the tile lists and the mixed
+    round's graph change) and reusing freed cell ranges (shock bits zeroed again)."""
+    reqs2 = _mix_2d()
+    reqs1 = _mix()
+    with _server_2d(PREC_MIXED, spr=7) as srv:
+        got = {}
+        for k in range(4):
+            got[srv.submit(reqs1[k])] = (reqs1[k], PREC_MIXED)
+            got[srv.submit(reqs2[k])] = (reqs2[k], PREC_FP64)
+            srv.run(2 + k)
+        again = reqs2[0].copy(tmax=0.025)
+        got[srv.submit(again)] = (again, PREC_FP64)
+        srv.run(0)
+        for rid, (pb, prec) in got.items():
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_result(pb, prec)
+            assert t == rt and ist == rist, pb.name
+            assert np.array_equal(prim, ref), pb.name
+
+
+def test_server_2d_refused_without_arena():
+    pb = _mix_2d()[0]
+    with Server(precision=PREC_MIXED, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
+        with pytest.raises(MdgError) as e:
+            srv.submit(pb)
+        assert e.value.code == 5
+    with _server_2d(PREC_MIXED) as srv:
+        big = P.kelvin_helmholtz(300, 300, seed=1).copy(tmax=0.01)
+        with pytest.raises(MdgError) as e:
+            srv.submit(big)
+        assert e.value.code == 6
+
+
 @pytest.mark.parametrize("bad,code", [
     (dict(tmax=1.0e100), 1),                 # no end time
     (dict(n=(5000, 1, 1)), 6),               # larger than max_zones
