@@ -279,6 +279,26 @@ int mdg_server_result(mdg_server *s, long long id, double *prim, double *t, int 
 int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st);
 int mdg_server_destroy(mdg_server *s);
 
+/*
+ * 3-D dendritic spherical grids (ndim = 3; the grid of DENDRITIC_GRID=TRUE builds,
+ * utils.c:181-525).  Radial row i has nj[i] theta zones and row (i, j) nk phi zones; the
+ * state of a 3-D problem is passed in the reference's zone order (ZLOOP: i, then j, then
+ * k).  Host-only calls (no device work):
+ *   mdg_grid3d_counts   nj[i] for i in [0, n1) (nj may be NULL), nk of every interior
+ *                       row in zone order (nk may be NULL; sum(nj) entries), *ncell the
+ *                       interior zone count;
+ *   mdg_grid3d_geometry the per-row zone geometry for every row i in [-2, n1+2),
+ *                       j in [-2, nj[i]+2) (ghost rows included), MDG_GEO3_FIELDS doubles
+ *                       each: volume, area[3], gcov[4][3], gcon[3], scale[4][3], then
+ *                       conn[l][m][n] for (lmn) = 000 011 022 101 110 111 122 202 220 212
+ *                       221 (the coefficients the spherical metric sets, init_conn);
+ *                       rows may be NULL, *nrows the row count.
+ * A 3-D solver advances one problem, plain FP64 (MDG_PREC_FP64).
+ */
+#define MDG_GEO3_FIELDS 42
+int mdg_grid3d_counts(const mdg_problem_desc *desc, int *nj, int *nk, long long *ncell);
+int mdg_grid3d_geometry(const mdg_problem_desc *desc, double *rows, long long *nrows);
+
 /* Library version as major*10000 + minor*100 + patch. */
 int mdg_version(void);
 

@@ -2,11 +2,13 @@
 // per-step launch sequence.
 #include <cuda_runtime.h>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
 #include "mdg_internal.h"
 #include "mdg_kernels.cuh"
+#include "mdg_grid3d.cuh"
 
 namespace mdg {
 void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
@@ -15,6 +17,7 @@ void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area
 void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
 void spherical_1d_constants(double &area_k, double &th1, double &th2, double &tc);
+void build_grid3(const mdg_problem_desc &d, Grid3Host &h);
 }
 
 using namespace mdg;
@@ -43,6 +46,7 @@ struct mdg_solver {
   double *d_stage = nullptr;      // AoS staging buffer, 5 doubles per zone of the largest problem
   double *d_stage_all = nullptr;  // AoS staging of every problem (mdg_upload_all / mdg_download_all)
   int64_t max_cells = 0;
+  Sweep3 *s3 = nullptr;           // 3-D: the dendritic sweep of the single problem
   int *d_err = nullptr;
   // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
   float *d_mx = nullptr;
@@ -87,8 +91,41 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
 {
   char buf[256];
   auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
-  if (d.ndim != 1 && d.ndim != 2) return bad("ndim must be 1 or 2");
+  if (d.ndim != 1 && d.ndim != 2 && d.ndim != 3) return bad("ndim must be 1, 2 or 3");
   if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
+  if (d.ndim == 3) {
+    // the dendritic spherical grid of prim_to_fluxes3 over the whole sphere
+    auto pow2 = [](int n) { return n > 0 && (n & (n - 1)) == 0; };
+    if (d.geom != MDG_SPHERICAL) { why = "3-D grids are spherical (dendritic) in this version"; return MDG_ERR_NOTIMPL; }
+    if (d.n1 < 2 || d.n1 > (1 << 16)) return bad("n1 out of range [2, 2^16]");
+    if (!pow2(d.n2) || d.n2 < 2 || d.n2 > (1 << 12)) return bad("n2 must be a power of two in [2, 4096]");
+    if (!pow2(d.n3) || d.n3 < 4 || d.n3 > (1 << 13)) return bad("n3 must be a power of two in [4, 8192]");
+    if (!(d.dx[0] > 0.0 && d.dx[1] > 0.0 && d.dx[2] > 0.0)) return bad("dx must be positive");
+    if (!(d.startx[0] >= 0.0)) return bad("the radial grid must start at r >= 0");
+    if (d.startx[1] != -1.0 || std::fabs(d.startx[1] + d.n2 * d.dx[1] - 1) >= 1.0e-15)
+      return bad("theta must cover the whole sphere (x1 from -1 to 1)");
+    if (d.startx[2] != 0.0 || std::fabs(d.n3 * d.dx[2] - 2.0 * M_PI) > 1.0e-12)
+      return bad("phi must cover [0, 2 pi)");
+    if (d.eos != MDG_GAMMA_LAW && d.eos != MDG_POLYTROPIC) return bad("eos must be gamma-law or polytrope");
+    if (d.hydro_interp_order < 1 || d.hydro_interp_order > 3) return bad("hydro_interp_order must be 1, 2 or 3");
+    if (!(d.gam > 1.0)) return bad("gam must exceed 1");
+    if (!(d.cfl > 0.0)) return bad("cfl must be positive");
+    if (d.enforce_floors != 0 && d.enforce_floors != 1) return bad("enforce_floors must be 0 or 1");
+    if (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0) {
+      why = "fixed gravity is not built for 3-D grids";
+      return MDG_ERR_NOTIMPL;
+    }
+    const bool ok = (d.bc_lo[0] == MDG_BC_REFLECT || d.bc_lo[0] == MDG_BC_SPHERICAL_ORIGIN) &&
+                    (d.bc_hi[0] == MDG_BC_OUTFLOW || d.bc_hi[0] == MDG_BC_REFLECT);
+    auto okj = [](int k) { return k == MDG_BC_REFLECT || k == MDG_BC_SPHERICAL_ORIGIN || k == MDG_BC_OUTFLOW; };
+    auto okk = [](int k) { return k == MDG_BC_PERIODIC || k == MDG_BC_REFLECT || k == MDG_BC_OUTFLOW; };
+    if (!ok || !okj(d.bc_lo[1]) || !okj(d.bc_hi[1]) || !okk(d.bc_lo[2]) || !okk(d.bc_hi[2])) {
+      why = "unsupported 3-D boundary kinds";
+      return MDG_ERR_NOTIMPL;
+    }
+    if ((d.bc_lo[2] == MDG_BC_PERIODIC) != (d.bc_hi[2] == MDG_BC_PERIODIC)) return bad("periodic boundaries must be paired");
+    return MDG_OK;
+  }
   if (d.n1 < 2 || d.n1 > (1 << 28)) return bad("n1 out of range [2, 2^28]");
   if (d.ndim == 2 && (d.n2 < 2 || (int64_t)d.n1 * d.n2 > (int64_t)1 << 31)) return bad("n2 out of range");
   if (d.eos != MDG_GAMMA_LAW && d.eos != MDG_POLYTROPIC) return bad("eos must be gamma-law or polytrope");
@@ -174,6 +211,7 @@ void mdg::make_probdev(const mdg_problem_desc &d, ProbDev &P)
   memset(&P, 0, sizeof P);
   P.ndim = d.ndim; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
   P.n1 = d.n1; P.n2 = (d.ndim > 1) ? d.n2 : 1;
+  P.ncell = (int64_t)P.n1 * P.n2;
   P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0]; P.bc_lo1 = d.bc_lo[1]; P.bc_hi1 = d.bc_hi[1];
   P.prob_kind = d.prob_kind;
   P.has_src = (d.geom == MDG_SPHERICAL);
@@ -199,13 +237,109 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
   cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
   cudaFree(s->d_mx); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
+  sweep3_destroy(s->s3);
+  s->s3 = nullptr;
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->stream) cudaStreamDestroy(s->stream);
+}
+
+// A solver of one 3-D dendritic spherical problem (validated by the caller): the grid
+// tables of mdg_sweep3d.cu, state P and PH of ncell zones in the reference's zone order.
+static int create_3d(const mdg_problem_desc &d, int device, mdg_solver **out)
+{
+  mdg_solver *s = new mdg_solver();
+  s->device = device;
+  s->ndim = 3;
+  s->nprob = 1;
+  s->precision = MDG_PREC_FP64;
+  s->descs.assign(1, d);
+  std::string why;
+  int rc = sweep3_create(d, &s->s3, why);
+  if (rc != MDG_OK) {
+    delete s;
+    return fail(rc, "3-D grid: " + why);
+  }
+  const int64_t n = sweep3_ncell(s->s3);
+  ProbDev P;
+  make_probdev(d, P);
+  P.n2 = d.n2;
+  P.ncell = n;
+  P.cell_off = 0;
+  s->hprobs.push_back(P);
+  s->ncell_total = n;
+  s->max_cells = n;
+  auto cleanup_fail = [&](cudaError_t e, const char *what) {
+    fail(e == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    free_all(s);
+    delete s;
+    return e == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA;
+  };
+#define CK3(call)                                   \
+  do {                                              \
+    cudaError_t e_ = (call);                        \
+    if (e_ != cudaSuccess) return cleanup_fail(e_, #call); \
+  } while (0)
+  CK3(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  CK3(cudaMalloc(&s->d_probs, sizeof(ProbDev)));
+  CK3(cudaMalloc(&s->d_times, sizeof(ProbTime)));
+  CK3(cudaMalloc(&s->d_state, sizeof(double) * 2 * NPRIM * n));
+  CK3(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * n));
+  CK3(cudaMalloc(&s->d_err, sizeof(int)));
+  CK3(cudaMalloc(&s->d_totals, sizeof(double) * 2));
+  CK3(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
+  CK3(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
+  CK3(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
+  CK3(cudaMemcpy(s->d_probs, &P, sizeof(ProbDev), cudaMemcpyHostToDevice));
+  CK3(cudaMemset(s->d_state, 0, sizeof(double) * 2 * NPRIM * n));
+  CK3(cudaMemset(s->d_err, 0, sizeof(int)));
+  CK3(cudaMemset(s->d_times, 0, sizeof(ProbTime)));
+  for (int v = 0; v < NPRIM; v++) {
+    s->P.v[v] = s->d_state + (int64_t)v * n;
+    s->PH.v[v] = s->d_state + (int64_t)(NPRIM + v) * n;
+  }
+#undef CK3
+  *out = s;
+  return MDG_OK;
 }
 
 extern "C" {
 
 int mdg_version(void) { return 100; }
+
+int mdg_grid3d_counts(const mdg_problem_desc *desc, int *nj, int *nk, long long *ncell)
+{
+  if (!desc) return fail(MDG_ERR_INVALID, "desc");
+  std::string why;
+  int rc = validate_desc(*desc, 3, why);
+  if (rc != MDG_OK) return fail(rc, why);
+  Grid3Host h;
+  build_grid3(*desc, h);
+  int64_t c = 0;
+  for (int i = 0; i < h.n1; i++) {
+    if (nj) nj[i] = h.njr(i);
+    for (int j = 0; j < h.njr(i); j++) {
+      if (nk) nk[c] = h.nk[h.row(i, j)];
+      c++;
+    }
+  }
+  if (ncell) *ncell = h.ncell;
+  return MDG_OK;
+}
+
+int mdg_grid3d_geometry(const mdg_problem_desc *desc, double *rows, long long *nrows)
+{
+  if (!desc) return fail(MDG_ERR_INVALID, "desc");
+  std::string why;
+  int rc = validate_desc(*desc, 3, why);
+  if (rc != MDG_OK) return fail(rc, why);
+  Grid3Host h;
+  build_grid3(*desc, h);
+  if (nrows) *nrows = h.nij;
+  if (rows)
+    for (int64_t r = 0; r < h.nij; r++)
+      for (int f = 0; f < G3_NFIELDS; f++) rows[r * G3_NFIELDS + f] = h.geo[(size_t)f * h.nij + r];
+  return MDG_OK;
+}
 
 const char *mdg_error_string(int code)
 {
@@ -245,10 +379,16 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
   }
+  if (ndim == 3) {
+    if (nprob != 1) return fail(MDG_ERR_NOTIMPL, "a 3-D solver advances one problem");
+    if (precision != MDG_PREC_FP64)
+      return fail(MDG_ERR_NOTIMPL, "the mixed-precision sweep is built for 1-D parabolic reconstruction");
+  }
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(MDG_ERR_INVALID, "device ordinal out of range");
   CK(cudaSetDevice(device));
+  if (ndim == 3) return create_3d(descs[0], device, out);
 
   mdg_solver *s = new mdg_solver();
   s->device = device;
@@ -379,11 +519,12 @@ int mdg_upload_state(mdg_solver *s, int prob, const double *prim)
   if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
   CK(cudaSetDevice(s->device));
   const ProbDev &P = s->hprobs[prob];
-  const int64_t n = (int64_t)P.n1 * P.n2;
+  const int64_t n = P.ncell;
   CK(cudaMemcpyAsync(s->d_stage, prim, sizeof(double) * NPRIM * n, cudaMemcpyHostToDevice, s->stream));
   launch_aos_to_soa(s->d_stage, s->P, P.cell_off, n, s->stream);
   launch_reset_time(s->d_times, prob, s->stream);
-  launch_initial_estimate_one(s->d_probs, s->d_times, prob, n, s->tb, s->P, s->stream);
+  if (s->ndim == 3) launch_initial_estimate3(s->s3, s->d_probs, s->d_times, s->P, s->stream);
+  else launch_initial_estimate_one(s->d_probs, s->d_times, prob, n, s->tb, s->P, s->stream);
   CK(cudaGetLastError());
   return MDG_OK;
 }
@@ -404,7 +545,8 @@ int mdg_upload_all(mdg_solver *s, const double *prim)
                      s->stream));
   launch_aos_to_soa(s->d_stage_all, s->P, 0, s->ncell_total, s->stream);
   launch_reset_time_all(s->d_times, s->nprob, s->stream);
-  launch_initial_estimate_all(s->d_probs, s->d_times, s->nprob, s->max_cells, s->tb, s->P, s->stream);
+  if (s->ndim == 3) launch_initial_estimate3(s->s3, s->d_probs, s->d_times, s->P, s->stream);
+  else launch_initial_estimate_all(s->d_probs, s->d_times, s->nprob, s->max_cells, s->tb, s->P, s->stream);
   CK(cudaGetLastError());
   return MDG_OK;
 }
@@ -437,6 +579,8 @@ static int queue_steps(mdg_solver *s, int nsteps)
     if (mixed)
       launch_stage1d_mixed(0, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
                            s->tb, s->P, s->P, s->PH, s->stream);
+    else if (s->ndim == 3)
+      launch_stage3d(0, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
     else if (s->ndim == 1)
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
     else
@@ -447,6 +591,8 @@ static int queue_steps(mdg_solver *s, int nsteps)
     if (mixed)
       launch_stage1d_mixed(1, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
                            s->tb, s->PH, s->P, s->P, s->stream);
+    else if (s->ndim == 3)
+      launch_stage3d(1, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
     else if (s->ndim == 1)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     else
@@ -648,7 +794,8 @@ int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy)
 {
   if (!s) return fail(MDG_ERR_INVALID, "solver");
   CK(cudaSetDevice(s->device));
-  launch_conserved_totals(s->d_probs, s->nprob, s->tb, s->P, s->d_totals, s->stream);
+  if (s->ndim == 3) launch_totals3(s->s3, s->P, s->d_totals, s->stream);
+  else launch_conserved_totals(s->d_probs, s->nprob, s->tb, s->P, s->d_totals, s->stream);
   CK(cudaGetLastError());
   std::vector<double> h(2 * (size_t)s->nprob);
   CK(cudaMemcpyAsync(h.data(), s->d_totals, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream));
@@ -666,7 +813,7 @@ int mdg_download_state(mdg_solver *s, int prob, double *prim, double *eos)
   if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
   CK(cudaSetDevice(s->device));
   const ProbDev &P = s->hprobs[prob];
-  const int64_t n = (int64_t)P.n1 * P.n2;
+  const int64_t n = P.ncell;
   launch_soa_to_aos(s->P, P.cell_off, n, s->d_stage, s->stream);
   CK(cudaMemcpyAsync(prim, s->d_stage, sizeof(double) * NPRIM * n, cudaMemcpyDeviceToHost, s->stream));
   if (eos) {

@@ -16,6 +16,8 @@
 #include <vector>
 #include "mdg_internal.h"
 #include "mdg_tables.cuh"
+#include "mdg_grid3d.cuh"
+#include <algorithm>
 #include "../../include/medusa_b200.h"
 
 namespace mdg {
@@ -305,6 +307,269 @@ void spherical_1d_constants(double &area_k, double &th1, double &th2, double &tc
   th1 = romb(x1lo, x1hi, f_sthdth_dx3) / vthf;
   th2 = romb(x1lo, x1hi, f_sth3dth_dx) / vthf;
   tc = romb(x1lo, x1hi, f_cthdth_dx2) / vthf;
+}
+
+}  // namespace mdg
+
+namespace mdg {
+
+static double f_xth1g(double x) { return x * std::sin(th_of_x(x)) * dth_dx(x); }
+static double f_xth2g(double x) { return x * x * std::sin(th_of_x(x)) * dth_dx(x); }
+
+// Grid, geometry and reconstruction tables of a 3-D spherical problem on the dendritic
+// grid, uniform radius and theta:
+//   zone counts      compute_dj / compute_dk (utils.c:181-354; MAX_LOG2_ASPECT utils.c:12)
+//   moments          init_interp_vol (metric_spherical_general.c:592-668)
+//   volume, area     init_volume / init_area (708-816), axis areas hard-zero
+//   gcov, gcon, scale, conn   (941-1051, 837-939), conn[1][1][1] from the dendritic
+//                    neighbour areas (897-916)
+// with the reference's operation order (every product and sum as written there).
+void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
+{
+  const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+  h.n1 = n1; h.n2 = n2; h.n3 = n3;
+  const double sx0 = d.startx[0], sx1 = d.startx[1], sx2 = d.startx[2];
+  const double dx0 = d.dx[0], dx1 = d.dx[1], dx2 = d.dx[2];
+  const double max_log2_aspect = 0.5;
+
+  // theta zones per radial row
+  h.nj.assign(n1 + 2 * NG, 0);
+  auto NJ = [&](int i) -> int & { return h.nj[i + NG]; };
+  NJ(0) = 2;
+  {
+    const double dth = th_of_x(sx1 + n2 * dx1) - th_of_x(sx1);
+    for (int i = 1; i < n1; i++) {
+      double r0 = r_of_x(sx0 + (i + 0.0) * dx0);
+      double rc = r_of_x(sx0 + (i + 0.5) * dx0);
+      double r1 = r_of_x(sx0 + (i + 1.0) * dx0);
+      double dr = r1 - r0;
+      double nj_ideal = rc * dth / dr;
+      NJ(i) = NJ(i - 1);
+      if (std::log2(nj_ideal / NJ(i)) > max_log2_aspect) NJ(i) *= 2;
+      NJ(i) = std::min(std::max(NJ(i), NJ(i - 1)), n2);
+    }
+  }
+  for (int i = -NG; i < 0; i++) NJ(i) = NJ(-i - 1);
+  for (int i = n1; i < n1 + NG; i++) NJ(i) = NJ(n1 - 1);
+  auto DJ = [&](int i) { return n2 / NJ(i); };
+
+  // row tables
+  h.rowbase.assign(n1 + 2 * NG, 0);
+  int64_t nij = 0;
+  for (int i = -NG; i < n1 + NG; i++) {
+    h.rowbase[i + NG] = (int)nij;
+    nij += NJ(i) + 2 * NG;
+  }
+  h.nij = nij;
+  h.nk.assign(nij, 0);
+  auto NK = [&](int i, int j) -> int & { return h.nk[h.rowbase[i + NG] + j + NG]; };
+
+  // phi zones per (i, j)
+  {
+    const int nk_min = 4;
+    const double dph = n3 * dx2;
+    NK(0, 0) = nk_min;
+    for (int j = 1; j < NJ(0); j++) {
+      double r0 = r_of_x(sx0 + (0.0) * dx0);
+      double rc = r_of_x(sx0 + (0.5) * dx0);
+      double r1 = r_of_x(sx0 + (1.0) * dx0);
+      double dr = r1 - r0;
+      double thc = th_of_x(sx1 + (j + 0.5) * DJ(0) * dx1);
+      double nk_ideal = rc * std::sin(thc) * dph / dr;
+      if (j < NJ(0) / 2) {
+        NK(0, j) = NK(0, j - 1);
+        if (std::log2(nk_ideal / NK(0, j)) > max_log2_aspect) NK(0, j) *= 2;
+        NK(0, j) = std::min(NK(0, j), n3);
+      } else {
+        NK(0, j) = NK(0, NJ(0) - 1 - j);
+      }
+    }
+    for (int i = 1; i < n1; i++) {
+      double r0 = r_of_x(sx0 + (i + 0.0) * dx0);
+      double rc = r_of_x(sx0 + (i + 0.5) * dx0);
+      double r1 = r_of_x(sx0 + (i + 1.0) * dx0);
+      double dr = r1 - r0;
+      NK(i, 0) = nk_min;
+      for (int j = 1; j < NJ(i); j++) {
+        double thc = th_of_x(sx1 + (j + 0.5) * DJ(i) * dx1);
+        double nk_ideal = rc * std::sin(thc) * dph / dr;
+        if (j < NJ(i) / 2) {
+          NK(i, j) = NK(i, j - 1);
+          if (std::log2(nk_ideal / NK(i, j)) > max_log2_aspect) NK(i, j) *= 2;
+          if (NJ(i - 1) == NJ(i)) NK(i, j) = std::min(std::max(NK(i, j), NK(i - 1, j)), n3);
+          else NK(i, j) = std::min(std::max(NK(i, j), NK(i - 1, j / 2)), n3);
+        } else {
+          NK(i, j) = NK(i, NJ(i) - 1 - j);
+        }
+      }
+    }
+    for (int i = -NG; i < 0; i++)
+      for (int j = 0; j < NJ(i); j++) NK(i, j) = NK(-i - 1, j);
+    for (int i = n1; i < n1 + NG; i++)
+      for (int j = 0; j < NJ(i); j++) NK(i, j) = NK(n1 - 1, j);
+    for (int i = -NG; i < n1 + NG; i++) {
+      for (int j = -NG; j < 0; j++) NK(i, j) = NK(i, -j - 1);
+      for (int j = NJ(i); j < NJ(i) + NG; j++) NK(i, j) = NK(i, 2 * NJ(i) - 1 - j);
+    }
+  }
+  auto DK = [&](int i, int j) { return n3 / NK(i, j); };
+
+  // zone and face offsets
+  h.cell.assign(nij, -1); h.f0.assign(nij, -1); h.f1.assign(nij, -1); h.f2.assign(nij, -1);
+  int64_t c = 0, f0 = 0, f1 = 0, f2 = 0;
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < NJ(i); j++) { h.cell[h.row(i, j)] = c; c += NK(i, j); }
+  for (int i = 0; i <= n1; i++)
+    for (int j = 0; j < NJ(i); j++) { h.f0[h.row(i, j)] = f0; f0 += NK(i, j); }
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j <= NJ(i); j++) { h.f1[h.row(i, j)] = f1; f1 += n3 / std::min(DK(i, j), DK(i, j - 1)); }
+  for (int i = 0; i < n1; i++)
+    for (int j = 0; j < NJ(i); j++) { h.f2[h.row(i, j)] = f2; f2 += NK(i, j) + 1; }
+  h.ncell = c; h.nf0 = f0; h.nf1 = f1; h.nf2 = f2;
+
+  // direction-0 reconstruction table (the 1-D spherical radial moments)
+  h.rc0.assign((size_t)RC_NFIELDS * (n1 + 2 * NG), 0.0);
+  build_recon_table(d, 0, h.rc0.data(), n1 + 2 * NG, 0);
+
+  // direction-1 and -2 tables per refinement level
+  int lev1 = 0, lev2 = 0;
+  for (int i = -NG; i < n1 + NG; i++) {
+    lev1 = std::max(lev1, ilog2(DJ(i)));
+    for (int j = -NG; j < NJ(i) + NG; j++) lev2 = std::max(lev2, ilog2(DK(i, j)));
+  }
+  h.nlev1 = lev1 + 1; h.nlev2 = lev2 + 1;
+  int64_t cols1 = 0, cols2 = 0;
+  for (int l = 0; l < h.nlev1; l++) { h.rc1_base[l] = (int)cols1; cols1 += (n2 >> l) + 2 * NG; }
+  for (int l = 0; l < h.nlev2; l++) { h.rc2_base[l] = (int)cols2; cols2 += (n3 >> l) + 2 * NG; }
+  h.cols1 = cols1; h.cols2 = cols2;
+  h.rc1.assign((size_t)RC_NFIELDS * cols1, 0.0); h.rc2.assign((size_t)RC_NFIELDS * cols2, 0.0);
+  h.xc1.assign(cols1, 0.0); h.xc2.assign(cols2, 0.0);
+  h.sth.assign(cols1, 0.0); h.cth.assign(cols1, 0.0);
+  h.sphc.assign(cols2, 0.0); h.cphc.assign(cols2, 0.0); h.sphl.assign(cols2, 0.0); h.cphl.assign(cols2, 0.0);
+  for (int l = 0; l < h.nlev1; l++) {
+    const int s = 1 << l, n = n2 >> l;
+    std::vector<double> al(n + 2 * NG), be(n + 2 * NG), ga(n + 2 * NG);
+    for (int j = -NG; j < n + NG; j++) {
+      double x0 = sx1 + j * s * dx1, x1 = sx1 + (j + 1) * s * dx1;
+      ga[j + NG] = romb(x0, x1, f_sthdth_dx);
+      be[j + NG] = romb(x0, x1, f_xth1g);
+      al[j + NG] = romb(x0, x1, f_xth2g);
+    }
+    for (int j = -NG; j < n + NG; j++) {
+      const int col = h.rc1_base[l] + j + NG;
+      int jm = (j - 1 < -NG) ? -NG : j - 1, jp = (j + 1 >= n + NG) ? n + NG - 1 : j + 1;
+      double v[RC_NFIELDS];
+      rc_fields(al[jm + NG], al[j + NG], al[jp + NG], be[jm + NG], be[j + NG], be[jp + NG], ga[jm + NG],
+                ga[j + NG], ga[jp + NG], sx1 + j * s * dx1, sx1 + (j + 1) * s * dx1, v);
+      for (int f = 0; f < RC_NFIELDS; f++) h.rc1[(size_t)f * cols1 + col] = v[f];
+      h.xc1[col] = be[j + NG] / ga[j + NG];
+      double th = th_of_x(be[j + NG] / ga[j + NG]);
+      h.sth[col] = std::sin(th);
+      h.cth[col] = std::cos(th);
+    }
+  }
+  for (int l = 0; l < h.nlev2; l++) {
+    const int s = 1 << l, n = n3 >> l;
+    std::vector<double> al(n + 2 * NG), be(n + 2 * NG), ga(n + 2 * NG);
+    for (int k = -NG; k < n + NG; k++) {
+      double x0 = sx2 + k * s * dx2, x1 = sx2 + (k + 1) * s * dx2;
+      ga[k + NG] = s * dx2;
+      be[k + NG] = (x1 * x1 - x0 * x0) / 2.0;
+      al[k + NG] = (x1 * x1 * x1 - x0 * x0 * x0) / 3.0;
+    }
+    for (int k = -NG; k < n + NG; k++) {
+      const int col = h.rc2_base[l] + k + NG;
+      int km = (k - 1 < -NG) ? -NG : k - 1, kp = (k + 1 >= n + NG) ? n + NG - 1 : k + 1;
+      double v[RC_NFIELDS];
+      rc_fields(al[km + NG], al[k + NG], al[kp + NG], be[km + NG], be[k + NG], be[kp + NG], ga[km + NG],
+                ga[k + NG], ga[kp + NG], sx2 + k * s * dx2, sx2 + (k + 1) * s * dx2, v);
+      for (int f = 0; f < RC_NFIELDS; f++) h.rc2[(size_t)f * cols2 + col] = v[f];
+      h.xc2[col] = be[k + NG] / ga[k + NG];
+      double phc = sx2 + (k + 0.5) * s * dx2, phl = sx2 + k * s * dx2;
+      h.sphc[col] = std::sin(phc); h.cphc[col] = std::cos(phc);
+      h.sphl[col] = std::sin(phl); h.cphl[col] = std::cos(phl);
+    }
+  }
+
+  // per-row geometry
+  h.geo.assign((size_t)G3_NFIELDS * nij, 0.0);
+  auto G = [&](int f, int i, int j) -> double & { return h.geo[(size_t)f * nij + h.row(i, j)]; };
+  for (int i = -NG; i < n1 + NG; i++) {
+    const double x0lo = sx0 + i * dx0, x0hi = sx0 + (i + 1) * dx0;
+    const double r2dr_int = romb(x0lo, x0hi, f_r2dr_dx);
+    const double rint_r2dr_dx3 = romb(x0lo, x0hi, f_r2dr_dx3);
+    const double r5 = std::pow(r_of_x(x0hi), 5) - std::pow(r_of_x(x0lo), 5);
+    for (int j = -NG; j < NJ(i) + NG; j++) {
+      const double x1lo = sx1 + j * DJ(i) * dx1, x1hi = sx1 + (j + 1) * DJ(i) * dx1;
+      const double sthdth_int = romb(x1lo, x1hi, f_sthdth_dx);
+      G(G3_VOL, i, j) = r2dr_int * sthdth_int * DK(i, j) * dx2;
+      if (i >= 0 && i <= n1 && j >= 0 && j <= NJ(i)) {
+        const double dph_int = DK(i, j) * dx2;
+        G(G3_A0, i, j) = f_r2dr_dx(x0lo) * sthdth_int * dph_int;
+        G(G3_A1, i, j) = r2dr_int * f_sthdth_dx(x1lo) * dph_int;
+        G(G3_A2, i, j) = r2dr_int * sthdth_int;
+      }
+      const double vrf = r2dr_int, vthf = sthdth_int;
+      const double th3 = romb(x1lo, x1hi, f_sthdth_dx3);
+      const double ts3 = romb(x1lo, x1hi, f_sth3dth_dx);
+      double gc[4][3];
+      gc[0][0] = rint_r2dr_dx3 / vrf;
+      gc[0][1] = std::fabs(0.2 * r5 / vrf * th3 / vthf);
+      gc[0][2] = std::fabs(0.2 * r5 / vrf * ts3 / vthf);
+      gc[1][0] = std::pow(dr_dx(x0lo), 2);
+      gc[1][1] = std::pow(r_of_x(x0lo), 2) * th3 / vthf;
+      gc[1][2] = std::pow(r_of_x(x0lo), 2) * ts3 / vthf;
+      gc[2][0] = gc[0][0];
+      gc[2][1] = std::fabs(0.2 * r5 / vrf * std::pow(dth_dx(x1lo), 2));
+      gc[2][2] = std::fabs(0.2 * r5 / vrf * std::pow(std::sin(th_of_x(x1lo)), 2));
+      gc[3][0] = gc[0][0]; gc[3][1] = gc[0][1]; gc[3][2] = gc[0][2];
+      for (int l = 0; l < 4; l++)
+        for (int m = 0; m < 3; m++) {
+          G(G3_GCOV + 3 * l + m, i, j) = gc[l][m];
+          G(G3_SCALE + 3 * l + m, i, j) = std::sqrt(gc[l][m]);
+        }
+      for (int m = 0; m < 3; m++) G(G3_GCON + m, i, j) = (std::fabs(gc[0][m]) > 1.0e-50) ? 1.0 / gc[0][m] : 0.0;
+    }
+  }
+  // the areas of the axis faces are exactly zero
+  if (sx1 == -1) {
+    for (int i = 0; i <= n1; i++) G(G3_A1, i, 0) = 0.0;
+  }
+  if (std::fabs(sx1 + n2 * dx1 - 1) < 1.0e-15) {
+    for (int i = 0; i <= n1; i++) G(G3_A1, i, NJ(i)) = 0.0;
+  }
+  // connection coefficients of the interior rows
+  for (int i = 0; i < n1; i++) {
+    const double x0lo = sx0 + i * dx0, x0hi = sx0 + (i + 1) * dx0;
+    const double ri_r2d2r = romb(x0lo, x0hi, f_r2d2r_dx2);
+    const double ri_r3 = romb(x0lo, x0hi, f_r3);
+    const double ri_rdr2 = romb(x0lo, x0hi, f_rdr_dx2);
+    const double vrf = romb(x0lo, x0lo + dx0, f_r2dr_dx);
+    for (int j = 0; j < NJ(i); j++) {
+      const double x1lo = sx1 + j * DJ(i) * dx1, x1hi = sx1 + (j + 1) * DJ(i) * dx1;
+      const double vthf = romb(x1lo, x1hi, f_sthdth_dx);
+      const double th3 = romb(x1lo, x1hi, f_sthdth_dx3);
+      const double tcth = romb(x1lo, x1hi, f_cthdth_dx2);
+      const double c000 = ri_r2d2r / vrf;
+      const double c011 = -(ri_r3 / vrf) * (th3 / vthf);
+      const double c101 = ri_rdr2 / vrf;
+      const double c110 = c101, c202 = c101, c220 = c202;
+      const double c212 = tcth / vthf, c221 = c212;
+      const double c022 = -c220 * G(G3_GCOV + 2, i, j) / G(G3_GCOV + 0, i, j);
+      const double c122 = -c221 * G(G3_GCOV + 2, i, j) / G(G3_GCOV + 1, i, j);
+      double dA;
+      if (DK(i, j + 1) < DK(i, j)) dA = G(G3_A1, i, j + 1) + G(G3_A1, i, j + 1);
+      else if (DK(i, j + 1) > DK(i, j)) dA = 0.5 * G(G3_A1, i, j + 1);
+      else dA = G(G3_A1, i, j + 1);
+      dA -= G(G3_A1, i, j);
+      const double dV = G(G3_VOL, i, j);
+      const double c111 = dA / dV - c212;
+      G(G3_C000, i, j) = c000; G(G3_C011, i, j) = c011; G(G3_C022, i, j) = c022;
+      G(G3_C101, i, j) = c101; G(G3_C110, i, j) = c110; G(G3_C111, i, j) = c111;
+      G(G3_C122, i, j) = c122; G(G3_C202, i, j) = c202; G(G3_C220, i, j) = c220;
+      G(G3_C212, i, j) = c212; G(G3_C221, i, j) = c221;
+    }
+  }
 }
 
 }  // namespace mdg

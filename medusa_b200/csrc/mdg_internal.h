@@ -78,6 +78,7 @@ struct ProbDev {
   int floors;               // ENFORCE_FLOORS: u_to_p clamps rho and u to the floors below
   int grav_on;              // GRAV=FIXED_GRAV: the fixed acceleration grav[] is applied
   int64_t cell_off;         // first zone of this problem in the state arrays
+  int64_t ncell;            // interior zones (n1*n2 on 1-D/2-D grids; the dendritic count in 3-D)
   int64_t geo_off;          // first record (i=-NG) in the 1-D geometry tables
   int64_t rc1_off;          // first record (j=-NG) of the direction-1 recon table (2-D)
   int64_t sh_off;           // first byte of the first-stage shock bits (2-D)

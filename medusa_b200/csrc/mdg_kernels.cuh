@@ -1,6 +1,7 @@
 // Shared declarations of the sweep kernels and their launch helpers.
 #pragma once
 #include <cuda_runtime.h>
+#include <string>
 #include "mdg_internal.h"
 
 namespace mdg {
@@ -67,6 +68,15 @@ void launch_conserved_totals(const ProbDev *probs, int nprob, const Tables &tb, 
 // from closed-form moments (the mixed-precision sweep's tables), at columns geo_off..+n1+3.
 void launch_build_tables_1d(const ProbDev *probs, int m, int n1, double *rc, double *geo, float *mx,
                             int64_t stride, cudaStream_t st);
+// 3-D dendritic spherical sweep (mdg_sweep3d.cu): one problem, in slot 0.
+struct Sweep3;
+int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why);
+void sweep3_destroy(Sweep3 *w);
+int64_t sweep3_ncell(const Sweep3 *w);
+void launch_stage3d(int stage, Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA stage_state,
+                    StateSoA state_n, StateSoA out, cudaStream_t st);
+void launch_initial_estimate3(Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA s, cudaStream_t st);
+void launch_totals3(Sweep3 *w, StateSoA s, double *out, cudaStream_t st);
 void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st);
 void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
 void launch_reset_time(ProbTime *times, int m, cudaStream_t st);

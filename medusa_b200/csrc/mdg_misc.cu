@@ -66,7 +66,7 @@ __device__ __forceinline__ void initial_estimate_block(const ProbDev *__restrict
 {
   __shared__ double sred[32];
   const ProbDev &P = probs[m];
-  const int64_t ncell = (int64_t)P.n1 * P.n2;
+  const int64_t ncell = P.ncell;
   const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   double lmin = 1.0e300;
   if (z < ncell) {
@@ -102,7 +102,7 @@ __global__ void initial_estimate_many_kernel(const ProbDev *__restrict__ probs, 
 {
   const int m = m0 + blockIdx.y;
   const ProbDev &P = probs[m];
-  if ((int64_t)blockIdx.x * blockDim.x >= (int64_t)P.n1 * P.n2) return;
+  if ((int64_t)blockIdx.x * blockDim.x >= P.ncell) return;
   initial_estimate_block(probs, times, m, tb, s);
 }
 
@@ -181,7 +181,7 @@ __global__ void conserved_totals_kernel(const ProbDev *__restrict__ probs, Table
   const int m = blockIdx.x;
   const int t = threadIdx.x;
   const ProbDev &P = probs[m];
-  const int64_t n = (int64_t)P.n1 * P.n2;
+  const int64_t n = P.ncell;
   double ms = 0.0, mc = 0.0, es = 0.0, ec = 0.0;
   for (int64_t z = t; z < n; z += blockDim.x) {
     const int64_t c = P.cell_off + z;

@@ -138,6 +138,7 @@ extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double
   memset(&P, 0, sizeof P);
   P.ndim = 1; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
   P.n1 = n1; P.n2 = 1;
+  P.ncell = n1;
   P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0];
   P.prob_kind = d.prob_kind;
   P.has_src = (d.geom == MDG_SPHERICAL);

@@ -1,0 +1,903 @@
+// 3-D spherical sweep on the dendritic grid (plain FP64, the reference's operation order).
+//
+// prim_to_fluxes3 (step.c:1088-1430) visits every zone once and does, in that order, its
+// lower direction-0 face, its lower direction-1 face(s) and its lower direction-2 face;
+// push (step.c:327-478) then differences the stored face fluxes with the dendritic
+// fan-in.  Here each of the three face families is one kernel (one thread per face, the
+// faces of a row (i, j) in 128-face tiles), the fluxes go to HBM, and a fourth kernel
+// applies push() per zone.  What the serial order of the reference decides is kept:
+//
+//  * pencils.  A direction-0 face of zone (i, j, k) reads radial zones i-2 .. i+1 at the
+//    face's own (theta, phi) resolution: a finer row is restricted (volume-weighted mean,
+//    restrict0 step.c:1012-1051; its Gamma slot takes the zone's phi velocity, as
+//    restrict0 reads p[..][GAMMA] = p[..][U3]), a coarser or equal row is prolonged by
+//    limited slopes in phi and then theta (prolongate0/kslopes0, step.c:905-955, 782-840).
+//    Direction-1 faces restrict/prolong across phi-refinement steps (restrict1,
+//    prolongate1/kslopes1, step.c:1053-1085, 957-1010, 842-900).
+//  * boundaries.  Ghost zones are not stored: a read of a ghost zone is mapped to the
+//    interior zone reset_boundaries_gpu copies into it (bc.c:705-1422, i-boundaries on
+//    interior (j, k), j-boundaries on interior (i, k), k-boundaries on interior (i, j));
+//    ghost zones that no boundary loop writes (corners) hold zeros, as the zero-filled
+//    allocation does (utils.c:164-174).
+//  * shock flags.  A direction-1 or -2 face uses HLLE next to a direction-0 shock
+//    (transverse_shock, fluid.c:189-210) with the flags the serial loop has set when it
+//    reaches the face: ghost flags are always "shock" (never reset), the current stage
+//    contributes only the zone's own direction-0 face (marks from rows i+1, i+2 come
+//    later in the loop), and in the second stage every first-stage mark counts
+//    (set_shock_flag(0) resets once per step).  own[c]: zone c's own face in the current
+//    stage; all0[c]: any first-stage mark of zone c (faces i, i+1, i+2 map down to it).
+//  * the polar-axis fix (step.c:1301-1401): on the last theta row of every radial row
+//    the phi-face states are the zone values with the velocity rotated through
+//    Cartesian components (host tables of the sines and cosines).
+#include "mdg_hydro.cuh"
+#include "mdg_kernels.cuh"
+#include "mdg_grid3d.cuh"
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace mdg {
+
+struct Tile3 { int i, j, k0, cnt; };
+constexpr int NT3 = 128;
+
+__device__ __forceinline__ int rowi(const Grid3 &g, int i, int j) { return __ldg(g.rowbase + i + NG) + j + NG; }
+__device__ __forceinline__ int nj_of(const Grid3 &g, int i) { return __ldg(g.nj + i + NG); }
+__device__ __forceinline__ int djs(const Grid3 &g, int i) { return g.n2 / nj_of(g, i); }
+__device__ __forceinline__ int nk_of(const Grid3 &g, int i, int j) { return __ldg(g.nk + rowi(g, i, j)); }
+__device__ __forceinline__ int dks(const Grid3 &g, int i, int j) { return g.n3 / nk_of(g, i, j); }
+__device__ __forceinline__ double geo3(const Grid3 &g, int f, int ij) { return __ldg(g.geo + (int64_t)f * g.nij + ij); }
+__device__ __forceinline__ double minmod(double a, double b)
+{
+  // MINMOD, decs.h:629-630
+  return 0.5 * ((a < 0.0 ? -1.0 : 1.0) + (b < 0.0 ? -1.0 : 1.0)) * (fabs(a) < fabs(b) ? fabs(a) : fabs(b));
+}
+
+// Interior zone that reset_boundaries_gpu copies into zone (i, j, k), with the velocity
+// components it negates (bit v set: component v flips sign); -1: a zone no boundary
+// loop writes (zero).
+__device__ int64_t locate3(const Grid3 &g, int i, int j, int k, int &flip)
+{
+  flip = 0;
+  const int n1 = g.n1;
+  const bool ig = (i < 0 || i >= n1);
+  const int nji = nj_of(g, i);
+  const bool jg = (j < 0 || j >= nji);
+  const int nkr = nk_of(g, i, j);
+  const bool kg = (k < 0 || k >= nkr);
+  int ip = i, jp = j, kp = k;
+  if (!ig && !jg && !kg) return __ldg(g.cell + rowi(g, i, j)) + k;
+  if (ig && !jg && !kg) {
+    if (i < 0) {
+      ip = -1 - i;
+      if (g.bc_lo0 == BC_SPHERICAL_ORIGIN) {
+        const int njp = g.n2 / djs(g, ip);
+        jp = njp - 1 - j;
+        const int nkp = g.n3 / dks(g, ip, jp);
+        kp = (k + nkp / 2) % nkp;
+        flip = (1 << U1) | (1 << U3);
+      } else {   // REFLECT
+        jp = j * djs(g, i) / djs(g, ip);
+        kp = k * dks(g, i, j) / dks(g, ip, jp);
+        flip = 1 << U1;
+      }
+    } else {
+      if (g.bc_hi0 == BC_REFLECT) {
+        ip = 2 * n1 - i - 1;
+        flip = 1 << U1;
+      } else {   // OUTFLOW
+        ip = n1 - 1;
+      }
+    }
+  } else if (!ig && jg && !kg) {
+    const int bc = (j < 0) ? g.bc_lo1 : g.bc_hi1;
+    if (bc == BC_OUTFLOW) {
+      jp = (j < 0) ? 0 : nji - 1;
+    } else {
+      jp = (j < 0) ? -1 - j : 2 * nji - 1 - j;
+      if (bc == BC_SPHERICAL_ORIGIN) {
+        const int nkp = g.n3 / dks(g, i, jp);
+        kp = (k + nkp / 2) % nkp;
+        flip = (1 << U2) | (1 << U3);
+      } else {   // REFLECT
+        kp = k * dks(g, i, j) / dks(g, i, jp);
+        flip = 1 << U2;
+      }
+    }
+  } else if (!ig && !jg && kg) {
+    const int bc = (k < 0) ? g.bc_lo2 : g.bc_hi2;
+    if (bc == BC_PERIODIC) {
+      kp = (k < 0) ? k + nkr : k - nkr;
+    } else {
+      kp = (k < 0) ? 0 : nkr - 1;
+      if (bc == BC_REFLECT) flip = 1 << U3;
+    }
+  } else {
+    return -1;
+  }
+  // a source outside the interior (boundary kinds that assume no refinement next to the
+  // boundary, used on a grid that has some there) reads as an unwritten zone
+  if (ip < 0 || ip >= n1 || jp < 0 || jp >= nj_of(g, ip) || kp < 0 || kp >= nk_of(g, ip, jp)) return -1;
+  return __ldg(g.cell + rowi(g, ip, jp)) + kp;
+}
+
+// Zone (i, j, k) as the pencils see it: primitives, PRESS and GAMMA of its EOS record
+// (update_eos / update_eos_ghost fill every zone, eos.c:4-34).
+__device__ __forceinline__ void load7(const Grid3 &g, const ProbDev &P, const StateSoA &s, int i, int j, int k,
+                                      double *w)
+{
+  int flip;
+  const int64_t c = locate3(g, i, j, k, flip);
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) {
+    double x = (c >= 0) ? s.v[v][c] : 0.0;
+    w[v] = ((flip >> v) & 1) ? -x : x;
+  }
+  w[5] = eos_press(P.eos, P.gam, P.Kpoly, w[RHO], w[UU]);
+  w[6] = P.gam;
+}
+
+// kslopes0 / kslopes1: limited phi slope of row (ii, jj) evaluated at the centroid x2p.
+__device__ void kslope_point(const Grid3 &g, const ProbDev &P, const StateSoA &s, int ii, int jj, int kk,
+                             double x2p, double *pp)
+{
+  const int lev = ilog2(dks(g, ii, jj));
+  const int base = g.rc2_base[lev] + NG;
+  const double x20 = __ldg(g.xc2 + base + kk - 1), x21 = __ldg(g.xc2 + base + kk), x22 = __ldg(g.xc2 + base + kk + 1);
+  const double idx2m = 1.0 / (x21 - x20), idx2p = 1.0 / (x22 - x21), idx2c = 1.0 / (x22 - x20);
+  double a[7], b[7], c[7];
+  load7(g, P, s, ii, jj, kk - 1, a);
+  load7(g, P, s, ii, jj, kk, b);
+  load7(g, P, s, ii, jj, kk + 1, c);
+#pragma unroll
+  for (int v = 0; v < 7; v++) {
+    const double sm = (b[v] - a[v]) * idx2m;
+    const double sp = (c[v] - b[v]) * idx2p;
+    const double sc = (c[v] - a[v]) * idx2c;
+    const double sg = minmod(2.0 * minmod(sm, sp), sc);
+    pp[v] = b[v] + sg * (x2p - x21);
+  }
+}
+
+// Pencil entry of radial row ii for the direction-0 face of zone (i, j, k).
+__device__ void pencil0(const Grid3 &g, const ProbDev &P, const StateSoA &s, int i, int j, int k, int ii, double *pp)
+{
+  const int dji = djs(g, i), djii = djs(g, ii);
+  if (djii < dji) {
+    // restrict0 (step.c:1012-1051)
+    const int njp = dji / djii, jp = j * njp;
+    const int dkij = dks(g, i, j);
+    double vol_sum = 0.0;
+    for (int jj = jp; jj < jp + njp; jj++) {
+      const int nkp = dkij / dks(g, ii, jj);
+      const double vol = geo3(g, G3_VOL, rowi(g, ii, jj));
+      for (int kk = k * nkp; kk < k * nkp + nkp; kk++) vol_sum += vol;
+    }
+    vol_sum = 1.0 / vol_sum;
+#pragma unroll
+    for (int v = 0; v < 7; v++) pp[v] = 0.0;
+    for (int jj = jp; jj < jp + njp; jj++) {
+      const int nkp = dkij / dks(g, ii, jj);
+      const double vol = geo3(g, G3_VOL, rowi(g, ii, jj));
+      for (int kk = k * nkp; kk < k * nkp + nkp; kk++) {
+        const double vol_frac = vol * vol_sum;
+        double w[7];
+        load7(g, P, s, ii, jj, kk, w);
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) pp[v] += w[v] * vol_frac;
+        pp[5] += w[5] * vol_frac;
+        pp[6] += w[U3] * vol_frac;   // p[..][GAMMA], GAMMA = 4 (decs.h:661)
+      }
+    }
+    return;
+  }
+  // prolongate0 (step.c:905-955)
+  const int jj = j * dji / djii;
+  const double x1p = __ldg(g.xc1 + g.rc1_base[ilog2(dji)] + NG + j);
+  const double x2p = __ldg(g.xc2 + g.rc2_base[ilog2(dks(g, i, j))] + NG + k);
+  const int dkij = dks(g, i, j);
+  double p0[7], p1[7], p2[7];
+  kslope_point(g, P, s, ii, jj - 1, k * dkij / dks(g, ii, jj - 1), x2p, p0);
+  kslope_point(g, P, s, ii, jj, k * dkij / dks(g, ii, jj), x2p, p1);
+  kslope_point(g, P, s, ii, jj + 1, k * dkij / dks(g, ii, jj + 1), x2p, p2);
+  const int base = g.rc1_base[ilog2(djii)] + NG;
+  const double x10 = __ldg(g.xc1 + base + jj - 1), x11 = __ldg(g.xc1 + base + jj), x12 = __ldg(g.xc1 + base + jj + 1);
+  const double idx1m = 1.0 / (x11 - x10), idx1p = 1.0 / (x12 - x11), idx1c = 1.0 / (x12 - x10);
+#pragma unroll
+  for (int v = 0; v < 7; v++) {
+    const double sm = (p1[v] - p0[v]) * idx1m;
+    const double sp = (p2[v] - p1[v]) * idx1p;
+    const double sc = (p2[v] - p0[v]) * idx1c;
+    const double sg = minmod(2.0 * minmod(sm, sp), sc);
+    pp[v] = p1[v] + sg * (x1p - x11);
+  }
+}
+
+// Pencil entry of theta row jj for the direction-1 sub-face kk of face row (i, j).
+__device__ void pencil1(const Grid3 &g, const ProbDev &P, const StateSoA &s, int i, int j, int kk, int jj,
+                        double *pp)
+{
+  const int dkj = dks(g, i, j), dkjm = dks(g, i, j - 1);
+  const int mn = dkj < dkjm ? dkj : dkjm;
+  const int dkjj = dks(g, i, jj);
+  if (dkjj < mn) {
+    // restrict1 (step.c:1053-1085)
+    const int nkp = mn / dkjj, kp = kk * nkp;
+    const double vol = geo3(g, G3_VOL, rowi(g, i, jj));
+    double vol_sum = 0.0;
+    for (int k = kp; k < kp + nkp; k++) vol_sum += vol;
+    vol_sum = 1.0 / vol_sum;
+#pragma unroll
+    for (int v = 0; v < 7; v++) pp[v] = 0.0;
+    for (int k = kp; k < kp + nkp; k++) {
+      const double vol_frac = vol * vol_sum;
+      double w[7];
+      load7(g, P, s, i, jj, k, w);
+#pragma unroll
+      for (int v = 0; v < 7; v++) pp[v] += w[v] * vol_frac;
+    }
+    return;
+  }
+  // prolongate1 (step.c:957-1010)
+  const int k2 = kk * mn / dkjj;
+  if (mn == dkjj) {
+    load7(g, P, s, i, jj, k2, pp);
+    return;
+  }
+  const double x2p = __ldg(g.xc2 + g.rc2_base[ilog2(mn)] + NG + kk);
+  kslope_point(g, P, s, i, jj, k2, x2p, pp);
+}
+
+// Wave-speed estimate with per-side Gamma (riemann.c:368-429 / 210-303): the pencils of
+// the dendritic grid can carry a reconstructed Gamma slot that differs between sides.
+__device__ __forceinline__ void wave_speeds_g(const double *pl, const double *pr, double u_l, double u_r, bool hlle,
+                                              double &sl, double &sr, double &ss, double &p_s, int &isshock)
+{
+  const double p_l = pl[5], p_r = pr[5], G_l = pl[6], G_r = pr[6];
+  const double cs_l = sqrt(G_l * p_l / pl[RHO]);
+  const double cs_r = sqrt(G_r * p_r / pr[RHO]);
+  double p_max, p_min;
+  if (p_l > p_r) { p_max = p_l; p_min = p_r; } else { p_max = p_r; p_min = p_l; }
+  const double pratio = p_max / p_min;
+  isshock = ((p_max - p_min) / p_min > 0.5) ? 1 : 0;
+  p_s = 0.5 * (p_l + p_r) - 0.125 * (u_r - u_l) * (pl[RHO] + pr[RHO]) * (cs_l + cs_r);
+  if (hlle) p_s = (p_s > 0.0) ? p_s : 0.0;
+  else p_s = (0.0 > p_s) ? 0.0 : p_s;
+  if (pratio < 2.0 && p_s >= p_min && p_s <= p_max) {
+  } else if (p_s < p_min) {
+    const double G_avg = 0.5 * (G_l + G_r);
+    const double plr = pow(p_l / p_r, (G_avg - 1.0) / (2.0 * G_avg));
+    const double s0 = (plr * u_l / cs_l + u_r / cs_r + 2.0 * (plr - 1.0) / (G_avg - 1.0)) / (plr / cs_l + 1.0 / cs_r);
+    p_s = 0.5 * (p_l * pow(1.0 + (G_l - 1.0) / (2.0 * cs_l) * (u_l - s0), 2.0 * G_l / (G_l - 1.0))
+               + p_r * pow(1.0 + (G_r - 1.0) / (2.0 * cs_r) * (s0 - u_r), 2.0 * G_r / (G_r - 1.0)));
+    p_s = (p_s > 0.0) ? p_s : 0.0;
+  } else {
+    const double a_l = 2.0 / ((G_l + 1.0) * pl[RHO]);
+    const double a_r = 2.0 / ((G_r + 1.0) * pr[RHO]);
+    const double b_l = (G_l - 1.0) / (G_l + 1.0) * p_l;
+    const double b_r = (G_r - 1.0) / (G_r + 1.0) * p_r;
+    const double g_l = sqrt(a_l / (p_s + b_l));
+    const double g_r = sqrt(a_r / (p_s + b_r));
+    p_s = (g_l * p_l + g_r * p_r - (u_r - u_l)) / (g_l + g_r);
+    p_s = (p_s > 0.0) ? p_s : 0.0;
+  }
+  const double q_l = (p_s <= p_l) ? 1.0 : sqrt(1.0 + (G_l + 1.0) / (2.0 * G_l) * (p_s / p_l - 1.0));
+  const double q_r = (p_s <= p_r) ? 1.0 : sqrt(1.0 + (G_r + 1.0) / (2.0 * G_r) * (p_s / p_r - 1.0));
+  sl = u_l - cs_l * q_l;
+  sr = u_r + cs_r * q_r;
+  ss = (p_r - p_l + pl[RHO] * u_l * (sl - u_l) - pr[RHO] * u_r * (sr - u_r))
+     / (pl[RHO] * (sl - u_l) - pr[RHO] * (sr - u_r));
+}
+
+// riemann_flux_HLLC (riemann.c:328-499) with per-side Gamma; returns isshock.
+template <int DIR>
+__device__ int hllc3(const double *pl, const double *pr, const FaceGeom<double> &g, double *flux, double &sig)
+{
+  int isshock = 0;
+  if (g.area < 1.0e-16) {
+    sig = 1.0e-200;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) flux[v] = 0.0;
+    return isshock;
+  }
+  const double sc = g.scale;
+  const double u_l = pl[U1 + DIR] * sc, u_r = pr[U1 + DIR] * sc;
+  double sl, sr, ss, p_s;
+  wave_speeds_g(pl, pr, u_l, u_r, false, sl, sr, ss, p_s, isshock);
+  if (ss > sr) sr = 1.001 * ss;
+  if (ss < sl) sl = 1.001 * ss;
+  sig = tmax(fabs(sl), fabs(sr)) / sc;
+  if (sl > 0.0) { pflux<DIR, false, double>(pl, pl[5], g, flux); return isshock; }
+  if (sr < 0.0) { pflux<DIR, false, double>(pr, pr[5], g, flux); return isshock; }
+  double u[NPRIM], fx[NPRIM], Us[NPRIM], pk[6];
+  const bool left = ss > 0.0;
+#pragma unroll
+  for (int v = 0; v < 6; v++) pk[v] = left ? pl[v] : pr[v];
+  const double sk = left ? sl : sr;
+  const double uk = left ? u_l : u_r;
+  p_uflux<DIR, false, double>(pk, g, pk[5], u, fx);
+  Us[0] = pk[RHO] * (sk - uk) / (sk - ss);
+  Us[UU] = (u[UU] * (sk - uk) - pk[5] * uk + p_s * ss) / (sk - ss);
+  Us[U1] = pk[U1]; Us[U2] = pk[U2]; Us[U3] = pk[U3];
+  Us[U1 + DIR] = ss / sc;
+  const double slr = sk / sc;
+  const double vc0 = g.g0 * Us[U1], vc1 = g.g1 * Us[U2], vc2 = g.g2 * Us[U3];
+  Us[U1] = vc0 * Us[0]; Us[U2] = vc1 * Us[0]; Us[U3] = vc2 * Us[0];
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) flux[v] = g.area * (fx[v] + slr * (Us[v] - u[v]));
+  return isshock;
+}
+
+// riemann_flux_HLLE (riemann.c:178-325) with per-side Gamma.
+template <int DIR>
+__device__ void hlle3(const double *pl, const double *pr, const FaceGeom<double> &g, double *flux, double &sig)
+{
+  if (g.area < 1.0e-16) {
+    sig = 1.0e-200;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) flux[v] = 0.0;
+    return;
+  }
+  const double sc = g.scale;
+  const double u_l = pl[U1 + DIR] * sc, u_r = pr[U1 + DIR] * sc;
+  double sl, sr, ss, p_s;
+  int isshock;
+  wave_speeds_g(pl, pr, u_l, u_r, true, sl, sr, ss, p_s, isshock);
+  double ul[NPRIM], ur[NPRIM], fl[NPRIM], fr[NPRIM];
+  p_uflux<DIR, false, double>(pl, g, pl[5], ul, fl);
+  p_uflux<DIR, false, double>(pr, g, pr[5], ur, fr);
+  const double cmax = tmax(sr / sc, 0.0);
+  const double cmin = fabs(tmin(sl / sc, 0.0));
+  sig = tmax(cmax, cmin);
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++)
+    flux[v] = g.area * (cmin * fr[v] + cmax * fl[v] - cmax * cmin * (ur[v] - ul[v])) / (cmax + cmin);
+}
+
+// Face geometry of direction d on row (i, j): area[d], scale[1+d][d], gcov[1+d][0..2].
+template <int DIR>
+__device__ __forceinline__ FaceGeom<double> face_geom3(const Grid3 &g, int ij)
+{
+  FaceGeom<double> f;
+  f.area = geo3(g, G3_A0 + DIR, ij);
+  f.scale = geo3(g, G3_SCALE + 3 * (1 + DIR) + DIR, ij);
+  f.g0 = geo3(g, G3_GCOV + 3 * (1 + DIR) + 0, ij);
+  f.g1 = geo3(g, G3_GCOV + 3 * (1 + DIR) + 1, ij);
+  f.g2 = geo3(g, G3_GCOV + 3 * (1 + DIR) + 2, ij);
+  return f;
+}
+
+// Right face value of pencil zone 1 and left face value of pencil zone 2 (interp() on a
+// 4-zone pencil, reconstruct.c:225-279), reconstruction columns c1, c2 of table rc.
+__device__ __forceinline__ void recon_face(int order, const double pen[4][7], const double *rc, int64_t stride,
+                                           int64_t c1, int64_t c2, double *pl, double *pr)
+{
+  const RcView<double, true> g1{rc + c1, stride}, g2{rc + c2, stride};
+#pragma unroll
+  for (int v = 0; v < 7; v++) {
+    double al, ar;
+    recon_zone<double>(order, pen[0][v], pen[1][v], pen[2][v], g1, al, ar);
+    pl[v] = ar;
+    recon_zone<double>(order, pen[1][v], pen[2][v], pen[3][v], g2, al, ar);
+    pr[v] = al;
+  }
+}
+
+
+// Flag of zone (i, jj, kc) as transverse_shock reads it at this point of the serial loop.
+template <int STAGE>
+__device__ __forceinline__ bool flag_shock(const Grid3 &g, int i, int jj, int kc, const unsigned char *own,
+                                           const unsigned char *all0)
+{
+  if (jj < 0 || jj >= nj_of(g, i)) return true;
+  if (kc < 0 || kc >= nk_of(g, i, jj)) return true;
+  const int64_t c = __ldg(g.cell + rowi(g, i, jj)) + kc;
+  return own[c] != 0 || (STAGE == 1 && all0[c] != 0);
+}
+
+// Direction-0 faces: face (i, j, k) is the lower radial face of zone (i, j, k), i in [0, n1].
+template <int STAGE>
+__global__ void __launch_bounds__(NT3) face0_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                                                     Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
+                                                     double *__restrict__ flux, unsigned char *__restrict__ own,
+                                                     unsigned char *__restrict__ all0)
+{
+  __shared__ double sred[32];
+  if (times[0].done) return;
+  const ProbDev &P = probs[0];
+  const Tile3 t = tiles[blockIdx.x];
+  const int i = t.i, j = t.j, k = t.k0 + (int)threadIdx.x;
+  double lmin = 1.0e300;
+  if ((int)threadIdx.x < t.cnt) {
+    double pen[4][7];
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) pencil0(g, P, s, i, j, k, i - 2 + q, pen[q]);
+    double pl[7], pr[7];
+    recon_face(P.interp_order, pen, g.rc0, g.n1 + 2 * NG, i - 1 + NG, i + NG, pl, pr);
+    const int ij = rowi(g, i, j);
+    double fl[NPRIM], ss;
+    const int isshock = hllc3<0>(pl, pr, face_geom3<0>(g, ij), fl, ss);
+    const int64_t f = __ldg(g.f0 + ij) + k;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) flux[v * g.nf0 + f] = fl[v];
+    if (i < g.n1) own[__ldg(g.cell + ij) + k] = (unsigned char)isshock;
+    if (STAGE == 0 && isshock) {
+      // shock marks of the zone and of the two zones inside it (step.c:1196-1204)
+      if (i < g.n1) all0[__ldg(g.cell + ij) + k] = 1;
+      for (int d = 1; d <= 2; d++) {
+        const int im = i - d;
+        if (im < 0) break;
+        const int jm = j * djs(g, i) / djs(g, im);
+        const int km = k * dks(g, i, j) / dks(g, im, jm);
+        all0[__ldg(g.cell + rowi(g, im, jm)) + km] = 1;
+      }
+    }
+    lmin = g.dx0 / fabs(ss);
+  }
+  block_min_to(lmin, &times[0].minacc, sred);
+}
+
+// Direction-1 faces: sub-face kk of face row (i, j), j in [0, nj(i)] (step.c:1212-1265).
+template <int STAGE>
+__global__ void __launch_bounds__(NT3) face1_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                                                     Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
+                                                     double *__restrict__ flux, const unsigned char *__restrict__ own,
+                                                     const unsigned char *__restrict__ all0)
+{
+  __shared__ double sred[32];
+  if (times[0].done) return;
+  const ProbDev &P = probs[0];
+  const Tile3 t = tiles[blockIdx.x];
+  const int i = t.i, j = t.j, kk = t.k0 + (int)threadIdx.x;
+  double lmin = 1.0e300;
+  if ((int)threadIdx.x < t.cnt) {
+    double pen[4][7];
+#pragma unroll 1
+    for (int q = 0; q < 4; q++) pencil1(g, P, s, i, j, kk, j - 2 + q, pen[q]);
+    double pl[7], pr[7];
+    const int64_t base = g.rc1_base[ilog2(djs(g, i))] + NG;
+    recon_face(P.interp_order, pen, g.rc1, g.cols1, base + j - 1, base + j, pl, pr);
+    // zone k of row j that owns the sub-face, and the transverse_shock test of zone k
+    const int dkj = dks(g, i, j), dkjm = dks(g, i, j - 1);
+    const int mn = dkj < dkjm ? dkj : dkjm;
+    const int k = kk / (dkj / mn);
+    const int nkm = dkj / dkjm;
+    bool hlle = flag_shock<STAGE>(g, i, j, k, own, all0);
+    for (int q = k * nkm; q < k * nkm + nkm; q++) hlle = hlle || flag_shock<STAGE>(g, i, j - 1, q, own, all0);
+    const int ij = rowi(g, i, j);
+    const FaceGeom<double> fg = face_geom3<1>(g, ij);
+    double fl[NPRIM], ss;
+    if (hlle) hlle3<1>(pl, pr, fg, fl, ss);
+    else hllc3<1>(pl, pr, fg, fl, ss);
+    const int64_t f = __ldg(g.f1 + ij) + kk;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) flux[v * g.nf1 + f] = fl[v];
+    lmin = djs(g, i) * g.dx1 / fabs(ss);
+  }
+  block_min_to(lmin, &times[0].minacc, sred);
+}
+
+// Direction-2 faces: face k in [0, nk] of row (i, j) (step.c:1267-1425), with the
+// polar-axis fix on the last theta row.
+template <int STAGE>
+__global__ void __launch_bounds__(NT3) face2_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                                                     Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
+                                                     double *__restrict__ flux, const unsigned char *__restrict__ own,
+                                                     const unsigned char *__restrict__ all0)
+{
+  __shared__ double sred[32];
+  if (times[0].done) return;
+  const ProbDev &P = probs[0];
+  const Tile3 t = tiles[blockIdx.x];
+  const int i = t.i, j = t.j, k = t.k0 + (int)threadIdx.x;
+  double lmin = 1.0e300;
+  if ((int)threadIdx.x < t.cnt) {
+    const int ij = rowi(g, i, j);
+    const int dk = dks(g, i, j);
+    const int64_t base = g.rc2_base[ilog2(dk)] + NG;
+    double pl[7], pr[7];
+    if (j == nj_of(g, i) - 1) {
+      // polar-axis fix: zone values, velocity rotated at the shared phi face
+      const int64_t b1 = g.rc1_base[ilog2(djs(g, i))] + NG + j;
+      const double sth = __ldg(g.sth + b1), cth = __ldg(g.cth + b1);
+      double s0[3], s3[3];
+#pragma unroll
+      for (int m = 0; m < 3; m++) {
+        s0[m] = geo3(g, G3_SCALE + m, ij);
+        s3[m] = geo3(g, G3_SCALE + 9 + m, ij);
+      }
+      const double sphf = __ldg(g.sphl + base + k), cphf = __ldg(g.cphl + base + k);
+      for (int side = 0; side < 2; side++) {
+        const int kt = k - 1 + side;
+        double w[7];
+        load7(g, P, s, i, j, kt, w);
+        const double sph = __ldg(g.sphc + base + kt), cph = __ldg(g.cphc + base + kt);
+        double lam[3][3] = {{sth * cph, cth * cph, -sph}, {sth * sph, cth * sph, cph}, {cth, -sth, 0.0}};
+        double v[3];
+        for (int l = 0; l < 3; l++) {
+          v[l] = 0.0;
+          for (int m = 0; m < 3; m++) v[l] += lam[l][m] * w[U1 + m] * s0[m];
+        }
+        double lf[3][3] = {{sth * cphf, cth * cphf, -sphf}, {sth * sphf, cth * sphf, cphf}, {cth, -sth, 0.0}};
+        double *o = side ? pr : pl;
+#pragma unroll
+        for (int q = 0; q < 7; q++) o[q] = w[q];
+        for (int l = 0; l < 3; l++) {
+          o[U1 + l] = 0.0;
+          for (int m = 0; m < 3; m++) o[U1 + l] += lf[m][l] * v[m] / s3[l];
+        }
+      }
+    } else {
+      double pen[4][7];
+#pragma unroll 1
+      for (int q = 0; q < 4; q++) load7(g, P, s, i, j, k - 2 + q, pen[q]);
+      recon_face(P.interp_order, pen, g.rc2, g.cols2, base + k - 1, base + k, pl, pr);
+    }
+    const bool hlle = flag_shock<STAGE>(g, i, j, k, own, all0) || flag_shock<STAGE>(g, i, j, k - 1, own, all0);
+    const FaceGeom<double> fg = face_geom3<2>(g, ij);
+    double fl[NPRIM], ss;
+    if (hlle) hlle3<2>(pl, pr, fg, fl, ss);
+    else hllc3<2>(pl, pr, fg, fl, ss);
+    const int64_t f = __ldg(g.f2 + ij) + k;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) flux[v * g.nf2 + f] = fl[v];
+    lmin = dk * g.dx2 / fabs(ss);
+  }
+  block_min_to(lmin, &times[0].minacc, sred);
+}
+
+// push() for zone (i, j, k) (step.c:327-478) with the dendritic flux fan-in, the
+// geometric sources of the stage state (rad_fluid.c:164-192, fluid.c:56-73) and, in the
+// second stage, the zone terms of the next estimate_dt (step.c:177-187).
+template <int STAGE>
+__global__ void __launch_bounds__(NT3) push3_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                                                     Grid3 g, const Tile3 *__restrict__ tiles, StateSoA sst,
+                                                     StateSoA sn, StateSoA out, const double *__restrict__ F0,
+                                                     const double *__restrict__ F1, const double *__restrict__ F2)
+{
+  __shared__ double sred[32];
+  if (times[0].done) return;
+  const ProbDev &P = probs[0];
+  const double dt = times[0].dt;
+  const Tile3 t = tiles[blockIdx.x];
+  const int i = t.i, j = t.j, k = t.k0 + (int)threadIdx.x;
+  double lmin = 1.0e300, lmax = 0.0;
+  if ((int)threadIdx.x < t.cnt) {
+    const int ij = rowi(g, i, j);
+    const int64_t c = __ldg(g.cell + ij) + k;
+    double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM], divF[NPRIM], pf[NPRIM];
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) ph[v] = sst.v[v][c];
+    if (STAGE == 0) {
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
+    } else {
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][c];
+    }
+    const double g0 = geo3(g, G3_GCOV + 0, ij), g1 = geo3(g, G3_GCOV + 1, ij), g2 = geo3(g, G3_GCOV + 2, ij);
+    const double press = eos_press(P.eos, P.gam, P.Kpoly, ph[RHO], ph[UU]);
+    {
+      // p_to_geom_src: src[U1+m] = sum_l sum_n T[l][n] conn[l][m][n] over the non-zero conn
+      const double vcov[3] = {g0 * ph[U1], g1 * ph[U2], g2 * ph[U3]};
+      double T[3][3];
+#pragma unroll
+      for (int l = 0; l < 3; l++) {
+#pragma unroll
+        for (int m = 0; m < 3; m++) T[l][m] = ph[RHO] * ph[U1 + m] * vcov[l];
+        T[l][l] += press;
+      }
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+      s0 += T[0][0] * geo3(g, G3_C000, ij);
+      s0 += T[1][1] * geo3(g, G3_C101, ij);
+      s0 += T[2][2] * geo3(g, G3_C202, ij);
+      s1 += T[0][1] * geo3(g, G3_C011, ij);
+      s1 += T[1][0] * geo3(g, G3_C110, ij);
+      s1 += T[1][1] * geo3(g, G3_C111, ij);
+      s1 += T[2][2] * geo3(g, G3_C212, ij);
+      s2 += T[0][2] * geo3(g, G3_C022, ij);
+      s2 += T[1][2] * geo3(g, G3_C122, ij);
+      s2 += T[2][0] * geo3(g, G3_C220, ij);
+      s2 += T[2][1] * geo3(g, G3_C221, ij);
+      src[RHO] = 0.0; src[UU] = 0.0; src[U1] = s0; src[U2] = s1; src[U3] = s2;
+    }
+    p_to_u(pn, u, g0, g1, g2);
+    p_to_u(ph, uh, g0, g1, g2);
+    lmin = dt_source_control(pn, u, src);
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) divF[v] = 0.0;
+    // direction 0: outer face(s) on row i+1, inner face
+    {
+      const int dji = djs(g, i), djo = djs(g, i + 1);
+      const int jp = j * dji / djo;
+      const int njp = (djo < dji) ? dji / djo : 1;
+      const int dkij = dks(g, i, j);
+      for (int jj = jp; jj < jp + njp; jj++) {
+        const int nkp = dkij / dks(g, i + 1, jj);
+        const int64_t fb = __ldg(g.f0 + rowi(g, i + 1, jj));
+        for (int kk = k * nkp; kk < k * nkp + nkp; kk++) {
+#pragma unroll
+          for (int v = 0; v < NPRIM; v++) divF[v] += F0[v * g.nf0 + fb + kk];
+        }
+      }
+      const int64_t fi = __ldg(g.f0 + ij) + k;
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) divF[v] -= F0[v * g.nf0 + fi];
+    }
+    // direction 1
+    {
+      const int dkj = dks(g, i, j), dkp = dks(g, i, j + 1), dkm = dks(g, i, j - 1);
+      const int64_t fo = __ldg(g.f1 + rowi(g, i, j + 1)), fin = __ldg(g.f1 + ij);
+      if (dkp > dkj) {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) divF[v] += 0.5 * F1[v * g.nf1 + fo + k];
+      } else if (dkp < dkj) {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) divF[v] += F1[v * g.nf1 + fo + 2 * k] + F1[v * g.nf1 + fo + 2 * k + 1];
+      } else {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) divF[v] += F1[v * g.nf1 + fo + k];
+      }
+      if (dkm < dkj) {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++)
+          divF[v] -= 0.5 * F1[v * g.nf1 + fin + 2 * k] + 0.5 * F1[v * g.nf1 + fin + 2 * k + 1];
+      } else {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) divF[v] -= F1[v * g.nf1 + fin + k];
+      }
+    }
+    // direction 2
+    {
+      const int64_t f2 = __ldg(g.f2 + ij) + k;
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) divF[v] += F2[v * g.nf2 + f2 + 1] - F2[v * g.nf2 + f2];
+    }
+    const double vol = geo3(g, G3_VOL, ij);
+    const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) {
+      const double ddt = divF[v] / vol - src[v];
+      u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
+    }
+    u_to_p(u, pf, geo3(g, G3_GCON + 0, ij), geo3(g, G3_GCON + 1, ij), geo3(g, G3_GCON + 2, ij), P.floors != 0,
+           P.rho_floor, P.e_floor);
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) out.v[v][c] = pf[v];
+    if (STAGE == 1) {
+      // next estimate_dt: velocity of the new state, sound speed of the stage state
+      const double cs = sqrt(P.gam * press / ph[RHO]);
+      double local_dt = 0.0;
+      local_dt += (fabs(pf[U1]) + cs / geo3(g, G3_SCALE + 0, ij)) / g.dx0;
+      lmin = tmin(lmin, 1.0 / local_dt);
+      local_dt += (fabs(pf[U2]) + cs / geo3(g, G3_SCALE + 1, ij)) / (g.dx1 * djs(g, i));
+      lmin = tmin(lmin, 1.0 / local_dt);
+      local_dt += (fabs(pf[U3]) + cs / geo3(g, G3_SCALE + 2, ij)) / (g.dx2 * dks(g, i, j));
+      lmin = tmin(lmin, 1.0 / local_dt);
+    }
+  }
+  (void)lmax;
+  block_min_to(lmin, &times[0].minacc, sred);
+}
+
+// First estimate_dt of the problem (step.c:171-187, the EOS of the state itself).
+__global__ void __launch_bounds__(NT3) estimate3_kernel(const ProbDev *__restrict__ probs,
+                                                         ProbTime *__restrict__ times, Grid3 g,
+                                                         const Tile3 *__restrict__ tiles, StateSoA s)
+{
+  __shared__ double sred[32];
+  const ProbDev &P = probs[0];
+  const Tile3 t = tiles[blockIdx.x];
+  const int i = t.i, j = t.j, k = t.k0 + (int)threadIdx.x;
+  double lmin = 1.0e300;
+  if ((int)threadIdx.x < t.cnt) {
+    const int ij = rowi(g, i, j);
+    const int64_t c = __ldg(g.cell + ij) + k;
+    const double rho = s.v[RHO][c], uu = s.v[UU][c];
+    const double cs = sqrt(P.gam * eos_press(P.eos, P.gam, P.Kpoly, rho, uu) / rho);
+    double local_dt = 0.0;
+    local_dt += (fabs(s.v[U1][c]) + cs / geo3(g, G3_SCALE + 0, ij)) / g.dx0;
+    lmin = tmin(lmin, 1.0 / local_dt);
+    local_dt += (fabs(s.v[U2][c]) + cs / geo3(g, G3_SCALE + 1, ij)) / (g.dx1 * djs(g, i));
+    lmin = tmin(lmin, 1.0 / local_dt);
+    local_dt += (fabs(s.v[U3][c]) + cs / geo3(g, G3_SCALE + 2, ij)) / (g.dx2 * dks(g, i, j));
+    lmin = tmin(lmin, 1.0 / local_dt);
+  }
+  block_min_to(lmin, &times[0].minacc, sred);
+}
+
+
+// Mass and total energy (utils.c:2337-2361, 2581-2612) with compensated sums: one CTA,
+// each thread over a fixed subset of the zone tiles, then the threads in order.
+__device__ __forceinline__ void neumaier3(double &s, double &c, double x)
+{
+  const double t = s + x;
+  if (fabs(s) >= fabs(x)) c += (s - t) + x;
+  else c += (x - t) + s;
+  s = t;
+}
+
+__global__ void __launch_bounds__(256) totals3_kernel(Grid3 g, const Tile3 *__restrict__ tiles, int ntiles,
+                                                       StateSoA s, double *__restrict__ out)
+{
+  __shared__ double sh[4][256];
+  const int t = threadIdx.x;
+  double ms = 0.0, mc = 0.0, es = 0.0, ec = 0.0;
+  for (int q = t; q < ntiles; q += blockDim.x) {
+    const Tile3 tl = tiles[q];
+    const int ij = rowi(g, tl.i, tl.j);
+    const double vol = geo3(g, G3_VOL, ij);
+    const double g0 = geo3(g, G3_GCOV + 0, ij), g1 = geo3(g, G3_GCOV + 1, ij), g2 = geo3(g, G3_GCOV + 2, ij);
+    for (int k = tl.k0; k < tl.k0 + tl.cnt; k++) {
+      const int64_t c = __ldg(g.cell + ij) + k;
+      double p[NPRIM], u[NPRIM];
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) p[v] = s.v[v][c];
+      p_to_u(p, u, g0, g1, g2);
+      neumaier3(ms, mc, p[RHO] * vol);
+      neumaier3(es, ec, u[UU] * vol);
+    }
+  }
+  sh[0][t] = ms; sh[1][t] = mc; sh[2][t] = es; sh[3][t] = ec;
+  __syncthreads();
+  if (t == 0) {
+    double S = 0.0, C = 0.0, E = 0.0, D = 0.0;
+    for (int k = 0; k < (int)blockDim.x; k++) {
+      neumaier3(S, C, sh[0][k]); C += sh[1][k];
+      neumaier3(E, D, sh[2][k]); D += sh[3][k];
+    }
+    out[0] = S + C;
+    out[1] = E + D;
+  }
+}
+
+// ------------------------------------------------------------------------ host driver
+
+void build_grid3(const mdg_problem_desc &d, Grid3Host &h);
+
+struct Sweep3 {
+  Grid3 g{};
+  char *d_tab = nullptr;           // all grid tables in one allocation
+  double *d_flux = nullptr;        // F0 | F1 | F2, 5 arrays each
+  unsigned char *d_bits = nullptr; // own0 | own1 | all0, one byte per zone each
+  Tile3 *d_tiles = nullptr;        // face0 | face1 | face2 | zone tiles
+  int nt[4] = {0, 0, 0, 0};
+  int64_t ncell = 0;
+};
+
+static void tiles_of_rows(std::vector<Tile3> &out, int i, int j, int count)
+{
+  for (int k0 = 0; k0 < count; k0 += NT3) out.push_back(Tile3{i, j, k0, (count - k0 < NT3) ? count - k0 : NT3});
+}
+
+int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
+{
+  *out = nullptr;
+  Grid3Host h;
+  build_grid3(d, h);
+  if (h.nlev1 > G3_MAXLEV || h.nlev2 > G3_MAXLEV) { why = "too many refinement levels"; return MDG_ERR_INVALID; }
+  Sweep3 *w = new Sweep3();
+  w->ncell = h.ncell;
+  // one allocation for every table, each part 256-byte aligned
+  std::vector<std::pair<const void *, size_t>> parts = {
+      {h.nj.data(), h.nj.size() * sizeof(int)},         {h.rowbase.data(), h.rowbase.size() * sizeof(int)},
+      {h.nk.data(), h.nk.size() * sizeof(int)},         {h.cell.data(), h.cell.size() * sizeof(int64_t)},
+      {h.f0.data(), h.f0.size() * sizeof(int64_t)},     {h.f1.data(), h.f1.size() * sizeof(int64_t)},
+      {h.f2.data(), h.f2.size() * sizeof(int64_t)},     {h.geo.data(), h.geo.size() * sizeof(double)},
+      {h.rc0.data(), h.rc0.size() * sizeof(double)},    {h.rc1.data(), h.rc1.size() * sizeof(double)},
+      {h.rc2.data(), h.rc2.size() * sizeof(double)},    {h.xc1.data(), h.xc1.size() * sizeof(double)},
+      {h.xc2.data(), h.xc2.size() * sizeof(double)},    {h.sth.data(), h.sth.size() * sizeof(double)},
+      {h.cth.data(), h.cth.size() * sizeof(double)},    {h.sphc.data(), h.sphc.size() * sizeof(double)},
+      {h.cphc.data(), h.cphc.size() * sizeof(double)},  {h.sphl.data(), h.sphl.size() * sizeof(double)},
+      {h.cphl.data(), h.cphl.size() * sizeof(double)}};
+  std::vector<size_t> off(parts.size());
+  size_t tot = 0;
+  for (size_t q = 0; q < parts.size(); q++) {
+    off[q] = tot;
+    tot += (parts[q].second + 255) / 256 * 256;
+  }
+  std::vector<char> host(tot, 0);
+  for (size_t q = 0; q < parts.size(); q++) std::memcpy(host.data() + off[q], parts[q].first, parts[q].second);
+  auto fail3 = [&](cudaError_t e) {
+    why = cudaGetErrorString(e);
+    cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles);
+    delete w;
+    return e == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA;
+  };
+  cudaError_t e = cudaMalloc(&w->d_tab, tot);
+  if (e != cudaSuccess) return fail3(e);
+  e = cudaMemcpy(w->d_tab, host.data(), tot, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail3(e);
+  Grid3 &g = w->g;
+  g.n1 = h.n1; g.n2 = h.n2; g.n3 = h.n3;
+  g.bc_lo0 = d.bc_lo[0]; g.bc_hi0 = d.bc_hi[0]; g.bc_lo1 = d.bc_lo[1]; g.bc_hi1 = d.bc_hi[1];
+  g.bc_lo2 = d.bc_lo[2]; g.bc_hi2 = d.bc_hi[2];
+  g.dx0 = d.dx[0]; g.dx1 = d.dx[1]; g.dx2 = d.dx[2];
+  g.nij = h.nij; g.ncell = h.ncell; g.nf0 = h.nf0; g.nf1 = h.nf1; g.nf2 = h.nf2;
+  g.cols1 = h.cols1; g.cols2 = h.cols2;
+  for (int l = 0; l < G3_MAXLEV; l++) { g.rc1_base[l] = h.rc1_base[l]; g.rc2_base[l] = h.rc2_base[l]; }
+  char *b = w->d_tab;
+  g.nj = (const int *)(b + off[0]); g.rowbase = (const int *)(b + off[1]); g.nk = (const int *)(b + off[2]);
+  g.cell = (const int64_t *)(b + off[3]); g.f0 = (const int64_t *)(b + off[4]);
+  g.f1 = (const int64_t *)(b + off[5]); g.f2 = (const int64_t *)(b + off[6]);
+  g.geo = (const double *)(b + off[7]); g.rc0 = (const double *)(b + off[8]);
+  g.rc1 = (const double *)(b + off[9]); g.rc2 = (const double *)(b + off[10]);
+  g.xc1 = (const double *)(b + off[11]); g.xc2 = (const double *)(b + off[12]);
+  g.sth = (const double *)(b + off[13]); g.cth = (const double *)(b + off[14]);
+  g.sphc = (const double *)(b + off[15]); g.cphc = (const double *)(b + off[16]);
+  g.sphl = (const double *)(b + off[17]); g.cphl = (const double *)(b + off[18]);
+  // flux arrays, shock bits
+  e = cudaMalloc(&w->d_flux, sizeof(double) * NPRIM * (size_t)(h.nf0 + h.nf1 + h.nf2));
+  if (e != cudaSuccess) return fail3(e);
+  e = cudaMalloc(&w->d_bits, (size_t)3 * h.ncell);
+  if (e != cudaSuccess) return fail3(e);
+  e = cudaMemset(w->d_bits, 0, (size_t)3 * h.ncell);
+  if (e != cudaSuccess) return fail3(e);
+  // tiles of each kernel
+  std::vector<Tile3> t0, t1, t2, tc;
+  for (int i = 0; i <= h.n1; i++)
+    for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t0, i, j, h.nk[h.row(i, j)]);
+  for (int i = 0; i < h.n1; i++)
+    for (int j = 0; j <= h.njr(i); j++) tiles_of_rows(t1, i, j, h.n3 / std::min(h.dk(i, j), h.dk(i, j - 1)));
+  for (int i = 0; i < h.n1; i++)
+    for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t2, i, j, h.nk[h.row(i, j)] + 1);
+  for (int i = 0; i < h.n1; i++)
+    for (int j = 0; j < h.njr(i); j++) tiles_of_rows(tc, i, j, h.nk[h.row(i, j)]);
+  w->nt[0] = (int)t0.size(); w->nt[1] = (int)t1.size(); w->nt[2] = (int)t2.size(); w->nt[3] = (int)tc.size();
+  std::vector<Tile3> all;
+  all.insert(all.end(), t0.begin(), t0.end());
+  all.insert(all.end(), t1.begin(), t1.end());
+  all.insert(all.end(), t2.begin(), t2.end());
+  all.insert(all.end(), tc.begin(), tc.end());
+  e = cudaMalloc(&w->d_tiles, sizeof(Tile3) * all.size());
+  if (e != cudaSuccess) return fail3(e);
+  e = cudaMemcpy(w->d_tiles, all.data(), sizeof(Tile3) * all.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail3(e);
+  *out = w;
+  return MDG_OK;
+}
+
+void sweep3_destroy(Sweep3 *w)
+{
+  if (!w) return;
+  cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles);
+  delete w;
+}
+
+int64_t sweep3_ncell(const Sweep3 *w) { return w->ncell; }
+
+// Kernel launches of one RK stage of the single 3-D problem (slot 0).
+void launch_stage3d(int stage, Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA sst, StateSoA sn,
+                    StateSoA out, cudaStream_t st)
+{
+  const Grid3 &g = w->g;
+  double *F0 = w->d_flux, *F1 = F0 + NPRIM * g.nf0, *F2 = F1 + NPRIM * g.nf1;
+  unsigned char *own = w->d_bits + (size_t)stage * g.ncell, *all0 = w->d_bits + (size_t)2 * g.ncell;
+  const Tile3 *t0 = w->d_tiles, *t1 = t0 + w->nt[0], *t2 = t1 + w->nt[1], *tc = t2 + w->nt[2];
+  if (stage == 0) {
+    cudaMemsetAsync(all0, 0, (size_t)g.ncell, st);
+    face0_kernel<0><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
+    face1_kernel<0><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
+    face2_kernel<0><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
+    push3_kernel<0><<<w->nt[3], NT3, 0, st>>>(probs, times, g, tc, sst, sn, out, F0, F1, F2);
+  } else {
+    face0_kernel<1><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
+    face1_kernel<1><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
+    face2_kernel<1><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
+    push3_kernel<1><<<w->nt[3], NT3, 0, st>>>(probs, times, g, tc, sst, sn, out, F0, F1, F2);
+  }
+}
+
+void launch_totals3(Sweep3 *w, StateSoA s, double *out, cudaStream_t st)
+{
+  const Tile3 *tc = w->d_tiles + w->nt[0] + w->nt[1] + w->nt[2];
+  totals3_kernel<<<1, 256, 0, st>>>(w->g, tc, w->nt[3], s, out);
+}
+
+void launch_initial_estimate3(Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA s, cudaStream_t st)
+{
+  const Tile3 *tc = w->d_tiles + w->nt[0] + w->nt[1] + w->nt[2];
+  estimate3_kernel<<<w->nt[3], NT3, 0, st>>>(probs, times, w->g, tc, s);
+}
+
+}  // namespace mdg

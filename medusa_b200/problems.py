@@ -71,9 +71,12 @@ class Problem:
     e_floor: float = -1.0         # io.c:5081
     grav: tuple = (0.0, 0.0, 0.0) # fixed gravitational acceleration g0 (GRAV=FIXED_GRAV when non-zero)
     nsteps: Optional[int] = None  # fixed step count for the workload, if any
+    cells: int = 0                # interior zone count when it is not n1*n2*n3 (dendritic grids)
 
     @property
     def ncell(self) -> int:
+        if self.cells > 0:
+            return int(self.cells)
         return int(self.n[0] * self.n[1] * self.n[2])
 
     def copy(self, **kw) -> "Problem":
@@ -254,6 +257,104 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                    startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
                    bc_lo=(SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW), bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
                    prob_kind=prob_kind, cfl=cfl, tmax=tmax, **fl)
+
+
+MAX_LOG2_ASPECT = 0.5   # utils.c:12
+
+
+def _r_of_x(x: float) -> float:
+    return abs(x)                       # RCOORD=UNIFORM, metric_spherical_general.c:149-153
+
+
+def _th_of_x(x: float) -> float:
+    if x < -1.0:
+        x = -2.0 - x
+    if x > 1.0:
+        x = 2.0 - x
+    return 0.5 * math.pi * (x + 1.0)    # THCOORD=UNIFORM, metric_spherical_general.c:222-230
+
+
+def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple):
+    """Zone counts of the dendritic spherical grid: nj[i] theta zones of radial row i and
+    nk[i][j] phi zones of row (i, j), for the interior rows (the rules of compute_dj and
+    compute_dk, utils.c:181-354, for a uniform radius and theta: theta zones double
+    outwards from 2 at the centre and phi zones from 4 at each pole while the zone aspect
+    ratio exceeds 2^0.5).  Returns (nj, nk) as lists; the interior zones in the
+    reference's zone order are i, then j < nj[i], then k < nk[i][j]."""
+    nj = [0] * n1
+    nj[0] = 2
+    dth = _th_of_x(startx[1] + n2 * dx[1]) - _th_of_x(startx[1])
+    for i in range(1, n1):
+        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0])
+        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0])
+        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0])
+        ideal = rc * dth / (r1 - r0)
+        nj[i] = nj[i - 1]
+        if math.log2(ideal / nj[i]) > MAX_LOG2_ASPECT:
+            nj[i] *= 2
+        nj[i] = min(max(nj[i], nj[i - 1]), n2)
+    dj = [n2 // v for v in nj]
+    dph = n3 * dx[2]
+    nk = []
+    for i in range(n1):
+        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0])
+        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0])
+        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0])
+        dr = r1 - r0
+        row = [0] * nj[i]
+        row[0] = 4
+        for j in range(1, nj[i]):
+            thc = _th_of_x(startx[1] + (j + 0.5) * dj[i] * dx[1])
+            ideal = rc * math.sin(thc) * dph / dr
+            if j < nj[i] // 2:
+                row[j] = row[j - 1]
+                if math.log2(ideal / row[j]) > MAX_LOG2_ASPECT:
+                    row[j] *= 2
+                if i == 0:
+                    row[j] = min(row[j], n3)
+                elif nj[i - 1] == nj[i]:
+                    row[j] = min(max(row[j], nk[i - 1][j]), n3)
+                else:
+                    row[j] = min(max(row[j], nk[i - 1][j // 2]), n3)
+            else:
+                row[j] = row[nj[i] - 1 - j]
+        nk.append(row)
+    return nj, nk
+
+
+def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, energy: float = 1.0,
+             r_dep: float = 0.02, p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100,
+             bc_inner: int = REFLECT, bc_pole: int = REFLECT, noise: float = 0.0,
+             seed: int = 20240603) -> Problem:
+    """3-D Sedov blast on the dendritic spherical grid (the structure of
+    problems/init_sedov.c:3-164): r in [0, 1] uniform, theta in [0, pi], phi in [0, 2 pi);
+    rho = 1, p = p_amb, at rest, and the energy `energy` deposited as a uniform internal
+    energy density in the zones whose centre lies inside r_dep (volume of those full
+    shells: 4/3 pi r_e^3); reflecting inner and pole boundaries, periodic in phi.  With
+    noise > 0 the density is scaled by 1 + noise*(2U-1) and the three coordinate
+    velocities are set to 0.1*noise*(2U-1) (U uniform, splitmix64 on `seed`), which breaks
+    the symmetry (shock tagging, rotation through the pole rows, restriction of v^phi)."""
+    startx, dx = (0.0, -1.0, 0.0), (1.0 / n1, 2.0 / n2, 2.0 * math.pi / n3)
+    nj, nk = dendritic_grid(n1, n2, n3, startx, dx)
+    counts = np.array([sum(row) for row in nk])
+    ncell = int(counts.sum())
+    rc = (np.arange(n1) + 0.5) * dx[0]
+    inside = rc < r_dep
+    r_e = (np.nonzero(inside)[0].max() + 1) * dx[0] if inside.any() else dx[0]
+    u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
+    u_row = np.where(inside, u_dep, p_amb / (gam - 1.0))
+    ic = np.zeros((ncell, NPRIM))
+    ic[:, 0] = 1.0
+    ic[:, 1] = np.repeat(u_row, counts)
+    if noise > 0.0:
+        u = uniform01(seed, 4 * ncell).reshape(ncell, 4)
+        ic[:, 0] *= 1.0 + noise * (2.0 * u[:, 0] - 1.0)
+        for v in range(3):
+            ic[:, 2 + v] = 0.1 * noise * (2.0 * u[:, 1 + v] - 1.0)
+    return Problem(name="sedov3d_%dx%dx%d" % (n1, n2, n3), ndim=3, geom=SPHERICAL, n=(n1, n2, n3),
+                   startx=startx, dx=dx, gam=gam, ic=ic,
+                   bc_lo=(bc_inner, bc_pole, PERIODIC), bc_hi=(OUTFLOW, bc_pole, PERIODIC),
+                   cfl=cfl, tmax=tmax, cells=ncell)
 
 
 def ensemble_1d(count: int = 2048, seed: int = 7, nmin: int = 128, nmax: int = 8192,

@@ -146,15 +146,43 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_server_result.argtypes = [vp, ll, vp, ctypes.POINTER(d), ctypes.POINTER(i), ctypes.POINTER(d)]
     L.mdg_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
     L.mdg_server_destroy.argtypes = [vp]
+    L.mdg_grid3d_counts.argtypes = [ctypes.POINTER(ProblemDesc), vp, vp, ctypes.POINTER(ll)]
+    L.mdg_grid3d_geometry.argtypes = [ctypes.POINTER(ProblemDesc), vp, ctypes.POINTER(ll)]
     for name in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step", "mdg_download_state",
                  "mdg_get_time", "mdg_get_stream", "mdg_synchronize", "mdg_destroy", "mdg_set_timing",
                  "mdg_get_timers", "mdg_get_launch_config", "mdg_set_launch_config", "mdg_autotune",
                  "mdg_conserved_totals", "mdg_upload_all", "mdg_download_all", "mdg_server_create", "mdg_server_submit", "mdg_server_run",
                  "mdg_server_start", "mdg_server_stop", "mdg_server_poll", "mdg_server_wait", "mdg_server_result",
-                 "mdg_server_get_stats", "mdg_server_destroy"):
+                 "mdg_server_get_stats", "mdg_server_destroy", "mdg_grid3d_counts", "mdg_grid3d_geometry"):
         getattr(L, name).restype = i
     _lib = L
     return L
+
+
+GEO3_FIELDS = 42
+
+
+def grid3d_counts(pb: "_pb.Problem"):
+    """(nj[i] for the n1 radial rows, nk of every interior row (i, j) in zone order, zone
+    count) of a 3-D dendritic spherical problem (mdg_grid3d_counts)."""
+    d = desc_of(pb)
+    n = ctypes.c_longlong()
+    nj = np.zeros(pb.n[0], dtype=np.int32)
+    _check(library().mdg_grid3d_counts(ctypes.byref(d), nj.ctypes.data, None, ctypes.byref(n)), "mdg_grid3d_counts")
+    nk = np.zeros(int(nj.sum()), dtype=np.int32)
+    _check(library().mdg_grid3d_counts(ctypes.byref(d), None, nk.ctypes.data, ctypes.byref(n)), "mdg_grid3d_counts")
+    return nj, nk, n.value
+
+
+def grid3d_geometry(pb: "_pb.Problem") -> np.ndarray:
+    """Per-row zone geometry [rows, 42] of a 3-D dendritic spherical problem, rows i in
+    [-2, n1+2), j in [-2, nj[i]+2) (mdg_grid3d_geometry)."""
+    d = desc_of(pb)
+    n = ctypes.c_longlong()
+    _check(library().mdg_grid3d_geometry(ctypes.byref(d), None, ctypes.byref(n)), "mdg_grid3d_geometry")
+    out = np.zeros((n.value, GEO3_FIELDS))
+    _check(library().mdg_grid3d_geometry(ctypes.byref(d), out.ctypes.data, ctypes.byref(n)), "mdg_grid3d_geometry")
+    return out
 
 
 def _check(rc: int, where: str):

@@ -70,6 +70,9 @@ CONFIGS = {
                         RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
     "sph1d_grav": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
+    # 3-D spherical on the dendritic grid (Sedov blast), uniform radius and theta
+    "sph3d": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                  RCOORD="UNIFORM", THCOORD="UNIFORM"),
 }
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]

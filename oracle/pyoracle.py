@@ -196,6 +196,36 @@ def run_reference(pb, nsteps: int, every: int = 1):
     return [(int(r[0]), r[1], r[2], r[3], r[4:].reshape(pb.ncell, 5).copy()) for r in raw]
 
 
+def _ref_dump(pb, what: str) -> bytes:
+    exe = os.path.join(REF_DIR, "ref_" + ref_config(pb))
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
+        _write_input(pb, fin)
+        subprocess.run([exe, what, fin, fout], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        with open(fout, "rb") as f:
+            return f.read()
+
+
+def reference_grid(pb):
+    """The reference's dendritic zone counts: nj[i] for i in [-NG, n1+NG) and, per row
+    (i, j) with j in [-NG, nj[i]+NG), nk[i][j] (lists of lists, ghost rows included)."""
+    raw = np.frombuffer(_ref_dump(pb, "grid"), dtype=np.int32)
+    n1 = pb.n[0]
+    nj = raw[:n1 + 4].tolist()
+    nk, c = [], n1 + 4
+    for i in range(n1 + 4):
+        nk.append(raw[c:c + nj[i] + 4].tolist())
+        c += nj[i] + 4
+    return nj, nk
+
+
+def reference_geometry(pb):
+    """ref_get_geom records (64 doubles: volume, area[NDIM], gcov[0..NDIM][3], gcon[3],
+    scale[0..NDIM][3], conn[27]) of zone (i, j, 0) for every row of reference_grid, in
+    the same order."""
+    return np.frombuffer(_ref_dump(pb, "geom"), dtype=np.float64).reshape(-1, 64).copy()
+
+
 def time_reference(pb, warmup: int, steps: int, fast: bool = True) -> dict:
     """Time the reference's own build (its Makefile flags when fast=True) in a
     subprocess; returns zone_updates_per_s, seconds, steps, cells."""

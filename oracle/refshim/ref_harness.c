@@ -308,3 +308,28 @@ REF_API int ref_get_geom(int i, int j, int k, double *out)
 }
 
 REF_API int ref_ndim(void) { return NDIM; }
+
+/* Dendritic zone counts (utils.c:181-354): nj[i] for i in [-NG, n1+NG), then nk[i][j]
+ * for each of those rows and j in [-NG, nj[i]+NG), row after row.  Returns the number
+ * of nk entries written (call with nk == NULL to size the buffer). */
+REF_API int ref_get_grid(int *njo, int *nko)
+{
+  int c = 0;
+  for (int i=-NG; i<n1+NG; i++) {
+#if (NDIM>1)
+    int nji = n2/DJS(i);
+#else
+    int nji = 1;
+#endif
+    if (njo) njo[i+NG] = nji;
+    for (int j=-NG; j<nji+NG; j++) {
+#if (NDIM==3)
+      if (nko) nko[c] = n3/DKS(i,j);
+#else
+      if (nko) nko[c] = 1;
+#endif
+      c++;
+    }
+  }
+  return c;
+}

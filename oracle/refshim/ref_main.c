@@ -11,6 +11,11 @@
  *               [istep, t, dt_used, min_dt] + interior prims [ncell][5] (all double)
  *   ref_<cfg> time  <input.bin> <warmup> <steps>
  *       prints one line: "zone_updates_per_s=<v> seconds=<s> steps=<n> cells=<c>"
+ *   ref_<cfg> grid  <input.bin> <output.bin>
+ *       output: int32 nj[n1+2NG], then int32 nk for every row (i, j) of ref_get_grid
+ *   ref_<cfg> geom  <input.bin> <output.bin>
+ *       output: for every row (i, j) of ref_get_grid, the ref_get_geom record of zone
+ *       (i, j, 0), 64 doubles each (unused tail zero)
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -44,6 +49,8 @@ double ref_get_min_dt(void);
 int ref_get_istep(void);
 int ref_cell_count(void);
 void ref_get_interior(double *prim, double *eos);
+int ref_get_grid(int *nj, int *nk);
+int ref_get_geom(int i, int j, int k, double *out);
 
 static void *read_all(const char *path, size_t *len)
 {
@@ -110,6 +117,28 @@ int main(int argc, char **argv)
     double el = now_s() - t0;
     printf("zone_updates_per_s=%.6e seconds=%.6f steps=%d cells=%d\n",
            (double)ncell*steps/el, el, steps, ncell);
+  } else if (strcmp(argv[1], "grid") == 0 || strcmp(argv[1], "geom") == 0) {
+    if (argc < 4) return 2;
+    int n1 = prm.n1;
+    int nrow = ref_get_grid(NULL, NULL);
+    int *nj = malloc(sizeof(int)*(n1+4));
+    int *nk = malloc(sizeof(int)*(size_t)nrow);
+    ref_get_grid(nj, nk);
+    FILE *out = fopen(argv[3], "wb");
+    if (argv[1][1] == 'r') {
+      fwrite(nj, sizeof(int), (size_t)(n1+4), out);
+      fwrite(nk, sizeof(int), (size_t)nrow, out);
+    } else {
+      double rec[64];
+      for (int i=-2; i<n1+2; i++) {
+        for (int j=-2; j<nj[i+2]+2; j++) {
+          memset(rec, 0, sizeof rec);
+          ref_get_geom(i, j, 0, rec);
+          fwrite(rec, sizeof(double), 64, out);
+        }
+      }
+    }
+    fclose(out);
   } else {
     return 2;
   }

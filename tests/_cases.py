@@ -16,6 +16,10 @@ def golden_cases():
     return make_golden.cases()
 
 
+def golden_cases3d():
+    return make_golden.cases3d()
+
+
 def load_golden(name):
     return np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
 

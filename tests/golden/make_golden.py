@@ -40,8 +40,27 @@ def cases():
     }
 
 
+def cases3d():
+    """3-D dendritic spherical cases (Sedov blast): name -> (problem, nsteps).  Their
+    fixtures also hold one step started afresh from the final state (prim1)."""
+    return {
+        "sedov3d_20x16x32": (P.sedov_3d(20, 16, 32, r_dep=0.2), 30),
+        "sedov3d_noisy_18x8x16": (P.sedov_3d(18, 8, 16, r_dep=0.25, noise=0.1), 30),
+        "sedov3d_noisy_origin_16x8x16": (P.sedov_3d(16, 8, 16, r_dep=0.25, noise=0.05, bc_inner=P.SPHERICAL_ORIGIN,
+                                                    bc_pole=P.SPHERICAL_ORIGIN), 30),
+    }
+
+
 def main():
     build_ref.build()
+    for name, (pb, n) in cases3d().items():
+        snaps = pyoracle.run_reference(pb, n, every=n)
+        last = snaps[-1]
+        one = pyoracle.run_reference(pb.copy(ic=last[4]), 1, every=1)[-1]
+        out = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(out, prim=last[4], t=last[1], dt=last[2], nsteps=n, istep=last[0],
+                            prim1=one[4], t1=one[1], dt1=one[2])
+        print(name, "steps", last[0], "t", last[1], "->", os.path.relpath(out, ROOT))
     for name, (pb, n) in cases().items():
         snaps = pyoracle.run_reference(pb, n, every=n)
         first, last = snaps[0], snaps[-1]

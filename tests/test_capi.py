@@ -40,13 +40,15 @@ def test_error_strings_and_version():
 
 
 @pytest.mark.parametrize("mutate,code", [
-    (dict(ndim=3), 1),
+    (dict(ndim=4), 1),
+    (dict(ndim=3), 5),                                # 3-D grids are spherical (dendritic)
     (dict(hydro_interp_order=4), 1),
     (dict(gam=1.0), 1),
     (dict(bc_lo=(P.SPHERICAL_ORIGIN, 0, 0)), 5),      # spherical origin on a Cartesian grid
     (dict(bc_lo=(P.PERIODIC, 0, 0)), 1),              # unpaired periodic boundary
 ])
 def test_create_rejects_invalid_descriptions(mutate, code):
+    """Checked before any device work (runs without a GPU)."""
     pb = P.sod(64).copy(**mutate)
     arr = (S.ProblemDesc * 1)(S.desc_of(pb))
     h = ctypes.c_void_p()
@@ -111,3 +113,13 @@ def test_server_calls_reject_null_handle():
     assert L.mdg_server_start(None) == 1
     assert L.mdg_server_stop(None) == 1
     assert L.mdg_server_destroy(None) == 0
+
+
+@pytest.mark.parametrize("precision,nprob,code", [(1, 1, 5), (0, 2, 5)])
+def test_3d_solver_scope_checked_before_device_work(precision, nprob, code):
+    """A 3-D solver advances one problem, plain FP64."""
+    pb = P.sedov_3d(12, 8, 16, r_dep=0.3)
+    arr = (S.ProblemDesc * nprob)(*[S.desc_of(pb)] * nprob)
+    h = ctypes.c_void_p()
+    assert S.library().mdg_create(arr, nprob, precision, 0, ctypes.byref(h)) == code
+    assert not h.value

@@ -1,0 +1,89 @@
+"""The 3-D dendritic spherical grid on the host: zone counts (compute_dj/compute_dk,
+utils.c:181-354) and per-row zone geometry (init_geometry, metric_spherical_general.c)
+of the library against the Python restatement and against the reference build itself;
+the 3-D fixtures against the problem generator and the live reference."""
+import numpy as np
+import pytest
+
+from medusa_b200 import problems as P
+from medusa_b200 import solver as S
+from medusa_b200.solver import MdgError
+from oracle import pyoracle
+from tests._cases import golden_cases3d, load_golden
+
+CASES3 = golden_cases3d()
+# the reference record of ref_get_geom: vol, area[3], gcov[4][3], gcon[3], scale[4][3],
+# conn[27]; the library keeps the 11 coefficients the spherical metric sets
+CONN_SET = [0, 4, 8, 10, 12, 13, 17, 20, 24, 23, 25]
+
+
+@pytest.mark.parametrize("dims", [(20, 16, 32), (64, 64, 128), (384, 128, 256), (7, 2, 4)])
+def test_zone_counts_match_restatement(dims):
+    pb = P.sedov_3d(*dims, r_dep=0.3)
+    nj, nk, n = S.grid3d_counts(pb)
+    pj, pk = P.dendritic_grid(*dims, pb.startx, pb.dx)
+    assert list(nj) == pj
+    assert list(nk) == [x for row in pk for x in row]
+    assert n == pb.ncell == sum(sum(r) for r in pk)
+
+
+def test_c3_grid_size():
+    """The measured 3-D workload: 384 x 128 x 256 before coarsening."""
+    pb = P.sedov_3d(384, 128, 256)
+    nj, nk, n = S.grid3d_counts(pb)
+    assert nj[0] == 2 and nj[-1] == 128 and nk.min() == 4 and nk.max() == 256
+    assert n == pb.ncell < 384 * 128 * 256
+
+
+@pytest.mark.parametrize("dims", [(24, 16, 32), (40, 32, 64), (48, 64, 128)])
+def test_geometry_bit_identical_to_reference(dims):
+    pb = P.sedov_3d(*dims, r_dep=0.2)
+    if not pyoracle.ref_available(pb):
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    rnj, _ = pyoracle.reference_grid(pb)
+    geo = S.grid3d_geometry(pb)
+    ref = pyoracle.reference_geometry(pb)
+    theirs = np.concatenate([ref[:, 0:31], ref[:, 31:58][:, CONN_SET]], axis=1)
+    assert geo.shape == theirs.shape
+    n1 = dims[0]
+    r = 0
+    for i in range(-2, n1 + 2):
+        for j in range(-2, rnj[i + 2] + 2):
+            # volume, gcov, gcon, scale on every row; areas on the face rows; conn inside
+            fields = [0] + list(range(4, 31))
+            if 0 <= i <= n1 and 0 <= j <= rnj[i + 2]:
+                fields += [1, 2, 3]
+            if 0 <= i < n1 and 0 <= j < rnj[i + 2]:
+                fields += list(range(31, 42))
+            assert np.array_equal(geo[r, fields], theirs[r, fields]), (i, j)
+            r += 1
+
+
+def test_grid_calls_validate():
+    pb = P.sedov_3d(16, 8, 16)
+    with pytest.raises(MdgError) as e:
+        S.grid3d_counts(pb.copy(n=(16, 12, 16)))
+    assert e.value.code == 1
+    with pytest.raises(MdgError) as e:
+        S.grid3d_counts(pb.copy(geom=P.CARTESIAN))
+    assert e.value.code == 5
+
+
+@pytest.mark.parametrize("name", sorted(CASES3))
+def test_fixture_matches_generator(name):
+    pb, n = CASES3[name]
+    g = load_golden(name)
+    assert g["prim"].shape == (pb.ncell, 5) and g["prim1"].shape == (pb.ncell, 5)
+    assert int(g["istep"]) == n
+    assert np.all(np.isfinite(g["prim"]))
+
+
+@pytest.mark.parametrize("name", sorted(CASES3))
+def test_fixture_reproduced_by_live_reference(name):
+    pb, n = CASES3[name]
+    if not pyoracle.ref_available(pb):
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    g = load_golden(name)
+    snaps = pyoracle.run_reference(pb, n, every=n)
+    assert np.array_equal(snaps[-1][4], g["prim"])
+    assert snaps[-1][1] == float(g["t"])
