@@ -311,7 +311,13 @@ def run_reference_arm(args, ctx):
     from medusa_b200 import problems as P
     if ctx.rank != 0:
         return
-    if args.workload == "kh2048":
+    if args.workload == "sedov3d":
+        cb = cpu_baseline_sedov3d(steps=max(1, min(args.steps, 2)))
+        config = {"workload": "sedov_3d_dendritic_spherical_%dx%dx%d_fp64" % SEDOV3D, "global_batch": 1,
+                  "seq_len": P.sedov_3d(*SEDOV3D).ncell, "parallelism": "replicas",
+                  "l2": "inputs larger than L2"}
+        dtype = "f64"
+    elif args.workload == "kh2048":
         pb = P.kelvin_helmholtz(NX)
         cb = cpu_baseline_kh(pb, steps=max(1, min(args.steps, 2)))
         config = {"workload": "kelvin_helmholtz_2d_%dx%d_fp64" % (NX, NX), "global_batch": 1,
@@ -552,6 +558,78 @@ def run_kh(args, ctx):
     print(json.dumps(line), flush=True)
 
 
+SEDOV3D = (384, 128, 256)
+SEDOV3D_SAMPLE = (96, 64, 128)
+
+
+def cpu_baseline_sedov3d(steps=2):
+    """Reference CPU build (its Makefile flags), one core, `steps` RK2 steps of the same
+    Sedov blast on a smaller dendritic grid (96 x 64 x 128 before coarsening): the full
+    grid needs several GB of host memory for the reference's per-zone geometry records."""
+    from medusa_b200 import problems as P
+    from oracle import pyoracle
+    pb = P.sedov_3d(*SEDOV3D_SAMPLE, r_dep=0.05)
+    if pyoracle.ref_available(pb, fast=True):
+        r = pyoracle.time_reference(pb, 1, steps, fast=True)
+        return {"value": r["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+                "sample": "%d RK2 steps of the Sedov blast on the %dx%dx%d dendritic grid (%d zones), reference "
+                          "build with its own flags (-O3 -ffast-math), 1 core, %.1f s"
+                          % (steps, *SEDOV3D_SAMPLE, pb.ncell, r["seconds"])}
+    return {"value": None, "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+            "sample": "unavailable: the 3-D reference build is absent"}
+
+
+def run_sedov3d(args, ctx):
+    import medusa_b200
+    from medusa_b200 import problems as P
+
+    K, W = args.steps, args.warmup
+    pb = P.sedov_3d(*SEDOV3D)
+    ncell = pb.ncell
+    s = medusa_b200.Solver(pb, device=ctx.local)
+    s.step(W)
+    s.synchronize()
+    ms, clocks = timed_steps(ctx, s, K, sample_clocks=True)
+    value = ctx.world * ncell * K / (ms / 1e3)
+    st = stage_times(s, min(K, 10))
+    s.close()
+    ms_e2e, h2d, d2h = e2e_run(ctx, lambda upload: medusa_b200.Solver(pb, device=ctx.local, upload=upload),
+                               [pb], K, W)
+    e2e = ctx.world * ncell * K / (ms_e2e / 1e3)
+    if ctx.rank != 0:
+        return
+    peak, peak_kind = read_peaks()
+    b_stage1 = 360.0
+    achieved = b_stage1 * ncell / (st["stage1"] / 1e3) / 1e9
+    traffic = read_profile_value("sweep3d_sedov_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
+        "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms / K,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "sedov_3d_dendritic_spherical_%dx%dx%d_fp64" % SEDOV3D, "global_batch": ctx.world,
+                   "seq_len": ncell, "parallelism": "replicas" if ctx.world > 1 else "single",
+                   "precision": "plain FP64 (reference operation order)",
+                   "grid": "uniform radius (the reference's metrics have no logarithmic radial map)",
+                   "l2": "inputs larger than L2 (state 2 x %.0f MB)" % (ncell * 40 / 1e6)},
+        "gpu_launches": 10 * K,
+        "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / K,
+                "d2h_bytes_per_step": d2h / K,
+                "timed": "upload initial state (pinned H2D) + %d steps + download state (pinned D2H)" % K,
+                "ms": ms_e2e},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "kernel": "second RK stage (face0/face1/face2/push3 kernels <1>)",
+                     "kernel_ms": st["stage1"], "stage0_ms": st["stage0"],
+                     "algorithmic_bytes_per_zone": b_stage1,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_sedov3d()
+    print(json.dumps(line), flush=True)
+
+
 def server_workload_name(args):
     if args.server_frac_2d > 0.0:
         return "server_stream_1d_spherical_256_8192_and_%d%%_2d_cartesian_128sq_1024sq" % round(
@@ -635,7 +713,7 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048", "server"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048", "server", "sedov3d"])
     ap.add_argument("--server-requests", type=int, default=6000)
     ap.add_argument("--server-rates", default="1000,4000,16000,inf",
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
@@ -665,6 +743,8 @@ def main():
             run_ensemble(args, ctx)
         elif args.workload == "server":
             run_server(args, ctx)
+        elif args.workload == "sedov3d":
+            run_sedov3d(args, ctx)
         else:
             run_kh(args, ctx)
     finally:

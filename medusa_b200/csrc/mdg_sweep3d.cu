@@ -192,6 +192,17 @@ __device__ void pencil0(const Grid3 &g, const ProbDev &P, const StateSoA &s, int
     return;
   }
   // prolongate0 (step.c:905-955)
+  if (djii == dji && dks(g, ii, j) == dks(g, i, j)) {
+    // same theta and phi level: both slope corrections are multiplied by an exact +0
+    // (the prolongation point is the zone's own centroid), so the result is the zone
+    // value itself unless that value is -0 (then the sign of the slope decides the sign
+    // of the zero sum, and the full computation below runs)
+    load7(g, P, s, ii, j, k, pp);
+    bool neg0 = false;
+#pragma unroll
+    for (int v = 0; v < 7; v++) neg0 = neg0 || (pp[v] == 0.0 && signbit(pp[v]));
+    if (!neg0) return;
+  }
   const int jj = j * dji / djii;
   const double x1p = __ldg(g.xc1 + g.rc1_base[ilog2(dji)] + NG + j);
   const double x2p = __ldg(g.xc2 + g.rc2_base[ilog2(dks(g, i, j))] + NG + k);
