@@ -489,25 +489,54 @@ __global__ void __launch_bounds__(NT3) face1_kernel(const ProbDev *__restrict__ 
 }
 
 // Direction-2 faces: face k in [0, nk] of row (i, j) (step.c:1267-1425), with the
-// polar-axis fix on the last theta row.
+// polar-axis fix on the last theta row.  A CTA takes NT3-2 consecutive faces of one row:
+// it stages the zones they read in shared memory (each zone loaded once) and
+// reconstructs every zone once (the reference reconstructs each zone for both of its
+// faces), then each thread solves one face.
+constexpr int T2 = NT3 - 2;
 template <int STAGE>
 __global__ void __launch_bounds__(NT3) face2_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, const unsigned char *__restrict__ own,
                                                      const unsigned char *__restrict__ all0)
 {
+  __shared__ double sv[7][T2 + 4];    // zones k0-2 .. k0+cnt+1
+  __shared__ double sal[7][T2 + 2];   // left / right face values of zones k0-1 .. k0+cnt
+  __shared__ double sar[7][T2 + 2];
   __shared__ double sred[32];
   if (times[0].done) return;
   const ProbDev &P = probs[0];
-  const Tile3 t = tiles[blockIdx.x];
-  const int i = t.i, j = t.j, k = t.k0 + (int)threadIdx.x;
+  const Tile3 tl = tiles[blockIdx.x];
+  const int i = tl.i, j = tl.j, k0 = tl.k0, cnt = tl.cnt;
+  const int t = (int)threadIdx.x;
+  const int ij = rowi(g, i, j);
+  const int dk = dks(g, i, j);
+  const int64_t base = g.rc2_base[ilog2(dk)] + NG;
+  const bool pole = (j == nj_of(g, i) - 1);
+  for (int q = t; q < cnt + 4; q += NT3) {
+    double w[7];
+    load7(g, P, s, i, j, k0 - 2 + q, w);
+#pragma unroll
+    for (int v = 0; v < 7; v++) sv[v][q] = w[v];
+  }
+  __syncthreads();
+  if (!pole && t < cnt + 2) {
+    // zone k0-1+t from the staged neighbours (interp() on its 3-zone stencil)
+    const RcView<double, true> gz{g.rc2 + base + k0 - 1 + t, g.cols2};
+#pragma unroll
+    for (int v = 0; v < 7; v++) {
+      double al, ar;
+      recon_zone<double>(P.interp_order, sv[v][t], sv[v][t + 1], sv[v][t + 2], gz, al, ar);
+      sal[v][t] = al;
+      sar[v][t] = ar;
+    }
+  }
+  __syncthreads();
   double lmin = 1.0e300;
-  if ((int)threadIdx.x < t.cnt) {
-    const int ij = rowi(g, i, j);
-    const int dk = dks(g, i, j);
-    const int64_t base = g.rc2_base[ilog2(dk)] + NG;
+  if (t < cnt) {
+    const int k = k0 + t;
     double pl[7], pr[7];
-    if (j == nj_of(g, i) - 1) {
+    if (pole) {
       // polar-axis fix: zone values, velocity rotated at the shared phi face
       const int64_t b1 = g.rc1_base[ilog2(djs(g, i))] + NG + j;
       const double sth = __ldg(g.sth + b1), cth = __ldg(g.cth + b1);
@@ -521,7 +550,8 @@ __global__ void __launch_bounds__(NT3) face2_kernel(const ProbDev *__restrict__ 
       for (int side = 0; side < 2; side++) {
         const int kt = k - 1 + side;
         double w[7];
-        load7(g, P, s, i, j, kt, w);
+#pragma unroll
+        for (int v = 0; v < 7; v++) w[v] = sv[v][t + 1 + side];
         const double sph = __ldg(g.sphc + base + kt), cph = __ldg(g.cphc + base + kt);
         double lam[3][3] = {{sth * cph, cth * cph, -sph}, {sth * sph, cth * sph, cph}, {cth, -sth, 0.0}};
         double v[3];
@@ -539,10 +569,11 @@ __global__ void __launch_bounds__(NT3) face2_kernel(const ProbDev *__restrict__ 
         }
       }
     } else {
-      double pen[4][7];
-#pragma unroll 1
-      for (int q = 0; q < 4; q++) load7(g, P, s, i, j, k - 2 + q, pen[q]);
-      recon_face(P.interp_order, pen, g.rc2, g.cols2, base + k - 1, base + k, pl, pr);
+#pragma unroll
+      for (int v = 0; v < 7; v++) {
+        pl[v] = sar[v][t];
+        pr[v] = sal[v][t + 1];
+      }
     }
     const bool hlle = flag_shock<STAGE>(g, i, j, k, own, all0) || flag_shock<STAGE>(g, i, j, k - 1, own, all0);
     const FaceGeom<double> fg = face_geom3<2>(g, ij);
@@ -776,9 +807,9 @@ struct Sweep3 {
   int64_t ncell = 0;
 };
 
-static void tiles_of_rows(std::vector<Tile3> &out, int i, int j, int count)
+static void tiles_of_rows(std::vector<Tile3> &out, int i, int j, int count, int chunk = NT3)
 {
-  for (int k0 = 0; k0 < count; k0 += NT3) out.push_back(Tile3{i, j, k0, (count - k0 < NT3) ? count - k0 : NT3});
+  for (int k0 = 0; k0 < count; k0 += chunk) out.push_back(Tile3{i, j, k0, (count - k0 < chunk) ? count - k0 : chunk});
 }
 
 int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
@@ -851,7 +882,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   for (int i = 0; i < h.n1; i++)
     for (int j = 0; j <= h.njr(i); j++) tiles_of_rows(t1, i, j, h.n3 / std::min(h.dk(i, j), h.dk(i, j - 1)));
   for (int i = 0; i < h.n1; i++)
-    for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t2, i, j, h.nk[h.row(i, j)] + 1);
+    for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t2, i, j, h.nk[h.row(i, j)] + 1, T2);
   for (int i = 0; i < h.n1; i++)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(tc, i, j, h.nk[h.row(i, j)]);
   w->nt[0] = (int)t0.size(); w->nt[1] = (int)t1.size(); w->nt[2] = (int)t2.size(); w->nt[3] = (int)tc.size();
