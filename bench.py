@@ -584,7 +584,8 @@ def run_sedov3d(args, ctx):
     from medusa_b200 import problems as P
 
     K, W = args.steps, args.warmup
-    pb = P.sedov_3d(*SEDOV3D)
+    dims = tuple(int(x) for x in args.sedov3d_dims.split(",")) if args.sedov3d_dims else SEDOV3D
+    pb = P.sedov_3d(*dims)
     ncell = pb.ncell
     s = medusa_b200.Solver(pb, device=ctx.local)
     s.step(W)
@@ -607,7 +608,7 @@ def run_sedov3d(args, ctx):
         "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "sedov_3d_dendritic_spherical_%dx%dx%d_fp64" % SEDOV3D, "global_batch": ctx.world,
+        "config": {"workload": "sedov_3d_dendritic_spherical_%dx%dx%d_fp64" % dims, "global_batch": ctx.world,
                    "seq_len": ncell, "parallelism": "replicas" if ctx.world > 1 else "single",
                    "precision": "plain FP64 (reference operation order)",
                    "grid": "uniform radius (the reference's metrics have no logarithmic radial map)",
@@ -717,6 +718,8 @@ def main():
     ap.add_argument("--server-requests", type=int, default=6000)
     ap.add_argument("--server-rates", default="1000,4000,16000,inf",
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
+    ap.add_argument("--sedov3d-dims", default="",
+                    help="sedov3d: n1,n2,n3 of the grid (default 384,128,256; smaller grids for profiling)")
     ap.add_argument("--server-frac-2d", type=float, default=0.0,
                     help="server: fraction of 2-D Cartesian requests (0.263 = the 70:25 share of 1-D and 2-D "
                          "requests of the mixed stream)")

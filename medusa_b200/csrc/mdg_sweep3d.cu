@@ -40,6 +40,15 @@ namespace mdg {
 
 struct Tile3 { int i, j, k0, cnt; };
 constexpr int NT3 = 128;
+// resident CTAs per SM requested from the compiler (register caps): the face kernels
+// wait on dependent gathers, and 8 CTAs of 4 warps (64 registers, a few spills) ran
+// 1.2x faster than 4 CTAs (128 registers) on the 384x128x256 Sedov grid
+#ifndef MDG_F3MINB
+#define MDG_F3MINB 8
+#endif
+#ifndef MDG_P3MINB
+#define MDG_P3MINB 8
+#endif
 
 __device__ __forceinline__ int rowi(const Grid3 &g, int i, int j) { return __ldg(g.rowbase + i + NG) + j + NG; }
 __device__ __forceinline__ int nj_of(const Grid3 &g, int i) { return __ldg(g.nj + i + NG); }
@@ -408,7 +417,7 @@ __device__ __forceinline__ bool flag_shock(const Grid3 &g, int i, int jj, int kc
 
 // Direction-0 faces: face (i, j, k) is the lower radial face of zone (i, j, k), i in [0, n1].
 template <int STAGE>
-__global__ void __launch_bounds__(NT3) face0_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+__global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, unsigned char *__restrict__ own,
                                                      unsigned char *__restrict__ all0)
@@ -450,7 +459,7 @@ __global__ void __launch_bounds__(NT3) face0_kernel(const ProbDev *__restrict__ 
 
 // Direction-1 faces: sub-face kk of face row (i, j), j in [0, nj(i)] (step.c:1212-1265).
 template <int STAGE>
-__global__ void __launch_bounds__(NT3) face1_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+__global__ void __launch_bounds__(NT3, MDG_F3MINB) face1_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, const unsigned char *__restrict__ own,
                                                      const unsigned char *__restrict__ all0)
@@ -495,7 +504,7 @@ __global__ void __launch_bounds__(NT3) face1_kernel(const ProbDev *__restrict__ 
 // faces), then each thread solves one face.
 constexpr int T2 = NT3 - 2;
 template <int STAGE>
-__global__ void __launch_bounds__(NT3) face2_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+__global__ void __launch_bounds__(NT3, MDG_F3MINB) face2_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, const unsigned char *__restrict__ own,
                                                      const unsigned char *__restrict__ all0)
@@ -592,7 +601,7 @@ __global__ void __launch_bounds__(NT3) face2_kernel(const ProbDev *__restrict__ 
 // geometric sources of the stage state (rad_fluid.c:164-192, fluid.c:56-73) and, in the
 // second stage, the zone terms of the next estimate_dt (step.c:177-187).
 template <int STAGE>
-__global__ void __launch_bounds__(NT3) push3_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+__global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA sst,
                                                      StateSoA sn, StateSoA out, const double *__restrict__ F0,
                                                      const double *__restrict__ F1, const double *__restrict__ F2)
