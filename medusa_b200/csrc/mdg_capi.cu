@@ -245,13 +245,13 @@ static void free_all(mdg_solver *s)
 
 // A solver of one 3-D dendritic spherical problem (validated by the caller): the grid
 // tables of mdg_sweep3d.cu, state P and PH of ncell zones in the reference's zone order.
-static int create_3d(const mdg_problem_desc &d, int device, mdg_solver **out)
+static int create_3d(const mdg_problem_desc &d, int precision, int device, mdg_solver **out)
 {
   mdg_solver *s = new mdg_solver();
   s->device = device;
   s->ndim = 3;
   s->nprob = 1;
-  s->precision = MDG_PREC_FP64;
+  s->precision = precision;
   s->descs.assign(1, d);
   std::string why;
   int rc = sweep3_create(d, &s->s3, why);
@@ -372,23 +372,23 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     std::string why;
     int rc = validate_desc(descs[m], ndim, why);
     if (rc != MDG_OK) return fail(rc, "problem " + std::to_string(m) + ": " + why);
-    if (precision == MDG_PREC_MIXED && (descs[m].ndim != 1 || descs[m].hydro_interp_order != 3))
+    if (precision == MDG_PREC_MIXED && (descs[m].ndim == 2 || descs[m].hydro_interp_order != 3))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
-                                       ": the mixed-precision sweep is built for 1-D parabolic reconstruction");
+                                       ": the mixed-precision sweeps are built for 1-D and 3-D parabolic reconstruction");
     if (precision == MDG_PREC_MIXED && descs[m].geom == MDG_SPHERICAL && !(descs[m].startx[0] >= 0.0))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
   }
   if (ndim == 3) {
     if (nprob != 1) return fail(MDG_ERR_NOTIMPL, "a 3-D solver advances one problem");
-    if (precision != MDG_PREC_FP64)
-      return fail(MDG_ERR_NOTIMPL, "the mixed-precision sweep is built for 1-D parabolic reconstruction");
+    if (precision == MDG_PREC_MIXED && descs[0].hydro_interp_order != 3)
+      return fail(MDG_ERR_NOTIMPL, "the mixed-precision 3-D sweep is built for parabolic reconstruction");
   }
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(MDG_ERR_INVALID, "device ordinal out of range");
   CK(cudaSetDevice(device));
-  if (ndim == 3) return create_3d(descs[0], device, out);
+  if (ndim == 3) return create_3d(descs[0], precision, device, out);
 
   mdg_solver *s = new mdg_solver();
   s->device = device;
@@ -568,7 +568,8 @@ int mdg_download_all(mdg_solver *s, double *prim)
 static int queue_steps(mdg_solver *s, int nsteps)
 {
   auto mark = [&](int k, int e) { if (s->timing) cudaEventRecord(s->ev[k][e], s->stream); };
-  const bool mixed = s->precision == MDG_PREC_MIXED;
+  const bool mix3 = s->ndim == 3 && s->precision == MDG_PREC_MIXED;
+  const bool mixed = s->ndim != 3 && s->precision == MDG_PREC_MIXED;   // the batched 1-D mixed sweep
   const int mgrid = mixed ? mixed_grid(s) : 0;
   const bool queue = s->cfg.ctas_per_sm > 0;
   for (int k = 0; k < nsteps; k++) {
@@ -580,7 +581,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
       launch_stage1d_mixed(0, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
                            s->tb, s->P, s->P, s->PH, s->stream);
     else if (s->ndim == 3)
-      launch_stage3d(0, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
+      launch_stage3d(0, mix3, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
     else if (s->ndim == 1)
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
     else
@@ -592,7 +593,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
       launch_stage1d_mixed(1, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
                            s->tb, s->PH, s->P, s->P, s->stream);
     else if (s->ndim == 3)
-      launch_stage3d(1, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
+      launch_stage3d(1, mix3, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
     else if (s->ndim == 1)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     else

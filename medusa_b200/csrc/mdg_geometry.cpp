@@ -430,6 +430,8 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
   // direction-0 reconstruction table (the 1-D spherical radial moments)
   h.rc0.assign((size_t)RC_NFIELDS * (n1 + 2 * NG), 0.0);
   build_recon_table(d, 0, h.rc0.data(), n1 + 2 * NG, 0);
+  h.mx0.assign((size_t)MX_NFIELDS * (n1 + 2 * NG), 0.0f);
+  build_mixed_table(d, 0, h.mx0.data(), n1 + 2 * NG, 0);
 
   // direction-1 and -2 tables per refinement level
   int lev1 = 0, lev2 = 0;
@@ -444,6 +446,7 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
   h.cols1 = cols1; h.cols2 = cols2;
   h.rc1.assign((size_t)RC_NFIELDS * cols1, 0.0); h.rc2.assign((size_t)RC_NFIELDS * cols2, 0.0);
   h.xc1.assign(cols1, 0.0); h.xc2.assign(cols2, 0.0);
+  h.mx1.assign((size_t)MX_NFIELDS * cols1, 0.0f); h.mx2.assign((size_t)MX_NFIELDS * cols2, 0.0f);
   h.sth.assign(cols1, 0.0); h.cth.assign(cols1, 0.0);
   h.sphc.assign(cols2, 0.0); h.cphc.assign(cols2, 0.0); h.sphl.assign(cols2, 0.0); h.cphl.assign(cols2, 0.0);
   for (int l = 0; l < h.nlev1; l++) {
@@ -462,6 +465,10 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
       rc_fields(al[jm + NG], al[j + NG], al[jp + NG], be[jm + NG], be[j + NG], be[jp + NG], ga[jm + NG],
                 ga[j + NG], ga[jp + NG], sx1 + j * s * dx1, sx1 + (j + 1) * s * dx1, v);
       for (int f = 0; f < RC_NFIELDS; f++) h.rc1[(size_t)f * cols1 + col] = v[f];
+      float w[MX_NFIELDS];
+      mx_fields(al[jm + NG], al[j + NG], al[jp + NG], be[jm + NG], be[j + NG], be[jp + NG], ga[jm + NG],
+                ga[j + NG], ga[jp + NG], sx1 + j * s * dx1, sx1 + (j + 1) * s * dx1, w);
+      for (int f = 0; f < MX_NFIELDS; f++) h.mx1[(size_t)f * cols1 + col] = w[f];
       h.xc1[col] = be[j + NG] / ga[j + NG];
       double th = th_of_x(be[j + NG] / ga[j + NG]);
       h.sth[col] = std::sin(th);
@@ -484,6 +491,10 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
       rc_fields(al[km + NG], al[k + NG], al[kp + NG], be[km + NG], be[k + NG], be[kp + NG], ga[km + NG],
                 ga[k + NG], ga[kp + NG], sx2 + k * s * dx2, sx2 + (k + 1) * s * dx2, v);
       for (int f = 0; f < RC_NFIELDS; f++) h.rc2[(size_t)f * cols2 + col] = v[f];
+      float w[MX_NFIELDS];
+      mx_fields(al[km + NG], al[k + NG], al[kp + NG], be[km + NG], be[k + NG], be[kp + NG], ga[km + NG],
+                ga[k + NG], ga[kp + NG], sx2 + k * s * dx2, sx2 + (k + 1) * s * dx2, w);
+      for (int f = 0; f < MX_NFIELDS; f++) h.mx2[(size_t)f * cols2 + col] = w[f];
       h.xc2[col] = be[k + NG] / ga[k + NG];
       double phc = sx2 + (k + 0.5) * s * dx2, phl = sx2 + k * s * dx2;
       h.sphc[col] = std::sin(phc); h.cphc[col] = std::cos(phc);

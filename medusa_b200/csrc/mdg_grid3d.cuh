@@ -55,6 +55,7 @@ struct Grid3 {
   const double *sth, *cth;    // sin/cos(theta(beta1s/Gamma1s)) in the rc1 columns (polar fix)
   const double *sphc, *cphc;  // sin/cos(phi) at the zone centre, rc2 columns
   const double *sphl, *cphl;  // sin/cos(phi) at the lower phi face, rc2 columns
+  const float *mx0, *mx1, *mx2;   // FP32 reconstruction weights (MixField) of the rc0/rc1/rc2 columns
 };
 
 MDG_HD inline int ilog2(int s)
@@ -70,6 +71,7 @@ struct Grid3Host {
   std::vector<int> nj, rowbase, nk;
   std::vector<int64_t> cell, f0, f1, f2;
   std::vector<double> geo, rc0, rc1, rc2, xc1, xc2, sth, cth, sphc, cphc, sphl, cphl;
+  std::vector<float> mx0, mx1, mx2;
   int64_t nij = 0, ncell = 0, nf0 = 0, nf1 = 0, nf2 = 0, cols1 = 0, cols2 = 0;
   int nlev1 = 0, nlev2 = 0;
   int rc1_base[G3_MAXLEV] = {}, rc2_base[G3_MAXLEV] = {};

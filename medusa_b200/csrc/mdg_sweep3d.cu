@@ -32,7 +32,9 @@
 #include "mdg_hydro.cuh"
 #include "mdg_kernels.cuh"
 #include "mdg_grid3d.cuh"
+#include "mdg_mixed.cuh"
 #include <cstring>
+#include <type_traits>
 #include <string>
 #include <vector>
 
@@ -403,6 +405,60 @@ __device__ __forceinline__ void recon_face(int order, const double pen[4][7], co
   }
 }
 
+// Mixed precision (MIX): the same pencils, para_recon in FP32 difference form with the
+// FP32 weights of the zone (face values a + da formed in FP64), HLLC with FP32 wave speeds
+// and star-state increments and an FP64 upwind flux.  Faces the FP32 solver declines
+// (ill-conditioned, MIX_COND_MAX) or whose Gamma slot is not the constant Gamma (the
+// restricted radial entries) are re-solved in FP64 from the pencil; HLLE faces (next to
+// a shock) take the FP64 solver on the mixed face states.
+__device__ __forceinline__ void recon_face_mixed(const double pen[4][7], const float *mx, int64_t stride,
+                                                 int64_t c1, int64_t c2, double *pl, double *pr)
+{
+  const MixW w1 = load_mixw(mx + c1, stride), w2 = load_mixw(mx + c2, stride);
+#pragma unroll
+  for (int v = 0; v < 7; v++) {
+    float dl, dr;
+    mixed_recon((float)(pen[1][v] - pen[0][v]), (float)(pen[2][v] - pen[1][v]), w1, dl, dr);
+    pl[v] = pen[1][v] + (double)dr;
+    mixed_recon((float)(pen[2][v] - pen[1][v]), (float)(pen[3][v] - pen[2][v]), w2, dl, dr);
+    pr[v] = pen[2][v] + (double)dl;
+  }
+}
+
+template <int DIR>
+__device__ __noinline__ int face_fp64_3d(int order, const double *pen, const double *rc, int64_t stride, int64_t c1,
+                                         int64_t c2, FaceGeom<double> fg, double *fl, double *ss)
+{
+  double p[4][7], pl[7], pr[7];
+  for (int q = 0; q < 28; q++) p[q / 7][q % 7] = pen[q];
+  recon_face(order, p, rc, stride, c1, c2, pl, pr);
+  return hllc3<DIR>(pl, pr, fg, fl, *ss);
+}
+
+// Reconstruction and solve of one face of the pencil; returns isshock.
+template <int DIR, bool MIX>
+__device__ __forceinline__ int solve_face(const ProbDev &P, const double pen[4][7], const double *rc, const float *mx,
+                                          int64_t stride, int64_t c1, int64_t c2, const FaceGeom<double> &fg,
+                                          bool hlle, double *fl, double &ss)
+{
+  double pl[7], pr[7];
+  if (!MIX) {
+    recon_face(P.interp_order, pen, rc, stride, c1, c2, pl, pr);
+    if (hlle) { hlle3<DIR>(pl, pr, fg, fl, ss); return 0; }
+    return hllc3<DIR>(pl, pr, fg, fl, ss);
+  }
+  recon_face_mixed(pen, mx, stride, c1, c2, pl, pr);
+  if (hlle) { hlle3<DIR>(pl, pr, fg, fl, ss); return 0; }
+  if (pl[6] == P.gam && pr[6] == P.gam) {
+    float sig;
+    int isshock;
+    if (riemann_hllc_mixed<DIR>(pl, pr, fg, gam_const<float>((float)P.gam), fl, sig, isshock)) {
+      ss = (double)sig;
+      return isshock;
+    }
+  }
+  return face_fp64_3d<DIR>(P.interp_order, &pen[0][0], rc, stride, c1, c2, fg, fl, &ss);
+}
 
 // Flag of zone (i, jj, kc) as transverse_shock reads it at this point of the serial loop.
 template <int STAGE>
@@ -416,7 +472,7 @@ __device__ __forceinline__ bool flag_shock(const Grid3 &g, int i, int jj, int kc
 }
 
 // Direction-0 faces: face (i, j, k) is the lower radial face of zone (i, j, k), i in [0, n1].
-template <int STAGE>
+template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, unsigned char *__restrict__ own,
@@ -432,11 +488,10 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *_
     double pen[4][7];
 #pragma unroll 1
     for (int q = 0; q < 4; q++) pencil0(g, P, s, i, j, k, i - 2 + q, pen[q]);
-    double pl[7], pr[7];
-    recon_face(P.interp_order, pen, g.rc0, g.n1 + 2 * NG, i - 1 + NG, i + NG, pl, pr);
     const int ij = rowi(g, i, j);
     double fl[NPRIM], ss;
-    const int isshock = hllc3<0>(pl, pr, face_geom3<0>(g, ij), fl, ss);
+    const int isshock = solve_face<0, MIX>(P, pen, g.rc0, g.mx0, g.n1 + 2 * NG, i - 1 + NG, i + NG,
+                                           face_geom3<0>(g, ij), false, fl, ss);
     const int64_t f = __ldg(g.f0 + ij) + k;
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) flux[v * g.nf0 + f] = fl[v];
@@ -458,7 +513,7 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *_
 }
 
 // Direction-1 faces: sub-face kk of face row (i, j), j in [0, nj(i)] (step.c:1212-1265).
-template <int STAGE>
+template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(NT3, MDG_F3MINB) face1_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, const unsigned char *__restrict__ own,
@@ -474,9 +529,7 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face1_kernel(const ProbDev *_
     double pen[4][7];
 #pragma unroll 1
     for (int q = 0; q < 4; q++) pencil1(g, P, s, i, j, kk, j - 2 + q, pen[q]);
-    double pl[7], pr[7];
     const int64_t base = g.rc1_base[ilog2(djs(g, i))] + NG;
-    recon_face(P.interp_order, pen, g.rc1, g.cols1, base + j - 1, base + j, pl, pr);
     // zone k of row j that owns the sub-face, and the transverse_shock test of zone k
     const int dkj = dks(g, i, j), dkjm = dks(g, i, j - 1);
     const int mn = dkj < dkjm ? dkj : dkjm;
@@ -487,8 +540,7 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face1_kernel(const ProbDev *_
     const int ij = rowi(g, i, j);
     const FaceGeom<double> fg = face_geom3<1>(g, ij);
     double fl[NPRIM], ss;
-    if (hlle) hlle3<1>(pl, pr, fg, fl, ss);
-    else hllc3<1>(pl, pr, fg, fl, ss);
+    solve_face<1, MIX>(P, pen, g.rc1, g.mx1, g.cols1, base + j - 1, base + j, fg, hlle, fl, ss);
     const int64_t f = __ldg(g.f1 + ij) + kk;
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) flux[v * g.nf1 + f] = fl[v];
@@ -503,7 +555,7 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face1_kernel(const ProbDev *_
 // reconstructs every zone once (the reference reconstructs each zone for both of its
 // faces), then each thread solves one face.
 constexpr int T2 = NT3 - 2;
-template <int STAGE>
+template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(NT3, MDG_F3MINB) face2_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                                                      Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, const unsigned char *__restrict__ own,
@@ -531,13 +583,25 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face2_kernel(const ProbDev *_
   __syncthreads();
   if (!pole && t < cnt + 2) {
     // zone k0-1+t from the staged neighbours (interp() on its 3-zone stencil)
-    const RcView<double, true> gz{g.rc2 + base + k0 - 1 + t, g.cols2};
+    if (MIX) {
+      const MixW w = load_mixw(g.mx2 + base + k0 - 1 + t, g.cols2);
 #pragma unroll
-    for (int v = 0; v < 7; v++) {
-      double al, ar;
-      recon_zone<double>(P.interp_order, sv[v][t], sv[v][t + 1], sv[v][t + 2], gz, al, ar);
-      sal[v][t] = al;
-      sar[v][t] = ar;
+      for (int v = 0; v < 7; v++) {
+        float dl, dr;
+        const double a = sv[v][t + 1];
+        mixed_recon((float)(a - sv[v][t]), (float)(sv[v][t + 2] - a), w, dl, dr);
+        sal[v][t] = a + (double)dl;
+        sar[v][t] = a + (double)dr;
+      }
+    } else {
+      const RcView<double, true> gz{g.rc2 + base + k0 - 1 + t, g.cols2};
+#pragma unroll
+      for (int v = 0; v < 7; v++) {
+        double al, ar;
+        recon_zone<double>(P.interp_order, sv[v][t], sv[v][t + 1], sv[v][t + 2], gz, al, ar);
+        sal[v][t] = al;
+        sar[v][t] = ar;
+      }
     }
   }
   __syncthreads();
@@ -587,8 +651,25 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face2_kernel(const ProbDev *_
     const bool hlle = flag_shock<STAGE>(g, i, j, k, own, all0) || flag_shock<STAGE>(g, i, j, k - 1, own, all0);
     const FaceGeom<double> fg = face_geom3<2>(g, ij);
     double fl[NPRIM], ss;
-    if (hlle) hlle3<2>(pl, pr, fg, fl, ss);
-    else hllc3<2>(pl, pr, fg, fl, ss);
+    if (hlle) {
+      hlle3<2>(pl, pr, fg, fl, ss);
+    } else if (!MIX) {
+      hllc3<2>(pl, pr, fg, fl, ss);
+    } else {
+      float sig;
+      int isshock;
+      if (pl[6] == P.gam && pr[6] == P.gam &&
+          riemann_hllc_mixed<2>(pl, pr, fg, gam_const<float>((float)P.gam), fl, sig, isshock)) {
+        ss = (double)sig;
+      } else if (pole) {
+        hllc3<2>(pl, pr, fg, fl, ss);
+      } else {
+        double pen[4][7];
+#pragma unroll
+        for (int q = 0; q < 28; q++) pen[q / 7][q % 7] = sv[q % 7][t + q / 7];
+        face_fp64_3d<2>(P.interp_order, &pen[0][0], g.rc2, g.cols2, base + k - 1, base + k, fg, fl, &ss);
+      }
+    }
     const int64_t f = __ldg(g.f2 + ij) + k;
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) flux[v * g.nf2 + f] = fl[v];
@@ -840,7 +921,8 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
       {h.xc2.data(), h.xc2.size() * sizeof(double)},    {h.sth.data(), h.sth.size() * sizeof(double)},
       {h.cth.data(), h.cth.size() * sizeof(double)},    {h.sphc.data(), h.sphc.size() * sizeof(double)},
       {h.cphc.data(), h.cphc.size() * sizeof(double)},  {h.sphl.data(), h.sphl.size() * sizeof(double)},
-      {h.cphl.data(), h.cphl.size() * sizeof(double)}};
+      {h.cphl.data(), h.cphl.size() * sizeof(double)},  {h.mx0.data(), h.mx0.size() * sizeof(float)},
+      {h.mx1.data(), h.mx1.size() * sizeof(float)},     {h.mx2.data(), h.mx2.size() * sizeof(float)}};
   std::vector<size_t> off(parts.size());
   size_t tot = 0;
   for (size_t q = 0; q < parts.size(); q++) {
@@ -877,6 +959,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   g.sth = (const double *)(b + off[13]); g.cth = (const double *)(b + off[14]);
   g.sphc = (const double *)(b + off[15]); g.cphc = (const double *)(b + off[16]);
   g.sphl = (const double *)(b + off[17]); g.cphl = (const double *)(b + off[18]);
+  g.mx0 = (const float *)(b + off[19]); g.mx1 = (const float *)(b + off[20]); g.mx2 = (const float *)(b + off[21]);
   // flux arrays, shock bits
   e = cudaMalloc(&w->d_flux, sizeof(double) * NPRIM * (size_t)(h.nf0 + h.nf1 + h.nf2));
   if (e != cudaSuccess) return fail3(e);
@@ -918,23 +1001,30 @@ void sweep3_destroy(Sweep3 *w)
 int64_t sweep3_ncell(const Sweep3 *w) { return w->ncell; }
 
 // Kernel launches of one RK stage of the single 3-D problem (slot 0).
-void launch_stage3d(int stage, Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA sst, StateSoA sn,
-                    StateSoA out, cudaStream_t st)
+void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA sst,
+                    StateSoA sn, StateSoA out, cudaStream_t st)
 {
   const Grid3 &g = w->g;
   double *F0 = w->d_flux, *F1 = F0 + NPRIM * g.nf0, *F2 = F1 + NPRIM * g.nf1;
   unsigned char *own = w->d_bits + (size_t)stage * g.ncell, *all0 = w->d_bits + (size_t)2 * g.ncell;
   const Tile3 *t0 = w->d_tiles, *t1 = t0 + w->nt[0], *t2 = t1 + w->nt[1], *tc = t2 + w->nt[2];
+  if (stage == 0) cudaMemsetAsync(all0, 0, (size_t)g.ncell, st);
+  auto faces = [&](auto s0, auto mix) {
+    constexpr int S = decltype(s0)::value;
+    constexpr bool M = decltype(mix)::value;
+    face0_kernel<S, M><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
+    face1_kernel<S, M><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
+    face2_kernel<S, M><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
+  };
+  using I0 = std::integral_constant<int, 0>;
+  using I1 = std::integral_constant<int, 1>;
+  using BF = std::integral_constant<bool, false>;
+  using BT = std::integral_constant<bool, true>;
   if (stage == 0) {
-    cudaMemsetAsync(all0, 0, (size_t)g.ncell, st);
-    face0_kernel<0><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
-    face1_kernel<0><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
-    face2_kernel<0><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
+    if (mixed) faces(I0{}, BT{}); else faces(I0{}, BF{});
     push3_kernel<0><<<w->nt[3], NT3, 0, st>>>(probs, times, g, tc, sst, sn, out, F0, F1, F2);
   } else {
-    face0_kernel<1><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
-    face1_kernel<1><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
-    face2_kernel<1><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
+    if (mixed) faces(I1{}, BT{}); else faces(I1{}, BF{});
     push3_kernel<1><<<w->nt[3], NT3, 0, st>>>(probs, times, g, tc, sst, sn, out, F0, F1, F2);
   }
 }

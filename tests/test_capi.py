@@ -115,10 +115,10 @@ def test_server_calls_reject_null_handle():
     assert L.mdg_server_destroy(None) == 0
 
 
-@pytest.mark.parametrize("precision,nprob,code", [(1, 1, 5), (0, 2, 5)])
-def test_3d_solver_scope_checked_before_device_work(precision, nprob, code):
-    """A 3-D solver advances one problem, plain FP64."""
-    pb = P.sedov_3d(12, 8, 16, r_dep=0.3)
+@pytest.mark.parametrize("precision,nprob,order,code", [(1, 1, 2, 5), (0, 2, 3, 5)])
+def test_3d_solver_scope_checked_before_device_work(precision, nprob, order, code):
+    """A 3-D solver advances one problem; its mixed-precision sweep is parabolic only."""
+    pb = P.sedov_3d(12, 8, 16, r_dep=0.3).copy(hydro_interp_order=order)
     arr = (S.ProblemDesc * nprob)(*[S.desc_of(pb)] * nprob)
     h = ctypes.c_void_p()
     assert S.library().mdg_create(arr, nprob, precision, 0, ctypes.byref(h)) == code
