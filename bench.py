@@ -580,6 +580,7 @@ def cpu_baseline_sedov3d(steps=2):
 
 
 def run_sedov3d(args, ctx):
+    import numpy as np
     import medusa_b200
     from medusa_b200 import problems as P
 
@@ -597,6 +598,34 @@ def run_sedov3d(args, ctx):
     ms_e2e, h2d, d2h = e2e_run(ctx, lambda upload: medusa_b200.Solver(pb, device=ctx.local, upload=upload),
                                [pb], K, W)
     e2e = ctx.world * ncell * K / (ms_e2e / 1e3)
+    # the mixed-precision sweep on the same grid, and its accuracy at equal physical time
+    from medusa_b200 import analytic as A
+    from medusa_b200.solver import PREC_MIXED, grid3d_radial_mean, grid3d_zone_volumes
+    sm = medusa_b200.Solver(pb, precision=PREC_MIXED, device=ctx.local)
+    sm.step(W)
+    sm.synchronize()
+    ms_mix, _ = timed_steps(ctx, sm, K)
+    sm.close()
+    nacc = args.sedov3d_accuracy_steps
+    with medusa_b200.Solver(pb, device=ctx.local) as sf:
+        sf.step(nacc)
+        ref = sf.update_cpu(0)
+        t_end = sf.time(0)[0]
+        m0, e0 = sf.conserved_totals()
+    with medusa_b200.Solver(pb.copy(tmax=t_end), precision=PREC_MIXED, device=ctx.local) as sa:
+        n_mix = 0
+        while sa.time(0)[0] < t_end * (1.0 - 1.0e-12) and n_mix < 4 * nacc:
+            sa.step(10)
+            n_mix += 10
+        mix = sa.update_cpu(0)
+        m1, e1 = sa.conserved_totals()
+    vol = grid3d_zone_volumes(pb)
+    r_of = lambda prim: (int(np.argmax(grid3d_radial_mean(pb, prim[:, 0]))) + 0.5) * pb.dx[0]
+    accuracy = {"steps": nacc, "t": t_end, "l1_rho": A.l1_rel(mix[:, 0], ref[:, 0], vol),
+                "l1_u": A.l1_rel(mix[:, 1], ref[:, 1], vol),
+                "mass_drift_vs_fp64": abs(m1[0] - m0[0]) / m0[0], "energy_drift_vs_fp64": abs(e1[0] - e0[0]) / e0[0],
+                "shock_radius_fp64": r_of(ref), "shock_radius_mixed": r_of(mix),
+                "shock_radius_sedov": A.sedov_shock_radius(1.0, t_end, 1.0, pb.gam), "dr": pb.dx[0]}
     if ctx.rank != 0:
         return
     peak, peak_kind = read_peaks()
@@ -625,6 +654,9 @@ def run_sedov3d(args, ctx):
                      "algorithmic_bytes_per_zone": b_stage1,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
         "clocks": clocks,
+        "mixed": {"value": ctx.world * ncell * K / (ms_mix / 1e3), "unit": "zone-updates/s", "ms_per_step": ms_mix / K,
+                  "precision": "FP32 reconstruction and HLLC wave speeds, FP64 state, fluxes, sources, dt",
+                  "accuracy_vs_fp64": accuracy},
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sedov3d()
@@ -720,6 +752,8 @@ def main():
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
     ap.add_argument("--sedov3d-dims", default="",
                     help="sedov3d: n1,n2,n3 of the grid (default 384,128,256; smaller grids for profiling)")
+    ap.add_argument("--sedov3d-accuracy-steps", type=int, default=60,
+                    help="sedov3d: steps of the FP64 run the mixed run is compared with at equal time")
     ap.add_argument("--server-frac-2d", type=float, default=0.0,
                     help="server: fraction of 2-D Cartesian requests (0.263 = the 70:25 share of 1-D and 2-D "
                          "requests of the mixed stream)")

@@ -138,6 +138,16 @@ def spherical_volumes(n1: int, r_lo: float = 0.0, r_hi: float = 1.0) -> np.ndarr
     return e[1:] ** 3 - e[:-1] ** 3
 
 
+# R_s = xi0 (E t^2 / rho)^(1/5) of the spherical Sedov-Taylor blast (Sedov 1959; the
+# constants used by G. I. Taylor 1950 and tabulated by Kamm & Timmes 2007)
+SEDOV_XI0 = {1.4: 1.033, 5.0 / 3.0: 1.152}
+
+
+def sedov_shock_radius(energy: float, t: float, rho: float = 1.0, gam: float = 1.4) -> float:
+    """Shock radius of the point blast of energy `energy` in gas of density rho at time t."""
+    return SEDOV_XI0[gam] * (energy * t * t / rho) ** 0.2
+
+
 def l1_rel(a: np.ndarray, b: np.ndarray, w=None) -> float:
     """sum |a - b| w / sum |b| w (w = zone volumes; uniform if None)."""
     a = np.asarray(a, dtype=np.float64)

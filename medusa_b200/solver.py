@@ -185,6 +185,39 @@ def grid3d_geometry(pb: "_pb.Problem") -> np.ndarray:
     return out
 
 
+def grid3d_zone_volumes(pb: "_pb.Problem") -> np.ndarray:
+    """Volume of every interior zone of a 3-D dendritic problem, in zone order."""
+    nj, nk, n = grid3d_counts(pb)
+    geo = grid3d_geometry(pb)
+    n1 = pb.n[0]
+    njx = [int(nj[1]), int(nj[0])] + [int(x) for x in nj] + [int(nj[-1])] * 2   # rows i = -2 .. n1+1
+    vol = np.empty(n)
+    r = c = q = 0
+    for i in range(-2, n1 + 2):
+        for j in range(-2, njx[i + 2] + 2):
+            if 0 <= i < n1 and 0 <= j < nj[i]:
+                vol[c:c + nk[q]] = geo[r, 0]
+                c += int(nk[q])
+                q += 1
+            r += 1
+    return vol
+
+
+def grid3d_radial_mean(pb: "_pb.Problem", field: np.ndarray) -> np.ndarray:
+    """Volume-weighted mean of a zone field over each radial row of a 3-D problem."""
+    nj, nk, n = grid3d_counts(pb)
+    vol = grid3d_zone_volumes(pb)
+    out = np.zeros(pb.n[0])
+    c = q = 0
+    for i in range(pb.n[0]):
+        cnt = int(nk[q:q + nj[i]].sum())
+        w = vol[c:c + cnt]
+        out[i] = float(np.sum(field[c:c + cnt] * w) / np.sum(w))
+        c += cnt
+        q += int(nj[i])
+    return out
+
+
 def _check(rc: int, where: str):
     if rc != 0:
         L = library()

@@ -74,41 +74,10 @@ def test_3d_mass_change_is_the_outer_boundary_flux():
 
 
 # ---------------------------------------------------------------- mixed precision
-SEDOV_XI0 = {1.4: 1.033, 5.0 / 3.0: 1.152}   # R_s = xi0 (E t^2 / rho)^(1/5), Sedov (1959)
-
-
-def _zone_volumes(pb):
-    """Volume of every interior zone in zone order, from the row geometry."""
-    from medusa_b200 import solver as S
-    nj, nk, n = S.grid3d_counts(pb)
-    geo = S.grid3d_geometry(pb)
-    n1 = pb.n[0]
-    njx = [nj[1], nj[0]] + list(nj) + [nj[-1], nj[-1]]   # rows i = -2 .. n1+1
-    vol = np.empty(n)
-    r, c, q = 0, 0, 0
-    for i in range(-2, n1 + 2):
-        for j in range(-2, njx[i + 2] + 2):
-            if 0 <= i < n1 and 0 <= j < nj[i]:
-                vol[c:c + nk[q]] = geo[r, 0]
-                c += nk[q]
-                q += 1
-            r += 1
-    assert c == n
-    return vol
-
-
 def _shock_radius(pb, prim):
-    """Radius of the density maximum, averaged over the zones of each radial row."""
-    from medusa_b200 import solver as S
-    nj, nk, _ = S.grid3d_counts(pb)
-    rho = np.zeros(pb.n[0])
-    c, q = 0, 0
-    for i in range(pb.n[0]):
-        cnt = int(sum(nk[q:q + nj[i]]))
-        rho[i] = prim[c:c + cnt, 0].mean()
-        c += cnt
-        q += nj[i]
-    return (np.argmax(rho) + 0.5) * pb.dx[0]
+    """Radius of the largest radial-row mean density."""
+    from medusa_b200.solver import grid3d_radial_mean
+    return (np.argmax(grid3d_radial_mean(pb, prim[:, 0])) + 0.5) * pb.dx[0]
 
 
 def test_3d_mixed_matches_fp64_at_equal_time():
@@ -135,13 +104,14 @@ def test_3d_mixed_matches_fp64_at_equal_time():
         t_mix = s.time(0)[0]
         m1, e1 = s.conserved_totals()
     assert abs(t_mix - t_end) <= 1.0e-8 * t_end
-    vol = _zone_volumes(pb)
+    from medusa_b200.solver import grid3d_zone_volumes
+    vol = grid3d_zone_volumes(pb)
     l1_rho = A.l1_rel(mix[:, 0], ref[:, 0], vol)
     l1_u = A.l1_rel(mix[:, 1], ref[:, 1], vol)
     drift_m = abs(m1[0] - m0[0]) / m0[0]
     drift_e = abs(e1[0] - e0[0]) / e0[0]
     r_ref, r_mix = _shock_radius(pb, ref), _shock_radius(pb, mix)
-    r_sedov = SEDOV_XI0[1.4] * (1.0 * t_end ** 2 / 1.0) ** 0.2
+    r_sedov = A.sedov_shock_radius(1.0, t_end, 1.0, 1.4)
     record("sweep3d_mixed_sedov_48x32x64", l1_rho=l1_rho, l1_u=l1_u, drift_mass=drift_m, drift_energy=drift_e,
            r_fp64=r_ref, r_mixed=r_mix, r_sedov=r_sedov, t=t_end)
     assert np.all(np.isfinite(mix))

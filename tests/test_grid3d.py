@@ -87,3 +87,12 @@ def test_fixture_reproduced_by_live_reference(name):
     snaps = pyoracle.run_reference(pb, n, every=n)
     assert np.array_equal(snaps[-1][4], g["prim"])
     assert snaps[-1][1] == float(g["t"])
+
+
+def test_zone_volumes_fill_the_sphere():
+    pb = P.sedov_3d(24, 16, 32, r_dep=0.2)
+    vol = S.grid3d_zone_volumes(pb)
+    assert vol.shape == (pb.ncell,) and np.all(vol > 0)
+    assert abs(vol.sum() - 4.0 / 3.0 * np.pi) <= 1.0e-12
+    prof = S.grid3d_radial_mean(pb, np.ones(pb.ncell))
+    assert np.allclose(prof, 1.0, rtol=0, atol=1e-14)
