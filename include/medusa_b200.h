@@ -216,13 +216,16 @@ int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double *prim_in, 
  * every admitted problem together, batching their uneven grids into the same stage
  * launches (1-D, for MDG_PREC_MIXED: persistent CTAs fed from a device work queue, each
  * round of steps_per_round steps replayed from one CUDA graph; 2-D: the plain FP64 split
- * sweep in either precision, on a second stream that runs beside the 1-D launches).  A
+ * sweep in either precision, on a second stream that runs beside the 1-D launches; 3-D
+ * dendritic spherical problems on that stream too, each with its own grid, in the
+ * server's precision).  A
  * request is a problem description, its initial state ([zone][5], as mdg_upload_state)
  * and its end time desc->tmax; it runs the main.c time loop until t >= tmax and is then
  * retired.
  *
  * Admission is by device-memory footprint: the arenas are sized once from hbm_bytes
- * (1-D states and every request's tables) and hbm_bytes_2d (2-D states), and a queued
+ * (1-D states and every request's tables) and hbm_bytes_2d (2-D states), a 3-D request
+ * holds its own grid and state counted against hbm_bytes_3d, and a queued
  * request is admitted between rounds when a slot and contiguous ranges of n1 + 4 zone
  * units (2-D: n1 + n2 + 8 table units and (n1 + 3) x n2 cells) are free (requests that do
  * not fit yet wait; smaller ones behind them may go first).  A finished problem's state
@@ -244,6 +247,8 @@ typedef struct mdg_server_config {
   int ctas_per_sm;          /* mixed sweep: persistent CTAs per SM (0: as many as fit) */
   long long hbm_bytes_2d;   /* device memory for resident 2-D states (0: 2-D requests refused) */
   int max_cells_2d;         /* largest n1 x n2 a 2-D request may have */
+  long long hbm_bytes_3d;   /* device memory for resident 3-D problems, state and grid
+                               (0: 3-D requests refused) */
 } mdg_server_config;
 
 #define MDG_REQ_QUEUED  0

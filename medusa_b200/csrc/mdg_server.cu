@@ -120,6 +120,9 @@ struct Request {
   int64_t seg = -1, units = 0;  // range of the unit arena
   int64_t seg2 = -1, cells = 0; // range of the cell arena (2-D)
   int64_t ncell = 0;            // zones of the problem
+  Sweep3 *s3 = nullptr;         // 3-D: its own grid tables, face fluxes and shock bits
+  double *d_state3 = nullptr;   // 3-D: state P then PH, 5 arrays of ncell each
+  int64_t bytes3 = 0;           // 3-D: device memory held (counted against hbm_bytes_3d)
   double t = 0.0;
   int istep = 0;
   Clock::time_point t_submit, t_admit, t_done;
@@ -167,6 +170,10 @@ struct mdg_server {
   cudaStream_t stream2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int graph_ntx2 = -1, graph_nty2 = -1;   // 2-D tile counts the graph was captured with
+  // 3-D lane: resident 3-D requests (each with its own grid), on the second stream
+  std::vector<Request *> jobs3;
+  int64_t bytes3_in_use = 0;
+  int jobs3_version = 0, graph_jobs3_version = -1;
   cudaGraphExec_t graph = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // requests
@@ -205,7 +212,18 @@ void free_server(mdg_server *s)
   if (s->h_ret) cudaFreeHost(s->h_ret);
   if (s->stream2) cudaStreamDestroy(s->stream2);
   if (s->stream) cudaStreamDestroy(s->stream);
-  for (auto &kv : s->reqs) delete kv.second;
+  for (auto &kv : s->reqs) {
+    sweep3_destroy(kv.second->s3);
+    cudaFree(kv.second->d_state3);
+    delete kv.second;
+  }
+}
+
+StateSoA soa3(const Request *r, int which)
+{
+  StateSoA q;
+  for (int v = 0; v < NPRIM; v++) q.v[v] = r->d_state3 + (int64_t)(which * NPRIM + v) * r->ncell;
+  return q;
 }
 
 // bytes of device memory per zone unit: state P and PH, RC and GF tables, FP32 weights
@@ -243,7 +261,7 @@ int queue_round(mdg_server *s, int nsteps)
 {
   const bool mixed = s->cfg.precision == MDG_PREC_MIXED;
   const int grid = mixed ? persistent_grid(s) : 0;
-  const bool lane2 = s->ntx2 > 0;
+  const bool lane2 = s->ntx2 > 0 || !s->jobs3.empty();
   for (int k = 0; k < nsteps; k++) {
     launch_dt_finalize(s->d_probs, s->d_times, s->max_probs, s->d_err, s->stream);
     if (lane2) {
@@ -260,10 +278,18 @@ int queue_round(mdg_server *s, int nsteps)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     }
     if (lane2) {
-      launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
-                     s->P2, s->P2, s->ACC2, s->PH2, s->d_shock0, s->d_shock1, s->stream2);
-      launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
-                     s->PH2, s->P2, s->ACC2, s->P2, s->d_shock0, s->d_shock1, s->stream2);
+      if (s->ntx2 > 0) {
+        launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+                       s->P2, s->P2, s->ACC2, s->PH2, s->d_shock0, s->d_shock1, s->stream2);
+        launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+                       s->PH2, s->P2, s->ACC2, s->P2, s->d_shock0, s->d_shock1, s->stream2);
+      }
+      for (Request *r : s->jobs3) {
+        ProbDev *pr = s->d_probs + r->slot;
+        ProbTime *tr = s->d_times + r->slot;
+        launch_stage3d(0, mixed, r->s3, pr, tr, soa3(r, 0), soa3(r, 0), soa3(r, 1), s->stream2);
+        launch_stage3d(1, mixed, r->s3, pr, tr, soa3(r, 1), soa3(r, 0), soa3(r, 0), s->stream2);
+      }
       SCK(cudaEventRecord(s->ev_join, s->stream2));
       SCK(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
     }
@@ -279,6 +305,22 @@ int admit(mdg_server *s, Request *r)
   const int64_t w = r->units, seg = r->seg;
   ProbDev P;
   make_probdev(d, P);
+  if (d.ndim == 3) {
+    // its own grid (built at submission); the AoS initial state is staged in PH
+    P.n2 = d.n2;
+    P.ncell = r->ncell;
+    SCK(cudaMemcpyAsync(s->d_probs + r->slot, &P, sizeof P, cudaMemcpyHostToDevice, s->stream));
+    double *stage = r->d_state3 + (int64_t)NPRIM * r->ncell;
+    SCK(cudaMemcpyAsync(stage, r->ic.data(), sizeof(double) * NPRIM * r->ncell, cudaMemcpyHostToDevice, s->stream));
+    launch_aos_to_soa(stage, soa3(r, 0), 0, r->ncell, s->stream);
+    launch_reset_time(s->d_times, r->slot, s->stream);
+    launch_initial_estimate3(r->s3, s->d_probs + r->slot, s->d_times + r->slot, soa3(r, 0), s->stream);
+    SCK(cudaGetLastError());
+    s->launches += 3;
+    s->jobs3.push_back(r);
+    s->jobs3_version++;
+    return MDG_OK;
+  }
   P.cell_off = seg;
   P.geo_off = seg;
   P.sparse_conn = r->sparse;
@@ -345,7 +387,11 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
     const int64_t n = r->ncell;
     const bool two = r->desc.ndim == 2;
     const double *src = two ? s->P2.v[0] + r->seg2 : s->P.v[0] + r->seg;
-    const size_t pitch = sizeof(double) * (two ? s->cells : s->units);
+    size_t pitch = sizeof(double) * (two ? s->cells : s->units);
+    if (r->desc.ndim == 3) {
+      src = r->d_state3;
+      pitch = sizeof(double) * n;
+    }
     SCK(cudaMemcpy2DAsync(s->h_ret + off, sizeof(double) * n, src, pitch, sizeof(double) * n, NPRIM,
                           cudaMemcpyDeviceToHost, s->stream));
     off += (size_t)NPRIM * n;
@@ -366,8 +412,19 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
     r->err = T.err;
     r->t_done = now;
     s->slots[k] = nullptr;
-    s->alloc.release(r->seg, r->units);
-    s->units_in_use -= r->units;
+    if (r->desc.ndim == 3) {
+      // the round has ended (retire_all waited for the stream): give its memory back
+      s->jobs3.erase(std::find(s->jobs3.begin(), s->jobs3.end(), r));
+      s->jobs3_version++;
+      sweep3_destroy(r->s3);
+      r->s3 = nullptr;
+      cudaFree(r->d_state3);
+      r->d_state3 = nullptr;
+      s->bytes3_in_use -= r->bytes3;
+    } else {
+      s->alloc.release(r->seg, r->units);
+      s->units_in_use -= r->units;
+    }
     if (r->cells > 0) {
       s->alloc2.release(r->seg2, r->cells);
       s->cells_in_use -= r->cells;
@@ -401,6 +458,17 @@ int round_once(mdg_server *s, int *active_out)
       for (int k = 0; k < s->max_probs; k++)
         if (!s->slots[k]) { slot = k; break; }
       if (slot < 0) break;
+      if (r->desc.ndim == 3) {
+        if (s->bytes3_in_use + r->bytes3 > s->cfg.hbm_bytes_3d) { ++it; continue; }
+        s->bytes3_in_use += r->bytes3;
+        r->slot = slot;
+        s->slots[slot] = r;
+        r->status = MDG_REQ_RUNNING;
+        r->t_admit = Clock::now();
+        adm.push_back(r);
+        it = s->queue.erase(it);
+        continue;
+      }
       const int64_t seg = s->alloc.alloc(r->units);
       if (seg < 0) { ++it; continue; }
       int64_t seg2 = -1;
@@ -436,7 +504,7 @@ int round_once(mdg_server *s, int *active_out)
     std::vector<Tile> tl, xt, yt;
     for (int k = 0; k < s->max_probs; k++) {
       const Request *r = s->slots[k];
-      if (!r) continue;
+      if (!r || r->desc.ndim == 3) continue;   // 3-D problems run on their own grids
       if (r->desc.ndim == 2) {
         // the solver's 2-D tiling: direction-0 tiles of TIX2 rows x NTX2 columns,
         // direction-1 tiles of TIY2 rows x TJY2 columns
@@ -477,7 +545,7 @@ int round_once(mdg_server *s, int *active_out)
     const int K = s->cfg.steps_per_round;
     SCK(cudaEventRecord(s->ev0, s->stream));
     if (s->cfg.precision == MDG_PREC_MIXED) {
-      if (s->graph && (s->graph_ntx2 != s->ntx2 || s->graph_nty2 != s->nty2)) {
+      if (s->graph && (s->graph_ntx2 != s->ntx2 || s->graph_nty2 != s->nty2 || s->graph_jobs3_version != s->jobs3_version)) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
       }
@@ -499,6 +567,7 @@ int round_once(mdg_server *s, int *active_out)
         }
         s->graph_ntx2 = s->ntx2;
         s->graph_nty2 = s->nty2;
+        s->graph_jobs3_version = s->jobs3_version;
       }
       SCK(cudaGraphLaunch(s->graph, s->stream));
     } else {
@@ -508,7 +577,9 @@ int round_once(mdg_server *s, int *active_out)
     SCK(cudaEventRecord(s->ev1, s->stream));
     SCK(cudaGetLastError());
     // per step: dt reduction, two 1-D stages, time update; four 2-D direction sweeps
-    s->launches += (long long)K * (4 + (s->ntx2 > 0 ? 4 : 0));
+    long long per_step = 4 + (s->ntx2 > 0 ? 4 : 0);
+    for (size_t q = 0; q < s->jobs3.size(); q++) per_step += 8;
+    s->launches += (long long)K * per_step;
   }
   // 4. retire the problems that reached their end time (or failed)
   SCK(cudaMemcpyAsync(s->h_times, s->d_times, sizeof(ProbTime) * s->max_probs, cudaMemcpyDeviceToHost, s->stream));
@@ -579,6 +650,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   const int64_t units = c.hbm_bytes / bpu;
   if (units < c.max_zones + 2 * NG) return sfail(MDG_ERR_INVALID, "hbm_bytes too small for one problem of max_zones");
   if (c.hbm_bytes_2d < 0) return sfail(MDG_ERR_INVALID, "hbm_bytes_2d must not be negative");
+  if (c.hbm_bytes_3d < 0) return sfail(MDG_ERR_INVALID, "hbm_bytes_3d must not be negative");
   const int64_t cells = c.hbm_bytes_2d / bytes_per_cell_2d();
   if (cells > 0) {
     if (c.max_cells_2d < 4 || c.max_cells_2d > (1 << 30))
@@ -661,11 +733,46 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
 {
   if (!s || !desc || !prim) return sfail(MDG_ERR_INVALID, "server/desc/prim");
   std::string why;
-  const int ndim = desc->ndim == 2 ? 2 : 1;
+  const int ndim = (desc->ndim == 2 || desc->ndim == 3) ? desc->ndim : 1;
   int rc = validate_desc(*desc, ndim, why);
   if (rc != MDG_OK) return sfail(rc, "request: " + why);
   if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
     return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
+  if (ndim == 3) {
+    if (s->cfg.hbm_bytes_3d <= 0) return sfail(MDG_ERR_NOTIMPL, "request: the server takes no 3-D requests");
+    if (s->cfg.precision == MDG_PREC_MIXED && desc->hydro_interp_order != 3)
+      return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep is built for parabolic reconstruction");
+    // its grid tables, face fluxes and state, built here in the submitting thread
+    SCK(cudaSetDevice(s->cfg.device));
+    Request *r = new Request();
+    r->desc = *desc;
+    rc = sweep3_create(*desc, &r->s3, why);
+    if (rc != MDG_OK) {
+      delete r;
+      return sfail(rc, "request: 3-D grid: " + why);
+    }
+    r->ncell = sweep3_ncell(r->s3);
+    const cudaError_t e = cudaMalloc(&r->d_state3, sizeof(double) * 2 * NPRIM * r->ncell);
+    r->bytes3 = sweep3_bytes(r->s3) + (int64_t)sizeof(double) * 2 * NPRIM * r->ncell;
+    if (e != cudaSuccess || r->bytes3 > s->cfg.hbm_bytes_3d) {
+      sweep3_destroy(r->s3);
+      if (e == cudaSuccess) cudaFree(r->d_state3);
+      delete r;
+      return sfail(MDG_ERR_OUTOFMEM, "request: the 3-D problem does not fit in hbm_bytes_3d");
+    }
+    r->ic.assign(prim, prim + (size_t)NPRIM * r->ncell);
+    r->t_submit = Clock::now();
+    {
+      std::lock_guard<std::mutex> lk(s->mu);
+      r->id = s->next_id++;
+      s->reqs[r->id] = r;
+      s->queue.push_back(r);
+      s->submitted++;
+    }
+    s->cv.notify_all();
+    if (id) *id = r->id;
+    return MDG_OK;
+  }
   if (ndim == 2) {
     if (s->cells == 0) return sfail(MDG_ERR_NOTIMPL, "request: the server was created without a 2-D arena");
     if ((int64_t)desc->n1 * desc->n2 > s->cfg.max_cells_2d)
@@ -815,8 +922,9 @@ int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st)
   st->wait_p50 = percentile(s->wait, 0.50);
   st->wait_p99 = percentile(s->wait, 0.99);
   const int64_t bpu = bytes_per_unit(s->cfg.precision);
-  st->hbm_capacity = (double)s->units * bpu + (double)s->cells * bytes_per_cell_2d();
-  st->hbm_in_use = (double)s->units_in_use * bpu + (double)s->cells_in_use * bytes_per_cell_2d();
+  st->hbm_capacity = (double)s->units * bpu + (double)s->cells * bytes_per_cell_2d() + (double)s->cfg.hbm_bytes_3d;
+  st->hbm_in_use = (double)s->units_in_use * bpu + (double)s->cells_in_use * bytes_per_cell_2d() +
+                   (double)s->bytes3_in_use;
   st->kernel_launches = s->launches.load();
   return MDG_OK;
 }

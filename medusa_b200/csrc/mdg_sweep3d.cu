@@ -895,6 +895,7 @@ struct Sweep3 {
   Tile3 *d_tiles = nullptr;        // face0 | face1 | face2 | zone tiles
   int nt[4] = {0, 0, 0, 0};
   int64_t ncell = 0;
+  int64_t bytes = 0;               // device memory held
 };
 
 static void tiles_of_rows(std::vector<Tile3> &out, int i, int j, int count, int chunk = NT3)
@@ -929,6 +930,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
     off[q] = tot;
     tot += (parts[q].second + 255) / 256 * 256;
   }
+  w->bytes = (int64_t)tot + (int64_t)sizeof(double) * NPRIM * (h.nf0 + h.nf1 + h.nf2) + 3 * h.ncell;
   std::vector<char> host(tot, 0);
   for (size_t q = 0; q < parts.size(); q++) std::memcpy(host.data() + off[q], parts[q].first, parts[q].second);
   auto fail3 = [&](cudaError_t e) {
@@ -999,6 +1001,7 @@ void sweep3_destroy(Sweep3 *w)
 }
 
 int64_t sweep3_ncell(const Sweep3 *w) { return w->ncell; }
+int64_t sweep3_bytes(const Sweep3 *w) { return w->bytes; }
 
 // Kernel launches of one RK stage of the single 3-D problem (slot 0).
 void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA sst,

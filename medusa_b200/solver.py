@@ -53,7 +53,8 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("precision", ctypes.c_int), ("hbm_bytes", ctypes.c_longlong),
                 ("max_problems", ctypes.c_int), ("max_zones", ctypes.c_int), ("steps_per_round", ctypes.c_int),
                 ("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("hbm_bytes_2d", ctypes.c_longlong), ("max_cells_2d", ctypes.c_int)]
+                ("hbm_bytes_2d", ctypes.c_longlong), ("max_cells_2d", ctypes.c_int),
+                ("hbm_bytes_3d", ctypes.c_longlong)]
 
 
 class ServerStats(ctypes.Structure):
@@ -367,16 +368,18 @@ REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
 
 
 class Server:
-    """Solve server (mdg_server_*): 1-D and 2-D problems resident on one GPU, admitted by
-    their device-memory footprint and advanced together; each request runs to its end
-    time (the problem's tmax).  2-D requests need hbm_bytes_2d > 0."""
+    """Solve server (mdg_server_*): 1-D, 2-D and 3-D problems resident on one GPU, admitted
+    by their device-memory footprint and advanced together; each request runs to its end
+    time (the problem's tmax).  2-D requests need hbm_bytes_2d > 0, 3-D requests
+    hbm_bytes_3d > 0."""
 
     def __init__(self, precision: int = PREC_MIXED, device: int = 0, hbm_bytes: int = 2 << 30,
                  max_problems: int = 4096, max_zones: int = 16384, steps_per_round: int = 20,
-                 threads: int = 64, ctas_per_sm: int = 0, hbm_bytes_2d: int = 0, max_cells_2d: int = 1 << 20):
+                 threads: int = 64, ctas_per_sm: int = 0, hbm_bytes_2d: int = 0, max_cells_2d: int = 1 << 20,
+                 hbm_bytes_3d: int = 0):
         L = library()
         c = ServerConfig(device, precision, int(hbm_bytes), max_problems, max_zones, steps_per_round, threads,
-                         ctas_per_sm, int(hbm_bytes_2d), int(max_cells_2d))
+                         ctas_per_sm, int(hbm_bytes_2d), int(max_cells_2d), int(hbm_bytes_3d))
         h = ctypes.c_void_p()
         _check(L.mdg_server_create(ctypes.byref(c), ctypes.byref(h)), "mdg_server_create")
         self._h = h

@@ -201,6 +201,46 @@ def test_server_2d_slot_reuse_and_graph_recapture():
             assert np.array_equal(prim, ref), pb.name
 
 
+def _mix_3d():
+    return [P.sedov_3d(12, 8, 16, r_dep=0.3).copy(tmax=0.004, name="sedov3d_a"),
+            P.sedov_3d(16, 8, 16, r_dep=0.3, noise=0.05).copy(tmax=0.006, name="sedov3d_b")]
+
+
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_server_3d_requests_equal_solver(precision):
+    """3-D requests (each with its own dendritic grid, in the server's precision) beside
+    1-D and 2-D ones: every result is the solver's run of the same problem, bit for bit."""
+    reqs3 = _mix_3d()
+    reqs = [(pb, precision) for pb in reqs3] + [(pb, precision) for pb in _mix()[:2]] + \
+           [(pb, PREC_FP64) for pb in _mix_2d()[:1]]
+    with Server(precision=precision, hbm_bytes=256 << 20, max_problems=32, max_zones=4096, steps_per_round=9,
+                hbm_bytes_2d=64 << 20, max_cells_2d=1 << 16, hbm_bytes_3d=512 << 20) as srv:
+        ids = []
+        for k, (pb, prec) in enumerate(reqs):
+            ids.append(srv.submit(pb))
+            srv.run(1 + k % 2)           # arrivals between rounds: graph recaptures
+        srv.run(0)
+        assert srv.stats()["completed"] == len(reqs)
+        for rid, (pb, prec) in zip(ids, reqs):
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_result(pb, prec)
+            assert t == rt and ist == rist, pb.name
+            assert np.array_equal(prim, ref), pb.name
+
+
+def test_server_3d_budget_and_refusal():
+    pb = _mix_3d()[0]
+    with Server(precision=PREC_FP64, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
+        with pytest.raises(MdgError) as e:
+            srv.submit(pb)
+        assert e.value.code == 5
+    with Server(precision=PREC_FP64, hbm_bytes=64 << 20, max_problems=4, max_zones=4096,
+                hbm_bytes_3d=1 << 16) as srv:
+        with pytest.raises(MdgError) as e:
+            srv.submit(pb)
+        assert e.value.code == 6
+
+
 def test_server_2d_refused_without_arena():
     pb = _mix_2d()[0]
     with Server(precision=PREC_MIXED, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
