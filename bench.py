@@ -325,7 +325,8 @@ def run_reference_arm(args, ctx):
         dtype = "f64"
     elif args.workload == "server":
         from medusa_b200 import loadgen
-        probs = loadgen.request_stream(args.server_requests, seed=11, frac_2d=args.server_frac_2d)
+        probs = loadgen.request_stream(args.server_requests, seed=11, frac_2d=args.server_frac_2d,
+                                       frac_3d=args.server_frac_3d)
         cb = cpu_baseline_ensemble(probs)
         config = {"workload": server_workload_name(args), "requests": len(probs)}
         dtype = "f64"
@@ -664,6 +665,10 @@ def run_sedov3d(args, ctx):
 
 
 def server_workload_name(args):
+    if args.server_frac_3d > 0.0:
+        return "server_stream_%d%%_1d_%d%%_2d_%d%%_3d_sedov_128x64x128" % (
+            round(100 * (1 - args.server_frac_2d - args.server_frac_3d)), round(100 * args.server_frac_2d),
+            round(100 * args.server_frac_3d))
     if args.server_frac_2d > 0.0:
         return "server_stream_1d_spherical_256_8192_and_%d%%_2d_cartesian_128sq_1024sq" % round(
             100 * args.server_frac_2d)
@@ -681,16 +686,19 @@ def run_server(args, ctx):
     from medusa_b200.solver import PREC_FP64, PREC_MIXED, Server
 
     rates = [float(r) for r in args.server_rates.split(",")]
-    reqs = loadgen.request_stream(args.server_requests, seed=11 + ctx.rank, frac_2d=args.server_frac_2d)
+    reqs = loadgen.request_stream(args.server_requests, seed=11 + ctx.rank, frac_2d=args.server_frac_2d,
+                                  frac_3d=args.server_frac_3d)
     spr = 20
     sweep = {}
     best = {}
     two_d = args.server_frac_2d > 0.0
+    three_d = args.server_frac_3d > 0.0
     for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64)):
         sweep[name] = []
         srv = Server(precision=prec, device=ctx.local, hbm_bytes=24 << 30, max_problems=16384, max_zones=8192,
                      steps_per_round=spr, threads=64, ctas_per_sm=12,
-                     hbm_bytes_2d=(32 << 30) if two_d else 0, max_cells_2d=(1 << 20) + 4096)
+                     hbm_bytes_2d=(32 << 30) if two_d else 0, max_cells_2d=(1 << 20) + 4096,
+                     hbm_bytes_3d=(24 << 30) if three_d else 0)
         srv.start()
         # warm-up: graph capture and first admissions
         loadgen.drive(srv, reqs[:32], math.inf)
@@ -719,9 +727,10 @@ def run_server(args, ctx):
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": server_workload_name(args),
                    "requests": len(reqs), "rates_req_per_s": args.server_rates,
-                   "mix": ("1-D spherical Sod/Noh/Sedov and %d%% 2-D Cartesian KH/RT (FP64 split sweep in both "
-                           "server precisions) to their end times; the 3-D share is left out (no 3-D sweep)"
-                           % round(100 * args.server_frac_2d)) if two_d else
+                   "mix": ("1-D spherical Sod/Noh/Sedov, %d%% 2-D Cartesian KH/RT (FP64 split sweep in both "
+                           "server precisions) and %d%% 3-D Sedov on the 128x64x128 dendritic grid (the "
+                           "server's precision) to their end times"
+                           % (round(100 * args.server_frac_2d), round(100 * args.server_frac_3d))) if two_d else
                           "1-D spherical Sod/Noh/Sedov to their end times (the 1-D part of the request mix)",
                    "steps_per_round": spr, "parallelism": "single" if ctx.world == 1 else "independent servers"},
         "p50_s": m["latency_p50_s"], "p99_s": m["latency_p99_s"],
@@ -757,6 +766,8 @@ def main():
     ap.add_argument("--server-frac-2d", type=float, default=0.0,
                     help="server: fraction of 2-D Cartesian requests (0.263 = the 70:25 share of 1-D and 2-D "
                          "requests of the mixed stream)")
+    ap.add_argument("--server-frac-3d", type=float, default=0.0,
+                    help="server: fraction of 3-D Sedov requests (0.05 with --server-frac-2d 0.25: the C5 mix)")
     ap.add_argument("--server-seconds", type=float, default=3.0,
                     help="server: length of the arrival window at each finite rate")
     ap.add_argument("--no-cpu-baseline", action="store_true")

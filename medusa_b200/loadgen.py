@@ -6,7 +6,8 @@ Sedov-type, zone counts log-uniform in a range, density/pressure ratios and gamm
 it runs a few hundred steps at the largest sizes; a fraction `frac_2d` of the requests are
 2-D Cartesian instead (Kelvin-Helmholtz on the unit square or Rayleigh-Taylor on
 [0, 0.5] x [0, 1] with rho 2 over 1, g = -0.1 and velocity noise 0.01, zone counts
-log-uniform in [zmin_2d, zmax_2d]).  :func:`drive` submits such a stream to a
+log-uniform in [zmin_2d, zmax_2d]) and a fraction `frac_3d` 3-D Sedov blasts on the
+dendritic spherical grid (dims_3d before coarsening).  :func:`drive` submits such a stream to a
 running :class:`medusa_b200.solver.Server` with Poisson arrivals at a given rate (all at
 once for rate=inf), waits for every result and reports throughput and latency
 percentiles.
@@ -22,7 +23,7 @@ import numpy as np
 from . import problems as P
 
 # end time per kind: a fixed fraction of the sound-crossing time of the unit sphere
-T_END = {"sod": 0.05, "noh": 0.08, "sedov": 0.02, "kh": 0.05, "rt": 0.1}
+T_END = {"sod": 0.05, "noh": 0.08, "sedov": 0.02, "kh": 0.05, "rt": 0.1, "sedov3d": 0.01}
 
 
 def _request_2d(m: int, u) -> "P.Problem":
@@ -41,7 +42,8 @@ def _request_2d(m: int, u) -> "P.Problem":
 
 
 def request_stream(count: int, seed: int = 11, nmin: int = 256, nmax: int = 8192, frac_2d: float = 0.0,
-                   zmin_2d: int = 128 * 128, zmax_2d: int = 1024 * 1024) -> list:
+                   zmin_2d: int = 128 * 128, zmax_2d: int = 1024 * 1024, frac_3d: float = 0.0,
+                   dims_3d: tuple = (128, 64, 128)) -> list:
     """`count` seeded requests (Problems whose tmax is the end time)."""
     u = P.uniform01(seed, 6 * count).reshape(count, 6)
     # the 2-D draws come from their own stream, so the 1-D requests of a seed stay the same
@@ -53,6 +55,12 @@ def request_stream(count: int, seed: int = 11, nmin: int = 256, nmax: int = 8192
         if u2[m, 0] < frac_2d:
             z = math.exp(math.log(zmin_2d) + u2[m, 1] * (math.log(zmax_2d) - math.log(zmin_2d)))
             out.append(_request_2d(m, (z, u2[m, 2], u2[m, 3])))
+            continue
+        if u2[m, 0] < frac_2d + frac_3d:
+            pb = P.sedov_3d(*dims_3d, r_dep=0.02, noise=0.01, seed=3000 + m)
+            pb = pb.copy(tmax=T_END["sedov3d"] * (0.5 + u2[m, 3]))
+            pb.name = "req%05d_sedov3d" % m
+            out.append(pb)
             continue
         n1 = int(round(math.exp(math.log(nmin) + u[m, 0] * (math.log(nmax) - math.log(nmin)))))
         n1 = max(nmin, min(nmax, n1))
