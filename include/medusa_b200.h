@@ -285,6 +285,26 @@ int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st);
 int mdg_server_destroy(mdg_server *s);
 
 /*
+ * Output path (the reference's update_cpu() + dump, main.c:289-291; its ASCII dump
+ * dump_ascii1, io.c:111-220, written for restarts at main.c:271).
+ *   mdg_snapshot           queues, on the solver's stream, a copy of problem `prob`'s
+ *                          state and EOS records ([zone][5] each, as mdg_download_state)
+ *                          and its time, then a copy to pinned host memory on a second
+ *                          stream; returns at once, and later mdg_step calls overlap the
+ *                          host copy (one snapshot in flight: a new one waits for the last);
+ *   mdg_snapshot_read      waits for the snapshot and copies it out (any pointer may be NULL);
+ *   mdg_snapshot_write_ascii1  waits and writes it as dump_ascii1 does (1-D problems):
+ *                          "# t", then per zone x (r on spherical grids), rho, u,
+ *                          scale[0][0] v^1, v^2, v^3, the EOS record, the enclosed mass at
+ *                          the zone centre and the two lapse columns, in its printf formats;
+ *   mdg_dump_ascii1        snapshot + write.
+ */
+int mdg_snapshot(mdg_solver *s, int prob);
+int mdg_snapshot_read(mdg_solver *s, double *prim, double *eos, double *t);
+int mdg_snapshot_write_ascii1(mdg_solver *s, const char *path);
+int mdg_dump_ascii1(mdg_solver *s, int prob, const char *path);
+
+/*
  * 3-D dendritic spherical grids (ndim = 3; the grid of DENDRITIC_GRID=TRUE builds,
  * utils.c:181-525).  Radial row i has nj[i] theta zones and row (i, j) nk phi zones; the
  * state of a 3-D problem is passed in the reference's zone order (ZLOOP: i, then j, then

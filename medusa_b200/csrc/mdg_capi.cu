@@ -47,6 +47,16 @@ struct mdg_solver {
   double *d_stage_all = nullptr;  // AoS staging of every problem (mdg_upload_all / mdg_download_all)
   int64_t max_cells = 0;
   Sweep3 *s3 = nullptr;           // 3-D: the dendritic sweep of the single problem
+  // output path: an asynchronous snapshot of one problem (state and EOS records, [zone][5]
+  // each, then its time) taken on the solver's stream and copied to pinned host memory on
+  // a copy stream while later steps run
+  double *d_snap = nullptr, *h_snap = nullptr;
+  size_t snap_cap = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_snap = nullptr, ev_snap_done = nullptr;
+  int snap_prob = -1;
+  int64_t snap_n = 0;
+  bool snap_pending = false;
   int *d_err = nullptr;
   // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
   float *d_mx = nullptr;
@@ -239,6 +249,12 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_mx); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
   sweep3_destroy(s->s3);
   s->s3 = nullptr;
+  if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+  cudaFree(s->d_snap);
+  if (s->h_snap) cudaFreeHost(s->h_snap);
+  if (s->ev_snap) cudaEventDestroy(s->ev_snap);
+  if (s->ev_snap_done) cudaEventDestroy(s->ev_snap_done);
+  if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   if (s->graph) cudaGraphExecDestroy(s->graph);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
@@ -828,6 +844,121 @@ int mdg_download_state(mdg_solver *s, int prob, double *prim, double *eos)
   CK(cudaStreamSynchronize(s->stream));
   CK(cudaGetLastError());
   return MDG_OK;
+}
+
+int mdg_snapshot(mdg_solver *s, int prob)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  CK(cudaSetDevice(s->device));
+  if (s->snap_pending) CK(cudaEventSynchronize(s->ev_snap_done));   // one snapshot in flight
+  const ProbDev &P = s->hprobs[prob];
+  const int64_t n = P.ncell;
+  const size_t need = (size_t)2 * NPRIM * n + sizeof(ProbTime) / sizeof(double) + 1;
+  if (need > s->snap_cap) {
+    cudaFree(s->d_snap);
+    s->d_snap = nullptr;
+    if (s->h_snap) cudaFreeHost(s->h_snap);
+    s->h_snap = nullptr;
+    s->snap_cap = 0;
+    CK(cudaMalloc(&s->d_snap, sizeof(double) * need));
+    CK(cudaMallocHost(&s->h_snap, sizeof(double) * need));
+    s->snap_cap = need;
+  }
+  if (!s->copy_stream) {
+    CK(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&s->ev_snap, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&s->ev_snap_done, cudaEventDisableTiming));
+  }
+  // device-side copies on the solver's stream (the next step waits only for these)
+  launch_soa_to_aos(s->P, P.cell_off, n, s->d_snap, s->stream);
+  launch_eos_aos_sel(s->P, s->PH, s->d_probs, s->d_times, prob, P.cell_off, n, s->d_snap + NPRIM * n, s->stream);
+  CK(cudaMemcpyAsync(s->d_snap + 2 * NPRIM * n, s->d_times + prob, sizeof(ProbTime), cudaMemcpyDeviceToDevice,
+                     s->stream));
+  CK(cudaEventRecord(s->ev_snap, s->stream));
+  // the host copy overlaps whatever the solver's stream does next
+  CK(cudaStreamWaitEvent(s->copy_stream, s->ev_snap, 0));
+  CK(cudaMemcpyAsync(s->h_snap, s->d_snap, sizeof(double) * need, cudaMemcpyDeviceToHost, s->copy_stream));
+  CK(cudaEventRecord(s->ev_snap_done, s->copy_stream));
+  CK(cudaGetLastError());
+  s->snap_prob = prob;
+  s->snap_n = n;
+  s->snap_pending = true;
+  return MDG_OK;
+}
+
+static int snap_wait(mdg_solver *s)
+{
+  if (!s->snap_pending) return fail(MDG_ERR_LOGICAL, "no snapshot has been taken");
+  CK(cudaSetDevice(s->device));
+  CK(cudaEventSynchronize(s->ev_snap_done));
+  return MDG_OK;
+}
+
+int mdg_snapshot_read(mdg_solver *s, double *prim, double *eos, double *t)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  int rc = snap_wait(s);
+  if (rc != MDG_OK) return rc;
+  const int64_t n = s->snap_n;
+  if (prim) std::memcpy(prim, s->h_snap, sizeof(double) * NPRIM * n);
+  if (eos) std::memcpy(eos, s->h_snap + NPRIM * n, sizeof(double) * NPRIM * n);
+  if (t) {
+    ProbTime T;
+    std::memcpy(&T, s->h_snap + 2 * NPRIM * n, sizeof T);
+    *t = T.t;
+  }
+  return MDG_OK;
+}
+
+int mdg_snapshot_write_ascii1(mdg_solver *s, const char *path)
+{
+  if (!s || !path) return fail(MDG_ERR_INVALID, "solver/path");
+  int rc = snap_wait(s);
+  if (rc != MDG_OK) return rc;
+  const mdg_problem_desc &d = s->descs[s->snap_prob];
+  if (d.ndim != 1) return fail(MDG_ERR_NOTIMPL, "dump_ascii1 writes 1-D problems");
+  const int64_t n = s->snap_n;
+  const double *prim = s->h_snap, *eos = s->h_snap + NPRIM * n;
+  ProbTime T;
+  std::memcpy(&T, s->h_snap + 2 * NPRIM * n, sizeof T);
+  // the reference's zone geometry (volume, scale[0][0]) from its Romberg tables
+  const int64_t w = d.n1 + 2 * NG;
+  std::vector<double> geo((size_t)GF_NFIELDS * w, 0.0);
+  build_geo_1d(d, geo.data(), w, 0);
+  FILE *fp = std::fopen(path, "w");
+  if (!fp) return fail(MDG_ERR_IO, std::string("cannot open ") + path);
+  // dump_ascii1 (io.c:111-220): "# t", then per zone x (r on spherical grids), the
+  // primitives with the velocity in physical units (scale[0][0] v^1), the EOS record, the
+  // enclosed mass at the zone centre and the two lapse columns (1 without GR_MONOPOLE)
+  std::fprintf(fp, "# %g\n", T.t);
+  double mass = 0.0;
+  for (int64_t i = 0; i < n; i++) {
+    double x = d.startx[0] + (i + 0.5) * d.dx[0];
+    if (d.geom == MDG_SPHERICAL) x = std::fabs(x);
+    const double s00 = geo[(size_t)GF_S00 * w + i + NG], vol = geo[(size_t)GF_VOL * w + i + NG];
+    std::fprintf(fp, "%16.14e ", x);
+    const double *p = prim + NPRIM * i;
+    const double scale[NPRIM] = {1.0, 1.0, s00, 1.0, 1.0};
+    for (int v = 0; v < NPRIM; v++) std::fprintf(fp, "%16.14e ", p[v] * scale[v]);
+    for (int v = 0; v < NPRIM; v++) std::fprintf(fp, "%16.15e ", eos[NPRIM * i + v]);
+    const double dm = vol * p[RHO];
+    std::fprintf(fp, "%16.15e ", mass + 0.5 * dm);
+    mass += dm;
+    std::fprintf(fp, "%16.15e %16.15e ", 1.0, 1.0);
+    std::fprintf(fp, "\n");
+  }
+  const bool ok = std::ferror(fp) == 0;
+  std::fclose(fp);
+  if (!ok) return fail(MDG_ERR_IO, std::string("write failed: ") + path);
+  return MDG_OK;
+}
+
+int mdg_dump_ascii1(mdg_solver *s, int prob, const char *path)
+{
+  int rc = mdg_snapshot(s, prob);
+  if (rc != MDG_OK) return rc;
+  return mdg_snapshot_write_ascii1(s, path);
 }
 
 int mdg_get_time(mdg_solver *s, int prob, double *t, double *dt_last, int *istep)

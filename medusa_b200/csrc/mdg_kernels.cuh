@@ -88,6 +88,8 @@ void launch_initial_estimate_all(const ProbDev *probs, ProbTime *times, int npro
                                  const Tables &tb, StateSoA s, cudaStream_t st);
 void launch_aos_to_soa(const double *aos, StateSoA s, int64_t off, int64_t n, cudaStream_t st);
 void launch_soa_to_aos(StateSoA s, int64_t off, int64_t n, double *aos, cudaStream_t st);
+void launch_eos_aos_sel(StateSoA p, StateSoA ph, const ProbDev *probs, const ProbTime *times, int m, int64_t off,
+                        int64_t n, double *aos, cudaStream_t st);
 void launch_eos_aos_m(StateSoA s, const ProbDev *probs, int m, int64_t off, int64_t n, double *aos,
                       cudaStream_t st);
 

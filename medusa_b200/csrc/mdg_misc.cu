@@ -143,12 +143,9 @@ __global__ void soa_to_aos_kernel(StateSoA s, int64_t off, int64_t n, double *__
 }
 
 // EOS record of each zone (PRESS, CS, TEMP, ENT, GAMMA), eos_gamma.c:45-58 / eos_poly.c:56-69
-__global__ void eos_aos_kernel(StateSoA s, const ProbDev *__restrict__ probs, int m, int64_t off, int64_t n,
-                               double *__restrict__ aos)
+__device__ __forceinline__ void eos_record(const StateSoA &s, const ProbDev &P, int64_t off, int64_t z,
+                                           double *__restrict__ aos)
 {
-  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (z >= n) return;
-  const ProbDev &P = probs[m];
   const double rho = s.v[RHO][off + z], uu = s.v[UU][off + z];
   const double press = eos_press(P.eos, P.gam, P.Kpoly, rho, uu);
   const double cs = sqrt(P.gam * press / rho);
@@ -159,6 +156,32 @@ __global__ void eos_aos_kernel(StateSoA s, const ProbDev *__restrict__ probs, in
   aos[z * 5 + 2] = tp;
   aos[z * 5 + 3] = 0.0;
   aos[z * 5 + 4] = P.gam;
+}
+
+__global__ void eos_aos_kernel(StateSoA s, const ProbDev *__restrict__ probs, int m, int64_t off, int64_t n,
+                               double *__restrict__ aos)
+{
+  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  eos_record(s, probs[m], off, z, aos);
+}
+
+// The same with the EOS source chosen on the device: the stage state PH once a step has
+// been taken (sim_eos was last filled by update_eos(sim_ph)), else the state P.
+__global__ void eos_aos_sel_kernel(StateSoA p, StateSoA ph, const ProbDev *__restrict__ probs,
+                                   const ProbTime *__restrict__ times, int m, int64_t off, int64_t n,
+                                   double *__restrict__ aos)
+{
+  const int64_t z = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (z >= n) return;
+  eos_record(times[m].istep > 0 ? ph : p, probs[m], off, z, aos);
+}
+
+void launch_eos_aos_sel(StateSoA p, StateSoA ph, const ProbDev *probs, const ProbTime *times, int m, int64_t off,
+                        int64_t n, double *aos, cudaStream_t st)
+{
+  if (n <= 0) return;
+  eos_aos_sel_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(p, ph, probs, times, m, off, n, aos);
 }
 
 // Neumaier's compensated summation: s + c carries the sum of the added terms with an

@@ -147,6 +147,10 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_server_result.argtypes = [vp, ll, vp, ctypes.POINTER(d), ctypes.POINTER(i), ctypes.POINTER(d)]
     L.mdg_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
     L.mdg_server_destroy.argtypes = [vp]
+    L.mdg_snapshot.argtypes = [vp, i]
+    L.mdg_snapshot_read.argtypes = [vp, vp, vp, vp]
+    L.mdg_snapshot_write_ascii1.argtypes = [vp, ctypes.c_char_p]
+    L.mdg_dump_ascii1.argtypes = [vp, i, ctypes.c_char_p]
     L.mdg_grid3d_counts.argtypes = [ctypes.POINTER(ProblemDesc), vp, vp, ctypes.POINTER(ll)]
     L.mdg_grid3d_geometry.argtypes = [ctypes.POINTER(ProblemDesc), vp, ctypes.POINTER(ll)]
     for name in ("mdg_create", "mdg_upload_state", "mdg_estimate_dt", "mdg_step", "mdg_download_state",
@@ -154,7 +158,8 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
                  "mdg_get_timers", "mdg_get_launch_config", "mdg_set_launch_config", "mdg_autotune",
                  "mdg_conserved_totals", "mdg_upload_all", "mdg_download_all", "mdg_server_create", "mdg_server_submit", "mdg_server_run",
                  "mdg_server_start", "mdg_server_stop", "mdg_server_poll", "mdg_server_wait", "mdg_server_result",
-                 "mdg_server_get_stats", "mdg_server_destroy", "mdg_grid3d_counts", "mdg_grid3d_geometry"):
+                 "mdg_server_get_stats", "mdg_server_destroy", "mdg_grid3d_counts", "mdg_grid3d_geometry",
+                 "mdg_snapshot", "mdg_snapshot_read", "mdg_snapshot_write_ascii1", "mdg_dump_ascii1"):
         getattr(L, name).restype = i
     _lib = L
     return L
@@ -307,6 +312,28 @@ class Solver:
 
     def download_ptr(self, m: int, host_ptr: int):
         _check(library().mdg_download_state(self._h, m, ctypes.c_void_p(host_ptr), None), "mdg_download_state")
+
+    # --- output path
+    def snapshot(self, m: int = 0):
+        """Queue a copy of problem m's state, EOS records and time; returns at once."""
+        self._snap_n = self.problems[m].ncell
+        _check(library().mdg_snapshot(self._h, m), "mdg_snapshot")
+
+    def snapshot_read(self):
+        """(prim [zone][5], eos [zone][5], t) of the last snapshot (waits for it)."""
+        n = getattr(self, "_snap_n", self.problems[0].ncell)
+        prim, eos, t = np.empty((n, 5)), np.empty((n, 5)), ctypes.c_double()
+        _check(library().mdg_snapshot_read(self._h, prim.ctypes.data, eos.ctypes.data, ctypes.byref(t)),
+               "mdg_snapshot_read")
+        return prim, eos, t.value
+
+    def snapshot_write_ascii1(self, path: str):
+        _check(library().mdg_snapshot_write_ascii1(self._h, str(path).encode()), "mdg_snapshot_write_ascii1")
+
+    def dump_ascii1(self, path: str, m: int = 0):
+        """Write problem m as the reference's dump_ascii1 (io.c:111-220) does."""
+        self._snap_n = self.problems[m].ncell
+        _check(library().mdg_dump_ascii1(self._h, m, str(path).encode()), "mdg_dump_ascii1")
 
     def time(self, m: int = 0):
         t, dt = ctypes.c_double(), ctypes.c_double()

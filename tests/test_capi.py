@@ -123,3 +123,11 @@ def test_3d_solver_scope_checked_before_device_work(precision, nprob, order, cod
     h = ctypes.c_void_p()
     assert S.library().mdg_create(arr, nprob, precision, 0, ctypes.byref(h)) == code
     assert not h.value
+
+
+def test_output_calls_reject_null_solver():
+    L = S.library()
+    assert L.mdg_snapshot(None, 0) == 1
+    assert L.mdg_snapshot_read(None, None, None, None) == 1
+    assert L.mdg_snapshot_write_ascii1(None, b"x") == 1
+    assert L.mdg_dump_ascii1(None, 0, b"x") == 1
