@@ -526,6 +526,30 @@ def run_kh(args, ctx):
     ms_e2e, h2d, d2h = e2e_run(ctx, lambda upload: medusa_b200.Solver(pb, device=ctx.local, upload=upload),
                                [pb], K, W)
     e2e = ctx.world * ncell * K / (ms_e2e / 1e3)
+    # the mixed-precision split sweep on the same grid, and its accuracy at equal time
+    from medusa_b200 import analytic as A
+    from medusa_b200.solver import PREC_MIXED
+    sm = medusa_b200.Solver(pb, precision=PREC_MIXED, device=ctx.local)
+    sm.step(W)
+    sm.synchronize()
+    ms_mix, _ = timed_steps(ctx, sm, K)
+    sm.close()
+    nacc = min(K, 50)
+    with medusa_b200.Solver(pb, device=ctx.local) as sf:
+        sf.step(nacc)
+        ref = sf.update_cpu(0)
+        t_end = sf.time(0)[0]
+        m0, e0 = sf.conserved_totals()
+    with medusa_b200.Solver(pb.copy(tmax=t_end), precision=PREC_MIXED, device=ctx.local) as sa:
+        n_mix = 0
+        while sa.time(0)[0] < t_end * (1.0 - 1.0e-12) and n_mix < 4 * nacc:
+            sa.step(10)
+            n_mix += 10
+        mix = sa.update_cpu(0)
+        m1, e1 = sa.conserved_totals()
+    accuracy = {"steps": nacc, "t": t_end, "l1_rho": A.l1_rel(mix[:, 0], ref[:, 0]),
+                "l1_u": A.l1_rel(mix[:, 1], ref[:, 1]),
+                "mass_drift_vs_fp64": abs(m1[0] - m0[0]) / m0[0], "energy_drift_vs_fp64": abs(e1[0] - e0[0]) / e0[0]}
     if ctx.rank != 0:
         return
     peak, peak_kind = read_peaks()
@@ -553,6 +577,9 @@ def run_kh(args, ctx):
                      "algorithmic_bytes_per_zone": b_stage1,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
         "clocks": clocks,
+        "mixed": {"value": ctx.world * ncell * K / (ms_mix / 1e3), "unit": "zone-updates/s", "ms_per_step": ms_mix / K,
+                  "precision": "FP32 reconstruction and HLLC wave speeds, FP64 fluxes, accumulation, update, dt",
+                  "accuracy_vs_fp64": accuracy},
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_kh(pb)

@@ -215,8 +215,8 @@ int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double *prim_in, 
  * per process.  A server keeps 1-D and 2-D problems resident on one GPU and advances
  * every admitted problem together, batching their uneven grids into the same stage
  * launches (1-D, for MDG_PREC_MIXED: persistent CTAs fed from a device work queue, each
- * round of steps_per_round steps replayed from one CUDA graph; 2-D: the plain FP64 split
- * sweep in either precision, on a second stream that runs beside the 1-D launches; 3-D
+ * round of steps_per_round steps replayed from one CUDA graph; 2-D: the split sweep in
+ * the server's precision, on a second stream that runs beside the 1-D launches; 3-D
  * dendritic spherical problems on that stream too, each with its own grid, in the
  * server's precision).  A
  * request is a problem description, its initial state ([zone][5], as mdg_upload_state)

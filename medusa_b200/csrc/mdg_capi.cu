@@ -59,7 +59,7 @@ struct mdg_solver {
   bool snap_pending = false;
   int *d_err = nullptr;
   // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
-  float *d_mx = nullptr;
+  float *d_mx = nullptr, *d_mx1 = nullptr;   // FP32 weights (mixed): 1-D or 2-D direction 0; 2-D direction 1
   WorkQueue *d_queue = nullptr;
   Tile *d_mtiles = nullptr;
   int mtiles_cap = 0, nmtiles = 0;
@@ -246,7 +246,7 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles);
   cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
   cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
-  cudaFree(s->d_mx); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
+  cudaFree(s->d_mx); cudaFree(s->d_mx1); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
   sweep3_destroy(s->s3);
   s->s3 = nullptr;
   if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
@@ -388,9 +388,9 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     std::string why;
     int rc = validate_desc(descs[m], ndim, why);
     if (rc != MDG_OK) return fail(rc, "problem " + std::to_string(m) + ": " + why);
-    if (precision == MDG_PREC_MIXED && (descs[m].ndim == 2 || descs[m].hydro_interp_order != 3))
+    if (precision == MDG_PREC_MIXED && descs[m].hydro_interp_order != 3)
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
-                                       ": the mixed-precision sweeps are built for 1-D and 3-D parabolic reconstruction");
+                                       ": the mixed-precision sweeps are built for parabolic reconstruction");
     if (precision == MDG_PREC_MIXED && descs[m].geom == MDG_SPHERICAL && !(descs[m].startx[0] >= 0.0))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
@@ -449,7 +449,9 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
 
   // host tables of the FP64 sweeps (Romberg moments, bit-identical to the reference's);
   // the mixed sweep's tables are built on the device from closed-form moments below
-  const bool dev_tables = precision == MDG_PREC_MIXED;
+  // 1-D mixed: tables built on the device from closed-form moments; 2-D mixed: the FP64
+  // tables (for declined faces) plus host-built FP32 weights of both directions
+  const bool dev_tables = precision == MDG_PREC_MIXED && ndim == 1;
   const size_t n_rc0 = (size_t)RC_NFIELDS * rc0, n_geo = (ndim == 2) ? 0 : (size_t)GF_NFIELDS * rc0;
   std::vector<double> h_rc0, h_rc1, h_geo;
   if (!dev_tables) h_rc0.assign(n_rc0, 0.0);
@@ -490,6 +492,16 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
   CKC(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
   if (precision == MDG_PREC_MIXED) CKC(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * rc0));
+  if (precision == MDG_PREC_MIXED && ndim == 2) {
+    CKC(cudaMalloc(&s->d_mx1, sizeof(float) * MX_NFIELDS * rc1));
+    std::vector<float> m0((size_t)MX_NFIELDS * rc0, 0.0f), m1((size_t)MX_NFIELDS * rc1, 0.0f);
+    for (int m = 0; m < nprob; m++) {
+      build_mixed_table(descs[m], 0, m0.data(), rc0, s->hprobs[m].geo_off);
+      build_mixed_table(descs[m], 1, m1.data(), rc1, s->hprobs[m].rc1_off);
+    }
+    CKC(cudaMemcpy(s->d_mx, m0.data(), sizeof(float) * m0.size(), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->d_mx1, m1.data(), sizeof(float) * m1.size(), cudaMemcpyHostToDevice));
+  }
   CKC(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock0, sh > 0 ? sh : 1));
   if (ndim == 2) CKC(cudaMalloc(&s->d_shock1, sh > 0 ? sh : 1));
@@ -520,8 +532,9 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   s->tb.rc1 = s->d_rc1; s->tb.rc1_stride = rc1;
   s->tb.geo = s->d_geo; s->tb.geo_stride = rc0;
   s->tb.mx = s->d_mx;
+  s->tb.mx1 = s->d_mx1;
 #undef CKC
-  if (precision == MDG_PREC_MIXED) {
+  if (precision == MDG_PREC_MIXED && ndim == 1) {
     int rc = build_mixed_tiles(s, s->cfg.threads);
     if (rc != MDG_OK) { free_all(s); delete s; return rc; }
   }
@@ -585,7 +598,8 @@ static int queue_steps(mdg_solver *s, int nsteps)
 {
   auto mark = [&](int k, int e) { if (s->timing) cudaEventRecord(s->ev[k][e], s->stream); };
   const bool mix3 = s->ndim == 3 && s->precision == MDG_PREC_MIXED;
-  const bool mixed = s->ndim != 3 && s->precision == MDG_PREC_MIXED;   // the batched 1-D mixed sweep
+  const bool mix2 = s->ndim == 2 && s->precision == MDG_PREC_MIXED;
+  const bool mixed = s->ndim == 1 && s->precision == MDG_PREC_MIXED;   // the batched 1-D mixed sweep
   const int mgrid = mixed ? mixed_grid(s) : 0;
   const bool queue = s->cfg.ctas_per_sm > 0;
   for (int k = 0; k < nsteps; k++) {
@@ -601,7 +615,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
     else if (s->ndim == 1)
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
     else
-      launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
+      launch_stage2d(0, mix2, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
                      s->P, s->P, s->ACC, s->PH, s->d_shock0, s->d_shock1, s->stream);
     mark(MDG_TIMER_STAGE0, 1);
     mark(MDG_TIMER_STAGE1, 0);
@@ -613,7 +627,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
     else if (s->ndim == 1)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     else
-      launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
+      launch_stage2d(1, mix2, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
                      s->PH, s->P, s->ACC, s->P, s->d_shock0, s->d_shock1, s->stream);
     mark(MDG_TIMER_STAGE1, 1);
     mark(MDG_TIMER_FINISH, 0);
@@ -716,10 +730,11 @@ int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
   CK(cudaSetDevice(s->device));
   CK(cudaStreamSynchronize(s->stream));
   const bool reshape = cfg->threads != s->cfg.threads;
-  if (reshape && s->precision == MDG_PREC_MIXED) {
+  const bool batched = s->precision == MDG_PREC_MIXED && s->ndim == 1;
+  if (reshape && batched) {
     int rc = build_mixed_tiles(s, cfg->threads);
     if (rc != MDG_OK) return rc;
-  } else if (s->precision == MDG_PREC_MIXED) {
+  } else if (batched) {
     WorkQueue q{{0u, 0u}, s->nmtiles, 0};
     CK(cudaMemcpy(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice));
   }
@@ -733,8 +748,8 @@ int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double
 {
   if (!s) return fail(MDG_ERR_INVALID, "solver");
   if (trial_steps < 1) return fail(MDG_ERR_INVALID, "trial_steps < 1");
-  if (s->precision != MDG_PREC_MIXED)
-    return fail(MDG_ERR_NOTIMPL, "the FP64 sweeps have fixed launch shapes");
+  if (s->precision != MDG_PREC_MIXED || s->ndim != 1)
+    return fail(MDG_ERR_NOTIMPL, "only the batched 1-D mixed sweep has tunable launch shapes");
   CK(cudaSetDevice(s->device));
   CK(cudaStreamSynchronize(s->stream));
   // the trials advance the state: keep a copy of everything a step changes

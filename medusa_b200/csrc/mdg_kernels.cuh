@@ -18,7 +18,9 @@ struct Tables {
   int64_t rc1_stride;
   const double *geo;     // 1-D face/zone geometry, GF_NFIELDS x geo_stride
   int64_t geo_stride;
-  const float *mx;       // 1-D FP32 reconstruction weights (mixed precision), MX_NFIELDS x geo_stride
+  const float *mx;       // FP32 reconstruction weights (mixed precision), MX_NFIELDS x geo_stride: 1-D problems,
+                         // and direction 0 of 2-D problems (indexed like rc0)
+  const float *mx1;      // direction-1 FP32 weights of 2-D problems, indexed like rc1
 };
 
 // Device work queue of the persistent mixed-precision sweep: one head counter per RK
@@ -53,7 +55,7 @@ constexpr int TIY2 = MDG_TIY2;    // rows per direction-1 tile
 void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
                     const Tables &tb, StateSoA stage_state, StateSoA state_n, StateSoA out,
                     cudaStream_t st);
-void launch_stage2d(int stage, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
+void launch_stage2d(int stage, bool mixed, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
                     const Tile *ytiles, int nyt, const Tables &tb, StateSoA stage_state, StateSoA state_n,
                     StateSoA acc, StateSoA out, unsigned char *shock0, unsigned char *shock1, cudaStream_t st);
 // Mixed-precision 1-D stage: nt threads per CTA (tile = nt-2 zones), grid CTAs; with

@@ -20,6 +20,18 @@ __device__ __forceinline__ MixW load_mixw(const float *__restrict__ w, int64_t s
   return m;
 }
 
+// The same from any address space (shared-memory copies of the weights): plain loads.
+__device__ __forceinline__ MixW load_mixw_any(const float *w, int64_t st)
+{
+  MixW m;
+  m.wlm = w[MX_WLM * st]; m.wlp = w[MX_WLP * st];
+  m.wrm = w[MX_WRM * st]; m.wrp = w[MX_WRP * st];
+  m.eal = w[MX_EAL * st]; m.ear = w[MX_EAR * st];
+  m.ebl = w[MX_EBL * st]; m.ebr = w[MX_EBR * st];
+  m.dxz = w[MX_DXZ * st]; m.mr = w[MX_MR * st]; m.ml = w[MX_ML * st];
+  return m;
+}
+
 // para_recon of one variable in difference form (reconstruct.c:142-201): returns the face
 // offsets dl = al - a and dr = ar - a.
 __device__ __forceinline__ void mixed_recon(float dqm, float dqp, const MixW &w, float &dl, float &dr)

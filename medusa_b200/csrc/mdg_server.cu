@@ -48,6 +48,7 @@ int validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why);
 void make_probdev(const mdg_problem_desc &d, ProbDev &P);
 void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
 }
 
@@ -113,6 +114,7 @@ struct Request {
   std::vector<double> ic;       // [zone][5]
   std::vector<double> result;   // [zone][5] once finished
   std::vector<double> rc, geo;  // FP64 sweeps: the reference's tables, built at submission
+  std::vector<float> mx;        // mixed 2-D: FP32 weights of both directions, laid out as rc
   int sparse = 0;
   int status = MDG_REQ_QUEUED;
   int err = MDG_OK;
@@ -279,9 +281,9 @@ int queue_round(mdg_server *s, int nsteps)
     }
     if (lane2) {
       if (s->ntx2 > 0) {
-        launch_stage2d(0, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+        launch_stage2d(0, mixed, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
                        s->P2, s->P2, s->ACC2, s->PH2, s->d_shock0, s->d_shock1, s->stream2);
-        launch_stage2d(1, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+        launch_stage2d(1, mixed, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
                        s->PH2, s->P2, s->ACC2, s->P2, s->d_shock0, s->d_shock1, s->stream2);
       }
       for (Request *r : s->jobs3) {
@@ -337,6 +339,9 @@ int admit(mdg_server *s, Request *r)
     // reference's calloc'd flag arrays (utils.c:164-174)
     SCK(cudaMemcpy2DAsync(s->d_rc0 + seg, sizeof(double) * s->units, r->rc.data(), sizeof(double) * w,
                           sizeof(double) * w, RC_NFIELDS, cudaMemcpyHostToDevice, s->stream));
+    if (!r->mx.empty())
+      SCK(cudaMemcpy2DAsync(s->d_mx + seg, sizeof(float) * s->units, r->mx.data(), sizeof(float) * w,
+                            sizeof(float) * w, MX_NFIELDS, cudaMemcpyHostToDevice, s->stream));
     SCK(cudaMemsetAsync(s->d_shock0 + r->seg2, 0, r->cells, s->stream));
     SCK(cudaMemsetAsync(s->d_shock1 + r->seg2, 0, r->cells, s->stream));
     SCK(cudaMemcpyAsync(s->d_stage, r->ic.data(), sizeof(double) * NPRIM * r->ncell, cudaMemcpyHostToDevice,
@@ -725,6 +730,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   s->tb.rc1 = s->d_rc0; s->tb.rc1_stride = units;
   s->tb.geo = s->d_geo; s->tb.geo_stride = units;
   s->tb.mx = s->d_mx;
+  s->tb.mx1 = s->d_mx;   // direction 1 of a 2-D request, after its direction-0 weights
   *out = s;
   return MDG_OK;
 }
@@ -799,6 +805,11 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
     r->rc.assign((size_t)RC_NFIELDS * r->units, 0.0);
     build_recon_table(r->desc, 0, r->rc.data(), r->units, 0);
     build_recon_table(r->desc, 1, r->rc.data(), r->units, desc->n1 + 2 * NG);
+    if (s->cfg.precision == MDG_PREC_MIXED) {
+      r->mx.assign((size_t)MX_NFIELDS * r->units, 0.0f);
+      build_mixed_table(r->desc, 0, r->mx.data(), r->units, 0);
+      build_mixed_table(r->desc, 1, r->mx.data(), r->units, desc->n1 + 2 * NG);
+    }
   } else if (s->cfg.precision == MDG_PREC_FP64) {
     // the reference's Romberg tables, built here in the submitting thread so that the
     // request loop does not spend its time on them

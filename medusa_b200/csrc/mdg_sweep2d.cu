@@ -38,6 +38,7 @@
 // (exact identities) are compiled out (UNIT = true).
 #include "mdg_hydro.cuh"
 #include "mdg_kernels.cuh"
+#include "mdg_mixed.cuh"
 
 namespace mdg {
 
@@ -112,16 +113,42 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-template <int STAGE>
+// FP64 re-solve of a direction-DIR face that the mixed solver declined (MIX_COND_MAX):
+// both face states reconstructed in FP64 from the stencil values a[0..3] (zones either side
+// of the face and their outer neighbours) and the reconstruction columns of the two zones.
+template <int DIR, typename GM, typename GZ>
+__device__ __noinline__ void face2d_fp64(int order, const double (&a)[6][4], const GM &gm, const GZ &gz, double gam,
+                                         const FaceGeom<double> &fg, double *f, double &sig)
+{
+  double pl[7], pr[7];
+  for (int v = 0; v < 6; v++) {
+    double lo, hi;
+    recon_zone<double>(order, a[v][0], a[v][1], a[v][2], gm, lo, hi);
+    pl[v] = hi;
+    recon_zone<double>(order, a[v][1], a[v][2], a[v][3], gz, lo, hi);
+    pr[v] = lo;
+  }
+  pl[6] = gam;
+  pr[6] = gam;
+  riemann_hllc<DIR, true, double>(pl, pr, fg, gam_const(gam), f, sig);
+}
+
+// MIX: the mixed-precision variant (FP32 difference-form reconstruction with the FP32
+// weights of each zone, FP32 HLLC wave speeds and star-state increments, FP64 fluxes,
+// accumulation, update and dt); faces the FP32 solver declines are re-solved in FP64,
+// which needs the zone before the face's left zone: the column ring keeps 5 rows.
+template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(NTX2, MDG_XMINB)
 xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                 const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA acc,
                 unsigned char *__restrict__ shock)
 {
+  constexpr int RING = MIX ? 5 : 4;
   // column stencil ring (rows r-1 .. r+2 of this thread's column), fed by cp.async
-  __shared__ double ring[4][6][NTX2];
+  __shared__ double ring[RING][6][NTX2];
   // direction-0 reconstruction coefficients of rows i0-1 .. i0+TIX2
   __shared__ double xrc[RC_NFIELDS][TIX2 + 2];
+  __shared__ float xmx[MIX ? MX_NFIELDS : 1][TIX2 + 2];
   __shared__ double sred[32];
   const Tile tile = tiles[blockIdx.x];
   if (times[tile.prob].done) return;   // past tmax: the time loop has ended (CTA-uniform)
@@ -137,11 +164,20 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   const FaceGeom<double> fg{P.area0, 1.0, 1.0, 1.0, 1.0};
   unsigned char *sh = shock + P.sh_off;
   double smax = 0.0;                               // max |signal speed| of this thread's faces
+  // ring slot of a row (rows >= i0-2)
+  auto slot = [&](int row) { return MIX ? (row - i0 + 2) % RING : (row & 3); };
 
   for (int k = t; k < RC_NFIELDS * (TIX2 + 2); k += NTX2) {
     const int f = k / (TIX2 + 2), rr = k - f * (TIX2 + 2);
     const int row = min(i0 - 1 + rr, n1);
     xrc[f][rr] = __ldg(tb.rc0 + f * tb.rc0_stride + P.geo_off + row + NG);
+  }
+  if (MIX) {
+    for (int k = t; k < MX_NFIELDS * (TIX2 + 2); k += NTX2) {
+      const int f = k / (TIX2 + 2), rr = k - f * (TIX2 + 2);
+      const int row = min(i0 - 1 + rr, n1);
+      xmx[f][rr] = __ldg(tb.mx + f * tb.rc0_stride + P.geo_off + row + NG);
+    }
   }
   __syncthreads();
 
@@ -149,7 +185,7 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     // rows inside the grid arrive by cp.async; boundary rows are produced by the
     // boundary index maps and stored directly.  One commit group per row.
     auto stage_row = [&](int row) {
-      double *dst0 = &ring[row & 3][0][t];
+      double *dst0 = &ring[slot(row)][0][t];
       if (row >= 0 && row < n1) {
         const int64_t c = P.cell_off + (int64_t)row * n2 + j;
 #pragma unroll
@@ -164,7 +200,7 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     };
     // pressure (eos_gamma.c:7 / eos_poly.c:7) of a landed row, stored as variable 5
     auto press_row = [&](int row) {
-      double *d = &ring[row & 3][0][t];
+      double *d = &ring[slot(row)][0][t];
       d[5 * NTX2] = eos_press(P.eos, P.gam, P.Kpoly, d[RHO * NTX2], d[UU * NTX2]);
     };
     stage_row(i0 - 2);
@@ -185,12 +221,23 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       press_row(r + 1);
       // reconstruct zone (r, j) along direction 0
       double xl[7], xr[6];
-      {
+      if (MIX) {
+        const MixW w = load_mixw_any(&xmx[0][r - i0 + 1], TIX2 + 2);
+#pragma unroll
+        for (int v = 0; v < 6; v++) {
+          const double a = ring[slot(r)][v][t];
+          float dl, dr;
+          mixed_recon((float)(a - ring[slot(r - 1)][v][t]), (float)(ring[slot(r + 1)][v][t] - a), w, dl, dr);
+          xl[v] = a + (double)dl;
+          xr[v] = a + (double)dr;
+        }
+        xl[6] = P.gam;
+      } else {
         const RcView<double, false> g{&xrc[0][r - i0 + 1], TIX2 + 2};
 #pragma unroll
         for (int v = 0; v < 6; v++)
-          recon_zone<double>(order, ring[(r - 1) & 3][v][t], ring[r & 3][v][t], ring[(r + 1) & 3][v][t], g, xl[v],
-                             xr[v]);
+          recon_zone<double>(order, ring[slot(r - 1)][v][t], ring[slot(r)][v][t], ring[slot(r + 1)][v][t], g,
+                             xl[v], xr[v]);
         xl[6] = P.gam;
       }
       if (r >= i0) {
@@ -199,7 +246,22 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 #pragma unroll
         for (int v = 0; v < 6; v++) pl[v] = xr_prev[v];
         pl[6] = P.gam;
-        const int sb = riemann_hllc<0, true, double>(pl, xl, fg, gc, f, sig);
+        int sb;
+        if (MIX) {
+          float sgf;
+          if (riemann_hllc_mixed<0>(pl, xl, fg, gam_const<float>((float)P.gam), f, sgf, sb)) {
+            sig = (double)sgf;
+          } else {
+            double a[6][4];
+#pragma unroll
+            for (int v = 0; v < 6; v++)
+              for (int q = 0; q < 4; q++) a[v][q] = ring[slot(r - 2 + q)][v][t];
+            const RcView<double, false> gm{&xrc[0][r - i0], TIX2 + 2}, gz{&xrc[0][r - i0 + 1], TIX2 + 2};
+            face2d_fp64<0>(order, a, gm, gz, P.gam, fg, f, sig);   // sb: the FP32 estimate's flag
+          }
+        } else {
+          sb = riemann_hllc<0, true, double>(pl, xl, fg, gc, f, sig);
+        }
         smax = tmax(smax, fabs(sig));
         sh[(int64_t)r * n2 + j] = (unsigned char)sb;
         // direction-0 part of divF of zone (r-1, j): (0 + F(r)) - F(r-1)
@@ -225,7 +287,7 @@ xsweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 }
 
 // ------------------------------------------------------------------ direction 1 + push
-template <int STAGE>
+template <int STAGE, bool MIX>
 __global__ void __launch_bounds__(NTY2, MDG_YMINB)
 ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                 const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA sn, StateSoA acc,
@@ -235,6 +297,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   __shared__ double syr[6][NTY2];
   __shared__ double sfy[NPRIM][NTY2];
   __shared__ double yrc[RC_NFIELDS][NTY2];    // direction-1 coefficients of each thread's column
+  __shared__ float ymx[MIX ? MX_NFIELDS : 1][NTY2];
   __shared__ unsigned char sflag[NTY2];
   __shared__ double sred[32];
 
@@ -262,6 +325,8 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   {
     const int jc = jx < -1 ? -1 : (jx > n2 ? n2 : jx);
     for (int f = 0; f < RC_NFIELDS; f++) yrc[f][t] = __ldg(tb.rc1 + f * tb.rc1_stride + P.rc1_off + jc + NG);
+    if (MIX)
+      for (int f = 0; f < MX_NFIELDS; f++) ymx[f][t] = __ldg(tb.mx1 + f * tb.rc1_stride + P.rc1_off + jc + NG);
   }
 
   for (int r = tile.i0; r < iend; r++) {
@@ -307,7 +372,18 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     __syncthreads();
     // reconstruct zone (r, jx) along direction 1
     double yl[7];
-    {
+    if (MIX) {
+      const MixW w = load_mixw_any(&ymx[0][t], NTY2);
+#pragma unroll
+      for (int v = 0; v < 6; v++) {
+        const double a = sv[v][t + 1];
+        float dl, dr;
+        mixed_recon((float)(a - sv[v][t]), (float)(sv[v][t + 2] - a), w, dl, dr);
+        yl[v] = a + (double)dl;
+        syr[v][t] = a + (double)dr;
+      }
+      yl[6] = gam;
+    } else {
       const RcView<double, false> g{&yrc[0][t], NTY2};
       double yr[6];
 #pragma unroll
@@ -323,8 +399,24 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       for (int v = 0; v < 6; v++) pl[v] = syr[v][t - 1];
       pl[6] = gam;
       const bool hlle = (jx == 0) || (jx == n2) || sflag[t] || sflag[t - 1];
-      if (hlle) riemann_hlle<1, true, double>(pl, yl, fg, gc, fy, sig);
-      else riemann_hllc<1, true, double>(pl, yl, fg, gc, fy, sig);
+      if (hlle) {
+        riemann_hlle<1, true, double>(pl, yl, fg, gc, fy, sig);
+      } else if (!MIX) {
+        riemann_hllc<1, true, double>(pl, yl, fg, gc, fy, sig);
+      } else {
+        float sgf;
+        int sb;
+        if (riemann_hllc_mixed<1>(pl, yl, fg, gam_const<float>((float)gam), fy, sgf, sb)) {
+          sig = (double)sgf;
+        } else {
+          double a[6][4];
+#pragma unroll
+          for (int v = 0; v < 6; v++)
+            for (int q = 0; q < 4; q++) a[v][q] = sv[v][t - 1 + q];
+          const RcView<double, false> gm{&yrc[0][t - 1], NTY2}, gz{&yrc[0][t], NTY2};
+          face2d_fp64<1>(order, a, gm, gz, gam, fg, fy, sig);
+        }
+      }
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) sfy[v][t] = fy[v];
       if (jx >= 0 && jx <= n2) smax = tmax(smax, fabs(sig));
@@ -380,17 +472,23 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   block_min_to(lmin, &times[tile.prob].minacc, sred);
 }
 
-void launch_stage2d(int stage, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
+void launch_stage2d(int stage, bool mixed, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
                     const Tile *ytiles, int nyt, const Tables &tb, StateSoA sst, StateSoA sn, StateSoA acc,
                     StateSoA out, unsigned char *shock0, unsigned char *shock1, cudaStream_t st)
 {
   if (nxt <= 0 || nyt <= 0) return;
-  if (stage == 0) {
-    xsweep2d_kernel<0><<<nxt, NTX2, 0, st>>>(probs, times, xtiles, tb, sst, acc, shock0);
-    ysweep2d_kernel<0><<<nyt, NTY2, 0, st>>>(probs, times, ytiles, tb, sst, sn, acc, out, shock0, shock1);
+  if (stage == 0 && !mixed) {
+    xsweep2d_kernel<0, false><<<nxt, NTX2, 0, st>>>(probs, times, xtiles, tb, sst, acc, shock0);
+    ysweep2d_kernel<0, false><<<nyt, NTY2, 0, st>>>(probs, times, ytiles, tb, sst, sn, acc, out, shock0, shock1);
+  } else if (!mixed) {
+    xsweep2d_kernel<1, false><<<nxt, NTX2, 0, st>>>(probs, times, xtiles, tb, sst, acc, shock1);
+    ysweep2d_kernel<1, false><<<nyt, NTY2, 0, st>>>(probs, times, ytiles, tb, sst, sn, acc, out, shock0, shock1);
+  } else if (stage == 0) {
+    xsweep2d_kernel<0, true><<<nxt, NTX2, 0, st>>>(probs, times, xtiles, tb, sst, acc, shock0);
+    ysweep2d_kernel<0, true><<<nyt, NTY2, 0, st>>>(probs, times, ytiles, tb, sst, sn, acc, out, shock0, shock1);
   } else {
-    xsweep2d_kernel<1><<<nxt, NTX2, 0, st>>>(probs, times, xtiles, tb, sst, acc, shock1);
-    ysweep2d_kernel<1><<<nyt, NTY2, 0, st>>>(probs, times, ytiles, tb, sst, sn, acc, out, shock0, shock1);
+    xsweep2d_kernel<1, true><<<nxt, NTX2, 0, st>>>(probs, times, xtiles, tb, sst, acc, shock1);
+    ysweep2d_kernel<1, true><<<nyt, NTY2, 0, st>>>(probs, times, ytiles, tb, sst, sn, acc, out, shock0, shock1);
   }
 }
 

@@ -65,10 +65,11 @@ def test_null_handles_are_rejected():
     assert L.mdg_destroy(None) == 0
 
 
-@pytest.mark.parametrize("pb", [P.kelvin_helmholtz(16, 16, nsteps=1), P.sod(64).copy(hydro_interp_order=2)],
-                         ids=["2d", "linear"])
+@pytest.mark.parametrize("pb", [P.sod(64).copy(hydro_interp_order=2),
+                                P.kelvin_helmholtz(16, 16, nsteps=1).copy(hydro_interp_order=1)],
+                         ids=["linear", "2d_pcm"])
 def test_mixed_precision_scope_is_checked_before_any_device_work(pb):
-    """The mixed sweep is built for 1-D parabolic reconstruction: other problems are
+    """The mixed sweeps are built for parabolic reconstruction: other problems are
     refused with MDG_ERR_NOTIMPL (validation runs before any CUDA call)."""
     arr = (S.ProblemDesc * 1)(S.desc_of(pb))
     h = ctypes.c_void_p()

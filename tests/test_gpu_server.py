@@ -159,8 +159,9 @@ def _server_2d(precision, spr=11):
 
 @pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
 def test_server_2d_requests_equal_solver(precision):
-    """2-D requests run on the FP64 split sweep beside the 1-D lane; each result is the
-    solver's FP64 run of the same problem, bit for bit, also with 1-D requests resident."""
+    """2-D requests run on the split sweep of the server's precision beside the 1-D lane;
+    each result is the solver's run of the same problem, bit for bit, also with 1-D
+    requests resident."""
     reqs2 = _mix_2d()
     reqs1 = _mix()[:3]
     with _server_2d(precision) as srv:
@@ -170,7 +171,7 @@ def test_server_2d_requests_equal_solver(precision):
         assert srv.stats()["completed"] == len(reqs1) + len(reqs2)
         for rid, pb in zip(ids2, reqs2):
             prim, t, ist, _ = srv.result(rid)
-            ref, (rt, _, rist) = _solver_result(pb, PREC_FP64)
+            ref, (rt, _, rist) = _solver_result(pb, precision)
             assert t >= pb.tmax and t == rt and ist == rist, pb.name
             assert np.array_equal(prim, ref), pb.name
         for rid, pb in zip(ids1, reqs1):
@@ -189,10 +190,10 @@ def test_server_2d_slot_reuse_and_graph_recapture():
         got = {}
         for k in range(4):
             got[srv.submit(reqs1[k])] = (reqs1[k], PREC_MIXED)
-            got[srv.submit(reqs2[k])] = (reqs2[k], PREC_FP64)
+            got[srv.submit(reqs2[k])] = (reqs2[k], PREC_MIXED)
             srv.run(2 + k)
         again = reqs2[0].copy(tmax=0.025)
-        got[srv.submit(again)] = (again, PREC_FP64)
+        got[srv.submit(again)] = (again, PREC_MIXED)
         srv.run(0)
         for rid, (pb, prec) in got.items():
             prim, t, ist, _ = srv.result(rid)
@@ -212,7 +213,7 @@ def test_server_3d_requests_equal_solver(precision):
     1-D and 2-D ones: every result is the solver's run of the same problem, bit for bit."""
     reqs3 = _mix_3d()
     reqs = [(pb, precision) for pb in reqs3] + [(pb, precision) for pb in _mix()[:2]] + \
-           [(pb, PREC_FP64) for pb in _mix_2d()[:1]]
+           [(pb, precision) for pb in _mix_2d()[:1]]
     with Server(precision=precision, hbm_bytes=256 << 20, max_problems=32, max_zones=4096, steps_per_round=9,
                 hbm_bytes_2d=64 << 20, max_cells_2d=1 << 16, hbm_bytes_3d=512 << 20) as srv:
         ids = []
