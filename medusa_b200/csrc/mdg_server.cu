@@ -169,8 +169,8 @@ struct mdg_server {
   StateSoA P2{}, PH2{}, ACC2{};
   Tile *d_tiles2 = nullptr;
   int tiles2_cap = 0, ntx2 = 0, nty2 = 0;
-  cudaStream_t stream2 = nullptr;
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaStream_t stream2 = nullptr, stream3 = nullptr;   // 2-D lane, 3-D lane
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
   int graph_ntx2 = -1, graph_nty2 = -1;   // 2-D tile counts the graph was captured with
   // 3-D lane: resident 3-D requests (each with its own grid), on the second stream
   std::vector<Request *> jobs3;
@@ -207,6 +207,8 @@ void free_server(mdg_server *s)
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
+  if (s->ev_join3) cudaEventDestroy(s->ev_join3);
+  if (s->stream3) cudaStreamDestroy(s->stream3);
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles); cudaFree(s->d_queue); cudaFree(s->d_err);
   cudaFree(s->d_state); cudaFree(s->d_rc0); cudaFree(s->d_geo); cudaFree(s->d_stage); cudaFree(s->d_mx);
   cudaFree(s->d_state2); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_tiles2);
@@ -263,13 +265,12 @@ int queue_round(mdg_server *s, int nsteps)
 {
   const bool mixed = s->cfg.precision == MDG_PREC_MIXED;
   const int grid = mixed ? persistent_grid(s) : 0;
-  const bool lane2 = s->ntx2 > 0 || !s->jobs3.empty();
+  const bool lane2 = s->ntx2 > 0, lane3 = !s->jobs3.empty();
   for (int k = 0; k < nsteps; k++) {
     launch_dt_finalize(s->d_probs, s->d_times, s->max_probs, s->d_err, s->stream);
-    if (lane2) {
-      SCK(cudaEventRecord(s->ev_fork, s->stream));
-      SCK(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-    }
+    if (lane2 || lane3) SCK(cudaEventRecord(s->ev_fork, s->stream));
+    if (lane2) SCK(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
+    if (lane3) SCK(cudaStreamWaitEvent(s->stream3, s->ev_fork, 0));
     if (mixed) {
       launch_stage1d_mixed(0, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
                            s->P, s->P, s->PH, s->stream);
@@ -280,20 +281,22 @@ int queue_round(mdg_server *s, int nsteps)
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     }
     if (lane2) {
-      if (s->ntx2 > 0) {
-        launch_stage2d(0, mixed, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
-                       s->P2, s->P2, s->ACC2, s->PH2, s->d_shock0, s->d_shock1, s->stream2);
-        launch_stage2d(1, mixed, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
-                       s->PH2, s->P2, s->ACC2, s->P2, s->d_shock0, s->d_shock1, s->stream2);
-      }
+      launch_stage2d(0, mixed, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+                     s->P2, s->P2, s->ACC2, s->PH2, s->d_shock0, s->d_shock1, s->stream2);
+      launch_stage2d(1, mixed, s->d_probs, s->d_times, s->d_tiles2, s->ntx2, s->d_tiles2 + s->ntx2, s->nty2, s->tb,
+                     s->PH2, s->P2, s->ACC2, s->P2, s->d_shock0, s->d_shock1, s->stream2);
+      SCK(cudaEventRecord(s->ev_join, s->stream2));
+      SCK(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+    }
+    if (lane3) {
       for (Request *r : s->jobs3) {
         ProbDev *pr = s->d_probs + r->slot;
         ProbTime *tr = s->d_times + r->slot;
-        launch_stage3d(0, mixed, r->s3, pr, tr, soa3(r, 0), soa3(r, 0), soa3(r, 1), s->stream2);
-        launch_stage3d(1, mixed, r->s3, pr, tr, soa3(r, 1), soa3(r, 0), soa3(r, 0), s->stream2);
+        launch_stage3d(0, mixed, r->s3, pr, tr, soa3(r, 0), soa3(r, 0), soa3(r, 1), s->stream3);
+        launch_stage3d(1, mixed, r->s3, pr, tr, soa3(r, 1), soa3(r, 0), soa3(r, 0), s->stream3);
       }
-      SCK(cudaEventRecord(s->ev_join, s->stream2));
-      SCK(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
+      SCK(cudaEventRecord(s->ev_join3, s->stream3));
+      SCK(cudaStreamWaitEvent(s->stream, s->ev_join3, 0));
     }
     launch_finish(s->d_times, s->max_probs, s->stream);
   }
@@ -688,10 +691,12 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   SCKB(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, c.device));
   SCKB(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   SCKB(cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
+  SCKB(cudaStreamCreateWithFlags(&s->stream3, cudaStreamNonBlocking));
   SCKB(cudaEventCreate(&s->ev0));
   SCKB(cudaEventCreate(&s->ev1));
   SCKB(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   SCKB(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
+  SCKB(cudaEventCreateWithFlags(&s->ev_join3, cudaEventDisableTiming));
   SCKB(cudaMalloc(&s->d_probs, sizeof(ProbDev) * s->max_probs));
   SCKB(cudaMalloc(&s->d_times, sizeof(ProbTime) * s->max_probs));
   SCKB(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->max_tiles));
