@@ -103,13 +103,17 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
   if (d.ndim != 1 && d.ndim != 2 && d.ndim != 3) return bad("ndim must be 1, 2 or 3");
   if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
-  if (d.ndim == 3) {
-    // the dendritic spherical grid of prim_to_fluxes3 over the whole sphere
+  if (is_dendritic(d)) {
+    // the dendritic spherical grid of prim_to_fluxes3 (3-D) or prim_to_fluxes2 (2-D,
+    // step.c:659-764) over the whole sphere; a 2-D grid has one phi zone of width 2 pi
+    // (init_coords, metric_spherical_general.c:570-572)
+    const bool three = d.ndim == 3;
     auto pow2 = [](int n) { return n > 0 && (n & (n - 1)) == 0; };
     if (d.geom != MDG_SPHERICAL) { why = "3-D grids are spherical (dendritic) in this version"; return MDG_ERR_NOTIMPL; }
     if (d.n1 < 2 || d.n1 > (1 << 16)) return bad("n1 out of range [2, 2^16]");
     if (!pow2(d.n2) || d.n2 < 2 || d.n2 > (1 << 12)) return bad("n2 must be a power of two in [2, 4096]");
-    if (!pow2(d.n3) || d.n3 < 4 || d.n3 > (1 << 13)) return bad("n3 must be a power of two in [4, 8192]");
+    if (three && (!pow2(d.n3) || d.n3 < 4 || d.n3 > (1 << 13))) return bad("n3 must be a power of two in [4, 8192]");
+    if (!three && d.n3 != 1) return bad("a 2-D spherical grid has n3 = 1");
     if (!(d.dx[0] > 0.0 && d.dx[1] > 0.0 && d.dx[2] > 0.0)) return bad("dx must be positive");
     if (!(d.startx[0] >= 0.0)) return bad("the radial grid must start at r >= 0");
     if (d.startx[1] != -1.0 || std::fabs(d.startx[1] + d.n2 * d.dx[1] - 1) >= 1.0e-15)
@@ -122,18 +126,19 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
     if (!(d.cfl > 0.0)) return bad("cfl must be positive");
     if (d.enforce_floors != 0 && d.enforce_floors != 1) return bad("enforce_floors must be 0 or 1");
     if (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0) {
-      why = "fixed gravity is not built for 3-D grids";
+      why = "fixed gravity is not built for dendritic spherical grids";
       return MDG_ERR_NOTIMPL;
     }
     const bool ok = (d.bc_lo[0] == MDG_BC_REFLECT || d.bc_lo[0] == MDG_BC_SPHERICAL_ORIGIN) &&
                     (d.bc_hi[0] == MDG_BC_OUTFLOW || d.bc_hi[0] == MDG_BC_REFLECT);
     auto okj = [](int k) { return k == MDG_BC_REFLECT || k == MDG_BC_SPHERICAL_ORIGIN || k == MDG_BC_OUTFLOW; };
     auto okk = [](int k) { return k == MDG_BC_PERIODIC || k == MDG_BC_REFLECT || k == MDG_BC_OUTFLOW; };
-    if (!ok || !okj(d.bc_lo[1]) || !okj(d.bc_hi[1]) || !okk(d.bc_lo[2]) || !okk(d.bc_hi[2])) {
-      why = "unsupported 3-D boundary kinds";
+    if (!ok || !okj(d.bc_lo[1]) || !okj(d.bc_hi[1]) || (three && (!okk(d.bc_lo[2]) || !okk(d.bc_hi[2])))) {
+      why = "unsupported dendritic-grid boundary kinds";
       return MDG_ERR_NOTIMPL;
     }
-    if ((d.bc_lo[2] == MDG_BC_PERIODIC) != (d.bc_hi[2] == MDG_BC_PERIODIC)) return bad("periodic boundaries must be paired");
+    if (three && (d.bc_lo[2] == MDG_BC_PERIODIC) != (d.bc_hi[2] == MDG_BC_PERIODIC))
+      return bad("periodic boundaries must be paired");
     return MDG_OK;
   }
   if (d.n1 < 2 || d.n1 > (1 << 28)) return bad("n1 out of range [2, 2^28]");
@@ -161,7 +166,7 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
     if (d.geom == MDG_SPHERICAL && (d.startx[0] != d.startx[0])) return bad("bad startx");
   } else {
     if (d.geom != MDG_CARTESIAN) {
-      why = "2-D grids are Cartesian in this version";
+      why = "2-D grids are Cartesian or dendritic spherical";
       return MDG_ERR_NOTIMPL;
     }
     for (int dir = 0; dir < 2; dir++) {
@@ -259,8 +264,10 @@ static void free_all(mdg_solver *s)
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
-// A solver of one 3-D dendritic spherical problem (validated by the caller): the grid
-// tables of mdg_sweep3d.cu, state P and PH of ncell zones in the reference's zone order.
+// A solver of one dendritic spherical problem, 3-D or 2-D (validated by the caller): the
+// grid tables of mdg_sweep3d.cu, state P and PH of ncell zones in the reference's zone
+// order.  Its solver runs the dendritic lane (ndim 3 inside the solver) whatever the
+// problem's own ndim.
 static int create_3d(const mdg_problem_desc &d, int precision, int device, mdg_solver **out)
 {
   mdg_solver *s = new mdg_solver();
@@ -326,7 +333,11 @@ int mdg_grid3d_counts(const mdg_problem_desc *desc, int *nj, int *nk, long long 
 {
   if (!desc) return fail(MDG_ERR_INVALID, "desc");
   std::string why;
-  int rc = validate_desc(*desc, 3, why);
+  int rc = validate_desc(*desc, desc->ndim, why);
+  if (rc == MDG_OK && !is_dendritic(*desc)) {
+    rc = MDG_ERR_NOTIMPL;
+    why = "not a dendritic spherical grid";
+  }
   if (rc != MDG_OK) return fail(rc, why);
   Grid3Host h;
   build_grid3(*desc, h);
@@ -346,7 +357,11 @@ int mdg_grid3d_geometry(const mdg_problem_desc *desc, double *rows, long long *n
 {
   if (!desc) return fail(MDG_ERR_INVALID, "desc");
   std::string why;
-  int rc = validate_desc(*desc, 3, why);
+  int rc = validate_desc(*desc, desc->ndim, why);
+  if (rc == MDG_OK && !is_dendritic(*desc)) {
+    rc = MDG_ERR_NOTIMPL;
+    why = "not a dendritic spherical grid";
+  }
   if (rc != MDG_OK) return fail(rc, why);
   Grid3Host h;
   build_grid3(*desc, h);
@@ -395,16 +410,13 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
   }
-  if (ndim == 3) {
-    if (nprob != 1) return fail(MDG_ERR_NOTIMPL, "a 3-D solver advances one problem");
-    if (precision == MDG_PREC_MIXED && descs[0].hydro_interp_order != 3)
-      return fail(MDG_ERR_NOTIMPL, "the mixed-precision 3-D sweep is built for parabolic reconstruction");
-  }
+  const bool dendritic = is_dendritic(descs[0]);
+  if (dendritic && nprob != 1) return fail(MDG_ERR_NOTIMPL, "a dendritic-grid solver advances one problem");
   int ndev = 0;
   CK(cudaGetDeviceCount(&ndev));
   if (device < 0 || device >= ndev) return fail(MDG_ERR_INVALID, "device ordinal out of range");
   CK(cudaSetDevice(device));
-  if (ndim == 3) return create_3d(descs[0], precision, device, out);
+  if (dendritic) return create_3d(descs[0], precision, device, out);
 
   mdg_solver *s = new mdg_solver();
   s->device = device;

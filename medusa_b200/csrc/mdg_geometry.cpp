@@ -326,7 +326,9 @@ static double f_xth2g(double x) { return x * x * std::sin(th_of_x(x)) * dth_dx(x
 // with the reference's operation order (every product and sum as written there).
 void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
 {
-  const int n1 = d.n1, n2 = d.n2, n3 = d.n3;
+  const bool three = d.ndim == 3;
+  const int n1 = d.n1, n2 = d.n2, n3 = three ? d.n3 : 1;
+  h.ndim = three ? 3 : 2;
   h.n1 = n1; h.n2 = n2; h.n3 = n3;
   const double sx0 = d.startx[0], sx1 = d.startx[1], sx2 = d.startx[2];
   const double dx0 = d.dx[0], dx1 = d.dx[1], dx2 = d.dx[2];
@@ -364,8 +366,10 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
   h.nk.assign(nij, 0);
   auto NK = [&](int i, int j) -> int & { return h.nk[h.rowbase[i + NG] + j + NG]; };
 
-  // phi zones per (i, j)
-  {
+  // phi zones per (i, j); a 2-D grid has one (compute_dk's branch for other grids)
+  if (!three) {
+    for (auto &v : h.nk) v = n3;
+  } else {
     const int nk_min = 4;
     const double dph = n3 * dx2;
     NK(0, 0) = nk_min;
@@ -423,7 +427,7 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
     for (int j = 0; j < NJ(i); j++) { h.f0[h.row(i, j)] = f0; f0 += NK(i, j); }
   for (int i = 0; i < n1; i++)
     for (int j = 0; j <= NJ(i); j++) { h.f1[h.row(i, j)] = f1; f1 += n3 / std::min(DK(i, j), DK(i, j - 1)); }
-  for (int i = 0; i < n1; i++)
+  for (int i = 0; i < n1 && three; i++)
     for (int j = 0; j < NJ(i); j++) { h.f2[h.row(i, j)] = f2; f2 += NK(i, j) + 1; }
   h.ncell = c; h.nf0 = f0; h.nf1 = f1; h.nf2 = f2;
 

@@ -32,6 +32,7 @@ static_assert(G3_NFIELDS == MDG_GEO3_FIELDS, "row geometry record of mdg_grid3d_
 
 // Device view of the grid and its tables (pointers into one device allocation).
 struct Grid3 {
+  int ndim;                   // 3, or 2 for the axisymmetric (r, theta) grid (n3 = 1, no phi faces)
   int n1, n2, n3;
   int bc_lo0, bc_hi0, bc_lo1, bc_hi1, bc_lo2, bc_hi2;
   double dx0, dx1, dx2;
@@ -67,7 +68,7 @@ MDG_HD inline int ilog2(int s)
 
 // Host-side tables of the grid (built by build_grid3 in mdg_geometry.cpp).
 struct Grid3Host {
-  int n1 = 0, n2 = 0, n3 = 0;
+  int ndim = 3, n1 = 0, n2 = 0, n3 = 0;
   std::vector<int> nj, rowbase, nk;
   std::vector<int64_t> cell, f0, f1, f2;
   std::vector<double> geo, rc0, rc1, rc2, xc1, xc2, sth, cth, sphc, cphc, sphl, cphl;

@@ -18,6 +18,13 @@ enum { RHO = 0, UU = 1, U1 = 2, U2 = 3, U3 = 4 };
 enum { BC_OUTFLOW = 0, BC_REFLECT = 1, BC_EXTRAP = 2, BC_PERIODIC = 3, BC_PROB = 4,
        BC_SPHERICAL_ORIGIN = 5 };
 
+// Problems on the dendritic spherical grid (DENDRITIC_GRID=TRUE with GEOM=SPHERICAL):
+// every 3-D problem, and 2-D problems in spherical (r, theta) coordinates.
+inline bool is_dendritic(const mdg_problem_desc &d)
+{
+  return d.ndim == 3 || (d.ndim == 2 && d.geom == MDG_SPHERICAL);
+}
+
 // Per-zone reconstruction coefficients along one direction: the geometry-only
 // sub-expressions of para_recon (reconstruct.c:151-157,174-175) and lin_recon
 // (reconstruct.c:100-104), precomputed on the host in the reference's operation order.

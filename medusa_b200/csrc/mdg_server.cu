@@ -244,7 +244,7 @@ int64_t bytes_per_cell_2d() { return 3 * NPRIM * 8 + 2; }
 // bytes each: the face count of set_shock_flag, as in the solver's layout).
 void footprint(const mdg_problem_desc &d, int64_t &units, int64_t &cells)
 {
-  if (d.ndim == 2) {
+  if (d.ndim == 2 && !is_dendritic(d)) {
     units = (int64_t)d.n1 + 2 * NG + d.n2 + 2 * NG;
     cells = (int64_t)(d.n1 + 3) * d.n2;
   } else {
@@ -310,7 +310,7 @@ int admit(mdg_server *s, Request *r)
   const int64_t w = r->units, seg = r->seg;
   ProbDev P;
   make_probdev(d, P);
-  if (d.ndim == 3) {
+  if (is_dendritic(d)) {
     // its own grid (built at submission); the AoS initial state is staged in PH
     P.n2 = d.n2;
     P.ncell = r->ncell;
@@ -393,10 +393,10 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
   for (int k : fin) {
     Request *r = s->slots[k];
     const int64_t n = r->ncell;
-    const bool two = r->desc.ndim == 2;
+    const bool two = r->desc.ndim == 2 && !is_dendritic(r->desc);
     const double *src = two ? s->P2.v[0] + r->seg2 : s->P.v[0] + r->seg;
     size_t pitch = sizeof(double) * (two ? s->cells : s->units);
-    if (r->desc.ndim == 3) {
+    if (is_dendritic(r->desc)) {
       src = r->d_state3;
       pitch = sizeof(double) * n;
     }
@@ -420,7 +420,7 @@ int retire_all(mdg_server *s, const std::vector<int> &fin)
     r->err = T.err;
     r->t_done = now;
     s->slots[k] = nullptr;
-    if (r->desc.ndim == 3) {
+    if (is_dendritic(r->desc)) {
       // the round has ended (retire_all waited for the stream): give its memory back
       s->jobs3.erase(std::find(s->jobs3.begin(), s->jobs3.end(), r));
       s->jobs3_version++;
@@ -466,7 +466,7 @@ int round_once(mdg_server *s, int *active_out)
       for (int k = 0; k < s->max_probs; k++)
         if (!s->slots[k]) { slot = k; break; }
       if (slot < 0) break;
-      if (r->desc.ndim == 3) {
+      if (is_dendritic(r->desc)) {
         if (s->bytes3_in_use + r->bytes3 > s->cfg.hbm_bytes_3d) { ++it; continue; }
         s->bytes3_in_use += r->bytes3;
         r->slot = slot;
@@ -512,7 +512,7 @@ int round_once(mdg_server *s, int *active_out)
     std::vector<Tile> tl, xt, yt;
     for (int k = 0; k < s->max_probs; k++) {
       const Request *r = s->slots[k];
-      if (!r || r->desc.ndim == 3) continue;   // 3-D problems run on their own grids
+      if (!r || is_dendritic(r->desc)) continue;   // dendritic problems run on their own grids
       if (r->desc.ndim == 2) {
         // the solver's 2-D tiling: direction-0 tiles of TIX2 rows x NTX2 columns,
         // direction-1 tiles of TIY2 rows x TJY2 columns
@@ -749,8 +749,9 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
   if (rc != MDG_OK) return sfail(rc, "request: " + why);
   if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
     return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
-  if (ndim == 3) {
-    if (s->cfg.hbm_bytes_3d <= 0) return sfail(MDG_ERR_NOTIMPL, "request: the server takes no 3-D requests");
+  if (is_dendritic(*desc)) {
+    // 3-D requests and 2-D spherical (r, theta) requests: the dendritic lane
+    if (s->cfg.hbm_bytes_3d <= 0) return sfail(MDG_ERR_NOTIMPL, "request: the server takes no dendritic-grid requests");
     if (s->cfg.precision == MDG_PREC_MIXED && desc->hydro_interp_order != 3)
       return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep is built for parabolic reconstruction");
     // its grid tables, face fluxes and state, built here in the submitting thread
@@ -760,7 +761,7 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
     rc = sweep3_create(*desc, &r->s3, why);
     if (rc != MDG_OK) {
       delete r;
-      return sfail(rc, "request: 3-D grid: " + why);
+      return sfail(rc, "request: dendritic grid: " + why);
     }
     r->ncell = sweep3_ncell(r->s3);
     const cudaError_t e = cudaMalloc(&r->d_state3, sizeof(double) * 2 * NPRIM * r->ncell);
@@ -769,7 +770,7 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
       sweep3_destroy(r->s3);
       if (e == cudaSuccess) cudaFree(r->d_state3);
       delete r;
-      return sfail(MDG_ERR_OUTOFMEM, "request: the 3-D problem does not fit in hbm_bytes_3d");
+      return sfail(MDG_ERR_OUTOFMEM, "request: the dendritic-grid problem does not fit in hbm_bytes_3d");
     }
     r->ic.assign(prim, prim + (size_t)NPRIM * r->ncell);
     r->t_submit = Clock::now();

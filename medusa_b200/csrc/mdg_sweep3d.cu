@@ -219,9 +219,16 @@ __device__ void pencil0(const Grid3 &g, const ProbDev &P, const StateSoA &s, int
   const double x2p = __ldg(g.xc2 + g.rc2_base[ilog2(dks(g, i, j))] + NG + k);
   const int dkij = dks(g, i, j);
   double p0[7], p1[7], p2[7];
-  kslope_point(g, P, s, ii, jj - 1, k * dkij / dks(g, ii, jj - 1), x2p, p0);
-  kslope_point(g, P, s, ii, jj, k * dkij / dks(g, ii, jj), x2p, p1);
-  kslope_point(g, P, s, ii, jj + 1, k * dkij / dks(g, ii, jj + 1), x2p, p2);
+  if (g.ndim == 2) {
+    // the 2-D prolongate0 (step.c:579-628) has no phi slopes
+    load7(g, P, s, ii, jj - 1, 0, p0);
+    load7(g, P, s, ii, jj, 0, p1);
+    load7(g, P, s, ii, jj + 1, 0, p2);
+  } else {
+    kslope_point(g, P, s, ii, jj - 1, k * dkij / dks(g, ii, jj - 1), x2p, p0);
+    kslope_point(g, P, s, ii, jj, k * dkij / dks(g, ii, jj), x2p, p1);
+    kslope_point(g, P, s, ii, jj + 1, k * dkij / dks(g, ii, jj + 1), x2p, p2);
+  }
   const int base = g.rc1_base[ilog2(djii)] + NG;
   const double x10 = __ldg(g.xc1 + base + jj - 1), x11 = __ldg(g.xc1 + base + jj), x12 = __ldg(g.xc1 + base + jj + 1);
   const double idx1m = 1.0 / (x11 - x10), idx1p = 1.0 / (x12 - x11), idx1c = 1.0 / (x12 - x10);
@@ -780,7 +787,7 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
       }
     }
     // direction 2
-    {
+    if (g.ndim == 3) {
       const int64_t f2 = __ldg(g.f2 + ij) + k;
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) divF[v] += F2[v * g.nf2 + f2 + 1] - F2[v * g.nf2 + f2];
@@ -804,8 +811,10 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
       lmin = tmin(lmin, 1.0 / local_dt);
       local_dt += (fabs(pf[U2]) + cs / geo3(g, G3_SCALE + 1, ij)) / (g.dx1 * djs(g, i));
       lmin = tmin(lmin, 1.0 / local_dt);
-      local_dt += (fabs(pf[U3]) + cs / geo3(g, G3_SCALE + 2, ij)) / (g.dx2 * dks(g, i, j));
-      lmin = tmin(lmin, 1.0 / local_dt);
+      if (g.ndim == 3) {
+        local_dt += (fabs(pf[U3]) + cs / geo3(g, G3_SCALE + 2, ij)) / (g.dx2 * dks(g, i, j));
+        lmin = tmin(lmin, 1.0 / local_dt);
+      }
     }
   }
   (void)lmax;
@@ -832,8 +841,10 @@ __global__ void __launch_bounds__(NT3) estimate3_kernel(const ProbDev *__restric
     lmin = tmin(lmin, 1.0 / local_dt);
     local_dt += (fabs(s.v[U2][c]) + cs / geo3(g, G3_SCALE + 1, ij)) / (g.dx1 * djs(g, i));
     lmin = tmin(lmin, 1.0 / local_dt);
-    local_dt += (fabs(s.v[U3][c]) + cs / geo3(g, G3_SCALE + 2, ij)) / (g.dx2 * dks(g, i, j));
-    lmin = tmin(lmin, 1.0 / local_dt);
+    if (g.ndim == 3) {
+      local_dt += (fabs(s.v[U3][c]) + cs / geo3(g, G3_SCALE + 2, ij)) / (g.dx2 * dks(g, i, j));
+      lmin = tmin(lmin, 1.0 / local_dt);
+    }
   }
   block_min_to(lmin, &times[0].minacc, sred);
 }
@@ -944,6 +955,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   e = cudaMemcpy(w->d_tab, host.data(), tot, cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail3(e);
   Grid3 &g = w->g;
+  g.ndim = h.ndim;
   g.n1 = h.n1; g.n2 = h.n2; g.n3 = h.n3;
   g.bc_lo0 = d.bc_lo[0]; g.bc_hi0 = d.bc_hi[0]; g.bc_lo1 = d.bc_lo[1]; g.bc_hi1 = d.bc_hi[1];
   g.bc_lo2 = d.bc_lo[2]; g.bc_hi2 = d.bc_hi[2];
@@ -975,7 +987,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t0, i, j, h.nk[h.row(i, j)]);
   for (int i = 0; i < h.n1; i++)
     for (int j = 0; j <= h.njr(i); j++) tiles_of_rows(t1, i, j, h.n3 / std::min(h.dk(i, j), h.dk(i, j - 1)));
-  for (int i = 0; i < h.n1; i++)
+  for (int i = 0; i < h.n1 && h.ndim == 3; i++)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t2, i, j, h.nk[h.row(i, j)] + 1, T2);
   for (int i = 0; i < h.n1; i++)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(tc, i, j, h.nk[h.row(i, j)]);
@@ -1017,7 +1029,7 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
     constexpr bool M = decltype(mix)::value;
     face0_kernel<S, M><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
     face1_kernel<S, M><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
-    face2_kernel<S, M><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
+    if (w->nt[2] > 0) face2_kernel<S, M><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
   };
   using I0 = std::integral_constant<int, 0>;
   using I1 = std::integral_constant<int, 1>;

@@ -274,13 +274,14 @@ def _th_of_x(x: float) -> float:
     return 0.5 * math.pi * (x + 1.0)    # THCOORD=UNIFORM, metric_spherical_general.c:222-230
 
 
-def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple):
+def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: int = 3):
     """Zone counts of the dendritic spherical grid: nj[i] theta zones of radial row i and
     nk[i][j] phi zones of row (i, j), for the interior rows (the rules of compute_dj and
     compute_dk, utils.c:181-354, for a uniform radius and theta: theta zones double
     outwards from 2 at the centre and phi zones from 4 at each pole while the zone aspect
-    ratio exceeds 2^0.5).  Returns (nj, nk) as lists; the interior zones in the
-    reference's zone order are i, then j < nj[i], then k < nk[i][j]."""
+    ratio exceeds 2^0.5; on a 2-D grid every row has n3 = 1 phi zone).  Returns (nj, nk) as
+    lists; the interior zones in the reference's zone order are i, then j < nj[i], then
+    k < nk[i][j]."""
     nj = [0] * n1
     nj[0] = 2
     dth = _th_of_x(startx[1] + n2 * dx[1]) - _th_of_x(startx[1])
@@ -294,6 +295,8 @@ def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple):
             nj[i] *= 2
         nj[i] = min(max(nj[i], nj[i - 1]), n2)
     dj = [n2 // v for v in nj]
+    if ndim == 2:
+        return nj, [[n3] * nj[i] for i in range(n1)]
     dph = n3 * dx[2]
     nk = []
     for i in range(n1):
@@ -354,6 +357,32 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
     return Problem(name="sedov3d_%dx%dx%d" % (n1, n2, n3), ndim=3, geom=SPHERICAL, n=(n1, n2, n3),
                    startx=startx, dx=dx, gam=gam, ic=ic,
                    bc_lo=(bc_inner, bc_pole, PERIODIC), bc_hi=(OUTFLOW, bc_pole, PERIODIC),
+                   cfl=cfl, tmax=tmax, cells=ncell)
+
+
+def sedov_2d_spherical(n1: int = 256, n2: int = 128, gam: float = 1.4, energy: float = 1.0, r_dep: float = 0.02,
+                       p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100, bc_inner: int = REFLECT,
+                       bc_pole: int = REFLECT, noise: float = 0.0, seed: int = 20240604) -> Problem:
+    """Axisymmetric (r, theta) Sedov blast on the 2-D dendritic spherical grid: theta zones
+    double outwards from 2 at the centre (compute_dj, utils.c:181-238); otherwise as
+    sedov_3d (energy in the zones inside r_dep, seeded noise in density and velocities)."""
+    startx, dx = (0.0, -1.0, 0.0), (1.0 / n1, 2.0 / n2, 2.0 * math.pi)
+    nj, _ = dendritic_grid(n1, n2, 1, startx, dx, ndim=2)
+    ncell = int(sum(nj))
+    rc = (np.arange(n1) + 0.5) * dx[0]
+    inside = rc < r_dep
+    r_e = (np.nonzero(inside)[0].max() + 1) * dx[0] if inside.any() else dx[0]
+    u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
+    ic = np.zeros((ncell, NPRIM))
+    ic[:, 0] = 1.0
+    ic[:, 1] = np.repeat(np.where(inside, u_dep, p_amb / (gam - 1.0)), nj)
+    if noise > 0.0:
+        u = uniform01(seed, 4 * ncell).reshape(ncell, 4)
+        ic[:, 0] *= 1.0 + noise * (2.0 * u[:, 0] - 1.0)
+        for v in range(3):
+            ic[:, 2 + v] = 0.1 * noise * (2.0 * u[:, 1 + v] - 1.0)
+    return Problem(name="sedov2dsph_%dx%d" % (n1, n2), ndim=2, geom=SPHERICAL, n=(n1, n2, 1), startx=startx,
+                   dx=dx, gam=gam, ic=ic, bc_lo=(bc_inner, bc_pole, PERIODIC), bc_hi=(OUTFLOW, bc_pole, PERIODIC),
                    cfl=cfl, tmax=tmax, cells=ncell)
 
 

@@ -170,7 +170,7 @@ GEO3_FIELDS = 42
 
 def grid3d_counts(pb: "_pb.Problem"):
     """(nj[i] for the n1 radial rows, nk of every interior row (i, j) in zone order, zone
-    count) of a 3-D dendritic spherical problem (mdg_grid3d_counts)."""
+    count) of a dendritic spherical problem, 3-D or 2-D (mdg_grid3d_counts)."""
     d = desc_of(pb)
     n = ctypes.c_longlong()
     nj = np.zeros(pb.n[0], dtype=np.int32)
@@ -181,7 +181,7 @@ def grid3d_counts(pb: "_pb.Problem"):
 
 
 def grid3d_geometry(pb: "_pb.Problem") -> np.ndarray:
-    """Per-row zone geometry [rows, 42] of a 3-D dendritic spherical problem, rows i in
+    """Per-row zone geometry [rows, 42] of a dendritic spherical problem (3-D or 2-D), rows i in
     [-2, n1+2), j in [-2, nj[i]+2) (mdg_grid3d_geometry)."""
     d = desc_of(pb)
     n = ctypes.c_longlong()
@@ -192,7 +192,7 @@ def grid3d_geometry(pb: "_pb.Problem") -> np.ndarray:
 
 
 def grid3d_zone_volumes(pb: "_pb.Problem") -> np.ndarray:
-    """Volume of every interior zone of a 3-D dendritic problem, in zone order."""
+    """Volume of every interior zone of a dendritic (3-D or 2-D spherical) problem, in zone order."""
     nj, nk, n = grid3d_counts(pb)
     geo = grid3d_geometry(pb)
     n1 = pb.n[0]
@@ -210,7 +210,7 @@ def grid3d_zone_volumes(pb: "_pb.Problem") -> np.ndarray:
 
 
 def grid3d_radial_mean(pb: "_pb.Problem", field: np.ndarray) -> np.ndarray:
-    """Volume-weighted mean of a zone field over each radial row of a 3-D problem."""
+    """Volume-weighted mean of a zone field over each radial row of a dendritic problem."""
     nj, nk, n = grid3d_counts(pb)
     vol = grid3d_zone_volumes(pb)
     out = np.zeros(pb.n[0])

@@ -73,6 +73,9 @@ CONFIGS = {
     # 3-D spherical on the dendritic grid (Sedov blast), uniform radius and theta
     "sph3d": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
                   RCOORD="UNIFORM", THCOORD="UNIFORM"),
+    # 2-D (r, theta) spherical on the dendritic grid
+    "sph2d": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                  RCOORD="UNIFORM", THCOORD="UNIFORM"),
 }
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]

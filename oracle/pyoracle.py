@@ -188,7 +188,7 @@ def run_reference(pb, nsteps: int, every: int = 1):
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         _write_input(pb, fin)
-        subprocess.run([exe, "run", fin, fout, str(nsteps), str(every)], check=True,
+        subprocess.run([exe, "run", fin, fout, str(nsteps), str(every)], check=True, cwd=td,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
         raw = np.fromfile(fout, dtype=np.float64)
     rec = 4 + 5 * pb.ncell
@@ -201,7 +201,8 @@ def _ref_dump(pb, what: str) -> bytes:
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         _write_input(pb, fin)
-        subprocess.run([exe, what, fin, fout], check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        subprocess.run([exe, what, fin, fout], check=True, cwd=td, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
         with open(fout, "rb") as f:
             return f.read()
 
@@ -233,7 +234,7 @@ def time_reference(pb, warmup: int, steps: int, fast: bool = True) -> dict:
     with tempfile.TemporaryDirectory() as td:
         fin = os.path.join(td, "in.bin")
         _write_input(pb, fin)
-        r = subprocess.run([exe, "time", fin, str(warmup), str(steps)], check=True,
+        r = subprocess.run([exe, "time", fin, str(warmup), str(steps)], check=True, cwd=td,
                            capture_output=True, text=True)
     out = {}
     for tok in r.stdout.split():

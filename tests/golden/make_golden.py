@@ -41,13 +41,19 @@ def cases():
 
 
 def cases3d():
-    """3-D dendritic spherical cases (Sedov blast): name -> (problem, nsteps).  Their
-    fixtures also hold one step started afresh from the final state (prim1)."""
+    """Dendritic spherical cases (Sedov blast, 3-D and 2-D): name -> (problem, nsteps).
+    Their fixtures also hold one step started afresh from the final state (prim1)."""
     return {
         "sedov3d_20x16x32": (P.sedov_3d(20, 16, 32, r_dep=0.2), 30),
         "sedov3d_noisy_18x8x16": (P.sedov_3d(18, 8, 16, r_dep=0.25, noise=0.1), 30),
         "sedov3d_noisy_origin_16x8x16": (P.sedov_3d(16, 8, 16, r_dep=0.25, noise=0.05, bc_inner=P.SPHERICAL_ORIGIN,
                                                     bc_pole=P.SPHERICAL_ORIGIN), 30),
+        # 2-D (r, theta) grids: the same machinery without phi faces
+        "sedov2dsph_24x16": (P.sedov_2d_spherical(24, 16, r_dep=0.2), 40),
+        "sedov2dsph_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.2, noise=0.1), 40),
+        "sedov2dsph_noisy_origin_32x16": (P.sedov_2d_spherical(32, 16, r_dep=0.25, noise=0.05,
+                                                               bc_inner=P.SPHERICAL_ORIGIN,
+                                                               bc_pole=P.SPHERICAL_ORIGIN), 40),
     }
 
 

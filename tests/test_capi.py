@@ -132,3 +132,22 @@ def test_output_calls_reject_null_solver():
     assert L.mdg_snapshot_read(None, None, None, None) == 1
     assert L.mdg_snapshot_write_ascii1(None, b"x") == 1
     assert L.mdg_dump_ascii1(None, 0, b"x") == 1
+
+
+@pytest.mark.parametrize("mutate,nprob,code", [
+    (dict(n=(24, 12, 1)), 1, 1),                        # n2 not a power of two
+    (dict(n=(24, 16, 4)), 1, 1),                        # a 2-D grid has one phi zone
+    (dict(dx=(1.0 / 24, 2.0 / 16, 1.0)), 1, 1),         # its phi zone spans 2 pi
+    (dict(startx=(0.0, -0.5, 0.0)), 1, 1),              # theta over the whole sphere
+    (dict(grav=(0.0, -1.0, 0.0)), 1, 5),                # fixed gravity not on dendritic grids
+    (dict(), 2, 5),                                     # one problem per dendritic solver
+])
+def test_2d_spherical_scope_checked_before_device_work(mutate, nprob, code):
+    """2-D (r, theta) spherical problems run on the dendritic grid: its geometry rules
+    are checked before any device work."""
+    pb = P.sedov_2d_spherical(24, 16, r_dep=0.3).copy(**mutate)
+    arr = (S.ProblemDesc * nprob)(*[S.desc_of(pb)] * nprob)
+    h = ctypes.c_void_p()
+    assert S.library().mdg_create(arr, nprob, 0, 0, ctypes.byref(h)) == code
+    assert not h.value
+    assert S.library().mdg_last_error_message()

@@ -203,14 +203,17 @@ def test_server_2d_slot_reuse_and_graph_recapture():
 
 
 def _mix_3d():
+    # 3-D grids and a 2-D (r, theta) one: all run on the dendritic lane
     return [P.sedov_3d(12, 8, 16, r_dep=0.3).copy(tmax=0.004, name="sedov3d_a"),
-            P.sedov_3d(16, 8, 16, r_dep=0.3, noise=0.05).copy(tmax=0.006, name="sedov3d_b")]
+            P.sedov_3d(16, 8, 16, r_dep=0.3, noise=0.05).copy(tmax=0.006, name="sedov3d_b"),
+            P.sedov_2d_spherical(32, 16, r_dep=0.25, noise=0.05).copy(tmax=0.005, name="sedov2dsph_c")]
 
 
 @pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
 def test_server_3d_requests_equal_solver(precision):
-    """3-D requests (each with its own dendritic grid, in the server's precision) beside
-    1-D and 2-D ones: every result is the solver's run of the same problem, bit for bit."""
+    """Dendritic-grid requests (3-D, and 2-D in r and theta; each with its own grid, in
+    the server's precision) beside 1-D and 2-D Cartesian ones: every result is the
+    solver's run of the same problem, bit for bit."""
     reqs3 = _mix_3d()
     reqs = [(pb, precision) for pb in reqs3] + [(pb, precision) for pb in _mix()[:2]] + \
            [(pb, precision) for pb in _mix_2d()[:1]]

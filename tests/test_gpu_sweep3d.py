@@ -1,8 +1,8 @@
-"""GPU parity of the 3-D dendritic spherical sweep against fixtures made by the
-reference itself (tests/golden/make_golden.py, cases3d): Sedov blasts on small
-dendritic grids, symmetric and with seeded noise (shock tagging, rotation through the
-pole rows, restriction of the phi velocity into the Gamma slot), reflecting and
-SPHERICAL_ORIGIN boundaries.
+"""GPU parity of the dendritic spherical sweep against fixtures made by the reference
+itself (tests/golden/make_golden.py, cases3d): Sedov blasts on small 3-D dendritic
+grids and on 2-D (r, theta) ones, symmetric and with seeded noise (shock tagging,
+rotation through the pole rows, restriction of the phi velocity into the Gamma slot),
+reflecting and SPHERICAL_ORIGIN boundaries.
 
 Error measure per variable: max |gpu - ref| over the zones divided by the largest
 magnitude of that variable (density, internal energy) or of any velocity component
@@ -73,6 +73,15 @@ def test_3d_mass_change_is_the_outer_boundary_flux():
     assert abs(m1[0] - m0[0]) <= 1.0e-13 * m0[0]
 
 
+def test_2d_spherical_mass_change_is_the_outer_boundary_flux():
+    pb, n = CASES3["sedov2dsph_24x16"]
+    with Solver(pb) as s:
+        m0, _ = s.conserved_totals()
+        s.step(10)
+        m1, _ = s.conserved_totals()
+    assert abs(m1[0] - m0[0]) <= 1.0e-13 * m0[0]
+
+
 # ---------------------------------------------------------------- mixed precision
 def _shock_radius(pb, prim):
     """Radius of the largest radial-row mean density."""
@@ -119,3 +128,36 @@ def test_3d_mixed_matches_fp64_at_equal_time():
     assert drift_m <= 1.0e-6 and drift_e <= 1.0e-6
     assert abs(r_mix - r_ref) <= pb.dx[0]
     assert abs(r_ref - r_sedov) <= 4 * pb.dx[0]
+
+
+def test_2d_spherical_mixed_matches_fp64_at_equal_time():
+    """The mixed-precision dendritic sweep on a 2-D (r, theta) Sedov blast: the same bars
+    as in 3-D against the plain FP64 sweep at the same time."""
+    from medusa_b200 import analytic as A
+    from medusa_b200.solver import PREC_MIXED, grid3d_zone_volumes
+    pb = P.sedov_2d_spherical(96, 64, r_dep=0.06, noise=0.02)
+    n = 80
+    with Solver(pb) as s:
+        s.step(n)
+        ref = s.update_cpu(0)
+        t_end = s.time(0)[0]
+        m0, e0 = s.conserved_totals()
+    with Solver(pb.copy(tmax=t_end), precision=PREC_MIXED) as s:
+        for _ in range(40):
+            s.step(5)
+            if s.time(0)[0] >= t_end * (1.0 - 1.0e-12):
+                break
+        mix = s.update_cpu(0)
+        t_mix = s.time(0)[0]
+        m1, e1 = s.conserved_totals()
+    assert abs(t_mix - t_end) <= 1.0e-8 * t_end
+    vol = grid3d_zone_volumes(pb)
+    l1_rho = A.l1_rel(mix[:, 0], ref[:, 0], vol)
+    l1_u = A.l1_rel(mix[:, 1], ref[:, 1], vol)
+    drift_m = abs(m1[0] - m0[0]) / m0[0]
+    drift_e = abs(e1[0] - e0[0]) / e0[0]
+    record("sweep2dsph_mixed_sedov_96x64", l1_rho=l1_rho, l1_u=l1_u, drift_mass=drift_m, drift_energy=drift_e, t=t_end)
+    assert np.all(np.isfinite(mix))
+    assert l1_rho <= 1.0e-4 and l1_u <= 1.0e-4
+    assert drift_m <= 1.0e-6 and drift_e <= 1.0e-6
+    assert abs(_shock_radius(pb, mix) - _shock_radius(pb, ref)) <= pb.dx[0]

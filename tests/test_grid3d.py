@@ -1,4 +1,4 @@
-"""The 3-D dendritic spherical grid on the host: zone counts (compute_dj/compute_dk,
+"""The dendritic spherical grid (3-D, and 2-D in r and theta) on the host: zone counts (compute_dj/compute_dk,
 utils.c:181-354) and per-row zone geometry (init_geometry, metric_spherical_general.c)
 of the library against the Python restatement and against the reference build itself;
 the 3-D fixtures against the problem generator and the live reference."""
@@ -59,6 +59,49 @@ def test_geometry_bit_identical_to_reference(dims):
             r += 1
 
 
+@pytest.mark.parametrize("dims", [(24, 16), (256, 128), (5, 2)])
+def test_2d_zone_counts_match_restatement(dims):
+    pb = P.sedov_2d_spherical(*dims, r_dep=0.3)
+    nj, nk, n = S.grid3d_counts(pb)
+    pj, _ = P.dendritic_grid(dims[0], dims[1], 1, pb.startx, pb.dx, ndim=2)
+    assert list(nj) == pj
+    assert np.all(nk == 1)
+    assert n == pb.ncell == sum(pj)
+
+
+# the NDIM=2 record of ref_get_geom: vol, area[2], gcov[3][3], gcon[3], scale[3][3], conn[27]
+@pytest.mark.parametrize("dims", [(24, 16), (48, 32), (40, 64)])
+def test_2d_geometry_bit_identical_to_reference(dims):
+    pb = P.sedov_2d_spherical(*dims, r_dep=0.2)
+    if not pyoracle.ref_available(pb):
+        pytest.skip("oracle/_ref not built (needs the reference tree)")
+    rnj, _ = pyoracle.reference_grid(pb)
+    geo = S.grid3d_geometry(pb)
+    ref = pyoracle.reference_geometry(pb)
+    assert geo.shape[0] == ref.shape[0]
+    assert not np.any(ref[:, 24:51][:, [c for c in range(27) if c not in CONN_SET]])
+    n1 = dims[0]
+    r = 0
+    for i in range(-2, n1 + 2):
+        for j in range(-2, rnj[i + 2] + 2):
+            pairs = [(geo[r, 0:1], ref[r, 0:1]), (geo[r, 4:13], ref[r, 3:12]), (geo[r, 16:19], ref[r, 12:15]),
+                     (geo[r, 19:28], ref[r, 15:24])]
+            if 0 <= i <= n1 and 0 <= j <= rnj[i + 2]:
+                pairs.append((geo[r, 1:3], ref[r, 1:3]))
+            if 0 <= i < n1 and 0 <= j < rnj[i + 2]:
+                pairs.append((geo[r, 31:42], ref[r, 24:51][CONN_SET]))
+            for a, b in pairs:
+                assert np.array_equal(a, b), (i, j)
+            r += 1
+
+
+def test_2d_zone_volumes_fill_the_sphere():
+    pb = P.sedov_2d_spherical(32, 16, r_dep=0.2)
+    vol = S.grid3d_zone_volumes(pb)
+    assert vol.shape == (pb.ncell,) and np.all(vol > 0)
+    assert abs(vol.sum() - 4.0 / 3.0 * np.pi) <= 1.0e-12
+
+
 def test_grid_calls_validate():
     pb = P.sedov_3d(16, 8, 16)
     with pytest.raises(MdgError) as e:
@@ -66,6 +109,9 @@ def test_grid_calls_validate():
     assert e.value.code == 1
     with pytest.raises(MdgError) as e:
         S.grid3d_counts(pb.copy(geom=P.CARTESIAN))
+    assert e.value.code == 5
+    with pytest.raises(MdgError) as e:
+        S.grid3d_counts(P.kelvin_helmholtz(16, 16, nsteps=1))
     assert e.value.code == 5
 
 
