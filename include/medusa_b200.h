@@ -55,6 +55,10 @@ extern "C" {
 /* PROB boundary hooks restated on the device (the reference's prob_bounds callbacks) */
 #define MDG_PROB_NONE 0
 #define MDG_PROB_NOH 1   /* problems/init_spherical_noh.c:63-79 */
+/* radial coordinate maps r(x) of spherical grids (RCOORD, metric_spherical_general.c:149-219) */
+#define MDG_RCOORD_UNIFORM 0   /* r = |x| */
+#define MDG_RCOORD_SINH 1      /* r = rtrans sinh(|x| / rtrans): zones of width dx near the
+                                  centre, growing geometrically outside rtrans */
 
 /* arithmetic of the sweep */
 #define MDG_PREC_FP64 0   /* plain: FP64 throughout, the reference's operation order */
@@ -71,8 +75,9 @@ extern "C" {
  * (geometry.c:4-63) are rebuilt from these fields by the library, bit-identically.
  */
 typedef struct mdg_problem_desc {
-  int ndim;                 /* 1 or 2 */
-  int geom;                 /* MDG_CARTESIAN (1-D, 2-D) or MDG_SPHERICAL (1-D) */
+  int ndim;                 /* 1, 2 or 3 */
+  int geom;                 /* MDG_CARTESIAN (1-D, 2-D) or MDG_SPHERICAL (1-D; 2-D and 3-D on
+                               the dendritic grid, DENDRITIC_GRID=TRUE) */
   int eos;                  /* MDG_GAMMA_LAW or MDG_POLYTROPIC */
   int n1, n2, n3;           /* interior zones; n2 = n3 = 1 in 1-D */
   double startx[3];         /* lower coordinate edge of zone 0 */
@@ -87,6 +92,9 @@ typedef struct mdg_problem_desc {
   double rho_floor, e_floor;/* floors set by the problem hook (io.c:5081-5082 defaults -1) */
   double grav[3];           /* fixed contravariant gravitational acceleration g0 (the GRAV=FIXED_GRAV
                                build, gravity.c:38-64; init_rt.c:57-59); all zero: NO_GRAV */
+  int rcoord;               /* MDG_RCOORD_* radial map of a spherical grid (the RCOORD build switch) */
+  double rtrans;            /* transition radius of the SINH map (rx_info.rtrans; problem hooks
+                               set it with rtrans_solve, e.g. problems/init_sedov.c:20) */
 } mdg_problem_desc;
 
 typedef struct mdg_solver mdg_solver;   /* opaque */

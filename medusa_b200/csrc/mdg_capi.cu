@@ -13,6 +13,7 @@
 namespace mdg {
 void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+double radial_coordinate(const mdg_problem_desc &d, double x);
 void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area0, double &area1);
 void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
@@ -103,6 +104,15 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
   if (d.ndim != 1 && d.ndim != 2 && d.ndim != 3) return bad("ndim must be 1, 2 or 3");
   if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
+  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH) return bad("unknown radial map (rcoord)");
+  if (d.rcoord == MDG_RCOORD_SINH) {
+    if (d.geom != MDG_SPHERICAL) return bad("radial maps apply to spherical grids");
+    if (!(d.rtrans > 0.0) || !(d.rtrans < 1.0e300)) return bad("rtrans must be positive and finite");
+    if (d.bc_lo[0] == MDG_BC_PROB || d.bc_hi[0] == MDG_BC_PROB) {
+      why = "the Noh inflow boundary is built for the uniform radial map";
+      return MDG_ERR_NOTIMPL;
+    }
+  }
   if (is_dendritic(d)) {
     // the dendritic spherical grid of prim_to_fluxes3 (3-D) or prim_to_fluxes2 (2-D,
     // step.c:659-764) over the whole sphere; a 2-D grid has one phi zone of width 2 pi
@@ -409,6 +419,9 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (precision == MDG_PREC_MIXED && descs[m].geom == MDG_SPHERICAL && !(descs[m].startx[0] >= 0.0))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
+    if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].rcoord != MDG_RCOORD_UNIFORM)
+      return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
+                                       ": the 1-D mixed-precision sweep computes the uniform-radius geometry in closed form");
   }
   const bool dendritic = is_dendritic(descs[0]);
   if (dendritic && nprob != 1) return fail(MDG_ERR_NOTIMPL, "a dendritic-grid solver advances one problem");
@@ -962,7 +975,7 @@ int mdg_snapshot_write_ascii1(mdg_solver *s, const char *path)
   double mass = 0.0;
   for (int64_t i = 0; i < n; i++) {
     double x = d.startx[0] + (i + 0.5) * d.dx[0];
-    if (d.geom == MDG_SPHERICAL) x = std::fabs(x);
+    if (d.geom == MDG_SPHERICAL) x = radial_coordinate(d, x);
     const double s00 = geo[(size_t)GF_S00 * w + i + NG], vol = geo[(size_t)GF_VOL * w + i + NG];
     std::fprintf(fp, "%16.14e ", x);
     const double *p = prim + NPRIM * i;

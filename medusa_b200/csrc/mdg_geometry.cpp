@@ -4,7 +4,7 @@
 //
 //   Cartesian: metrics/metric_cartesian.c:47-55 (volume moments), 127-295 (volume,
 //              area, gcov, gcon, scale; conn = 0)
-//   Spherical, 1-D, uniform radius (RCOORD=UNIFORM, THCOORD=UNIFORM):
+//   Spherical, 1-D, radius UNIFORM or SINH (the RCOORD switch), THCOORD=UNIFORM:
 //              metrics/metric_spherical_general.c:149-243 (maps), 558-568 (moments),
 //              708-740 (volume), 745-779 (area), 820-930 (conn), 941-1051 (gcov, gcon,
 //              scale); Romberg integration as utils.c:16-62.
@@ -53,10 +53,51 @@ static double romb(double x0, double x1, double (*f)(double))
   return rvec[15];
 }
 
-// uniform-radius / uniform-theta maps and the integrands of the spherical metric
-static double r_of_x(double x) { return std::fabs(x); }
-static double dr_dx(double) { return 1.0; }
-static double d2r_dx2(double) { return 0.0; }
+// The radial map r(x) of the problem being built (RCOORD, metric_spherical_general.c:
+// 149-219): UNIFORM r = |x|, or SINH r = rtrans sinh(|x|/rtrans).  The integrands below
+// are plain functions handed to romb(), so the map is per-thread state that RadialMap
+// sets for the duration of one public build call (the solve server builds tables in the
+// submitting threads).
+static thread_local int t_rcoord = MDG_RCOORD_UNIFORM;
+static thread_local double t_rtrans = 1.0;
+namespace {
+struct RadialMap {
+  int rc;
+  double rt;
+  explicit RadialMap(const mdg_problem_desc &d) : rc(t_rcoord), rt(t_rtrans)
+  {
+    t_rcoord = d.rcoord;
+    t_rtrans = d.rtrans;
+  }
+  ~RadialMap()
+  {
+    t_rcoord = rc;
+    t_rtrans = rt;
+  }
+};
+}  // namespace
+static double r_of_x(double x)
+{
+  if (t_rcoord == MDG_RCOORD_SINH) return t_rtrans * std::sinh(std::fabs(x) / t_rtrans);
+  return std::fabs(x);
+}
+static double dr_dx(double x)
+{
+  if (t_rcoord == MDG_RCOORD_SINH) return std::cosh(std::fabs(x) / t_rtrans);
+  return 1.0;
+}
+static double d2r_dx2(double x)
+{
+  if (t_rcoord == MDG_RCOORD_SINH) return std::sinh(std::fabs(x) / t_rtrans) / t_rtrans;
+  return 0.0;
+}
+// r(x) of a problem's radial map (ijk_to_x + r_of_x as the dumps use them, io.c:171-174)
+double radial_coordinate(const mdg_problem_desc &d, double x)
+{
+  RadialMap rmap(d);
+  return r_of_x(x);
+}
+// uniform theta (THCOORD=UNIFORM) and the integrands of the spherical metric
 static double th_of_x(double x)
 {
   if (x < -1.0) x = -2.0 - x;
@@ -82,6 +123,7 @@ static double f_cthdth_dx2(double x) { return std::cos(th_of_x(x)) * std::pow(dt
 void build_moments(const mdg_problem_desc &d, int dir, std::vector<double> &al,
                    std::vector<double> &be, std::vector<double> &ga)
 {
+  RadialMap rmap(d);
   const int n = (dir == 0) ? d.n1 : (dir == 1 ? d.n2 : d.n3);
   al.assign(n + 2 * NG, 0.0); be.assign(n + 2 * NG, 0.0); ga.assign(n + 2 * NG, 0.0);
   for (int i = -NG; i < n + NG; i++) {
@@ -123,6 +165,7 @@ void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t 
 // Face and zone geometry of a 1-D problem (GF_NFIELDS x stride, starting at column off).
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off)
 {
+  RadialMap rmap(d);
   const int n1 = d.n1;
   auto put = [&](int f, int i, double v) { tab[f * stride + off + i + NG] = v; };
   for (int i = -NG; i < n1 + NG; i++)
@@ -214,6 +257,7 @@ namespace mdg {
 // memory (al/be/ga hold n+2*NG entries each).
 void build_moments_into(const mdg_problem_desc &d, int dir, double *al, double *be, double *ga)
 {
+  RadialMap rmap(d);
   const int n = (dir == 0) ? d.n1 : (dir == 1 ? d.n2 : d.n3);
   for (int i = -NG; i < n + NG; i++) {
     if (d.geom == MDG_CARTESIAN) {
@@ -326,6 +370,7 @@ static double f_xth2g(double x) { return x * x * std::sin(th_of_x(x)) * dth_dx(x
 // with the reference's operation order (every product and sum as written there).
 void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
 {
+  RadialMap rmap(d);
   const bool three = d.ndim == 3;
   const int n1 = d.n1, n2 = d.n2, n3 = three ? d.n3 : 1;
   h.ndim = three ? 3 : 2;

@@ -96,6 +96,11 @@ int check_desc(const mdg_problem_desc &d)
   if (!lo_ok || !hi_ok) return fail(MDG_ERR_NOTIMPL, "mdg_advance_1d_noalloc: boundary kinds");
   if ((lo == MDG_BC_PERIODIC) != (hi == MDG_BC_PERIODIC))
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: periodic boundaries must be paired");
+  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH)
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: rcoord");
+  if (d.rcoord == MDG_RCOORD_SINH && (!sph || !(d.rtrans > 0.0) || lo == MDG_BC_PROB || hi == MDG_BC_PROB))
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: the SINH radial map needs a spherical grid, rtrans > 0 "
+                                 "and no PROB boundary");
   return MDG_OK;
 }
 

@@ -37,6 +37,9 @@ SPHERICAL_ORIGIN = 5
 PROB_NONE = 0
 PROB_NOH = 1
 
+RCOORD_UNIFORM = 0          # radial maps r(x), metric_spherical_general.c:149-219
+RCOORD_SINH = 1
+
 NG = 2
 NPRIM = 5
 
@@ -64,7 +67,8 @@ class Problem:
     dtmax: float = 1.0e200        # io.c:5037
     dtmin: float = 1.0e-200       # io.c:5038
     tmax: float = 1.0e100
-    rtrans: float = 1.0
+    rcoord: int = RCOORD_UNIFORM  # radial map of a spherical grid (the RCOORD build switch)
+    rtrans: float = 1.0           # its transition radius (RCOORD_SINH)
     hydro_interp_order: int = 3   # io.c:5055
     enforce_floors: int = 0       # ENFORCE_FLOORS build switch (fluid.c:43-46)
     rho_floor: float = -1.0       # io.c:5082 default; problem hooks set their own
@@ -213,9 +217,9 @@ def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240
 
 def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                  p_ratio: float = 100.0, r0: float = 0.5, cfl: float = 0.8,
-                 tmax: float = 1.0e100, floors: bool = True) -> Problem:
-    """1-D spherical problem on r in [0,1] (uniform radius), SPHERICAL_ORIGIN inner
-    boundary (bc.c:776-803).
+                 tmax: float = 1.0e100, floors: bool = True, dr_min: Optional[float] = None) -> Problem:
+    """1-D spherical problem on r in [0,1] (uniform radius; with dr_min the SINH radial
+    map, innermost zones dr_min wide), SPHERICAL_ORIGIN inner boundary (bc.c:776-803).
 
     kind='sod'   : rho, p = rho_ratio, p_ratio inside r<r0; 1, 1 outside; at rest;
                    OUTFLOW outer boundary.
@@ -226,8 +230,8 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                    the hook's floors rho 1e-6, e 1e-7/(gam-1) (init_spherical_noh.c:22-23),
                    enforced (ENFORCE_FLOORS) unless floors=False.
     """
-    dx = 1.0 / n1
-    rc = (np.arange(n1) + 0.5) * dx
+    _, dx, map_ = _radial_grid(n1, dr_min)
+    rc = np.array([_r_of_x((i + 0.5) * dx, map_.get("rtrans")) for i in range(n1)])
     ic = np.zeros((n1, NPRIM))
     bc_hi = OUTFLOW
     prob_kind = PROB_NONE
@@ -244,6 +248,8 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
         ic[:, 0] = 1.0
         ic[:, 1] = np.where(inside, p_amb * p_ratio, p_amb) / (gam - 1.0)
     elif kind == "noh":
+        if map_:
+            raise ValueError("the Noh inflow boundary is built for the uniform radial map")
         ic[:, 0] = 1.0
         ic[:, 1] = 1.0e-6 / (gam - 1.0)
         ic[:, 2] = -1.0   # vr / scale[0][0], scale[0][0] = 1 for a uniform radius
@@ -253,17 +259,61 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
             fl = dict(enforce_floors=1, rho_floor=1.0e-6, e_floor=1.0e-7 / (gam - 1.0))
     else:
         raise ValueError("unknown 1-D spherical problem kind %r" % kind)
-    return Problem(name="sph1d_%s_%d" % (kind, n1), ndim=1, geom=SPHERICAL, n=(n1, 1, 1),
-                   startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
+    return Problem(name="sph1d_%s%s_%d" % ("sinh_" if map_ else "", kind, n1), ndim=1, geom=SPHERICAL,
+                   n=(n1, 1, 1), startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
                    bc_lo=(SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW), bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
-                   prob_kind=prob_kind, cfl=cfl, tmax=tmax, **fl)
+                   prob_kind=prob_kind, cfl=cfl, tmax=tmax, **fl, **map_)
 
 
 MAX_LOG2_ASPECT = 0.5   # utils.c:12
 
 
-def _r_of_x(x: float) -> float:
-    return abs(x)                       # RCOORD=UNIFORM, metric_spherical_general.c:149-153
+def _r_of_x(x: float, rtrans: Optional[float] = None) -> float:
+    """r(x) of the UNIFORM map (rtrans None) or of the SINH map (metric_spherical_general.c:
+    149-160)."""
+    if rtrans is None:
+        return abs(x)
+    return rtrans * math.sinh(abs(x) / rtrans)
+
+
+def sinh_rtrans(n1: int, dx0: float, r_out: float) -> float:
+    """Transition radius of the SINH map whose n1 zones of coordinate width dx0 reach
+    r_out: the root of rtrans sinh(n1 dx0 / rtrans) = r_out, by bracketing and bisection
+    to a relative width of 1e-10 (the method of rtrans_solve, metric_spherical_general.c:
+    16-78, which the reference's problem hooks call, e.g. problems/init_sedov.c:20).  Needs
+    r_out > n1 dx0 (the map only stretches).  The zones then start dx0 wide at the centre
+    and widen geometrically outside r ~ rtrans."""
+    X = n1 * dx0
+    if not r_out > X:
+        raise ValueError("the SINH map needs r_out > n1*dx0")
+    f = lambda rt: rt * math.sinh(X / rt) - r_out if X / rt < 700.0 else math.inf
+    lo = 0.1 * dx0
+    while not math.isfinite(f(lo)):
+        lo *= 1.1
+    hi = 100.0 * r_out
+    flo = f(lo)
+    if flo * f(hi) > 0.0:
+        raise ValueError("rtrans not bracketed")
+    while abs((lo - hi) / hi) > 1.0e-10:
+        mid = 0.5 * (lo + hi)
+        fm = f(mid)
+        if fm * flo <= 0.0:
+            hi = mid
+        else:
+            lo, flo = mid, fm
+    return 0.5 * (lo + hi)
+
+
+def radial_edges(pb: Problem) -> np.ndarray:
+    """r at the n1+1 radial zone edges of a spherical problem (its radial map)."""
+    rt = pb.rtrans if pb.rcoord == RCOORD_SINH else None
+    return np.array([_r_of_x(pb.startx[0] + i * pb.dx[0], rt) for i in range(pb.n[0] + 1)])
+
+
+def radial_centers(pb: Problem) -> np.ndarray:
+    """r at the n1 radial zone centres (ijk_to_x then r_of_x, as the dumps place them)."""
+    rt = pb.rtrans if pb.rcoord == RCOORD_SINH else None
+    return np.array([_r_of_x(pb.startx[0] + (i + 0.5) * pb.dx[0], rt) for i in range(pb.n[0])])
 
 
 def _th_of_x(x: float) -> float:
@@ -274,21 +324,22 @@ def _th_of_x(x: float) -> float:
     return 0.5 * math.pi * (x + 1.0)    # THCOORD=UNIFORM, metric_spherical_general.c:222-230
 
 
-def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: int = 3):
+def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: int = 3,
+                   rtrans: Optional[float] = None):
     """Zone counts of the dendritic spherical grid: nj[i] theta zones of radial row i and
     nk[i][j] phi zones of row (i, j), for the interior rows (the rules of compute_dj and
     compute_dk, utils.c:181-354, for a uniform radius and theta: theta zones double
     outwards from 2 at the centre and phi zones from 4 at each pole while the zone aspect
-    ratio exceeds 2^0.5; on a 2-D grid every row has n3 = 1 phi zone).  Returns (nj, nk) as
-    lists; the interior zones in the reference's zone order are i, then j < nj[i], then
-    k < nk[i][j]."""
+    ratio exceeds 2^0.5; on a 2-D grid every row has n3 = 1 phi zone; rtrans selects the
+    SINH radial map).  Returns (nj, nk) as lists; the interior zones in the reference's
+    zone order are i, then j < nj[i], then k < nk[i][j]."""
     nj = [0] * n1
     nj[0] = 2
     dth = _th_of_x(startx[1] + n2 * dx[1]) - _th_of_x(startx[1])
     for i in range(1, n1):
-        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0])
-        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0])
-        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0])
+        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0], rtrans)
+        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0], rtrans)
+        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0], rtrans)
         ideal = rc * dth / (r1 - r0)
         nj[i] = nj[i - 1]
         if math.log2(ideal / nj[i]) > MAX_LOG2_ASPECT:
@@ -300,9 +351,9 @@ def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: in
     dph = n3 * dx[2]
     nk = []
     for i in range(n1):
-        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0])
-        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0])
-        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0])
+        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0], rtrans)
+        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0], rtrans)
+        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0], rtrans)
         dr = r1 - r0
         row = [0] * nj[i]
         row[0] = 4
@@ -325,10 +376,32 @@ def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: in
     return nj, nk
 
 
+def _radial_grid(n1: int, dr_min: Optional[float]):
+    """(startx, dx0, map fields) of a radial grid on r in [0, 1]: uniform, or the SINH map
+    with innermost zones dr_min wide."""
+    startx = (0.0, -1.0, 0.0)
+    if dr_min is None:
+        return startx, 1.0 / n1, {}
+    return startx, dr_min, dict(rcoord=RCOORD_SINH, rtrans=sinh_rtrans(n1, dr_min, 1.0))
+
+
+def _blast_energy_rows(n1, startx, dx0, map_, r_dep, energy, gam, p_amb) -> np.ndarray:
+    """Internal energy density per radial row of a blast: energy / (4/3 pi r_e^3) in the
+    rows whose centre lies inside r_dep (r_e the outer edge of the last of them), the
+    ambient p_amb / (gam - 1) elsewhere."""
+    rt = map_.get("rtrans")
+    rc = np.array([_r_of_x(startx[0] + (i + 0.5) * dx0, rt) for i in range(n1)])
+    inside = rc < r_dep
+    i_e = (np.nonzero(inside)[0].max() + 1) if inside.any() else 1
+    r_e = _r_of_x(startx[0] + i_e * dx0, rt)
+    u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
+    return np.where(inside, u_dep, p_amb / (gam - 1.0))
+
+
 def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, energy: float = 1.0,
              r_dep: float = 0.02, p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100,
              bc_inner: int = REFLECT, bc_pole: int = REFLECT, noise: float = 0.0,
-             seed: int = 20240603) -> Problem:
+             seed: int = 20240603, dr_min: Optional[float] = None) -> Problem:
     """3-D Sedov blast on the dendritic spherical grid (the structure of
     problems/init_sedov.c:3-164): r in [0, 1] uniform, theta in [0, pi], phi in [0, 2 pi);
     rho = 1, p = p_amb, at rest, and the energy `energy` deposited as a uniform internal
@@ -336,16 +409,16 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
     shells: 4/3 pi r_e^3); reflecting inner and pole boundaries, periodic in phi.  With
     noise > 0 the density is scaled by 1 + noise*(2U-1) and the three coordinate
     velocities are set to 0.1*noise*(2U-1) (U uniform, splitmix64 on `seed`), which breaks
-    the symmetry (shock tagging, rotation through the pole rows, restriction of v^phi)."""
-    startx, dx = (0.0, -1.0, 0.0), (1.0 / n1, 2.0 / n2, 2.0 * math.pi / n3)
-    nj, nk = dendritic_grid(n1, n2, n3, startx, dx)
+    the symmetry (shock tagging, rotation through the pole rows, restriction of v^phi).
+    With dr_min the radius follows the SINH map instead (RCOORD=SINH, the map of the
+    reference's own Sedov hook): the innermost zones are dr_min wide and the zone widths
+    grow geometrically outwards to r = 1."""
+    startx, dx, map_ = _radial_grid(n1, dr_min)
+    dx = (dx, 2.0 / n2, 2.0 * math.pi / n3)
+    nj, nk = dendritic_grid(n1, n2, n3, startx, dx, rtrans=map_.get("rtrans"))
     counts = np.array([sum(row) for row in nk])
     ncell = int(counts.sum())
-    rc = (np.arange(n1) + 0.5) * dx[0]
-    inside = rc < r_dep
-    r_e = (np.nonzero(inside)[0].max() + 1) * dx[0] if inside.any() else dx[0]
-    u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
-    u_row = np.where(inside, u_dep, p_amb / (gam - 1.0))
+    u_row = _blast_energy_rows(n1, startx, dx[0], map_, r_dep, energy, gam, p_amb)
     ic = np.zeros((ncell, NPRIM))
     ic[:, 0] = 1.0
     ic[:, 1] = np.repeat(u_row, counts)
@@ -354,36 +427,35 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
         ic[:, 0] *= 1.0 + noise * (2.0 * u[:, 0] - 1.0)
         for v in range(3):
             ic[:, 2 + v] = 0.1 * noise * (2.0 * u[:, 1 + v] - 1.0)
-    return Problem(name="sedov3d_%dx%dx%d" % (n1, n2, n3), ndim=3, geom=SPHERICAL, n=(n1, n2, n3),
-                   startx=startx, dx=dx, gam=gam, ic=ic,
+    return Problem(name="sedov3d_%s%dx%dx%d" % ("sinh_" if map_ else "", n1, n2, n3), ndim=3, geom=SPHERICAL,
+                   n=(n1, n2, n3), startx=startx, dx=dx, gam=gam, ic=ic,
                    bc_lo=(bc_inner, bc_pole, PERIODIC), bc_hi=(OUTFLOW, bc_pole, PERIODIC),
-                   cfl=cfl, tmax=tmax, cells=ncell)
+                   cfl=cfl, tmax=tmax, cells=ncell, **map_)
 
 
 def sedov_2d_spherical(n1: int = 256, n2: int = 128, gam: float = 1.4, energy: float = 1.0, r_dep: float = 0.02,
                        p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100, bc_inner: int = REFLECT,
-                       bc_pole: int = REFLECT, noise: float = 0.0, seed: int = 20240604) -> Problem:
+                       bc_pole: int = REFLECT, noise: float = 0.0, seed: int = 20240604,
+                       dr_min: Optional[float] = None) -> Problem:
     """Axisymmetric (r, theta) Sedov blast on the 2-D dendritic spherical grid: theta zones
     double outwards from 2 at the centre (compute_dj, utils.c:181-238); otherwise as
-    sedov_3d (energy in the zones inside r_dep, seeded noise in density and velocities)."""
-    startx, dx = (0.0, -1.0, 0.0), (1.0 / n1, 2.0 / n2, 2.0 * math.pi)
-    nj, _ = dendritic_grid(n1, n2, 1, startx, dx, ndim=2)
+    sedov_3d (energy in the zones inside r_dep, seeded noise in density and velocities,
+    the SINH radial map with dr_min)."""
+    startx, dx, map_ = _radial_grid(n1, dr_min)
+    dx = (dx, 2.0 / n2, 2.0 * math.pi)
+    nj, _ = dendritic_grid(n1, n2, 1, startx, dx, ndim=2, rtrans=map_.get("rtrans"))
     ncell = int(sum(nj))
-    rc = (np.arange(n1) + 0.5) * dx[0]
-    inside = rc < r_dep
-    r_e = (np.nonzero(inside)[0].max() + 1) * dx[0] if inside.any() else dx[0]
-    u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
     ic = np.zeros((ncell, NPRIM))
     ic[:, 0] = 1.0
-    ic[:, 1] = np.repeat(np.where(inside, u_dep, p_amb / (gam - 1.0)), nj)
+    ic[:, 1] = np.repeat(_blast_energy_rows(n1, startx, dx[0], map_, r_dep, energy, gam, p_amb), nj)
     if noise > 0.0:
         u = uniform01(seed, 4 * ncell).reshape(ncell, 4)
         ic[:, 0] *= 1.0 + noise * (2.0 * u[:, 0] - 1.0)
         for v in range(3):
             ic[:, 2 + v] = 0.1 * noise * (2.0 * u[:, 1 + v] - 1.0)
-    return Problem(name="sedov2dsph_%dx%d" % (n1, n2), ndim=2, geom=SPHERICAL, n=(n1, n2, 1), startx=startx,
-                   dx=dx, gam=gam, ic=ic, bc_lo=(bc_inner, bc_pole, PERIODIC), bc_hi=(OUTFLOW, bc_pole, PERIODIC),
-                   cfl=cfl, tmax=tmax, cells=ncell)
+    return Problem(name="sedov2dsph_%s%dx%d" % ("sinh_" if map_ else "", n1, n2), ndim=2, geom=SPHERICAL,
+                   n=(n1, n2, 1), startx=startx, dx=dx, gam=gam, ic=ic, bc_lo=(bc_inner, bc_pole, PERIODIC),
+                   bc_hi=(OUTFLOW, bc_pole, PERIODIC), cfl=cfl, tmax=tmax, cells=ncell, **map_)
 
 
 def ensemble_1d(count: int = 2048, seed: int = 7, nmin: int = 128, nmax: int = 8192,

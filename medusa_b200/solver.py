@@ -81,7 +81,7 @@ class ProblemDesc(ctypes.Structure):
                 ("dtmax", ctypes.c_double), ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
                 ("hydro_interp_order", ctypes.c_int),
                 ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double), ("e_floor", ctypes.c_double),
-                ("grav", ctypes.c_double * 3)]
+                ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int), ("rtrans", ctypes.c_double)]
 
 
 def desc_of(pb: "_pb.Problem") -> ProblemDesc:
@@ -100,6 +100,7 @@ def desc_of(pb: "_pb.Problem") -> ProblemDesc:
     d.enforce_floors, d.rho_floor, d.e_floor = int(pb.enforce_floors), pb.rho_floor, pb.e_floor
     for k in range(3):
         d.grav[k] = pb.grav[k]
+    d.rcoord, d.rtrans = pb.rcoord, pb.rtrans
     return d
 
 

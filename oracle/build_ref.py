@@ -76,6 +76,13 @@ CONFIGS = {
     # 2-D (r, theta) spherical on the dendritic grid
     "sph2d": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
                   RCOORD="UNIFORM", THCOORD="UNIFORM"),
+    # the spherical grids with the SINH radial map (r = rtrans sinh(x/rtrans))
+    "sph1d_sinh": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                       RCOORD="SINH", THCOORD="UNIFORM"),
+    "sph2d_sinh": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                       RCOORD="SINH", THCOORD="UNIFORM"),
+    "sph3d_sinh": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                       RCOORD="SINH", THCOORD="UNIFORM"),
 }
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]

@@ -92,6 +92,7 @@ typedef struct {
   int enforce_floors;
   double rho_floor, e_floor;
   double grav[3];
+  int rcoord;          /* radial map: 0 UNIFORM, 1 SINH (the RCOORD build switch) */
 } orc_params;
 
 typedef struct {
@@ -155,10 +156,26 @@ static double romb(double x0, double x1, double (*f)(double))
   return rvec[15];
 }
 
-/* metric_spherical_general.c integrands for RCOORD=UNIFORM, THCOORD=UNIFORM */
-static double r_of_x(double x) { return fabs(x); }
-static double dr_dx(double x) { (void)x; return 1.0; }
-static double d2r_dx2(double x) { (void)x; return 0.0; }
+/* metric_spherical_general.c maps (149-219) and integrands, RCOORD=UNIFORM or SINH,
+ * THCOORD=UNIFORM; the map of the problem being built (the integrands are plain
+ * functions handed to romb) */
+static int g_rcoord = 0;
+static double g_rtrans = 1.0;
+static double r_of_x(double x)
+{
+  if (g_rcoord == 1) return g_rtrans*sinh(fabs(x)/g_rtrans);
+  return fabs(x);
+}
+static double dr_dx(double x)
+{
+  if (g_rcoord == 1) return cosh(fabs(x)/g_rtrans);
+  return 1.0;
+}
+static double d2r_dx2(double x)
+{
+  if (g_rcoord == 1) return sinh(fabs(x)/g_rtrans)/g_rtrans;
+  return 0.0;
+}
 static double th_of_x(double x)
 {
   if (x < -1.0) x = -2.0 - x;
@@ -179,6 +196,13 @@ static double f_sthdth_dx3(double x) { return sin(th_of_x(x))*pow(dth_dx(x),3); 
 static double f_sth3dth_dx(double x) { return pow(sin(th_of_x(x)),3)*dth_dx(x); }
 static double f_sthd2th_dx2(double x) { return sin(th_of_x(x))*d2th_dx2(x); }
 static double f_cthdth_dx2(double x) { return cos(th_of_x(x))*pow(dth_dx(x),2); }
+
+/* make o's radial map the one the maps above evaluate */
+static void use_map(const orc_t *o)
+{
+  g_rcoord = o->prm.rcoord;
+  g_rtrans = o->prm.rtrans;
+}
 
 static void init_geometry(orc_t *o)
 {
@@ -856,6 +880,7 @@ static void set_shock_flag0(orc_t *o)
 /* step.c:28-129 */
 void orc_step(orc_t *o, double dtin)
 {
+  use_map(o);
   o->dt = dtin;
   o->min_dt = 1.0e100;
   set_shock_flag0(o);
@@ -878,6 +903,7 @@ void orc_step(orc_t *o, double dtin)
 /* step.c:163-203 */
 double orc_estimate_dt(orc_t *o)
 {
+  use_map(o);
   const orc_params *P = &o->prm;
   if (o->est_first) { o->min_dt = 1.0e100; o->est_first = 0; }
   for (int i=0; i<o->n1; i++) {
@@ -947,6 +973,7 @@ orc_t *orc_create(const orc_params *prm, int ndim, int geom, const double *ic)
   o->grav_on = (prm->grav[0] != 0.0 || prm->grav[1] != 0.0 || prm->grav[2] != 0.0);
   o->est_first = 1;
   o->dtold = 1.0e100;
+  use_map(o);
   init_geometry(o);
   int cidx = 0;
   for (int i=0; i<o->n1; i++) for (int j=0; j<o->n2; j++) {

@@ -40,7 +40,7 @@ class Params(ctypes.Structure):
                 ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
                 ("rtrans", ctypes.c_double), ("hydro_interp_order", ctypes.c_int),
                 ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double),
-                ("e_floor", ctypes.c_double), ("grav", ctypes.c_double * 3)]
+                ("e_floor", ctypes.c_double), ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int)]
 
 
 def params_of(pb) -> Params:
@@ -62,6 +62,7 @@ def params_of(pb) -> Params:
     p.e_floor = getattr(pb, "e_floor", -1.0)
     for d in range(3):
         p.grav[d] = getattr(pb, "grav", (0.0, 0.0, 0.0))[d]
+    p.rcoord = int(getattr(pb, "rcoord", 0))
     return p
 
 
@@ -161,9 +162,11 @@ class Oracle:
 
 # ----------------------------------------------------------------------------- reference
 def ref_config(pb) -> str:
-    """The oracle/_ref build of a problem: its geometry and dimension, and whether the
-    ENFORCE_FLOORS switch is compiled in."""
+    """The oracle/_ref build of a problem: its geometry and dimension, its radial map,
+    and whether the FIXED_GRAV and ENFORCE_FLOORS switches are compiled in."""
     name = ("cart%dd" if pb.geom == 0 else "sph%dd") % pb.ndim
+    if getattr(pb, "rcoord", 0) == 1:
+        name += "_sinh"
     if any(g != 0.0 for g in getattr(pb, "grav", (0.0, 0.0, 0.0))):
         name += "_grav"
     return name + ("_floors" if getattr(pb, "enforce_floors", 0) else "")

@@ -45,6 +45,7 @@ typedef struct {
   int enforce_floors;  /* must match the ENFORCE_FLOORS of the build */
   double rho_floor, e_floor;
   double grav[3];     /* fixed gravitational acceleration g0 (GRAV=FIXED_GRAV builds) */
+  int rcoord;         /* radial map; must match the RCOORD of the build (rtrans above) */
 } ref_params;
 
 static ref_params g_prm;
@@ -154,6 +155,11 @@ REF_API int ref_init(const ref_params *prm, const double *ic)
 {
   g_prm = *prm;
   g_ic = ic;
+#if (RCOORD == SINH)
+  if (prm->rcoord != 1) { fprintf(stderr, "ref_init: this build has the SINH radial map\n"); return -1; }
+#else
+  if (prm->rcoord != 0) { fprintf(stderr, "ref_init: this build has the uniform radial map\n"); return -1; }
+#endif
 
   /* parse_input defaults, io.c:5000-5117, then the keys this build sets */
   rx_info.facta = 10*1e5;

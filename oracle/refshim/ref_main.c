@@ -40,6 +40,7 @@ typedef struct {
   int enforce_floors;
   double rho_floor, e_floor;
   double grav[3];
+  int rcoord;
 } ref_params;
 
 int ref_init(const ref_params *prm, const double *ic);
@@ -82,7 +83,7 @@ int main(int argc, char **argv)
   memcpy(&prm, buf, sizeof prm);
   const double *ic = (const double *)(buf + sizeof prm);
 
-  ref_init(&prm, ic);
+  if (ref_init(&prm, ic) < 0) return 2;
   int ncell = ref_cell_count();
   double *prim = malloc(sizeof(double)*5*ncell);
   double *eos = malloc(sizeof(double)*5*ncell);

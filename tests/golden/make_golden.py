@@ -37,6 +37,8 @@ def cases():
         "blast2d_40x48_reflect": (P.blast_2d(40, 48, bc=P.REFLECT), 40),
         "blast2d_44x36_outflow": (P.blast_2d(44, 36, bc=P.OUTFLOW), 40),
         "rt2d_32x64_grav": (P.rayleigh_taylor_2d(32, 64, g=-0.5, noise=0.05), 40),
+        # the SINH radial map (zones 2e-3 wide at the centre, widening outwards)
+        "sph1d_sinh_sedov_192": (P.spherical_1d("sedov", 192, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3), 100),
     }
 
 
@@ -54,6 +56,9 @@ def cases3d():
         "sedov2dsph_noisy_origin_32x16": (P.sedov_2d_spherical(32, 16, r_dep=0.25, noise=0.05,
                                                                bc_inner=P.SPHERICAL_ORIGIN,
                                                                bc_pole=P.SPHERICAL_ORIGIN), 40),
+        # the SINH radial map on both dendritic grids
+        "sedov3d_sinh_24x16x32": (P.sedov_3d(24, 16, 32, r_dep=0.2, dr_min=0.02), 30),
+        "sedov2dsph_sinh_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.15, noise=0.05, dr_min=0.01), 40),
     }
 
 

@@ -151,3 +151,17 @@ def test_2d_spherical_scope_checked_before_device_work(mutate, nprob, code):
     assert S.library().mdg_create(arr, nprob, 0, 0, ctypes.byref(h)) == code
     assert not h.value
     assert S.library().mdg_last_error_message()
+
+
+@pytest.mark.parametrize("pb,precision,code", [
+    (P.sod(64).copy(rcoord=P.RCOORD_SINH, rtrans=0.2), 0, 1),                        # Cartesian
+    (P.spherical_1d("sedov", 64, 1.4, dr_min=0.01).copy(rtrans=-1.0), 0, 1),         # rtrans <= 0
+    (P.spherical_1d("sedov", 64, 1.4).copy(rcoord=7), 0, 1),                          # unknown map
+    (P.spherical_1d("sedov", 64, 1.4, dr_min=0.01), 1, 5),                            # 1-D mixed: closed form
+    (P.spherical_1d("noh", 64, 1.4).copy(rcoord=P.RCOORD_SINH, rtrans=0.2), 0, 5),    # Noh inflow boundary
+])
+def test_radial_map_scope_checked_before_device_work(pb, precision, code):
+    arr = (S.ProblemDesc * 1)(S.desc_of(pb))
+    h = ctypes.c_void_p()
+    assert S.library().mdg_create(arr, 1, precision, 0, ctypes.byref(h)) == code
+    assert not h.value

@@ -27,6 +27,19 @@ def test_zone_counts_match_restatement(dims):
     assert n == pb.ncell == sum(sum(r) for r in pk)
 
 
+@pytest.mark.parametrize("dims,dr_min", [((24, 16, 32), 0.02), ((384, 128, 256), 1.0e-3)])
+def test_sinh_zone_counts_match_restatement_and_reference(dims, dr_min):
+    pb = P.sedov_3d(*dims, r_dep=0.2, dr_min=dr_min)
+    nj, nk, n = S.grid3d_counts(pb)
+    pj, pk = P.dendritic_grid(*dims, pb.startx, pb.dx, rtrans=pb.rtrans)
+    assert list(nj) == pj and list(nk) == [x for row in pk for x in row] and n == pb.ncell
+    if dims[0] <= 64 and pyoracle.ref_available(pb):
+        rnj, rnk = pyoracle.reference_grid(pb)
+        assert list(nj) == rnj[2:-2]
+    edges = P.radial_edges(pb)
+    assert abs(edges[-1] - 1.0) <= 1.0e-9 and abs(edges[1] - dr_min) <= 1.0e-2 * dr_min
+
+
 def test_c3_grid_size():
     """The measured 3-D workload: 384 x 128 x 256 before coarsening."""
     pb = P.sedov_3d(384, 128, 256)
@@ -35,9 +48,11 @@ def test_c3_grid_size():
     assert n == pb.ncell < 384 * 128 * 256
 
 
-@pytest.mark.parametrize("dims", [(24, 16, 32), (40, 32, 64), (48, 64, 128)])
-def test_geometry_bit_identical_to_reference(dims):
-    pb = P.sedov_3d(*dims, r_dep=0.2)
+@pytest.mark.parametrize("dims,dr_min", [((24, 16, 32), None), ((40, 32, 64), None), ((48, 64, 128), None),
+                                         ((24, 16, 32), 0.02), ((48, 32, 64), 0.01)])
+def test_geometry_bit_identical_to_reference(dims, dr_min):
+    """Uniform radius and the SINH radial map (against the reference's RCOORD=SINH build)."""
+    pb = P.sedov_3d(*dims, r_dep=0.2, dr_min=dr_min)
     if not pyoracle.ref_available(pb):
         pytest.skip("oracle/_ref not built (needs the reference tree)")
     rnj, _ = pyoracle.reference_grid(pb)
@@ -70,9 +85,9 @@ def test_2d_zone_counts_match_restatement(dims):
 
 
 # the NDIM=2 record of ref_get_geom: vol, area[2], gcov[3][3], gcon[3], scale[3][3], conn[27]
-@pytest.mark.parametrize("dims", [(24, 16), (48, 32), (40, 64)])
-def test_2d_geometry_bit_identical_to_reference(dims):
-    pb = P.sedov_2d_spherical(*dims, r_dep=0.2)
+@pytest.mark.parametrize("dims,dr_min", [((24, 16), None), ((48, 32), None), ((40, 64), None), ((40, 32), 0.01)])
+def test_2d_geometry_bit_identical_to_reference(dims, dr_min):
+    pb = P.sedov_2d_spherical(*dims, r_dep=0.2, dr_min=dr_min)
     if not pyoracle.ref_available(pb):
         pytest.skip("oracle/_ref not built (needs the reference tree)")
     rnj, _ = pyoracle.reference_grid(pb)
