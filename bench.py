@@ -312,9 +312,9 @@ def run_reference_arm(args, ctx):
     if ctx.rank != 0:
         return
     if args.workload == "sedov3d":
-        cb = cpu_baseline_sedov3d(steps=max(1, min(args.steps, 2)))
-        config = {"workload": "sedov_3d_dendritic_spherical_%dx%dx%d_fp64" % SEDOV3D, "global_batch": 1,
-                  "seq_len": P.sedov_3d(*SEDOV3D).ncell, "parallelism": "replicas",
+        cb = cpu_baseline_sedov3d(steps=max(1, min(args.steps, 2)), radius=args.sedov3d_radius)
+        config = {"workload": sedov3d_workload_name(SEDOV3D, args.sedov3d_radius), "global_batch": 1,
+                  "seq_len": sedov3d_problem(SEDOV3D, args.sedov3d_radius).ncell, "parallelism": "replicas",
                   "l2": "inputs larger than L2"}
         dtype = "f64"
     elif args.workload == "kh2048":
@@ -588,21 +588,36 @@ def run_kh(args, ctx):
 
 SEDOV3D = (384, 128, 256)
 SEDOV3D_SAMPLE = (96, 64, 128)
+SEDOV3D_DR_MIN = 1.0e-3     # innermost zone width of the SINH radial map; r spans [0, 1]
 
 
-def cpu_baseline_sedov3d(steps=2):
-    """Reference CPU build (its Makefile flags), one core, `steps` RK2 steps of the same
-    Sedov blast on a smaller dendritic grid (96 x 64 x 128 before coarsening): the full
-    grid needs several GB of host memory for the reference's per-zone geometry records."""
+def sedov3d_problem(dims, radius="sinh"):
+    """The 3-D Sedov workload: E = 1 deposited inside r < 0.02, on the SINH radial map
+    (zones SEDOV3D_DR_MIN x 384/n1 wide at the centre, log-like spacing outside rtrans)
+    or the uniform radius."""
     from medusa_b200 import problems as P
+    if radius == "uniform":
+        return P.sedov_3d(*dims)
+    return P.sedov_3d(*dims, r_dep=0.02, dr_min=SEDOV3D_DR_MIN * SEDOV3D[0] / dims[0])
+
+
+def sedov3d_workload_name(dims, radius="sinh"):
+    return "sedov_3d_dendritic_spherical_%s%dx%dx%d_fp64" % ("sinh_r_" if radius == "sinh" else "", *dims)
+
+
+def cpu_baseline_sedov3d(steps=2, radius="sinh"):
+    """Reference CPU build (its Makefile flags), one core, `steps` RK2 steps of the same
+    Sedov blast on a smaller dendritic grid (96 x 64 x 128 before coarsening, the same
+    radial map scaled to 96 zones): the full grid needs several GB of host memory for the
+    reference's per-zone geometry records."""
     from oracle import pyoracle
-    pb = P.sedov_3d(*SEDOV3D_SAMPLE, r_dep=0.05)
+    pb = sedov3d_problem(SEDOV3D_SAMPLE, radius)
     if pyoracle.ref_available(pb, fast=True):
         r = pyoracle.time_reference(pb, 1, steps, fast=True)
         return {"value": r["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1, "kind": "reference",
-                "sample": "%d RK2 steps of the Sedov blast on the %dx%dx%d dendritic grid (%d zones), reference "
-                          "build with its own flags (-O3 -ffast-math), 1 core, %.1f s"
-                          % (steps, *SEDOV3D_SAMPLE, pb.ncell, r["seconds"])}
+                "sample": "%d RK2 steps of the Sedov blast on the %dx%dx%d dendritic grid (%d zones, %s radius), "
+                          "reference build with its own flags (-O3 -ffast-math), 1 core, %.1f s"
+                          % (steps, *SEDOV3D_SAMPLE, pb.ncell, radius, r["seconds"])}
     return {"value": None, "unit": "zone-updates/s", "cores": 1, "kind": "reference",
             "sample": "unavailable: the 3-D reference build is absent"}
 
@@ -614,7 +629,7 @@ def run_sedov3d(args, ctx):
 
     K, W = args.steps, args.warmup
     dims = tuple(int(x) for x in args.sedov3d_dims.split(",")) if args.sedov3d_dims else SEDOV3D
-    pb = P.sedov_3d(*dims)
+    pb = sedov3d_problem(dims, args.sedov3d_radius)
     ncell = pb.ncell
     s = medusa_b200.Solver(pb, device=ctx.local)
     s.step(W)
@@ -648,27 +663,32 @@ def run_sedov3d(args, ctx):
         mix = sa.update_cpu(0)
         m1, e1 = sa.conserved_totals()
     vol = grid3d_zone_volumes(pb)
-    r_of = lambda prim: (int(np.argmax(grid3d_radial_mean(pb, prim[:, 0]))) + 0.5) * pb.dx[0]
+    rc = P.radial_centers(pb)
+    r_of = lambda prim: float(rc[int(np.argmax(grid3d_radial_mean(pb, prim[:, 0])))])
     accuracy = {"steps": nacc, "t": t_end, "l1_rho": A.l1_rel(mix[:, 0], ref[:, 0], vol),
                 "l1_u": A.l1_rel(mix[:, 1], ref[:, 1], vol),
                 "mass_drift_vs_fp64": abs(m1[0] - m0[0]) / m0[0], "energy_drift_vs_fp64": abs(e1[0] - e0[0]) / e0[0],
                 "shock_radius_fp64": r_of(ref), "shock_radius_mixed": r_of(mix),
-                "shock_radius_sedov": A.sedov_shock_radius(1.0, t_end, 1.0, pb.gam), "dr": pb.dx[0]}
+                "shock_radius_sedov": A.sedov_shock_radius(1.0, t_end, 1.0, pb.gam),
+                "dr_at_shock": float(np.interp(r_of(ref), rc, np.diff(P.radial_edges(pb))))}
     if ctx.rank != 0:
         return
     peak, peak_kind = read_peaks()
     b_stage1 = 360.0
     achieved = b_stage1 * ncell / (st["stage1"] / 1e3) / 1e9
-    traffic = read_profile_value("sweep3d_sedov_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
+    traffic = read_profile_value("sweep3d_sedov_sinh_ncu.md" if args.sedov3d_radius == "sinh" else
+                                 "sweep3d_sedov_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
     line = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
         "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms / K,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "sedov_3d_dendritic_spherical_%dx%dx%d_fp64" % dims, "global_batch": ctx.world,
+        "config": {"workload": sedov3d_workload_name(dims, args.sedov3d_radius), "global_batch": ctx.world,
                    "seq_len": ncell, "parallelism": "replicas" if ctx.world > 1 else "single",
                    "precision": "plain FP64 (reference operation order)",
-                   "grid": "uniform radius (the reference's metrics have no logarithmic radial map)",
+                   "grid": ("SINH radial map (RCOORD=SINH, rtrans %.4f): zones %.1e wide at the centre, %.1e at "
+                            "r = 1" % (pb.rtrans, P.radial_edges(pb)[1], 1.0 - P.radial_edges(pb)[-2])
+                            if args.sedov3d_radius == "sinh" else "uniform radius"),
                    "l2": "inputs larger than L2 (state 2 x %.0f MB)" % (ncell * 40 / 1e6)},
         "gpu_launches": 10 * K,
         "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / K,
@@ -687,7 +707,7 @@ def run_sedov3d(args, ctx):
                   "accuracy_vs_fp64": accuracy},
     }
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sedov3d()
+        line["cpu_baseline"] = cpu_baseline_sedov3d(radius=args.sedov3d_radius)
     print(json.dumps(line), flush=True)
 
 
@@ -788,6 +808,9 @@ def main():
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
     ap.add_argument("--sedov3d-dims", default="",
                     help="sedov3d: n1,n2,n3 of the grid (default 384,128,256; smaller grids for profiling)")
+    ap.add_argument("--sedov3d-radius", default="sinh", choices=["sinh", "uniform"],
+                    help="sedov3d: radial map; sinh = zones 1e-3 wide at the centre widening geometrically "
+                         "to r = 1 (RCOORD=SINH), uniform = 1/n1 wide")
     ap.add_argument("--sedov3d-accuracy-steps", type=int, default=60,
                     help="sedov3d: steps of the FP64 run the mixed run is compared with at equal time")
     ap.add_argument("--server-frac-2d", type=float, default=0.0,
