@@ -55,6 +55,7 @@ extern "C" {
 /* PROB boundary hooks restated on the device (the reference's prob_bounds callbacks) */
 #define MDG_PROB_NONE 0
 #define MDG_PROB_NOH 1   /* problems/init_spherical_noh.c:63-79 */
+#define MDG_PROB_DUST 2  /* problems/init_dustcollapse.c:77-113: outflow, v^r = -1/sqrt(r) in the ghost zones */
 /* radial coordinate maps r(x) of spherical grids (RCOORD, metric_spherical_general.c:149-219) */
 #define MDG_RCOORD_UNIFORM 0   /* r = |x| */
 #define MDG_RCOORD_SINH 1      /* r = rtrans sinh(|x| / rtrans): zones of width dx near the
@@ -95,6 +96,9 @@ typedef struct mdg_problem_desc {
   int rcoord;               /* MDG_RCOORD_* radial map of a spherical grid (the RCOORD build switch) */
   double rtrans;            /* transition radius of the SINH map (rx_info.rtrans; problem hooks
                                set it with rtrans_solve, e.g. problems/init_sedov.c:20) */
+  int monopole;             /* 1: self-gravity in the monopole approximation, the
+                               GRAV=SPHERICAL_MONOPOLE_GRAV build with GR_MONOPOLE=FALSE
+                               (gravity.c:145-425); spherical grids, grav[] all zero */
 } mdg_problem_desc;
 
 typedef struct mdg_solver mdg_solver;   /* opaque */

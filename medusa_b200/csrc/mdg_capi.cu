@@ -14,6 +14,7 @@ namespace mdg {
 void build_recon_table(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
 double radial_coordinate(const mdg_problem_desc &d, double x);
+void dust_ghost_u1(const mdg_problem_desc &d, double *u1);
 void cartesian_2d_constants(const mdg_problem_desc &d, double &vol, double &area0, double &area1);
 void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t stride, int64_t off);
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
@@ -61,6 +62,8 @@ struct mdg_solver {
   int *d_err = nullptr;
   // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
   float *d_mx = nullptr, *d_mx1 = nullptr;   // FP32 weights (mixed): 1-D or 2-D direction 0; 2-D direction 1
+  double *d_gmono = nullptr;      // monopole gravity at the zone centroids of the 1-D problems
+  bool any_mono = false;          // a 1-D problem has monopole gravity
   WorkQueue *d_queue = nullptr;
   Tile *d_mtiles = nullptr;
   int mtiles_cap = 0, nmtiles = 0;
@@ -105,10 +108,17 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   if (d.ndim != 1 && d.ndim != 2 && d.ndim != 3) return bad("ndim must be 1, 2 or 3");
   if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
   if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH) return bad("unknown radial map (rcoord)");
+  if (d.monopole != 0 && d.monopole != 1) return bad("monopole must be 0 or 1");
+  if (d.monopole) {
+    if (d.geom != MDG_SPHERICAL) return bad("monopole gravity needs a spherical grid");
+    if (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0)
+      return bad("monopole and fixed gravity are exclusive (one GRAV switch)");
+  }
+  if (d.prob_kind < MDG_PROB_NONE || d.prob_kind > MDG_PROB_DUST) return bad("unknown prob_kind");
   if (d.rcoord == MDG_RCOORD_SINH) {
     if (d.geom != MDG_SPHERICAL) return bad("radial maps apply to spherical grids");
     if (!(d.rtrans > 0.0) || !(d.rtrans < 1.0e300)) return bad("rtrans must be positive and finite");
-    if (d.bc_lo[0] == MDG_BC_PROB || d.bc_hi[0] == MDG_BC_PROB) {
+    if ((d.bc_lo[0] == MDG_BC_PROB || d.bc_hi[0] == MDG_BC_PROB) && d.prob_kind == MDG_PROB_NOH) {
       why = "the Noh inflow boundary is built for the uniform radial map";
       return MDG_ERR_NOTIMPL;
     }
@@ -166,7 +176,8 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
                  (lo == MDG_BC_PROB && d.geom == MDG_SPHERICAL && d.prob_kind == MDG_PROB_NOH) ||
                  (lo == MDG_BC_SPHERICAL_ORIGIN && d.geom == MDG_SPHERICAL);
     bool hi_ok = hi == MDG_BC_OUTFLOW || hi == MDG_BC_REFLECT || hi == MDG_BC_EXTRAP || hi == MDG_BC_PERIODIC ||
-                 (hi == MDG_BC_PROB && d.geom == MDG_SPHERICAL && d.prob_kind == MDG_PROB_NOH);
+                 (hi == MDG_BC_PROB && d.geom == MDG_SPHERICAL &&
+                  (d.prob_kind == MDG_PROB_NOH || d.prob_kind == MDG_PROB_DUST));
     if (!lo_ok || !hi_ok) {
       snprintf(buf, sizeof buf, "unsupported 1-D boundary kinds lo=%d hi=%d for geom=%d", lo, hi, d.geom);
       why = buf;
@@ -249,7 +260,9 @@ void mdg::make_probdev(const mdg_problem_desc &d, ProbDev &P)
   P.grav[0] = d.grav[0]; P.grav[1] = d.grav[1]; P.grav[2] = d.grav[2];
   P.grav_on = (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0);
   P.x0 = d.startx[0];
+  P.mono = d.monopole;
   if (d.ndim == 1 && d.geom == MDG_SPHERICAL) spherical_1d_constants(P.gk_area, P.gk_th1, P.gk_th2, P.gk_tc);
+  if (d.ndim == 1 && d.prob_kind == MDG_PROB_DUST) dust_ghost_u1(d, P.u1_hi);
 }
 
 static void free_all(mdg_solver *s)
@@ -262,6 +275,7 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_rc0); cudaFree(s->d_rc1); cudaFree(s->d_geo);
   cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
   cudaFree(s->d_mx); cudaFree(s->d_mx1); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
+  cudaFree(s->d_gmono);
   sweep3_destroy(s->s3);
   s->s3 = nullptr;
   if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
@@ -419,6 +433,9 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (precision == MDG_PREC_MIXED && descs[m].geom == MDG_SPHERICAL && !(descs[m].startx[0] >= 0.0))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
+    if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].monopole)
+      return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
+                                       ": the 1-D mixed-precision sweep has no monopole gravity");
     if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].rcoord != MDG_RCOORD_UNIFORM)
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the 1-D mixed-precision sweep computes the uniform-radius geometry in closed form");
@@ -446,10 +463,12 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     ProbDev P;
     make_probdev(d, P);
     P.cell_off = cell;
+    P.mono_off = cell;
     P.geo_off = rc0;
     P.rc1_off = rc1;
     P.sh_off = sh;
     s->hprobs.push_back(P);
+    if (d.monopole) s->any_mono = true;
     const int64_t nc = (int64_t)P.n1 * P.n2;
     if (nc > s->max_cells) s->max_cells = nc;
     cell += nc;
@@ -511,6 +530,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   if (ndim == 2) CKC(cudaMalloc(&s->d_rc1, sizeof(double) * h_rc1.size()));
   else CKC(cudaMalloc(&s->d_geo, sizeof(double) * n_geo));
   CKC(cudaMalloc(&s->d_state, sizeof(double) * nstate * NPRIM * cell));
+  if (s->any_mono) CKC(cudaMalloc(&s->d_gmono, sizeof(double) * cell));
   CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
   CKC(cudaMalloc(&s->d_err, sizeof(int)));
   CKC(cudaMalloc(&s->d_totals, sizeof(double) * 2 * nprob));
@@ -558,6 +578,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   s->tb.geo = s->d_geo; s->tb.geo_stride = rc0;
   s->tb.mx = s->d_mx;
   s->tb.mx1 = s->d_mx1;
+  s->tb.gmono = s->d_gmono;
 #undef CKC
   if (precision == MDG_PREC_MIXED && ndim == 1) {
     int rc = build_mixed_tiles(s, s->cfg.threads);
@@ -637,8 +658,10 @@ static int queue_steps(mdg_solver *s, int nsteps)
                            s->tb, s->P, s->P, s->PH, s->stream);
     else if (s->ndim == 3)
       launch_stage3d(0, mix3, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
-    else if (s->ndim == 1)
+    else if (s->ndim == 1) {
+      if (s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->P, s->stream);
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
+    }
     else
       launch_stage2d(0, mix2, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
                      s->P, s->P, s->ACC, s->PH, s->d_shock0, s->d_shock1, s->stream);
@@ -649,8 +672,10 @@ static int queue_steps(mdg_solver *s, int nsteps)
                            s->tb, s->PH, s->P, s->P, s->stream);
     else if (s->ndim == 3)
       launch_stage3d(1, mix3, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
-    else if (s->ndim == 1)
+    else if (s->ndim == 1) {
+      if (s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->PH, s->stream);
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
+    }
     else
       launch_stage2d(1, mix2, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
                      s->PH, s->P, s->ACC, s->P, s->d_shock0, s->d_shock1, s->stream);

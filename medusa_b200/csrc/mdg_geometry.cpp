@@ -91,6 +91,28 @@ static double d2r_dx2(double x)
   if (t_rcoord == MDG_RCOORD_SINH) return std::sinh(std::fabs(x) / t_rtrans) / t_rtrans;
   return 0.0;
 }
+// v^1 of the two outer ghost zones under the dust-collapse boundary hook
+// (problems/init_dustcollapse.c:104-113): r at the zone centroid beta0/Gamma0,
+// v^r = -1/sqrt(r), divided by the zone's scale[0][0].
+void build_moments(const mdg_problem_desc &d, int dir, std::vector<double> &al, std::vector<double> &be,
+                   std::vector<double> &ga);
+void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
+void dust_ghost_u1(const mdg_problem_desc &d, double *u1)
+{
+  RadialMap rmap(d);
+  std::vector<double> al, be, ga;
+  build_moments(d, 0, al, be, ga);
+  const int64_t w = d.n1 + 2 * NG;
+  std::vector<double> geo((size_t)GF_NFIELDS * w, 0.0);
+  build_geo_1d(d, geo.data(), w, 0);
+  for (int q = 0; q < 2; q++) {
+    const int i = d.n1 + q;
+    const double r = r_of_x(be[i + NG] / ga[i + NG]);
+    const double vr = -1.0 / std::sqrt(r);
+    u1[q] = vr / geo[(size_t)GF_S00 * w + i + NG];
+  }
+}
+
 // r(x) of a problem's radial map (ijk_to_x + r_of_x as the dumps use them, io.c:171-174)
 double radial_coordinate(const mdg_problem_desc &d, double x)
 {
@@ -214,6 +236,11 @@ void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_
     put(GF_GC2, i, (std::fabs(g02) > 1.0e-50) ? 1.0 / g02 : 0.0);
     put(GF_S00, i, std::sqrt(g00));
     put(GF_FSCALE, i, std::sqrt(g10));
+    // radial edge i as init_coords (metric_spherical_general.c:577-583) and
+    // monopole_gravity_finish (gravity.c:300-303) use it
+    const double re = r_of_x(std::fabs(i * d.dx[0] + d.startx[0]));
+    put(GF_RE2, i, re * re);
+    put(GF_DRDX, i, dr_dx(d.startx[0] + i * d.dx[0]));
     if (i >= 0 && i < n1) {
       double c[3][3][3];
       std::memset(c, 0, sizeof c);
@@ -378,6 +405,15 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
   const double sx0 = d.startx[0], sx1 = d.startx[1], sx2 = d.startx[2];
   const double dx0 = d.dx[0], dx1 = d.dx[1], dx2 = d.dx[2];
   const double max_log2_aspect = 0.5;
+
+  // radial edges for the monopole gravity (init_coords, metric_spherical_general.c:577-583;
+  // gravity.c:300-303)
+  h.medge.assign((size_t)2 * (n1 + 1), 0.0);
+  for (int i = 0; i <= n1; i++) {
+    const double re = r_of_x(std::fabs(i * dx0 + sx0));
+    h.medge[i] = re * re;
+    h.medge[n1 + 1 + i] = dr_dx(sx0 + i * dx0);
+  }
 
   // theta zones per radial row
   h.nj.assign(n1 + 2 * NG, 0);

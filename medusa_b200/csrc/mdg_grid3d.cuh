@@ -57,6 +57,10 @@ struct Grid3 {
   const double *sphc, *cphc;  // sin/cos(phi) at the zone centre, rc2 columns
   const double *sphl, *cphl;  // sin/cos(phi) at the lower phi face, rc2 columns
   const float *mx0, *mx1, *mx2;   // FP32 reconstruction weights (MixField) of the rc0/rc1/rc2 columns
+  const double *medge;        // [2][n1+1] SQR(redge[i]), dr_dx at radial edge i (monopole gravity)
+  double *gmono;              // [n1] monopole gravity at the radial zone centroids (shell masses first)
+  double x0;                  // startx[0]
+  int mono;                   // GRAV=SPHERICAL_MONOPOLE_GRAV
 };
 
 MDG_HD inline int ilog2(int s)
@@ -71,7 +75,7 @@ struct Grid3Host {
   int ndim = 3, n1 = 0, n2 = 0, n3 = 0;
   std::vector<int> nj, rowbase, nk;
   std::vector<int64_t> cell, f0, f1, f2;
-  std::vector<double> geo, rc0, rc1, rc2, xc1, xc2, sth, cth, sphc, cphc, sphl, cphl;
+  std::vector<double> geo, rc0, rc1, rc2, xc1, xc2, sth, cth, sphc, cphc, sphl, cphl, medge;
   std::vector<float> mx0, mx1, mx2;
   int64_t nij = 0, ncell = 0, nf0 = 0, nf1 = 0, nf2 = 0, cols1 = 0, cols2 = 0;
   int nlev1 = 0, nlev2 = 0;

@@ -329,6 +329,30 @@ __device__ __forceinline__ void u_to_p(double *u, double *p, double gc0, double 
   }
 }
 
+// Gravitational constant of constants.h:3 (cgs).
+constexpr double GNEWT = 6.67384e-8;
+
+// The monopole gravity sources of a zone (monopole_gravity_finish, gravity.c:389-407):
+// momentum rho g, and energy g times the mass flux density interpolated linearly in x
+// from the inner face (vl) to the outer face(s) (vr) to the zone centroid beta0/Gamma0.
+__device__ __forceinline__ void add_monopole_gravity(double rho, double g, double vl, double vr, double x0l,
+                                                     double dx0, double b0, double g0, double *src)
+{
+  const double A = (vr - vl) / dx0;
+  const double B = vl - A * x0l;
+  src[U1] += rho * g;
+  src[UU] += (A * b0 / g0 + B) * g;
+}
+
+// One step of the edge-to-centroid interpolation of the monopole acceleration
+// (gravity.c:302-319): zone ii between edges with accelerations gl, gr.
+__device__ __forceinline__ double monopole_centroid(double gl, double gr, double x0l, double dx0, double b0, double g0)
+{
+  const double A = (gr - gl) / dx0;
+  const double B = gl - A * x0l;
+  return A * b0 / g0 + B;
+}
+
 // fixed_gravity (gravity.c:38-64) added to the sources of a zone: src[ETOT] += rho
 // geom_dot(v, g0, gcov) (geometry.c:65-73, over all three components) and
 // src[P1+d] += rho g0[d] gcov[d] for the grid's directions d < ndim.

@@ -65,7 +65,9 @@ enum GeoField {
   GF_GC0, GF_GC1, GF_GC2,     // zone i: gcon[0..2]
   GF_S00,                     // zone i: scale[0][0]
   GF_CONN,                    // zone i: conn[l][m][n], 27 consecutive fields
-  GF_NFIELDS = GF_CONN + 27
+  GF_RE2 = GF_CONN + 27,      // edge i (lower edge of zone i): SQR(redge[i]) (init_coords)
+  GF_DRDX,                    // edge i: dr_dx(startx[0] + i*dx[0])
+  GF_NFIELDS
 };
 
 // The connection coefficients conn[l][m][n] (index l*9+m*3+n) that the 1-D spherical
@@ -84,6 +86,8 @@ struct ProbDev {
   int sparse_conn;          // 1-D: only the 9 connection coefficients of SPARSE_CONN are non-zero
   int floors;               // ENFORCE_FLOORS: u_to_p clamps rho and u to the floors below
   int grav_on;              // GRAV=FIXED_GRAV: the fixed acceleration grav[] is applied
+  int mono;                 // GRAV=SPHERICAL_MONOPOLE_GRAV: self-gravity, monopole approximation
+  int64_t mono_off;         // first zone of this problem in the monopole acceleration array
   int64_t cell_off;         // first zone of this problem in the state arrays
   int64_t ncell;            // interior zones (n1*n2 on 1-D/2-D grids; the dendritic count in 3-D)
   int64_t geo_off;          // first record (i=-NG) in the 1-D geometry tables
@@ -95,6 +99,7 @@ struct ProbDev {
   double cfl, dt_init_safety, dt_grow_safety, initial_dt, dtmax, dtmin, tmax;
   double rho_floor, e_floor;
   double grav[3];           // contravariant g0
+  double u1_hi[2];          // MDG_PROB_DUST: v^1 of the outer ghost zones n1, n1+1
   // 1-D geometry in closed form (mixed-precision sweep): lower edge of zone 0 and the
   // angular integrals of the 1-D spherical metric (spherical_1d_constants)
   double x0, gk_area, gk_th1, gk_th2, gk_tc;

@@ -21,6 +21,7 @@ struct Tables {
   const float *mx;       // FP32 reconstruction weights (mixed precision), MX_NFIELDS x geo_stride: 1-D problems,
                          // and direction 0 of 2-D problems (indexed like rc0)
   const float *mx1;      // direction-1 FP32 weights of 2-D problems, indexed like rc1
+  double *gmono;         // monopole gravity at the zone centroids of 1-D problems (ProbDev::mono_off)
 };
 
 // Device work queue of the persistent mixed-precision sweep: one head counter per RK
@@ -64,6 +65,10 @@ void launch_stage1d_mixed(int stage, int nt, int grid, bool use_queue, const Pro
                           const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA stage_state,
                           StateSoA state_n, StateSoA out, cudaStream_t st);
 int mixed_max_ctas_per_sm(int nt);
+// Monopole self-gravity of every 1-D problem with ProbDev::mono from its stage state:
+// the acceleration at each zone centroid into tb.gmono (gravity.c:145-425).
+void launch_monopole1d(const ProbDev *probs, ProbTime *times, int nprob, const Tables &tb, StateSoA stage_state,
+                       cudaStream_t st);
 void launch_conserved_totals(const ProbDev *probs, int nprob, const Tables &tb, StateSoA s, double *out,
                              cudaStream_t st);
 // Reconstruction, geometry and FP32-weight tables of 1-D problem m, built on the device

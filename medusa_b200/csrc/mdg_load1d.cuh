@@ -63,8 +63,14 @@ __device__ __forceinline__ void load_cell_1d(const ProbDev &P, const StateSoA &s
         for (int v = 0; v < NPRIM; v++) w[v] = a[v] + (i - n + 1) * (a[v] - b[v]);
       } break;
       case BC_PROB:
-        prob_bounds_noh(P.gam, __ldg(rc + RC_B0 * rcs + P.geo_off + i + NG),
-                        __ldg(rc + RC_G0 * rcs + P.geo_off + i + NG), t_bc, w);
+        if (P.prob_kind == MDG_PROB_DUST) {
+          // outflow, with v^r = -1/sqrt(r) / scale[0][0] of the ghost zone (init_dustcollapse.c:104-113)
+          rd(n - 1, w);
+          w[U1] = P.u1_hi[i - n];
+        } else {
+          prob_bounds_noh(P.gam, __ldg(rc + RC_B0 * rcs + P.geo_off + i + NG),
+                          __ldg(rc + RC_G0 * rcs + P.geo_off + i + NG), t_bc, w);
+        }
         break;
       default: rd(n - 1, w); break;   // OUTFLOW
     }

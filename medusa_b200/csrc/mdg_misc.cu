@@ -58,6 +58,39 @@ __global__ void finish_kernel(ProbTime *__restrict__ times, int nprob)
   times[m].dt_ready = 0;
 }
 
+// monopole_gravity_start/finish (gravity.c:145-425, GR_MONOPOLE=FALSE) of a 1-D problem,
+// one thread per problem, in the reference's serial order: shell masses vol*rho of the
+// stage state, enclosed mass mr at the radial edges, g = -G mr / r^2 dr/dx there
+// (g = 0 at the inner edge), interpolated linearly to each zone centroid.
+__global__ void monopole1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, int nprob,
+                                  Tables tb, StateSoA s)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nprob) return;
+  const ProbDev &P = probs[m];
+  if (!P.mono || times[m].done) return;
+  const double *geo = tb.geo;
+  const int64_t gs = tb.geo_stride, rcs = tb.rc0_stride;
+  double mr = 0.0, gl = 0.0;
+  for (int ii = 0; ii < P.n1; ii++) {
+    const int64_t gi = P.geo_off + ii + NG;
+    double ms = 0.0;
+    ms += __ldg(geo + GF_VOL * gs + gi) * s.v[RHO][P.cell_off + ii];
+    mr = mr + ms;
+    const double gr = -GNEWT * mr / __ldg(geo + GF_RE2 * gs + gi + 1) * __ldg(geo + GF_DRDX * gs + gi + 1);
+    const double x0l = P.x0 + ii * P.dx0;
+    tb.gmono[P.mono_off + ii] = monopole_centroid(gl, gr, x0l, P.dx0, __ldg(tb.rc0 + RC_B0 * rcs + gi),
+                                                  __ldg(tb.rc0 + RC_G0 * rcs + gi));
+    gl = gr;
+  }
+}
+
+void launch_monopole1d(const ProbDev *probs, ProbTime *times, int nprob, const Tables &tb, StateSoA s,
+                       cudaStream_t st)
+{
+  monopole1d_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(probs, times, nprob, tb, s);
+}
+
 // First estimate_dt() of a problem (step.c:171-187 with firstc): zone terms of the
 // initial state with its own EOS (main.c:180-182 fills sim_eos from sim_p).
 __device__ __forceinline__ void initial_estimate_block(const ProbDev *__restrict__ probs,

@@ -98,6 +98,8 @@ int check_desc(const mdg_problem_desc &d)
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: periodic boundaries must be paired");
   if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH)
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: rcoord");
+  if (d.monopole != 0 || d.prob_kind == MDG_PROB_DUST)
+    return fail(MDG_ERR_NOTIMPL, "mdg_advance_1d_noalloc: monopole gravity and the dust-collapse hook are not built here");
   if (d.rcoord == MDG_RCOORD_SINH && (!sph || !(d.rtrans > 0.0) || lo == MDG_BC_PROB || hi == MDG_BC_PROB))
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: the SINH radial map needs a spherical grid, rtrans > 0 "
                                  "and no PROB boundary");

@@ -749,6 +749,8 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
   if (rc != MDG_OK) return sfail(rc, "request: " + why);
   if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
     return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
+  if (desc->monopole != 0 || desc->prob_kind == MDG_PROB_DUST)
+    return sfail(MDG_ERR_NOTIMPL, "request: monopole gravity and the dust-collapse hook run in mdg_create solvers only");
   if (is_dendritic(*desc)) {
     // 3-D requests and 2-D spherical (r, theta) requests: the dendritic lane
     if (s->cfg.hbm_bytes_3d <= 0) return sfail(MDG_ERR_NOTIMPL, "request: the server takes no dendritic-grid requests");

@@ -122,9 +122,19 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
     }
     if (P.grav_on) add_fixed_gravity(ph, P.grav, gc0, gc1, gc2, 1, src);
+    if (P.mono) {
+      // mass flux density at the outer and inner face (gravity.c:380-401)
+      double vr = 0.0, area = 0.0;
+      vr += sfl[RHO][t + 1];
+      area += __ldg(geo + GF_AREA * gs + gi + 1) + 1.0e-16;
+      vr /= area;
+      const double vl = sfl[RHO][t] / (__ldg(geo + GF_AREA * gs + gi) + 1.0e-16);
+      add_monopole_gravity(ph[RHO], tb.gmono[P.mono_off + z], vl, vr, P.x0 + z * P.dx0, P.dx0,
+                           __ldg(rc + RC_B0 * rcs + gi), __ldg(rc + RC_G0 * rcs + gi), src);
+    }
     p_to_u(pn, u, gc0, gc1, gc2);
     p_to_u(ph, uh, gc0, gc1, gc2);
-    if (P.has_src || P.grav_on) lmin = tmin(lmin, dt_source_control(pn, u, src));
+    if (P.has_src || P.grav_on || P.mono) lmin = tmin(lmin, dt_source_control(pn, u, src));
     else nmin = tmin(nmin, src_dt_numerator_min(pn, u));   // zero sources: shared denominator
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) { divF[v] = 0.0; divF[v] += sfl[v][t + 1]; divF[v] -= sfl[v][t]; }

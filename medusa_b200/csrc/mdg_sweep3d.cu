@@ -685,6 +685,41 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face2_kernel(const ProbDev *_
   block_min_to(lmin, &times[0].minacc, sred);
 }
 
+// monopole_gravity_start (gravity.c:238-246): mass vol*rho of radial shell i, summed over
+// its zones in zone order (one thread per shell, the reference's serial order).
+__global__ void shell_mass3_kernel(const ProbTime *__restrict__ times, Grid3 g, StateSoA s)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.n1 || times[0].done) return;
+  double ms = 0.0;
+  for (int j = 0; j < nj_of(g, i); j++) {
+    const int ij = rowi(g, i, j);
+    const double vol = geo3(g, G3_VOL, ij);
+    const int64_t c0 = __ldg(g.cell + ij);
+    const int nk = __ldg(g.nk + ij);
+#pragma unroll 8
+    for (int k = 0; k < nk; k++) ms += vol * s.v[RHO][c0 + k];
+  }
+  g.gmono[i] = ms;
+}
+
+// monopole_gravity_finish (gravity.c:300-319, GR_MONOPOLE=FALSE): enclosed mass at the
+// radial edges, g = -G mr / r^2 dr/dx there, interpolated to the zone centroids (in place
+// over the shell masses).
+__global__ void monopole_profile3_kernel(const ProbTime *__restrict__ times, Grid3 g)
+{
+  if (threadIdx.x != 0 || times[0].done) return;
+  const int64_t rcs = g.n1 + 2 * NG;
+  double mr = 0.0, gl = 0.0;
+  for (int ii = 0; ii < g.n1; ii++) {
+    mr = mr + g.gmono[ii];
+    const double gr = -GNEWT * mr / __ldg(g.medge + ii + 1) * __ldg(g.medge + g.n1 + 1 + ii + 1);
+    g.gmono[ii] = monopole_centroid(gl, gr, g.x0 + ii * g.dx0, g.dx0, __ldg(g.rc0 + RC_B0 * rcs + ii + NG),
+                                    __ldg(g.rc0 + RC_G0 * rcs + ii + NG));
+    gl = gr;
+  }
+}
+
 // push() for zone (i, j, k) (step.c:327-478) with the dendritic flux fan-in, the
 // geometric sources of the stage state (rad_fluid.c:164-192, fluid.c:56-73) and, in the
 // second stage, the zone terms of the next estimate_dt (step.c:177-187).
@@ -739,6 +774,28 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
       s2 += T[2][0] * geo3(g, G3_C220, ij);
       s2 += T[2][1] * geo3(g, G3_C221, ij);
       src[RHO] = 0.0; src[UU] = 0.0; src[U1] = s0; src[U2] = s1; src[U3] = s2;
+    }
+    if (g.mono) {
+      // monopole gravity (gravity.c:373-401): mass flux density on the outer faces of the
+      // zone (row i+1, the fan-in below) and on its inner face
+      const int dji = djs(g, i), djo = djs(g, i + 1);
+      const int jp = j * dji / djo, njp = dji / djo, dkij = dks(g, i, j);
+      double vr = 0.0, area = 0.0;
+      for (int jj = jp; jj < jp + njp; jj++) {
+        const int nkp = dkij / dks(g, i + 1, jj);
+        const int ijo = rowi(g, i + 1, jj);
+        const int64_t fb = __ldg(g.f0 + ijo);
+        const double ao = geo3(g, G3_A0, ijo);
+        for (int kk = k * nkp; kk < k * nkp + nkp; kk++) {
+          vr += F0[RHO * g.nf0 + fb + kk];
+          area += ao + 1.0e-16;
+        }
+      }
+      vr /= area;
+      const double vl = F0[RHO * g.nf0 + __ldg(g.f0 + ij) + k] / (geo3(g, G3_A0, ij) + 1.0e-16);
+      const int64_t rcs = g.n1 + 2 * NG;
+      add_monopole_gravity(ph[RHO], g.gmono[i], vl, vr, g.x0 + i * g.dx0, g.dx0, __ldg(g.rc0 + RC_B0 * rcs + i + NG),
+                           __ldg(g.rc0 + RC_G0 * rcs + i + NG), src);
     }
     p_to_u(pn, u, g0, g1, g2);
     p_to_u(ph, uh, g0, g1, g2);
@@ -904,6 +961,7 @@ struct Sweep3 {
   double *d_flux = nullptr;        // F0 | F1 | F2, 5 arrays each
   unsigned char *d_bits = nullptr; // own0 | own1 | all0, one byte per zone each
   Tile3 *d_tiles = nullptr;        // face0 | face1 | face2 | zone tiles
+  double *d_gmono = nullptr;       // monopole gravity per radial row
   int nt[4] = {0, 0, 0, 0};
   int64_t ncell = 0;
   int64_t bytes = 0;               // device memory held
@@ -934,19 +992,21 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
       {h.cth.data(), h.cth.size() * sizeof(double)},    {h.sphc.data(), h.sphc.size() * sizeof(double)},
       {h.cphc.data(), h.cphc.size() * sizeof(double)},  {h.sphl.data(), h.sphl.size() * sizeof(double)},
       {h.cphl.data(), h.cphl.size() * sizeof(double)},  {h.mx0.data(), h.mx0.size() * sizeof(float)},
-      {h.mx1.data(), h.mx1.size() * sizeof(float)},     {h.mx2.data(), h.mx2.size() * sizeof(float)}};
+      {h.mx1.data(), h.mx1.size() * sizeof(float)},     {h.mx2.data(), h.mx2.size() * sizeof(float)},
+      {h.medge.data(), h.medge.size() * sizeof(double)}};
   std::vector<size_t> off(parts.size());
   size_t tot = 0;
   for (size_t q = 0; q < parts.size(); q++) {
     off[q] = tot;
     tot += (parts[q].second + 255) / 256 * 256;
   }
-  w->bytes = (int64_t)tot + (int64_t)sizeof(double) * NPRIM * (h.nf0 + h.nf1 + h.nf2) + 3 * h.ncell;
+  w->bytes = (int64_t)tot + (int64_t)sizeof(double) * NPRIM * (h.nf0 + h.nf1 + h.nf2) + 3 * h.ncell +
+             (int64_t)sizeof(double) * h.n1;
   std::vector<char> host(tot, 0);
   for (size_t q = 0; q < parts.size(); q++) std::memcpy(host.data() + off[q], parts[q].first, parts[q].second);
   auto fail3 = [&](cudaError_t e) {
     why = cudaGetErrorString(e);
-    cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles);
+    cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles); cudaFree(w->d_gmono);
     delete w;
     return e == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA;
   };
@@ -974,6 +1034,12 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   g.sphc = (const double *)(b + off[15]); g.cphc = (const double *)(b + off[16]);
   g.sphl = (const double *)(b + off[17]); g.cphl = (const double *)(b + off[18]);
   g.mx0 = (const float *)(b + off[19]); g.mx1 = (const float *)(b + off[20]); g.mx2 = (const float *)(b + off[21]);
+  g.medge = (const double *)(b + off[22]);
+  g.x0 = d.startx[0];
+  g.mono = d.monopole;
+  e = cudaMalloc(&w->d_gmono, sizeof(double) * (size_t)h.n1);
+  if (e != cudaSuccess) return fail3(e);
+  g.gmono = w->d_gmono;
   // flux arrays, shock bits
   e = cudaMalloc(&w->d_flux, sizeof(double) * NPRIM * (size_t)(h.nf0 + h.nf1 + h.nf2));
   if (e != cudaSuccess) return fail3(e);
@@ -1008,7 +1074,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
 void sweep3_destroy(Sweep3 *w)
 {
   if (!w) return;
-  cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles);
+  cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles); cudaFree(w->d_gmono);
   delete w;
 }
 
@@ -1024,6 +1090,10 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
   unsigned char *own = w->d_bits + (size_t)stage * g.ncell, *all0 = w->d_bits + (size_t)2 * g.ncell;
   const Tile3 *t0 = w->d_tiles, *t1 = t0 + w->nt[0], *t2 = t1 + w->nt[1], *tc = t2 + w->nt[2];
   if (stage == 0) cudaMemsetAsync(all0, 0, (size_t)g.ncell, st);
+  if (g.mono) {
+    shell_mass3_kernel<<<(g.n1 + 127) / 128, 128, 0, st>>>(times, g, sst);
+    monopole_profile3_kernel<<<1, 32, 0, st>>>(times, g);
+  }
   auto faces = [&](auto s0, auto mix) {
     constexpr int S = decltype(s0)::value;
     constexpr bool M = decltype(mix)::value;

@@ -36,6 +36,7 @@ SPHERICAL_ORIGIN = 5
 # problem-specific PROB boundary hooks
 PROB_NONE = 0
 PROB_NOH = 1
+PROB_DUST = 2               # problems/init_dustcollapse.c:104-113 (outer v^r hook)
 
 RCOORD_UNIFORM = 0          # radial maps r(x), metric_spherical_general.c:149-219
 RCOORD_SINH = 1
@@ -69,6 +70,7 @@ class Problem:
     tmax: float = 1.0e100
     rcoord: int = RCOORD_UNIFORM  # radial map of a spherical grid (the RCOORD build switch)
     rtrans: float = 1.0           # its transition radius (RCOORD_SINH)
+    monopole: int = 0             # self-gravity, monopole approximation (GRAV=SPHERICAL_MONOPOLE_GRAV)
     hydro_interp_order: int = 3   # io.c:5055
     enforce_floors: int = 0       # ENFORCE_FLOORS build switch (fluid.c:43-46)
     rho_floor: float = -1.0       # io.c:5082 default; problem hooks set their own
@@ -456,6 +458,74 @@ def sedov_2d_spherical(n1: int = 256, n2: int = 128, gam: float = 1.4, energy: f
     return Problem(name="sedov2dsph_%s%dx%d" % ("sinh_" if map_ else "", n1, n2), ndim=2, geom=SPHERICAL,
                    n=(n1, n2, 1), startx=startx, dx=dx, gam=gam, ic=ic, bc_lo=(bc_inner, bc_pole, PERIODIC),
                    bc_hi=(OUTFLOW, bc_pole, PERIODIC), cfl=cfl, tmax=tmax, cells=ncell, **map_)
+
+
+GNEWT = 6.67384e-8   # constants.h:3 (cgs)
+
+
+def dust_collapse(n1: int = 200, n2: int = 16, n3: int = 32, ndim: int = 1, dr: float = 5.0e4,
+                  r_out: float = 7.0e8, rho0: float = 1.0e9, r0: float = 6.5e8, t0: float = 1.0,
+                  mach: float = 2.0, gam: float = 5.0 / 3.0, cfl: float = 0.9, tmax: float = 1.0e100,
+                  radius: str = "sinh", floors: bool = True, hook: Optional[bool] = None) -> Problem:
+    """Collapse of a uniform, nearly pressureless sphere under its own gravity in the
+    monopole approximation (problems/init_dustcollapse.c, setups/dustcollapse_1d.mk; cgs):
+    rho0 inside r0 (the zone that straddles r0 gets the volume-weighted share), the
+    floor 1e-5 rho0 outside, p0 = rho0 (r0/t0/mach)^2 / gam everywhere, at rest;
+    SPHERICAL_ORIGIN at the centre.  The radius follows the SINH map with innermost zones
+    `dr` wide reaching r_out (rtrans_solve as the hook calls it), or with radius="uniform"
+    zones of width r_out/n1.  In 1-D the outer boundary is outflow with the hook's
+    v^r = -1/sqrt(r) (hook=True, the default there); the dendritic grids (ndim 2 or 3,
+    SPHERICAL_ORIGIN poles, periodic phi) use plain outflow.  floors: the ENFORCE_FLOORS
+    build with the hook's rho_floor = 1e-5 rho0 and e_floor = p0/(gam-1)."""
+    if hook is None:
+        hook = ndim == 1
+    if hook and ndim != 1:
+        raise ValueError("the dust-collapse boundary hook is built for 1-D grids")
+    if radius == "sinh":
+        dx0 = dr
+        map_ = dict(rcoord=RCOORD_SINH, rtrans=sinh_rtrans(n1, dr, r_out))
+    else:
+        dx0 = r_out / n1
+        map_ = {}
+    rt = map_.get("rtrans")
+    v0 = r0 / t0
+    p0 = rho0 * (v0 / mach) ** 2 / gam
+    rho_floor = 1.0e-5 * rho0
+    e_floor = p0 / (gam - 1.0)
+    rho_row = np.empty(n1)
+    for i in range(n1):
+        rm, rp = _r_of_x(i * dx0, rt), _r_of_x((i + 1) * dx0, rt)
+        if rp < r0:
+            rho_row[i] = rho0
+        elif rm < r0:
+            rho_row[i] = rho0 * (math.pow(r0, 3) - math.pow(rm, 3)) / (math.pow(rp, 3) - math.pow(rm, 3))
+        else:
+            rho_row[i] = rho_floor
+    fl = dict(enforce_floors=1, rho_floor=rho_floor, e_floor=e_floor) if floors else \
+        dict(rho_floor=rho_floor, e_floor=e_floor)
+    if ndim == 1:
+        counts = np.ones(n1, dtype=int)
+        n, startx, dx = (n1, 1, 1), (0.0, -1.0, 0.0), (dx0, 2.0, 2.0 * math.pi)
+        bc_lo = (SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW)
+        bc_hi = (PROB if hook else OUTFLOW, OUTFLOW, OUTFLOW)
+        cells = 0
+    else:
+        n3e = n3 if ndim == 3 else 1
+        startx, dx = (0.0, -1.0, 0.0), (dx0, 2.0 / n2, 2.0 * math.pi / n3e)
+        nj, nk = dendritic_grid(n1, n2, n3e, startx, dx, ndim=ndim, rtrans=rt)
+        counts = np.array([sum(row) for row in nk])
+        n = (n1, n2, n3e)
+        bc_lo = (SPHERICAL_ORIGIN, SPHERICAL_ORIGIN, PERIODIC)
+        bc_hi = (OUTFLOW, SPHERICAL_ORIGIN, PERIODIC)
+        cells = int(counts.sum())
+    ncell = int(counts.sum())
+    ic = np.zeros((ncell, NPRIM))
+    ic[:, 0] = np.repeat(rho_row, counts)
+    ic[:, 1] = p0 / (gam - 1.0)
+    return Problem(name="dust%dd_%s%d" % (ndim, "sinh_" if map_ else "", n1), ndim=ndim, geom=SPHERICAL, n=n,
+                   startx=startx, dx=dx, gam=gam, ic=ic, bc_lo=bc_lo, bc_hi=bc_hi,
+                   prob_kind=PROB_DUST if hook else PROB_NONE, cfl=cfl, tmax=tmax, monopole=1, cells=cells,
+                   **fl, **map_)
 
 
 def ensemble_1d(count: int = 2048, seed: int = 7, nmin: int = 128, nmax: int = 8192,

@@ -81,7 +81,8 @@ class ProblemDesc(ctypes.Structure):
                 ("dtmax", ctypes.c_double), ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
                 ("hydro_interp_order", ctypes.c_int),
                 ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double), ("e_floor", ctypes.c_double),
-                ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int), ("rtrans", ctypes.c_double)]
+                ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int), ("rtrans", ctypes.c_double),
+                ("monopole", ctypes.c_int)]
 
 
 def desc_of(pb: "_pb.Problem") -> ProblemDesc:
@@ -101,6 +102,7 @@ def desc_of(pb: "_pb.Problem") -> ProblemDesc:
     for k in range(3):
         d.grav[k] = pb.grav[k]
     d.rcoord, d.rtrans = pb.rcoord, pb.rtrans
+    d.monopole = int(pb.monopole)
     return d
 
 

@@ -83,6 +83,18 @@ CONFIGS = {
                        RCOORD="SINH", THCOORD="UNIFORM"),
     "sph3d_sinh": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
                        RCOORD="SINH", THCOORD="UNIFORM"),
+    # self-gravity in the monopole approximation (GRAV=SPHERICAL_MONOPOLE_GRAV,
+    # GR_MONOPOLE=FALSE; setups/dustcollapse_1d.mk): 1-D on the SINH radius with floors,
+    # and the dendritic grids
+    "sph1d_sinh_mono_floors": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                                   RCOORD="SINH", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV",
+                                   ENFORCE_FLOORS="TRUE"),
+    "sph1d_mono": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                       RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
+    "sph2d_mono": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                       RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
+    "sph3d_mono": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                       RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
 }
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]

@@ -163,12 +163,15 @@ class Oracle:
 # ----------------------------------------------------------------------------- reference
 def ref_config(pb) -> str:
     """The oracle/_ref build of a problem: its geometry and dimension, its radial map,
-    and whether the FIXED_GRAV and ENFORCE_FLOORS switches are compiled in."""
+    its gravity (FIXED_GRAV, SPHERICAL_MONOPOLE_GRAV) and whether ENFORCE_FLOORS is
+    compiled in."""
     name = ("cart%dd" if pb.geom == 0 else "sph%dd") % pb.ndim
     if getattr(pb, "rcoord", 0) == 1:
         name += "_sinh"
     if any(g != 0.0 for g in getattr(pb, "grav", (0.0, 0.0, 0.0))):
         name += "_grav"
+    if getattr(pb, "monopole", 0):
+        name += "_mono"
     return name + ("_floors" if getattr(pb, "enforce_floors", 0) else "")
 
 

@@ -121,6 +121,11 @@ void init_problem()
       bc[vv].hi[dd] = g_prm.bc_hi[dd];
     }
   }
+  if (g_prm.prob_kind == 2) {
+    /* problems/init_dustcollapse.c:77-86: outflow, with the PROB hook on v^r only */
+    VLOOP bc[vv].hi[0] = OUTFLOW;
+    bc[U1].hi[0] = PROB;
+  }
   ZLOOP {
     for (vv=0; vv<NPRIM; vv++) NDP_ELEM_LINEAR(sim_p,ii,jj,kk,vv) = g_ic[NPRIM*c+vv];
     c++;
@@ -140,6 +145,11 @@ void prob_bounds(int i, int j, int k, double *p)
     p[U3] = 0.;
     p[RHO] += t/r;
     p[RHO] *= p[RHO];
+  } else if (g_prm.prob_kind == 2) {
+    /* problems/init_dustcollapse.c:104-113 */
+    double r = r_of_x(rx_info, beta0[i]/Gamma0[i]);
+    double vr = -1.0/sqrt(r);
+    p[U1] = vr/ND_ELEM_LINEAR(geom,i,j,k).scale[0][0];
   }
 }
 

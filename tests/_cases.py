@@ -20,6 +20,10 @@ def golden_cases3d():
     return make_golden.cases3d()
 
 
+def golden_cases_gravity():
+    return make_golden.cases_gravity()
+
+
 def load_golden(name):
     return np.load(os.path.join(GOLDEN_DIR, name + ".npz"))
 

@@ -62,9 +62,23 @@ def cases3d():
     }
 
 
+def cases_gravity():
+    """Self-gravity in the monopole approximation (the reference's
+    GRAV=SPHERICAL_MONOPOLE_GRAV builds; the C restatement does not cover it): the
+    dust-collapse setup of problems/init_dustcollapse.c in 1-D (SINH radius, floors,
+    the outer v^r hook; uniform radius without floors) and on the 2-D and 3-D dendritic
+    grids.  Fixtures as for cases3d (the state after n steps and one step from it)."""
+    return {
+        "dust1d_sinh_200": (P.dust_collapse(200), 60),
+        "dust1d_uniform_nofloor_128": (P.dust_collapse(128, radius="uniform", floors=False), 60),
+        "dust2d_uniform_24x16": (P.dust_collapse(24, 16, ndim=2, radius="uniform", floors=False), 40),
+        "dust3d_uniform_16x8x16": (P.dust_collapse(16, 8, 16, ndim=3, radius="uniform", floors=False), 30),
+    }
+
+
 def main():
     build_ref.build()
-    for name, (pb, n) in cases3d().items():
+    for name, (pb, n) in list(cases3d().items()) + list(cases_gravity().items()):
         snaps = pyoracle.run_reference(pb, n, every=n)
         last = snaps[-1]
         one = pyoracle.run_reference(pb.copy(ic=last[4]), 1, every=1)[-1]

@@ -1,0 +1,116 @@
+"""GPU parity of the monopole self-gravity (gravity.c:145-425, GR_MONOPOLE=FALSE) against
+fixtures made by the reference's GRAV=SPHERICAL_MONOPOLE_GRAV builds: the dust collapse
+of problems/init_dustcollapse.c in 1-D (SINH radius with floors and the outer v^r hook;
+uniform radius) and on the 2-D and 3-D dendritic grids.  Bars as for the other sweeps:
+1e-9 after a whole fixture run, 1e-12 for one step (error per variable relative to its
+largest magnitude, the velocities sharing one scale)."""
+import numpy as np
+import pytest
+
+from medusa_b200 import problems as P
+from medusa_b200.solver import MdgError, PREC_MIXED, Server, Solver
+from tests._cases import golden_cases_gravity, load_golden, record
+
+pytestmark = pytest.mark.gpu
+
+CASES = golden_cases_gravity()
+FULL_RUN_TOL = 1.0e-9
+PER_STEP_TOL = 1.0e-12
+
+
+def err(a, b):
+    out = 0.0
+    vscale = max(np.abs(b[:, 2:5]).max(), 1.0e-300)
+    for v in range(5):
+        scale = vscale if v >= 2 else max(np.abs(b[:, v]).max(), 1.0e-300)
+        out = max(out, float(np.abs(a[:, v] - b[:, v]).max() / scale))
+    return out
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gravity_full_run_matches_reference_fixture(name):
+    pb, n = CASES[name]
+    g = load_golden(name)
+    with Solver(pb) as s:
+        s.step(n)
+        prim = s.update_cpu(0)
+        t, _, istep = s.time(0)
+    e = err(prim, g["prim"])
+    record("gravity_full_" + name, steps=n, err=e, bit_identical=float(np.mean(prim == g["prim"])))
+    assert istep == n
+    assert e <= FULL_RUN_TOL
+    assert abs(t - float(g["t"])) <= FULL_RUN_TOL * float(g["t"])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_gravity_one_step_from_developed_state(name):
+    pb, n = CASES[name]
+    g = load_golden(name)
+    with Solver(pb.copy(ic=np.array(g["prim"]))) as s:
+        s.step(1)
+        prim = s.update_cpu(0)
+    e = err(prim, g["prim1"])
+    record("gravity_step_" + name, err=e, bit_identical=float(np.mean(prim == g["prim1"])))
+    assert e <= PER_STEP_TOL
+
+
+def test_monopole_problem_alone_and_in_a_batch():
+    """A 1-D self-gravitating problem batched with problems without gravity: every result
+    equals its run alone, bit for bit."""
+    dust = P.dust_collapse(200)
+    others = [P.spherical_1d("sedov", 300, 1.4, p_ratio=1.0e4, r0=0.05), P.sod(257)]
+    with Solver([others[0], dust, others[1]]) as s:
+        s.step(40)
+        batch = [s.update_cpu(m) for m in range(3)]
+    for m, pb in enumerate([others[0], dust, others[1]]):
+        with Solver(pb) as s:
+            s.step(40)
+            alone = s.update_cpu(0)
+        assert np.array_equal(alone, batch[m]), pb.name
+
+
+def test_collapse_accelerates_inwards():
+    """Free fall from rest: after a short time the radial velocity inside the sphere is
+    close to -g t with g = G M(<r) / r^2 (pressure is 1/gam/mach^2 of the free-fall scale)."""
+    pb = P.dust_collapse(200, radius="uniform", floors=False)
+    with Solver(pb) as s:
+        s.step(40)
+        prim = s.update_cpu(0)
+        t = s.time(0)[0]
+    rc = P.radial_centers(pb)
+    i = int(np.searchsorted(rc, 3.0e8))
+    m_in = 4.0 / 3.0 * np.pi * rc[i] ** 3 * 1.0e9
+    v_ff = -P.GNEWT * m_in / rc[i] ** 2 * t
+    record("gravity_freefall", t=t, v=float(prim[i, 2]), v_ff=v_ff)
+    assert abs(prim[i, 2] - v_ff) <= 0.05 * abs(v_ff)
+
+
+def test_dendritic_mixed_matches_fp64():
+    """The mixed-precision dendritic sweep with self-gravity: L1 of rho and u against the
+    plain FP64 sweep at equal time <= 1e-4."""
+    from medusa_b200 import analytic as A
+    from medusa_b200.solver import grid3d_zone_volumes
+    pb = P.dust_collapse(32, 16, 32, ndim=3, radius="uniform", floors=False)
+    with Solver(pb) as s:
+        s.step(40)
+        ref = s.update_cpu(0)
+        t_end = s.time(0)[0]
+    with Solver(pb.copy(tmax=t_end), precision=PREC_MIXED) as s:
+        for _ in range(40):
+            s.step(5)
+            if s.time(0)[0] >= t_end * (1.0 - 1.0e-12):
+                break
+        mix = s.update_cpu(0)
+    vol = grid3d_zone_volumes(pb)
+    l1_rho = A.l1_rel(mix[:, 0], ref[:, 0], vol)
+    l1_u = A.l1_rel(mix[:, 1], ref[:, 1], vol)
+    record("gravity_mixed_dust3d_32x16x32", l1_rho=l1_rho, l1_u=l1_u)
+    assert l1_rho <= 1.0e-4 and l1_u <= 1.0e-4
+
+
+def test_server_refuses_monopole_requests():
+    pb = P.dust_collapse(64).copy(tmax=1.0e-3)
+    with Server(precision=0, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
+        with pytest.raises(MdgError) as e:
+            srv.submit(pb)
+        assert e.value.code == 5
