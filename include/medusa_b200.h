@@ -129,6 +129,18 @@ int mdg_estimate_dt(mdg_solver *s, double *dt_out);
  * respect to the host (work is queued on the solver's stream). */
 int mdg_step(mdg_solver *s, int nsteps);
 
+/* For a host that runs the main.c time loop itself (its own dump/pdump/tmax clipping of
+ * dt, main.c:228-251):
+ *   mdg_estimate_dt_raw  what estimate_dt() (step.c:163-203) leaves in the global dt:
+ *                        cfl * min(CFL and source limits of the last step or, before the
+ *                        first step, of the state; initial_dt at step 0; dtmax), one per
+ *                        problem in dt_out[nprob].  Synchronous; changes nothing.
+ *   mdg_step_dt          one step() (step.c:28-129) of every problem with the host's
+ *                        dt[nprob]; each problem's t advances by dt as main.c's t += dt
+ *                        does.  Asynchronous. */
+int mdg_estimate_dt_raw(mdg_solver *s, double *dt_out);
+int mdg_step_dt(mdg_solver *s, const double *dt);
+
 /* update_cpu() equivalent: copy problem `prob`'s interior primitives ([zone][5]) and,
  * if eos != NULL, its EOS record ([zone][5]: PRESS, CS, TEMP, ENT(=0), GAMMA; the EOS
  * of the most recent stage state, as the reference's sim_eos holds) to host memory. */

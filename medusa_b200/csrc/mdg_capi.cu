@@ -63,6 +63,7 @@ struct mdg_solver {
   // mixed precision: FP32 weights, the work queue and its tile list (tile = threads-2 zones)
   float *d_mx = nullptr, *d_mx1 = nullptr;   // FP32 weights (mixed): 1-D or 2-D direction 0; 2-D direction 1
   double *d_gmono = nullptr;      // monopole gravity at the zone centroids of the 1-D problems
+  double *d_dtbuf = nullptr;      // per-problem dt of mdg_estimate_dt_raw / mdg_step_dt
   bool any_mono = false;          // a 1-D problem has monopole gravity
   WorkQueue *d_queue = nullptr;
   Tile *d_mtiles = nullptr;
@@ -276,6 +277,7 @@ static void free_all(mdg_solver *s)
   cudaFree(s->d_state); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_stage); cudaFree(s->d_err);
   cudaFree(s->d_mx); cudaFree(s->d_mx1); cudaFree(s->d_queue); cudaFree(s->d_mtiles); cudaFree(s->d_totals); cudaFree(s->d_stage_all);
   cudaFree(s->d_gmono);
+  cudaFree(s->d_dtbuf);
   sweep3_destroy(s->s3);
   s->s3 = nullptr;
   if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
@@ -640,6 +642,12 @@ int mdg_download_all(mdg_solver *s, double *prim)
   return MDG_OK;
 }
 
+static cudaError_t ensure_dt_buffer(mdg_solver *s)
+{
+  if (s->d_dtbuf) return cudaSuccess;
+  return cudaMalloc(&s->d_dtbuf, sizeof(double) * s->nprob);
+}
+
 static int queue_steps(mdg_solver *s, int nsteps)
 {
   auto mark = [&](int k, int e) { if (s->timing) cudaEventRecord(s->ev[k][e], s->stream); };
@@ -710,6 +718,31 @@ int mdg_estimate_dt(mdg_solver *s, double *dt_out)
     for (int m = 0; m < s->nprob; m++) dt_out[m] = T[m].dt;
   }
   return MDG_OK;
+}
+
+int mdg_estimate_dt_raw(mdg_solver *s, double *dt_out)
+{
+  if (!s || !dt_out) return fail(MDG_ERR_INVALID, "solver/dt_out");
+  CK(cudaSetDevice(s->device));
+  CK(ensure_dt_buffer(s));
+  launch_raw_estimate(s->d_probs, s->d_times, s->nprob, s->d_dtbuf, s->stream);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dt_out, s->d_dtbuf, sizeof(double) * s->nprob, cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MDG_OK;
+}
+
+int mdg_step_dt(mdg_solver *s, const double *dt)
+{
+  if (!s || !dt) return fail(MDG_ERR_INVALID, "solver/dt");
+  for (int m = 0; m < s->nprob; m++)
+    if (!(dt[m] > 0.0) || !(dt[m] < 1.0e300)) return fail(MDG_ERR_INVALID, "dt must be positive and finite");
+  CK(cudaSetDevice(s->device));
+  CK(ensure_dt_buffer(s));
+  // the copy is staged from pageable memory before the call returns
+  CK(cudaMemcpyAsync(s->d_dtbuf, dt, sizeof(double) * s->nprob, cudaMemcpyHostToDevice, s->stream));
+  launch_set_dt(s->d_times, s->nprob, s->d_dtbuf, s->stream);
+  return queue_steps(s, 1);
 }
 
 // Capture cfg.steps_per_graph steps of the launch sequence into a CUDA graph (once per

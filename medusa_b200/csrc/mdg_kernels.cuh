@@ -87,6 +87,9 @@ void launch_initial_estimate3(Sweep3 *w, const ProbDev *probs, ProbTime *times, 
 void launch_totals3(Sweep3 *w, StateSoA s, double *out, cudaStream_t st);
 void launch_dt_finalize(const ProbDev *probs, ProbTime *times, int nprob, int *err, cudaStream_t st);
 void launch_finish(ProbTime *times, int nprob, cudaStream_t st);
+// estimate_dt() alone into out[m]; and the time record of a step with the host's dt[m]
+void launch_raw_estimate(const ProbDev *probs, const ProbTime *times, int nprob, double *out, cudaStream_t st);
+void launch_set_dt(ProbTime *times, int nprob, const double *dt, cudaStream_t st);
 void launch_reset_time(ProbTime *times, int m, cudaStream_t st);
 void launch_initial_estimate_one(const ProbDev *probs, ProbTime *times, int m, int64_t ncell,
                                  const Tables &tb, StateSoA s, cudaStream_t st);

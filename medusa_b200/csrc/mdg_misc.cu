@@ -47,6 +47,49 @@ __global__ void dt_finalize_kernel(const ProbDev *__restrict__ probs, ProbTime *
   times[m] = T;
 }
 
+// estimate_dt() (step.c:192-198) alone: what it leaves in the reference's global dt.
+__global__ void raw_estimate_kernel(const ProbDev *__restrict__ probs, const ProbTime *__restrict__ times, int nprob,
+                                    double *__restrict__ out)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nprob) return;
+  const ProbDev &P = probs[m];
+  const ProbTime &T = times[m];
+  double min_dt = ord_to_dbl(T.minacc);
+  if (T.istep == 0) min_dt = tmin(min_dt, P.initial_dt);
+  min_dt = tmin(min_dt, P.dtmax);
+  min_dt *= P.cfl;
+  out[m] = min_dt;
+}
+
+// The time record of one step() with a dt chosen by the host's own time loop: the
+// boundary times of reset_boundaries_gpu (bc.c:721, 1418) and main.c's t += dt.
+__global__ void set_dt_kernel(ProbTime *__restrict__ times, int nprob, const double *__restrict__ dts)
+{
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nprob) return;
+  ProbTime T = times[m];
+  const double dt = dts[m];
+  T.dt = dt;
+  T.dtold = dt;
+  T.t_bc1 = T.t + dt;
+  T.t_next = (T.t_bc1 - dt) + dt;
+  T.minacc = dbl_to_ord(1.0e100);
+  T.done = 0;
+  T.dt_ready = 1;
+  times[m] = T;
+}
+
+void launch_raw_estimate(const ProbDev *probs, const ProbTime *times, int nprob, double *out, cudaStream_t st)
+{
+  raw_estimate_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(probs, times, nprob, out);
+}
+
+void launch_set_dt(ProbTime *times, int nprob, const double *dt, cudaStream_t st)
+{
+  set_dt_kernel<<<(nprob + 127) / 128, 128, 0, st>>>(times, nprob, dt);
+}
+
 __global__ void finish_kernel(ProbTime *__restrict__ times, int nprob)
 {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;

@@ -148,14 +148,73 @@ def build_config(name, cfg, ref_root, force=False):
     return built
 
 
-def build(ref_root=DEFAULT_REF_ROOT, force=False):
-    """Build every configuration; returns the list of binaries.  Needs the reference tree."""
+# The reference's own main.c driving a problem end to end (oracle/refshim/dropin_glue.c):
+# dropin_cpu_<prob> links the reference's step.c, dropin_gpu_<prob> links
+# medusa_b200/host/fornax_binding.c and libmedusa_b200 instead.  name -> (config,
+# DROPIN_PROB, MDG_BINDING_PROB_KIND)
+DROPIN = {
+    "sod": ("cart1d", 1, "MDG_PROB_NONE"),
+    "dust": ("sph1d_sinh_mono_floors", 2, "MDG_PROB_DUST"),
+}
+ROOT = os.path.dirname(HERE)
+LIBDIR = os.path.join(ROOT, "medusa_b200", "_lib")
+BINDING = os.path.join(ROOT, "medusa_b200", "host", "fornax_binding.c")
+
+
+def build_dropin(name, ref_root, force=False):
+    cfgname, prob, kind = DROPIN[name]
+    defs = dict(BASE_DEFS)
+    defs.update(CONFIGS[cfgname])
+    cdir = os.path.join(OUT, cfgname)
+    os.makedirs(cdir, exist_ok=True)
+    write_build_h(os.path.join(cdir, "build.h"), defs)
+    srcs = [os.path.join(ref_root, "main.c")] + [os.path.join(ref_root, s) for s in REF_SOURCES]
+    if defs["GRAV"] != "NO_GRAV":
+        srcs.append(os.path.join(ref_root, "gravity.c"))
+    if defs["GEOM"] == "SPHERICAL":
+        srcs.append(os.path.join(ref_root, "metrics", "metric_spherical_general.c"))
+    else:
+        srcs.append(os.path.join(SHIM, "metric_cartesian_current.c"))
+    srcs.append(os.path.join(SHIM, "dropin_glue.c"))
+    built = []
+    lib = os.path.join(LIBDIR, "libmedusa_b200.so")
+    for kind_name in ("cpu", "gpu"):
+        target = os.path.join(OUT, "dropin_%s_%s" % (kind_name, name))
+        s = list(srcs)
+        extra = []
+        if kind_name == "gpu":
+            s = [x for x in s if os.path.basename(x) != "step.c"] + [BINDING]
+            extra = ["-I" + os.path.join(ROOT, "include"), "-DMDG_BINDING_PROB_KIND=" + kind,
+                     "-L" + LIBDIR, "-lmedusa_b200", "-Wl,-rpath,$ORIGIN/../../medusa_b200/_lib"]
+            if not os.path.exists(lib):
+                raise FileNotFoundError("build libmedusa_b200.so first (python -m medusa_b200.build)")
+        deps = s + [os.path.join(cdir, "build.h"), os.path.abspath(__file__)] + ([lib] if kind_name == "gpu" else [])
+        if (not force and os.path.exists(target)
+                and os.path.getmtime(target) >= max(os.path.getmtime(d) for d in deps)):
+            built.append(target)
+            continue
+        cmd = (["gcc", "-std=gnu99", "-w"] + PARITY_FLAGS + ["-DDROPIN_PROB=%d" % prob] +
+               ["-I" + cdir, "-I" + ref_root, "-include", "limits.h", "-o", target] + s + extra + ["-lm"])
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+            raise RuntimeError("oracle/_ref build failed for %s" % target)
+        built.append(target)
+    return built
+
+
+def build(ref_root=DEFAULT_REF_ROOT, force=False, dropin=True):
+    """Build every configuration (and, when libmedusa_b200.so is built, the drop-in
+    runs); returns the list of binaries.  Needs the reference tree."""
     if not os.path.isdir(ref_root):
         raise FileNotFoundError("reference tree not found at %s" % ref_root)
     os.makedirs(OUT, exist_ok=True)
     out = []
     for name, cfg in CONFIGS.items():
         out += build_config(name, cfg, ref_root, force)
+    if dropin and os.path.exists(os.path.join(LIBDIR, "libmedusa_b200.so")):
+        for name in DROPIN:
+            out += build_dropin(name, ref_root, force)
     return out
 
 
