@@ -60,6 +60,12 @@ extern "C" {
 #define MDG_RCOORD_UNIFORM 0   /* r = |x| */
 #define MDG_RCOORD_SINH 1      /* r = rtrans sinh(|x| / rtrans): zones of width dx near the
                                   centre, growing geometrically outside rtrans */
+#define MDG_RCOORD_SINH_MODIFIED 2  /* the SINH map minus facta [sigmoid((|x| - factb) / factc)
+                                       - sigmoid(-factb / factc)] (the reference's default) */
+/* theta maps th(x), x in [-1, 1] (THCOORD, metric_spherical_general.c:222-290) */
+#define MDG_THCOORD_UNIFORM 0  /* th = pi (x + 1) / 2 */
+#define MDG_THCOORD_POLYTH 1   /* th = poly_norm x (1 + (x/poly_xt)^poly_alpha / (poly_alpha + 1)) + pi/2,
+                                  zones concentrated at the equator (the reference's default) */
 
 /* arithmetic of the sweep */
 #define MDG_PREC_FP64 0   /* plain: FP64 throughout, the reference's operation order */
@@ -96,6 +102,10 @@ typedef struct mdg_problem_desc {
   int rcoord;               /* MDG_RCOORD_* radial map of a spherical grid (the RCOORD build switch) */
   double rtrans;            /* transition radius of the SINH map (rx_info.rtrans; problem hooks
                                set it with rtrans_solve, e.g. problems/init_sedov.c:20) */
+  double rfact[3];          /* facta, factb, factc of MDG_RCOORD_SINH_MODIFIED (rx_info; parse_input
+                               sets 1e6, 1.5e6, 5e5, io.c:5008-5010) */
+  int thcoord;              /* MDG_THCOORD_* theta map of a spherical grid (the THCOORD build switch) */
+  double poly_xt, poly_alpha;  /* MDG_THCOORD_POLYTH parameters (thx_info; parse_input sets 1.2, 4) */
   int monopole;             /* 1: self-gravity in the monopole approximation, the
                                GRAV=SPHERICAL_MONOPOLE_GRAV build with GR_MONOPOLE=FALSE
                                (gravity.c:145-425); spherical grids, grav[] all zero */

@@ -108,7 +108,17 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
   if (d.ndim != 1 && d.ndim != 2 && d.ndim != 3) return bad("ndim must be 1, 2 or 3");
   if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
-  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH) return bad("unknown radial map (rcoord)");
+  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH && d.rcoord != MDG_RCOORD_SINH_MODIFIED)
+    return bad("unknown radial map (rcoord)");
+  if (d.thcoord != MDG_THCOORD_UNIFORM && d.thcoord != MDG_THCOORD_POLYTH) return bad("unknown theta map (thcoord)");
+  if (d.thcoord != MDG_THCOORD_UNIFORM) {
+    if (d.geom != MDG_SPHERICAL) return bad("theta maps apply to spherical grids");
+    if (!(d.poly_xt > 0.0 && d.poly_xt < 1.0e300) || !(d.poly_alpha >= 1.0 && d.poly_alpha < 1.0e3))
+      return bad("POLYTH needs poly_xt > 0 and poly_alpha >= 1");
+  }
+  if (d.rcoord == MDG_RCOORD_SINH_MODIFIED &&
+      (!(d.rfact[2] != 0.0) || !std::isfinite(d.rfact[0]) || !std::isfinite(d.rfact[1]) || !std::isfinite(d.rfact[2])))
+    return bad("SINH_MODIFIED needs finite facta, factb and a non-zero factc");
   if (d.monopole != 0 && d.monopole != 1) return bad("monopole must be 0 or 1");
   if (d.monopole) {
     if (d.geom != MDG_SPHERICAL) return bad("monopole gravity needs a spherical grid");
@@ -116,7 +126,7 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
       return bad("monopole and fixed gravity are exclusive (one GRAV switch)");
   }
   if (d.prob_kind < MDG_PROB_NONE || d.prob_kind > MDG_PROB_DUST) return bad("unknown prob_kind");
-  if (d.rcoord == MDG_RCOORD_SINH) {
+  if (d.rcoord != MDG_RCOORD_UNIFORM) {
     if (d.geom != MDG_SPHERICAL) return bad("radial maps apply to spherical grids");
     if (!(d.rtrans > 0.0) || !(d.rtrans < 1.0e300)) return bad("rtrans must be positive and finite");
     if ((d.bc_lo[0] == MDG_BC_PROB || d.bc_hi[0] == MDG_BC_PROB) && d.prob_kind == MDG_PROB_NOH) {
@@ -438,7 +448,8 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].monopole)
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the 1-D mixed-precision sweep has no monopole gravity");
-    if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].rcoord != MDG_RCOORD_UNIFORM)
+    if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 &&
+        (descs[m].rcoord != MDG_RCOORD_UNIFORM || descs[m].thcoord != MDG_THCOORD_UNIFORM))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the 1-D mixed-precision sweep computes the uniform-radius geometry in closed form");
   }

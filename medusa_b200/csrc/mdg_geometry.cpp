@@ -53,42 +53,70 @@ static double romb(double x0, double x1, double (*f)(double))
   return rvec[15];
 }
 
-// The radial map r(x) of the problem being built (RCOORD, metric_spherical_general.c:
-// 149-219): UNIFORM r = |x|, or SINH r = rtrans sinh(|x|/rtrans).  The integrands below
-// are plain functions handed to romb(), so the map is per-thread state that RadialMap
-// sets for the duration of one public build call (the solve server builds tables in the
-// submitting threads).
-static thread_local int t_rcoord = MDG_RCOORD_UNIFORM;
-static thread_local double t_rtrans = 1.0;
+// The coordinate maps of the problem being built (RCOORD and THCOORD,
+// metric_spherical_general.c:149-290): r(x) UNIFORM |x|, SINH rtrans sinh(|x|/rtrans) or
+// SINH_MODIFIED (the SINH map minus a sigmoid step of height facta), th(x) UNIFORM or
+// POLYTH.  The integrands below are plain functions handed to romb(), so the maps are
+// per-thread state that CoordMap sets for the duration of one public build call (the
+// solve server builds tables in the submitting threads).
 namespace {
-struct RadialMap {
-  int rc;
-  double rt;
-  explicit RadialMap(const mdg_problem_desc &d) : rc(t_rcoord), rt(t_rtrans)
+struct MapState {
+  int rcoord = MDG_RCOORD_UNIFORM;
+  double rtrans = 1.0, facta = 0.0, factb = 0.0, factc = 1.0;
+  int thcoord = MDG_THCOORD_UNIFORM;
+  double poly_norm = 0.0, poly_xt = 1.0, poly_alpha = 0.0;
+};
+thread_local MapState t_map;
+struct CoordMap {
+  MapState saved;
+  explicit CoordMap(const mdg_problem_desc &d) : saved(t_map)
   {
-    t_rcoord = d.rcoord;
-    t_rtrans = d.rtrans;
+    t_map.rcoord = d.rcoord;
+    t_map.rtrans = d.rtrans;
+    t_map.facta = d.rfact[0];
+    t_map.factb = d.rfact[1];
+    t_map.factc = d.rfact[2];
+    t_map.thcoord = d.thcoord;
+    t_map.poly_xt = d.poly_xt;
+    t_map.poly_alpha = d.poly_alpha;
+    // init_coords (metric_spherical_general.c:565-567)
+    if (d.thcoord == MDG_THCOORD_POLYTH)
+      t_map.poly_norm = 0.5 * M_PI * 1.0 / (1.0 + 1.0 / (d.poly_alpha + 1.0) * 1.0 / std::pow(d.poly_xt, d.poly_alpha));
   }
-  ~RadialMap()
-  {
-    t_rcoord = rc;
-    t_rtrans = rt;
-  }
+  ~CoordMap() { t_map = saved; }
 };
 }  // namespace
+using RadialMap = CoordMap;
+static double sigmoid(double x) { return 1.0 / (1.0 + std::exp(-x)); }
 static double r_of_x(double x)
 {
-  if (t_rcoord == MDG_RCOORD_SINH) return t_rtrans * std::sinh(std::fabs(x) / t_rtrans);
+  const MapState &m = t_map;
+  if (m.rcoord == MDG_RCOORD_SINH) return m.rtrans * std::sinh(std::fabs(x) / m.rtrans);
+  if (m.rcoord == MDG_RCOORD_SINH_MODIFIED)
+    return m.rtrans * std::sinh(std::fabs(x) / m.rtrans) - m.facta * sigmoid((std::fabs(x) - m.factb) / m.factc) +
+           m.facta * sigmoid(-m.factb / m.factc);
   return std::fabs(x);
 }
 static double dr_dx(double x)
 {
-  if (t_rcoord == MDG_RCOORD_SINH) return std::cosh(std::fabs(x) / t_rtrans);
+  const MapState &m = t_map;
+  if (m.rcoord == MDG_RCOORD_SINH) return std::cosh(std::fabs(x) / m.rtrans);
+  if (m.rcoord == MDG_RCOORD_SINH_MODIFIED) {
+    const double expval = std::exp(-(std::fabs(x) - m.factb) / m.factc);
+    return std::cosh(std::fabs(x) / m.rtrans) - m.facta * expval / m.factc / (1 + expval) / (1 + expval);
+  }
   return 1.0;
 }
 static double d2r_dx2(double x)
 {
-  if (t_rcoord == MDG_RCOORD_SINH) return std::sinh(std::fabs(x) / t_rtrans) / t_rtrans;
+  const MapState &m = t_map;
+  if (m.rcoord == MDG_RCOORD_SINH) return std::sinh(std::fabs(x) / m.rtrans) / m.rtrans;
+  if (m.rcoord == MDG_RCOORD_SINH_MODIFIED) {
+    const double expval = std::exp(-(std::fabs(x) - m.factb) / m.factc);
+    return std::sinh(std::fabs(x) / m.rtrans) / m.rtrans -
+           m.facta / m.factc / m.factc *
+               (2 * expval * expval / (1 + expval) / (1 + expval) / (1 + expval) - expval / (1 + expval) / (1 + expval));
+  }
   return 0.0;
 }
 // v^1 of the two outer ghost zones under the dust-collapse boundary hook
@@ -119,15 +147,33 @@ double radial_coordinate(const mdg_problem_desc &d, double x)
   RadialMap rmap(d);
   return r_of_x(x);
 }
-// uniform theta (THCOORD=UNIFORM) and the integrands of the spherical metric
+// theta map with the reflection about the polar axis (metric_spherical_general.c:222-290)
 static double th_of_x(double x)
 {
   if (x < -1.0) x = -2.0 - x;
   if (x > 1.0) x = 2.0 - x;
+  const MapState &m = t_map;
+  if (m.thcoord == MDG_THCOORD_POLYTH)
+    return m.poly_norm * x * (1.0 + std::pow(x / m.poly_xt, m.poly_alpha) / (m.poly_alpha + 1.0)) + 0.5 * M_PI;
   return 0.5 * M_PI * (x + 1.0);
 }
-static double dth_dx(double) { return 0.5 * M_PI; }
-static double d2th_dx2(double) { return 0.0; }
+static double dth_dx(double x)
+{
+  if (x < -1.0) x = -2.0 - x;
+  if (x > 1.0) x = 2.0 - x;
+  const MapState &m = t_map;
+  if (m.thcoord == MDG_THCOORD_POLYTH) return m.poly_norm * (1.0 + std::pow(x / m.poly_xt, m.poly_alpha));
+  return 0.5 * M_PI;
+}
+static double d2th_dx2(double x)
+{
+  if (x < -1.0) x = -2.0 - x;
+  if (x > 1.0) x = 2.0 - x;
+  const MapState &m = t_map;
+  if (m.thcoord == MDG_THCOORD_POLYTH)
+    return m.poly_norm * m.poly_alpha * std::pow(x / m.poly_xt, m.poly_alpha - 1.0) / m.poly_xt;
+  return 0.0;
+}
 static double f_r2dr_dx(double x) { return std::pow(r_of_x(x), 2) * dr_dx(x); }
 static double f_xr1g(double x) { return x * std::pow(r_of_x(x), 2) * dr_dx(x); }
 static double f_xr2g(double x) { return x * x * std::pow(r_of_x(x), 2) * dr_dx(x); }

@@ -96,11 +96,16 @@ int check_desc(const mdg_problem_desc &d)
   if (!lo_ok || !hi_ok) return fail(MDG_ERR_NOTIMPL, "mdg_advance_1d_noalloc: boundary kinds");
   if ((lo == MDG_BC_PERIODIC) != (hi == MDG_BC_PERIODIC))
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: periodic boundaries must be paired");
-  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH)
+  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH && d.rcoord != MDG_RCOORD_SINH_MODIFIED)
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: rcoord");
+  if (d.thcoord != MDG_THCOORD_UNIFORM && (d.thcoord != MDG_THCOORD_POLYTH || !sph || !(d.poly_xt > 0.0) ||
+                                           !(d.poly_alpha >= 1.0)))
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: thcoord");
+  if (d.rcoord == MDG_RCOORD_SINH_MODIFIED && !(d.rfact[2] != 0.0))
+    return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: factc");
   if (d.monopole != 0 || d.prob_kind == MDG_PROB_DUST)
     return fail(MDG_ERR_NOTIMPL, "mdg_advance_1d_noalloc: monopole gravity and the dust-collapse hook are not built here");
-  if (d.rcoord == MDG_RCOORD_SINH && (!sph || !(d.rtrans > 0.0) || lo == MDG_BC_PROB || hi == MDG_BC_PROB))
+  if (d.rcoord != MDG_RCOORD_UNIFORM && (!sph || !(d.rtrans > 0.0) || lo == MDG_BC_PROB || hi == MDG_BC_PROB))
     return fail(MDG_ERR_INVALID, "mdg_advance_1d_noalloc: the SINH radial map needs a spherical grid, rtrans > 0 "
                                  "and no PROB boundary");
   return MDG_OK;

@@ -801,8 +801,8 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
       return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep is built for parabolic reconstruction");
     if (desc->geom == MDG_SPHERICAL && !(desc->startx[0] >= 0.0))
       return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep needs a spherical grid starting at r >= 0");
-    if (desc->rcoord != MDG_RCOORD_UNIFORM)
-      return sfail(MDG_ERR_NOTIMPL, "request: the 1-D mixed-precision sweep is built for the uniform radial map");
+    if (desc->rcoord != MDG_RCOORD_UNIFORM || desc->thcoord != MDG_THCOORD_UNIFORM)
+      return sfail(MDG_ERR_NOTIMPL, "request: the 1-D mixed-precision sweep is built for the uniform coordinate maps");
   }
   Request *r = new Request();
   r->desc = *desc;

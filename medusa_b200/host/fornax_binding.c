@@ -94,10 +94,22 @@ static void describe(mdg_problem_desc *d)
 #endif
 #if (GEOM == SPHERICAL && RCOORD == SINH)
   d->rcoord = MDG_RCOORD_SINH;
+#elif (GEOM == SPHERICAL && RCOORD == SINH_MODIFIED)
+  d->rcoord = MDG_RCOORD_SINH_MODIFIED;
 #else
   d->rcoord = MDG_RCOORD_UNIFORM;
 #endif
   d->rtrans = rx_info.rtrans;
+  d->rfact[0] = rx_info.facta;
+  d->rfact[1] = rx_info.factb;
+  d->rfact[2] = rx_info.factc;
+#if (GEOM == SPHERICAL && THCOORD == POLYTH)
+  d->thcoord = MDG_THCOORD_POLYTH;
+#else
+  d->thcoord = MDG_THCOORD_UNIFORM;
+#endif
+  d->poly_xt = thx_info.poly_xt;
+  d->poly_alpha = thx_info.poly_alpha;
 }
 
 static void attach(void)

@@ -40,6 +40,11 @@ PROB_DUST = 2               # problems/init_dustcollapse.c:104-113 (outer v^r ho
 
 RCOORD_UNIFORM = 0          # radial maps r(x), metric_spherical_general.c:149-219
 RCOORD_SINH = 1
+RCOORD_SINH_MODIFIED = 2
+THCOORD_UNIFORM = 0         # theta maps th(x), metric_spherical_general.c:222-290
+THCOORD_POLYTH = 1
+RFACT_DEFAULT = (10 * 1e5, 15 * 1e5, 5 * 1e5)   # rx_info.facta/b/c, io.c:5008-5010
+POLY_XT_DEFAULT, POLY_ALPHA_DEFAULT = 1.2, 4.0  # thx_info, io.c:5014-5015
 
 NG = 2
 NPRIM = 5
@@ -69,7 +74,11 @@ class Problem:
     dtmin: float = 1.0e-200       # io.c:5038
     tmax: float = 1.0e100
     rcoord: int = RCOORD_UNIFORM  # radial map of a spherical grid (the RCOORD build switch)
-    rtrans: float = 1.0           # its transition radius (RCOORD_SINH)
+    rtrans: float = 1.0           # its transition radius (RCOORD_SINH, RCOORD_SINH_MODIFIED)
+    rfact: tuple = RFACT_DEFAULT  # facta, factb, factc of RCOORD_SINH_MODIFIED
+    thcoord: int = THCOORD_UNIFORM  # theta map of a spherical grid (the THCOORD build switch)
+    poly_xt: float = POLY_XT_DEFAULT
+    poly_alpha: float = POLY_ALPHA_DEFAULT
     monopole: int = 0             # self-gravity, monopole approximation (GRAV=SPHERICAL_MONOPOLE_GRAV)
     hydro_interp_order: int = 3   # io.c:5055
     enforce_floors: int = 0       # ENFORCE_FLOORS build switch (fluid.c:43-46)
@@ -219,7 +228,8 @@ def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240
 
 def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                  p_ratio: float = 100.0, r0: float = 0.5, cfl: float = 0.8,
-                 tmax: float = 1.0e100, floors: bool = True, dr_min: Optional[float] = None) -> Problem:
+                 tmax: float = 1.0e100, floors: bool = True, dr_min: Optional[float] = None,
+                 coords: str = "sinh") -> Problem:
     """1-D spherical problem on r in [0,1] (uniform radius; with dr_min the SINH radial
     map, innermost zones dr_min wide), SPHERICAL_ORIGIN inner boundary (bc.c:776-803).
 
@@ -232,8 +242,8 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                    the hook's floors rho 1e-6, e 1e-7/(gam-1) (init_spherical_noh.c:22-23),
                    enforced (ENFORCE_FLOORS) unless floors=False.
     """
-    _, dx, map_ = _radial_grid(n1, dr_min)
-    rc = np.array([_r_of_x((i + 0.5) * dx, map_.get("rtrans")) for i in range(n1)])
+    _, dx, map_ = _radial_grid(n1, dr_min, coords)
+    rc = np.array([_maps(map_).r((i + 0.5) * dx) for i in range(n1)])
     ic = np.zeros((n1, NPRIM))
     bc_hi = OUTFLOW
     prob_kind = PROB_NONE
@@ -261,13 +271,50 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
             fl = dict(enforce_floors=1, rho_floor=1.0e-6, e_floor=1.0e-7 / (gam - 1.0))
     else:
         raise ValueError("unknown 1-D spherical problem kind %r" % kind)
-    return Problem(name="sph1d_%s%s_%d" % ("sinh_" if map_ else "", kind, n1), ndim=1, geom=SPHERICAL,
+    return Problem(name="sph1d_%s%s_%d" % (_map_tag(map_), kind, n1), ndim=1, geom=SPHERICAL,
                    n=(n1, 1, 1), startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
                    bc_lo=(SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW), bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
                    prob_kind=prob_kind, cfl=cfl, tmax=tmax, **fl, **map_)
 
 
 MAX_LOG2_ASPECT = 0.5   # utils.c:12
+
+
+class CoordMaps:
+    """The radial and theta maps r(x), th(x) of a spherical grid (RCOORD and THCOORD,
+    metric_spherical_general.c:149-290), restated for the grid counts and the problem
+    generators (the library evaluates its own copy)."""
+
+    def __init__(self, rcoord=RCOORD_UNIFORM, rtrans=1.0, rfact=RFACT_DEFAULT, thcoord=THCOORD_UNIFORM,
+                 poly_xt=POLY_XT_DEFAULT, poly_alpha=POLY_ALPHA_DEFAULT):
+        self.rcoord, self.rtrans, self.rfact = rcoord, rtrans, tuple(rfact)
+        self.thcoord, self.poly_xt, self.poly_alpha = thcoord, poly_xt, poly_alpha
+        # init_coords (metric_spherical_general.c:565-567)
+        self.poly_norm = 0.5 * math.pi * 1.0 / (1.0 + 1.0 / (poly_alpha + 1.0) * 1.0 / math.pow(poly_xt, poly_alpha))
+
+    @classmethod
+    def of(cls, pb):
+        return cls(pb.rcoord, pb.rtrans, pb.rfact, pb.thcoord, pb.poly_xt, pb.poly_alpha)
+
+    def r(self, x: float) -> float:
+        ax = abs(x)
+        if self.rcoord == RCOORD_SINH:
+            return self.rtrans * math.sinh(ax / self.rtrans)
+        if self.rcoord == RCOORD_SINH_MODIFIED:
+            fa, fb, fc = self.rfact
+            sig = lambda y: 1.0 / (1.0 + math.exp(-y))
+            return self.rtrans * math.sinh(ax / self.rtrans) - fa * sig((ax - fb) / fc) + fa * sig(-fb / fc)
+        return ax
+
+    def th(self, x: float) -> float:
+        if x < -1.0:
+            x = -2.0 - x
+        if x > 1.0:
+            x = 2.0 - x
+        if self.thcoord == THCOORD_POLYTH:
+            return self.poly_norm * x * (1.0 + math.pow(x / self.poly_xt, self.poly_alpha) /
+                                         (self.poly_alpha + 1.0)) + 0.5 * math.pi
+        return 0.5 * math.pi * (x + 1.0)
 
 
 def _r_of_x(x: float, rtrans: Optional[float] = None) -> float:
@@ -278,24 +325,28 @@ def _r_of_x(x: float, rtrans: Optional[float] = None) -> float:
     return rtrans * math.sinh(abs(x) / rtrans)
 
 
-def sinh_rtrans(n1: int, dx0: float, r_out: float) -> float:
-    """Transition radius of the SINH map whose n1 zones of coordinate width dx0 reach
-    r_out: the root of rtrans sinh(n1 dx0 / rtrans) = r_out, by bracketing and bisection
-    to a relative width of 1e-10 (the method of rtrans_solve, metric_spherical_general.c:
-    16-78, which the reference's problem hooks call, e.g. problems/init_sedov.c:20).  Needs
-    r_out > n1 dx0 (the map only stretches).  The zones then start dx0 wide at the centre
-    and widen geometrically outside r ~ rtrans."""
+def sinh_rtrans(n1: int, dx0: float, r_out: float, rcoord: int = RCOORD_SINH,
+                rfact: tuple = RFACT_DEFAULT) -> float:
+    """Transition radius of the SINH (or SINH_MODIFIED) map whose n1 zones of coordinate
+    width dx0 reach r_out: the root of r(n1 dx0) = r_out, by bracketing and bisection to a
+    relative width of 1e-10 (the method of rtrans_solve, metric_spherical_general.c:16-78,
+    which the reference's problem hooks call, e.g. problems/init_sedov.c:20).  Needs a map
+    that stretches to r_out.  The zones then start about dx0 wide at the centre and widen
+    geometrically outside r ~ rtrans."""
     X = n1 * dx0
-    if not r_out > X:
-        raise ValueError("the SINH map needs r_out > n1*dx0")
-    f = lambda rt: rt * math.sinh(X / rt) - r_out if X / rt < 700.0 else math.inf
+
+    def f(rt):
+        if X / rt >= 700.0:
+            return math.inf
+        return CoordMaps(rcoord, rt, rfact).r(X) - r_out
+
     lo = 0.1 * dx0
     while not math.isfinite(f(lo)):
         lo *= 1.1
     hi = 100.0 * r_out
     flo = f(lo)
     if flo * f(hi) > 0.0:
-        raise ValueError("rtrans not bracketed")
+        raise ValueError("rtrans not bracketed: the map does not reach r_out")
     while abs((lo - hi) / hi) > 1.0e-10:
         mid = 0.5 * (lo + hi)
         fm = f(mid)
@@ -308,40 +359,36 @@ def sinh_rtrans(n1: int, dx0: float, r_out: float) -> float:
 
 def radial_edges(pb: Problem) -> np.ndarray:
     """r at the n1+1 radial zone edges of a spherical problem (its radial map)."""
-    rt = pb.rtrans if pb.rcoord == RCOORD_SINH else None
-    return np.array([_r_of_x(pb.startx[0] + i * pb.dx[0], rt) for i in range(pb.n[0] + 1)])
+    m = CoordMaps.of(pb)
+    return np.array([m.r(pb.startx[0] + i * pb.dx[0]) for i in range(pb.n[0] + 1)])
 
 
 def radial_centers(pb: Problem) -> np.ndarray:
     """r at the n1 radial zone centres (ijk_to_x then r_of_x, as the dumps place them)."""
-    rt = pb.rtrans if pb.rcoord == RCOORD_SINH else None
-    return np.array([_r_of_x(pb.startx[0] + (i + 0.5) * pb.dx[0], rt) for i in range(pb.n[0])])
-
-
-def _th_of_x(x: float) -> float:
-    if x < -1.0:
-        x = -2.0 - x
-    if x > 1.0:
-        x = 2.0 - x
-    return 0.5 * math.pi * (x + 1.0)    # THCOORD=UNIFORM, metric_spherical_general.c:222-230
+    m = CoordMaps.of(pb)
+    return np.array([m.r(pb.startx[0] + (i + 0.5) * pb.dx[0]) for i in range(pb.n[0])])
 
 
 def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: int = 3,
-                   rtrans: Optional[float] = None):
+                   rtrans: Optional[float] = None, maps: Optional[CoordMaps] = None):
     """Zone counts of the dendritic spherical grid: nj[i] theta zones of radial row i and
     nk[i][j] phi zones of row (i, j), for the interior rows (the rules of compute_dj and
     compute_dk, utils.c:181-354, for a uniform radius and theta: theta zones double
     outwards from 2 at the centre and phi zones from 4 at each pole while the zone aspect
     ratio exceeds 2^0.5; on a 2-D grid every row has n3 = 1 phi zone; rtrans selects the
-    SINH radial map).  Returns (nj, nk) as lists; the interior zones in the reference's
-    zone order are i, then j < nj[i], then k < nk[i][j]."""
+    SINH radial map, maps any pair of coordinate maps).  Returns (nj, nk) as lists; the
+    interior zones in the reference's zone order are i, then j < nj[i], then k < nk[i][j]."""
+    if maps is None:
+        maps = CoordMaps(RCOORD_SINH, rtrans) if rtrans is not None else CoordMaps()
+    _r_of = maps.r
+    _th_of = maps.th
     nj = [0] * n1
     nj[0] = 2
-    dth = _th_of_x(startx[1] + n2 * dx[1]) - _th_of_x(startx[1])
+    dth = _th_of(startx[1] + n2 * dx[1]) - _th_of(startx[1])
     for i in range(1, n1):
-        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0], rtrans)
-        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0], rtrans)
-        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0], rtrans)
+        r0 = _r_of(startx[0] + (i + 0.0) * dx[0])
+        rc = _r_of(startx[0] + (i + 0.5) * dx[0])
+        r1 = _r_of(startx[0] + (i + 1.0) * dx[0])
         ideal = rc * dth / (r1 - r0)
         nj[i] = nj[i - 1]
         if math.log2(ideal / nj[i]) > MAX_LOG2_ASPECT:
@@ -353,14 +400,14 @@ def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: in
     dph = n3 * dx[2]
     nk = []
     for i in range(n1):
-        r0 = _r_of_x(startx[0] + (i + 0.0) * dx[0], rtrans)
-        rc = _r_of_x(startx[0] + (i + 0.5) * dx[0], rtrans)
-        r1 = _r_of_x(startx[0] + (i + 1.0) * dx[0], rtrans)
+        r0 = _r_of(startx[0] + (i + 0.0) * dx[0])
+        rc = _r_of(startx[0] + (i + 0.5) * dx[0])
+        r1 = _r_of(startx[0] + (i + 1.0) * dx[0])
         dr = r1 - r0
         row = [0] * nj[i]
         row[0] = 4
         for j in range(1, nj[i]):
-            thc = _th_of_x(startx[1] + (j + 0.5) * dj[i] * dx[1])
+            thc = _th_of(startx[1] + (j + 0.5) * dj[i] * dx[1])
             ideal = rc * math.sin(thc) * dph / dr
             if j < nj[i] // 2:
                 row[j] = row[j - 1]
@@ -378,24 +425,40 @@ def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: in
     return nj, nk
 
 
-def _radial_grid(n1: int, dr_min: Optional[float]):
-    """(startx, dx0, map fields) of a radial grid on r in [0, 1]: uniform, or the SINH map
-    with innermost zones dr_min wide."""
+def _radial_grid(n1: int, dr_min: Optional[float], coords: str = "sinh"):
+    """(startx, dx0, map fields) of a radial grid on r in [0, 1]: uniform, or with dr_min
+    the SINH map with innermost zones about dr_min wide (coords "sinh"), or the
+    reference's default build maps, SINH_MODIFIED radius and POLYTH theta with the
+    parse_input parameters (coords "default")."""
     startx = (0.0, -1.0, 0.0)
     if dr_min is None:
         return startx, 1.0 / n1, {}
+    if coords == "default":
+        rt = sinh_rtrans(n1, dr_min, 1.0, RCOORD_SINH_MODIFIED)
+        return startx, dr_min, dict(rcoord=RCOORD_SINH_MODIFIED, rtrans=rt, thcoord=THCOORD_POLYTH)
     return startx, dr_min, dict(rcoord=RCOORD_SINH, rtrans=sinh_rtrans(n1, dr_min, 1.0))
+
+
+def _maps(map_: dict) -> CoordMaps:
+    return CoordMaps(map_.get("rcoord", RCOORD_UNIFORM), map_.get("rtrans", 1.0), RFACT_DEFAULT,
+                     map_.get("thcoord", THCOORD_UNIFORM))
+
+
+def _map_tag(map_: dict) -> str:
+    if not map_:
+        return ""
+    return "default_" if map_.get("thcoord", THCOORD_UNIFORM) == THCOORD_POLYTH else "sinh_"
 
 
 def _blast_energy_rows(n1, startx, dx0, map_, r_dep, energy, gam, p_amb) -> np.ndarray:
     """Internal energy density per radial row of a blast: energy / (4/3 pi r_e^3) in the
     rows whose centre lies inside r_dep (r_e the outer edge of the last of them), the
     ambient p_amb / (gam - 1) elsewhere."""
-    rt = map_.get("rtrans")
-    rc = np.array([_r_of_x(startx[0] + (i + 0.5) * dx0, rt) for i in range(n1)])
+    m = _maps(map_)
+    rc = np.array([m.r(startx[0] + (i + 0.5) * dx0) for i in range(n1)])
     inside = rc < r_dep
     i_e = (np.nonzero(inside)[0].max() + 1) if inside.any() else 1
-    r_e = _r_of_x(startx[0] + i_e * dx0, rt)
+    r_e = m.r(startx[0] + i_e * dx0)
     u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
     return np.where(inside, u_dep, p_amb / (gam - 1.0))
 
@@ -403,7 +466,7 @@ def _blast_energy_rows(n1, startx, dx0, map_, r_dep, energy, gam, p_amb) -> np.n
 def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, energy: float = 1.0,
              r_dep: float = 0.02, p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100,
              bc_inner: int = REFLECT, bc_pole: int = REFLECT, noise: float = 0.0,
-             seed: int = 20240603, dr_min: Optional[float] = None) -> Problem:
+             seed: int = 20240603, dr_min: Optional[float] = None, coords: str = "sinh") -> Problem:
     """3-D Sedov blast on the dendritic spherical grid (the structure of
     problems/init_sedov.c:3-164): r in [0, 1] uniform, theta in [0, pi], phi in [0, 2 pi);
     rho = 1, p = p_amb, at rest, and the energy `energy` deposited as a uniform internal
@@ -414,10 +477,11 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
     the symmetry (shock tagging, rotation through the pole rows, restriction of v^phi).
     With dr_min the radius follows the SINH map instead (RCOORD=SINH, the map of the
     reference's own Sedov hook): the innermost zones are dr_min wide and the zone widths
-    grow geometrically outwards to r = 1."""
-    startx, dx, map_ = _radial_grid(n1, dr_min)
+    grow geometrically outwards to r = 1 (coords "default": the reference's default
+    build maps, SINH_MODIFIED radius and POLYTH theta)."""
+    startx, dx, map_ = _radial_grid(n1, dr_min, coords)
     dx = (dx, 2.0 / n2, 2.0 * math.pi / n3)
-    nj, nk = dendritic_grid(n1, n2, n3, startx, dx, rtrans=map_.get("rtrans"))
+    nj, nk = dendritic_grid(n1, n2, n3, startx, dx, maps=_maps(map_))
     counts = np.array([sum(row) for row in nk])
     ncell = int(counts.sum())
     u_row = _blast_energy_rows(n1, startx, dx[0], map_, r_dep, energy, gam, p_amb)
@@ -429,7 +493,7 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
         ic[:, 0] *= 1.0 + noise * (2.0 * u[:, 0] - 1.0)
         for v in range(3):
             ic[:, 2 + v] = 0.1 * noise * (2.0 * u[:, 1 + v] - 1.0)
-    return Problem(name="sedov3d_%s%dx%dx%d" % ("sinh_" if map_ else "", n1, n2, n3), ndim=3, geom=SPHERICAL,
+    return Problem(name="sedov3d_%s%dx%dx%d" % (_map_tag(map_), n1, n2, n3), ndim=3, geom=SPHERICAL,
                    n=(n1, n2, n3), startx=startx, dx=dx, gam=gam, ic=ic,
                    bc_lo=(bc_inner, bc_pole, PERIODIC), bc_hi=(OUTFLOW, bc_pole, PERIODIC),
                    cfl=cfl, tmax=tmax, cells=ncell, **map_)
@@ -438,14 +502,14 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
 def sedov_2d_spherical(n1: int = 256, n2: int = 128, gam: float = 1.4, energy: float = 1.0, r_dep: float = 0.02,
                        p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100, bc_inner: int = REFLECT,
                        bc_pole: int = REFLECT, noise: float = 0.0, seed: int = 20240604,
-                       dr_min: Optional[float] = None) -> Problem:
+                       dr_min: Optional[float] = None, coords: str = "sinh") -> Problem:
     """Axisymmetric (r, theta) Sedov blast on the 2-D dendritic spherical grid: theta zones
     double outwards from 2 at the centre (compute_dj, utils.c:181-238); otherwise as
     sedov_3d (energy in the zones inside r_dep, seeded noise in density and velocities,
-    the SINH radial map with dr_min)."""
-    startx, dx, map_ = _radial_grid(n1, dr_min)
+    the SINH radial map with dr_min, the default build maps with coords "default")."""
+    startx, dx, map_ = _radial_grid(n1, dr_min, coords)
     dx = (dx, 2.0 / n2, 2.0 * math.pi)
-    nj, _ = dendritic_grid(n1, n2, 1, startx, dx, ndim=2, rtrans=map_.get("rtrans"))
+    nj, _ = dendritic_grid(n1, n2, 1, startx, dx, ndim=2, maps=_maps(map_))
     ncell = int(sum(nj))
     ic = np.zeros((ncell, NPRIM))
     ic[:, 0] = 1.0
@@ -455,7 +519,7 @@ def sedov_2d_spherical(n1: int = 256, n2: int = 128, gam: float = 1.4, energy: f
         ic[:, 0] *= 1.0 + noise * (2.0 * u[:, 0] - 1.0)
         for v in range(3):
             ic[:, 2 + v] = 0.1 * noise * (2.0 * u[:, 1 + v] - 1.0)
-    return Problem(name="sedov2dsph_%s%dx%d" % ("sinh_" if map_ else "", n1, n2), ndim=2, geom=SPHERICAL,
+    return Problem(name="sedov2dsph_%s%dx%d" % (_map_tag(map_), n1, n2), ndim=2, geom=SPHERICAL,
                    n=(n1, n2, 1), startx=startx, dx=dx, gam=gam, ic=ic, bc_lo=(bc_inner, bc_pole, PERIODIC),
                    bc_hi=(OUTFLOW, bc_pole, PERIODIC), cfl=cfl, tmax=tmax, cells=ncell, **map_)
 

@@ -82,7 +82,8 @@ class ProblemDesc(ctypes.Structure):
                 ("hydro_interp_order", ctypes.c_int),
                 ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double), ("e_floor", ctypes.c_double),
                 ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int), ("rtrans", ctypes.c_double),
-                ("monopole", ctypes.c_int)]
+                ("rfact", ctypes.c_double * 3), ("thcoord", ctypes.c_int), ("poly_xt", ctypes.c_double),
+                ("poly_alpha", ctypes.c_double), ("monopole", ctypes.c_int)]
 
 
 def desc_of(pb: "_pb.Problem") -> ProblemDesc:
@@ -102,6 +103,9 @@ def desc_of(pb: "_pb.Problem") -> ProblemDesc:
     for k in range(3):
         d.grav[k] = pb.grav[k]
     d.rcoord, d.rtrans = pb.rcoord, pb.rtrans
+    for k in range(3):
+        d.rfact[k] = pb.rfact[k]
+    d.thcoord, d.poly_xt, d.poly_alpha = pb.thcoord, pb.poly_xt, pb.poly_alpha
     d.monopole = int(pb.monopole)
     return d
 

@@ -83,6 +83,14 @@ CONFIGS = {
                        RCOORD="SINH", THCOORD="UNIFORM"),
     "sph3d_sinh": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
                        RCOORD="SINH", THCOORD="UNIFORM"),
+    # the reference's default coordinate maps (Makefile:26-27: RCOORD=SINH_MODIFIED,
+    # THCOORD=POLYTH), which every setup that does not override them runs with
+    "sph1d_default": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                          RCOORD="SINH_MODIFIED", THCOORD="POLYTH"),
+    "sph2d_default": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                          RCOORD="SINH_MODIFIED", THCOORD="POLYTH"),
+    "sph3d_default": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                          RCOORD="SINH_MODIFIED", THCOORD="POLYTH"),
     # self-gravity in the monopole approximation (GRAV=SPHERICAL_MONOPOLE_GRAV,
     # GR_MONOPOLE=FALSE; setups/dustcollapse_1d.mk): 1-D on the SINH radius with floors,
     # and the dendritic grids

@@ -93,6 +93,9 @@ typedef struct {
   double rho_floor, e_floor;
   double grav[3];
   int rcoord;          /* radial map: 0 UNIFORM, 1 SINH (the RCOORD build switch) */
+  double rfact[3];     /* SINH_MODIFIED parameters: not restated here (the reference's own builds check it) */
+  int thcoord;         /* theta map: 0 UNIFORM only here */
+  double poly_xt, poly_alpha;
 } orc_params;
 
 typedef struct {

@@ -40,7 +40,9 @@ class Params(ctypes.Structure):
                 ("dtmin", ctypes.c_double), ("tmax", ctypes.c_double),
                 ("rtrans", ctypes.c_double), ("hydro_interp_order", ctypes.c_int),
                 ("enforce_floors", ctypes.c_int), ("rho_floor", ctypes.c_double),
-                ("e_floor", ctypes.c_double), ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int)]
+                ("e_floor", ctypes.c_double), ("grav", ctypes.c_double * 3), ("rcoord", ctypes.c_int),
+                ("rfact", ctypes.c_double * 3), ("thcoord", ctypes.c_int), ("poly_xt", ctypes.c_double),
+                ("poly_alpha", ctypes.c_double)]
 
 
 def params_of(pb) -> Params:
@@ -63,6 +65,11 @@ def params_of(pb) -> Params:
     for d in range(3):
         p.grav[d] = getattr(pb, "grav", (0.0, 0.0, 0.0))[d]
     p.rcoord = int(getattr(pb, "rcoord", 0))
+    for d in range(3):
+        p.rfact[d] = getattr(pb, "rfact", (1.0e6, 1.5e6, 5.0e5))[d]
+    p.thcoord = int(getattr(pb, "thcoord", 0))
+    p.poly_xt = getattr(pb, "poly_xt", 1.2)
+    p.poly_alpha = getattr(pb, "poly_alpha", 4.0)
     return p
 
 
@@ -168,6 +175,8 @@ def ref_config(pb) -> str:
     name = ("cart%dd" if pb.geom == 0 else "sph%dd") % pb.ndim
     if getattr(pb, "rcoord", 0) == 1:
         name += "_sinh"
+    elif getattr(pb, "rcoord", 0) == 2 and getattr(pb, "thcoord", 0) == 1:
+        name += "_default"
     if any(g != 0.0 for g in getattr(pb, "grav", (0.0, 0.0, 0.0))):
         name += "_grav"
     if getattr(pb, "monopole", 0):

@@ -46,6 +46,9 @@ typedef struct {
   double rho_floor, e_floor;
   double grav[3];     /* fixed gravitational acceleration g0 (GRAV=FIXED_GRAV builds) */
   int rcoord;         /* radial map; must match the RCOORD of the build (rtrans above) */
+  double rfact[3];    /* rx_info.facta/b/c (SINH_MODIFIED) */
+  int thcoord;        /* theta map; must match the THCOORD of the build */
+  double poly_xt, poly_alpha;   /* thx_info (POLYTH) */
 } ref_params;
 
 static ref_params g_prm;
@@ -167,17 +170,24 @@ REF_API int ref_init(const ref_params *prm, const double *ic)
   g_ic = ic;
 #if (RCOORD == SINH)
   if (prm->rcoord != 1) { fprintf(stderr, "ref_init: this build has the SINH radial map\n"); return -1; }
+#elif (RCOORD == SINH_MODIFIED)
+  if (prm->rcoord != 2) { fprintf(stderr, "ref_init: this build has the SINH_MODIFIED radial map\n"); return -1; }
 #else
   if (prm->rcoord != 0) { fprintf(stderr, "ref_init: this build has the uniform radial map\n"); return -1; }
 #endif
+#if (THCOORD == POLYTH)
+  if (prm->thcoord != 1) { fprintf(stderr, "ref_init: this build has the POLYTH theta map\n"); return -1; }
+#else
+  if (prm->thcoord != 0) { fprintf(stderr, "ref_init: this build has the uniform theta map\n"); return -1; }
+#endif
 
   /* parse_input defaults, io.c:5000-5117, then the keys this build sets */
-  rx_info.facta = 10*1e5;
-  rx_info.factb = 15*1e5;
-  rx_info.factc = 5*1e5;
+  rx_info.facta = prm->rfact[0];       /* io.c:5008-5010 defaults 1e6, 1.5e6, 5e5 */
+  rx_info.factb = prm->rfact[1];
+  rx_info.factc = prm->rfact[2];
   thx_info.nice_alpha = 1.01;
-  thx_info.poly_xt = 1.2;
-  thx_info.poly_alpha = 4;
+  thx_info.poly_xt = prm->poly_xt;      /* io.c:5014-5015 defaults 1.2, 4 */
+  thx_info.poly_alpha = prm->poly_alpha;
   Nskip = 1;
   n1 = prm->n1; n2 = prm->n2; n3 = prm->n3;
   cfl = prm->cfl;

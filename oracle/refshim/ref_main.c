@@ -41,6 +41,9 @@ typedef struct {
   double rho_floor, e_floor;
   double grav[3];
   int rcoord;
+  double rfact[3];
+  int thcoord;
+  double poly_xt, poly_alpha;
 } ref_params;
 
 int ref_init(const ref_params *prm, const double *ic);

@@ -59,6 +59,13 @@ def cases3d():
         # the SINH radial map on both dendritic grids
         "sedov3d_sinh_24x16x32": (P.sedov_3d(24, 16, 32, r_dep=0.2, dr_min=0.02), 30),
         "sedov2dsph_sinh_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.15, noise=0.05, dr_min=0.01), 40),
+        # the reference's default build maps (SINH_MODIFIED radius, POLYTH theta); the 1-D
+        # case is here because the C restatement covers the uniform and SINH maps only
+        "sedov3d_default_24x16x32": (P.sedov_3d(24, 16, 32, r_dep=0.2, dr_min=0.02, coords="default"), 30),
+        "sedov2dsph_default_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.15, noise=0.05, dr_min=0.01,
+                                                                coords="default"), 40),
+        "sph1d_default_sedov_192": (P.spherical_1d("sedov", 192, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3,
+                                                   coords="default"), 60),
     }
 
 

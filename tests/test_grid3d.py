@@ -48,11 +48,14 @@ def test_c3_grid_size():
     assert n == pb.ncell < 384 * 128 * 256
 
 
-@pytest.mark.parametrize("dims,dr_min", [((24, 16, 32), None), ((40, 32, 64), None), ((48, 64, 128), None),
-                                         ((24, 16, 32), 0.02), ((48, 32, 64), 0.01)])
-def test_geometry_bit_identical_to_reference(dims, dr_min):
-    """Uniform radius and the SINH radial map (against the reference's RCOORD=SINH build)."""
-    pb = P.sedov_3d(*dims, r_dep=0.2, dr_min=dr_min)
+@pytest.mark.parametrize("dims,dr_min,coords", [((24, 16, 32), None, "sinh"), ((40, 32, 64), None, "sinh"),
+                                                ((48, 64, 128), None, "sinh"), ((24, 16, 32), 0.02, "sinh"),
+                                                ((48, 32, 64), 0.01, "sinh"), ((24, 16, 32), 0.02, "default"),
+                                                ((48, 32, 64), 0.01, "default")])
+def test_geometry_bit_identical_to_reference(dims, dr_min, coords):
+    """Uniform radius, the SINH radial map (against the reference's RCOORD=SINH build) and
+    the default build maps SINH_MODIFIED + POLYTH."""
+    pb = P.sedov_3d(*dims, r_dep=0.2, dr_min=dr_min, coords=coords)
     if not pyoracle.ref_available(pb):
         pytest.skip("oracle/_ref not built (needs the reference tree)")
     rnj, _ = pyoracle.reference_grid(pb)
@@ -85,9 +88,11 @@ def test_2d_zone_counts_match_restatement(dims):
 
 
 # the NDIM=2 record of ref_get_geom: vol, area[2], gcov[3][3], gcon[3], scale[3][3], conn[27]
-@pytest.mark.parametrize("dims,dr_min", [((24, 16), None), ((48, 32), None), ((40, 64), None), ((40, 32), 0.01)])
-def test_2d_geometry_bit_identical_to_reference(dims, dr_min):
-    pb = P.sedov_2d_spherical(*dims, r_dep=0.2, dr_min=dr_min)
+@pytest.mark.parametrize("dims,dr_min,coords", [((24, 16), None, "sinh"), ((48, 32), None, "sinh"),
+                                                ((40, 64), None, "sinh"), ((40, 32), 0.01, "sinh"),
+                                                ((40, 32), 0.01, "default")])
+def test_2d_geometry_bit_identical_to_reference(dims, dr_min, coords):
+    pb = P.sedov_2d_spherical(*dims, r_dep=0.2, dr_min=dr_min, coords=coords)
     if not pyoracle.ref_available(pb):
         pytest.skip("oracle/_ref not built (needs the reference tree)")
     rnj, _ = pyoracle.reference_grid(pb)
