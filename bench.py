@@ -132,7 +132,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(backend=None):
+    """(world, rank, local rank, torch.distributed or None) from the torchrun environment;
+    NCCL by default (MDG_DIST_BACKEND=gloo runs the same rank logic on CPU)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -140,13 +142,15 @@ def dist_setup():
         import datetime
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=None)
+        backend = backend or os.environ.get("MDG_DIST_BACKEND", "nccl")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
         return world, rank, local, dist
     return 1, 0, 0, None
 
 
 class Ctx:
-    """Rank bookkeeping: barrier and max over ranks of a device time."""
+    """Rank bookkeeping: barrier, max over ranks of a device time and sums of the units
+    each rank processed (every rank calls these in the same order)."""
 
     def __init__(self, world, rank, local, dist):
         self.world, self.rank, self.local, self.dist = world, rank, local, dist
@@ -155,13 +159,23 @@ class Ctx:
         if self.dist is not None:
             self.dist.barrier()
 
+    def _reduce(self, x, op):
+        import torch
+        dev = "cuda" if self.dist.get_backend() == "nccl" else "cpu"
+        tt = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(tt, op=op)
+        return float(tt.item())
+
     def max_ms(self, ms):
         if self.dist is None:
             return ms
-        import torch
-        tt = torch.tensor([ms], device="cuda")
-        self.dist.all_reduce(tt, op=self.dist.ReduceOp.MAX)
-        return float(tt.item())
+        return self._reduce(ms, self.dist.ReduceOp.MAX)
+
+    def total(self, x):
+        """Sum over ranks (the whole job's units: zones, zone-updates/s of independent servers)."""
+        if self.dist is None:
+            return x
+        return self._reduce(x, self.dist.ReduceOp.SUM)
 
 
 def timed_steps(ctx, solver, K, sample_clocks=False):
@@ -363,6 +377,7 @@ def run_ensemble(args, ctx):
     K, W = args.steps, args.warmup
     probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED + ctx.rank)
     ncell = sum(p.ncell for p in probs)
+    ncell_all = ctx.total(ncell)   # each rank advances its own ensemble
     NT = 10   # timer-instrumented steps (roofline)
 
     # ---- headline: batched mixed precision, autotuned, CUDA graphs
@@ -376,7 +391,7 @@ def run_ensemble(args, ctx):
     mix.step(W)
     mix.synchronize()
     ms_mix, clocks = timed_steps(ctx, mix, K, sample_clocks=True)
-    value = ctx.world * ncell * K / (ms_mix / 1e3)
+    value = ncell_all * K / (ms_mix / 1e3)
     st_mix = stage_times(mix, NT)
 
     # ---- the same ensemble batched through the plain FP64 sweep (same step count)
@@ -464,7 +479,7 @@ def run_ensemble(args, ctx):
         s.set_launch_config(**tuned)
         return s
     ms_e2e, h2d, d2h = e2e_run(ctx, make, probs, K, W)
-    e2e = ctx.world * ncell * K / (ms_e2e / 1e3)
+    e2e = ncell_all * K / (ms_e2e / 1e3)
 
     if ctx.rank != 0:
         return
@@ -488,7 +503,7 @@ def run_ensemble(args, ctx):
                          "final states (pinned D2H)" % (len(probs), K),
                 "ms": ms_e2e},
         "comparison": {
-            "fp64_batched": {"value": ctx.world * ncell * K / (ms_f64 / 1e3), "ms_per_step": ms_f64 / K,
+            "fp64_batched": {"value": ncell_all * K / (ms_f64 / 1e3), "ms_per_step": ms_f64 / K,
                              "stage_ms": st_f64},
             "fp64_one_at_a_time": {"value": one_rate, "sample": "%d problems (every 32nd), %d steps "
                                                                 "each, one solver at a time" % (len(sample), K1)},
@@ -761,12 +776,12 @@ def run_server(args, ctx):
         best[name]["device_seconds_total"] = st["device_seconds"]
         best[name]["rounds_total"] = st["rounds"]
         best[name]["kernel_launches_total"] = st["kernel_launches"]
+    value = ctx.total(best["mixed"]["zone_updates_per_s"])   # independent servers, one per rank
     if ctx.rank != 0:
         return
     peak, peak_kind = read_peaks()
     m = best["mixed"]
     zu_dev = m["zone_updates_per_s"]
-    value = ctx.world * m["zone_updates_per_s"]
     h2d = sum(pb.ncell for pb in reqs[:m["requests"]]) * 40
     line = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": ctx.world,
