@@ -1099,6 +1099,11 @@ int mdg_synchronize(mdg_solver *s)
   int err = 0;
   CK(cudaMemcpy(&err, s->d_err, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) return fail(err, "a time step estimate dropped below dtmin");
+  // non-finite states flagged by the update kernels, per problem
+  std::vector<ProbTime> T(s->nprob);
+  CK(cudaMemcpy(T.data(), s->d_times, sizeof(ProbTime) * s->nprob, cudaMemcpyDeviceToHost));
+  for (int m = 0; m < s->nprob; m++)
+    if (T[m].err) return fail(T[m].err, "problem " + std::to_string(m) + ": non-finite state or dt below dtmin");
   return MDG_OK;
 }
 

@@ -329,6 +329,16 @@ __device__ __forceinline__ void u_to_p(double *u, double *p, double gc0, double 
   }
 }
 
+// A non-finite updated state marks its problem (ProbTime::err, reported by
+// mdg_synchronize and the server's results); the values themselves are left as computed.
+__device__ __forceinline__ void flag_nonfinite(const double *pf, ProbTime *T)
+{
+  bool bad = false;
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) bad = bad || !isfinite(pf[v]);
+  if (bad) T->err = MDG_ERR_NONFINITE;
+}
+
 // Gravitational constant of constants.h:3 (cgs).
 constexpr double GNEWT = 6.67384e-8;
 

@@ -920,7 +920,7 @@ int mdg_server_result(mdg_server *s, long long id, double *prim, double *t, int 
   const int err = r->err;
   s->reqs.erase(it);
   delete r;
-  return err ? sfail(err, "request stopped: time step dropped below dtmin") : MDG_OK;
+  return err ? sfail(err, "request stopped: non-finite state or time step below dtmin") : MDG_OK;
 }
 
 int mdg_server_get_stats(mdg_server *s, mdg_server_stats *st)

@@ -149,6 +149,7 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
            P.floors != 0, P.rho_floor, P.e_floor);
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+    flag_nonfinite(pf, &times[tile.prob]);
     if (STAGE == 1) {
       // zone term of the next estimate_dt (step.c:177-187): velocity of the new state,
       // sound speed of the stage state (sim_eos was last filled from sim_ph)

@@ -308,6 +308,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
       }
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+      flag_nonfinite(pf, &times[tile.prob]);
       if (STAGE == 1) {
         // zone term of the next estimate_dt (step.c:177-187)
         const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);

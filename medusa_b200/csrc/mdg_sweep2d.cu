@@ -453,6 +453,7 @@ ysweep2d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       u_to_p(u, pf, 1.0, 1.0, 1.0, P.floors != 0, P.rho_floor, P.e_floor);
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+      flag_nonfinite(pf, &times[tile.prob]);
       if (STAGE == 1) {
         // zone terms of the next estimate_dt (step.c:177-187): new velocities, sound
         // speed of the stage state

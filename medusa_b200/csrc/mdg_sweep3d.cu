@@ -860,6 +860,7 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
            P.rho_floor, P.e_floor);
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) out.v[v][c] = pf[v];
+    flag_nonfinite(pf, &times[0]);
     if (STAGE == 1) {
       // next estimate_dt: velocity of the new state, sound speed of the stage state
       const double cs = sqrt(P.gam * press / ph[RHO]);
