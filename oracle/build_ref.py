@@ -163,6 +163,7 @@ def build_config(name, cfg, ref_root, force=False):
 DROPIN = {
     "sod": ("cart1d", 1, "MDG_PROB_NONE"),
     "dust": ("sph1d_sinh_mono_floors", 2, "MDG_PROB_DUST"),
+    "sedov3d": ("sph3d_default", 3, "MDG_PROB_NONE"),
 }
 ROOT = os.path.dirname(HERE)
 LIBDIR = os.path.join(ROOT, "medusa_b200", "_lib")

@@ -13,7 +13,10 @@
  *   - parse_input restates the key = value reader of io.c:4979-5785 for the keys the
  *     hydro run uses (defaults as io.c:5000-5117);
  *   - the problem hooks restate, in the current API, problems/init_sod.c:31-99
- *     (DROPIN_PROB 1) and problems/init_dustcollapse.c:27-113 (DROPIN_PROB 2);
+ *     (DROPIN_PROB 1), problems/init_dustcollapse.c:27-113 (DROPIN_PROB 2) and
+ *     problems/init_sedov.c:3-164 on the 3-D dendritic grid (DROPIN_PROB 3; its outer
+ *     PROB boundary, a fixed ambient state equal to the initial outer zones, is OUTFLOW
+ *     here, the same ghost values until the blast reaches the outer radius);
  *   - the gamma-law EOS fill loops as eos/burrows/eos_stuff.c:521-532,668-683 with the
  *     arithmetic of eos/gamma/eos_gamma.c:5-12,45-58;
  *   - dumps, logs and restarts are no-ops; analysis_postloop brings the state to the
@@ -248,6 +251,61 @@ void prob_bounds(int i, int j, int k, double *p)
   double vr = -1.0/sqrt(r);
   p[U1] = vr/ND_ELEM_LINEAR(geom,i,j,k).scale[0][0];
 }
+
+#elif (DROPIN_PROB == 3)
+/* problems/init_sedov.c:3-164 (3-D) */
+void init_grid()
+{
+  startx[0] = 0.;
+  startx[1] = -1.;
+  startx[2] = 0.;
+  dx[0] = 0.4*1.2/n1;
+  dx[1] = 2./n2;
+  dx[2] = 2.*M_PI/n3;
+  rx_info.rtrans = rtrans_solve(dx[0], 1.2);
+  periodic[0] = 0;
+  periodic[1] = 0;
+  periodic[2] = 1;
+}
+
+void init_problem()
+{
+  int ii=0, jj=0, kk=0, vv;
+  double rho_amb = 1., e_amb = 1.e-12, u_amb = 0.;
+  double E_expl = 0.851072, R_expl = 0.075, Edens;
+  gam = 1.4;
+  VLOOP {
+    bc[vv].lo[0] = SPHERICAL_ORIGIN;
+    bc[vv].hi[0] = OUTFLOW;
+    bc[vv].lo[1] = REFLECT;
+    bc[vv].hi[1] = REFLECT;
+    bc[vv].lo[2] = PERIODIC;
+    bc[vv].hi[2] = PERIODIC;
+  }
+  ZLOOP {
+    NDP_ELEM_LINEAR(sim_p,ii,jj,kk,RHO) = rho_amb;
+    NDP_ELEM_LINEAR(sim_p,ii,jj,kk,UU) = e_amb;
+    NDP_ELEM_LINEAR(sim_p,ii,jj,kk,U1) = u_amb;
+    NDP_ELEM_LINEAR(sim_p,ii,jj,kk,U2) = 0.;
+    NDP_ELEM_LINEAR(sim_p,ii,jj,kk,U3) = 0.;
+  }
+  Edens = E_expl/(4./3.*M_PI*pow(R_expl,3.));
+  if (redge[istart[0]] < R_expl) {
+    for (ii=istart[0]; ii<istop[0]; ii++) {
+      if (redge[ii+1] < R_expl) {
+        JSLOOP(ii,jj) { KSLOOP(ii,jj,kk) { NDP_ELEM_LINEAR(sim_p,ii,jj,kk,UU) = Edens; } }
+      } else if (redge[ii] < R_expl) {
+        Edens *= (pow(R_expl,3.)-pow(redge[ii],3.))/(pow(redge[ii+1],3.)-pow(redge[ii],3.));
+        JSLOOP(ii,jj) { KSLOOP(ii,jj,kk) { NDP_ELEM_LINEAR(sim_p,ii,jj,kk,UU) = Edens; } }
+        break;
+      } else {
+        break;
+      }
+    }
+  }
+}
+
+void prob_bounds(int i, int j, int k, double *p) { (void)i; (void)j; (void)k; (void)p; }
 #endif
 
 /* ---------------- analysis hooks ---------------- */

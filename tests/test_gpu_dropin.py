@@ -26,6 +26,9 @@ def rel_err(a, b):
 @pytest.mark.parametrize("prob,inputs,n", [
     ("sod", dict(n1=1024, cfl=0.8, tmax=0.2), 1024),
     ("dust", dict(n1=200, cfl=0.9, tmax=0.004), 200),
+    # problems/init_sedov.c on the 3-D dendritic grid with the default build maps
+    # (SINH_MODIFIED radius, POLYTH theta; rtrans from the hook's own rtrans_solve)
+    ("sedov3d", dict(n1=24, n2=16, n3=32, cfl=0.8, tmax=0.02), None),
 ])
 def test_dropin_gpu_run_equals_reference_run(prob, inputs, n, tmp_path):
     ic, tc, pc, ec = run_dropin("cpu", prob, inputs, tmp_path, n)
