@@ -149,6 +149,7 @@ struct mdg_server {
   WorkQueue *d_queue = nullptr;
   int *d_err = nullptr;
   double *d_state = nullptr, *d_rc0 = nullptr, *d_geo = nullptr, *d_stage = nullptr;
+  double *d_gmono = nullptr;   // monopole gravity per zone unit (FP64 servers)
   float *d_mx = nullptr;
   StateSoA P{}, PH{};
   Tables tb{};
@@ -211,6 +212,7 @@ void free_server(mdg_server *s)
   if (s->stream3) cudaStreamDestroy(s->stream3);
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles); cudaFree(s->d_queue); cudaFree(s->d_err);
   cudaFree(s->d_state); cudaFree(s->d_rc0); cudaFree(s->d_geo); cudaFree(s->d_stage); cudaFree(s->d_mx);
+  cudaFree(s->d_gmono);
   cudaFree(s->d_state2); cudaFree(s->d_shock0); cudaFree(s->d_shock1); cudaFree(s->d_tiles2);
   if (s->h_times) cudaFreeHost(s->h_times);
   if (s->h_ret) cudaFreeHost(s->h_ret);
@@ -233,7 +235,9 @@ StateSoA soa3(const Request *r, int which)
 // bytes of device memory per zone unit: state P and PH, RC and GF tables, FP32 weights
 int64_t bytes_per_unit(int precision)
 {
-  return 2 * NPRIM * 8 + RC_NFIELDS * 8 + GF_NFIELDS * 8 + (precision == MDG_PREC_MIXED ? MX_NFIELDS * 4 : 0);
+  // state P and PH, the RC and GF tables, and the FP32 weights (mixed) or the monopole
+  // gravity per zone (FP64)
+  return 2 * NPRIM * 8 + RC_NFIELDS * 8 + GF_NFIELDS * 8 + (precision == MDG_PREC_MIXED ? MX_NFIELDS * 4 : 8);
 }
 
 // bytes per cell of the 2-D arena: state P, PH and accumulator, two shock bytes
@@ -277,7 +281,11 @@ int queue_round(mdg_server *s, int nsteps)
       launch_stage1d_mixed(1, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
                            s->PH, s->P, s->P, s->stream);
     } else {
+      // monopole gravity of the 1-D requests that have it (one thread per slot; the others
+      // return at once), from each stage's state
+      launch_monopole1d(s->d_probs, s->d_times, s->max_probs, s->tb, s->P, s->stream);
       launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
+      launch_monopole1d(s->d_probs, s->d_times, s->max_probs, s->tb, s->PH, s->stream);
       launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
     }
     if (lane2) {
@@ -328,6 +336,7 @@ int admit(mdg_server *s, Request *r)
   }
   P.cell_off = seg;
   P.geo_off = seg;
+  P.mono_off = seg;
   P.sparse_conn = r->sparse;
   if (d.ndim == 2) {
     P.cell_off = r->seg2;
@@ -707,6 +716,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   SCKB(cudaMalloc(&s->d_geo, sizeof(double) * GF_NFIELDS * units));
   SCKB(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * std::max<int64_t>(c.max_zones, cells > 0 ? c.max_cells_2d : 0)));
   if (c.precision == MDG_PREC_MIXED) SCKB(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * units));
+  else SCKB(cudaMalloc(&s->d_gmono, sizeof(double) * units));
   if (cells > 0) {
     SCKB(cudaMalloc(&s->d_state2, sizeof(double) * 3 * NPRIM * cells));
     SCKB(cudaMalloc(&s->d_shock0, cells));
@@ -734,6 +744,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   s->tb.rc0 = s->d_rc0; s->tb.rc0_stride = units;
   s->tb.rc1 = s->d_rc0; s->tb.rc1_stride = units;
   s->tb.geo = s->d_geo; s->tb.geo_stride = units;
+  s->tb.gmono = s->d_gmono;
   s->tb.mx = s->d_mx;
   s->tb.mx1 = s->d_mx;   // direction 1 of a 2-D request, after its direction-0 weights
   *out = s;
@@ -749,8 +760,8 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
   if (rc != MDG_OK) return sfail(rc, "request: " + why);
   if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
     return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
-  if (desc->monopole != 0 || desc->prob_kind == MDG_PROB_DUST)
-    return sfail(MDG_ERR_NOTIMPL, "request: monopole gravity and the dust-collapse hook run in mdg_create solvers only");
+  if (desc->monopole != 0 && ndim == 1 && s->cfg.precision == MDG_PREC_MIXED)
+    return sfail(MDG_ERR_NOTIMPL, "request: the 1-D mixed-precision sweep has no monopole gravity");
   if (is_dendritic(*desc)) {
     // 3-D requests and 2-D spherical (r, theta) requests: the dendritic lane
     if (s->cfg.hbm_bytes_3d <= 0) return sfail(MDG_ERR_NOTIMPL, "request: the server takes no dendritic-grid requests");

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from medusa_b200 import problems as P
-from medusa_b200.solver import MdgError, PREC_MIXED, Server, Solver
+from medusa_b200.solver import MdgError, PREC_FP64, PREC_MIXED, Server, Solver
 from tests._cases import golden_cases_gravity, load_golden, record
 
 pytestmark = pytest.mark.gpu
@@ -108,9 +108,32 @@ def test_dendritic_mixed_matches_fp64():
     assert l1_rho <= 1.0e-4 and l1_u <= 1.0e-4
 
 
-def test_server_refuses_monopole_requests():
-    pb = P.dust_collapse(64).copy(tmax=1.0e-3)
-    with Server(precision=0, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
+def _solver_to_end(pb, precision):
+    with Solver(pb, precision=precision) as s:
+        for _ in range(100000):
+            s.step(1)
+            if s.time(0)[0] >= pb.tmax:
+                break
+        return s.update_cpu(0), s.time(0)
+
+
+def test_server_runs_monopole_requests():
+    """Self-gravitating requests in an FP64 server (1-D with the dust-collapse hook, 3-D
+    dendritic) beside plain ones: each result equals the solver's, bit for bit; a mixed
+    server refuses 1-D monopole requests."""
+    reqs = [P.dust_collapse(200).copy(tmax=2.0e-3),
+            P.spherical_1d("sod", 256, 1.4).copy(tmax=0.02),
+            P.dust_collapse(16, 8, 16, ndim=3, radius="uniform", floors=False).copy(tmax=1.0e-3)]
+    with Server(precision=PREC_FP64, hbm_bytes=128 << 20, max_problems=8, max_zones=4096,
+                hbm_bytes_3d=256 << 20) as srv:
+        ids = [srv.submit(pb) for pb in reqs]
+        srv.run(0)
+        for rid, pb in zip(ids, reqs):
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_to_end(pb, PREC_FP64)
+            assert t == rt and ist == rist, pb.name
+            assert np.array_equal(prim, ref), pb.name
+    with Server(precision=PREC_MIXED, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
         with pytest.raises(MdgError) as e:
-            srv.submit(pb)
+            srv.submit(reqs[0])
         assert e.value.code == 5
