@@ -126,6 +126,8 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_upload_state.argtypes = [vp, i, vp]
     L.mdg_estimate_dt.argtypes = [vp, vp]
     L.mdg_step.argtypes = [vp, i]
+    L.mdg_estimate_dt_raw.argtypes = [vp, vp]
+    L.mdg_step_dt.argtypes = [vp, vp]
     L.mdg_download_state.argtypes = [vp, i, vp, vp]
     L.mdg_get_time.argtypes = [vp, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(i)]
     L.mdg_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
@@ -308,6 +310,19 @@ class Solver:
 
     def step(self, nsteps: int = 1):
         _check(library().mdg_step(self._h, int(nsteps)), "mdg_step")
+
+    # --- for a host that runs the main.c time loop itself
+    def estimate_dt_raw(self) -> np.ndarray:
+        """What estimate_dt() leaves in the reference's dt, per problem (before main.c's
+        safety, growth and clipping)."""
+        out = np.zeros(len(self.problems))
+        _check(library().mdg_estimate_dt_raw(self._h, out.ctypes.data), "mdg_estimate_dt_raw")
+        return out
+
+    def step_dt(self, dt):
+        """One step() of every problem with the host's dt (scalar or one per problem)."""
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(dt, dtype=np.float64), (len(self.problems),)))
+        _check(library().mdg_step_dt(self._h, d.ctypes.data), "mdg_step_dt")
 
     def update_cpu(self, m: int = 0, with_eos: bool = False):
         n = self.problems[m].ncell

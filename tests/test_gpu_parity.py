@@ -199,3 +199,27 @@ def test_gpu_upload_all_download_all_equal_per_problem(precision):
         assert [s.time(m) for m in range(len(probs))] == tref
     for a, b in zip(ref, got):
         assert np.array_equal(a, b)
+
+
+def test_host_driven_time_loop_equals_device_loop():
+    """mdg_estimate_dt_raw + main.c's dt rules on the host + mdg_step_dt (a host that keeps
+    the reference's time loop) against mdg_step's device-side loop: the same states and
+    times, bit for bit, for a batch of two problems."""
+    probs = [P.sod(256).copy(cfl=0.8, tmax=0.05), P.spherical_1d("sedov", 200, 1.4, p_ratio=1.0e4, r0=0.05)]
+    with Solver(probs) as a, Solver(probs) as b:
+        dtold = np.full(2, 1.0e100)
+        for istep in range(30):
+            dt = b.estimate_dt_raw()
+            dt = dt * np.array([pb.dt_init_safety for pb in probs]) if istep == 0 else \
+                np.minimum(dtold * np.array([pb.dt_grow_safety for pb in probs]), dt)
+            dtold = dt.copy()
+            for m, pb in enumerate(probs):
+                t = b.time(m)[0]
+                if t + dt[m] > pb.tmax:
+                    dt[m] = 1.000000001 * (pb.tmax - t)
+                dt[m] = max(dt[m], pb.dtmin)
+            b.step_dt(dt)
+            a.step(1)
+        for m in range(2):
+            assert a.time(m)[0] == b.time(m)[0]
+            assert np.array_equal(a.update_cpu(m), b.update_cpu(m))
