@@ -334,7 +334,24 @@ def run_reference_arm(args, ctx):
     from medusa_b200 import problems as P
     if ctx.rank != 0:
         return
-    if args.workload == "sedov3d":
+    if args.workload == "sod1d":
+        # the whole C1 job: its step count from the CPU restatement (bit-identical to the
+        # reference), then the reference build timed over exactly those steps
+        from oracle import pyoracle
+        pb = P.sod(1024).copy(cfl=0.8, tmax=0.2)
+        o = pyoracle.Oracle(pb)
+        nsteps = 0
+        while o.t < pb.tmax and nsteps < 10000:
+            o.advance(1)
+            nsteps += 1
+        r = pyoracle.time_reference(pb, 0, nsteps, fast=True)
+        cb = {"value": r["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1, "kind": "reference",
+              "sample": "the whole job (%d RK2 steps to t = 0.2), reference build with its own flags "
+                        "(-O3 -ffast-math), 1 core, %.3f s" % (nsteps, r["seconds"])}
+        config = {"workload": "sod_1d_cartesian_1024_to_t0.2_fp64", "global_batch": 1, "seq_len": 1024,
+                  "parallelism": "replicas", "l2": "resident in L2 (80 KB state)"}
+        dtype = "f64"
+    elif args.workload == "sedov3d":
         cb = cpu_baseline_sedov3d(steps=max(1, min(args.steps, 2)), radius=args.sedov3d_radius)
         config = {"workload": sedov3d_workload_name(SEDOV3D, args.sedov3d_radius), "global_batch": 1,
                   "seq_len": sedov3d_problem(SEDOV3D, args.sedov3d_radius).ncell, "parallelism": "replicas",
@@ -735,6 +752,74 @@ def run_sedov3d(args, ctx):
     print(json.dumps(line), flush=True)
 
 
+def run_sod1d(args, ctx):
+    """Config C1: the Sod tube of problems/init_sod.c, 1024 zones, CFL 0.8, run to t = 0.2
+    in plain FP64, timed as a whole (device time from t = 0 to the end, every step in
+    one CUDA-graph stream), compared zone by zone with the reference's own run of the same
+    job and with the exact Riemann solution."""
+    import numpy as np
+    import torch
+    from medusa_b200 import analytic as A
+    from medusa_b200 import problems as P
+    from medusa_b200.solver import Solver
+    pb = P.sod(1024).copy(cfl=0.8, tmax=0.2)
+    nmax = 4000                      # at most; steps past t = 0.2 leave the problem unchanged
+    with Solver(pb, device=ctx.local) as s:
+        # the job's step count first (untimed), then exactly that many steps timed
+        s.step(nmax)
+        s.synchronize()
+        nmax = s.time(0)[2]
+        warm_up(s, args.warmup)
+        s.upload(0, pb.ic)
+        stream = torch.cuda.ExternalStream(s.stream, device=ctx.local)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ctx.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(nmax)
+        e1.record(stream)
+        e1.synchronize()
+        s.synchronize()
+        ms = ctx.max_ms(e0.elapsed_time(e1))
+        prim = s.update_cpu(0)
+        t, _, istep = s.time(0)
+    value = ctx.world * pb.ncell * istep / (ms / 1e3)
+    l1 = A.l1_rel(prim[:, 0], A.sod_exact_state(1024, t)[:, 0])
+    if ctx.rank != 0:
+        return
+    from oracle import pyoracle
+    ref = {}
+    if pyoracle.ref_available(pb) and not args.no_cpu_baseline:
+        last = pyoracle.run_reference(pb, istep, every=istep)[-1]
+        d = np.abs(prim - last[4]) / np.maximum(np.abs(last[4]), 1.0e-300)
+        d[prim == last[4]] = 0.0
+        ref = {"max_rel_diff_vs_reference": float(d.max()), "bit_identical_fraction": float(np.mean(prim == last[4])),
+               "reference_t": last[1], "reference_steps": last[0]}
+    peak, peak_kind = read_peaks()
+    achieved = 200.0 * pb.ncell * istep / (ms / 1e3) / 1e9
+    line = {
+        "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s", "n_gpus": ctx.world,
+        "steps": istep, "warmup": args.warmup, "ms_per_step": ms / istep, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "sod_1d_cartesian_1024_to_t0.2_fp64", "global_batch": ctx.world, "seq_len": 1024,
+                   "parallelism": "replicas" if ctx.world > 1 else "single",
+                   "l2": "resident in L2 (80 KB state): a latency-bound job, timed whole"},
+        "gpu_launches": 2 * nmax + 2 * nmax // 10,
+        "time_to_solution_ms": ms, "t": t,
+        "accuracy": dict({"l1_rho_vs_exact_riemann": l1}, **ref),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "note": "1024 zones per launch: bound by launch latency, not HBM",
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+    }
+    if not args.no_cpu_baseline and pyoracle.ref_available(pb, fast=True):
+        r = pyoracle.time_reference(pb, 0, istep, fast=True)
+        line["cpu_baseline"] = {"value": r["zone_updates_per_s"], "unit": "zone-updates/s", "cores": 1,
+                                "kind": "reference",
+                                "sample": "the whole job (%d RK2 steps), reference build with its own flags "
+                                          "(-O3 -ffast-math), 1 core, %.3f s" % (istep, r["seconds"])}
+    print(json.dumps(line), flush=True)
+
+
 def server_workload_name(args):
     if args.server_frac_3d > 0.0:
         return "server_stream_%d%%_1d_%d%%_2d_%d%%_3d_sedov_128x64x128" % (
@@ -826,7 +911,7 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048", "server", "sedov3d"])
+    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048", "server", "sedov3d", "sod1d"])
     ap.add_argument("--server-requests", type=int, default=6000)
     ap.add_argument("--server-rates", default="1000,4000,16000,inf",
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
@@ -867,6 +952,8 @@ def main():
             run_server(args, ctx)
         elif args.workload == "sedov3d":
             run_sedov3d(args, ctx)
+        elif args.workload == "sod1d":
+            run_sod1d(args, ctx)
         else:
             run_kh(args, ctx)
     finally:
