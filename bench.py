@@ -773,6 +773,8 @@ def run_sod1d(args, ctx):
         s.upload(0, pb.ic)
         stream = torch.cuda.ExternalStream(s.stream, device=ctx.local)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(ctx.local)
+        sampler.start()
         ctx.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
@@ -781,6 +783,7 @@ def run_sod1d(args, ctx):
         e1.synchronize()
         s.synchronize()
         ms = ctx.max_ms(e0.elapsed_time(e1))
+        clocks = sampler.stop()
         prim = s.update_cpu(0)
         t, _, istep = s.time(0)
     value = ctx.world * pb.ncell * istep / (ms / 1e3)
@@ -804,8 +807,8 @@ def run_sod1d(args, ctx):
         "config": {"workload": "sod_1d_cartesian_1024_to_t0.2_fp64", "global_batch": ctx.world, "seq_len": 1024,
                    "parallelism": "replicas" if ctx.world > 1 else "single",
                    "l2": "resident in L2 (80 KB state): a latency-bound job, timed whole"},
-        "gpu_launches": 2 * nmax + 2 * nmax // 10,
-        "time_to_solution_ms": ms, "t": t,
+        "gpu_launches": 4 * nmax,       # dt, two stages and the time update per step
+        "time_to_solution_ms": ms, "t": t, "clocks": clocks,
         "accuracy": dict({"l1_rho_vs_exact_riemann": l1}, **ref),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "note": "1024 zones per launch: bound by launch latency, not HBM",
