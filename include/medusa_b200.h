@@ -227,9 +227,11 @@ int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy);
  * nsteps passes of the reference time loop, exactly as mdg_create + mdg_upload_state +
  * mdg_step would, starting from t = 0.  prim_in and prim_out are DEVICE pointers owned
  * by the caller, laid out [var][zone] (5 x n1 doubles; they may be the same buffer);
- * work is queued on `stream` (a cudaStream_t, 0 for the legacy default stream).  If
- * t_out/dt_out are non-NULL the call waits for the stream and returns the final time
- * and the last dt there.
+ * work is queued on `stream` (a cudaStream_t, 0 for the legacy default stream).  The
+ * call waits for that work to finish before it returns; it then stores the final time
+ * and the last dt in t_out/dt_out (when non-NULL) and returns MDG_ERR_NONFINITE, as
+ * mdg_synchronize does, when the state became non-finite or a dt estimate dropped below
+ * desc->dtmin.
  *
  * Everything else the sweep needs lives in one file-scope device array of fixed size
  * (about 4.4 MB, held by every GPU that loads this library until exit).  Rules:
@@ -237,7 +239,9 @@ int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy);
  *   - the first call on a device performs the device set-up (it looks up the array's
  *     device address); make that first call before any stream capture;
  *   - all calls share the array: calls whose work overlaps on the GPU race;
- *   - the array keeps the last call's contents; each call re-initialises what it uses.
+ *   - the array keeps the last call's contents; each call re-initialises what it uses;
+ *   - the tables are built in one process-wide host buffer under a lock, so calls from
+ *     several host threads wait for each other while their tables are copied.
  * Calls no cudaMalloc, cudaFree or other allocating routine.
  */
 #define MDG_NOALLOC_MAX_ZONES 8192

@@ -17,7 +17,13 @@
 //  * the first call on a device resolves the array's device address with
 //    cudaGetSymbolAddress (device set-up); make that first call before any stream capture;
 //  * the array keeps the previous call's contents: each call re-initialises everything it
-//    reads (time record, error flag, tables, tile list) before use.
+//    reads (time record, error flag, tables, tile list) before use;
+//  * every call waits for its own work on the stream before it returns: it reads back the
+//    problem's time record and error flag and reports a non-finite state or a dt below
+//    dtmin as MDG_ERR_NONFINITE, as mdg_synchronize does for the allocating path;
+//  * the host-side staging of the tables is one process-wide set, held under a lock from
+//    the table build until its copies have landed, so calls from different host threads
+//    (on one GPU or on several) never share it while it is in use.
 // This entry point calls no cudaMalloc, cudaFree or other allocating library routine.
 #include <cuda_runtime.h>
 #include <cstring>
@@ -26,6 +32,7 @@
 #include "mdg_kernels.cuh"
 
 namespace mdg {
+void make_probdev(const mdg_problem_desc &d, ProbDev &P);
 void build_recon_table_into(const mdg_problem_desc &d, int dir, double *tab, int64_t stride, int64_t off,
                             double *al, double *be, double *ga);
 void build_geo_1d(const mdg_problem_desc &d, double *tab, int64_t stride, int64_t off);
@@ -61,6 +68,7 @@ namespace {
 constexpr int MAX_DEVICES = 64;
 unsigned char *g_scratch[MAX_DEVICES] = {nullptr};
 std::mutex g_setup_mutex;
+std::mutex g_staging_mutex;   // held while the host staging below is filled and copied
 
 // Host staging of the tables (host memory reserved at load time, not allocated per call).
 double h_rc[RC_NFIELDS * NCOL];
@@ -147,26 +155,11 @@ extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double
 
   // problem record, tables and tiles (host staging, copied into the scratch)
   ProbDev P;
-  memset(&P, 0, sizeof P);
-  P.ndim = 1; P.geom = d.geom; P.eos = d.eos; P.interp_order = d.hydro_interp_order;
-  P.n1 = n1; P.n2 = 1;
-  P.ncell = n1;
-  P.bc_lo0 = d.bc_lo[0]; P.bc_hi0 = d.bc_hi[0];
-  P.prob_kind = d.prob_kind;
-  P.has_src = (d.geom == MDG_SPHERICAL);
-  P.cell_off = 0; P.geo_off = 0;
-  P.gam = d.gam; P.Kpoly = d.Kpoly; P.dx0 = d.dx[0]; P.dx1 = d.dx[1];
-  P.cfl = d.cfl; P.dt_init_safety = d.dt_init_safety; P.dt_grow_safety = d.dt_grow_safety;
-  P.initial_dt = d.initial_dt; P.dtmax = d.dtmax; P.dtmin = d.dtmin; P.tmax = d.tmax;
-  P.floors = d.enforce_floors; P.rho_floor = d.rho_floor; P.e_floor = d.e_floor;
-  P.grav[0] = d.grav[0]; P.grav[1] = d.grav[1]; P.grav[2] = d.grav[2];
-  P.grav_on = (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0);
+  make_probdev(d, P);
+  P.cell_off = 0;
+  P.mono_off = 0;
+  P.geo_off = 0;
   const int64_t ncol = n1 + 2 * NG;
-  build_recon_table_into(d, 0, h_rc, ncol, 0, h_al, h_be, h_ga);
-  build_geo_1d(d, h_geo, ncol, 0);
-  P.sparse_conn = conn_is_sparse(h_geo, ncol, 0, (int)ncol);
-  int ntiles = 0;
-  for (int i0 = 0; i0 < n1; i0 += TILE1) h_tiles[ntiles++] = Tile{0, i0, 0, 0};
 
   double *ph = reinterpret_cast<double *>(base + OFF_PH);
   double *rcd = reinterpret_cast<double *>(base + OFF_RC);
@@ -181,15 +174,23 @@ extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double
     cudaError_t e_ = (call);                                                 \
     if (e_ != cudaSuccess) return fail(MDG_ERR_CUDA, cudaGetErrorString(e_)); \
   } while (0)
-  CKN(cudaMemcpyAsync(rcd, h_rc, sizeof(double) * RC_NFIELDS * ncol, cudaMemcpyHostToDevice, st));
-  CKN(cudaMemcpyAsync(geo, h_geo, sizeof(double) * GF_NFIELDS * ncol, cudaMemcpyHostToDevice, st));
-  CKN(cudaMemcpyAsync(probs, &P, sizeof P, cudaMemcpyHostToDevice, st));
-  CKN(cudaMemcpyAsync(tiles, h_tiles, sizeof(Tile) * ntiles, cudaMemcpyHostToDevice, st));
-  CKN(cudaMemsetAsync(err, 0, sizeof(int), st));        // the error flag must start at zero
-  if (prim_out != prim_in)
-    CKN(cudaMemcpyAsync(prim_out, prim_in, sizeof(double) * NPRIM * n1, cudaMemcpyDeviceToDevice, st));
-  // the host staging above is reused by the next call: wait until the copies have landed
-  CKN(cudaStreamSynchronize(st));
+  int ntiles = 0;
+  {
+    // the staging is shared by all host threads: hold it until the copies have landed
+    std::lock_guard<std::mutex> lk(g_staging_mutex);
+    build_recon_table_into(d, 0, h_rc, ncol, 0, h_al, h_be, h_ga);
+    build_geo_1d(d, h_geo, ncol, 0);
+    P.sparse_conn = conn_is_sparse(h_geo, ncol, 0, (int)ncol);
+    for (int i0 = 0; i0 < n1; i0 += TILE1) h_tiles[ntiles++] = Tile{0, i0, 0, 0};
+    CKN(cudaMemcpyAsync(rcd, h_rc, sizeof(double) * RC_NFIELDS * ncol, cudaMemcpyHostToDevice, st));
+    CKN(cudaMemcpyAsync(geo, h_geo, sizeof(double) * GF_NFIELDS * ncol, cudaMemcpyHostToDevice, st));
+    CKN(cudaMemcpyAsync(probs, &P, sizeof P, cudaMemcpyHostToDevice, st));
+    CKN(cudaMemcpyAsync(tiles, h_tiles, sizeof(Tile) * ntiles, cudaMemcpyHostToDevice, st));
+    CKN(cudaMemsetAsync(err, 0, sizeof(int), st));        // the error flag must start at zero
+    if (prim_out != prim_in)
+      CKN(cudaMemcpyAsync(prim_out, prim_in, sizeof(double) * NPRIM * n1, cudaMemcpyDeviceToDevice, st));
+    CKN(cudaStreamSynchronize(st));
+  }
 
   Tables tb{};
   tb.rc0 = rcd; tb.rc0_stride = ncol;
@@ -206,13 +207,16 @@ extern "C" int mdg_advance_1d_noalloc(const mdg_problem_desc *desc, const double
     launch_finish(times, 1, st);
   }
   CKN(cudaGetLastError());
-  if (t_out || dt_out) {
-    ProbTime T;
-    CKN(cudaMemcpyAsync(&T, times, sizeof T, cudaMemcpyDeviceToHost, st));
-    CKN(cudaStreamSynchronize(st));
-    if (t_out) *t_out = T.t;
-    if (dt_out) *dt_out = T.dt;
-  }
+  // the outcome: the time record (non-finite state, dt below dtmin) and the error word
+  ProbTime T;
+  int errw = 0;
+  CKN(cudaMemcpyAsync(&T, times, sizeof T, cudaMemcpyDeviceToHost, st));
+  CKN(cudaMemcpyAsync(&errw, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKN(cudaStreamSynchronize(st));
+  if (t_out) *t_out = T.t;
+  if (dt_out) *dt_out = T.dt;
+  if (errw) return fail(errw, "mdg_advance_1d_noalloc: a time step estimate dropped below dtmin");
+  if (T.err) return fail(T.err, "mdg_advance_1d_noalloc: non-finite state or dt below dtmin");
 #undef CKN
   return MDG_OK;
 }

@@ -218,6 +218,25 @@ def grid3d_zone_volumes(pb: "_pb.Problem") -> np.ndarray:
     return vol
 
 
+def grid3d_zone_gcov(pb: "_pb.Problem") -> np.ndarray:
+    """Zone-centred metric diagonal gcov[0][0..2] of every interior zone of a dendritic
+    (3-D or 2-D spherical) problem, in zone order, shape [zones, 3]."""
+    nj, nk, n = grid3d_counts(pb)
+    geo = grid3d_geometry(pb)
+    n1 = pb.n[0]
+    njx = [int(nj[1]), int(nj[0])] + [int(x) for x in nj] + [int(nj[-1])] * 2   # rows i = -2 .. n1+1
+    out = np.empty((n, 3))
+    r = c = q = 0
+    for i in range(-2, n1 + 2):
+        for j in range(-2, njx[i + 2] + 2):
+            if 0 <= i < n1 and 0 <= j < nj[i]:
+                out[c:c + nk[q], :] = geo[r, 4:7]
+                c += int(nk[q])
+                q += 1
+            r += 1
+    return out
+
+
 def grid3d_radial_mean(pb: "_pb.Problem", field: np.ndarray) -> np.ndarray:
     """Volume-weighted mean of a zone field over each radial row of a dendritic problem."""
     nj, nk, n = grid3d_counts(pb)

@@ -12,6 +12,7 @@ Two binaries per configuration:
   reffast_<cfg>    the reference's own flags (Makefile:14), used as the timed CPU baseline
 
 Usage: python oracle/build_ref.py [--ref-root DIR] [--force]
+The reference tree defaults to $MDG_REFERENCE_ROOT, else /root/reference.
 """
 import argparse
 import os
@@ -21,9 +22,10 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "refshim")
-DEFAULT_REF_ROOT = "/root/reference"
+DEFAULT_REF_ROOT = os.environ.get("MDG_REFERENCE_ROOT", "/root/reference")
 
-# hot-path sources compiled unmodified (SURVEY-verified link set minus main.c/io.c)
+# hot-path sources compiled unmodified (the link set of the hydro executable minus main.c/io.c,
+# whose HDF5 I/O is replaced by the glue)
 REF_SOURCES = ["array.c", "mpi.c", "utils.c", "step.c", "geometry.c", "rad_fluid.c",
                "fluid.c", "riemann.c", "reconstruct.c", "bc.c", "eos.c", "timer.c",
                "quadrupole.c", "tracer.c"]

@@ -2,14 +2,15 @@
 fixtures made by the reference's GRAV=SPHERICAL_MONOPOLE_GRAV builds: the dust collapse
 of problems/init_dustcollapse.c in 1-D (SINH radius with floors and the outer v^r hook;
 uniform radius) and on the 2-D and 3-D dendritic grids.  Bars as for the other sweeps:
-1e-9 after a whole fixture run, 1e-12 for one step (error per variable relative to its
-largest magnitude, the velocities sharing one scale)."""
+1e-9 after a whole fixture run, 1e-12 for one step, on two measures: pointwise
+(tests/_cases.py pointwise_rel_err) and per variable relative to its largest magnitude,
+the velocities sharing one scale."""
 import numpy as np
 import pytest
 
 from medusa_b200 import problems as P
 from medusa_b200.solver import MdgError, PREC_FP64, PREC_MIXED, Server, Solver
-from tests._cases import golden_cases_gravity, load_golden, record
+from tests._cases import golden_cases_gravity, load_golden, pointwise_rel_err, record, zone_gcov
 
 pytestmark = pytest.mark.gpu
 
@@ -36,9 +37,11 @@ def test_gravity_full_run_matches_reference_fixture(name):
         prim = s.update_cpu(0)
         t, _, istep = s.time(0)
     e = err(prim, g["prim"])
-    record("gravity_full_" + name, steps=n, err=e, bit_identical=float(np.mean(prim == g["prim"])))
+    pw = pointwise_rel_err(prim, g["prim"], pb, zone_gcov(pb))
+    record("gravity_full_" + name, steps=n, err=e, pointwise=pw, bit_identical=float(np.mean(prim == g["prim"])))
     assert istep == n
     assert e <= FULL_RUN_TOL
+    assert pw <= FULL_RUN_TOL
     assert abs(t - float(g["t"])) <= FULL_RUN_TOL * float(g["t"])
 
 
@@ -50,7 +53,9 @@ def test_gravity_one_step_from_developed_state(name):
         s.step(1)
         prim = s.update_cpu(0)
     e = err(prim, g["prim1"])
-    record("gravity_step_" + name, err=e, bit_identical=float(np.mean(prim == g["prim1"])))
+    pw = pointwise_rel_err(prim, g["prim1"], pb, zone_gcov(pb))
+    record("gravity_step_" + name, err=e, pointwise=pw, bit_identical=float(np.mean(prim == g["prim1"])))
+    assert pw <= PER_STEP_TOL
     assert e <= PER_STEP_TOL
 
 

@@ -1,8 +1,12 @@
 """GPU parity: the CUDA sweep through the C ABI against the reference's golden fixtures
 and the CPU oracle.
 
-Error measure: per primitive variable, max|gpu - ref| / max(|gpu|, |ref|) over the field
-(field-relative).  Bars:
+Error measures (tests/_cases.py):
+  * pointwise: zone by zone, |gpu - ref| / |ref| for density and internal energy, and
+    each physical velocity component's error over the zone's own speed scale
+    max(|v|, c_s) (pointwise_rel_err);
+  * field-relative: per variable, max|gpu - ref| / max(|gpu|, |ref|) over the field.
+Bars, both measures:
   * one step from the same input state: <= 1e-12 (PER_STEP_TOL);
   * a whole fixture run (25-100 steps) from the initial state: <= 1e-9 (FULL_RUN_TOL).
 The FP64 kernels keep the reference's operation order without multiply-add
@@ -19,7 +23,7 @@ from medusa_b200 import problems as P
 from medusa_b200.solver import Solver, MdgError
 from oracle import pyoracle
 from tests._cases import (bit_identical_fraction, field_rel_err, golden_cases, load_golden,
-                          record)
+                          pointwise_rel_err, record)
 
 pytestmark = pytest.mark.gpu
 
@@ -39,10 +43,12 @@ def test_gpu_full_run_matches_reference_fixture(name):
         prim = s.update_cpu(0)
         t, dt, istep = s.time(0)
     err = field_rel_err(prim, g["prim"])
-    record("full_run_" + name, steps=n, field_rel_err=err, bit_identical=bit_identical_fraction(prim, g["prim"]),
-           t_rel_err=abs(t - float(g["t"])) / float(g["t"]))
+    pw = pointwise_rel_err(prim, g["prim"], pb)
+    record("full_run_" + name, steps=n, field_rel_err=err, pointwise=pw,
+           bit_identical=bit_identical_fraction(prim, g["prim"]), t_rel_err=abs(t - float(g["t"])) / float(g["t"]))
     assert istep == n
     assert err <= FULL_RUN_TOL
+    assert pw <= FULL_RUN_TOL
     assert abs(t - float(g["t"])) <= FULL_RUN_TOL * abs(float(g["t"]))
     assert abs(dt - float(g["dt"])) <= 1e-6 * abs(float(g["dt"]))
 
@@ -62,8 +68,10 @@ def test_gpu_one_step_from_developed_state(name):
         prim = s.update_cpu(0)
         t, dt, _ = s.time(0)
     err = field_rel_err(prim, oprim)
-    record("one_step_" + name, field_rel_err=err, bit_identical=bit_identical_fraction(prim, oprim))
+    pw = pointwise_rel_err(prim, oprim, pb2)
+    record("one_step_" + name, field_rel_err=err, pointwise=pw, bit_identical=bit_identical_fraction(prim, oprim))
     assert err <= PER_STEP_TOL
+    assert pw <= PER_STEP_TOL
     assert abs(t - o.t) <= PER_STEP_TOL * o.t
 
 
@@ -94,20 +102,33 @@ def test_gpu_eos_download_matches_oracle():
 
 
 def test_kh_full_size_per_step_parity():
-    """Kelvin-Helmholtz 2048^2 (the measured workload): two steps from the same initial
-    state on the GPU and on the oracle."""
+    """Kelvin-Helmholtz 2048^2 (the measured workload), one step from the same input
+    state on the GPU and on the oracle, twice: from the initial state, and from the
+    oracle's state after that step (a fresh run from it, as the reference would start)."""
     pb = P.kelvin_helmholtz(2048)
     o = pyoracle.Oracle(pb)
+    o.advance(1)
+    oprim, _ = o.state()
     with Solver(pb) as s:
-        for k in range(2):
-            o.advance(1)
-            s.step(1)
-            prim = s.update_cpu(0)
-            oprim, _ = o.state()
-            err = field_rel_err(prim, oprim)
-            record("kh2048_step%d" % (k + 1), field_rel_err=err, bit_identical=bit_identical_fraction(prim, oprim))
-            assert err <= PER_STEP_TOL, "step %d" % (k + 1)
-            assert s.time(0)[0] == o.t
+        s.step(1)
+        prim = s.update_cpu(0)
+        assert s.time(0)[0] == o.t
+    cases = [("kh2048_step1", prim, oprim, pb)]
+    pb2 = pb.copy(ic=oprim)
+    o2 = pyoracle.Oracle(pb2)
+    o2.advance(1)
+    oprim2, _ = o2.state()
+    with Solver(pb2) as s:
+        s.step(1)
+        prim2 = s.update_cpu(0)
+        assert s.time(0)[0] == o2.t
+    cases.append(("kh2048_step_from_step1", prim2, oprim2, pb2))
+    for name, a, b, q in cases:
+        err = field_rel_err(a, b)
+        pw = pointwise_rel_err(a, b, q)
+        record(name, field_rel_err=err, pointwise=pw, bit_identical=bit_identical_fraction(a, b))
+        assert err <= PER_STEP_TOL, name
+        assert pw <= PER_STEP_TOL, name
 
 
 def test_kh_full_size_mass_conservation():
@@ -139,8 +160,10 @@ def test_batched_ensemble_equals_one_at_a_time_and_oracle():
         o.advance(n)
         oprim, _ = o.state()
         err = field_rel_err(batched[m], oprim)
-        record("ensemble_" + pb.name, steps=n, field_rel_err=err)
+        pw = pointwise_rel_err(batched[m], oprim, pb)
+        record("ensemble_" + pb.name, steps=n, field_rel_err=err, pointwise=pw)
         assert err <= FULL_RUN_TOL, pb.name
+        assert pw <= FULL_RUN_TOL, pb.name
         assert abs(times[m][0] - o.t) <= FULL_RUN_TOL * o.t
 
 
@@ -162,8 +185,11 @@ def test_gpu_fixed_gravity_1d_matches_oracle(case):
     o.advance(n)
     oprim, _ = o.state()
     err = field_rel_err(prim, oprim)
-    record("gravity_" + pb.name, steps=n, field_rel_err=err, bit_identical=bit_identical_fraction(prim, oprim))
+    pw = pointwise_rel_err(prim, oprim, pb)
+    record("gravity_" + pb.name, steps=n, field_rel_err=err, pointwise=pw,
+           bit_identical=bit_identical_fraction(prim, oprim))
     assert err <= FULL_RUN_TOL
+    assert pw <= FULL_RUN_TOL
     assert abs(t - o.t) <= FULL_RUN_TOL * o.t
     # the acceleration acts: the result differs from the run without it
     o0 = pyoracle.Oracle(pb.copy(grav=(0.0, 0.0, 0.0)))

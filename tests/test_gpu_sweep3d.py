@@ -4,18 +4,20 @@ grids and on 2-D (r, theta) ones, symmetric and with seeded noise (shock tagging
 rotation through the pole rows, restriction of the phi velocity into the Gamma slot),
 reflecting and SPHERICAL_ORIGIN boundaries.
 
-Error measure per variable: max |gpu - ref| over the zones divided by the largest
-magnitude of that variable (density, internal energy) or of any velocity component
-(the three velocities share one scale: in the symmetric blast v^theta and v^phi are
-round-off).  Bars as for the 1-D/2-D sweeps: 1e-9 after a whole fixture run, 1e-12
-for one step.
+Error measures: pointwise (tests/_cases.py pointwise_rel_err: density and internal
+energy relative at every zone, each physical velocity component over the zone's own
+speed scale max(|v|, c_s), with the library's zone metric), and field-relative per
+variable (max |gpu - ref| over the zones divided by the largest magnitude of that
+variable, or of any velocity component: the three velocities share one scale, since in
+the symmetric blast v^theta and v^phi are round-off).  Bars as for the 1-D/2-D sweeps,
+both measures: 1e-9 after a whole fixture run, 1e-12 for one step.
 """
 import numpy as np
 import pytest
 
 from medusa_b200 import problems as P
 from medusa_b200.solver import Solver
-from tests._cases import golden_cases3d, load_golden, record
+from tests._cases import golden_cases3d, load_golden, pointwise_rel_err, record, zone_gcov
 
 pytestmark = pytest.mark.gpu
 
@@ -42,9 +44,11 @@ def test_3d_full_run_matches_reference_fixture(name):
         prim = s.update_cpu(0)
         t, dt, istep = s.time(0)
     e = err3(prim, g["prim"])
-    record("sweep3d_full_" + name, steps=n, err=e, bit_identical=float(np.mean(prim == g["prim"])))
+    pw = pointwise_rel_err(prim, g["prim"], pb, zone_gcov(pb))
+    record("sweep3d_full_" + name, steps=n, err=e, pointwise=pw, bit_identical=float(np.mean(prim == g["prim"])))
     assert istep == n
     assert e <= FULL_RUN_TOL
+    assert pw <= FULL_RUN_TOL
     assert abs(t - float(g["t"])) <= FULL_RUN_TOL * float(g["t"])
 
 
@@ -57,7 +61,9 @@ def test_3d_one_step_from_developed_state(name):
         prim = s.update_cpu(0)
         t, _, _ = s.time(0)
     e = err3(prim, g["prim1"])
-    record("sweep3d_step_" + name, err=e, bit_identical=float(np.mean(prim == g["prim1"])))
+    pw = pointwise_rel_err(prim, g["prim1"], pb, zone_gcov(pb))
+    record("sweep3d_step_" + name, err=e, pointwise=pw, bit_identical=float(np.mean(prim == g["prim1"])))
+    assert pw <= PER_STEP_TOL
     assert e <= PER_STEP_TOL
     assert abs(t - float(g["t1"])) <= PER_STEP_TOL * float(g["t1"])
 
