@@ -43,6 +43,7 @@ KH: a replica); there is no collective on the data path.
 """
 import argparse
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -629,24 +630,45 @@ def run_kh(args, ctx):
 
 SEDOV3D = (384, 128, 256)
 SEDOV3D_SAMPLE = (96, 64, 128)
-SEDOV3D_DR_MIN = 1.0e-3     # innermost zone width of the SINH radial map; r spans [0, 1]
+SEDOV3D_DR_MIN = 1.0e-3     # innermost zone width of the "sinh" radial map; r spans [0, 1]
+SEDOV3D_R_LOG = 1.0e-3      # the "sinh-r1e-3" map: log-spaced zones from r = 1e-3 to 1
 
 
-def sedov3d_problem(dims, radius="sinh"):
-    """The 3-D Sedov workload: E = 1 deposited inside r < 0.02, on the SINH radial map
-    (zones SEDOV3D_DR_MIN x 384/n1 wide at the centre, log-like spacing outside rtrans)
-    or the uniform radius."""
+def sedov3d_problem(dims, radius="sinh-r1e-3"):
+    """The 3-D Sedov workload: E = 1 deposited inside r < 0.02, on
+      - "sinh-r1e-3" (default): the SINH radial map with rtrans = 1e-3, i.e. zones
+        log-spaced from r = 1e-3 to 1 (about 2e-5 wide inside r = 1e-3).  A purely
+        log-spaced radius starting at r = 1e-3 (RCOORD=LOG) is rejected on the 3-D
+        dendritic grid by the reference's own init_dendritic (4-to-1 phi refinement) and
+        by the library alike;
+      - "sinh": the SINH map with zones SEDOV3D_DR_MIN x 384/n1 wide at the centre;
+      - "uniform": the uniform radius."""
     from medusa_b200 import problems as P
     if radius == "uniform":
         return P.sedov_3d(*dims)
+    if radius == "sinh-r1e-3":
+        return P.sedov_3d(*dims, r_dep=0.02, coords="sinh_rt", r_in=SEDOV3D_R_LOG)
     return P.sedov_3d(*dims, r_dep=0.02, dr_min=SEDOV3D_DR_MIN * SEDOV3D[0] / dims[0])
 
 
-def sedov3d_workload_name(dims, radius="sinh"):
-    return "sedov_3d_dendritic_spherical_%s%dx%dx%d_fp64" % ("sinh_r_" if radius == "sinh" else "", *dims)
+def sedov3d_workload_name(dims, radius="sinh-r1e-3"):
+    tag = {"sinh": "sinh_r_", "uniform": "", "sinh-r1e-3": "log_r_1e-3_to_1_sinh_"}[radius]
+    return "sedov_3d_dendritic_spherical_%s%dx%dx%d_fp64" % (tag, *dims)
 
 
-def cpu_baseline_sedov3d(steps=2, radius="sinh"):
+def sedov3d_grid_text(pb, radius):
+    from medusa_b200 import problems as P
+    e = P.radial_edges(pb)
+    if radius == "uniform":
+        return "uniform radius"
+    if radius == "sinh-r1e-3":
+        return ("SINH radial map with rtrans %.1e (RCOORD=SINH): zones log-spaced from r = 1e-3 to 1 "
+                "(d ln r = %.4f at r = 1), %.2e wide inside r = 1e-3" % (pb.rtrans, math.log(e[-1] / e[-2]), e[1]))
+    return ("SINH radial map (RCOORD=SINH, rtrans %.4f): zones %.1e wide at the centre, %.1e at r = 1"
+            % (pb.rtrans, e[1], 1.0 - e[-2]))
+
+
+def cpu_baseline_sedov3d(steps=2, radius="sinh-r1e-3"):
     """Reference CPU build (its Makefile flags), one core, `steps` RK2 steps of the same
     Sedov blast on a smaller dendritic grid (96 x 64 x 128 before coarsening, the same
     radial map scaled to 96 zones): the full grid needs several GB of host memory for the
@@ -712,13 +734,15 @@ def run_sedov3d(args, ctx):
                 "shock_radius_fp64": r_of(ref), "shock_radius_mixed": r_of(mix),
                 "shock_radius_sedov": A.sedov_shock_radius(1.0, t_end, 1.0, pb.gam),
                 "dr_at_shock": float(np.interp(r_of(ref), rc, np.diff(P.radial_edges(pb))))}
+    full = sedov3d_full_run(ctx, pb, args.sedov3d_t_end) if args.sedov3d_t_end > 0.0 else None
     if ctx.rank != 0:
         return
     peak, peak_kind = read_peaks()
     b_stage1 = 360.0
     achieved = b_stage1 * ncell / (st["stage1"] / 1e3) / 1e9
-    traffic = read_profile_value("sweep3d_sedov_sinh_ncu.md" if args.sedov3d_radius == "sinh" else
-                                 "sweep3d_sedov_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
+    traffic = read_profile_value({"sinh": "sweep3d_sedov_sinh_ncu.md", "uniform": "sweep3d_sedov_ncu.md",
+                                  "sinh-r1e-3": "sweep3d_sedov_log_r1e-3_ncu.md"}[args.sedov3d_radius],
+                                 "TRAFFIC_PER_LAUNCH_STAGE1_BYTES")
     line = {
         "metric": "zone-updates/s", "value": value, "unit": "zone-updates/s",
         "n_gpus": ctx.world, "steps": K, "warmup": W, "ms_per_step": ms / K,
@@ -727,9 +751,7 @@ def run_sedov3d(args, ctx):
         "config": {"workload": sedov3d_workload_name(dims, args.sedov3d_radius), "global_batch": ctx.world,
                    "seq_len": ncell, "parallelism": "replicas" if ctx.world > 1 else "single",
                    "precision": "plain FP64 (reference operation order)",
-                   "grid": ("SINH radial map (RCOORD=SINH, rtrans %.4f): zones %.1e wide at the centre, %.1e at "
-                            "r = 1" % (pb.rtrans, P.radial_edges(pb)[1], 1.0 - P.radial_edges(pb)[-2])
-                            if args.sedov3d_radius == "sinh" else "uniform radius"),
+                   "grid": sedov3d_grid_text(pb, args.sedov3d_radius),
                    "l2": "inputs larger than L2 (state 2 x %.0f MB)" % (ncell * 40 / 1e6)},
         "gpu_launches": 10 * K,
         "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / K,
@@ -747,9 +769,79 @@ def run_sedov3d(args, ctx):
                   "precision": "FP32 reconstruction and HLLC wave speeds, FP64 state, fluxes, sources, dt",
                   "accuracy_vs_fp64": accuracy},
     }
+    if full is not None:
+        line["full_run"] = full
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_sedov3d(radius=args.sedov3d_radius)
     print(json.dumps(line), flush=True)
+
+
+def sedov3d_full_run(ctx, pb, t_end, chunk=2000):
+    """The Sedov blast run from t = 0 to t_end in plain FP64 and in mixed precision (each
+    step the main.c loop, the last one clipped onto t_end); device time with CUDA events;
+    L1 of density and total energy density against the Sedov-Taylor solution (shell
+    averages of the analytic state per radial row, volume-weighted over the zones), the
+    mixed result against the FP64 one, and mass and energy drift over the run."""
+    import numpy as np
+    import torch
+    import medusa_b200
+    from medusa_b200 import analytic as A
+    from medusa_b200 import problems as P
+    from medusa_b200.solver import PREC_FP64, PREC_MIXED, grid3d_counts, grid3d_zone_gcov, grid3d_zone_volumes
+
+    vol = grid3d_zone_volumes(pb)
+    gcov = grid3d_zone_gcov(pb)
+    nj, nk, _ = grid3d_counts(pb)
+    per_row = np.add.reduceat(nk, np.concatenate([[0], np.cumsum(nj)[:-1]]))
+    edges = P.radial_edges(pb)
+
+    def etot(prim):
+        return 0.5 * prim[:, 0] * np.sum(gcov * prim[:, 2:5] ** 2, axis=1) + prim[:, 1]
+
+    def run(precision):
+        with medusa_b200.Solver(pb.copy(tmax=t_end), precision=precision, device=ctx.local) as s:
+            m0, e0 = s.conserved_totals()
+            stream = torch.cuda.ExternalStream(s.stream, device=ctx.local)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            w0 = time.time()
+            ev0.record(stream)
+            while True:
+                s.step(chunk)
+                t, _, istep = s.time(0)
+                if t >= t_end * (1.0 - 1.0e-12):
+                    break
+            ev1.record(stream)
+            ev1.synchronize()
+            s.synchronize()
+            wall = time.time() - w0
+            m1, e1 = s.conserved_totals()
+            prim = s.update_cpu(0)
+            return {"prim": prim, "t": t, "steps": istep, "device_ms": ev0.elapsed_time(ev1), "wall_s": wall,
+                    "mass_drift": float((m1[0] - m0[0]) / m0[0]), "energy_drift": float((e1[0] - e0[0]) / e0[0])}
+
+    out = {"t_end": t_end}
+    res = {}
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        r = run(prec)
+        ana = A.sedov_row_averages(edges, r["t"], pb.gam, energy=1.0, rho0=1.0, p_amb=1.0e-5)
+        rho_a = np.repeat(ana[:, 0], per_row)
+        e_a = np.repeat(ana[:, 3], per_row)
+        res[name] = r
+        out[name] = {"steps": r["steps"], "t": r["t"], "device_ms": r["device_ms"], "wall_s": r["wall_s"],
+                     "zone_updates_per_s": pb.ncell * r["steps"] / (r["device_ms"] / 1e3),
+                     "l1_rho_vs_sedov": A.l1_rel(r["prim"][:, 0], rho_a, vol),
+                     "l1_etot_vs_sedov": A.l1_rel(etot(r["prim"]), e_a, vol),
+                     "mass_drift": r["mass_drift"], "energy_drift": r["energy_drift"]}
+    a, b = res["mixed"]["prim"], res["fp64"]["prim"]
+    out["mixed_vs_fp64"] = {"l1_rho": A.l1_rel(a[:, 0], b[:, 0], vol), "l1_u": A.l1_rel(a[:, 1], b[:, 1], vol),
+                            "l1_etot": A.l1_rel(etot(a), etot(b), vol),
+                            "l1_rho_over_fp64_truncation": A.l1_rel(a[:, 0], b[:, 0], vol) /
+                            out["fp64"]["l1_rho_vs_sedov"]}
+    S = A.SedovTaylor(pb.gam)
+    out["sedov"] = {"xi0": S.xi0, "shock_radius": S.shock_radius(1.0, res["fp64"]["t"]),
+                    "reference": "Sedov-Taylor point blast, closed form (Sedov 1959; Kamm & Timmes 2007), "
+                                 "shell averages per radial row"}
+    return out
 
 
 def run_sod1d(args, ctx):
@@ -920,9 +1012,14 @@ def main():
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
     ap.add_argument("--sedov3d-dims", default="",
                     help="sedov3d: n1,n2,n3 of the grid (default 384,128,256; smaller grids for profiling)")
-    ap.add_argument("--sedov3d-radius", default="sinh", choices=["sinh", "uniform"],
-                    help="sedov3d: radial map; sinh = zones 1e-3 wide at the centre widening geometrically "
-                         "to r = 1 (RCOORD=SINH), uniform = 1/n1 wide")
+    ap.add_argument("--sedov3d-radius", default="sinh-r1e-3", choices=["sinh-r1e-3", "sinh", "uniform"],
+                    help="sedov3d: radial map; sinh-r1e-3 = zones log-spaced from r = 1e-3 to 1 (RCOORD=SINH "
+                         "with rtrans 1e-3), sinh = zones 1e-3 wide at the centre widening geometrically to "
+                         "r = 1, uniform = 1/n1 wide")
+    ap.add_argument("--sedov3d-t-end", type=float, default=0.0,
+                    help="sedov3d: also run the blast to this time in FP64 and in mixed precision and report "
+                         "L1 of density and energy against the Sedov-Taylor solution and against each other, "
+                         "and the mass and energy drift (0: skip; the configured end time is 0.05)")
     ap.add_argument("--sedov3d-accuracy-steps", type=int, default=60,
                     help="sedov3d: steps of the FP64 run the mixed run is compared with at equal time")
     ap.add_argument("--server-frac-2d", type=float, default=0.0,

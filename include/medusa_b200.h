@@ -62,6 +62,10 @@ extern "C" {
                                   centre, growing geometrically outside rtrans */
 #define MDG_RCOORD_SINH_MODIFIED 2  /* the SINH map minus facta [sigmoid((|x| - factb) / factc)
                                        - sigmoid(-factb / factc)] (the reference's default) */
+#define MDG_RCOORD_LOG 3       /* r = rtrans exp(|x| / rtrans): zones log-spaced outwards from
+                                  r = rtrans at x = 0 (inner zone width dx there).  Not one of
+                                  the reference's maps: added in the form of its SINH branch
+                                  for grids that start away from the origin */
 /* theta maps th(x), x in [-1, 1] (THCOORD, metric_spherical_general.c:222-290) */
 #define MDG_THCOORD_UNIFORM 0  /* th = pi (x + 1) / 2 */
 #define MDG_THCOORD_POLYTH 1   /* th = poly_norm x (1 + (x/poly_xt)^poly_alpha / (poly_alpha + 1)) + pi/2,

@@ -20,6 +20,8 @@ void build_mixed_table(const mdg_problem_desc &d, int dir, float *tab, int64_t s
 int conn_is_sparse(const double *tab, int64_t stride, int64_t off, int nrec);
 void spherical_1d_constants(double &area_k, double &th1, double &th2, double &tc);
 void build_grid3(const mdg_problem_desc &d, Grid3Host &h);
+void dendritic_zone_counts(const mdg_problem_desc &d, Grid3Host &h);
+int64_t dendritic_refine_errors(const Grid3Host &h);
 }
 
 using namespace mdg;
@@ -108,7 +110,8 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   auto bad = [&](const char *m) { why = m; return MDG_ERR_INVALID; };
   if (d.ndim != 1 && d.ndim != 2 && d.ndim != 3) return bad("ndim must be 1, 2 or 3");
   if (d.ndim != ndim0) return bad("all problems of a solver must have the same ndim");
-  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH && d.rcoord != MDG_RCOORD_SINH_MODIFIED)
+  if (d.rcoord != MDG_RCOORD_UNIFORM && d.rcoord != MDG_RCOORD_SINH && d.rcoord != MDG_RCOORD_SINH_MODIFIED &&
+      d.rcoord != MDG_RCOORD_LOG)
     return bad("unknown radial map (rcoord)");
   if (d.thcoord != MDG_THCOORD_UNIFORM && d.thcoord != MDG_THCOORD_POLYTH) return bad("unknown theta map (thcoord)");
   if (d.thcoord != MDG_THCOORD_UNIFORM) {
@@ -170,6 +173,20 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
     }
     if (three && (d.bc_lo[2] == MDG_BC_PERIODIC) != (d.bc_hi[2] == MDG_BC_PERIODIC))
       return bad("periodic boundaries must be paired");
+    if (three) {
+      // the reference's init_dendritic exits on 4-to-1 phi refinement (utils.c:548-586)
+      Grid3Host h;
+      dendritic_zone_counts(d, h);
+      const int64_t cells = dendritic_refine_errors(h);
+      if (cells > 0) {
+        snprintf(buf, sizeof buf,
+                 "the dendritic grid refines 4-to-1 in phi in %lld cells (the reference's init_dendritic "
+                 "rejects it): the radius grows too fast for 2-to-1 coarsening near r = r(startx)",
+                 (long long)cells);
+        why = buf;
+        return MDG_ERR_INVALID;
+      }
+    }
     return MDG_OK;
   }
   if (d.n1 < 2 || d.n1 > (1 << 28)) return bad("n1 out of range [2, 2^28]");

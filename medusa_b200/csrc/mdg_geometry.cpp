@@ -54,9 +54,12 @@ static double romb(double x0, double x1, double (*f)(double))
 }
 
 // The coordinate maps of the problem being built (RCOORD and THCOORD,
-// metric_spherical_general.c:149-290): r(x) UNIFORM |x|, SINH rtrans sinh(|x|/rtrans) or
-// SINH_MODIFIED (the SINH map minus a sigmoid step of height facta), th(x) UNIFORM or
-// POLYTH.  The integrands below are plain functions handed to romb(), so the maps are
+// metric_spherical_general.c:149-290): r(x) UNIFORM |x|, SINH rtrans sinh(|x|/rtrans),
+// SINH_MODIFIED (the SINH map minus a sigmoid step of height facta) or LOG
+// rtrans exp(|x|/rtrans) (zones log-spaced outwards from r = rtrans at x = 0; the
+// reference has no such map: it is written in the form of its SINH branch, and the
+// oracle's reference builds with RCOORD=LOG carry the same three expressions), th(x)
+// UNIFORM or POLYTH.  The integrands below are plain functions handed to romb(), so the maps are
 // per-thread state that CoordMap sets for the duration of one public build call (the
 // solve server builds tables in the submitting threads).
 namespace {
@@ -92,6 +95,7 @@ static double r_of_x(double x)
 {
   const MapState &m = t_map;
   if (m.rcoord == MDG_RCOORD_SINH) return m.rtrans * std::sinh(std::fabs(x) / m.rtrans);
+  if (m.rcoord == MDG_RCOORD_LOG) return m.rtrans * std::exp(std::fabs(x) / m.rtrans);
   if (m.rcoord == MDG_RCOORD_SINH_MODIFIED)
     return m.rtrans * std::sinh(std::fabs(x) / m.rtrans) - m.facta * sigmoid((std::fabs(x) - m.factb) / m.factc) +
            m.facta * sigmoid(-m.factb / m.factc);
@@ -101,6 +105,7 @@ static double dr_dx(double x)
 {
   const MapState &m = t_map;
   if (m.rcoord == MDG_RCOORD_SINH) return std::cosh(std::fabs(x) / m.rtrans);
+  if (m.rcoord == MDG_RCOORD_LOG) return std::exp(std::fabs(x) / m.rtrans);
   if (m.rcoord == MDG_RCOORD_SINH_MODIFIED) {
     const double expval = std::exp(-(std::fabs(x) - m.factb) / m.factc);
     return std::cosh(std::fabs(x) / m.rtrans) - m.facta * expval / m.factc / (1 + expval) / (1 + expval);
@@ -111,6 +116,7 @@ static double d2r_dx2(double x)
 {
   const MapState &m = t_map;
   if (m.rcoord == MDG_RCOORD_SINH) return std::sinh(std::fabs(x) / m.rtrans) / m.rtrans;
+  if (m.rcoord == MDG_RCOORD_LOG) return std::exp(std::fabs(x) / m.rtrans) / m.rtrans;
   if (m.rcoord == MDG_RCOORD_SINH_MODIFIED) {
     const double expval = std::exp(-(std::fabs(x) - m.factb) / m.factc);
     return std::sinh(std::fabs(x) / m.rtrans) / m.rtrans -
@@ -441,26 +447,18 @@ static double f_xth2g(double x) { return x * x * std::sin(th_of_x(x)) * dth_dx(x
 //   gcov, gcon, scale, conn   (941-1051, 837-939), conn[1][1][1] from the dendritic
 //                    neighbour areas (897-916)
 // with the reference's operation order (every product and sum as written there).
-void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
+// Zone counts of the dendritic grid, compute_dj / compute_dk (utils.c:181-366): nj per
+// radial row and nk per (i, j) row, ghost rows and columns included, and the row tables.
+void dendritic_zone_counts(const mdg_problem_desc &d, Grid3Host &h)
 {
   RadialMap rmap(d);
   const bool three = d.ndim == 3;
   const int n1 = d.n1, n2 = d.n2, n3 = three ? d.n3 : 1;
   h.ndim = three ? 3 : 2;
   h.n1 = n1; h.n2 = n2; h.n3 = n3;
-  const double sx0 = d.startx[0], sx1 = d.startx[1], sx2 = d.startx[2];
+  const double sx0 = d.startx[0], sx1 = d.startx[1];
   const double dx0 = d.dx[0], dx1 = d.dx[1], dx2 = d.dx[2];
   const double max_log2_aspect = 0.5;
-
-  // radial edges for the monopole gravity (init_coords, metric_spherical_general.c:577-583;
-  // gravity.c:300-303)
-  h.medge.assign((size_t)2 * (n1 + 1), 0.0);
-  for (int i = 0; i <= n1; i++) {
-    const double re = r_of_x(std::fabs(i * dx0 + sx0));
-    h.medge[i] = re * re;
-    h.medge[n1 + 1 + i] = dr_dx(sx0 + i * dx0);
-  }
-
   // theta zones per radial row
   h.nj.assign(n1 + 2 * NG, 0);
   auto NJ = [&](int i) -> int & { return h.nj[i + NG]; };
@@ -543,6 +541,52 @@ void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
       for (int j = NJ(i); j < NJ(i) + NG; j++) NK(i, j) = NK(i, 2 * NJ(i) - 1 - j);
     }
   }
+}
+
+// The refinement test of init_dendritic (utils.c:548-586): where theta refines 2:1 from
+// radial row i to i+1, phi must not refine 4:1 between the cell (i, j) and either of
+// the two cells (i+1, j') beside it; the reference prints each such cell (once per phi
+// zone of the row) and exits.  Returns the number of such (i, j, k) cells.  The
+// reference's other branch there (an inner row coarser in phi than the outer one,
+// which it coarsens to match) cannot occur: compute_dk takes every row's phi count at
+// least as large as its inner neighbour's.
+int64_t dendritic_refine_errors(const Grid3Host &h)
+{
+  if (h.ndim != 3) return 0;
+  int64_t bad = 0;
+  for (int i0 = 0; i0 < h.n1; i0++) {
+    const int i1 = i0 + 1;
+    if (h.dj(i0) / h.dj(i1) != 2) continue;
+    for (int j00 = 0; j00 < h.njr(i0); j00++) {
+      const int j10 = j00 * h.dj(i0) / h.dj(i1), j11 = j10 + 1;
+      if (h.dk(i0, j00) / h.dk(i1, j10) == 4 || h.dk(i0, j00) / h.dk(i1, j11) == 4) bad += h.n3 / h.dk(i0, j00);
+    }
+  }
+  return bad;
+}
+
+void build_grid3(const mdg_problem_desc &d, Grid3Host &h)
+{
+  RadialMap rmap(d);
+  const bool three = d.ndim == 3;
+  const int n1 = d.n1, n2 = d.n2, n3 = three ? d.n3 : 1;
+  const double sx0 = d.startx[0], sx1 = d.startx[1], sx2 = d.startx[2];
+  const double dx0 = d.dx[0], dx1 = d.dx[1], dx2 = d.dx[2];
+
+  // radial edges for the monopole gravity (init_coords, metric_spherical_general.c:577-583;
+  // gravity.c:300-303)
+  h.medge.assign((size_t)2 * (n1 + 1), 0.0);
+  for (int i = 0; i <= n1; i++) {
+    const double re = r_of_x(std::fabs(i * dx0 + sx0));
+    h.medge[i] = re * re;
+    h.medge[n1 + 1 + i] = dr_dx(sx0 + i * dx0);
+  }
+
+  dendritic_zone_counts(d, h);
+  auto NJ = [&](int i) -> int & { return h.nj[i + NG]; };
+  auto DJ = [&](int i) { return n2 / NJ(i); };
+  auto NK = [&](int i, int j) -> int & { return h.nk[h.rowbase[i + NG] + j + NG]; };
+  const int64_t nij = h.nij;
   auto DK = [&](int i, int j) { return n3 / NK(i, j); };
 
   // zone and face offsets

@@ -96,6 +96,8 @@ static void describe(mdg_problem_desc *d)
   d->rcoord = MDG_RCOORD_SINH;
 #elif (GEOM == SPHERICAL && RCOORD == SINH_MODIFIED)
   d->rcoord = MDG_RCOORD_SINH_MODIFIED;
+#elif (GEOM == SPHERICAL && defined(LOG) && RCOORD == LOG)
+  d->rcoord = MDG_RCOORD_LOG;   /* the RCOORD=LOG build of the oracle's reference sources */
 #else
   d->rcoord = MDG_RCOORD_UNIFORM;
 #endif

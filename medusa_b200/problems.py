@@ -41,6 +41,7 @@ PROB_DUST = 2               # problems/init_dustcollapse.c:104-113 (outer v^r ho
 RCOORD_UNIFORM = 0          # radial maps r(x), metric_spherical_general.c:149-219
 RCOORD_SINH = 1
 RCOORD_SINH_MODIFIED = 2
+RCOORD_LOG = 3              # r = rtrans exp(|x|/rtrans): log-spaced from r = rtrans (not a reference map)
 THCOORD_UNIFORM = 0         # theta maps th(x), metric_spherical_general.c:222-290
 THCOORD_POLYTH = 1
 RFACT_DEFAULT = (10 * 1e5, 15 * 1e5, 5 * 1e5)   # rx_info.facta/b/c, io.c:5008-5010
@@ -229,9 +230,10 @@ def kelvin_helmholtz(n1: int = 2048, n2: Optional[int] = None, seed: int = 20240
 def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                  p_ratio: float = 100.0, r0: float = 0.5, cfl: float = 0.8,
                  tmax: float = 1.0e100, floors: bool = True, dr_min: Optional[float] = None,
-                 coords: str = "sinh") -> Problem:
+                 coords: str = "sinh", r_in: Optional[float] = None) -> Problem:
     """1-D spherical problem on r in [0,1] (uniform radius; with dr_min the SINH radial
-    map, innermost zones dr_min wide), SPHERICAL_ORIGIN inner boundary (bc.c:776-803).
+    map, innermost zones dr_min wide), SPHERICAL_ORIGIN inner boundary (bc.c:776-803);
+    coords "log": r in [r_in, 1], log-spaced zones, reflecting inner boundary.
 
     kind='sod'   : rho, p = rho_ratio, p_ratio inside r<r0; 1, 1 outside; at rest;
                    OUTFLOW outer boundary.
@@ -242,7 +244,7 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
                    the hook's floors rho 1e-6, e 1e-7/(gam-1) (init_spherical_noh.c:22-23),
                    enforced (ENFORCE_FLOORS) unless floors=False.
     """
-    _, dx, map_ = _radial_grid(n1, dr_min, coords)
+    _, dx, map_ = _radial_grid(n1, dr_min, coords, r_in)
     rc = np.array([_maps(map_).r((i + 0.5) * dx) for i in range(n1)])
     ic = np.zeros((n1, NPRIM))
     bc_hi = OUTFLOW
@@ -273,7 +275,8 @@ def spherical_1d(kind: str, n1: int, gam: float, rho_ratio: float = 10.0,
         raise ValueError("unknown 1-D spherical problem kind %r" % kind)
     return Problem(name="sph1d_%s%s_%d" % (_map_tag(map_), kind, n1), ndim=1, geom=SPHERICAL,
                    n=(n1, 1, 1), startx=(0.0, -1.0, 0.0), dx=(dx, 2.0, 2.0 * math.pi), gam=gam, ic=ic,
-                   bc_lo=(SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW), bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
+                   bc_lo=(REFLECT if coords == "log" else SPHERICAL_ORIGIN, OUTFLOW, OUTFLOW),
+                   bc_hi=(bc_hi, OUTFLOW, OUTFLOW),
                    prob_kind=prob_kind, cfl=cfl, tmax=tmax, **fl, **map_)
 
 
@@ -304,6 +307,8 @@ class CoordMaps:
             fa, fb, fc = self.rfact
             sig = lambda y: 1.0 / (1.0 + math.exp(-y))
             return self.rtrans * math.sinh(ax / self.rtrans) - fa * sig((ax - fb) / fc) + fa * sig(-fb / fc)
+        if self.rcoord == RCOORD_LOG:
+            return self.rtrans * math.exp(ax / self.rtrans)
         return ax
 
     def th(self, x: float) -> float:
@@ -425,12 +430,46 @@ def dendritic_grid(n1: int, n2: int, n3: int, startx: tuple, dx: tuple, ndim: in
     return nj, nk
 
 
-def _radial_grid(n1: int, dr_min: Optional[float], coords: str = "sinh"):
+def dendritic_refine_errors(n2: int, n3: int, nj: list, nk: list) -> int:
+    """Cells (i, j, k) where phi refines 4-to-1 across a 2:1 theta refinement from radial
+    row i to i+1 -- the grids that init_dendritic (utils.c:548-586) rejects.  nj, nk as
+    dendritic_grid returns them (interior rows); the outer ghost row copies row n1-1."""
+    n1 = len(nj)
+    bad = 0
+    for i0 in range(n1 - 1):
+        dj0, dj1 = n2 // nj[i0], n2 // nj[i0 + 1]
+        if dj0 // dj1 != 2:
+            continue
+        row1 = nk[i0 + 1]
+        for j00 in range(nj[i0]):
+            j10 = j00 * dj0 // dj1
+            j11 = j10 + 1
+            # the ghost column j = nj reflects column nj - 1
+            k10 = row1[j10]
+            k11 = row1[j11] if j11 < len(row1) else row1[2 * len(row1) - 1 - j11]
+            dk0 = n3 // nk[i0][j00]
+            if dk0 // (n3 // k10) == 4 or dk0 // (n3 // k11) == 4:
+                bad += nk[i0][j00]
+    return bad
+
+
+def _radial_grid(n1: int, dr_min: Optional[float], coords: str = "sinh", r_in: Optional[float] = None):
     """(startx, dx0, map fields) of a radial grid on r in [0, 1]: uniform, or with dr_min
     the SINH map with innermost zones about dr_min wide (coords "sinh"), or the
     reference's default build maps, SINH_MODIFIED radius and POLYTH theta with the
-    parse_input parameters (coords "default")."""
+    parse_input parameters (coords "default"); coords "log" is the grid on [r_in, 1] with
+    log-spaced zones (RCOORD_LOG, rtrans = r_in, zone edges r_in (1/r_in)^(i/n1))."""
     startx = (0.0, -1.0, 0.0)
+    if coords == "log":
+        if not (r_in is not None and 0.0 < r_in < 1.0):
+            raise ValueError("the log-spaced radius needs 0 < r_in < 1")
+        return startx, r_in * math.log(1.0 / r_in) / n1, dict(rcoord=RCOORD_LOG, rtrans=r_in)
+    if coords == "sinh_rt":
+        # the SINH map with rtrans = r_in: uniform zones (dx wide) inside r ~ r_in, log-spaced
+        # outside it (r ~ (r_in/2) exp(x/r_in)), n1 zones to r = 1
+        if not (r_in is not None and 0.0 < r_in < 1.0):
+            raise ValueError("coords 'sinh_rt' needs 0 < r_in < 1 (the transition radius)")
+        return startx, r_in * math.asinh(1.0 / r_in) / n1, dict(rcoord=RCOORD_SINH, rtrans=r_in)
     if dr_min is None:
         return startx, 1.0 / n1, {}
     if coords == "default":
@@ -447,26 +486,31 @@ def _maps(map_: dict) -> CoordMaps:
 def _map_tag(map_: dict) -> str:
     if not map_:
         return ""
+    if map_.get("rcoord") == RCOORD_LOG:
+        return "log_"
     return "default_" if map_.get("thcoord", THCOORD_UNIFORM) == THCOORD_POLYTH else "sinh_"
 
 
 def _blast_energy_rows(n1, startx, dx0, map_, r_dep, energy, gam, p_amb) -> np.ndarray:
-    """Internal energy density per radial row of a blast: energy / (4/3 pi r_e^3) in the
-    rows whose centre lies inside r_dep (r_e the outer edge of the last of them), the
-    ambient p_amb / (gam - 1) elsewhere."""
+    """Internal energy density per radial row of a blast: energy / (4/3 pi (r_e^3 - r_0^3))
+    in the rows whose centre lies inside r_dep (r_e the outer edge of the last of them,
+    r_0 the inner edge of the grid: 0 for a grid from the origin), the ambient
+    p_amb / (gam - 1) elsewhere."""
     m = _maps(map_)
     rc = np.array([m.r(startx[0] + (i + 0.5) * dx0) for i in range(n1)])
     inside = rc < r_dep
     i_e = (np.nonzero(inside)[0].max() + 1) if inside.any() else 1
     r_e = m.r(startx[0] + i_e * dx0)
-    u_dep = energy / (4.0 / 3.0 * math.pi * r_e ** 3)
+    r_0 = m.r(startx[0])
+    u_dep = energy / (4.0 / 3.0 * math.pi * (r_e ** 3 - r_0 ** 3))
     return np.where(inside, u_dep, p_amb / (gam - 1.0))
 
 
 def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, energy: float = 1.0,
              r_dep: float = 0.02, p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100,
              bc_inner: int = REFLECT, bc_pole: int = REFLECT, noise: float = 0.0,
-             seed: int = 20240603, dr_min: Optional[float] = None, coords: str = "sinh") -> Problem:
+             seed: int = 20240603, dr_min: Optional[float] = None, coords: str = "sinh",
+             r_in: Optional[float] = None) -> Problem:
     """3-D Sedov blast on the dendritic spherical grid (the structure of
     problems/init_sedov.c:3-164): r in [0, 1] uniform, theta in [0, pi], phi in [0, 2 pi);
     rho = 1, p = p_amb, at rest, and the energy `energy` deposited as a uniform internal
@@ -478,8 +522,12 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
     With dr_min the radius follows the SINH map instead (RCOORD=SINH, the map of the
     reference's own Sedov hook): the innermost zones are dr_min wide and the zone widths
     grow geometrically outwards to r = 1 (coords "default": the reference's default
-    build maps, SINH_MODIFIED radius and POLYTH theta)."""
-    startx, dx, map_ = _radial_grid(n1, dr_min, coords)
+    build maps, SINH_MODIFIED radius and POLYTH theta).  coords "log" puts the grid on
+    r in [r_in, 1] with log-spaced zones (RCOORD_LOG): the inner boundary is the sphere
+    r = r_in (reflecting by default) and the deposit fills the shells from r_in; coords
+    "sinh_rt" is the SINH map with its transition radius at r_in: zones log-spaced from
+    about r_in to 1 and uniform inside (the origin stays in the grid)."""
+    startx, dx, map_ = _radial_grid(n1, dr_min, coords, r_in)
     dx = (dx, 2.0 / n2, 2.0 * math.pi / n3)
     nj, nk = dendritic_grid(n1, n2, n3, startx, dx, maps=_maps(map_))
     counts = np.array([sum(row) for row in nk])
@@ -502,12 +550,15 @@ def sedov_3d(n1: int = 384, n2: int = 128, n3: int = 256, gam: float = 1.4, ener
 def sedov_2d_spherical(n1: int = 256, n2: int = 128, gam: float = 1.4, energy: float = 1.0, r_dep: float = 0.02,
                        p_amb: float = 1.0e-5, cfl: float = 0.8, tmax: float = 1.0e100, bc_inner: int = REFLECT,
                        bc_pole: int = REFLECT, noise: float = 0.0, seed: int = 20240604,
-                       dr_min: Optional[float] = None, coords: str = "sinh") -> Problem:
+                       dr_min: Optional[float] = None, coords: str = "sinh",
+                       r_in: Optional[float] = None) -> Problem:
     """Axisymmetric (r, theta) Sedov blast on the 2-D dendritic spherical grid: theta zones
     double outwards from 2 at the centre (compute_dj, utils.c:181-238); otherwise as
     sedov_3d (energy in the zones inside r_dep, seeded noise in density and velocities,
-    the SINH radial map with dr_min, the default build maps with coords "default")."""
-    startx, dx, map_ = _radial_grid(n1, dr_min, coords)
+    the SINH radial map with dr_min, the default build maps with coords "default", the
+    log-spaced radius on [r_in, 1] with coords "log", the SINH map with rtrans = r_in with
+    coords "sinh_rt")."""
+    startx, dx, map_ = _radial_grid(n1, dr_min, coords, r_in)
     dx = (dx, 2.0 / n2, 2.0 * math.pi)
     nj, _ = dendritic_grid(n1, n2, 1, startx, dx, ndim=2, maps=_maps(map_))
     ncell = int(sum(nj))

@@ -105,7 +105,46 @@ CONFIGS = {
                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
     "sph3d_mono": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
+    # a radius log-spaced outwards from rtrans (RCOORD=LOG, r = rtrans exp(|x|/rtrans)): not
+    # one of the reference's maps, added to a generated copy of its spherical metric (see
+    # log_metric_source below) for grids that start away from the origin
+    "sph1d_log": dict(NDIM="1", GEOM="SPHERICAL", DENDRITIC_GRID="FALSE",
+                      RCOORD="LOG", THCOORD="UNIFORM"),
+    "sph2d_log": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                      RCOORD="LOG", THCOORD="UNIFORM"),
+    "sph3d_log": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                      RCOORD="LOG", THCOORD="UNIFORM"),
 }
+
+# Value of the LOG enumerator in the generated build.h (enumerators.h:5-11 uses 0-6).
+LOG_ENUM = 7
+
+# The three branches added to r_of_x, dr_dx and d2r_dx2 of the generated metric copy
+# (metrics/metric_spherical_general.c:149-219), in the form of their SINH branches.
+LOG_BRANCHES = {
+    "double r_of_x(r_of_x_struct_t rx_info,double x)\n{":
+        "  #if (RCOORD==LOG)\n  return rx_info.rtrans*exp(fabs(x)/rx_info.rtrans);\n  #endif\n",
+    "double dr_dx(double x)\n{":
+        "  #if (RCOORD==LOG)\n  return exp(fabs(x)/rx_info.rtrans);\n  #endif\n",
+    "double d2r_dx2(double x)\n{":
+        "  #if (RCOORD==LOG)\n  return exp(fabs(x)/rx_info.rtrans)/rx_info.rtrans;\n  #endif\n",
+}
+
+
+def log_metric_source(ref_root, cdir):
+    """Write <cdir>/metric_spherical_general_log.c: the reference's spherical metric with a
+    LOG branch inserted at the top of r_of_x, dr_dx and d2r_dx2 (nothing else changed),
+    and return its path.  The copy is a build product under oracle/_ref/ only."""
+    src = open(os.path.join(ref_root, "metrics", "metric_spherical_general.c")).read()
+    for anchor, branch in LOG_BRANCHES.items():
+        if src.count(anchor) != 1:
+            raise RuntimeError("metric_spherical_general.c: cannot place the LOG branch after %r" % anchor)
+        src = src.replace(anchor, anchor + "\n" + branch)
+    out = os.path.join(cdir, "metric_spherical_general_log.c")
+    if not (os.path.exists(out) and open(out).read() == src):
+        with open(out, "w") as f:
+            f.write(src)
+    return out
 
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]
 FAST_FLAGS = ["-O3", "-ffast-math", "-ftree-vectorize", "-fpeel-loops"]
@@ -113,6 +152,8 @@ FAST_FLAGS = ["-O3", "-ffast-math", "-ftree-vectorize", "-fpeel-loops"]
 
 def write_build_h(path, defs):
     lines = ["#ifndef BUILD_H_", "#define BUILD_H_", "", '#include "enumerators.h"', ""]
+    if defs.get("RCOORD") == "LOG":
+        lines.append("#define LOG %d" % LOG_ENUM)
     for k in DEF_ORDER:
         lines.append("#define %s %s" % (k, defs[k]))
     lines.append("")
@@ -135,7 +176,9 @@ def build_config(name, cfg, ref_root, force=False):
     srcs = [os.path.join(ref_root, s) for s in REF_SOURCES]
     if defs["GRAV"] != "NO_GRAV":
         srcs.append(os.path.join(ref_root, "gravity.c"))
-    if defs["GEOM"] == "SPHERICAL":
+    if defs["GEOM"] == "SPHERICAL" and defs["RCOORD"] == "LOG":
+        srcs.append(log_metric_source(ref_root, cdir))
+    elif defs["GEOM"] == "SPHERICAL":
         srcs.append(os.path.join(ref_root, "metrics", "metric_spherical_general.c"))
     else:
         srcs.append(os.path.join(SHIM, "metric_cartesian_current.c"))
@@ -148,8 +191,10 @@ def build_config(name, cfg, ref_root, force=False):
                 and os.path.getmtime(target) >= max(os.path.getmtime(d) for d in deps)):
             built.append(target)
             continue
+        # the generated LOG copy includes "../decs.h" as its original does from metrics/
+        inc = ["-I" + os.path.join(ref_root, "metrics")] if defs["RCOORD"] == "LOG" else []
         cmd = (["gcc", "-std=gnu99", "-w"] + flags +
-               ["-I" + cdir, "-I" + ref_root, "-include", "limits.h", "-o", target] + srcs + ["-lm"])
+               ["-I" + cdir, "-I" + ref_root] + inc + ["-include", "limits.h", "-o", target] + srcs + ["-lm"])
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)

@@ -92,7 +92,7 @@ typedef struct {
   int enforce_floors;
   double rho_floor, e_floor;
   double grav[3];
-  int rcoord;          /* radial map: 0 UNIFORM, 1 SINH (the RCOORD build switch) */
+  int rcoord;          /* radial map: 0 UNIFORM, 1 SINH, 3 LOG (the RCOORD build switch) */
   double rfact[3];     /* SINH_MODIFIED parameters: not restated here (the reference's own builds check it) */
   int thcoord;         /* theta map: 0 UNIFORM only here */
   double poly_xt, poly_alpha;
@@ -160,23 +160,27 @@ static double romb(double x0, double x1, double (*f)(double))
 }
 
 /* metric_spherical_general.c maps (149-219) and integrands, RCOORD=UNIFORM or SINH,
- * THCOORD=UNIFORM; the map of the problem being built (the integrands are plain
- * functions handed to romb) */
+ * THCOORD=UNIFORM, and the LOG map r = rtrans exp(|x|/rtrans) that the oracle's
+ * RCOORD=LOG reference builds add in the form of the SINH branch; the map of the
+ * problem being built (the integrands are plain functions handed to romb) */
 static int g_rcoord = 0;
 static double g_rtrans = 1.0;
 static double r_of_x(double x)
 {
   if (g_rcoord == 1) return g_rtrans*sinh(fabs(x)/g_rtrans);
+  if (g_rcoord == 3) return g_rtrans*exp(fabs(x)/g_rtrans);
   return fabs(x);
 }
 static double dr_dx(double x)
 {
   if (g_rcoord == 1) return cosh(fabs(x)/g_rtrans);
+  if (g_rcoord == 3) return exp(fabs(x)/g_rtrans);
   return 1.0;
 }
 static double d2r_dx2(double x)
 {
   if (g_rcoord == 1) return sinh(fabs(x)/g_rtrans)/g_rtrans;
+  if (g_rcoord == 3) return exp(fabs(x)/g_rtrans)/g_rtrans;
   return 0.0;
 }
 static double th_of_x(double x)

@@ -175,6 +175,8 @@ def ref_config(pb) -> str:
     name = ("cart%dd" if pb.geom == 0 else "sph%dd") % pb.ndim
     if getattr(pb, "rcoord", 0) == 1:
         name += "_sinh"
+    elif getattr(pb, "rcoord", 0) == 3:
+        name += "_log"
     elif getattr(pb, "rcoord", 0) == 2 and getattr(pb, "thcoord", 0) == 1:
         name += "_default"
     if any(g != 0.0 for g in getattr(pb, "grav", (0.0, 0.0, 0.0))):

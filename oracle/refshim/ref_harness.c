@@ -172,6 +172,8 @@ REF_API int ref_init(const ref_params *prm, const double *ic)
   if (prm->rcoord != 1) { fprintf(stderr, "ref_init: this build has the SINH radial map\n"); return -1; }
 #elif (RCOORD == SINH_MODIFIED)
   if (prm->rcoord != 2) { fprintf(stderr, "ref_init: this build has the SINH_MODIFIED radial map\n"); return -1; }
+#elif (defined(LOG) && RCOORD == LOG)
+  if (prm->rcoord != 3) { fprintf(stderr, "ref_init: this build has the LOG radial map\n"); return -1; }
 #else
   if (prm->rcoord != 0) { fprintf(stderr, "ref_init: this build has the uniform radial map\n"); return -1; }
 #endif

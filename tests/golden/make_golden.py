@@ -6,7 +6,7 @@ primitive states, the time and the last dt as compressed .npz files next to this
 The fixtures pin the CPU oracle (tests/test_golden.py) and the GPU sweep
 (tests/test_gpu_parity.py) without needing the reference tree at test time.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [fixture names]
 """
 import os
 import sys
@@ -39,6 +39,9 @@ def cases():
         "rt2d_32x64_grav": (P.rayleigh_taylor_2d(32, 64, g=-0.5, noise=0.05), 40),
         # the SINH radial map (zones 2e-3 wide at the centre, widening outwards)
         "sph1d_sinh_sedov_192": (P.spherical_1d("sedov", 192, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3), 100),
+        # the log-spaced radius on [1e-3, 1] with a reflecting inner sphere (RCOORD=LOG)
+        "sph1d_log_sedov_160": (P.spherical_1d("sedov", 160, 1.4, p_ratio=1.0e4, r0=0.02, coords="log",
+                                               r_in=1.0e-3), 100),
     }
 
 
@@ -66,6 +69,13 @@ def cases3d():
                                                                 coords="default"), 40),
         "sph1d_default_sedov_192": (P.spherical_1d("sedov", 192, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3,
                                                    coords="default"), 60),
+        # the log-spaced radius (RCOORD=LOG) on the 2-D grid, which the reference accepts (on
+        # the 3-D grid its init_dendritic rejects it), and the 3-D workload's map: SINH with the
+        # transition radius small, zones log-spaced outside it
+        "sedov2dsph_log_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.15, noise=0.02, coords="log",
+                                                            r_in=1.0e-2), 40),
+        "sedov3d_sinhrt_noisy_24x16x32": (P.sedov_3d(24, 16, 32, r_dep=0.1, noise=0.02, coords="sinh_rt",
+                                                     r_in=1.0e-2), 30),
     }
 
 
@@ -83,9 +93,12 @@ def cases_gravity():
     }
 
 
-def main():
+def main(only=()):
+    """Regenerate every fixture, or only those named in `only`."""
     build_ref.build()
     for name, (pb, n) in list(cases3d().items()) + list(cases_gravity().items()):
+        if only and name not in only:
+            continue
         snaps = pyoracle.run_reference(pb, n, every=n)
         last = snaps[-1]
         one = pyoracle.run_reference(pb.copy(ic=last[4]), 1, every=1)[-1]
@@ -94,6 +107,8 @@ def main():
                             prim1=one[4], t1=one[1], dt1=one[2])
         print(name, "steps", last[0], "t", last[1], "->", os.path.relpath(out, ROOT))
     for name, (pb, n) in cases().items():
+        if only and name not in only:
+            continue
         snaps = pyoracle.run_reference(pb, n, every=n)
         first, last = snaps[0], snaps[-1]
         out = os.path.join(HERE, name + ".npz")
@@ -103,4 +118,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

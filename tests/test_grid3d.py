@@ -2,6 +2,8 @@
 utils.c:181-354) and per-row zone geometry (init_geometry, metric_spherical_general.c)
 of the library against the Python restatement and against the reference build itself;
 the 3-D fixtures against the problem generator and the live reference."""
+import subprocess
+
 import numpy as np
 import pytest
 
@@ -40,6 +42,39 @@ def test_sinh_zone_counts_match_restatement_and_reference(dims, dr_min):
     assert abs(edges[-1] - 1.0) <= 1.0e-9 and abs(edges[1] - dr_min) <= 1.0e-2 * dr_min
 
 
+@pytest.mark.parametrize("dims,r_in", [((24, 16, 32), 1.0e-2), ((48, 32, 64), 1.0e-3), ((384, 128, 256), 1.0e-3)])
+def test_log_radius_3d_grid_refused_as_by_the_reference(dims, r_in):
+    """The log-spaced radius (RCOORD=LOG, zone edges r_in (1/r_in)^(i/n1)) on the 3-D
+    dendritic grid: theta zones double at every radial row from nj = 2 and the phi zones
+    then refine 4-to-1 between neighbouring rows, which the reference's init_dendritic
+    rejects (it prints the cells and exits, utils.c:548-586).  The library refuses the
+    same grids with MDG_ERR_INVALID; the restatement finds 4-to-1 cells too."""
+    pb = P.sedov_3d(*dims, r_dep=0.2, coords="log", r_in=r_in)
+    with pytest.raises(MdgError) as e:
+        S.grid3d_counts(pb)
+    assert e.value.code == 1 and "4-to-1" in str(e.value)
+    nj, nk = P.dendritic_grid(*dims, pb.startx, pb.dx, maps=P.CoordMaps.of(pb))
+    assert P.dendritic_refine_errors(dims[1], dims[2], nj, nk) > 0
+    if dims[0] <= 64 and pyoracle.ref_available(pb):
+        with pytest.raises(subprocess.CalledProcessError):
+            pyoracle.reference_grid(pb)
+
+
+@pytest.mark.parametrize("dims,r_in", [((24, 16), 1.0e-2), ((48, 32), 1.0e-3), ((384, 128), 1.0e-3)])
+def test_log_radius_2d_zone_counts_match_restatement_and_reference(dims, r_in):
+    """On the 2-D (r, theta) grid the log-spaced radius is accepted (no phi refinement)."""
+    pb = P.sedov_2d_spherical(*dims, r_dep=0.2, coords="log", r_in=r_in)
+    nj, nk, n = S.grid3d_counts(pb)
+    pj, _ = P.dendritic_grid(dims[0], dims[1], 1, pb.startx, pb.dx, ndim=2, maps=P.CoordMaps.of(pb))
+    assert list(nj) == pj and n == pb.ncell == sum(pj)
+    if dims[0] <= 64 and pyoracle.ref_available(pb):
+        rnj, _ = pyoracle.reference_grid(pb)
+        assert list(nj) == rnj[2:-2]
+    edges = P.radial_edges(pb)
+    want = r_in * (1.0 / r_in) ** (np.arange(dims[0] + 1) / dims[0])
+    assert np.allclose(edges, want, rtol=1.0e-12, atol=0.0)
+
+
 def test_c3_grid_size():
     """The measured 3-D workload: 384 x 128 x 256 before coarsening."""
     pb = P.sedov_3d(384, 128, 256)
@@ -51,10 +86,12 @@ def test_c3_grid_size():
 @pytest.mark.parametrize("dims,dr_min,coords", [((24, 16, 32), None, "sinh"), ((40, 32, 64), None, "sinh"),
                                                 ((48, 64, 128), None, "sinh"), ((24, 16, 32), 0.02, "sinh"),
                                                 ((48, 32, 64), 0.01, "sinh"), ((24, 16, 32), 0.02, "default"),
-                                                ((48, 32, 64), 0.01, "default")])
+                                                ((48, 32, 64), 0.01, "default"), ((384, 128, 256), 1.98e-5, "sinh")])
 def test_geometry_bit_identical_to_reference(dims, dr_min, coords):
-    """Uniform radius, the SINH radial map (against the reference's RCOORD=SINH build) and
-    the default build maps SINH_MODIFIED + POLYTH."""
+    """Uniform radius, the SINH radial map (against the reference's RCOORD=SINH build; the
+    last case is the measured 3-D workload's grid, rtrans about 1e-3: zones log-spaced
+    from r = 1e-3 to 1, 2e-5 wide inside) and the default build maps SINH_MODIFIED +
+    POLYTH."""
     pb = P.sedov_3d(*dims, r_dep=0.2, dr_min=dr_min, coords=coords)
     if not pyoracle.ref_available(pb):
         pytest.skip("oracle/_ref not built (needs the reference tree)")
@@ -90,9 +127,14 @@ def test_2d_zone_counts_match_restatement(dims):
 # the NDIM=2 record of ref_get_geom: vol, area[2], gcov[3][3], gcon[3], scale[3][3], conn[27]
 @pytest.mark.parametrize("dims,dr_min,coords", [((24, 16), None, "sinh"), ((48, 32), None, "sinh"),
                                                 ((40, 64), None, "sinh"), ((40, 32), 0.01, "sinh"),
-                                                ((40, 32), 0.01, "default")])
+                                                ((40, 32), 0.01, "default"), ((40, 32), 1.0e-2, "log"),
+                                                ((64, 32), 1.0e-3, "log")])
 def test_2d_geometry_bit_identical_to_reference(dims, dr_min, coords):
-    pb = P.sedov_2d_spherical(*dims, r_dep=0.2, dr_min=dr_min, coords=coords)
+    """As the 3-D test; for coords "log" (the RCOORD=LOG build) dr_min is the inner radius."""
+    if coords == "log":
+        pb = P.sedov_2d_spherical(*dims, r_dep=0.2, coords="log", r_in=dr_min)
+    else:
+        pb = P.sedov_2d_spherical(*dims, r_dep=0.2, dr_min=dr_min, coords=coords)
     if not pyoracle.ref_available(pb):
         pytest.skip("oracle/_ref not built (needs the reference tree)")
     rnj, _ = pyoracle.reference_grid(pb)

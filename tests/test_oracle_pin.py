@@ -22,6 +22,9 @@ def _cases():
     out.append(P.rayleigh_taylor_2d(24, 40, g=-0.3, noise=0.05))
     out.append(P.sod(160).copy(grav=(-0.9, 0.0, 0.0), name="sod_grav"))
     out.append(P.spherical_1d("sod", 120, 1.4).copy(grav=(-0.4, 0.0, 0.0), name="sph_sod_grav"))
+    # the log-spaced radius on [r_in, 1] with a reflecting inner sphere (RCOORD=LOG)
+    out.append(P.spherical_1d("sedov", 160, 1.4, p_ratio=1.0e4, r0=0.02, coords="log", r_in=1.0e-3))
+    out.append(P.spherical_1d("sod", 96, 5.0 / 3.0, rho_ratio=5.0, p_ratio=50.0, r0=0.1, coords="log", r_in=1.0e-2))
     return out
 
 
