@@ -57,6 +57,11 @@ sys.path.insert(0, ROOT)
 NX = 2048
 ENSEMBLE_COUNT = 2048
 ENSEMBLE_SEED = 7
+# geometry-table bytes the plain FP64 1-D stage kernel reads per zone: 19 of the 22
+# reconstruction coefficients (the linear-reconstruction ones are not read) and 22 face and
+# zone geometry fields (area, scale, 3 face gcov, 3 zone gcov, 3 gcon, volume, scale[0][0],
+# 9 connection coefficients)
+FP64_1D_TABLE_BYTES = 8 * (19 + 22)
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -289,46 +294,53 @@ def cpu_baseline_kh(pb_full, steps=2):
             "sample": "1 RK2 step of the %dx%d grid, CPU oracle, 1 core, %.1f s" % (NX, NX, el)}
 
 
-def cpu_baseline_ensemble(problems, every=8, steps=50, warm=2, zu_cap=2.0e6):
-    """The reference CPU build on every `every`-th problem of the ensemble, `steps` timed
-    RK2 steps each (fewer for large 2-D grids: at most zu_cap zone-updates, at least 2
-    steps), as independent single-threaded processes over all host cores (the reference
-    has no host threading on this path; problem-parallel is its best use of the host).
-    Rate = timed zone-updates / (summed timed seconds / processes), i.e. perfect packing
-    of the processes (the reference's best case)."""
+def cpu_baseline_ensemble(problems, steps=20, warm=2, min_wall=10.0, zu_round=1.5e8):
+    """The reference CPU build on the ensemble's problems as independent single-threaded
+    processes over all host cores (the reference has no host threading on this path;
+    problem-parallel is its best use of the host): every problem (or every n-th, so that
+    one round is about zu_round zone-updates) runs `steps` timed RK2 steps (the GPU arm's
+    step count, at most 200) after `warm` untimed ones; rounds repeat until at least
+    min_wall seconds of wall time have passed.  Rate = timed zone-updates / (summed timed
+    seconds / processes), i.e. perfect packing of the processes (the reference's best
+    case).  Both the GPU arm's cpu_baseline and the --impl reference line use this."""
     from concurrent.futures import ThreadPoolExecutor
 
     from oracle import pyoracle
+    steps = max(2, min(int(steps), 200))
+    total = sum(p.ncell for p in problems) * steps
+    every = max(1, int(math.ceil(total / zu_round)))
     sample = problems[::every]
     procs = os.cpu_count() or 1
     if pyoracle.ref_available(sample[0], fast=True):
         kind = "reference"
 
         def job(pb):
-            r = pyoracle.time_reference(pb, warm, max(2, min(steps, int(zu_cap / pb.ncell))), fast=True)
+            r = pyoracle.time_reference(pb, warm, steps, fast=True)
             return r["cells"] * r["steps"], r["seconds"]
     else:
         kind = "port"
 
         def job(pb):
-            n = max(2, min(steps, int(zu_cap / pb.ncell)))
             o = pyoracle.Oracle(pb)
             o.advance(warm)
             t0 = time.perf_counter()
-            o.advance(n)
-            return pb.ncell * n, time.perf_counter() - t0
+            o.advance(steps)
+            return pb.ncell * steps, time.perf_counter() - t0
     t0 = time.perf_counter()
+    zu = busy = 0.0
+    rounds = 0
     with ThreadPoolExecutor(max_workers=procs) as ex:
-        res = list(ex.map(job, sample))
+        while rounds == 0 or time.perf_counter() - t0 < min_wall:
+            res = list(ex.map(job, sample))
+            zu += sum(r[0] for r in res)
+            busy += sum(r[1] for r in res)
+            rounds += 1
     wall = time.perf_counter() - t0
-    zu = sum(r[0] for r in res)
-    busy = sum(r[1] for r in res)
     return {"value": zu / (busy / procs), "unit": "zone-updates/s", "cores": procs, "kind": kind,
-            "sample": "%d of the %d problems (every %dth), %d timed RK2 steps each (at most %.0e zone-updates) "
-                      "after %d warm-up, "
-                      "%d concurrent single-threaded processes, %s build%s; %.1f s wall"
-                      % (len(sample), len(problems), every, steps, zu_cap, warm, procs, kind,
-                         " with its own flags (-O3 -ffast-math)" if kind == "reference" else "", wall)}
+            "sample": "%d of the %d problems (every %dth), %d timed RK2 steps each after %d warm-up, %d round(s), "
+                      "%d concurrent single-threaded processes, %s build%s; %.1f s wall, %.3g zone-updates"
+                      % (len(sample), len(problems), every, steps, warm, rounds, procs, kind,
+                         " with its own flags (-O3 -ffast-math)" if kind == "reference" else "", wall, zu)}
 
 
 def run_reference_arm(args, ctx):
@@ -368,12 +380,12 @@ def run_reference_arm(args, ctx):
         from medusa_b200 import loadgen
         probs = loadgen.request_stream(args.server_requests, seed=11, frac_2d=args.server_frac_2d,
                                        frac_3d=args.server_frac_3d)
-        cb = cpu_baseline_ensemble(probs)
+        cb = cpu_baseline_ensemble(probs, steps=args.steps)
         config = {"workload": server_workload_name(args), "requests": len(probs)}
         dtype = "f64"
     else:
         probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED)
-        cb = cpu_baseline_ensemble(probs)
+        cb = cpu_baseline_ensemble(probs, steps=args.steps)
         config = ensemble_config(probs, 1)
         dtype = "f64"
     line = {"metric": "zone-updates/s", "value": cb["value"], "unit": "zone-updates/s", "n_gpus": ctx.world,
@@ -546,8 +558,26 @@ def run_ensemble(args, ctx):
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
         "clocks": clocks,
     }
+    # the batched plain FP64 sweep against the same roofline: its second-stage kernel, the
+    # 120 B/zone of the state accounting, and beside it the bytes it really needs per zone
+    # with the geometry tables the reference's Romberg geometry requires (19 reconstruction
+    # coefficients and 22 face/zone geometry fields of 8 B, read once per zone)
+    fp64_ms = st_f64["stage1"]
+    fp64_ach = b_stage1 * ncell / (fp64_ms / 1e3) / 1e9
+    line["roofline_fp64"] = {
+        "bound": "hbm", "achieved": fp64_ach, "peak": peak, "unit": "GB/s", "frac": fp64_ach / peak,
+        "kernel": "stage1d_kernel<1> (plain FP64 second RK stage)", "kernel_ms": fp64_ms,
+        "stage0_ms": st_f64["stage0"], "algorithmic_bytes_per_zone": b_stage1,
+        "table_bytes_per_zone": FP64_1D_TABLE_BYTES,
+        "achieved_with_tables": (b_stage1 + FP64_1D_TABLE_BYTES) * ncell / (fp64_ms / 1e3) / 1e9,
+        "traffic": read_profile_value("stage1d_fp64_ensemble_ncu.md", "TRAFFIC_PER_LAUNCH_STAGE1_BYTES"),
+        "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"}
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_ensemble(probs)
+        cb = cpu_baseline_ensemble(probs, steps=K)
+        line["cpu_baseline"] = cb
+        fp64_rate = ncell_all * K / (ms_f64 / 1e3)
+        line["comparison"]["fp64_batched_over_cpu_reference"] = fp64_rate / cb["value"]
+        line["comparison"]["mixed_over_cpu_reference"] = value / cb["value"]
     print(json.dumps(line), flush=True)
 
 
@@ -808,6 +838,10 @@ def sedov3d_full_run(ctx, pb, t_end, chunk=2000):
             while True:
                 s.step(chunk)
                 t, _, istep = s.time(0)
+                sys.stderr.write("sedov3d %s: step %d, t %.6e of %.3e, %.1f s\n"
+                                 % ("fp64" if precision == PREC_FP64 else "mixed", istep, t, t_end,
+                                    time.time() - w0))
+                sys.stderr.flush()
                 if t >= t_end * (1.0 - 1.0e-12):
                     break
             ev1.record(stream)

@@ -99,9 +99,40 @@ __device__ __forceinline__ void lin_recon_zone(T am_v, T a, T ap_v, const G &g, 
   ar = A * g(RC_XR) + B;
 }
 
+// How the FP64 reconstruction is emitted, chosen per translation unit before this header
+// is included (the results are the same either way):
+//   MDG_RECON_OUTLINE 1 -- recon_zone calls one out-of-line copy of para_recon/lin_recon
+//                          (kernels whose many inlined copies overflow the instruction
+//                          cache: the 1-D stage and the 3-D face kernels);
+//   MDG_RECON_UNROLL n  -- unroll factor of the loops over the reconstructed variables
+//                          (1: one inlined copy per loop, the 2-D split sweep).
+#ifndef MDG_RECON_OUTLINE
+#define MDG_RECON_OUTLINE 0
+#endif
+#ifndef MDG_RECON_UNROLL
+#define MDG_RECON_UNROLL 8
+#endif
+constexpr int kReconUnroll = MDG_RECON_UNROLL;
+struct FacePair { double al, ar; };
+template <typename G>
+__device__ __noinline__ FacePair recon_zone_call(int order, double am_v, double a, double ap_v, G g)
+{
+  FacePair o;
+  if (order == 3) para_recon_zone(am_v, a, ap_v, g, o.al, o.ar);
+  else if (order == 2) lin_recon_zone(am_v, a, ap_v, g, o.al, o.ar);
+  else { o.al = a; o.ar = a; }
+  return o;
+}
+
 template <typename T, typename G>
 __device__ __forceinline__ void recon_zone(int order, T am_v, T a, T ap_v, const G &g, T &al, T &ar)
 {
+  if (MDG_RECON_OUTLINE && sizeof(T) == 8) {
+    const FacePair o = recon_zone_call<G>(order, am_v, a, ap_v, g);
+    al = o.al;
+    ar = o.ar;
+    return;
+  }
   if (order == 3) para_recon_zone(am_v, a, ap_v, g, al, ar);
   else if (order == 2) lin_recon_zone(am_v, a, ap_v, g, al, ar);
   else { al = a; ar = a; }
