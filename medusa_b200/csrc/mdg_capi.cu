@@ -8,6 +8,7 @@
 #include <vector>
 #include "mdg_internal.h"
 #include "mdg_kernels.cuh"
+#include "mdg_tma.cuh"
 #include "mdg_grid3d.cuh"
 
 namespace mdg {
@@ -43,6 +44,7 @@ struct mdg_solver {
   unsigned char *d_shock1 = nullptr;
   double *d_rc0 = nullptr, *d_rc1 = nullptr, *d_geo = nullptr;
   Tables tb{};
+  TmaTables1d tm1{};              // 1-D FP64: tensor maps of rc0/geo (tile staging by TMA)
   double *d_state = nullptr;      // 10 arrays: P (5) then PH (5)
   StateSoA P{}, PH{};
   int64_t ncell_total = 0;
@@ -514,6 +516,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
       for (int i0 = 0; i0 < P.n1; i0 += TILE1) tiles.push_back(Tile{m, i0, 0, 0});
     }
   }
+  rc0 += rc0 & 1;                     // an even table stride: 16-byte rows for the TMA maps
   s->ncell_total = cell;
   s->ntx = (int)tiles.size();
   s->nty = (int)ytiles.size();
@@ -609,6 +612,14 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   s->tb.mx = s->d_mx;
   s->tb.mx1 = s->d_mx1;
   s->tb.gmono = s->d_gmono;
+  if (ndim == 1 && precision == MDG_PREC_FP64) {
+    // tile staging of the FP64 tables by TMA; without the driver's encoder the kernel
+    // reads the tables directly (same results)
+    std::string why;
+    const uint64_t row = sizeof(double) * (uint64_t)rc0;
+    s->tm1.valid = tma_encode_2d_f64(&s->tm1.rc, s->d_rc0, rc0, RC_NFIELDS, row, TMA_COLS1, RC_TMA_ROWS, &why) &&
+                   tma_encode_2d_f64(&s->tm1.geo, s->d_geo, rc0, GF_NFIELDS, row, TMA_COLS1, GF_TMA_ROWS, &why);
+  }
 #undef CKC
   if (precision == MDG_PREC_MIXED && ndim == 1) {
     int rc = build_mixed_tiles(s, s->cfg.threads);
@@ -696,7 +707,8 @@ static int queue_steps(mdg_solver *s, int nsteps)
       launch_stage3d(0, mix3, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
     else if (s->ndim == 1) {
       if (s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->P, s->stream);
-      launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream);
+      launch_stage1d(0, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->P, s->P, s->PH, s->stream,
+                     &s->tm1);
     }
     else
       launch_stage2d(0, mix2, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,
@@ -710,7 +722,8 @@ static int queue_steps(mdg_solver *s, int nsteps)
       launch_stage3d(1, mix3, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
     else if (s->ndim == 1) {
       if (s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->PH, s->stream);
-      launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream);
+      launch_stage1d(1, s->d_probs, s->d_times, s->d_tiles, s->ntiles, s->tb, s->PH, s->P, s->P, s->stream,
+                     &s->tm1);
     }
     else
       launch_stage2d(1, mix2, s->d_probs, s->d_times, s->d_tiles, s->ntx, s->d_tiles + s->ntx, s->nty, s->tb,

@@ -53,9 +53,12 @@ constexpr int NTY2 = 128;         // threads per direction-1 tile (126 output co
 constexpr int TJY2 = NTY2 - 2;
 constexpr int TIY2 = MDG_TIY2;    // rows per direction-1 tile
 
+struct TmaTables1d;
+// One RK stage of the plain FP64 1-D sweep; tm (may be NULL): tensor maps of tb's rc0 and
+// geo tables, with which each tile's tables are staged into shared memory by TMA.
 void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
                     const Tables &tb, StateSoA stage_state, StateSoA state_n, StateSoA out,
-                    cudaStream_t st);
+                    cudaStream_t st, const TmaTables1d *tm = nullptr);
 void launch_stage2d(int stage, bool mixed, const ProbDev *probs, ProbTime *times, const Tile *xtiles, int nxt,
                     const Tile *ytiles, int nyt, const Tables &tb, StateSoA stage_state, StateSoA state_n,
                     StateSoA acc, StateSoA out, unsigned char *shock0, unsigned char *shock1, cudaStream_t st);

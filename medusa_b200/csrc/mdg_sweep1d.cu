@@ -19,18 +19,32 @@
 #include "mdg_hydro.cuh"
 #include "mdg_kernels.cuh"
 #include "mdg_load1d.cuh"
+#include "mdg_tma.cuh"
 
 namespace mdg {
 
-template <int STAGE>
+// TMA: the tile's reconstruction coefficients (all RC_TMA_ROWS rows) and face/zone geometry
+// (GF_TMA_ROWS rows) arrive in shared memory by two tensor loads issued at the start,
+// which overlap the state loads; otherwise every field is read from the tables in HBM
+// when used.  The results are the same.
+template <int STAGE, bool TMA>
 __global__ void __launch_bounds__(NT1)
 stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
-               const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA sn, StateSoA out)
+               const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA sn, StateSoA out,
+               const __grid_constant__ TmaTables1d tm)
 {
   __shared__ double sv[6][NT1 + 2];     // stage-state pencil: 5 primitives + pressure
-  __shared__ double sar[6][NT1];        // right face values of each reconstructed zone
-  __shared__ double sfl[NPRIM][NT1];    // face fluxes
   __shared__ double sred[32];
+  __shared__ __align__(128) double s_rc[TMA ? RC_TMA_ROWS : 1][TMA ? TMA_COLS1 : 1];
+  __shared__ __align__(128) double s_geo[TMA ? GF_TMA_ROWS : 1][TMA ? TMA_COLS1 : 1];
+  __shared__ __align__(8) uint64_t s_bar;
+  // right face values of each reconstructed zone and the face fluxes; with TMA they
+  // reuse the reconstruction rows, which are dead once every zone is reconstructed
+  __shared__ double sar_own[TMA ? 1 : 6][NT1];
+  __shared__ double sfl_own[TMA ? 1 : NPRIM][NT1];
+  static_assert(!TMA || (6 + NPRIM) * NT1 <= RC_TMA_ROWS * TMA_COLS1, "exchange buffers fit the recon rows");
+  double (*sar)[NT1] = TMA ? reinterpret_cast<double(*)[NT1]>(&s_rc[0][0]) : sar_own;
+  double (*sfl)[NT1] = TMA ? reinterpret_cast<double(*)[NT1]>(&s_rc[0][0] + 6 * NT1) : sfl_own;
 
   const Tile tile = tiles[blockIdx.x];
   if (times[tile.prob].done) return;   // past tmax: the time loop has ended (CTA-uniform)
@@ -44,6 +58,23 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   const int64_t rcs = tb.rc0_stride;
   const double *geo = tb.geo;
   const int64_t gs = tb.geo_stride;
+  // first table column of the box: the column of zone i0-1 rounded down to even (TMA
+  // start coordinates are 16-byte aligned); a table column c sits at box column c - bx
+  const int64_t bx = (P.geo_off + NG + tile.i0 - 1) & ~int64_t(1);
+  if (TMA) {
+    if (t == 0) mbar_init(&s_bar, 1);
+    __syncthreads();
+    if (t == 0) {
+      mbar_arrive_expect_tx(&s_bar, (unsigned)((RC_TMA_ROWS + GF_TMA_ROWS) * TMA_COLS1 * sizeof(double)));
+      tma_load_2d(&s_rc[0][0], &tm.rc, (int)bx, 0, &s_bar);
+      tma_load_2d(&s_geo[0][0], &tm.geo, (int)bx, 0, &s_bar);
+    }
+  }
+  // geometry field f of table column c (faces and zones of this tile)
+  auto gf = [&](int f, int64_t c) -> double {
+    if (TMA) return s_geo[f][c - bx];
+    return __ldg(geo + f * gs + c);
+  };
 
   double w[6];
   load_cell_1d(P, sst, rc, rcs, z, t_bc, w);
@@ -61,6 +92,16 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 #pragma unroll
     for (int v = 0; v < 6; v++) sv[v][NT1 + 1] = w2[v];
   }
+  if (TMA) {
+    // the tables have landed (bounded wait: a copy that never completes flags the
+    // problem and the CTA leaves after waiting once more, as bounded)
+    const bool ok = mbar_wait(&s_bar, 0);
+    if (__syncthreads_or(!ok)) {
+      if (t == 0) times[tile.prob].err = MDG_ERR_INTERNAL;
+      mbar_wait(&s_bar, 0);
+      return;
+    }
+  }
   __syncthreads();
 
   // reconstruct zone z once (interp(), reconstruct.c:225-279); Gamma is the constant
@@ -68,11 +109,13 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   double al[7], ar[7];
   {
     int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
-    const RcView<double, true> g{rc + P.geo_off + zc + NG, rcs};
+    const int64_t c = P.geo_off + zc + NG;
+    const RcView<double, !TMA> g{TMA ? &s_rc[0][c - bx] : rc + c, TMA ? (int64_t)TMA_COLS1 : rcs};
 #pragma unroll kReconUnroll
     for (int v = 0; v < 6; v++) recon_zone<double>(P.interp_order, sv[v][t], sv[v][t + 1], sv[v][t + 2], g, al[v], ar[v]);
     al[6] = P.gam; ar[6] = P.gam;
   }
+  if (TMA) __syncthreads();   // every zone reconstructed: the recon rows may be overwritten
 #pragma unroll
   for (int v = 0; v < 6; v++) sar[v][t] = ar[v];
   __syncthreads();
@@ -90,11 +133,11 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     FaceGeom<double> fg;
     int zf = z < 0 ? 0 : (z > n1 ? n1 : z);
     const int64_t gi = P.geo_off + zf + NG;
-    fg.area = __ldg(geo + GF_AREA * gs + gi);
-    fg.scale = __ldg(geo + GF_FSCALE * gs + gi);
-    fg.g0 = __ldg(geo + GF_FG0 * gs + gi);
-    fg.g1 = __ldg(geo + GF_FG1 * gs + gi);
-    fg.g2 = __ldg(geo + GF_FG2 * gs + gi);
+    fg.area = gf(GF_AREA, gi);
+    fg.scale = gf(GF_FSCALE, gi);
+    fg.g0 = gf(GF_FG0, gi);
+    fg.g1 = gf(GF_FG1, gi);
+    fg.g2 = gf(GF_FG2, gi);
     riemann_hllc<0, false, double>(pl, al, fg, gc, flux, sig);
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) sfl[v][t] = flux[v];
@@ -116,8 +159,7 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
     }
-    const double gc0 = __ldg(geo + GF_G0 * gs + gi), gc1 = __ldg(geo + GF_G1 * gs + gi),
-                 gc2 = __ldg(geo + GF_G2 * gs + gi);
+    const double gc0 = gf(GF_G0, gi), gc1 = gf(GF_G1, gi), gc2 = gf(GF_G2, gi);
     // geometric source terms from the stage state (rad_fluid.c:164-192, fluid.c:56-73)
     if (P.has_src) {
       geo_sources_1d(geo, gs, gi, P.sparse_conn != 0, ph, sv[5][t + 1], gc0, gc1, gc2, src);
@@ -130,9 +172,9 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       // mass flux density at the outer and inner face (gravity.c:380-401)
       double vr = 0.0, area = 0.0;
       vr += sfl[RHO][t + 1];
-      area += __ldg(geo + GF_AREA * gs + gi + 1) + 1.0e-16;
+      area += gf(GF_AREA, gi + 1) + 1.0e-16;
       vr /= area;
-      const double vl = sfl[RHO][t] / (__ldg(geo + GF_AREA * gs + gi) + 1.0e-16);
+      const double vl = sfl[RHO][t] / (gf(GF_AREA, gi) + 1.0e-16);
       add_monopole_gravity(ph[RHO], tb.gmono[P.mono_off + z], vl, vr, P.x0 + z * P.dx0, P.dx0,
                            __ldg(rc + RC_B0 * rcs + gi), __ldg(rc + RC_G0 * rcs + gi), src);
     }
@@ -142,15 +184,14 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
     else nmin = tmin(nmin, src_dt_numerator_min(pn, u));   // zero sources: shared denominator
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) { divF[v] = 0.0; divF[v] += sfl[v][t + 1]; divF[v] -= sfl[v][t]; }
-    const double vol = __ldg(geo + GF_VOL * gs + gi);
+    const double vol = gf(GF_VOL, gi);
     const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) {
       double ddt = divF[v] / vol - src[v];
       u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
     }
-    u_to_p(u, pf, __ldg(geo + GF_GC0 * gs + gi), __ldg(geo + GF_GC1 * gs + gi), __ldg(geo + GF_GC2 * gs + gi),
-           P.floors != 0, P.rho_floor, P.e_floor);
+    u_to_p(u, pf, gf(GF_GC0, gi), gf(GF_GC1, gi), gf(GF_GC2, gi), P.floors != 0, P.rho_floor, P.e_floor);
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
     flag_nonfinite(pf, &times[tile.prob]);
@@ -159,7 +200,7 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
       // sound speed of the stage state (sim_eos was last filled from sim_ph)
       const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
       double local_dt = 0.0;
-      local_dt += (fabs(pf[U1]) + cs / __ldg(geo + GF_S00 * gs + gi)) / P.dx0;
+      local_dt += (fabs(pf[U1]) + cs / gf(GF_S00, gi)) / P.dx0;
       lmax = tmax(lmax, local_dt);
     }
   }
@@ -172,11 +213,17 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 }
 
 void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,
-                    const Tables &tb, StateSoA sst, StateSoA sn, StateSoA out, cudaStream_t st)
+                    const Tables &tb, StateSoA sst, StateSoA sn, StateSoA out, cudaStream_t st,
+                    const TmaTables1d *tm)
 {
   if (ntiles <= 0) return;
-  if (stage == 0) stage1d_kernel<0><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out);
-  else stage1d_kernel<1><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out);
+  static const TmaTables1d none{};
+  const bool tma = tm && tm->valid;
+  const TmaTables1d &m = tma ? *tm : none;
+  if (stage == 0 && tma) stage1d_kernel<0, true><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out, m);
+  else if (stage == 0) stage1d_kernel<0, false><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out, m);
+  else if (tma) stage1d_kernel<1, true><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out, m);
+  else stage1d_kernel<1, false><<<ntiles, NT1, 0, st>>>(probs, times, tiles, tb, sst, sn, out, m);
 }
 
 }  // namespace mdg
