@@ -135,6 +135,20 @@ int mdg_upload_state(mdg_solver *s, int prob, const double *prim);
 int mdg_upload_all(mdg_solver *s, const double *prim);
 int mdg_download_all(mdg_solver *s, double *prim);
 
+/* No counterpart in the reference (its executable holds one problem in host memory).
+ * Advance several solvers from host buffers with their transfers overlapping each other's
+ * steps: solver i uploads h_in[i] (every problem's state, as mdg_upload_all), takes nsteps
+ * steps (mdg_step) and downloads into h_out[i] (as mdg_download_all), each on its own
+ * stream; the uploads are issued in solver order, so solver i's upload runs while earlier
+ * solvers step and their downloads run while later ones step.  A caller with one large
+ * batch of independent problems splits it into a few solvers to hide the copies.  Host
+ * buffers must be page-locked for the copies to overlap.  Returns when every result is in
+ * host memory; *elapsed_ms (may be NULL) receives the device time from the start of the
+ * first upload to the end of the last download.  All solvers on one device, event timers
+ * off. */
+int mdg_run_host(mdg_solver *const *solvers, int n, const double *const *h_in, double *const *h_out, int nsteps,
+                 float *elapsed_ms);
+
 /* The next time step of every problem as estimate_dt() + main.c:239-251 would produce
  * it; written to dt_out[nprob] (may be NULL).  Idempotent until the next mdg_step. */
 int mdg_estimate_dt(mdg_solver *s, double *dt_out);

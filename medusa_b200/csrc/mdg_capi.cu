@@ -836,6 +836,82 @@ int mdg_step(mdg_solver *s, int nsteps)
   return queue_steps(s, nsteps % k);
 }
 
+int mdg_run_host(mdg_solver *const *solvers, int n, const double *const *h_in, double *const *h_out, int nsteps,
+                 float *elapsed_ms)
+{
+  if (!solvers || !h_in || !h_out || n < 1) return fail(MDG_ERR_INVALID, "solvers/buffers");
+  if (nsteps < 0) return fail(MDG_ERR_INVALID, "nsteps < 0");
+  for (int i = 0; i < n; i++) {
+    if (!solvers[i] || !h_in[i] || !h_out[i]) return fail(MDG_ERR_INVALID, "null solver or buffer");
+    if (solvers[i]->device != solvers[0]->device) return fail(MDG_ERR_INVALID, "solvers on different devices");
+    if (solvers[i]->timing) return fail(MDG_ERR_INVALID, "event timers are on (mdg_set_timing)");
+  }
+  CK(cudaSetDevice(solvers[0]->device));
+  // everything that allocates or captures happens before the first copy
+  for (int i = 0; i < n; i++) {
+    mdg_solver *s = solvers[i];
+    int rc = stage_all(s);
+    if (rc != MDG_OK) return rc;
+    if (s->cfg.steps_per_graph > 0 && nsteps >= s->cfg.steps_per_graph && (rc = ensure_graph(s)) != MDG_OK) return rc;
+  }
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> done(n, nullptr);
+  auto cleanup = [&]() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    for (auto &e : done)
+      if (e) cudaEventDestroy(e);
+  };
+#define CKR(call)                                                                      \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess) {                                                           \
+      cleanup();                                                                       \
+      return fail(MDG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    }                                                                                  \
+  } while (0)
+  CKR(cudaEventCreate(&ev0));
+  CKR(cudaEventCreate(&ev1));
+  for (int i = 0; i < n; i++) CKR(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming));
+  cudaStream_t st0 = solvers[0]->stream;
+  CKR(cudaEventRecord(ev0, st0));
+  // the uploads first, in solver order (the copy engine serves them in turn), then every
+  // solver's steps, each waiting only for its own upload on its own stream, then the
+  // downloads
+  for (int i = 0; i < n; i++) {
+    mdg_solver *s = solvers[i];
+    if (i > 0) CKR(cudaStreamWaitEvent(s->stream, ev0, 0));
+    CKR(cudaMemcpyAsync(s->d_stage_all, h_in[i], sizeof(double) * NPRIM * s->ncell_total, cudaMemcpyHostToDevice,
+                        s->stream));
+    launch_aos_to_soa(s->d_stage_all, s->P, 0, s->ncell_total, s->stream);
+    launch_reset_time_all(s->d_times, s->nprob, s->stream);
+    if (s->ndim == 3) launch_initial_estimate3(s->s3, s->d_probs, s->d_times, s->P, s->stream);
+    else launch_initial_estimate_all(s->d_probs, s->d_times, s->nprob, s->max_cells, s->tb, s->P, s->stream);
+  }
+  int rc = MDG_OK;
+  for (int i = 0; i < n && rc == MDG_OK; i++) rc = mdg_step(solvers[i], nsteps);
+  if (rc != MDG_OK) {
+    for (int i = 0; i < n; i++) cudaStreamSynchronize(solvers[i]->stream);
+    cleanup();
+    return rc;
+  }
+  for (int i = 0; i < n; i++) {
+    mdg_solver *s = solvers[i];
+    launch_soa_to_aos(s->P, 0, s->ncell_total, s->d_stage_all, s->stream);
+    CKR(cudaMemcpyAsync(h_out[i], s->d_stage_all, sizeof(double) * NPRIM * s->ncell_total, cudaMemcpyDeviceToHost,
+                        s->stream));
+    CKR(cudaEventRecord(done[i], s->stream));
+    if (i > 0) CKR(cudaStreamWaitEvent(st0, done[i], 0));
+  }
+  CKR(cudaEventRecord(ev1, st0));
+  CKR(cudaEventSynchronize(ev1));
+  CKR(cudaGetLastError());
+  if (elapsed_ms) CKR(cudaEventElapsedTime(elapsed_ms, ev0, ev1));
+#undef CKR
+  cleanup();
+  return MDG_OK;
+}
+
 int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg)
 {
   if (!s || !cfg) return fail(MDG_ERR_INVALID, "solver/cfg");

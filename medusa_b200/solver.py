@@ -126,6 +126,7 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_upload_state.argtypes = [vp, i, vp]
     L.mdg_estimate_dt.argtypes = [vp, vp]
     L.mdg_step.argtypes = [vp, i]
+    L.mdg_run_host.argtypes = [vp, i, vp, vp, i, ctypes.POINTER(ctypes.c_float)]
     L.mdg_estimate_dt_raw.argtypes = [vp, vp]
     L.mdg_step_dt.argtypes = [vp, vp]
     L.mdg_download_state.argtypes = [vp, i, vp, vp]
@@ -250,6 +251,21 @@ def grid3d_radial_mean(pb: "_pb.Problem", field: np.ndarray) -> np.ndarray:
         c += cnt
         q += int(nj[i])
     return out
+
+
+def run_host(solvers, h_in, h_out, nsteps: int) -> float:
+    """mdg_run_host: every solver uploads its host buffer h_in[i] (address of [zone][5]
+    doubles of all its problems, page-locked for overlap), takes nsteps steps and downloads
+    into h_out[i], the transfers of each overlapping the others' steps; returns the device
+    milliseconds from the first upload to the last download."""
+    n = len(solvers)
+    L = library()
+    arr = (ctypes.c_void_p * n)(*[s._h for s in solvers])
+    ins = (ctypes.c_void_p * n)(*h_in)
+    outs = (ctypes.c_void_p * n)(*h_out)
+    ms = ctypes.c_float(0.0)
+    _check(L.mdg_run_host(arr, n, ins, outs, nsteps, ctypes.byref(ms)), "mdg_run_host")
+    return float(ms.value)
 
 
 def _check(rc: int, where: str):

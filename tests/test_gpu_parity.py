@@ -296,3 +296,37 @@ def test_host_driven_time_loop_equals_device_loop():
         for m in range(2):
             assert a.time(m)[0] == b.time(m)[0]
             assert np.array_equal(a.update_cpu(m), b.update_cpu(m))
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_run_host_equals_one_solver(precision):
+    """mdg_run_host over three solvers (the batch split in three, copies overlapping the
+    steps) gives every problem the result of one solver holding the whole batch, bit for
+    bit (problems are independent; batching does not change a result)."""
+    from medusa_b200.solver import run_host
+    probs = P.ensemble_1d(30, seed=5, nmin=128, nmax=900)
+    n = 12
+    with Solver(probs, precision=precision) as s:
+        s.step(n)
+        ref = s.download_all()
+    parts = [probs[:7], probs[7:19], probs[19:]]
+    solvers = [Solver(p, precision=precision, upload=False) for p in parts]
+    h_in = [np.ascontiguousarray(np.concatenate([q.ic for q in p])) for p in parts]
+    h_out = [np.zeros_like(x) for x in h_in]
+    try:
+        ms = run_host(solvers, [x.ctypes.data for x in h_in], [x.ctypes.data for x in h_out], n)
+        for sv in solvers:
+            sv.synchronize()
+    finally:
+        for sv in solvers:
+            sv.close()
+    assert ms > 0.0
+    got = []
+    for p, out in zip(parts, h_out):
+        off = 0
+        for q in p:
+            got.append(out[off:off + q.ncell])
+            off += q.ncell
+    assert len(got) == len(ref)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
