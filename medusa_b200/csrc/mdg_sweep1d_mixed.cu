@@ -201,6 +201,22 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
     const double t_bc = STAGE ? times[tile.prob].t_bc1 : times[tile.prob].t;
     const int n1 = P.n1;
     const int z = tile.i0 - 1 + t;
+#ifndef MDG_MIX_EARLY
+#define MDG_MIX_EARLY 0
+#endif
+    // with MDG_MIX_EARLY the base state of the push and the FP32 weights are requested
+    // together with the stencil, so their latencies overlap
+    const bool pushes = (t >= 1 && t <= NT - 2 && z >= 0 && z < n1);
+    double pn_early[NPRIM];
+    MixW w_early;
+    if (MDG_MIX_EARLY) {
+      if (STAGE == 1 && pushes) {
+#pragma unroll
+        for (int v = 0; v < NPRIM; v++) pn_early[v] = sn.v[v][P.cell_off + z];
+      }
+      const int zc0 = z < -1 ? -1 : (z > n1 ? n1 : z);
+      w_early = load_mixw(tb.mx + P.geo_off + zc0 + NG, gs);
+    }
 
     {
       double w[6];
@@ -226,7 +242,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
     double al[6];
     {
       const int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
-      const MixW w = load_mixw(tb.mx + P.geo_off + zc + NG, gs);
+      const MixW w = MDG_MIX_EARLY ? w_early : load_mixw(tb.mx + P.geo_off + zc + NG, gs);
 #pragma unroll
       for (int v = 0; v < 6; v++) {
         const double a = sv[v][t + 1];
@@ -273,7 +289,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
         for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
       } else {
 #pragma unroll
-        for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
+        for (int v = 0; v < NPRIM; v++) pn[v] = MDG_MIX_EARLY ? pn_early[v] : sn.v[v][cell];
       }
       const ZoneGeo1 zg = zone_geom_1d(P, z);
       if (P.has_src) {
