@@ -467,10 +467,6 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].monopole)
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the 1-D mixed-precision sweep has no monopole gravity");
-    if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 &&
-        (descs[m].rcoord != MDG_RCOORD_UNIFORM || descs[m].thcoord != MDG_THCOORD_UNIFORM))
-      return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
-                                       ": the 1-D mixed-precision sweep computes the uniform-radius geometry in closed form");
   }
   const bool dendritic = is_dendritic(descs[0]);
   if (dendritic && nprob != 1) return fail(MDG_ERR_NOTIMPL, "a dendritic-grid solver advances one problem");
@@ -525,15 +521,34 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   const int nstate = (ndim == 2) ? 3 : 2;   // P, PH (+ ACC in 2-D)
 
   // host tables of the FP64 sweeps (Romberg moments, bit-identical to the reference's);
-  // the mixed sweep's tables are built on the device from closed-form moments below
-  // 1-D mixed: tables built on the device from closed-form moments; 2-D mixed: the FP64
-  // tables (for declined faces) plus host-built FP32 weights of both directions
+  // 1-D mixed: tables built on the device from closed-form moments on the uniform maps,
+  // host Romberg tables otherwise; 2-D mixed: the FP64 tables (for declined faces) plus
+  // host-built FP32 weights of both directions
   const bool dev_tables = precision == MDG_PREC_MIXED && ndim == 1;
   const size_t n_rc0 = (size_t)RC_NFIELDS * rc0, n_geo = (ndim == 2) ? 0 : (size_t)GF_NFIELDS * rc0;
   std::vector<double> h_rc0, h_rc1, h_geo;
   if (!dev_tables) h_rc0.assign(n_rc0, 0.0);
   if (ndim == 2) h_rc1.assign((size_t)RC_NFIELDS * rc1, 0.0);
   else if (!dev_tables) h_geo.assign(n_geo, 0.0);
+  // mixed 1-D problems on a non-uniform coordinate map read the Romberg tables (built here,
+  // columns of the problem only) instead of the closed-form uniform-radius geometry
+  struct HostCols { int m; std::vector<double> rc, geo; std::vector<float> mx; };
+  std::vector<HostCols> tab_probs;
+  for (int m = 0; m < nprob && dev_tables; m++) {
+    if (descs[m].rcoord == MDG_RCOORD_UNIFORM && descs[m].thcoord == MDG_THCOORD_UNIFORM) continue;
+    const int64_t ncol = descs[m].n1 + 2 * NG;
+    HostCols hc;
+    hc.m = m;
+    hc.rc.assign((size_t)RC_NFIELDS * ncol, 0.0);
+    hc.geo.assign((size_t)GF_NFIELDS * ncol, 0.0);
+    hc.mx.assign((size_t)MX_NFIELDS * ncol, 0.0f);
+    build_recon_table(descs[m], 0, hc.rc.data(), ncol, 0);
+    build_geo_1d(descs[m], hc.geo.data(), ncol, 0);
+    build_mixed_table(descs[m], 0, hc.mx.data(), ncol, 0);
+    s->hprobs[m].geo_tab = 1;
+    s->hprobs[m].sparse_conn = conn_is_sparse(hc.geo.data(), ncol, 0, (int)ncol);
+    tab_probs.push_back(std::move(hc));
+  }
   for (int m = 0; m < nprob && !dev_tables; m++) {
     build_recon_table(descs[m], 0, h_rc0.data(), rc0, s->hprobs[m].geo_off);
     if (ndim == 2) {
@@ -588,9 +603,19 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMemcpy(s->d_tiles, tiles.data(), sizeof(Tile) * s->ntiles, cudaMemcpyHostToDevice));
   if (dev_tables) {
     for (int m = 0; m < nprob; m++)
-      launch_build_tables_1d(s->d_probs, m, descs[m].n1, s->d_rc0, s->d_geo, s->d_mx, rc0, s->stream);
+      if (!s->hprobs[m].geo_tab)
+        launch_build_tables_1d(s->d_probs, m, descs[m].n1, s->d_rc0, s->d_geo, s->d_mx, rc0, s->stream);
     CKC(cudaGetLastError());
     CKC(cudaStreamSynchronize(s->stream));
+    for (const HostCols &hc : tab_probs) {
+      const int64_t ncol = descs[hc.m].n1 + 2 * NG, off = s->hprobs[hc.m].geo_off;
+      CKC(cudaMemcpy2D(s->d_rc0 + off, sizeof(double) * rc0, hc.rc.data(), sizeof(double) * ncol,
+                       sizeof(double) * ncol, RC_NFIELDS, cudaMemcpyHostToDevice));
+      CKC(cudaMemcpy2D(s->d_geo + off, sizeof(double) * rc0, hc.geo.data(), sizeof(double) * ncol,
+                       sizeof(double) * ncol, GF_NFIELDS, cudaMemcpyHostToDevice));
+      CKC(cudaMemcpy2D(s->d_mx + off, sizeof(float) * rc0, hc.mx.data(), sizeof(float) * ncol,
+                       sizeof(float) * ncol, MX_NFIELDS, cudaMemcpyHostToDevice));
+    }
   } else {
     CKC(cudaMemcpy(s->d_rc0, h_rc0.data(), sizeof(double) * n_rc0, cudaMemcpyHostToDevice));
     if (ndim != 2) CKC(cudaMemcpy(s->d_geo, h_geo.data(), sizeof(double) * n_geo, cudaMemcpyHostToDevice));

@@ -87,6 +87,8 @@ struct ProbDev {
   int floors;               // ENFORCE_FLOORS: u_to_p clamps rho and u to the floors below
   int grav_on;              // GRAV=FIXED_GRAV: the fixed acceleration grav[] is applied
   int mono;                 // GRAV=SPHERICAL_MONOPOLE_GRAV: self-gravity, monopole approximation
+  int geo_tab;              // mixed 1-D sweep: geometry from the Romberg tables (a non-uniform
+                            // coordinate map), not in closed form
   int64_t mono_off;         // first zone of this problem in the monopole acceleration array
   int64_t cell_off;         // first zone of this problem in the state arrays
   int64_t ncell;            // interior zones (n1*n2 on 1-D/2-D grids; the dendritic count in 3-D)

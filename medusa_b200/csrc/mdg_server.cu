@@ -338,6 +338,8 @@ int admit(mdg_server *s, Request *r)
   P.geo_off = seg;
   P.mono_off = seg;
   P.sparse_conn = r->sparse;
+  // a mixed 1-D request on a non-uniform coordinate map reads its Romberg tables
+  if (s->cfg.precision == MDG_PREC_MIXED && d.ndim == 1 && !r->geo.empty()) P.geo_tab = 1;
   if (d.ndim == 2) {
     P.cell_off = r->seg2;
     P.rc1_off = seg + d.n1 + 2 * NG;
@@ -365,7 +367,7 @@ int admit(mdg_server *s, Request *r)
     s->launches += 3;
     return MDG_OK;
   }
-  if (s->cfg.precision == MDG_PREC_MIXED) {
+  if (s->cfg.precision == MDG_PREC_MIXED && r->geo.empty()) {
     launch_build_tables_1d(s->d_probs, r->slot, d.n1, s->d_rc0, s->d_geo, s->d_mx, s->units, s->stream);
   } else {
     const size_t pitch = sizeof(double) * s->units;
@@ -373,6 +375,9 @@ int admit(mdg_server *s, Request *r)
                           cudaMemcpyHostToDevice, s->stream));
     SCK(cudaMemcpy2DAsync(s->d_geo + seg, pitch, r->geo.data(), sizeof(double) * w, sizeof(double) * w,
                           GF_NFIELDS, cudaMemcpyHostToDevice, s->stream));
+    if (!r->mx.empty())
+      SCK(cudaMemcpy2DAsync(s->d_mx + seg, sizeof(float) * s->units, r->mx.data(), sizeof(float) * w,
+                            sizeof(float) * w, MX_NFIELDS, cudaMemcpyHostToDevice, s->stream));
   }
   SCK(cudaMemcpyAsync(s->d_stage, r->ic.data(), sizeof(double) * NPRIM * d.n1, cudaMemcpyHostToDevice, s->stream));
   launch_aos_to_soa(s->d_stage, s->P, seg, d.n1, s->stream);
@@ -812,8 +817,6 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
       return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep is built for parabolic reconstruction");
     if (desc->geom == MDG_SPHERICAL && !(desc->startx[0] >= 0.0))
       return sfail(MDG_ERR_NOTIMPL, "request: the mixed-precision sweep needs a spherical grid starting at r >= 0");
-    if (desc->rcoord != MDG_RCOORD_UNIFORM || desc->thcoord != MDG_THCOORD_UNIFORM)
-      return sfail(MDG_ERR_NOTIMPL, "request: the 1-D mixed-precision sweep is built for the uniform coordinate maps");
   }
   Request *r = new Request();
   r->desc = *desc;
@@ -831,14 +834,20 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
       build_mixed_table(r->desc, 0, r->mx.data(), r->units, 0);
       build_mixed_table(r->desc, 1, r->mx.data(), r->units, desc->n1 + 2 * NG);
     }
-  } else if (s->cfg.precision == MDG_PREC_FP64) {
+  } else if (s->cfg.precision == MDG_PREC_FP64 || desc->rcoord != MDG_RCOORD_UNIFORM ||
+             desc->thcoord != MDG_THCOORD_UNIFORM) {
     // the reference's Romberg tables, built here in the submitting thread so that the
-    // request loop does not spend its time on them
+    // request loop does not spend its time on them (the mixed sweep reads them, with
+    // FP32 weights from the same moments, on a non-uniform coordinate map)
     r->rc.assign((size_t)RC_NFIELDS * r->units, 0.0);
     r->geo.assign((size_t)GF_NFIELDS * r->units, 0.0);
     build_recon_table(r->desc, 0, r->rc.data(), r->units, 0);
     build_geo_1d(r->desc, r->geo.data(), r->units, 0);
     r->sparse = conn_is_sparse(r->geo.data(), r->units, 0, (int)r->units);
+    if (s->cfg.precision == MDG_PREC_MIXED) {
+      r->mx.assign((size_t)MX_NFIELDS * r->units, 0.0f);
+      build_mixed_table(r->desc, 0, r->mx.data(), r->units, 0);
+    }
   }
   r->t_submit = Clock::now();
   {

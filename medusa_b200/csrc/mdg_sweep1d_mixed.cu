@@ -67,7 +67,10 @@ __device__ __noinline__ float face_fp64(const double *c, int cs, const double *r
 //              conn[1][0][1] = conn[1][1][0] = conn[2][0][2] = conn[2][2][0] = int r dr / int r^2 dr,
 //              conn[0][1][1] = -(int r^3 dr / int r^2 dr) th1, conn[2][1][2] = conn[2][2][1] = tc,
 //              conn[0][2][2] = -conn[2][2][0] gcov[2], conn[1][2][2] = -tc gcov[2]/gcov[1]   (820-930)
-// Cartesian: unit metric, area 1, volume dx, no connection.
+// Cartesian: unit metric, area 1, volume dx, no connection.  Problems on a non-uniform
+// coordinate map (SINH, SINH_MODIFIED or LOG radius, POLYTH theta; ProbDev::geo_tab) read
+// the reference's Romberg geometry tables instead, with the FP64 source routine of the
+// plain sweep.
 __device__ __forceinline__ FaceGeom<double> face_geom_1d(const ProbDev &P, int zf)
 {
   FaceGeom<double> g;
@@ -201,23 +204,6 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
     const double t_bc = STAGE ? times[tile.prob].t_bc1 : times[tile.prob].t;
     const int n1 = P.n1;
     const int z = tile.i0 - 1 + t;
-#ifndef MDG_MIX_EARLY
-#define MDG_MIX_EARLY 0
-#endif
-    // with MDG_MIX_EARLY the base state of the push and the FP32 weights are requested
-    // together with the stencil, so their latencies overlap
-    const bool pushes = (t >= 1 && t <= NT - 2 && z >= 0 && z < n1);
-    double pn_early[NPRIM];
-    MixW w_early;
-    if (MDG_MIX_EARLY) {
-      if (STAGE == 1 && pushes) {
-#pragma unroll
-        for (int v = 0; v < NPRIM; v++) pn_early[v] = sn.v[v][P.cell_off + z];
-      }
-      const int zc0 = z < -1 ? -1 : (z > n1 ? n1 : z);
-      w_early = load_mixw(tb.mx + P.geo_off + zc0 + NG, gs);
-    }
-
     {
       double w[6];
       load_cell_1d(P, sst, rc, rcs, z, t_bc, w);
@@ -242,7 +228,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
     double al[6];
     {
       const int zc = z < -1 ? -1 : (z > n1 ? n1 : z);
-      const MixW w = MDG_MIX_EARLY ? w_early : load_mixw(tb.mx + P.geo_off + zc + NG, gs);
+      const MixW w = load_mixw(tb.mx + P.geo_off + zc + NG, gs);
 #pragma unroll
       for (int v = 0; v < 6; v++) {
         const double a = sv[v][t + 1];
@@ -262,7 +248,18 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
 #pragma unroll
       for (int v = 0; v < 6; v++) pl[v] = sar[v][t - 1];
       const int zf = z < 0 ? 0 : (z > n1 ? n1 : z);
-      const FaceGeom<double> fg = face_geom_1d(P, zf);
+      FaceGeom<double> fg;
+      if (P.geo_tab) {
+        // a non-uniform coordinate map: the face geometry of the Romberg tables
+        const int64_t gi = P.geo_off + zf + NG;
+        fg.area = __ldg(tb.geo + GF_AREA * gs + gi);
+        fg.scale = __ldg(tb.geo + GF_FSCALE * gs + gi);
+        fg.g0 = __ldg(tb.geo + GF_FG0 * gs + gi);
+        fg.g1 = __ldg(tb.geo + GF_FG1 * gs + gi);
+        fg.g2 = __ldg(tb.geo + GF_FG2 * gs + gi);
+      } else {
+        fg = face_geom_1d(P, zf);
+      }
       const GamConst<float> gc = gam_const<float>((float)P.gam);
       int isshock_unused;
       if (riemann_hllc_mixed<0>(pl, al, fg, gc, flux, sig, isshock_unused)) {
@@ -289,20 +286,39 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
         for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
       } else {
 #pragma unroll
-        for (int v = 0; v < NPRIM; v++) pn[v] = MDG_MIX_EARLY ? pn_early[v] : sn.v[v][cell];
+        for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
       }
-      const ZoneGeo1 zg = zone_geom_1d(P, z);
-      if (P.has_src) {
-        geo_sources_closed(P, zg, ph, sv[5][t + 1], src);
-      } else {
+      // zone geometry: closed form on the uniform maps (gcov[0][0] = gcon[0] = scale[0][0]
+      // = 1 there), the Romberg tables otherwise
+      double vol, g0 = 1.0, g1, g2, gc0 = 1.0, gc1, gc2, s00 = 1.0;
+      if (P.geo_tab) {
+        const int64_t gi = P.geo_off + z + NG;
+        const double *geo = tb.geo;
+        vol = __ldg(geo + GF_VOL * gs + gi);
+        g0 = __ldg(geo + GF_G0 * gs + gi); g1 = __ldg(geo + GF_G1 * gs + gi); g2 = __ldg(geo + GF_G2 * gs + gi);
+        gc0 = __ldg(geo + GF_GC0 * gs + gi); gc1 = __ldg(geo + GF_GC1 * gs + gi); gc2 = __ldg(geo + GF_GC2 * gs + gi);
+        s00 = __ldg(geo + GF_S00 * gs + gi);
+        if (P.has_src) {
+          geo_sources_1d(geo, gs, gi, P.sparse_conn != 0, ph, sv[5][t + 1], g0, g1, g2, src);
+        } else {
 #pragma unroll
-        for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+          for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+        }
+      } else {
+        const ZoneGeo1 zg = zone_geom_1d(P, z);
+        vol = zg.vol; g1 = zg.g1; g2 = zg.g2; gc1 = zg.gc1; gc2 = zg.gc2;
+        if (P.has_src) {
+          geo_sources_closed(P, zg, ph, sv[5][t + 1], src);
+        } else {
+#pragma unroll
+          for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+        }
       }
-      if (P.grav_on) add_fixed_gravity(ph, P.grav, 1.0, zg.g1, zg.g2, 1, src);
-      p_to_u(pn, u, 1.0, zg.g1, zg.g2);
-      p_to_u(ph, uh, 1.0, zg.g1, zg.g2);
+      if (P.grav_on) add_fixed_gravity(ph, P.grav, g0, g1, g2, 1, src);
+      p_to_u(pn, u, g0, g1, g2);
+      p_to_u(ph, uh, g0, g1, g2);
       lmin = dt_source_control_1div(pn, u, src);
-      const double ivol = 1.0 / zg.vol;
+      const double ivol = 1.0 / vol;
       const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) {
@@ -314,9 +330,9 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
       const double irho = 1.0 / u[RHO];
       const double w1 = u[U1] * irho, w2 = u[U2] * irho, w3 = u[U3] * irho;
       pf[RHO] = u[RHO];
-      pf[U1] = w1;
-      pf[U2] = zg.gc1 * w2;
-      pf[U3] = zg.gc2 * w3;
+      pf[U1] = gc0 * w1;
+      pf[U2] = gc1 * w2;
+      pf[U3] = gc2 * w3;
       pf[UU] = u[UU] - 0.5 * pf[RHO] * (w1 * pf[U1] + w2 * pf[U2] + w3 * pf[U3]);
       if (P.floors) {   // ENFORCE_FLOORS, fluid.c:43-46
         pf[RHO] = fmax(pf[RHO], P.rho_floor);
@@ -328,7 +344,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
       if (STAGE == 1) {
         // zone term of the next estimate_dt (step.c:177-187)
         const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
-        lmax = (fabs(pf[U1]) + cs) / P.dx0;   // scale[0][0] = 1 on both grids
+        lmax = (fabs(pf[U1]) + cs / s00) / P.dx0;
       }
     }
     lmin = fmin(lmin, P.dx0 / (double)smax);

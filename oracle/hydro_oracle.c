@@ -24,7 +24,9 @@
  *                                   SPHERICAL_ORIGIN, PROB) incl. the t+=dt / t-=dt shift
  *   gamma-law / polytrope EOS       eos/gamma/eos_gamma.c:5-12,45-58, eos/polytropic/eos_poly.c:5-11
  *   geometry                        metrics/metric_cartesian.c:47-295,
- *                                   metrics/metric_spherical_general.c:149-1051 (RCOORD=UNIFORM, 1-D),
+ *                                   metrics/metric_spherical_general.c:145-300, 558-1051 (RCOORD =
+ *                                   UNIFORM, SINH, SINH_MODIFIED and LOG, THCOORD = UNIFORM
+ *                                   and POLYTH; 1-D),
  *                                   utils.c:32-62 (romb)
  * Parity is pinned against the reference itself, built unmodified by
  * oracle/build_ref.py (tests/test_oracle_pin.py) and against the golden fixtures in
@@ -92,10 +94,10 @@ typedef struct {
   int enforce_floors;
   double rho_floor, e_floor;
   double grav[3];
-  int rcoord;          /* radial map: 0 UNIFORM, 1 SINH, 3 LOG (the RCOORD build switch) */
-  double rfact[3];     /* SINH_MODIFIED parameters: not restated here (the reference's own builds check it) */
-  int thcoord;         /* theta map: 0 UNIFORM only here */
-  double poly_xt, poly_alpha;
+  int rcoord;          /* radial map: 0 UNIFORM, 1 SINH, 2 SINH_MODIFIED, 3 LOG (the RCOORD build switch) */
+  double rfact[3];     /* SINH_MODIFIED: facta, factb, factc */
+  int thcoord;         /* theta map: 0 UNIFORM, 1 POLYTH (the THCOORD build switch) */
+  double poly_xt, poly_alpha;   /* POLYTH */
 } orc_params;
 
 typedef struct {
@@ -159,38 +161,73 @@ static double romb(double x0, double x1, double (*f)(double))
   return rvec[15];
 }
 
-/* metric_spherical_general.c maps (149-219) and integrands, RCOORD=UNIFORM or SINH,
- * THCOORD=UNIFORM, and the LOG map r = rtrans exp(|x|/rtrans) that the oracle's
- * RCOORD=LOG reference builds add in the form of the SINH branch; the map of the
- * problem being built (the integrands are plain functions handed to romb) */
-static int g_rcoord = 0;
-static double g_rtrans = 1.0;
+/* metric_spherical_general.c maps and integrands: r(x) for RCOORD = UNIFORM, SINH and
+ * SINH_MODIFIED (r_of_x 149-178 with sigmoid 145-147, dr_dx 180-198, d2r_dx2 200-219),
+ * the LOG map r = rtrans exp(|x|/rtrans) that the oracle's RCOORD=LOG reference builds add
+ * in the form of the SINH branch, and th(x) for THCOORD = UNIFORM and POLYTH (th_of_x
+ * 222-256, dth_dx 258-279, d2th_dx2 281-300, poly_norm as init_coords sets it, 568).
+ * The maps are those of the problem being built (the integrands are plain functions
+ * handed to romb). */
+enum { RC_UNIFORM = 0, RC_SINH = 1, RC_SINH_MODIFIED = 2, RC_LOG = 3 };
+enum { TH_UNIFORM = 0, TH_POLYTH = 1 };
+static int g_rcoord = RC_UNIFORM, g_thcoord = TH_UNIFORM;
+static double g_rtrans = 1.0, g_facta = 0.0, g_factb = 0.0, g_factc = 1.0;
+static double g_poly_norm = 0.0, g_poly_xt = 1.0, g_poly_alpha = 0.0;
+static double sigmoid(double x) { return 1.0/(1.0+exp(-x)); }
 static double r_of_x(double x)
 {
-  if (g_rcoord == 1) return g_rtrans*sinh(fabs(x)/g_rtrans);
-  if (g_rcoord == 3) return g_rtrans*exp(fabs(x)/g_rtrans);
+  if (g_rcoord == RC_SINH) return g_rtrans*sinh(fabs(x)/g_rtrans);
+  if (g_rcoord == RC_SINH_MODIFIED)
+    return g_rtrans*sinh(fabs(x)/g_rtrans) - g_facta*sigmoid((fabs(x)-g_factb)/g_factc)
+           + g_facta*sigmoid(-g_factb/g_factc);
+  if (g_rcoord == RC_LOG) return g_rtrans*exp(fabs(x)/g_rtrans);
   return fabs(x);
 }
 static double dr_dx(double x)
 {
-  if (g_rcoord == 1) return cosh(fabs(x)/g_rtrans);
-  if (g_rcoord == 3) return exp(fabs(x)/g_rtrans);
+  if (g_rcoord == RC_SINH) return cosh(fabs(x)/g_rtrans);
+  if (g_rcoord == RC_SINH_MODIFIED) {
+    double e = exp(-(fabs(x)-g_factb)/g_factc);
+    return cosh(fabs(x)/g_rtrans) - g_facta*e/g_factc/(1+e)/(1+e);
+  }
+  if (g_rcoord == RC_LOG) return exp(fabs(x)/g_rtrans);
   return 1.0;
 }
 static double d2r_dx2(double x)
 {
-  if (g_rcoord == 1) return sinh(fabs(x)/g_rtrans)/g_rtrans;
-  if (g_rcoord == 3) return exp(fabs(x)/g_rtrans)/g_rtrans;
+  if (g_rcoord == RC_SINH) return sinh(fabs(x)/g_rtrans)/g_rtrans;
+  if (g_rcoord == RC_SINH_MODIFIED) {
+    double e = exp(-(fabs(x)-g_factb)/g_factc);
+    return sinh(fabs(x)/g_rtrans)/g_rtrans
+           - g_facta/g_factc/g_factc*(2*e*e/(1+e)/(1+e)/(1+e) - e/(1+e)/(1+e));
+  }
+  if (g_rcoord == RC_LOG) return exp(fabs(x)/g_rtrans)/g_rtrans;
   return 0.0;
 }
+/* theta maps, reflected about the polar axis */
 static double th_of_x(double x)
 {
   if (x < -1.0) x = -2.0 - x;
   if (x >  1.0) x =  2.0 - x;
+  if (g_thcoord == TH_POLYTH)
+    return g_poly_norm*x*(1.0 + pow(x/g_poly_xt,g_poly_alpha)/(g_poly_alpha+1.0)) + 0.5*M_PI;
   return 0.5*M_PI*(x+1.0);
 }
-static double dth_dx(double x) { (void)x; return 0.5*M_PI; }
-static double d2th_dx2(double x) { (void)x; return 0.0; }
+static double dth_dx(double x)
+{
+  if (x < -1.0) x = -2.0 - x;
+  if (x >  1.0) x =  2.0 - x;
+  if (g_thcoord == TH_POLYTH) return g_poly_norm*(1.0 + pow(x/g_poly_xt,g_poly_alpha));
+  return 0.5*M_PI;
+}
+static double d2th_dx2(double x)
+{
+  if (x < -1.0) x = -2.0 - x;
+  if (x >  1.0) x =  2.0 - x;
+  if (g_thcoord == TH_POLYTH)
+    return g_poly_norm*g_poly_alpha*pow(x/g_poly_xt,g_poly_alpha-1.0)/g_poly_xt;
+  return 0.0;
+}
 static double f_r2dr_dx(double x) { return pow(r_of_x(x),2)*dr_dx(x); }
 static double f_xr1g(double x) { return x*pow(r_of_x(x),2)*dr_dx(x); }
 static double f_xr2g(double x) { return x*x*pow(r_of_x(x),2)*dr_dx(x); }
@@ -209,6 +246,14 @@ static void use_map(const orc_t *o)
 {
   g_rcoord = o->prm.rcoord;
   g_rtrans = o->prm.rtrans;
+  g_facta = o->prm.rfact[0];
+  g_factb = o->prm.rfact[1];
+  g_factc = o->prm.rfact[2];
+  g_thcoord = o->prm.thcoord;
+  g_poly_xt = o->prm.poly_xt;
+  g_poly_alpha = o->prm.poly_alpha;
+  if (g_thcoord == TH_POLYTH)
+    g_poly_norm = 0.5*M_PI*1.0/(1.0 + 1.0/(g_poly_alpha+1.0) * 1.0/pow(g_poly_xt,g_poly_alpha));
 }
 
 static void init_geometry(orc_t *o)
@@ -950,6 +995,10 @@ double orc_advance_one(orc_t *o)
 /* ------------------------------------------------------------------ lifecycle */
 orc_t *orc_create(const orc_params *prm, int ndim, int geom, const double *ic)
 {
+  /* maps the oracle does not restate are refused, not approximated */
+  if (prm->rcoord < RC_UNIFORM || prm->rcoord > RC_LOG || prm->thcoord < TH_UNIFORM || prm->thcoord > TH_POLYTH)
+    return NULL;
+  if (geom == 0 && (prm->rcoord != RC_UNIFORM || prm->thcoord != TH_UNIFORM)) return NULL;
   orc_t *o = calloc(1, sizeof *o);
   int v;
   o->prm = *prm;

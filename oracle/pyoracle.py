@@ -121,6 +121,9 @@ class Oracle:
         self._prm = params_of(pb)
         ic = np.ascontiguousarray(pb.ic, dtype=np.float64)
         self._h = lib().orc_create(ctypes.byref(self._prm), pb.ndim, pb.geom, ic.ctypes.data)
+        if not self._h:
+            raise ValueError("the oracle does not restate this problem's coordinate maps "
+                             "(rcoord %d, thcoord %d)" % (self._prm.rcoord, self._prm.thcoord))
 
     def __del__(self):
         if getattr(self, "_h", None):

@@ -63,7 +63,7 @@ def cases3d():
         "sedov3d_sinh_24x16x32": (P.sedov_3d(24, 16, 32, r_dep=0.2, dr_min=0.02), 30),
         "sedov2dsph_sinh_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.15, noise=0.05, dr_min=0.01), 40),
         # the reference's default build maps (SINH_MODIFIED radius, POLYTH theta); the 1-D
-        # case is here because the C restatement covers the uniform and SINH maps only
+        # case carries the one-step-afresh state (prim1) of this group as well
         "sedov3d_default_24x16x32": (P.sedov_3d(24, 16, 32, r_dep=0.2, dr_min=0.02, coords="default"), 30),
         "sedov2dsph_default_noisy_40x32": (P.sedov_2d_spherical(40, 32, r_dep=0.15, noise=0.05, dr_min=0.01,
                                                                 coords="default"), 40),

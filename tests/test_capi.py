@@ -157,13 +157,11 @@ def test_2d_spherical_scope_checked_before_device_work(mutate, nprob, code):
     (P.sod(64).copy(rcoord=P.RCOORD_SINH, rtrans=0.2), 0, 1),                        # Cartesian
     (P.spherical_1d("sedov", 64, 1.4, dr_min=0.01).copy(rtrans=-1.0), 0, 1),         # rtrans <= 0
     (P.spherical_1d("sedov", 64, 1.4).copy(rcoord=7), 0, 1),                          # unknown map
-    (P.spherical_1d("sedov", 64, 1.4, dr_min=0.01), 1, 5),                            # 1-D mixed: closed form
     (P.spherical_1d("noh", 64, 1.4).copy(rcoord=P.RCOORD_SINH, rtrans=0.2), 0, 5),    # Noh inflow boundary
     (P.spherical_1d("sedov", 64, 1.4).copy(thcoord=3), 0, 1),                         # unknown theta map
     (P.sod(64).copy(thcoord=P.THCOORD_POLYTH), 0, 1),                                 # Cartesian
     (P.spherical_1d("sedov", 64, 1.4).copy(thcoord=P.THCOORD_POLYTH, poly_xt=0.0), 0, 1),
     (P.spherical_1d("sedov", 64, 1.4, dr_min=0.01, coords="default").copy(rfact=(1.0e6, 1.5e6, 0.0)), 0, 1),
-    (P.spherical_1d("sedov", 64, 1.4, dr_min=0.01, coords="default"), 1, 5),          # 1-D mixed: closed form
 ])
 def test_radial_map_scope_checked_before_device_work(pb, precision, code):
     arr = (S.ProblemDesc * 1)(S.desc_of(pb))

@@ -37,6 +37,12 @@ def _cases():
         "sph_sedov_256": (P.spherical_1d("sedov", 256, 1.4, p_ratio=1.0e4, r0=0.05), 200),
         "sph_sod_384_g43": (P.spherical_1d("sod", 384, 4.0 / 3.0, rho_ratio=50.0, p_ratio=3.0e3), 250),
         "grav_sod1d_512": (P.sod(512, tmax=0.2).copy(grav=(-0.8, 0.0, 0.0), name="grav_sod1d_512"), 200),
+        # non-uniform radial maps: the geometry of the reference's Romberg tables
+        "sph_sinh_sedov_256": (P.spherical_1d("sedov", 256, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3), 200),
+        "sph_log_sedov_160": (P.spherical_1d("sedov", 160, 1.4, p_ratio=1.0e4, r0=0.02, coords="log",
+                                             r_in=1.0e-3), 200),
+        "sph_default_sod_256": (P.spherical_1d("sod", 256, 1.4, rho_ratio=10.0, p_ratio=100.0, dr_min=1.0e-3,
+                                               coords="default"), 200),
     }
 
 
@@ -44,8 +50,10 @@ CASES = _cases()
 
 
 def _weights(pb):
+    """Zone volumes (up to 4 pi / 3) of a spherical problem on its radial map."""
     if pb.geom == P.SPHERICAL:
-        return A.spherical_volumes(pb.n[0])
+        e = P.radial_edges(pb)
+        return e[1:] ** 3 - e[:-1] ** 3
     return None
 
 

@@ -66,6 +66,27 @@ def test_server_results_equal_solver(precision):
             assert lat > 0.0
 
 
+@pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
+def test_server_nonuniform_radial_maps_equal_solver(precision):
+    """Requests on the SINH, LOG and SINH_MODIFIED + POLYTH maps (geometry from the
+    Romberg tables built in the submitting thread) next to a uniform-radius one."""
+    reqs = [
+        _req("sedov", 256, 1.4, 0.01, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3),
+        _req("sedov", 160, 1.4, 0.004, p_ratio=1.0e4, r0=0.02, coords="log", r_in=1.0e-3),
+        _req("sod", 200, 1.4, 0.03, rho_ratio=10.0, p_ratio=100.0, dr_min=1.0e-3, coords="default"),
+        _req("sod", 300, 1.4, 0.05, rho_ratio=10.0, p_ratio=100.0),
+    ]
+    with Server(precision=precision, hbm_bytes=256 << 20, max_problems=8, max_zones=4096,
+                steps_per_round=13) as srv:
+        ids = [srv.submit(pb) for pb in reqs]
+        assert srv.run(0) == 0
+        for rid, pb in zip(ids, reqs):
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_result(pb, precision)
+            assert t >= pb.tmax and t == rt and ist == rist
+            assert np.array_equal(prim, ref)
+
+
 def test_server_result_same_alone_and_in_mix():
     """Continuous batching: a request's result does not depend on what else is resident,
     nor on when the others arrive."""

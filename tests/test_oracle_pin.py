@@ -25,6 +25,9 @@ def _cases():
     # the log-spaced radius on [r_in, 1] with a reflecting inner sphere (RCOORD=LOG)
     out.append(P.spherical_1d("sedov", 160, 1.4, p_ratio=1.0e4, r0=0.02, coords="log", r_in=1.0e-3))
     out.append(P.spherical_1d("sod", 96, 5.0 / 3.0, rho_ratio=5.0, p_ratio=50.0, r0=0.1, coords="log", r_in=1.0e-2))
+    # the reference's default build maps (SINH_MODIFIED radius, POLYTH theta)
+    out.append(P.spherical_1d("sod", 256, 1.4, rho_ratio=10.0, p_ratio=100.0, dr_min=1.0e-3, coords="default"))
+    out.append(P.spherical_1d("sedov", 200, 5.0 / 3.0, p_ratio=3.0e3, r0=0.08, dr_min=3.0e-3, coords="default"))
     return out
 
 
