@@ -161,10 +161,6 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
     if (!(d.gam > 1.0)) return bad("gam must exceed 1");
     if (!(d.cfl > 0.0)) return bad("cfl must be positive");
     if (d.enforce_floors != 0 && d.enforce_floors != 1) return bad("enforce_floors must be 0 or 1");
-    if (d.grav[0] != 0.0 || d.grav[1] != 0.0 || d.grav[2] != 0.0) {
-      why = "fixed gravity is not built for dendritic spherical grids";
-      return MDG_ERR_NOTIMPL;
-    }
     const bool ok = (d.bc_lo[0] == MDG_BC_REFLECT || d.bc_lo[0] == MDG_BC_SPHERICAL_ORIGIN) &&
                     (d.bc_hi[0] == MDG_BC_OUTFLOW || d.bc_hi[0] == MDG_BC_REFLECT);
     auto okj = [](int k) { return k == MDG_BC_REFLECT || k == MDG_BC_SPHERICAL_ORIGIN || k == MDG_BC_OUTFLOW; };

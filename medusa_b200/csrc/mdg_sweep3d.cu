@@ -726,7 +726,8 @@ __global__ void monopole_profile3_kernel(const ProbTime *__restrict__ times, Gri
 }
 
 // push() for zone (i, j, k) (step.c:327-478) with the dendritic flux fan-in, the
-// geometric sources of the stage state (rad_fluid.c:164-192, fluid.c:56-73) and, in the
+// geometric sources of the stage state (rad_fluid.c:164-192, fluid.c:56-73), fixed or
+// monopole gravity and, in the
 // second stage, the zone terms of the next estimate_dt (step.c:177-187).
 template <int STAGE>
 __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
@@ -780,6 +781,9 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
       s2 += T[2][1] * geo3(g, G3_C221, ij);
       src[RHO] = 0.0; src[UU] = 0.0; src[U1] = s0; src[U2] = s1; src[U3] = s2;
     }
+    // GRAV=FIXED_GRAV (gravity.c:38-64): the constant contravariant acceleration, lowered
+    // with the zone's metric, on the momenta of the grid's directions and the energy
+    if (P.grav_on) add_fixed_gravity(ph, P.grav, g0, g1, g2, g.ndim, src);
     if (g.mono) {
       // monopole gravity (gravity.c:373-401): mass flux density on the outer faces of the
       // zone (row i+1, the fan-in below) and on its inner face

@@ -105,6 +105,13 @@ CONFIGS = {
                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
     "sph3d_mono": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
                        RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="SPHERICAL_MONOPOLE_GRAV"),
+    # the fixed acceleration of GRAV=FIXED_GRAV on the dendritic grids
+    "sph2d_grav": dict(NDIM="2", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                       RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
+    "sph3d_grav": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                       RCOORD="UNIFORM", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
+    "sph3d_sinh_grav": dict(NDIM="3", GEOM="SPHERICAL", DENDRITIC_GRID="TRUE",
+                            RCOORD="SINH", THCOORD="UNIFORM", GRAV="FIXED_GRAV"),
     # a radius log-spaced outwards from rtrans (RCOORD=LOG, r = rtrans exp(|x|/rtrans)): not
     # one of the reference's maps, added to a generated copy of its spherical metric (see
     # log_metric_source below) for grids that start away from the origin

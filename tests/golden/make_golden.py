@@ -84,12 +84,21 @@ def cases_gravity():
     GRAV=SPHERICAL_MONOPOLE_GRAV builds; the C restatement does not cover it): the
     dust-collapse setup of problems/init_dustcollapse.c in 1-D (SINH radius, floors,
     the outer v^r hook; uniform radius without floors) and on the 2-D and 3-D dendritic
-    grids.  Fixtures as for cases3d (the state after n steps and one step from it)."""
+    grids; and fixed gravity (GRAV=FIXED_GRAV builds) on the dendritic grids.  Fixtures
+    as for cases3d (the state after n steps and one step from it)."""
     return {
         "dust1d_sinh_200": (P.dust_collapse(200), 60),
         "dust1d_uniform_nofloor_128": (P.dust_collapse(128, radius="uniform", floors=False), 60),
         "dust2d_uniform_24x16": (P.dust_collapse(24, 16, ndim=2, radius="uniform", floors=False), 40),
         "dust3d_uniform_16x8x16": (P.dust_collapse(16, 8, 16, ndim=3, radius="uniform", floors=False), 30),
+        # the constant acceleration of GRAV=FIXED_GRAV (a contravariant vector, gravity.c:38-64)
+        # on the dendritic grids: inward radial, and with theta and phi components as well
+        "sedov3d_grav_noisy_16x8x16": (P.sedov_3d(16, 8, 16, r_dep=0.25, noise=0.05).copy(
+            grav=(-0.5, 0.0, 0.0), name="sedov3d_grav_noisy_16x8x16"), 30),
+        "sedov3d_sinh_grav3_18x8x16": (P.sedov_3d(18, 8, 16, r_dep=0.2, noise=0.05, dr_min=0.02).copy(
+            grav=(-0.4, 0.3, 0.2), name="sedov3d_sinh_grav3_18x8x16"), 30),
+        "sedov2dsph_grav_noisy_24x16": (P.sedov_2d_spherical(24, 16, r_dep=0.2, noise=0.05).copy(
+            grav=(-0.6, 0.25, 0.1), name="sedov2dsph_grav_noisy_24x16"), 40),
     }
 
 

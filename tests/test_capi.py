@@ -139,7 +139,6 @@ def test_output_calls_reject_null_solver():
     (dict(n=(24, 16, 4)), 1, 1),                        # a 2-D grid has one phi zone
     (dict(dx=(1.0 / 24, 2.0 / 16, 1.0)), 1, 1),         # its phi zone spans 2 pi
     (dict(startx=(0.0, -0.5, 0.0)), 1, 1),              # theta over the whole sphere
-    (dict(grav=(0.0, -1.0, 0.0)), 1, 5),                # fixed gravity not on dendritic grids
     (dict(), 2, 5),                                     # one problem per dendritic solver
 ])
 def test_2d_spherical_scope_checked_before_device_work(mutate, nprob, code):

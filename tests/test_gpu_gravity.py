@@ -1,7 +1,8 @@
 """GPU parity of the monopole self-gravity (gravity.c:145-425, GR_MONOPOLE=FALSE) against
 fixtures made by the reference's GRAV=SPHERICAL_MONOPOLE_GRAV builds: the dust collapse
 of problems/init_dustcollapse.c in 1-D (SINH radius with floors and the outer v^r hook;
-uniform radius) and on the 2-D and 3-D dendritic grids.  Bars as for the other sweeps:
+uniform radius) and on the 2-D and 3-D dendritic grids; and of fixed gravity
+(gravity.c:38-64, GRAV=FIXED_GRAV builds) on the dendritic grids.  Bars as for the other sweeps:
 1e-9 after a whole fixture run, 1e-12 for one step, on two measures: pointwise
 (tests/_cases.py pointwise_rel_err) and per variable relative to its largest magnitude,
 the velocities sharing one scale."""
