@@ -460,9 +460,6 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     if (precision == MDG_PREC_MIXED && descs[m].geom == MDG_SPHERICAL && !(descs[m].startx[0] >= 0.0))
       return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
                                        ": the mixed-precision sweep needs a spherical grid starting at r >= 0");
-    if (precision == MDG_PREC_MIXED && descs[m].ndim == 1 && descs[m].monopole)
-      return fail(MDG_ERR_NOTIMPL, "problem " + std::to_string(m) +
-                                       ": the 1-D mixed-precision sweep has no monopole gravity");
   }
   const bool dendritic = is_dendritic(descs[0]);
   if (dendritic && nprob != 1) return fail(MDG_ERR_NOTIMPL, "a dendritic-grid solver advances one problem");
@@ -526,12 +523,14 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   if (!dev_tables) h_rc0.assign(n_rc0, 0.0);
   if (ndim == 2) h_rc1.assign((size_t)RC_NFIELDS * rc1, 0.0);
   else if (!dev_tables) h_geo.assign(n_geo, 0.0);
-  // mixed 1-D problems on a non-uniform coordinate map read the Romberg tables (built here,
-  // columns of the problem only) instead of the closed-form uniform-radius geometry
+  // mixed 1-D problems on a non-uniform coordinate map, or with monopole gravity (whose
+  // enclosed-mass solve reads the edge radii of the tables), read the Romberg tables
+  // (built here, columns of the problem only) instead of the closed-form geometry
   struct HostCols { int m; std::vector<double> rc, geo; std::vector<float> mx; };
   std::vector<HostCols> tab_probs;
   for (int m = 0; m < nprob && dev_tables; m++) {
-    if (descs[m].rcoord == MDG_RCOORD_UNIFORM && descs[m].thcoord == MDG_THCOORD_UNIFORM) continue;
+    if (descs[m].rcoord == MDG_RCOORD_UNIFORM && descs[m].thcoord == MDG_THCOORD_UNIFORM && !descs[m].monopole)
+      continue;
     const int64_t ncol = descs[m].n1 + 2 * NG;
     HostCols hc;
     hc.m = m;
@@ -721,6 +720,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
     launch_dt_finalize(s->d_probs, s->d_times, s->nprob, s->d_err, s->stream);
     mark(MDG_TIMER_DT, 1);
     mark(MDG_TIMER_STAGE0, 0);
+    if (mixed && s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->P, s->stream);
     if (mixed)
       launch_stage1d_mixed(0, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
                            s->tb, s->P, s->P, s->PH, s->stream);
@@ -736,6 +736,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
                      s->P, s->P, s->ACC, s->PH, s->d_shock0, s->d_shock1, s->stream);
     mark(MDG_TIMER_STAGE0, 1);
     mark(MDG_TIMER_STAGE1, 0);
+    if (mixed && s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->PH, s->stream);
     if (mixed)
       launch_stage1d_mixed(1, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
                            s->tb, s->PH, s->P, s->P, s->stream);

@@ -149,7 +149,7 @@ struct mdg_server {
   WorkQueue *d_queue = nullptr;
   int *d_err = nullptr;
   double *d_state = nullptr, *d_rc0 = nullptr, *d_geo = nullptr, *d_stage = nullptr;
-  double *d_gmono = nullptr;   // monopole gravity per zone unit (FP64 servers)
+  double *d_gmono = nullptr;   // monopole gravity per zone unit
   float *d_mx = nullptr;
   StateSoA P{}, PH{};
   Tables tb{};
@@ -161,6 +161,8 @@ struct mdg_server {
   int64_t units_in_use = 0;
   int ntiles = 0;
   bool tiles_dirty = true;
+  bool mono1d = false;                      // a resident 1-D request has monopole gravity
+  int graph_mono1d = -1;                    // mono1d when the graph was captured
   // 2-D lane: cell arena, shock bits, tile lists (x tiles then y tiles), second stream
   int64_t cells = 0;
   RangeAlloc alloc2;
@@ -235,9 +237,9 @@ StateSoA soa3(const Request *r, int which)
 // bytes of device memory per zone unit: state P and PH, RC and GF tables, FP32 weights
 int64_t bytes_per_unit(int precision)
 {
-  // state P and PH, the RC and GF tables, and the FP32 weights (mixed) or the monopole
-  // gravity per zone (FP64)
-  return 2 * NPRIM * 8 + RC_NFIELDS * 8 + GF_NFIELDS * 8 + (precision == MDG_PREC_MIXED ? MX_NFIELDS * 4 : 8);
+  // state P and PH, the RC and GF tables, the monopole gravity per zone and the FP32
+  // weights (mixed)
+  return 2 * NPRIM * 8 + RC_NFIELDS * 8 + GF_NFIELDS * 8 + 8 + (precision == MDG_PREC_MIXED ? MX_NFIELDS * 4 : 0);
 }
 
 // bytes per cell of the 2-D arena: state P, PH and accumulator, two shock bytes
@@ -276,8 +278,12 @@ int queue_round(mdg_server *s, int nsteps)
     if (lane2) SCK(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
     if (lane3) SCK(cudaStreamWaitEvent(s->stream3, s->ev_fork, 0));
     if (mixed) {
+      // monopole gravity of the 1-D requests that have it, from each stage's state (only
+      // while such a request is resident)
+      if (s->mono1d) launch_monopole1d(s->d_probs, s->d_times, s->max_probs, s->tb, s->P, s->stream);
       launch_stage1d_mixed(0, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
                            s->P, s->P, s->PH, s->stream);
+      if (s->mono1d) launch_monopole1d(s->d_probs, s->d_times, s->max_probs, s->tb, s->PH, s->stream);
       launch_stage1d_mixed(1, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
                            s->PH, s->P, s->P, s->stream);
     } else {
@@ -524,9 +530,11 @@ int round_once(mdg_server *s, int *active_out)
   for (int k = 0; k < s->max_probs; k++) active += s->slots[k] != nullptr;
   if (s->tiles_dirty) {
     std::vector<Tile> tl, xt, yt;
+    s->mono1d = false;
     for (int k = 0; k < s->max_probs; k++) {
       const Request *r = s->slots[k];
       if (!r || is_dendritic(r->desc)) continue;   // dendritic problems run on their own grids
+      if (r->desc.ndim == 1 && r->desc.monopole) s->mono1d = true;
       if (r->desc.ndim == 2) {
         // the solver's 2-D tiling: direction-0 tiles of TIX2 rows x NTX2 columns,
         // direction-1 tiles of TIY2 rows x TJY2 columns
@@ -567,7 +575,8 @@ int round_once(mdg_server *s, int *active_out)
     const int K = s->cfg.steps_per_round;
     SCK(cudaEventRecord(s->ev0, s->stream));
     if (s->cfg.precision == MDG_PREC_MIXED) {
-      if (s->graph && (s->graph_ntx2 != s->ntx2 || s->graph_nty2 != s->nty2 || s->graph_jobs3_version != s->jobs3_version)) {
+      if (s->graph && (s->graph_ntx2 != s->ntx2 || s->graph_nty2 != s->nty2 ||
+                       s->graph_jobs3_version != s->jobs3_version || s->graph_mono1d != (int)s->mono1d)) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
       }
@@ -590,6 +599,7 @@ int round_once(mdg_server *s, int *active_out)
         s->graph_ntx2 = s->ntx2;
         s->graph_nty2 = s->nty2;
         s->graph_jobs3_version = s->jobs3_version;
+        s->graph_mono1d = (int)s->mono1d;
       }
       SCK(cudaGraphLaunch(s->graph, s->stream));
     } else {
@@ -721,7 +731,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   SCKB(cudaMalloc(&s->d_geo, sizeof(double) * GF_NFIELDS * units));
   SCKB(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * std::max<int64_t>(c.max_zones, cells > 0 ? c.max_cells_2d : 0)));
   if (c.precision == MDG_PREC_MIXED) SCKB(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * units));
-  else SCKB(cudaMalloc(&s->d_gmono, sizeof(double) * units));
+  SCKB(cudaMalloc(&s->d_gmono, sizeof(double) * units));
   if (cells > 0) {
     SCKB(cudaMalloc(&s->d_state2, sizeof(double) * 3 * NPRIM * cells));
     SCKB(cudaMalloc(&s->d_shock0, cells));
@@ -765,8 +775,6 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
   if (rc != MDG_OK) return sfail(rc, "request: " + why);
   if (!(desc->tmax > 0.0) || !(desc->tmax < 1.0e99))
     return sfail(MDG_ERR_INVALID, "request: tmax must state a finite end time");
-  if (desc->monopole != 0 && ndim == 1 && s->cfg.precision == MDG_PREC_MIXED)
-    return sfail(MDG_ERR_NOTIMPL, "request: the 1-D mixed-precision sweep has no monopole gravity");
   if (is_dendritic(*desc)) {
     // 3-D requests and 2-D spherical (r, theta) requests: the dendritic lane
     if (s->cfg.hbm_bytes_3d <= 0) return sfail(MDG_ERR_NOTIMPL, "request: the server takes no dendritic-grid requests");
@@ -835,10 +843,11 @@ int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double 
       build_mixed_table(r->desc, 1, r->mx.data(), r->units, desc->n1 + 2 * NG);
     }
   } else if (s->cfg.precision == MDG_PREC_FP64 || desc->rcoord != MDG_RCOORD_UNIFORM ||
-             desc->thcoord != MDG_THCOORD_UNIFORM) {
+             desc->thcoord != MDG_THCOORD_UNIFORM || desc->monopole) {
     // the reference's Romberg tables, built here in the submitting thread so that the
     // request loop does not spend its time on them (the mixed sweep reads them, with
-    // FP32 weights from the same moments, on a non-uniform coordinate map)
+    // FP32 weights from the same moments, on a non-uniform coordinate map or with
+    // monopole gravity)
     r->rc.assign((size_t)RC_NFIELDS * r->units, 0.0);
     r->geo.assign((size_t)GF_NFIELDS * r->units, 0.0);
     build_recon_table(r->desc, 0, r->rc.data(), r->units, 0);

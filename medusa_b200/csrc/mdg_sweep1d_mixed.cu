@@ -315,6 +315,15 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
         }
       }
       if (P.grav_on) add_fixed_gravity(ph, P.grav, g0, g1, g2, 1, src);
+      if (P.mono) {
+        // monopole gravity (gravity.c:373-401) with the mass flux densities of the zone's
+        // FP64 face fluxes; such problems carry the Romberg tables (geo_tab)
+        const int64_t gi = P.geo_off + z + NG;
+        const double vr = sfl[RHO][t + 1] / (__ldg(tb.geo + GF_AREA * gs + gi + 1) + 1.0e-16);
+        const double vl = sfl[RHO][t] / (__ldg(tb.geo + GF_AREA * gs + gi) + 1.0e-16);
+        add_monopole_gravity(ph[RHO], tb.gmono[P.mono_off + z], vl, vr, P.x0 + z * P.dx0, P.dx0,
+                             __ldg(rc + RC_B0 * rcs + gi), __ldg(rc + RC_G0 * rcs + gi), src);
+      }
       p_to_u(pn, u, g0, g1, g2);
       p_to_u(ph, uh, g0, g1, g2);
       lmin = dt_source_control_1div(pn, u, src);

@@ -125,8 +125,8 @@ def _solver_to_end(pb, precision):
 
 def test_server_runs_monopole_requests():
     """Self-gravitating requests in an FP64 server (1-D with the dust-collapse hook, 3-D
-    dendritic) beside plain ones: each result equals the solver's, bit for bit; a mixed
-    server refuses 1-D monopole requests."""
+    dendritic) beside plain ones, and the 1-D ones in a mixed server: each result equals
+    the solver's, bit for bit."""
     reqs = [P.dust_collapse(200).copy(tmax=2.0e-3),
             P.spherical_1d("sod", 256, 1.4).copy(tmax=0.02),
             P.dust_collapse(16, 8, 16, ndim=3, radius="uniform", floors=False).copy(tmax=1.0e-3)]
@@ -139,7 +139,57 @@ def test_server_runs_monopole_requests():
             ref, (rt, _, rist) = _solver_to_end(pb, PREC_FP64)
             assert t == rt and ist == rist, pb.name
             assert np.array_equal(prim, ref), pb.name
-    with Server(precision=PREC_MIXED, hbm_bytes=64 << 20, max_problems=4, max_zones=4096) as srv:
-        with pytest.raises(MdgError) as e:
-            srv.submit(reqs[0])
-        assert e.value.code == 5
+    # a mixed server: the 1-D requests (one with monopole gravity) equal the mixed solver's
+    with Server(precision=PREC_MIXED, hbm_bytes=64 << 20, max_problems=4, max_zones=4096,
+                steps_per_round=9) as srv:
+        ids = [srv.submit(pb) for pb in reqs[:2]]
+        srv.run(0)
+        for rid, pb in zip(ids, reqs[:2]):
+            prim, t, ist, _ = srv.result(rid)
+            ref, (rt, _, rist) = _solver_to_end(pb, PREC_MIXED)
+            assert t == rt and ist == rist, pb.name
+            assert np.array_equal(prim, ref), pb.name
+
+
+@pytest.mark.parametrize("radius,floors,n1,nsteps", [("sinh", True, 200, 200), ("uniform", False, 128, 150)])
+def test_mixed_1d_monopole_matches_fp64(radius, floors, n1, nsteps):
+    """The mixed-precision 1-D sweep with monopole self-gravity (the dust collapse, with its
+    outer v^r hook) against the plain FP64 sweep at equal time: volume-weighted L1 of rho
+    and u <= 1e-4, mass difference <= 1e-6 relative; batched with problems without
+    gravity, its result equals its run alone.  (Without floors the collapse empties the
+    zones behind the sphere's edge: both sweeps reach negative density after ~190 steps.)"""
+    from medusa_b200 import analytic as A
+    pb = P.dust_collapse(n1, radius=radius, floors=floors)
+    with Solver(pb) as s:
+        s.step(nsteps)
+        ref = s.update_cpu(0)
+        t_end = s.time(0)[0]
+        m_ref, _ = s.conserved_totals()
+    with Solver(pb.copy(tmax=t_end), precision=PREC_MIXED) as s:
+        for _ in range(100):
+            s.step(5)
+            if s.time(0)[0] >= t_end * (1.0 - 1.0e-12):
+                break
+        mix = s.update_cpu(0)
+        t_mix = s.time(0)[0]
+        m_mix, _ = s.conserved_totals()
+    e = P.radial_edges(pb)
+    vol = e[1:] ** 3 - e[:-1] ** 3
+    l1_rho = A.l1_rel(mix[:, 0], ref[:, 0], vol)
+    l1_u = A.l1_rel(mix[:, 1], ref[:, 1], vol)
+    l1_v = A.l1_rel(mix[:, 2], ref[:, 2], vol)
+    drift_m = abs(m_mix[0] - m_ref[0]) / abs(m_ref[0])
+    record("gravity_mixed_dust1d_%s_%d" % (radius, n1), t=t_end, l1_rho=l1_rho, l1_u=l1_u, l1_vr=l1_v,
+           mass_drift=drift_m)
+    assert abs(t_mix - t_end) <= 1.0e-8 * t_end
+    assert l1_rho <= 1.0e-4 and l1_u <= 1.0e-4 and l1_v <= 1.0e-4
+    assert drift_m <= 1.0e-6
+    others = [P.spherical_1d("sedov", 300, 1.4, p_ratio=1.0e4, r0=0.05), P.sod(257)]
+    batch_probs = [others[0], pb, others[1]]
+    with Solver(batch_probs, precision=PREC_MIXED) as s:
+        s.step(30)
+        batch = [s.update_cpu(m) for m in range(3)]
+    for m, q in enumerate(batch_probs):
+        with Solver(q, precision=PREC_MIXED) as s:
+            s.step(30)
+            assert np.array_equal(s.update_cpu(0), batch[m]), q.name

@@ -62,7 +62,6 @@ def _create(pb, precision=0, nprob=1):
     (dict(grav=(0.0, -1.0, 0.0)), 0, 1),        # one gravity switch at a time
     (dict(monopole=2), 0, 1),
     (dict(prob_kind=7), 0, 1),
-    (dict(), 1, 5),                             # the 1-D mixed sweep has no monopole gravity
 ])
 def test_monopole_scope_checked_before_device_work(mutate, precision, code):
     pb = P.dust_collapse(64).copy(**mutate)
