@@ -484,42 +484,141 @@ __device__ __forceinline__ bool flag_shock(const Grid3 &g, int i, int jj, int kc
 }
 
 // Direction-0 faces: face (i, j, k) is the lower radial face of zone (i, j, k), i in [0, n1].
-template <int STAGE, bool MIX>
+// A work item is a run of up to RUN0 consecutive radial faces i0 .. i0+ni-1 of one (j, k)
+// column whose face rows share their theta and phi resolution (djs(i), dks(i, j)), so
+// every pencil entry (radial row ii at that resolution) is the same for all faces of the
+// run: each thread walks outwards through its column with a ring of pencil entries in
+// shared memory, loads one new entry and reconstructs one zone per face (zone i's left
+// face value for face i, its right face value kept for face i+1), where the reference's
+// interp() builds a 4-zone pencil and reconstructs two zones per face.  The values are
+// the same; only their reuse differs.
+struct Tile3R { int i0, ni, j, k0, cnt; };
+constexpr int RUN0 = 16;
+
+// The RK stage is a run-time argument here (not a template argument as in the other
+// face kernels): both stages then run the same code, which measured faster for stage 1
+// than its own specialisation.
+template <bool MIX>
 __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
-                                                     Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
+                                                     Grid3 g, const Tile3R *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, unsigned char *__restrict__ own,
-                                                     unsigned char *__restrict__ all0)
+                                                     unsigned char *__restrict__ all0, int stage)
 {
+  // ring of pencil entries (radial rows i-1 .. i+1; i-2 as well for the FP64 re-solve of
+  // the mixed sweep) and the right face values of the previous zone, [slot][var][thread]
+  constexpr int NS = MIX ? 4 : 3;
+  __shared__ double win[NS][7][NT3];
+  __shared__ double arb[7][NT3];
   __shared__ double sred[32];
   if (times[0].done) return;
   const ProbDev &P = probs[0];
-  const Tile3 t = tiles[blockIdx.x];
-  const int i = t.i, j = t.j, k = t.k0 + (int)threadIdx.x;
+  const Tile3R t = tiles[blockIdx.x];
+  const int tid = (int)threadIdx.x;
+  const int i0 = t.i0, j = t.j, k = t.k0 + tid;
   double lmin = 1.0e300;
-  if ((int)threadIdx.x < t.cnt) {
-    double pen[4][7];
+  if (tid < t.cnt) {
+    const int64_t rcs = g.n1 + 2 * NG;
+    auto slot = [&](int ii) { return (ii - i0 + 2) % NS; };
 #pragma unroll 1
-    for (int q = 0; q < 4; q++) pencil0(g, P, s, i, j, k, i - 2 + q, pen[q]);
-    const int ij = rowi(g, i, j);
-    double fl[NPRIM], ss;
-    const int isshock = solve_face<0, MIX>(P, pen, g.rc0, g.mx0, g.n1 + 2 * NG, i - 1 + NG, i + NG,
-                                           face_geom3<0>(g, ij), false, fl, ss);
-    const int64_t f = __ldg(g.f0 + ij) + k;
+    for (int ii = i0 - 2; ii <= i0; ii++) {
+      double w[7];
+      pencil0(g, P, s, i0, j, k, ii, w);
 #pragma unroll
-    for (int v = 0; v < NPRIM; v++) flux[v * g.nf0 + f] = fl[v];
-    if (i < g.n1) own[__ldg(g.cell + ij) + k] = (unsigned char)isshock;
-    if (STAGE == 0 && isshock) {
-      // shock marks of the zone and of the two zones inside it (step.c:1196-1204)
-      if (i < g.n1) all0[__ldg(g.cell + ij) + k] = 1;
-      for (int d = 1; d <= 2; d++) {
-        const int im = i - d;
-        if (im < 0) break;
-        const int jm = j * djs(g, i) / djs(g, im);
-        const int km = k * dks(g, i, j) / dks(g, im, jm);
-        all0[__ldg(g.cell + rowi(g, im, jm)) + km] = 1;
+      for (int v = 0; v < 7; v++) win[slot(ii)][v][tid] = w[v];
+    }
+    {
+      // right face values of zone i0-1
+      const int sm = slot(i0 - 2), s0 = slot(i0 - 1), sp = slot(i0);
+      if (MIX) {
+        const MixW w = load_mixw(g.mx0 + i0 - 1 + NG, rcs);
+#pragma unroll
+        for (int v = 0; v < 7; v++) {
+          const double a = win[s0][v][tid];
+          float dl, dr;
+          mixed_recon((float)(a - win[sm][v][tid]), (float)(win[sp][v][tid] - a), w, dl, dr);
+          arb[v][tid] = a + (double)dr;
+        }
+      } else {
+        const RcView<double, true> gz{g.rc0 + i0 - 1 + NG, rcs};
+#pragma unroll kReconUnroll
+        for (int v = 0; v < 7; v++) {
+          double al, ar;
+          recon_zone<double>(P.interp_order, win[sm][v][tid], win[s0][v][tid], win[sp][v][tid], gz, al, ar);
+          arb[v][tid] = ar;
+        }
       }
     }
-    lmin = g.dx0 / fabs(ss);
+#pragma unroll 1
+    for (int i = i0; i < i0 + t.ni; i++) {
+      {
+        double w[7];
+        pencil0(g, P, s, i0, j, k, i + 1, w);
+#pragma unroll
+        for (int v = 0; v < 7; v++) win[slot(i + 1)][v][tid] = w[v];
+      }
+      double pl[7], pr[7];
+      const int sm = slot(i - 1), s0 = slot(i), sp = slot(i + 1);
+      if (MIX) {
+        const MixW w = load_mixw(g.mx0 + i + NG, rcs);
+#pragma unroll
+        for (int v = 0; v < 7; v++) {
+          pl[v] = arb[v][tid];
+          const double a = win[s0][v][tid];
+          float dl, dr;
+          mixed_recon((float)(a - win[sm][v][tid]), (float)(win[sp][v][tid] - a), w, dl, dr);
+          pr[v] = a + (double)dl;
+          arb[v][tid] = a + (double)dr;
+        }
+      } else {
+        const RcView<double, true> gz{g.rc0 + i + NG, rcs};
+#pragma unroll kReconUnroll
+        for (int v = 0; v < 7; v++) {
+          pl[v] = arb[v][tid];
+          double al, ar;
+          recon_zone<double>(P.interp_order, win[sm][v][tid], win[s0][v][tid], win[sp][v][tid], gz, al, ar);
+          pr[v] = al;
+          arb[v][tid] = ar;
+        }
+      }
+      const int ij = rowi(g, i, j);
+      const FaceGeom<double> fg = face_geom3<0>(g, ij);
+      double fl[NPRIM], ss;
+      int isshock = -1;
+      if (!MIX) {
+        isshock = hllc3<0>(pl, pr, fg, fl, ss);
+      } else {
+        if (pl[6] == P.gam && pr[6] == P.gam) {
+          float sig;
+          int sh;
+          if (riemann_hllc_mixed<0>(pl, pr, fg, gam_const<float>((float)P.gam), fl, sig, sh)) {
+            ss = (double)sig;
+            isshock = sh;
+          }
+        }
+        if (isshock < 0) {
+          double pen[28];
+#pragma unroll
+          for (int q = 0; q < 28; q++) pen[q] = win[slot(i - 2 + q / 7)][q % 7][tid];
+          isshock = face_fp64_3d<0>(P.interp_order, pen, g.rc0, rcs, i - 1 + NG, i + NG, fg, fl, &ss);
+        }
+      }
+      const int64_t f = __ldg(g.f0 + ij) + k;
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) flux[v * g.nf0 + f] = fl[v];
+      if (i < g.n1) own[__ldg(g.cell + ij) + k] = (unsigned char)isshock;
+      if (stage == 0 && isshock) {
+        // shock marks of the zone and of the two zones inside it (step.c:1196-1204)
+        if (i < g.n1) all0[__ldg(g.cell + ij) + k] = 1;
+        for (int d = 1; d <= 2; d++) {
+          const int im = i - d;
+          if (im < 0) break;
+          const int jm = j * djs(g, i) / djs(g, im);
+          const int km = k * dks(g, i, j) / dks(g, im, jm);
+          all0[__ldg(g.cell + rowi(g, im, jm)) + km] = 1;
+        }
+      }
+      lmin = tmin(lmin, g.dx0 / fabs(ss));
+    }
   }
   block_min_to(lmin, &times[0].minacc, sred);
 }
@@ -970,7 +1069,8 @@ struct Sweep3 {
   char *d_tab = nullptr;           // all grid tables in one allocation
   double *d_flux = nullptr;        // F0 | F1 | F2, 5 arrays each
   unsigned char *d_bits = nullptr; // own0 | own1 | all0, one byte per zone each
-  Tile3 *d_tiles = nullptr;        // face0 | face1 | face2 | zone tiles
+  Tile3 *d_tiles = nullptr;        // face1 | face2 | zone tiles
+  Tile3R *d_runs0 = nullptr;       // direction-0 face runs
   double *d_gmono = nullptr;       // monopole gravity per radial row
   int nt[4] = {0, 0, 0, 0};
   int64_t ncell = 0;
@@ -1017,6 +1117,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   auto fail3 = [&](cudaError_t e) {
     why = cudaGetErrorString(e);
     cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles); cudaFree(w->d_gmono);
+    cudaFree(w->d_runs0);
     delete w;
     return e == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA;
   };
@@ -1058,9 +1159,26 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   e = cudaMemset(w->d_bits, 0, (size_t)3 * h.ncell);
   if (e != cudaSuccess) return fail3(e);
   // tiles of each kernel
-  std::vector<Tile3> t0, t1, t2, tc;
-  for (int i = 0; i <= h.n1; i++)
-    for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t0, i, j, h.nk[h.row(i, j)]);
+  std::vector<Tile3> t1, t2, tc;
+  std::vector<Tile3R> t0;
+  // direction-0 runs: faces i in [0, n1] grouped by constant theta resolution, then per
+  // theta row j by constant phi resolution, cut into RUN0 faces and NT3 phi columns
+  for (int i = 0; i <= h.n1;) {
+    int ie = i + 1;
+    while (ie <= h.n1 && h.dj(ie) == h.dj(i)) ie++;
+    for (int j = 0; j < h.njr(i); j++) {
+      for (int a = i; a < ie;) {
+        int b = a + 1;
+        while (b < ie && h.dk(b, j) == h.dk(a, j)) b++;
+        const int nk = h.nk[h.row(a, j)];
+        for (int c = a; c < b; c += RUN0)
+          for (int k0 = 0; k0 < nk; k0 += NT3)
+            t0.push_back(Tile3R{c, std::min(RUN0, b - c), j, k0, std::min(NT3, nk - k0)});
+        a = b;
+      }
+    }
+    i = ie;
+  }
   for (int i = 0; i < h.n1; i++)
     for (int j = 0; j <= h.njr(i); j++) tiles_of_rows(t1, i, j, h.n3 / std::min(h.dk(i, j), h.dk(i, j - 1)));
   for (int i = 0; i < h.n1 && h.ndim == 3; i++)
@@ -1069,13 +1187,16 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(tc, i, j, h.nk[h.row(i, j)]);
   w->nt[0] = (int)t0.size(); w->nt[1] = (int)t1.size(); w->nt[2] = (int)t2.size(); w->nt[3] = (int)tc.size();
   std::vector<Tile3> all;
-  all.insert(all.end(), t0.begin(), t0.end());
   all.insert(all.end(), t1.begin(), t1.end());
   all.insert(all.end(), t2.begin(), t2.end());
   all.insert(all.end(), tc.begin(), tc.end());
   e = cudaMalloc(&w->d_tiles, sizeof(Tile3) * all.size());
   if (e != cudaSuccess) return fail3(e);
   e = cudaMemcpy(w->d_tiles, all.data(), sizeof(Tile3) * all.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return fail3(e);
+  e = cudaMalloc(&w->d_runs0, sizeof(Tile3R) * t0.size());
+  if (e != cudaSuccess) return fail3(e);
+  e = cudaMemcpy(w->d_runs0, t0.data(), sizeof(Tile3R) * t0.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail3(e);
   *out = w;
   return MDG_OK;
@@ -1085,6 +1206,7 @@ void sweep3_destroy(Sweep3 *w)
 {
   if (!w) return;
   cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles); cudaFree(w->d_gmono);
+  cudaFree(w->d_runs0);
   delete w;
 }
 
@@ -1098,7 +1220,8 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
   const Grid3 &g = w->g;
   double *F0 = w->d_flux, *F1 = F0 + NPRIM * g.nf0, *F2 = F1 + NPRIM * g.nf1;
   unsigned char *own = w->d_bits + (size_t)stage * g.ncell, *all0 = w->d_bits + (size_t)2 * g.ncell;
-  const Tile3 *t0 = w->d_tiles, *t1 = t0 + w->nt[0], *t2 = t1 + w->nt[1], *tc = t2 + w->nt[2];
+  const Tile3R *t0 = w->d_runs0;
+  const Tile3 *t1 = w->d_tiles, *t2 = t1 + w->nt[1], *tc = t2 + w->nt[2];
   if (stage == 0) cudaMemsetAsync(all0, 0, (size_t)g.ncell, st);
   if (g.mono) {
     shell_mass3_kernel<<<(g.n1 + 127) / 128, 128, 0, st>>>(times, g, sst);
@@ -1107,7 +1230,7 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
   auto faces = [&](auto s0, auto mix) {
     constexpr int S = decltype(s0)::value;
     constexpr bool M = decltype(mix)::value;
-    face0_kernel<S, M><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0);
+    face0_kernel<M><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0, S);
     face1_kernel<S, M><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
     if (w->nt[2] > 0) face2_kernel<S, M><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
   };
@@ -1126,13 +1249,13 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
 
 void launch_totals3(Sweep3 *w, StateSoA s, double *out, cudaStream_t st)
 {
-  const Tile3 *tc = w->d_tiles + w->nt[0] + w->nt[1] + w->nt[2];
+  const Tile3 *tc = w->d_tiles + w->nt[1] + w->nt[2];
   totals3_kernel<<<1, 256, 0, st>>>(w->g, tc, w->nt[3], s, out);
 }
 
 void launch_initial_estimate3(Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA s, cudaStream_t st)
 {
-  const Tile3 *tc = w->d_tiles + w->nt[0] + w->nt[1] + w->nt[2];
+  const Tile3 *tc = w->d_tiles + w->nt[1] + w->nt[2];
   estimate3_kernel<<<w->nt[3], NT3, 0, st>>>(probs, times, w->g, tc, s);
 }
 
