@@ -492,7 +492,9 @@ __device__ __forceinline__ bool flag_shock(const Grid3 &g, int i, int jj, int kc
 // face value for face i, its right face value kept for face i+1), where the reference's
 // interp() builds a 4-zone pencil and reconstructs two zones per face.  The values are
 // the same; only their reuse differs.
-struct Tile3R { int i0, ni, j, k0, cnt; };
+// A run of faces along one direction: faces r0 .. r0+nr-1 of the fixed row `row` (the
+// theta row j for direction 0, the radial row i for direction 1), columns k0 .. k0+cnt-1.
+struct Tile3R { int r0, nr, row, k0, cnt; };
 constexpr int RUN0 = 16;
 
 // The RK stage is a run-time argument here (not a template argument as in the other
@@ -514,7 +516,7 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *_
   const ProbDev &P = probs[0];
   const Tile3R t = tiles[blockIdx.x];
   const int tid = (int)threadIdx.x;
-  const int i0 = t.i0, j = t.j, k = t.k0 + tid;
+  const int i0 = t.r0, j = t.row, k = t.k0 + tid;
   double lmin = 1.0e300;
   if (tid < t.cnt) {
     const int64_t rcs = g.n1 + 2 * NG;
@@ -549,7 +551,7 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *_
       }
     }
 #pragma unroll 1
-    for (int i = i0; i < i0 + t.ni; i++) {
+    for (int i = i0; i < i0 + t.nr; i++) {
       {
         double w[7];
         pencil0(g, P, s, i0, j, k, i + 1, w);
@@ -624,38 +626,130 @@ __global__ void __launch_bounds__(NT3, MDG_F3MINB) face0_kernel(const ProbDev *_
 }
 
 // Direction-1 faces: sub-face kk of face row (i, j), j in [0, nj(i)] (step.c:1212-1265).
-template <int STAGE, bool MIX>
+// As for direction 0, a work item is a run of up to RUN0 consecutive faces j0 .. j0+nj-1
+// of radial row i and sub-face column kk whose face rows share their phi resolution
+// mn = min(dks(i, j), dks(i, j-1)) (every pencil entry, theta row jj at that resolution,
+// is then the same for all faces of the run); a thread walks northwards through its
+// column, one new entry and one zone reconstruction per face.  Tile3R fields here:
+// r0 = j0, nr = faces, row = i.
+template <bool MIX>
 __global__ void __launch_bounds__(NT3, MDG_F3MINB) face1_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
-                                                     Grid3 g, const Tile3 *__restrict__ tiles, StateSoA s,
+                                                     Grid3 g, const Tile3R *__restrict__ tiles, StateSoA s,
                                                      double *__restrict__ flux, const unsigned char *__restrict__ own,
-                                                     const unsigned char *__restrict__ all0)
+                                                     const unsigned char *__restrict__ all0, int stage)
 {
+  constexpr int NS = MIX ? 4 : 3;
+  __shared__ double win[NS][7][NT3];
+  __shared__ double arb[7][NT3];
   __shared__ double sred[32];
   if (times[0].done) return;
   const ProbDev &P = probs[0];
-  const Tile3 t = tiles[blockIdx.x];
-  const int i = t.i, j = t.j, kk = t.k0 + (int)threadIdx.x;
+  const Tile3R t = tiles[blockIdx.x];
+  const int tid = (int)threadIdx.x;
+  const int j0 = t.r0, i = t.row, kk = t.k0 + tid;
   double lmin = 1.0e300;
-  if ((int)threadIdx.x < t.cnt) {
-    double pen[4][7];
-#pragma unroll 1
-    for (int q = 0; q < 4; q++) pencil1(g, P, s, i, j, kk, j - 2 + q, pen[q]);
+  if (tid < t.cnt) {
+    const int64_t cs = g.cols1;
     const int64_t base = g.rc1_base[ilog2(djs(g, i))] + NG;
-    // zone k of row j that owns the sub-face, and the transverse_shock test of zone k
-    const int dkj = dks(g, i, j), dkjm = dks(g, i, j - 1);
-    const int mn = dkj < dkjm ? dkj : dkjm;
-    const int k = kk / (dkj / mn);
-    const int nkm = dkj / dkjm;
-    bool hlle = flag_shock<STAGE>(g, i, j, k, own, all0);
-    for (int q = k * nkm; q < k * nkm + nkm; q++) hlle = hlle || flag_shock<STAGE>(g, i, j - 1, q, own, all0);
-    const int ij = rowi(g, i, j);
-    const FaceGeom<double> fg = face_geom3<1>(g, ij);
-    double fl[NPRIM], ss;
-    solve_face<1, MIX>(P, pen, g.rc1, g.mx1, g.cols1, base + j - 1, base + j, fg, hlle, fl, ss);
-    const int64_t f = __ldg(g.f1 + ij) + kk;
+    auto slot = [&](int jj) { return (jj - j0 + 2) % NS; };
+#pragma unroll 1
+    for (int jj = j0 - 2; jj <= j0; jj++) {
+      double w[7];
+      pencil1(g, P, s, i, j0, kk, jj, w);
 #pragma unroll
-    for (int v = 0; v < NPRIM; v++) flux[v * g.nf1 + f] = fl[v];
-    lmin = djs(g, i) * g.dx1 / fabs(ss);
+      for (int v = 0; v < 7; v++) win[slot(jj)][v][tid] = w[v];
+    }
+    {
+      // right face values of zone j0-1
+      const int sm = slot(j0 - 2), s0 = slot(j0 - 1), sp = slot(j0);
+      if (MIX) {
+        const MixW w = load_mixw(g.mx1 + base + j0 - 1, cs);
+#pragma unroll
+        for (int v = 0; v < 7; v++) {
+          const double a = win[s0][v][tid];
+          float dl, dr;
+          mixed_recon((float)(a - win[sm][v][tid]), (float)(win[sp][v][tid] - a), w, dl, dr);
+          arb[v][tid] = a + (double)dr;
+        }
+      } else {
+        const RcView<double, true> gz{g.rc1 + base + j0 - 1, cs};
+#pragma unroll kReconUnroll
+        for (int v = 0; v < 7; v++) {
+          double al, ar;
+          recon_zone<double>(P.interp_order, win[sm][v][tid], win[s0][v][tid], win[sp][v][tid], gz, al, ar);
+          arb[v][tid] = ar;
+        }
+      }
+    }
+#pragma unroll 1
+    for (int j = j0; j < j0 + t.nr; j++) {
+      {
+        double w[7];
+        pencil1(g, P, s, i, j0, kk, j + 1, w);
+#pragma unroll
+        for (int v = 0; v < 7; v++) win[slot(j + 1)][v][tid] = w[v];
+      }
+      double pl[7], pr[7];
+      const int sm = slot(j - 1), s0 = slot(j), sp = slot(j + 1);
+      if (MIX) {
+        const MixW w = load_mixw(g.mx1 + base + j, cs);
+#pragma unroll
+        for (int v = 0; v < 7; v++) {
+          pl[v] = arb[v][tid];
+          const double a = win[s0][v][tid];
+          float dl, dr;
+          mixed_recon((float)(a - win[sm][v][tid]), (float)(win[sp][v][tid] - a), w, dl, dr);
+          pr[v] = a + (double)dl;
+          arb[v][tid] = a + (double)dr;
+        }
+      } else {
+        const RcView<double, true> gz{g.rc1 + base + j, cs};
+#pragma unroll kReconUnroll
+        for (int v = 0; v < 7; v++) {
+          pl[v] = arb[v][tid];
+          double al, ar;
+          recon_zone<double>(P.interp_order, win[sm][v][tid], win[s0][v][tid], win[sp][v][tid], gz, al, ar);
+          pr[v] = al;
+          arb[v][tid] = ar;
+        }
+      }
+      // zone k of row j that owns the sub-face, and the transverse_shock test of zone k
+      const int dkj = dks(g, i, j), dkjm = dks(g, i, j - 1);
+      const int mn = dkj < dkjm ? dkj : dkjm;
+      const int k = kk / (dkj / mn);
+      const int nkm = dkj / dkjm;
+      bool hlle = (stage == 0) ? flag_shock<0>(g, i, j, k, own, all0) : flag_shock<1>(g, i, j, k, own, all0);
+      for (int q = k * nkm; q < k * nkm + nkm; q++)
+        hlle = hlle || ((stage == 0) ? flag_shock<0>(g, i, j - 1, q, own, all0) : flag_shock<1>(g, i, j - 1, q, own, all0));
+      const int ij = rowi(g, i, j);
+      const FaceGeom<double> fg = face_geom3<1>(g, ij);
+      double fl[NPRIM], ss;
+      if (hlle) {
+        hlle3<1>(pl, pr, fg, fl, ss);
+      } else if (!MIX) {
+        hllc3<1>(pl, pr, fg, fl, ss);
+      } else {
+        bool done = false;
+        if (pl[6] == P.gam && pr[6] == P.gam) {
+          float sig;
+          int sh;
+          if (riemann_hllc_mixed<1>(pl, pr, fg, gam_const<float>((float)P.gam), fl, sig, sh)) {
+            ss = (double)sig;
+            done = true;
+          }
+        }
+        if (!done) {
+          double pen[28];
+#pragma unroll
+          for (int q = 0; q < 28; q++) pen[q] = win[slot(j - 2 + q / 7)][q % 7][tid];
+          face_fp64_3d<1>(P.interp_order, pen, g.rc1, cs, base + j - 1, base + j, fg, fl, &ss);
+        }
+      }
+      const int64_t f = __ldg(g.f1 + ij) + kk;
+#pragma unroll
+      for (int v = 0; v < NPRIM; v++) flux[v * g.nf1 + f] = fl[v];
+      lmin = tmin(lmin, djs(g, i) * g.dx1 / fabs(ss));
+    }
   }
   block_min_to(lmin, &times[0].minacc, sred);
 }
@@ -1069,8 +1163,8 @@ struct Sweep3 {
   char *d_tab = nullptr;           // all grid tables in one allocation
   double *d_flux = nullptr;        // F0 | F1 | F2, 5 arrays each
   unsigned char *d_bits = nullptr; // own0 | own1 | all0, one byte per zone each
-  Tile3 *d_tiles = nullptr;        // face1 | face2 | zone tiles
-  Tile3R *d_runs0 = nullptr;       // direction-0 face runs
+  Tile3 *d_tiles = nullptr;        // face2 | zone tiles
+  Tile3R *d_runs = nullptr;        // direction-0 face runs | direction-1 face runs
   double *d_gmono = nullptr;       // monopole gravity per radial row
   int nt[4] = {0, 0, 0, 0};
   int64_t ncell = 0;
@@ -1117,7 +1211,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   auto fail3 = [&](cudaError_t e) {
     why = cudaGetErrorString(e);
     cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles); cudaFree(w->d_gmono);
-    cudaFree(w->d_runs0);
+    cudaFree(w->d_runs);
     delete w;
     return e == cudaErrorMemoryAllocation ? MDG_ERR_OUTOFMEM : MDG_ERR_CUDA;
   };
@@ -1159,8 +1253,8 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   e = cudaMemset(w->d_bits, 0, (size_t)3 * h.ncell);
   if (e != cudaSuccess) return fail3(e);
   // tiles of each kernel
-  std::vector<Tile3> t1, t2, tc;
-  std::vector<Tile3R> t0;
+  std::vector<Tile3> t2, tc;
+  std::vector<Tile3R> t0, t1;
   // direction-0 runs: faces i in [0, n1] grouped by constant theta resolution, then per
   // theta row j by constant phi resolution, cut into RUN0 faces and NT3 phi columns
   for (int i = 0; i <= h.n1;) {
@@ -1179,24 +1273,37 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
     }
     i = ie;
   }
-  for (int i = 0; i < h.n1; i++)
-    for (int j = 0; j <= h.njr(i); j++) tiles_of_rows(t1, i, j, h.n3 / std::min(h.dk(i, j), h.dk(i, j - 1)));
+  // direction-1 runs: faces j in [0, nj(i)] of radial row i grouped by constant phi
+  // resolution of the face, min(dk(i, j), dk(i, j-1)), cut into RUN0 faces and NT3 columns
+  for (int i = 0; i < h.n1; i++) {
+    const int nj = h.njr(i);
+    auto mn = [&](int j) { return std::min(h.dk(i, j), h.dk(i, j - 1)); };
+    for (int a = 0; a <= nj;) {
+      int b = a + 1;
+      while (b <= nj && mn(b) == mn(a)) b++;
+      const int cnt = h.n3 / mn(a);
+      for (int c = a; c < b; c += RUN0)
+        for (int k0 = 0; k0 < cnt; k0 += NT3)
+          t1.push_back(Tile3R{c, std::min(RUN0, b - c), i, k0, std::min(NT3, cnt - k0)});
+      a = b;
+    }
+  }
   for (int i = 0; i < h.n1 && h.ndim == 3; i++)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t2, i, j, h.nk[h.row(i, j)] + 1, T2);
   for (int i = 0; i < h.n1; i++)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(tc, i, j, h.nk[h.row(i, j)]);
   w->nt[0] = (int)t0.size(); w->nt[1] = (int)t1.size(); w->nt[2] = (int)t2.size(); w->nt[3] = (int)tc.size();
   std::vector<Tile3> all;
-  all.insert(all.end(), t1.begin(), t1.end());
   all.insert(all.end(), t2.begin(), t2.end());
   all.insert(all.end(), tc.begin(), tc.end());
   e = cudaMalloc(&w->d_tiles, sizeof(Tile3) * all.size());
   if (e != cudaSuccess) return fail3(e);
   e = cudaMemcpy(w->d_tiles, all.data(), sizeof(Tile3) * all.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail3(e);
-  e = cudaMalloc(&w->d_runs0, sizeof(Tile3R) * t0.size());
+  t0.insert(t0.end(), t1.begin(), t1.end());
+  e = cudaMalloc(&w->d_runs, sizeof(Tile3R) * t0.size());
   if (e != cudaSuccess) return fail3(e);
-  e = cudaMemcpy(w->d_runs0, t0.data(), sizeof(Tile3R) * t0.size(), cudaMemcpyHostToDevice);
+  e = cudaMemcpy(w->d_runs, t0.data(), sizeof(Tile3R) * t0.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail3(e);
   *out = w;
   return MDG_OK;
@@ -1206,7 +1313,7 @@ void sweep3_destroy(Sweep3 *w)
 {
   if (!w) return;
   cudaFree(w->d_tab); cudaFree(w->d_flux); cudaFree(w->d_bits); cudaFree(w->d_tiles); cudaFree(w->d_gmono);
-  cudaFree(w->d_runs0);
+  cudaFree(w->d_runs);
   delete w;
 }
 
@@ -1220,8 +1327,8 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
   const Grid3 &g = w->g;
   double *F0 = w->d_flux, *F1 = F0 + NPRIM * g.nf0, *F2 = F1 + NPRIM * g.nf1;
   unsigned char *own = w->d_bits + (size_t)stage * g.ncell, *all0 = w->d_bits + (size_t)2 * g.ncell;
-  const Tile3R *t0 = w->d_runs0;
-  const Tile3 *t1 = w->d_tiles, *t2 = t1 + w->nt[1], *tc = t2 + w->nt[2];
+  const Tile3R *t0 = w->d_runs, *t1 = t0 + w->nt[0];
+  const Tile3 *t2 = w->d_tiles, *tc = t2 + w->nt[2];
   if (stage == 0) cudaMemsetAsync(all0, 0, (size_t)g.ncell, st);
   if (g.mono) {
     shell_mass3_kernel<<<(g.n1 + 127) / 128, 128, 0, st>>>(times, g, sst);
@@ -1231,7 +1338,7 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
     constexpr int S = decltype(s0)::value;
     constexpr bool M = decltype(mix)::value;
     face0_kernel<M><<<w->nt[0], NT3, 0, st>>>(probs, times, g, t0, sst, F0, own, all0, S);
-    face1_kernel<S, M><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0);
+    face1_kernel<M><<<w->nt[1], NT3, 0, st>>>(probs, times, g, t1, sst, F1, own, all0, S);
     if (w->nt[2] > 0) face2_kernel<S, M><<<w->nt[2], NT3, 0, st>>>(probs, times, g, t2, sst, F2, own, all0);
   };
   using I0 = std::integral_constant<int, 0>;
@@ -1249,13 +1356,13 @@ void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, Prob
 
 void launch_totals3(Sweep3 *w, StateSoA s, double *out, cudaStream_t st)
 {
-  const Tile3 *tc = w->d_tiles + w->nt[1] + w->nt[2];
+  const Tile3 *tc = w->d_tiles + w->nt[2];
   totals3_kernel<<<1, 256, 0, st>>>(w->g, tc, w->nt[3], s, out);
 }
 
 void launch_initial_estimate3(Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA s, cudaStream_t st)
 {
-  const Tile3 *tc = w->d_tiles + w->nt[1] + w->nt[2];
+  const Tile3 *tc = w->d_tiles + w->nt[2];
   estimate3_kernel<<<w->nt[3], NT3, 0, st>>>(probs, times, w->g, tc, s);
 }
 
