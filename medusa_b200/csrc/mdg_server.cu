@@ -172,8 +172,11 @@ struct mdg_server {
   StateSoA P2{}, PH2{}, ACC2{};
   Tile *d_tiles2 = nullptr;
   int tiles2_cap = 0, ntx2 = 0, nty2 = 0;
-  cudaStream_t stream2 = nullptr, stream3 = nullptr;   // 2-D lane, 3-D lane
-  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3 = nullptr;
+  // 2-D lane; 3-D lane: resident dendritic requests spread over NS3 streams, so that
+  // several grids (each too small to fill the GPU alone) run side by side
+  static constexpr int NS3 = 4;
+  cudaStream_t stream2 = nullptr, stream3[NS3] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3[NS3] = {};
   int graph_ntx2 = -1, graph_nty2 = -1;   // 2-D tile counts the graph was captured with
   // 3-D lane: resident 3-D requests (each with its own grid), on the second stream
   std::vector<Request *> jobs3;
@@ -210,8 +213,10 @@ void free_server(mdg_server *s)
   if (s->ev1) cudaEventDestroy(s->ev1);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->ev_join) cudaEventDestroy(s->ev_join);
-  if (s->ev_join3) cudaEventDestroy(s->ev_join3);
-  if (s->stream3) cudaStreamDestroy(s->stream3);
+  for (int q = 0; q < mdg_server::NS3; q++) {
+    if (s->ev_join3[q]) cudaEventDestroy(s->ev_join3[q]);
+    if (s->stream3[q]) cudaStreamDestroy(s->stream3[q]);
+  }
   cudaFree(s->d_probs); cudaFree(s->d_times); cudaFree(s->d_tiles); cudaFree(s->d_queue); cudaFree(s->d_err);
   cudaFree(s->d_state); cudaFree(s->d_rc0); cudaFree(s->d_geo); cudaFree(s->d_stage); cudaFree(s->d_mx);
   cudaFree(s->d_gmono);
@@ -276,7 +281,8 @@ int queue_round(mdg_server *s, int nsteps)
     launch_dt_finalize(s->d_probs, s->d_times, s->max_probs, s->d_err, s->stream);
     if (lane2 || lane3) SCK(cudaEventRecord(s->ev_fork, s->stream));
     if (lane2) SCK(cudaStreamWaitEvent(s->stream2, s->ev_fork, 0));
-    if (lane3) SCK(cudaStreamWaitEvent(s->stream3, s->ev_fork, 0));
+    const int n3s = lane3 ? std::min<int>(mdg_server::NS3, (int)s->jobs3.size()) : 0;
+    for (int q = 0; q < n3s; q++) SCK(cudaStreamWaitEvent(s->stream3[q], s->ev_fork, 0));
     if (mixed) {
       // monopole gravity of the 1-D requests that have it, from each stage's state (only
       // while such a request is resident)
@@ -303,14 +309,18 @@ int queue_round(mdg_server *s, int nsteps)
       SCK(cudaStreamWaitEvent(s->stream, s->ev_join, 0));
     }
     if (lane3) {
-      for (Request *r : s->jobs3) {
+      for (size_t n = 0; n < s->jobs3.size(); n++) {
+        Request *r = s->jobs3[n];
+        cudaStream_t st = s->stream3[n % mdg_server::NS3];
         ProbDev *pr = s->d_probs + r->slot;
         ProbTime *tr = s->d_times + r->slot;
-        launch_stage3d(0, mixed, r->s3, pr, tr, soa3(r, 0), soa3(r, 0), soa3(r, 1), s->stream3);
-        launch_stage3d(1, mixed, r->s3, pr, tr, soa3(r, 1), soa3(r, 0), soa3(r, 0), s->stream3);
+        launch_stage3d(0, mixed, r->s3, pr, tr, soa3(r, 0), soa3(r, 0), soa3(r, 1), st);
+        launch_stage3d(1, mixed, r->s3, pr, tr, soa3(r, 1), soa3(r, 0), soa3(r, 0), st);
       }
-      SCK(cudaEventRecord(s->ev_join3, s->stream3));
-      SCK(cudaStreamWaitEvent(s->stream, s->ev_join3, 0));
+      for (int q = 0; q < n3s; q++) {
+        SCK(cudaEventRecord(s->ev_join3[q], s->stream3[q]));
+        SCK(cudaStreamWaitEvent(s->stream, s->ev_join3[q], 0));
+      }
     }
     launch_finish(s->d_times, s->max_probs, s->stream);
   }
@@ -715,12 +725,12 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   SCKB(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, c.device));
   SCKB(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
   SCKB(cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
-  SCKB(cudaStreamCreateWithFlags(&s->stream3, cudaStreamNonBlocking));
+  for (int q = 0; q < mdg_server::NS3; q++) SCKB(cudaStreamCreateWithFlags(&s->stream3[q], cudaStreamNonBlocking));
   SCKB(cudaEventCreate(&s->ev0));
   SCKB(cudaEventCreate(&s->ev1));
   SCKB(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
   SCKB(cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
-  SCKB(cudaEventCreateWithFlags(&s->ev_join3, cudaEventDisableTiming));
+  for (int q = 0; q < mdg_server::NS3; q++) SCKB(cudaEventCreateWithFlags(&s->ev_join3[q], cudaEventDisableTiming));
   SCKB(cudaMalloc(&s->d_probs, sizeof(ProbDev) * s->max_probs));
   SCKB(cudaMalloc(&s->d_times, sizeof(ProbTime) * s->max_probs));
   SCKB(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->max_tiles));
