@@ -31,6 +31,24 @@ enum Geo3Field {
 static_assert(G3_NFIELDS == MDG_GEO3_FIELDS, "row geometry record of mdg_grid3d_geometry");
 
 // Device view of the grid and its tables (pointers into one device allocation).
+// Flux addresses push() reads for the zones of one interior row (i, j), precomputed on the
+// host from the dendritic structure (the device then issues every flux load of a zone at
+// once instead of walking the row tables): the direction-0 faces of the one or two rows
+// of radial row i+1 over it (zone k collects nkp consecutive faces of each, from face
+// k*nkp), its own lower direction-0 faces, the direction-1 faces of rows (i, j+1) and
+// (i, j) with their fan-in, and its direction-2 faces.
+struct PushRow3 {
+  int64_t f0o[2];   // first direction-0 face of the outer rows (i+1, jp), (i+1, jp+1)
+  int64_t f0i;      // first direction-0 face of row (i, j)
+  int64_t f1o, f1i; // first direction-1 face of rows (i, j+1) and (i, j)
+  int64_t f2;       // first direction-2 face of row (i, j) (3-D grids)
+  int64_t cell;     // first zone of row (i, j)
+  int nf0o;         // outer rows: 1 or 2
+  int nkp[2];       // outer faces per zone of each outer row
+  int mo;           // outer theta faces: 0 one per zone, 1 half of a coarser row's face, 2 two faces
+  int mi;           // inner theta faces: 0 one per zone, 1 halves of two faces
+};
+
 struct Grid3 {
   int ndim;                   // 3, or 2 for the axisymmetric (r, theta) grid (n3 = 1, no phi faces)
   int n1, n2, n3;
@@ -61,6 +79,7 @@ struct Grid3 {
   double *gmono;              // [n1] monopole gravity at the radial zone centroids (shell masses first)
   double x0;                  // startx[0]
   int mono;                   // GRAV=SPHERICAL_MONOPOLE_GRAV
+  const PushRow3 *prow;       // [nij] push() flux addresses of interior rows
 };
 
 MDG_HD inline int ilog2(int s)

@@ -937,7 +937,8 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
   double lmin = 1.0e300, lmax = 0.0;
   if ((int)threadIdx.x < t.cnt) {
     const int ij = rowi(g, i, j);
-    const int64_t c = __ldg(g.cell + ij) + k;
+    const PushRow3 &pr = g.prow[ij];
+    const int64_t c = pr.cell + k;
     double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM], divF[NPRIM], pf[NPRIM];
 #pragma unroll
     for (int v = 0; v < NPRIM; v++) ph[v] = sst.v[v][c];
@@ -1006,37 +1007,34 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
     for (int v = 0; v < NPRIM; v++) divF[v] = 0.0;
     // direction 0: outer face(s) on row i+1, inner face
     {
-      const int dji = djs(g, i), djo = djs(g, i + 1);
-      const int jp = j * dji / djo;
-      const int njp = (djo < dji) ? dji / djo : 1;
-      const int dkij = dks(g, i, j);
-      for (int jj = jp; jj < jp + njp; jj++) {
-        const int nkp = dkij / dks(g, i + 1, jj);
-        const int64_t fb = __ldg(g.f0 + rowi(g, i + 1, jj));
+      const int nf0o = pr.nf0o;
+      for (int q = 0; q < nf0o; q++) {
+        const int nkp = pr.nkp[q];
+        const int64_t fb = pr.f0o[q];
         for (int kk = k * nkp; kk < k * nkp + nkp; kk++) {
 #pragma unroll
           for (int v = 0; v < NPRIM; v++) divF[v] += F0[v * g.nf0 + fb + kk];
         }
       }
-      const int64_t fi = __ldg(g.f0 + ij) + k;
+      const int64_t fi = pr.f0i + k;
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) divF[v] -= F0[v * g.nf0 + fi];
     }
     // direction 1
     {
-      const int dkj = dks(g, i, j), dkp = dks(g, i, j + 1), dkm = dks(g, i, j - 1);
-      const int64_t fo = __ldg(g.f1 + rowi(g, i, j + 1)), fin = __ldg(g.f1 + ij);
-      if (dkp > dkj) {
+      const int64_t fo = pr.f1o, fin = pr.f1i;
+      const int mo = pr.mo, mi = pr.mi;
+      if (mo == 1) {
 #pragma unroll
         for (int v = 0; v < NPRIM; v++) divF[v] += 0.5 * F1[v * g.nf1 + fo + k];
-      } else if (dkp < dkj) {
+      } else if (mo == 2) {
 #pragma unroll
         for (int v = 0; v < NPRIM; v++) divF[v] += F1[v * g.nf1 + fo + 2 * k] + F1[v * g.nf1 + fo + 2 * k + 1];
       } else {
 #pragma unroll
         for (int v = 0; v < NPRIM; v++) divF[v] += F1[v * g.nf1 + fo + k];
       }
-      if (dkm < dkj) {
+      if (mi == 1) {
 #pragma unroll
         for (int v = 0; v < NPRIM; v++)
           divF[v] -= 0.5 * F1[v * g.nf1 + fin + 2 * k] + 0.5 * F1[v * g.nf1 + fin + 2 * k + 1];
@@ -1047,7 +1045,7 @@ __global__ void __launch_bounds__(NT3, MDG_P3MINB) push3_kernel(const ProbDev *_
     }
     // direction 2
     if (g.ndim == 3) {
-      const int64_t f2 = __ldg(g.f2 + ij) + k;
+      const int64_t f2 = pr.f2 + k;
 #pragma unroll
       for (int v = 0; v < NPRIM; v++) divF[v] += F2[v * g.nf2 + f2 + 1] - F2[v * g.nf2 + f2];
     }
@@ -1184,6 +1182,30 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   if (h.nlev1 > G3_MAXLEV || h.nlev2 > G3_MAXLEV) { why = "too many refinement levels"; return MDG_ERR_INVALID; }
   Sweep3 *w = new Sweep3();
   w->ncell = h.ncell;
+  // push() flux addresses of every interior row (the fan-in rules of push3_kernel)
+  std::vector<PushRow3> prow((size_t)h.nij);
+  for (int i = 0; i < h.n1; i++) {
+    for (int j = 0; j < h.njr(i); j++) {
+      PushRow3 r{};
+      const int ij = h.row(i, j);
+      const int dji = h.dj(i), djo = h.dj(i + 1), dkij = h.dk(i, j);
+      const int jp = j * dji / djo;
+      r.nf0o = (djo < dji) ? dji / djo : 1;
+      for (int q = 0; q < r.nf0o; q++) {
+        r.nkp[q] = dkij / h.dk(i + 1, jp + q);
+        r.f0o[q] = h.f0[h.row(i + 1, jp + q)];
+      }
+      r.f0i = h.f0[ij];
+      const int dkp = h.dk(i, j + 1), dkm = h.dk(i, j - 1);
+      r.f1o = h.f1[h.row(i, j + 1)];
+      r.f1i = h.f1[ij];
+      r.mo = (dkp > dkij) ? 1 : (dkp < dkij ? 2 : 0);
+      r.mi = (dkm < dkij) ? 1 : 0;
+      r.f2 = h.ndim == 3 ? h.f2[ij] : 0;
+      r.cell = h.cell[ij];
+      prow[ij] = r;
+    }
+  }
   // one allocation for every table, each part 256-byte aligned
   std::vector<std::pair<const void *, size_t>> parts = {
       {h.nj.data(), h.nj.size() * sizeof(int)},         {h.rowbase.data(), h.rowbase.size() * sizeof(int)},
@@ -1197,7 +1219,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
       {h.cphc.data(), h.cphc.size() * sizeof(double)},  {h.sphl.data(), h.sphl.size() * sizeof(double)},
       {h.cphl.data(), h.cphl.size() * sizeof(double)},  {h.mx0.data(), h.mx0.size() * sizeof(float)},
       {h.mx1.data(), h.mx1.size() * sizeof(float)},     {h.mx2.data(), h.mx2.size() * sizeof(float)},
-      {h.medge.data(), h.medge.size() * sizeof(double)}};
+      {h.medge.data(), h.medge.size() * sizeof(double)},    {prow.data(), prow.size() * sizeof(PushRow3)}};
   std::vector<size_t> off(parts.size());
   size_t tot = 0;
   for (size_t q = 0; q < parts.size(); q++) {
@@ -1240,6 +1262,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   g.sphl = (const double *)(b + off[17]); g.cphl = (const double *)(b + off[18]);
   g.mx0 = (const float *)(b + off[19]); g.mx1 = (const float *)(b + off[20]); g.mx2 = (const float *)(b + off[21]);
   g.medge = (const double *)(b + off[22]);
+  g.prow = (const PushRow3 *)(b + off[23]);
   g.x0 = d.startx[0];
   g.mono = d.monopole;
   e = cudaMalloc(&w->d_gmono, sizeof(double) * (size_t)h.n1);
