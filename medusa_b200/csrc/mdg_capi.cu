@@ -72,6 +72,7 @@ struct mdg_solver {
   WorkQueue *d_queue = nullptr;
   Tile *d_mtiles = nullptr;
   int mtiles_cap = 0, nmtiles = 0;
+  int nmtab = 0;                  // the last nmtab mixed tiles: problems reading the Romberg tables
   int num_sms = 0;
   mdg_launch_config cfg{128, 0, 10};
   // CUDA graph of cfg.steps_per_graph steps (rebuilt when the launch shape changes)
@@ -232,14 +233,21 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   return MDG_OK;
 }
 
-// Tile list of the mixed sweep for nt threads per CTA (tiles of nt-2 zones) and the work
-// queue's item count.  Caller has synchronized the solver's stream.
+// Tile list of the mixed sweep for nt threads per CTA (tiles of nt-2 zones): the tiles of
+// problems with closed-form geometry, then those of problems reading the Romberg tables
+// (each part has its own launch and work queue).  Caller has synchronized the solver's
+// stream.
 static int build_mixed_tiles(mdg_solver *s, int nt)
 {
   const int tl = nt - 2;
   std::vector<Tile> t;
+  for (int pass = 0; pass < 2; pass++)
+    for (int m = 0; m < s->nprob; m++)
+      if ((s->hprobs[m].geo_tab != 0) == (pass == 1))
+        for (int i0 = 0; i0 < s->hprobs[m].n1; i0 += tl) t.push_back(Tile{m, i0, 0, 0});
+  int ntab = 0;
   for (int m = 0; m < s->nprob; m++)
-    for (int i0 = 0; i0 < s->hprobs[m].n1; i0 += tl) t.push_back(Tile{m, i0, 0, 0});
+    if (s->hprobs[m].geo_tab) ntab += (s->hprobs[m].n1 + tl - 1) / tl;
   if ((int)t.size() > s->mtiles_cap) {
     cudaFree(s->d_mtiles);
     s->d_mtiles = nullptr;
@@ -249,22 +257,23 @@ static int build_mixed_tiles(mdg_solver *s, int nt)
     s->mtiles_cap = (int)t.size();
   }
   CK(cudaMemcpy(s->d_mtiles, t.data(), sizeof(Tile) * t.size(), cudaMemcpyHostToDevice));
-  WorkQueue q{{0u, 0u}, (int)t.size(), 0};
-  CK(cudaMemcpy(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice));
   s->nmtiles = (int)t.size();
+  s->nmtab = ntab;
+  const WorkQueue q[2] = {{{0u, 0u}, s->nmtiles - ntab, 0}, {{0u, 0u}, ntab, 0}};
+  CK(cudaMemcpy(s->d_queue, q, sizeof q, cudaMemcpyHostToDevice));
   return MDG_OK;
 }
 
-// CTAs of one mixed-sweep launch: one per tile, or ctas_per_sm persistent CTAs per SM
-// (bounded by the occupancy of the kernel and by the number of tiles)
-static int mixed_grid(const mdg_solver *s)
+// CTAs of one mixed-sweep launch over ntiles tiles: one per tile, or ctas_per_sm
+// persistent CTAs per SM (bounded by the occupancy of the kernel and by the tile count)
+static int mixed_grid(const mdg_solver *s, int ntiles)
 {
-  if (s->cfg.ctas_per_sm <= 0) return s->nmtiles;
+  if (s->cfg.ctas_per_sm <= 0) return ntiles;
   int k = mixed_max_ctas_per_sm(s->cfg.threads);
   if (k <= 0) k = 1;
   if (s->cfg.ctas_per_sm < k) k = s->cfg.ctas_per_sm;
   const int64_t g = (int64_t)k * s->num_sms;
-  return (int)(g < s->nmtiles ? g : s->nmtiles);
+  return (int)(g < ntiles ? g : ntiles);
 }
 
 // Device record of one problem from its description (offsets left at zero).
@@ -577,8 +586,8 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
   CKC(cudaMalloc(&s->d_err, sizeof(int)));
   CKC(cudaMalloc(&s->d_totals, sizeof(double) * 2 * nprob));
-  CKC(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
-  CKC(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
+  CKC(cudaMalloc(&s->d_queue, 2 * sizeof(WorkQueue)));
+  CKC(cudaMemset(s->d_queue, 0, 2 * sizeof(WorkQueue)));
   if (precision == MDG_PREC_MIXED) CKC(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * rc0));
   if (precision == MDG_PREC_MIXED && ndim == 2) {
     CKC(cudaMalloc(&s->d_mx1, sizeof(float) * MX_NFIELDS * rc1));
@@ -713,7 +722,8 @@ static int queue_steps(mdg_solver *s, int nsteps)
   const bool mix3 = s->ndim == 3 && s->precision == MDG_PREC_MIXED;
   const bool mix2 = s->ndim == 2 && s->precision == MDG_PREC_MIXED;
   const bool mixed = s->ndim == 1 && s->precision == MDG_PREC_MIXED;   // the batched 1-D mixed sweep
-  const int mgrid = mixed ? mixed_grid(s) : 0;
+  const int nmu = s->nmtiles - s->nmtab;
+  const int mgrid = mixed ? mixed_grid(s, nmu) : 0, mgrid_tab = mixed ? mixed_grid(s, s->nmtab) : 0;
   const bool queue = s->cfg.ctas_per_sm > 0;
   for (int k = 0; k < nsteps; k++) {
     mark(MDG_TIMER_DT, 0);
@@ -721,9 +731,12 @@ static int queue_steps(mdg_solver *s, int nsteps)
     mark(MDG_TIMER_DT, 1);
     mark(MDG_TIMER_STAGE0, 0);
     if (mixed && s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->P, s->stream);
-    if (mixed)
+    if (mixed) {
       launch_stage1d_mixed(0, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
-                           s->tb, s->P, s->P, s->PH, s->stream);
+                           s->tb, s->P, s->P, s->PH, s->stream, false);
+      launch_stage1d_mixed(0, s->cfg.threads, mgrid_tab, queue, s->d_probs, s->d_times, s->d_mtiles + nmu,
+                           s->d_queue + 1, s->tb, s->P, s->P, s->PH, s->stream, true);
+    }
     else if (s->ndim == 3)
       launch_stage3d(0, mix3, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
     else if (s->ndim == 1) {
@@ -737,9 +750,12 @@ static int queue_steps(mdg_solver *s, int nsteps)
     mark(MDG_TIMER_STAGE0, 1);
     mark(MDG_TIMER_STAGE1, 0);
     if (mixed && s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->PH, s->stream);
-    if (mixed)
+    if (mixed) {
       launch_stage1d_mixed(1, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
-                           s->tb, s->PH, s->P, s->P, s->stream);
+                           s->tb, s->PH, s->P, s->P, s->stream, false);
+      launch_stage1d_mixed(1, s->cfg.threads, mgrid_tab, queue, s->d_probs, s->d_times, s->d_mtiles + nmu,
+                           s->d_queue + 1, s->tb, s->PH, s->P, s->P, s->stream, true);
+    }
     else if (s->ndim == 3)
       launch_stage3d(1, mix3, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
     else if (s->ndim == 1) {
@@ -957,8 +973,8 @@ int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
     int rc = build_mixed_tiles(s, cfg->threads);
     if (rc != MDG_OK) return rc;
   } else if (batched) {
-    WorkQueue q{{0u, 0u}, s->nmtiles, 0};
-    CK(cudaMemcpy(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice));
+    const WorkQueue q[2] = {{{0u, 0u}, s->nmtiles - s->nmtab, 0}, {{0u, 0u}, s->nmtab, 0}};
+    CK(cudaMemcpy(s->d_queue, q, sizeof q, cudaMemcpyHostToDevice));
   }
   if (reshape || cfg->ctas_per_sm != s->cfg.ctas_per_sm || cfg->steps_per_graph != s->cfg.steps_per_graph)
     drop_graph(s);

@@ -63,10 +63,12 @@ void launch_stage2d(int stage, bool mixed, const ProbDev *probs, ProbTime *times
                     const Tile *ytiles, int nyt, const Tables &tb, StateSoA stage_state, StateSoA state_n,
                     StateSoA acc, StateSoA out, unsigned char *shock0, unsigned char *shock1, cudaStream_t st);
 // Mixed-precision 1-D stage: nt threads per CTA (tile = nt-2 zones), grid CTAs; with
-// use_queue the CTAs are persistent and pull tiles from q, else CTA b takes tile b.
+// use_queue the CTAs are persistent and pull tiles from q, else CTA b takes tile b.  tab:
+// the tiles' problems read the Romberg tables (ProbDev::geo_tab), the others' geometry is
+// evaluated in closed form.
 void launch_stage1d_mixed(int stage, int nt, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
                           const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA stage_state,
-                          StateSoA state_n, StateSoA out, cudaStream_t st);
+                          StateSoA state_n, StateSoA out, cudaStream_t st, bool tab);
 int mixed_max_ctas_per_sm(int nt);
 // Monopole self-gravity of every 1-D problem with ProbDev::mono from its stage state:
 // the acceleration at each zone centroid into tb.gmono (gravity.c:145-425).

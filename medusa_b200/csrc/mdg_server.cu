@@ -146,7 +146,8 @@ struct mdg_server {
   ProbDev *d_probs = nullptr;
   ProbTime *d_times = nullptr;
   Tile *d_tiles = nullptr;
-  WorkQueue *d_queue = nullptr;
+  WorkQueue *d_queue = nullptr;   // [2]: closed-form 1-D tiles, tiles reading the Romberg tables
+  WorkQueue h_queue[2] = {};
   int *d_err = nullptr;
   double *d_state = nullptr, *d_rc0 = nullptr, *d_geo = nullptr, *d_stage = nullptr;
   double *d_gmono = nullptr;   // monopole gravity per zone unit
@@ -163,6 +164,8 @@ struct mdg_server {
   bool tiles_dirty = true;
   bool mono1d = false;                      // a resident 1-D request has monopole gravity
   int graph_mono1d = -1;                    // mono1d when the graph was captured
+  int ntab1d = 0;                           // the last ntab1d 1-D tiles: requests reading the Romberg tables
+  int graph_tab1d = -1;                     // ntab1d > 0 when the graph was captured
   // 2-D lane: cell arena, shock bits, tile lists (x tiles then y tiles), second stream
   int64_t cells = 0;
   RangeAlloc alloc2;
@@ -286,12 +289,21 @@ int queue_round(mdg_server *s, int nsteps)
     if (mixed) {
       // monopole gravity of the 1-D requests that have it, from each stage's state (only
       // while such a request is resident)
+      // closed-form tiles, then (while such requests are resident) the tiles of requests
+      // that read the Romberg tables, each with its own work queue
+      const int nu = s->ntiles - s->ntab1d;
       if (s->mono1d) launch_monopole1d(s->d_probs, s->d_times, s->max_probs, s->tb, s->P, s->stream);
       launch_stage1d_mixed(0, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
-                           s->P, s->P, s->PH, s->stream);
+                           s->P, s->P, s->PH, s->stream, false);
+      if (s->ntab1d > 0)
+        launch_stage1d_mixed(0, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles + nu, s->d_queue + 1,
+                             s->tb, s->P, s->P, s->PH, s->stream, true);
       if (s->mono1d) launch_monopole1d(s->d_probs, s->d_times, s->max_probs, s->tb, s->PH, s->stream);
       launch_stage1d_mixed(1, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles, s->d_queue, s->tb,
-                           s->PH, s->P, s->P, s->stream);
+                           s->PH, s->P, s->P, s->stream, false);
+      if (s->ntab1d > 0)
+        launch_stage1d_mixed(1, s->cfg.threads, grid, true, s->d_probs, s->d_times, s->d_tiles + nu, s->d_queue + 1,
+                             s->tb, s->PH, s->P, s->P, s->stream, true);
     } else {
       // monopole gravity of the 1-D requests that have it (one thread per slot; the others
       // return at once), from each stage's state
@@ -539,12 +551,18 @@ int round_once(mdg_server *s, int *active_out)
   int active = 0;
   for (int k = 0; k < s->max_probs; k++) active += s->slots[k] != nullptr;
   if (s->tiles_dirty) {
-    std::vector<Tile> tl, xt, yt;
+    std::vector<Tile> tl, tl_tab, xt, yt;
     s->mono1d = false;
+    const bool mixed1d = s->cfg.precision == MDG_PREC_MIXED;
     for (int k = 0; k < s->max_probs; k++) {
       const Request *r = s->slots[k];
       if (!r || is_dendritic(r->desc)) continue;   // dendritic problems run on their own grids
       if (r->desc.ndim == 1 && r->desc.monopole) s->mono1d = true;
+      if (r->desc.ndim == 1 && mixed1d && !r->geo.empty()) {
+        // a mixed request that reads the Romberg tables: the second 1-D list
+        for (int i0 = 0; i0 < r->desc.n1; i0 += s->tile_len) tl_tab.push_back(Tile{k, i0, 0, 0});
+        continue;
+      }
       if (r->desc.ndim == 2) {
         // the solver's 2-D tiling: direction-0 tiles of TIX2 rows x NTX2 columns,
         // direction-1 tiles of TIY2 rows x TJY2 columns
@@ -556,11 +574,15 @@ int round_once(mdg_server *s, int *active_out)
         for (int i0 = 0; i0 < r->desc.n1; i0 += s->tile_len) tl.push_back(Tile{k, i0, 0, 0});
       }
     }
+    s->ntab1d = (int)tl_tab.size();
+    const int nu = (int)tl.size();
+    tl.insert(tl.end(), tl_tab.begin(), tl_tab.end());
     if ((int)tl.size() > s->max_tiles) return sfail(MDG_ERR_INTERNAL, "tile list exceeds its capacity");
     if (!tl.empty())
       SCK(cudaMemcpyAsync(s->d_tiles, tl.data(), sizeof(Tile) * tl.size(), cudaMemcpyHostToDevice, s->stream));
-    WorkQueue q{{0u, 0u}, (int)tl.size(), 0};
-    SCK(cudaMemcpyAsync(s->d_queue, &q, sizeof q, cudaMemcpyHostToDevice, s->stream));
+    s->h_queue[0] = WorkQueue{{0u, 0u}, nu, 0};
+    s->h_queue[1] = WorkQueue{{0u, 0u}, s->ntab1d, 0};
+    SCK(cudaMemcpyAsync(s->d_queue, s->h_queue, sizeof s->h_queue, cudaMemcpyHostToDevice, s->stream));
     s->ntiles = (int)tl.size();
     const int n2d = (int)(xt.size() + yt.size());
     if (n2d > s->tiles2_cap) {
@@ -586,7 +608,8 @@ int round_once(mdg_server *s, int *active_out)
     SCK(cudaEventRecord(s->ev0, s->stream));
     if (s->cfg.precision == MDG_PREC_MIXED) {
       if (s->graph && (s->graph_ntx2 != s->ntx2 || s->graph_nty2 != s->nty2 ||
-                       s->graph_jobs3_version != s->jobs3_version || s->graph_mono1d != (int)s->mono1d)) {
+                       s->graph_jobs3_version != s->jobs3_version || s->graph_mono1d != (int)s->mono1d ||
+                       s->graph_tab1d != (int)(s->ntab1d > 0))) {
         cudaGraphExecDestroy(s->graph);
         s->graph = nullptr;
       }
@@ -610,6 +633,7 @@ int round_once(mdg_server *s, int *active_out)
         s->graph_nty2 = s->nty2;
         s->graph_jobs3_version = s->jobs3_version;
         s->graph_mono1d = (int)s->mono1d;
+        s->graph_tab1d = (int)(s->ntab1d > 0);
       }
       SCK(cudaGraphLaunch(s->graph, s->stream));
     } else {
@@ -734,7 +758,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   SCKB(cudaMalloc(&s->d_probs, sizeof(ProbDev) * s->max_probs));
   SCKB(cudaMalloc(&s->d_times, sizeof(ProbTime) * s->max_probs));
   SCKB(cudaMalloc(&s->d_tiles, sizeof(Tile) * s->max_tiles));
-  SCKB(cudaMalloc(&s->d_queue, sizeof(WorkQueue)));
+  SCKB(cudaMalloc(&s->d_queue, 2 * sizeof(WorkQueue)));
   SCKB(cudaMalloc(&s->d_err, sizeof(int)));
   SCKB(cudaMalloc(&s->d_state, sizeof(double) * 2 * NPRIM * units));
   SCKB(cudaMalloc(&s->d_rc0, sizeof(double) * RC_NFIELDS * units));
@@ -752,7 +776,7 @@ int mdg_server_create(const mdg_server_config *cfg, mdg_server **out)
   // empty slots: a zero record has tmax = 0, so the time loop treats it as finished
   SCKB(cudaMemset(s->d_probs, 0, sizeof(ProbDev) * s->max_probs));
   SCKB(cudaMemset(s->d_times, 0, sizeof(ProbTime) * s->max_probs));
-  SCKB(cudaMemset(s->d_queue, 0, sizeof(WorkQueue)));
+  SCKB(cudaMemset(s->d_queue, 0, 2 * sizeof(WorkQueue)));
   SCKB(cudaMemset(s->d_err, 0, sizeof(int)));
   SCKB(cudaMemset(s->d_state, 0, sizeof(double) * 2 * NPRIM * units));
 #undef SCKB

@@ -152,6 +152,88 @@ __device__ __forceinline__ double dt_source_control_1div(const double *p, const 
   return fmin(1.0e100, num / den);
 }
 
+// Face geometry of a problem on a non-uniform coordinate map (the Romberg tables).
+__device__ __forceinline__ FaceGeom<double> face_geom_tab(const double *geo, int64_t gs, int64_t gi)
+{
+  FaceGeom<double> fg;
+  fg.area = __ldg(geo + GF_AREA * gs + gi);
+  fg.scale = __ldg(geo + GF_FSCALE * gs + gi);
+  fg.g0 = __ldg(geo + GF_FG0 * gs + gi);
+  fg.g1 = __ldg(geo + GF_FG1 * gs + gi);
+  fg.g2 = __ldg(geo + GF_FG2 * gs + gi);
+  return fg;
+}
+
+// push() of zone z (thread t of the tile) for a problem that reads the Romberg tables (a
+// non-uniform coordinate map, or monopole gravity): the zone geometry and connection of
+// the tables with the FP64 source routine of the plain sweep, fixed or monopole gravity,
+// the update, u -> p and the next-dt zone term.  sv and sfl are the kernel's shared
+// pencil ([6][NT+2]) and face fluxes ([NPRIM][NT]).  Returns (source dt limit, zone term).
+template <int STAGE, int NT>
+__device__ __forceinline__ double2 push_zone_tab(const ProbDev &P, const Tables &tb, int z, int t, double dt,
+                                              const double *sv, const double *sfl, StateSoA sn, StateSoA out,
+                                              int64_t cell, ProbTime *tm)
+{
+  const int64_t gs = tb.geo_stride, rcs = tb.rc0_stride;
+  const int64_t gi = P.geo_off + z + NG;
+  const double *geo = tb.geo;
+  double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM];
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) ph[v] = sv[v * (NT + 2) + t + 1];
+  const double press = sv[5 * (NT + 2) + t + 1];
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) pn[v] = STAGE ? sn.v[v][cell] : ph[v];
+  const double vol = __ldg(geo + GF_VOL * gs + gi);
+  const double g0 = __ldg(geo + GF_G0 * gs + gi), g1 = __ldg(geo + GF_G1 * gs + gi), g2 = __ldg(geo + GF_G2 * gs + gi);
+  const double gc0 = __ldg(geo + GF_GC0 * gs + gi), gc1 = __ldg(geo + GF_GC1 * gs + gi);
+  const double gc2 = __ldg(geo + GF_GC2 * gs + gi), s00 = __ldg(geo + GF_S00 * gs + gi);
+  if (P.has_src) {
+    geo_sources_1d(geo, gs, gi, P.sparse_conn != 0, ph, press, g0, g1, g2, src);
+  } else {
+#pragma unroll
+    for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+  }
+  if (P.grav_on) add_fixed_gravity(ph, P.grav, g0, g1, g2, 1, src);
+  if (P.mono) {
+    // monopole gravity (gravity.c:373-401) with the mass flux densities of the zone's
+    // FP64 face fluxes
+    const double vr = sfl[RHO * NT + t + 1] / (__ldg(geo + GF_AREA * gs + gi + 1) + 1.0e-16);
+    const double vl = sfl[RHO * NT + t] / (__ldg(geo + GF_AREA * gs + gi) + 1.0e-16);
+    add_monopole_gravity(ph[RHO], tb.gmono[P.mono_off + z], vl, vr, P.x0 + z * P.dx0, P.dx0,
+                         __ldg(tb.rc0 + RC_B0 * rcs + gi), __ldg(tb.rc0 + RC_G0 * rcs + gi), src);
+  }
+  p_to_u(pn, u, g0, g1, g2);
+  p_to_u(ph, uh, g0, g1, g2);
+  double lmin = dt_source_control_1div(pn, u, src), lmax = 0.0;
+  const double ivol = 1.0 / vol;
+  const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) {
+    const double ddt = (sfl[v * NT + t + 1] - sfl[v * NT + t]) * ivol - src[v];
+    u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
+  }
+  double pf[NPRIM];
+  const double irho = 1.0 / u[RHO];
+  const double w1 = u[U1] * irho, w2 = u[U2] * irho, w3 = u[U3] * irho;
+  pf[RHO] = u[RHO];
+  pf[U1] = gc0 * w1;
+  pf[U2] = gc1 * w2;
+  pf[U3] = gc2 * w3;
+  pf[UU] = u[UU] - 0.5 * pf[RHO] * (w1 * pf[U1] + w2 * pf[U2] + w3 * pf[U3]);
+  if (P.floors) {
+    pf[RHO] = fmax(pf[RHO], P.rho_floor);
+    pf[UU] = fmax(pf[UU], P.e_floor);
+  }
+#pragma unroll
+  for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+  flag_nonfinite(pf, tm);
+  if (STAGE == 1) {
+    const double cs = sqrt(P.gam * press / ph[RHO]);
+    lmax = (fabs(pf[U1]) + cs / s00) / P.dx0;
+  }
+  return make_double2(lmin, lmax);
+}
+
 // Resident 64-thread-equivalents per SM the register allocation is bounded for (0: none).
 // The kernel waits mostly on global loads (state pencils, FP32 weights), so occupancy
 // pays: on the 2048-problem ensemble 16 x 64 threads per SM (64 registers, a few spilled
@@ -161,7 +243,10 @@ __device__ __forceinline__ double dt_source_control_1div(const double *p, const 
 #define MDG_MIX_MINB64 16
 #endif
 
-template <int NT, int STAGE>
+// TAB: the launch's problems read the Romberg tables (ProbDev::geo_tab: a non-uniform
+// coordinate map or monopole gravity); the solver and the server put their tiles in a
+// list of their own, so the closed-form instantiation carries none of that code.
+template <int NT, int STAGE, bool TAB>
 __global__ void __launch_bounds__(NT, MDG_MIX_MINB64 * 64 / NT)
 stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
                      const Tile *__restrict__ tiles, WorkQueue *__restrict__ q, bool use_queue,
@@ -248,18 +333,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
 #pragma unroll
       for (int v = 0; v < 6; v++) pl[v] = sar[v][t - 1];
       const int zf = z < 0 ? 0 : (z > n1 ? n1 : z);
-      FaceGeom<double> fg;
-      if (P.geo_tab) {
-        // a non-uniform coordinate map: the face geometry of the Romberg tables
-        const int64_t gi = P.geo_off + zf + NG;
-        fg.area = __ldg(tb.geo + GF_AREA * gs + gi);
-        fg.scale = __ldg(tb.geo + GF_FSCALE * gs + gi);
-        fg.g0 = __ldg(tb.geo + GF_FG0 * gs + gi);
-        fg.g1 = __ldg(tb.geo + GF_FG1 * gs + gi);
-        fg.g2 = __ldg(tb.geo + GF_FG2 * gs + gi);
-      } else {
-        fg = face_geom_1d(P, zf);
-      }
+      const FaceGeom<double> fg = TAB ? face_geom_tab(tb.geo, gs, P.geo_off + zf + NG) : face_geom_1d(P, zf);
       const GamConst<float> gc = gam_const<float>((float)P.gam);
       int isshock_unused;
       if (riemann_hllc_mixed<0>(pl, al, fg, gc, flux, sig, isshock_unused)) {
@@ -278,82 +352,62 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
     // push() for zone z in FP64 (step.c:380-470)
     if (t >= 1 && t <= NT - 2 && z >= 0 && z < n1) {
       const int64_t cell = P.cell_off + z;
-      double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM];
-#pragma unroll
-      for (int v = 0; v < NPRIM; v++) ph[v] = sv[v][t + 1];
-      if (STAGE == 0) {
-#pragma unroll
-        for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
+      if (TAB) {
+        const double2 r = push_zone_tab<STAGE, NT>(P, tb, z, t, dt, &sv[0][0], &sfl[0][0], sn, out, cell,
+                                                   &times[tile.prob]);
+        lmin = r.x;
+        lmax = r.y;
       } else {
-#pragma unroll
-        for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
-      }
-      // zone geometry: closed form on the uniform maps (gcov[0][0] = gcon[0] = scale[0][0]
-      // = 1 there), the Romberg tables otherwise
-      double vol, g0 = 1.0, g1, g2, gc0 = 1.0, gc1, gc2, s00 = 1.0;
-      if (P.geo_tab) {
-        const int64_t gi = P.geo_off + z + NG;
-        const double *geo = tb.geo;
-        vol = __ldg(geo + GF_VOL * gs + gi);
-        g0 = __ldg(geo + GF_G0 * gs + gi); g1 = __ldg(geo + GF_G1 * gs + gi); g2 = __ldg(geo + GF_G2 * gs + gi);
-        gc0 = __ldg(geo + GF_GC0 * gs + gi); gc1 = __ldg(geo + GF_GC1 * gs + gi); gc2 = __ldg(geo + GF_GC2 * gs + gi);
-        s00 = __ldg(geo + GF_S00 * gs + gi);
-        if (P.has_src) {
-          geo_sources_1d(geo, gs, gi, P.sparse_conn != 0, ph, sv[5][t + 1], g0, g1, g2, src);
+        // the uniform maps: gcov[0][0] = gcon[0] = scale[0][0] = 1
+        double ph[NPRIM], pn[NPRIM], u[NPRIM], uh[NPRIM], src[NPRIM];
+  #pragma unroll
+        for (int v = 0; v < NPRIM; v++) ph[v] = sv[v][t + 1];
+        if (STAGE == 0) {
+  #pragma unroll
+          for (int v = 0; v < NPRIM; v++) pn[v] = ph[v];
         } else {
-#pragma unroll
-          for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
+  #pragma unroll
+          for (int v = 0; v < NPRIM; v++) pn[v] = sn.v[v][cell];
         }
-      } else {
         const ZoneGeo1 zg = zone_geom_1d(P, z);
-        vol = zg.vol; g1 = zg.g1; g2 = zg.g2; gc1 = zg.gc1; gc2 = zg.gc2;
         if (P.has_src) {
           geo_sources_closed(P, zg, ph, sv[5][t + 1], src);
         } else {
-#pragma unroll
+  #pragma unroll
           for (int v = 0; v < NPRIM; v++) src[v] = 0.0;
         }
-      }
-      if (P.grav_on) add_fixed_gravity(ph, P.grav, g0, g1, g2, 1, src);
-      if (P.mono) {
-        // monopole gravity (gravity.c:373-401) with the mass flux densities of the zone's
-        // FP64 face fluxes; such problems carry the Romberg tables (geo_tab)
-        const int64_t gi = P.geo_off + z + NG;
-        const double vr = sfl[RHO][t + 1] / (__ldg(tb.geo + GF_AREA * gs + gi + 1) + 1.0e-16);
-        const double vl = sfl[RHO][t] / (__ldg(tb.geo + GF_AREA * gs + gi) + 1.0e-16);
-        add_monopole_gravity(ph[RHO], tb.gmono[P.mono_off + z], vl, vr, P.x0 + z * P.dx0, P.dx0,
-                             __ldg(rc + RC_B0 * rcs + gi), __ldg(rc + RC_G0 * rcs + gi), src);
-      }
-      p_to_u(pn, u, g0, g1, g2);
-      p_to_u(ph, uh, g0, g1, g2);
-      lmin = dt_source_control_1div(pn, u, src);
-      const double ivol = 1.0 / vol;
-      const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
-#pragma unroll
-      for (int v = 0; v < NPRIM; v++) {
-        const double ddt = (sfl[v][t + 1] - sfl[v][t]) * ivol - src[v];
-        u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
-      }
-      // hydro_u_to_p (fluid.c:27-53) with one division
-      double pf[NPRIM];
-      const double irho = 1.0 / u[RHO];
-      const double w1 = u[U1] * irho, w2 = u[U2] * irho, w3 = u[U3] * irho;
-      pf[RHO] = u[RHO];
-      pf[U1] = gc0 * w1;
-      pf[U2] = gc1 * w2;
-      pf[U3] = gc2 * w3;
-      pf[UU] = u[UU] - 0.5 * pf[RHO] * (w1 * pf[U1] + w2 * pf[U2] + w3 * pf[U3]);
-      if (P.floors) {   // ENFORCE_FLOORS, fluid.c:43-46
-        pf[RHO] = fmax(pf[RHO], P.rho_floor);
-        pf[UU] = fmax(pf[UU], P.e_floor);
-      }
-#pragma unroll
-      for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
-      flag_nonfinite(pf, &times[tile.prob]);
-      if (STAGE == 1) {
-        // zone term of the next estimate_dt (step.c:177-187)
-        const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
-        lmax = (fabs(pf[U1]) + cs / s00) / P.dx0;
+        if (P.grav_on) add_fixed_gravity(ph, P.grav, 1.0, zg.g1, zg.g2, 1, src);
+        p_to_u(pn, u, 1.0, zg.g1, zg.g2);
+        p_to_u(ph, uh, 1.0, zg.g1, zg.g2);
+        lmin = dt_source_control_1div(pn, u, src);
+        const double ivol = 1.0 / zg.vol;
+        const double pfact = STAGE ? 0.5 : 1.0, phfact = STAGE ? 0.5 : 0.0, ffact = STAGE ? 0.5 : 1.0;
+  #pragma unroll
+        for (int v = 0; v < NPRIM; v++) {
+          const double ddt = (sfl[v][t + 1] - sfl[v][t]) * ivol - src[v];
+          u[v] = pfact * u[v] + phfact * uh[v] - ffact * dt * ddt;
+        }
+        // hydro_u_to_p (fluid.c:27-53) with one division
+        double pf[NPRIM];
+        const double irho = 1.0 / u[RHO];
+        const double w1 = u[U1] * irho, w2 = u[U2] * irho, w3 = u[U3] * irho;
+        pf[RHO] = u[RHO];
+        pf[U1] = w1;
+        pf[U2] = zg.gc1 * w2;
+        pf[U3] = zg.gc2 * w3;
+        pf[UU] = u[UU] - 0.5 * pf[RHO] * (w1 * pf[U1] + w2 * pf[U2] + w3 * pf[U3]);
+        if (P.floors) {   // ENFORCE_FLOORS, fluid.c:43-46
+          pf[RHO] = fmax(pf[RHO], P.rho_floor);
+          pf[UU] = fmax(pf[UU], P.e_floor);
+        }
+  #pragma unroll
+        for (int v = 0; v < NPRIM; v++) out.v[v][cell] = pf[v];
+        flag_nonfinite(pf, &times[tile.prob]);
+        if (STAGE == 1) {
+          // zone term of the next estimate_dt (step.c:177-187)
+          const double cs = sqrt(P.gam * sv[5][t + 1] / ph[RHO]);
+          lmax = (fabs(pf[U1]) + cs) / P.dx0;
+        }
       }
     }
     lmin = fmin(lmin, P.dx0 / (double)smax);
@@ -365,27 +419,36 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
   }
 }
 
-template <int NT>
+template <int NT, bool TAB>
 static void launch_mixed_nt(int stage, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
                             const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA sst, StateSoA sn,
                             StateSoA out, cudaStream_t st)
 {
   if (stage == 0)
-    stage1d_mixed_kernel<NT, 0><<<grid, NT, 0, st>>>(probs, times, tiles, q, use_queue, tb, sst, sn, out);
+    stage1d_mixed_kernel<NT, 0, TAB><<<grid, NT, 0, st>>>(probs, times, tiles, q, use_queue, tb, sst, sn, out);
   else
-    stage1d_mixed_kernel<NT, 1><<<grid, NT, 0, st>>>(probs, times, tiles, q, use_queue, tb, sst, sn, out);
+    stage1d_mixed_kernel<NT, 1, TAB><<<grid, NT, 0, st>>>(probs, times, tiles, q, use_queue, tb, sst, sn, out);
+}
+
+template <bool TAB>
+static void launch_mixed_tab(int stage, int nt, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
+                             const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA sst, StateSoA sn,
+                             StateSoA out, cudaStream_t st)
+{
+  switch (nt) {
+    case 64: launch_mixed_nt<64, TAB>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
+    case 256: launch_mixed_nt<256, TAB>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
+    default: launch_mixed_nt<128, TAB>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
+  }
 }
 
 void launch_stage1d_mixed(int stage, int nt, int grid, bool use_queue, const ProbDev *probs, ProbTime *times,
                           const Tile *tiles, WorkQueue *q, const Tables &tb, StateSoA sst, StateSoA sn,
-                          StateSoA out, cudaStream_t st)
+                          StateSoA out, cudaStream_t st, bool tab)
 {
   if (grid <= 0) return;
-  switch (nt) {
-    case 64: launch_mixed_nt<64>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
-    case 256: launch_mixed_nt<256>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
-    default: launch_mixed_nt<128>(stage, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st); break;
-  }
+  if (tab) launch_mixed_tab<true>(stage, nt, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st);
+  else launch_mixed_tab<false>(stage, nt, grid, use_queue, probs, times, tiles, q, tb, sst, sn, out, st);
 }
 
 int mixed_max_ctas_per_sm(int nt)
@@ -393,9 +456,9 @@ int mixed_max_ctas_per_sm(int nt)
   int n = 0;
   cudaError_t e;
   switch (nt) {
-    case 64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<64, 1>, 64, 0); break;
-    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<256, 1>, 256, 0); break;
-    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<128, 1>, 128, 0); break;
+    case 64: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<64, 1, false>, 64, 0); break;
+    case 256: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<256, 1, false>, 256, 0); break;
+    default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, stage1d_mixed_kernel<128, 1, false>, 128, 0); break;
   }
   return e == cudaSuccess ? n : 0;
 }

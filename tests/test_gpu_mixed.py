@@ -181,6 +181,24 @@ def test_mixed_batched_equals_alone():
         assert at[0] == bt[m]
 
 
+def test_mixed_closed_form_and_table_problems_batched_equal_alone():
+    """Problems whose geometry is evaluated in closed form and problems that read the
+    Romberg tables (SINH and LOG radii, SINH_MODIFIED + POLYTH) run in two launches per
+    stage with their own work queues: each result is the same alone and in the batch, in
+    persistent and one-CTA-per-tile mode."""
+    probs = [P.spherical_1d("sedov", 300, 1.4, p_ratio=1.0e4, r0=0.05),
+             P.spherical_1d("sedov", 256, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3),
+             P.sod(257),
+             P.spherical_1d("sedov", 160, 1.4, p_ratio=1.0e4, r0=0.02, coords="log", r_in=1.0e-3),
+             P.spherical_1d("sod", 200, 1.4, rho_ratio=10.0, p_ratio=100.0, dr_min=1.0e-3, coords="default")]
+    for cfg in (dict(), dict(ctas_per_sm=0)):
+        batched, bt = _run(probs, PREC_MIXED, 25, **cfg)
+        for m, pb in enumerate(probs):
+            alone, at = _run([pb], PREC_MIXED, 25, **cfg)
+            assert np.array_equal(alone[0], batched[m]), pb.name
+            assert at[0] == bt[m]
+
+
 @pytest.mark.parametrize("cfg", [dict(threads=64), dict(threads=256), dict(ctas_per_sm=2),
                                  dict(threads=64, ctas_per_sm=8), dict(steps_per_graph=0),
                                  dict(steps_per_graph=7)])
