@@ -212,20 +212,25 @@ int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
  *   ctas_per_sm      mixed 1-D sweep: 0 = one CTA per tile; k > 0 = k persistent CTAs
  *                    per SM that pull (problem, tile) items from a device work queue;
  *   steps_per_graph  steps captured in one CUDA graph and replayed by mdg_step
- *                    (0 = direct launches; timing enabled always launches directly).
+ *                    (0 = direct launches; timing enabled always launches directly);
+ *   run_length       dendritic (3-D and 2-D spherical) sweeps: radial and theta faces
+ *                    one thread walks per work item, 1..64 (default 16); the results do
+ *                    not depend on it.
  */
 typedef struct mdg_launch_config {
   int threads;
   int ctas_per_sm;
   int steps_per_graph;
+  int run_length;
 } mdg_launch_config;
 int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg);
 int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg);
 
-/* Time every admissible (threads, ctas_per_sm) of the mixed sweep over trial_steps
- * steps of the solver's own problems, keep the fastest and restore the state, times
- * and error flag as they were.  best/ms_per_step may be NULL.  MDG_ERR_NOTIMPL for FP64
- * solvers, whose shapes are fixed. */
+/* Time every admissible launch shape over trial_steps steps of the solver's own
+ * problems, keep the fastest and restore the state, times and error flag as they were:
+ * (threads, ctas_per_sm) of the batched 1-D mixed sweep, run_length (4, 8, 16, 32) of a
+ * dendritic-grid solver of either precision.  best/ms_per_step may be NULL.
+ * MDG_ERR_NOTIMPL for the FP64 1-D and 2-D Cartesian solvers, whose shapes are fixed. */
 int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double *ms_per_step);
 
 /* Conserved totals of every problem after all queued work: mass[m] = sum rho dV and

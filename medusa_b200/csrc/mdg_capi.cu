@@ -74,7 +74,7 @@ struct mdg_solver {
   int mtiles_cap = 0, nmtiles = 0;
   int nmtab = 0;                  // the last nmtab mixed tiles: problems reading the Romberg tables
   int num_sms = 0;
-  mdg_launch_config cfg{128, 0, 10};
+  mdg_launch_config cfg{128, 0, 10, 16};
   // CUDA graph of cfg.steps_per_graph steps (rebuilt when the launch shape changes)
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -965,8 +965,15 @@ int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
   if (cfg->ctas_per_sm < 0 || cfg->ctas_per_sm > 64) return fail(MDG_ERR_INVALID, "ctas_per_sm out of [0, 64]");
   if (cfg->steps_per_graph < 0 || cfg->steps_per_graph > 10000)
     return fail(MDG_ERR_INVALID, "steps_per_graph out of [0, 10000]");
+  if (cfg->run_length < 1 || cfg->run_length > 64) return fail(MDG_ERR_INVALID, "run_length out of [1, 64]");
   CK(cudaSetDevice(s->device));
   CK(cudaStreamSynchronize(s->stream));
+  if (s->ndim == 3 && cfg->run_length != s->cfg.run_length) {
+    std::string why;
+    const int rc = sweep3_set_run_length(s->s3, cfg->run_length, why);
+    if (rc != MDG_OK) return fail(rc, "run_length: " + why);
+    drop_graph(s);
+  }
   const bool reshape = cfg->threads != s->cfg.threads;
   const bool batched = s->precision == MDG_PREC_MIXED && s->ndim == 1;
   if (reshape && batched) {
@@ -986,8 +993,9 @@ int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double
 {
   if (!s) return fail(MDG_ERR_INVALID, "solver");
   if (trial_steps < 1) return fail(MDG_ERR_INVALID, "trial_steps < 1");
-  if (s->precision != MDG_PREC_MIXED || s->ndim != 1)
-    return fail(MDG_ERR_NOTIMPL, "only the batched 1-D mixed sweep has tunable launch shapes");
+  const bool dendritic = s->ndim == 3;
+  if (!dendritic && (s->precision != MDG_PREC_MIXED || s->ndim != 1))
+    return fail(MDG_ERR_NOTIMPL, "only the batched 1-D mixed sweep and the dendritic sweeps have tunable launch shapes");
   CK(cudaSetDevice(s->device));
   CK(cudaStreamSynchronize(s->stream));
   // the trials advance the state: keep a copy of everything a step changes
@@ -1019,15 +1027,23 @@ int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double
       rc = fail(MDG_ERR_CUDA, "autotune: set-up");
       break;
     }
-    const int threads[3] = {64, 128, 256};
-    const int ctas[9] = {0, 1, 2, 3, 4, 6, 8, 12, 16};
+    // candidate shapes: (threads, ctas_per_sm) of the mixed 1-D sweep, or the run length
+    // of a dendritic sweep
+    std::vector<mdg_launch_config> cand;
     const int k = orig.steps_per_graph;
+    if (dendritic) {
+      for (int len : {4, 8, 16, 32}) cand.push_back(mdg_launch_config{orig.threads, orig.ctas_per_sm, k, len});
+    } else {
+      for (int nt : {64, 128, 256}) {
+        const int occ = mixed_max_ctas_per_sm(nt);
+        for (int c : {0, 1, 2, 3, 4, 6, 8, 12, 16})
+          if (c <= occ) cand.push_back(mdg_launch_config{nt, c, k, orig.run_length});
+      }
+    }
     const int steps = (k > 0) ? ((trial_steps + k - 1) / k) * k : trial_steps;
-    for (int ti = 0; ti < 3 && rc == MDG_OK; ti++) {
-      const int occ = mixed_max_ctas_per_sm(threads[ti]);
-      for (int ci = 0; ci < 9 && rc == MDG_OK; ci++) {
-        if (ctas[ci] > occ) continue;
-        mdg_launch_config c{threads[ti], ctas[ci], k};
+    {
+      for (size_t ci = 0; ci < cand.size() && rc == MDG_OK; ci++) {
+        const mdg_launch_config c = cand[ci];
         if ((rc = mdg_set_launch_config(s, &c)) != MDG_OK) break;
         if ((rc = restore()) != MDG_OK) break;
         if ((rc = mdg_step(s, k > 0 ? k : 1)) != MDG_OK) break;   // warm-up (and graph capture)

@@ -86,6 +86,8 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why);
 void sweep3_destroy(Sweep3 *w);
 int64_t sweep3_ncell(const Sweep3 *w);
 int64_t sweep3_bytes(const Sweep3 *w);   // device memory of the grid tables, face fluxes and bits
+// Faces per work item of the radial and theta run kernels (1..64); rebuilds the work lists.
+int sweep3_set_run_length(Sweep3 *w, int run_length, std::string &why);
 void launch_stage3d(int stage, bool mixed, Sweep3 *w, const ProbDev *probs, ProbTime *times,
                     StateSoA stage_state, StateSoA state_n, StateSoA out, cudaStream_t st);
 void launch_initial_estimate3(Sweep3 *w, const ProbDev *probs, ProbTime *times, StateSoA s, cudaStream_t st);

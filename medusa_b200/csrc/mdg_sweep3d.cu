@@ -495,7 +495,7 @@ __device__ __forceinline__ bool flag_shock(const Grid3 &g, int i, int jj, int kc
 // A run of faces along one direction: faces r0 .. r0+nr-1 of the fixed row `row` (the
 // theta row j for direction 0, the radial row i for direction 1), columns k0 .. k0+cnt-1.
 struct Tile3R { int r0, nr, row, k0, cnt; };
-constexpr int RUN0 = 16;
+constexpr int RUN0 = 16;          // default faces per work item (mdg_launch_config::run_length)
 
 // The RK stage is a run-time argument here (not a template argument as in the other
 // face kernels): both stages then run the same code, which measured faster for stage 1
@@ -1163,6 +1163,11 @@ struct Sweep3 {
   unsigned char *d_bits = nullptr; // own0 | own1 | all0, one byte per zone each
   Tile3 *d_tiles = nullptr;        // face2 | zone tiles
   Tile3R *d_runs = nullptr;        // direction-0 face runs | direction-1 face runs
+  size_t runs_cap = 0;             // Tile3R entries d_runs holds
+  int run_len = RUN0;
+  // the row structure the run lists are cut from (a copy of the host grid's)
+  int n1 = 0, n2 = 0, n3 = 0;
+  std::vector<int> nj, rowbase, nk;
   double *d_gmono = nullptr;       // monopole gravity per radial row
   int nt[4] = {0, 0, 0, 0};
   int64_t ncell = 0;
@@ -1172,6 +1177,75 @@ struct Sweep3 {
 static void tiles_of_rows(std::vector<Tile3> &out, int i, int j, int count, int chunk = NT3)
 {
   for (int k0 = 0; k0 < count; k0 += chunk) out.push_back(Tile3{i, j, k0, (count - k0 < chunk) ? count - k0 : chunk});
+}
+
+// Work lists of the radial and theta run kernels for runs of at most run_len faces.
+static void build_runs(const Sweep3 &w, int run_len, std::vector<Tile3R> &t0, std::vector<Tile3R> &t1)
+{
+  auto njr = [&](int i) { return w.nj[i + NG]; };
+  auto row = [&](int i, int j) { return w.rowbase[i + NG] + j + NG; };
+  auto dj = [&](int i) { return w.n2 / w.nj[i + NG]; };
+  auto dk = [&](int i, int j) { return w.n3 / w.nk[row(i, j)]; };
+  t0.clear();
+  t1.clear();
+  // direction-0 runs: faces i in [0, n1] grouped by constant theta resolution, then per
+  // theta row j by constant phi resolution, cut into run_len faces and NT3 phi columns
+  for (int i = 0; i <= w.n1;) {
+    int ie = i + 1;
+    while (ie <= w.n1 && dj(ie) == dj(i)) ie++;
+    for (int j = 0; j < njr(i); j++) {
+      for (int a = i; a < ie;) {
+        int b = a + 1;
+        while (b < ie && dk(b, j) == dk(a, j)) b++;
+        const int nk = w.nk[row(a, j)];
+        for (int c = a; c < b; c += run_len)
+          for (int k0 = 0; k0 < nk; k0 += NT3)
+            t0.push_back(Tile3R{c, std::min(run_len, b - c), j, k0, std::min(NT3, nk - k0)});
+        a = b;
+      }
+    }
+    i = ie;
+  }
+  // direction-1 runs: faces j in [0, nj(i)] of radial row i grouped by constant phi
+  // resolution of the face, min(dk(i, j), dk(i, j-1)), cut into run_len faces and NT3 columns
+  for (int i = 0; i < w.n1; i++) {
+    const int nj = njr(i);
+    auto mn = [&](int j) { return std::min(dk(i, j), dk(i, j - 1)); };
+    for (int a = 0; a <= nj;) {
+      int b = a + 1;
+      while (b <= nj && mn(b) == mn(a)) b++;
+      const int cnt = w.n3 / mn(a);
+      for (int c = a; c < b; c += run_len)
+        for (int k0 = 0; k0 < cnt; k0 += NT3)
+          t1.push_back(Tile3R{c, std::min(run_len, b - c), i, k0, std::min(NT3, cnt - k0)});
+      a = b;
+    }
+  }
+}
+
+int sweep3_set_run_length(Sweep3 *w, int run_length, std::string &why)
+{
+  if (run_length < 1 || run_length > 64) { why = "run_length out of [1, 64]"; return MDG_ERR_INVALID; }
+  if (run_length == w->run_len) return MDG_OK;
+  std::vector<Tile3R> t0, t1;
+  build_runs(*w, run_length, t0, t1);
+  const int n0 = (int)t0.size(), n1 = (int)t1.size();
+  t0.insert(t0.end(), t1.begin(), t1.end());
+  cudaError_t e = cudaSuccess;
+  if (t0.size() > w->runs_cap) {
+    Tile3R *d = nullptr;
+    e = cudaMalloc(&d, sizeof(Tile3R) * t0.size());
+    if (e != cudaSuccess) { why = cudaGetErrorString(e); return MDG_ERR_OUTOFMEM; }
+    cudaFree(w->d_runs);
+    w->d_runs = d;
+    w->runs_cap = t0.size();
+  }
+  e = cudaMemcpy(w->d_runs, t0.data(), sizeof(Tile3R) * t0.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { why = cudaGetErrorString(e); return MDG_ERR_CUDA; }
+  w->nt[0] = n0;
+  w->nt[1] = n1;
+  w->run_len = run_length;
+  return MDG_OK;
 }
 
 int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
@@ -1278,39 +1352,9 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   // tiles of each kernel
   std::vector<Tile3> t2, tc;
   std::vector<Tile3R> t0, t1;
-  // direction-0 runs: faces i in [0, n1] grouped by constant theta resolution, then per
-  // theta row j by constant phi resolution, cut into RUN0 faces and NT3 phi columns
-  for (int i = 0; i <= h.n1;) {
-    int ie = i + 1;
-    while (ie <= h.n1 && h.dj(ie) == h.dj(i)) ie++;
-    for (int j = 0; j < h.njr(i); j++) {
-      for (int a = i; a < ie;) {
-        int b = a + 1;
-        while (b < ie && h.dk(b, j) == h.dk(a, j)) b++;
-        const int nk = h.nk[h.row(a, j)];
-        for (int c = a; c < b; c += RUN0)
-          for (int k0 = 0; k0 < nk; k0 += NT3)
-            t0.push_back(Tile3R{c, std::min(RUN0, b - c), j, k0, std::min(NT3, nk - k0)});
-        a = b;
-      }
-    }
-    i = ie;
-  }
-  // direction-1 runs: faces j in [0, nj(i)] of radial row i grouped by constant phi
-  // resolution of the face, min(dk(i, j), dk(i, j-1)), cut into RUN0 faces and NT3 columns
-  for (int i = 0; i < h.n1; i++) {
-    const int nj = h.njr(i);
-    auto mn = [&](int j) { return std::min(h.dk(i, j), h.dk(i, j - 1)); };
-    for (int a = 0; a <= nj;) {
-      int b = a + 1;
-      while (b <= nj && mn(b) == mn(a)) b++;
-      const int cnt = h.n3 / mn(a);
-      for (int c = a; c < b; c += RUN0)
-        for (int k0 = 0; k0 < cnt; k0 += NT3)
-          t1.push_back(Tile3R{c, std::min(RUN0, b - c), i, k0, std::min(NT3, cnt - k0)});
-      a = b;
-    }
-  }
+  w->n1 = h.n1; w->n2 = h.n2; w->n3 = h.n3;
+  w->nj = h.nj; w->rowbase = h.rowbase; w->nk = h.nk;
+  build_runs(*w, RUN0, t0, t1);
   for (int i = 0; i < h.n1 && h.ndim == 3; i++)
     for (int j = 0; j < h.njr(i); j++) tiles_of_rows(t2, i, j, h.nk[h.row(i, j)] + 1, T2);
   for (int i = 0; i < h.n1; i++)
@@ -1326,6 +1370,7 @@ int sweep3_create(const mdg_problem_desc &d, Sweep3 **out, std::string &why)
   t0.insert(t0.end(), t1.begin(), t1.end());
   e = cudaMalloc(&w->d_runs, sizeof(Tile3R) * t0.size());
   if (e != cudaSuccess) return fail3(e);
+  w->runs_cap = t0.size();
   e = cudaMemcpy(w->d_runs, t0.data(), sizeof(Tile3R) * t0.size(), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail3(e);
   *out = w;

@@ -243,7 +243,8 @@ def test_autotune_rejected_for_fp64():
 
 def test_launch_config_validation():
     with Solver(P.sod(64), precision=PREC_MIXED) as s:
-        for bad in (dict(threads=96), dict(ctas_per_sm=-1), dict(steps_per_graph=-3)):
+        for bad in (dict(threads=96), dict(ctas_per_sm=-1), dict(steps_per_graph=-3), dict(run_length=0),
+                    dict(run_length=65)):
             with pytest.raises(MdgError) as e:
                 s.set_launch_config(**bad)
             assert e.value.code == 1

@@ -16,7 +16,7 @@ import numpy as np
 import pytest
 
 from medusa_b200 import problems as P
-from medusa_b200.solver import Solver
+from medusa_b200.solver import PREC_FP64, PREC_MIXED, Solver
 from tests._cases import golden_cases3d, load_golden, pointwise_rel_err, record, zone_gcov
 
 pytestmark = pytest.mark.gpu
@@ -210,3 +210,29 @@ def test_c3_full_size_invariants():
     assert drift <= 1.0e-13
     assert vphi <= 1.0e-10
     assert max(asym) <= 1.0e-10
+
+
+@pytest.mark.parametrize("precision", [PREC_FP64, PREC_MIXED])
+def test_3d_run_length_does_not_change_results(precision):
+    """The radial and theta run kernels give the same bits for every run length (each
+    face's pencil entries and reconstructions are the same whichever work item computes
+    them); the autotuner picks a run length and leaves the state as it was."""
+    pb = P.sedov_3d(24, 16, 32, r_dep=0.2, noise=0.05, dr_min=0.02)
+    out = {}
+    for run in (1, 3, 16, 64):
+        with Solver(pb, precision=precision) as s:
+            s.set_launch_config(run_length=run)
+            assert s.launch_config()["run_length"] == run
+            s.step(12)
+            out[run] = (s.update_cpu(0), s.time(0))
+    for run in (1, 3, 64):
+        assert np.array_equal(out[run][0], out[16][0])
+        assert out[run][1] == out[16][1]
+    with Solver(pb, precision=precision) as s:
+        s.step(4)
+        cfg, ms = s.autotune(trial_steps=2)
+        assert cfg["run_length"] in (4, 8, 16, 32) and ms > 0
+        assert s.launch_config()["run_length"] == cfg["run_length"]
+        s.step(8)
+        assert np.array_equal(s.update_cpu(0), out[16][0])
+        assert s.time(0) == out[16][1]
