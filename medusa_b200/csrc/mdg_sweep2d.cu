@@ -39,7 +39,9 @@
 // The per-variable reconstruction loops are not unrolled here (one inlined copy of
 // para_recon per loop): 7.5 % faster on the 2048^2 Kelvin-Helmholtz grid on a B200 than
 // unrolled, and faster than an out-of-line call there (same results).
+#ifndef MDG_RECON_UNROLL
 #define MDG_RECON_UNROLL 1
+#endif
 #include "mdg_hydro.cuh"
 #include "mdg_kernels.cuh"
 #include "mdg_mixed.cuh"
