@@ -178,6 +178,20 @@ int mdg_download_state(mdg_solver *s, int prob, double *prim, double *eos);
  * step and the step count. */
 int mdg_get_time(mdg_solver *s, int prob, double *t, double *dt_last, int *istep);
 
+/* Checkpoint / resume (the reference's restart_dump_v2 / restart_read_v2, io.c:3237-3583,
+ * 4318-4936, whose files are HDF5; these are a flat binary file of the same content for
+ * the hydro state: a 48-byte header -- "MDGRST1\0", int32 ndim, n1, n2, n3, istep, 0,
+ * int64 zone count, double t -- then the zones' 5 primitives in sim_p's [zone][var]
+ * order).  mdg_set_time gives problem `prob` the time record of a run resumed from a
+ * restart: Time and Step of the file and, as a new reference process has, no step of its
+ * own yet (dtold = 1e100, main.c:194, so the first step's dt is not limited by the
+ * growth factor); call it after mdg_upload_state, whose state the first estimate_dt of
+ * the resumed run uses (step.c:171-174).  mdg_restart_read checks that the file belongs
+ * to the problem's grid (MDG_ERR_INVALID otherwise) and does both. */
+int mdg_set_time(mdg_solver *s, int prob, double t, int istep);
+int mdg_restart_write(mdg_solver *s, int prob, const char *path);
+int mdg_restart_read(mdg_solver *s, int prob, const char *path);
+
 /* The CUDA stream all work of this solver is queued on (a cudaStream_t). */
 int mdg_get_stream(mdg_solver *s, void **stream);
 

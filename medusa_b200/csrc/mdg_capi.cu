@@ -1244,6 +1244,88 @@ int mdg_get_time(mdg_solver *s, int prob, double *t, double *dt_last, int *istep
   return MDG_OK;
 }
 
+int mdg_set_time(mdg_solver *s, int prob, double t, int istep)
+{
+  if (!s) return fail(MDG_ERR_INVALID, "solver");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  if (!std::isfinite(t) || istep < 0) return fail(MDG_ERR_INVALID, "t must be finite and istep >= 0");
+  CK(cudaSetDevice(s->device));
+  ProbTime T;
+  CK(cudaMemcpyAsync(&T, s->d_times + prob, sizeof(ProbTime), cudaMemcpyDeviceToHost, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  // the record a run resumed from a restart starts with: Time and Step of the file, no
+  // step of this process yet (dtold = 1e100, main.c:194); the running min_dt holds the
+  // zone terms of the uploaded state (estimate_dt's first call, step.c:171-174)
+  T.t = t;
+  T.istep = istep;
+  T.dt = 0.0;
+  T.dtold = 1.0e100;
+  T.t_bc1 = 0.0;
+  T.t_next = 0.0;
+  T.dt_ready = 0;
+  T.done = 0;
+  CK(cudaMemcpyAsync(s->d_times + prob, &T, sizeof(ProbTime), cudaMemcpyHostToDevice, s->stream));
+  CK(cudaStreamSynchronize(s->stream));
+  return MDG_OK;
+}
+
+namespace {
+// restart file: this header, then ncell x 5 doubles in the [zone][var] order of sim_p
+struct RestartHeader {
+  char magic[8];       // "MDGRST1" and a NUL
+  int32_t ndim, n1, n2, n3;
+  int32_t istep, reserved;
+  int64_t ncell;
+  double t;
+};
+const char kRestartMagic[8] = {'M', 'D', 'G', 'R', 'S', 'T', '1', '\0'};
+}  // namespace
+
+int mdg_restart_write(mdg_solver *s, int prob, const char *path)
+{
+  if (!s || !path) return fail(MDG_ERR_INVALID, "solver/path");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  const mdg_problem_desc &d = s->descs[prob];
+  const int64_t n = s->hprobs[prob].ncell;
+  std::vector<double> prim((size_t)NPRIM * n);
+  int rc = mdg_download_state(s, prob, prim.data(), nullptr);
+  if (rc != MDG_OK) return rc;
+  RestartHeader h{};
+  std::memcpy(h.magic, kRestartMagic, 8);
+  h.ndim = d.ndim; h.n1 = d.n1; h.n2 = d.ndim > 1 ? d.n2 : 1; h.n3 = d.ndim > 2 ? d.n3 : 1;
+  h.ncell = n;
+  rc = mdg_get_time(s, prob, &h.t, nullptr, &h.istep);
+  if (rc != MDG_OK) return rc;
+  FILE *f = std::fopen(path, "wb");
+  if (!f) return fail(MDG_ERR_IO, std::string("cannot open ") + path);
+  const bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 &&
+                  std::fwrite(prim.data(), sizeof(double), prim.size(), f) == prim.size();
+  if (std::fclose(f) != 0 || !ok) return fail(MDG_ERR_IO, std::string("cannot write ") + path);
+  return MDG_OK;
+}
+
+int mdg_restart_read(mdg_solver *s, int prob, const char *path)
+{
+  if (!s || !path) return fail(MDG_ERR_INVALID, "solver/path");
+  if (prob < 0 || prob >= s->nprob) return fail(MDG_ERR_INDEX, "problem index out of range");
+  const mdg_problem_desc &d = s->descs[prob];
+  const int64_t n = s->hprobs[prob].ncell;
+  FILE *f = std::fopen(path, "rb");
+  if (!f) return fail(MDG_ERR_IO, std::string("cannot open ") + path);
+  RestartHeader h{};
+  std::vector<double> prim((size_t)NPRIM * n);
+  bool ok = std::fread(&h, sizeof h, 1, f) == 1;
+  const bool same = ok && std::memcmp(h.magic, kRestartMagic, 8) == 0 && h.ndim == d.ndim && h.n1 == d.n1 &&
+                    h.n2 == (d.ndim > 1 ? d.n2 : 1) && h.n3 == (d.ndim > 2 ? d.n3 : 1) && h.ncell == n;
+  if (same) ok = std::fread(prim.data(), sizeof(double), prim.size(), f) == prim.size();
+  std::fclose(f);
+  if (!ok) return fail(MDG_ERR_IO, std::string("cannot read ") + path);
+  if (!same) return fail(MDG_ERR_INVALID, std::string(path) + ": not a restart file of this problem's grid");
+  int rc = mdg_upload_state(s, prob, prim.data());
+  if (rc != MDG_OK) return rc;
+  return mdg_set_time(s, prob, h.t, h.istep);
+}
+
 int mdg_get_stream(mdg_solver *s, void **stream)
 {
   if (!s || !stream) return fail(MDG_ERR_INVALID, "solver/stream");

@@ -134,6 +134,9 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_download_state.argtypes = [vp, i, vp, vp]
     L.mdg_get_time.argtypes = [vp, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(i)]
     L.mdg_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    L.mdg_set_time.argtypes = [vp, i, d, i]
+    L.mdg_restart_write.argtypes = [vp, i, ctypes.c_char_p]
+    L.mdg_restart_read.argtypes = [vp, i, ctypes.c_char_p]
     L.mdg_synchronize.argtypes = [vp]
     L.mdg_destroy.argtypes = [vp]
     L.mdg_error_string.restype = ctypes.c_char_p
@@ -437,6 +440,18 @@ class Solver:
         ms = ctypes.c_double()
         _check(library().mdg_autotune(self._h, int(trial_steps), ctypes.byref(c), ctypes.byref(ms)), "mdg_autotune")
         return c.as_dict(), ms.value
+
+    def set_time(self, m: int, t: float, istep: int):
+        """The time record of a run resumed from a restart (mdg_set_time)."""
+        _check(library().mdg_set_time(self._h, int(m), float(t), int(istep)), "mdg_set_time")
+
+    def restart_write(self, path: str, m: int = 0):
+        """Write problem m's restart file (state, t, step count)."""
+        _check(library().mdg_restart_write(self._h, int(m), os.fsencode(path)), "mdg_restart_write")
+
+    def restart_read(self, path: str, m: int = 0):
+        """Resume problem m from a restart file."""
+        _check(library().mdg_restart_read(self._h, int(m), os.fsencode(path)), "mdg_restart_read")
 
     def conserved_totals(self):
         """(mass, energy) arrays over the problems, compensated FP64 sums on the device."""

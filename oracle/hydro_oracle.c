@@ -1075,6 +1075,19 @@ void orc_set_interior(orc_t *o, const double *prim)
   }
 }
 
+/* A run resumed from a restart file (io.c restart_read_v2: the state, Time and Step) in a
+ * new process: the EOS records of the state (main.c:180-182), dtold = 1e100 (main.c:194)
+ * and estimate_dt's first-call reset of min_dt (step.c:171-174). */
+void orc_restart(orc_t *o, const double *prim, double t, int istep)
+{
+  orc_set_interior(o, prim);
+  update_eos(o, o->p, 0);
+  o->t = t;
+  o->istep = istep;
+  o->dtold = 1.0e100;
+  o->est_first = 1;
+}
+
 void orc_get_moments0(const orc_t *o, double *a, double *b, double *g)
 {
   for (int i=0; i<o->s1; i++) { a[i] = o->alpha0[i]; b[i] = o->beta0[i]; g[i] = o->Gamma0[i]; }

@@ -107,6 +107,7 @@ def lib():
         L.orc_get_istep.argtypes = [ctypes.c_void_p]
         L.orc_get_interior.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.orc_set_interior.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_restart.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.orc_get_moments0.argtypes = [ctypes.c_void_p] * 4
         L.orc_get_geom.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
         _lib = L
@@ -157,6 +158,12 @@ class Oracle:
     def set_state(self, prim):
         prim = np.ascontiguousarray(prim, dtype=np.float64)
         lib().orc_set_interior(self._h, prim.ctypes.data)
+
+    def restart(self, prim, t: float, istep: int):
+        """Resume from a restart (state, time, step) as a new reference process does:
+        EOS of the state, dtold = 1e100, estimate_dt's first-call reset."""
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        lib().orc_restart(self._h, prim.ctypes.data, float(t), int(istep))
 
     def moments0(self):
         n = self.pb.n[0] + 4

@@ -92,6 +92,9 @@ def test_launch_config_calls_reject_null_solver():
     assert L.mdg_set_launch_config(None, ctypes.byref(c)) == 1
     assert L.mdg_autotune(None, 3, None, None) == 1
     assert L.mdg_conserved_totals(None, None, None) == 1
+    assert L.mdg_set_time(None, 0, 0.0, 0) == 1
+    assert L.mdg_restart_write(None, 0, b"x") == 1
+    assert L.mdg_restart_read(None, 0, b"x") == 1
 
 
 @pytest.mark.parametrize("field,value", [("precision", 7), ("max_problems", 0), ("max_zones", 2),

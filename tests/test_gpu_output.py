@@ -78,3 +78,69 @@ def test_snapshot_3d_and_errors():
         with pytest.raises(MdgError) as e:
             s.snapshot_write_ascii1("/dev/null")
         assert e.value.code == 5
+
+
+def _restart_against_oracle(pb, n_before, n_after, tmp_path):
+    """Run n_before steps, write a restart file, resume it in a new solver for n_after
+    steps; the oracle does the same through its restart (a new reference process reading
+    the file: the state's EOS, dtold = 1e100, estimate_dt's first-call reset)."""
+    path = str(tmp_path / "restart.bin")
+    with Solver(pb) as s:
+        s.step(n_before)
+        s.synchronize()
+        saved = s.update_cpu(0)
+        t0, _, ist0 = s.time(0)
+        s.restart_write(path, 0)
+    raw = np.fromfile(path, dtype=np.uint8)
+    assert raw[:8].tobytes() == b"MDGRST1\x00"
+    hdr = np.frombuffer(raw[:48].tobytes(), dtype=np.dtype([("m", "S8"), ("ndim", "<i4"), ("n1", "<i4"),
+                                                          ("n2", "<i4"), ("n3", "<i4"), ("istep", "<i4"),
+                                                          ("res", "<i4"), ("ncell", "<i8"), ("t", "<f8")]))[0]
+    assert hdr["istep"] == ist0 and hdr["t"] == t0 and hdr["ncell"] == saved.shape[0]
+    assert np.array_equal(np.frombuffer(raw[48:].tobytes(), dtype="<f8").reshape(-1, 5), saved)
+    with Solver(pb) as s:
+        s.restart_read(path, 0)
+        t1, _, ist1 = s.time(0)
+        assert t1 == t0 and ist1 == ist0
+        s.step(n_after)
+        s.synchronize()
+        got = s.update_cpu(0)
+        tg, _, istg = s.time(0)
+    return saved, t0, got, tg, istg
+
+
+@pytest.mark.parametrize("pb", [P.spherical_1d("sedov", 200, 1.4, p_ratio=1.0e4, r0=0.05),
+                                P.kelvin_helmholtz(48, 40, seed=2)], ids=["sph_sedov", "kh"])
+def test_restart_resumes_as_the_reference_does(pb, tmp_path):
+    from tests._cases import pointwise_rel_err
+    saved, t0, got, tg, istg = _restart_against_oracle(pb, 30, 20, tmp_path)
+    o = pyoracle.Oracle(pb)
+    o.advance(30)
+    ostate, _ = o.state()
+    assert pointwise_rel_err(saved, ostate, pb) <= 1.0e-9
+    o2 = pyoracle.Oracle(pb)
+    o2.restart(saved, t0, 30)
+    o2.advance(20)
+    ref, _ = o2.state()
+    assert istg == 50
+    assert abs(tg - o2.t) <= 1.0e-12 * o2.t
+    assert pointwise_rel_err(got, ref, pb) <= 1.0e-9
+
+
+def test_restart_of_a_dendritic_grid_and_wrong_file(tmp_path):
+    """3-D dendritic: resuming from the file equals uploading the saved state and setting
+    the time record by hand, bit for bit; a file of another grid is refused."""
+    pb = P.sedov_3d(16, 8, 16, r_dep=0.25, noise=0.05)
+    saved, t0, got, tg, istg = _restart_against_oracle(pb, 10, 6, tmp_path)
+    with Solver(pb) as s:
+        s.upload(0, saved)
+        s.set_time(0, t0, 10)
+        s.step(6)
+        s.synchronize()
+        by_hand = s.update_cpu(0)
+        assert s.time(0)[0] == tg
+    assert np.array_equal(got, by_hand)
+    with Solver(P.sedov_3d(16, 8, 32, r_dep=0.25)) as s:
+        with pytest.raises(MdgError) as e:
+            s.restart_read(str(tmp_path / "restart.bin"), 0)
+        assert e.value.code == 1
