@@ -177,7 +177,10 @@ struct mdg_server {
   int tiles2_cap = 0, ntx2 = 0, nty2 = 0;
   // 2-D lane; 3-D lane: resident dendritic requests spread over NS3 streams, so that
   // several grids (each too small to fill the GPU alone) run side by side
-  static constexpr int NS3 = 4;
+#ifndef MDG_SERVER_NS3
+#define MDG_SERVER_NS3 4
+#endif
+  static constexpr int NS3 = MDG_SERVER_NS3;
   cudaStream_t stream2 = nullptr, stream3[NS3] = {};
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join3[NS3] = {};
   int graph_ntx2 = -1, graph_nty2 = -1;   // 2-D tile counts the graph was captured with
