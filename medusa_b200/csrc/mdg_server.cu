@@ -178,7 +178,7 @@ struct mdg_server {
   // 2-D lane; 3-D lane: resident dendritic requests spread over NS3 streams, so that
   // several grids (each too small to fill the GPU alone) run side by side
 #ifndef MDG_SERVER_NS3
-#define MDG_SERVER_NS3 4
+#define MDG_SERVER_NS3 32
 #endif
   static constexpr int NS3 = MDG_SERVER_NS3;
   cudaStream_t stream2 = nullptr, stream3[NS3] = {};
