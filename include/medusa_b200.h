@@ -229,21 +229,28 @@ int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
  *                    (0 = direct launches; timing enabled always launches directly);
  *   run_length       dendritic (3-D and 2-D spherical) sweeps: radial and theta faces
  *                    one thread walks per work item, 1..64 (default 16); the results do
- *                    not depend on it.
+ *                    not depend on it;
+ *   lanes            mixed 1-D sweep: the problems split into 1..4 groups of about equal
+ *                    zone count, each group's steps queued on a stream of its own, so that
+ *                    one group's short kernels and kernel tails overlap another's stage
+ *                    kernels (default 1); the results do not depend on it.
  */
+#define MDG_MAX_LANES 4
 typedef struct mdg_launch_config {
   int threads;
   int ctas_per_sm;
   int steps_per_graph;
   int run_length;
+  int lanes;
 } mdg_launch_config;
 int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg);
 int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg);
 
 /* Time every admissible launch shape over trial_steps steps of the solver's own
  * problems, keep the fastest and restore the state, times and error flag as they were:
- * (threads, ctas_per_sm) of the batched 1-D mixed sweep, run_length (4, 8, 16, 32) of a
- * dendritic-grid solver of either precision.  best/ms_per_step may be NULL.
+ * (threads, ctas_per_sm) of the batched 1-D mixed sweep and then its lanes (1, 2, 4) with
+ * the best of those, run_length (4, 8, 16, 32) of a dendritic-grid solver of either
+ * precision.  best/ms_per_step may be NULL.
  * MDG_ERR_NOTIMPL for the FP64 1-D and 2-D Cartesian solvers, whose shapes are fixed. */
 int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double *ms_per_step);
 

@@ -72,9 +72,18 @@ struct mdg_solver {
   WorkQueue *d_queue = nullptr;
   Tile *d_mtiles = nullptr;
   int mtiles_cap = 0, nmtiles = 0;
-  int nmtab = 0;                  // the last nmtab mixed tiles: problems reading the Romberg tables
+  int nmtab = 0;                  // mixed tiles of problems reading the Romberg tables (all lanes)
+  // mixed 1-D sweep in lanes (mdg_launch_config::lanes): lane l advances problems
+  // [m0, m1), whose tiles are d_mtiles[t0, t0+ntu) (closed-form geometry, queue 2l) and
+  // [t0+ntu, t0+ntu+ntt) (Romberg tables, queue 2l+1); lane 0 runs on `stream`
+  struct Lane { int m0 = 0, m1 = 0, t0 = 0, ntu = 0, ntt = 0; };
+  Lane lane[MDG_MAX_LANES];
+  int nlanes = 1;
+  cudaStream_t lane_st[MDG_MAX_LANES] = {};
+  cudaEvent_t lane_ev[MDG_MAX_LANES] = {};
+  cudaEvent_t ev_fork = nullptr;
   int num_sms = 0;
-  mdg_launch_config cfg{128, 0, 10, 16};
+  mdg_launch_config cfg{128, 0, 10, 16, 1};
   // CUDA graph of cfg.steps_per_graph steps (rebuilt when the launch shape changes)
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -233,21 +242,42 @@ int mdg::validate_desc(const mdg_problem_desc &d, int ndim0, std::string &why)
   return MDG_OK;
 }
 
-// Tile list of the mixed sweep for nt threads per CTA (tiles of nt-2 zones): the tiles of
+// Tile list of the mixed sweep for nt threads per CTA (tiles of nt-2 zones) in `lanes`
+// lanes (contiguous problem ranges of about equal zone count): per lane the tiles of
 // problems with closed-form geometry, then those of problems reading the Romberg tables
 // (each part has its own launch and work queue).  Caller has synchronized the solver's
 // stream.
-static int build_mixed_tiles(mdg_solver *s, int nt)
+static int build_mixed_tiles(mdg_solver *s, int nt, int lanes)
 {
   const int tl = nt - 2;
   std::vector<Tile> t;
-  for (int pass = 0; pass < 2; pass++)
-    for (int m = 0; m < s->nprob; m++)
-      if ((s->hprobs[m].geo_tab != 0) == (pass == 1))
-        for (int i0 = 0; i0 < s->hprobs[m].n1; i0 += tl) t.push_back(Tile{m, i0, 0, 0});
   int ntab = 0;
-  for (int m = 0; m < s->nprob; m++)
-    if (s->hprobs[m].geo_tab) ntab += (s->hprobs[m].n1 + tl - 1) / tl;
+  // lane boundaries: cut the problem list where the running zone count passes l/lanes
+  int64_t total = 0, run = 0;
+  for (int m = 0; m < s->nprob; m++) total += s->hprobs[m].n1;
+  int nl = 0, m0 = 0;
+  for (int m = 0; m <= s->nprob && nl < lanes; m++) {
+    const bool last = (nl == lanes - 1);
+    if (m == s->nprob || (!last && m > m0 && run * lanes >= total * (nl + 1))) {
+      if (m == m0) break;
+      mdg_solver::Lane &L = s->lane[nl];
+      L.m0 = m0;
+      L.m1 = m;
+      L.t0 = (int)t.size();
+      for (int pass = 0; pass < 2; pass++) {
+        for (int q = m0; q < m; q++)
+          if ((s->hprobs[q].geo_tab != 0) == (pass == 1))
+            for (int i0 = 0; i0 < s->hprobs[q].n1; i0 += tl) t.push_back(Tile{q, i0, 0, 0});
+        (pass == 0 ? L.ntu : L.ntt) = (int)t.size() - L.t0 - (pass == 0 ? 0 : L.ntu);
+      }
+      ntab += L.ntt;
+      nl++;
+      m0 = m;
+      if (m == s->nprob) break;
+    }
+    if (m < s->nprob) run += s->hprobs[m].n1;
+  }
+  s->nlanes = nl;
   if ((int)t.size() > s->mtiles_cap) {
     cudaFree(s->d_mtiles);
     s->d_mtiles = nullptr;
@@ -259,8 +289,20 @@ static int build_mixed_tiles(mdg_solver *s, int nt)
   CK(cudaMemcpy(s->d_mtiles, t.data(), sizeof(Tile) * t.size(), cudaMemcpyHostToDevice));
   s->nmtiles = (int)t.size();
   s->nmtab = ntab;
-  const WorkQueue q[2] = {{{0u, 0u}, s->nmtiles - ntab, 0}, {{0u, 0u}, ntab, 0}};
+  WorkQueue q[2 * MDG_MAX_LANES] = {};
+  for (int l = 0; l < s->nlanes; l++) {
+    q[2 * l].ntiles = s->lane[l].ntu;
+    q[2 * l + 1].ntiles = s->lane[l].ntt;
+  }
   CK(cudaMemcpy(s->d_queue, q, sizeof q, cudaMemcpyHostToDevice));
+  // streams and events of the extra lanes, created once
+  if (s->nlanes > 1 && !s->ev_fork) {
+    CK(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+    for (int l = 1; l < MDG_MAX_LANES; l++) {
+      CK(cudaStreamCreateWithFlags(&s->lane_st[l], cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&s->lane_ev[l], cudaEventDisableTiming));
+    }
+  }
   return MDG_OK;
 }
 
@@ -321,6 +363,11 @@ static void free_all(mdg_solver *s)
   if (s->ev_snap_done) cudaEventDestroy(s->ev_snap_done);
   if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
   if (s->graph) cudaGraphExecDestroy(s->graph);
+  for (int l = 0; l < MDG_MAX_LANES; l++) {
+    if (s->lane_ev[l]) cudaEventDestroy(s->lane_ev[l]);
+    if (s->lane_st[l]) cudaStreamDestroy(s->lane_st[l]);
+  }
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->stream) cudaStreamDestroy(s->stream);
 }
 
@@ -586,8 +633,8 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   CKC(cudaMalloc(&s->d_stage, sizeof(double) * NPRIM * s->max_cells));
   CKC(cudaMalloc(&s->d_err, sizeof(int)));
   CKC(cudaMalloc(&s->d_totals, sizeof(double) * 2 * nprob));
-  CKC(cudaMalloc(&s->d_queue, 2 * sizeof(WorkQueue)));
-  CKC(cudaMemset(s->d_queue, 0, 2 * sizeof(WorkQueue)));
+  CKC(cudaMalloc(&s->d_queue, 2 * MDG_MAX_LANES * sizeof(WorkQueue)));
+  CKC(cudaMemset(s->d_queue, 0, 2 * MDG_MAX_LANES * sizeof(WorkQueue)));
   if (precision == MDG_PREC_MIXED) CKC(cudaMalloc(&s->d_mx, sizeof(float) * MX_NFIELDS * rc0));
   if (precision == MDG_PREC_MIXED && ndim == 2) {
     CKC(cudaMalloc(&s->d_mx1, sizeof(float) * MX_NFIELDS * rc1));
@@ -651,7 +698,7 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
   }
 #undef CKC
   if (precision == MDG_PREC_MIXED && ndim == 1) {
-    int rc = build_mixed_tiles(s, s->cfg.threads);
+    int rc = build_mixed_tiles(s, s->cfg.threads, s->cfg.lanes);
     if (rc != MDG_OK) { free_all(s); delete s; return rc; }
   }
   *out = s;
@@ -722,9 +769,41 @@ static int queue_steps(mdg_solver *s, int nsteps)
   const bool mix3 = s->ndim == 3 && s->precision == MDG_PREC_MIXED;
   const bool mix2 = s->ndim == 2 && s->precision == MDG_PREC_MIXED;
   const bool mixed = s->ndim == 1 && s->precision == MDG_PREC_MIXED;   // the batched 1-D mixed sweep
-  const int nmu = s->nmtiles - s->nmtab;
-  const int mgrid = mixed ? mixed_grid(s, nmu) : 0, mgrid_tab = mixed ? mixed_grid(s, s->nmtab) : 0;
   const bool queue = s->cfg.ctas_per_sm > 0;
+  // the mixed stage launches of every lane (each lane's two tile lists), on stream st
+  auto mixed_stage = [&](int stage, int l, cudaStream_t st) {
+    const mdg_solver::Lane &L = s->lane[l];
+    const StateSoA sst = stage ? s->PH : s->P, out = stage ? s->P : s->PH;
+    launch_stage1d_mixed(stage, s->cfg.threads, mixed_grid(s, L.ntu), queue, s->d_probs, s->d_times,
+                         s->d_mtiles + L.t0, s->d_queue + 2 * l, s->tb, sst, s->P, out, st, false);
+    launch_stage1d_mixed(stage, s->cfg.threads, mixed_grid(s, L.ntt), queue, s->d_probs, s->d_times,
+                         s->d_mtiles + L.t0 + L.ntu, s->d_queue + 2 * l + 1, s->tb, sst, s->P, out, st, true);
+  };
+  if (mixed && s->nlanes > 1 && !s->timing) {
+    // lanes: each lane's whole step sequence on its own stream (its problems' time
+    // records, dt and sweeps touch nothing of the other lanes)
+    CK(cudaEventRecord(s->ev_fork, s->stream));
+    for (int l = 1; l < s->nlanes; l++) CK(cudaStreamWaitEvent(s->lane_st[l], s->ev_fork, 0));
+    for (int k = 0; k < nsteps; k++) {
+      for (int l = 0; l < s->nlanes; l++) {
+        const mdg_solver::Lane &L = s->lane[l];
+        cudaStream_t st = l ? s->lane_st[l] : s->stream;
+        const int n = L.m1 - L.m0;
+        launch_dt_finalize(s->d_probs + L.m0, s->d_times + L.m0, n, s->d_err, st);
+        if (s->any_mono) launch_monopole1d(s->d_probs + L.m0, s->d_times + L.m0, n, s->tb, s->P, st);
+        mixed_stage(0, l, st);
+        if (s->any_mono) launch_monopole1d(s->d_probs + L.m0, s->d_times + L.m0, n, s->tb, s->PH, st);
+        mixed_stage(1, l, st);
+        launch_finish(s->d_times + L.m0, n, st);
+      }
+    }
+    for (int l = 1; l < s->nlanes; l++) {
+      CK(cudaEventRecord(s->lane_ev[l], s->lane_st[l]));
+      CK(cudaStreamWaitEvent(s->stream, s->lane_ev[l], 0));
+    }
+    CK(cudaGetLastError());
+    return MDG_OK;
+  }
   for (int k = 0; k < nsteps; k++) {
     mark(MDG_TIMER_DT, 0);
     launch_dt_finalize(s->d_probs, s->d_times, s->nprob, s->d_err, s->stream);
@@ -732,10 +811,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
     mark(MDG_TIMER_STAGE0, 0);
     if (mixed && s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->P, s->stream);
     if (mixed) {
-      launch_stage1d_mixed(0, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
-                           s->tb, s->P, s->P, s->PH, s->stream, false);
-      launch_stage1d_mixed(0, s->cfg.threads, mgrid_tab, queue, s->d_probs, s->d_times, s->d_mtiles + nmu,
-                           s->d_queue + 1, s->tb, s->P, s->P, s->PH, s->stream, true);
+      for (int l = 0; l < s->nlanes; l++) mixed_stage(0, l, s->stream);
     }
     else if (s->ndim == 3)
       launch_stage3d(0, mix3, s->s3, s->d_probs, s->d_times, s->P, s->P, s->PH, s->stream);
@@ -751,10 +827,7 @@ static int queue_steps(mdg_solver *s, int nsteps)
     mark(MDG_TIMER_STAGE1, 0);
     if (mixed && s->any_mono) launch_monopole1d(s->d_probs, s->d_times, s->nprob, s->tb, s->PH, s->stream);
     if (mixed) {
-      launch_stage1d_mixed(1, s->cfg.threads, mgrid, queue, s->d_probs, s->d_times, s->d_mtiles, s->d_queue,
-                           s->tb, s->PH, s->P, s->P, s->stream, false);
-      launch_stage1d_mixed(1, s->cfg.threads, mgrid_tab, queue, s->d_probs, s->d_times, s->d_mtiles + nmu,
-                           s->d_queue + 1, s->tb, s->PH, s->P, s->P, s->stream, true);
+      for (int l = 0; l < s->nlanes; l++) mixed_stage(1, l, s->stream);
     }
     else if (s->ndim == 3)
       launch_stage3d(1, mix3, s->s3, s->d_probs, s->d_times, s->PH, s->P, s->P, s->stream);
@@ -966,6 +1039,7 @@ int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
   if (cfg->steps_per_graph < 0 || cfg->steps_per_graph > 10000)
     return fail(MDG_ERR_INVALID, "steps_per_graph out of [0, 10000]");
   if (cfg->run_length < 1 || cfg->run_length > 64) return fail(MDG_ERR_INVALID, "run_length out of [1, 64]");
+  if (cfg->lanes < 1 || cfg->lanes > MDG_MAX_LANES) return fail(MDG_ERR_INVALID, "lanes out of [1, 4]");
   CK(cudaSetDevice(s->device));
   CK(cudaStreamSynchronize(s->stream));
   if (s->ndim == 3 && cfg->run_length != s->cfg.run_length) {
@@ -974,14 +1048,12 @@ int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
     if (rc != MDG_OK) return fail(rc, "run_length: " + why);
     drop_graph(s);
   }
-  const bool reshape = cfg->threads != s->cfg.threads;
+  const bool reshape = cfg->threads != s->cfg.threads || cfg->lanes != s->cfg.lanes;
   const bool batched = s->precision == MDG_PREC_MIXED && s->ndim == 1;
-  if (reshape && batched) {
-    int rc = build_mixed_tiles(s, cfg->threads);
+  if (batched) {
+    // rebuilds the tile lists (a new shape) or just resets every work queue
+    int rc = build_mixed_tiles(s, cfg->threads, cfg->lanes);
     if (rc != MDG_OK) return rc;
-  } else if (batched) {
-    const WorkQueue q[2] = {{{0u, 0u}, s->nmtiles - s->nmtab, 0}, {{0u, 0u}, s->nmtab, 0}};
-    CK(cudaMemcpy(s->d_queue, q, sizeof q, cudaMemcpyHostToDevice));
   }
   if (reshape || cfg->ctas_per_sm != s->cfg.ctas_per_sm || cfg->steps_per_graph != s->cfg.steps_per_graph)
     drop_graph(s);
@@ -1032,33 +1104,41 @@ int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double
     std::vector<mdg_launch_config> cand;
     const int k = orig.steps_per_graph;
     if (dendritic) {
-      for (int len : {4, 8, 16, 32}) cand.push_back(mdg_launch_config{orig.threads, orig.ctas_per_sm, k, len});
+      for (int len : {4, 8, 16, 32}) cand.push_back(mdg_launch_config{orig.threads, orig.ctas_per_sm, k, len, 1});
     } else {
       for (int nt : {64, 128, 256}) {
         const int occ = mixed_max_ctas_per_sm(nt);
         for (int c : {0, 1, 2, 3, 4, 6, 8, 12, 16})
-          if (c <= occ) cand.push_back(mdg_launch_config{nt, c, k, orig.run_length});
+          if (c <= occ) cand.push_back(mdg_launch_config{nt, c, k, orig.run_length, 1});
       }
     }
     const int steps = (k > 0) ? ((trial_steps + k - 1) / k) * k : trial_steps;
-    {
-      for (size_t ci = 0; ci < cand.size() && rc == MDG_OK; ci++) {
-        const mdg_launch_config c = cand[ci];
-        if ((rc = mdg_set_launch_config(s, &c)) != MDG_OK) break;
-        if ((rc = restore()) != MDG_OK) break;
-        if ((rc = mdg_step(s, k > 0 ? k : 1)) != MDG_OK) break;   // warm-up (and graph capture)
-        float ms = 0.f;
-        cudaError_t ce = cudaEventRecord(e0, s->stream);
-        if (ce == cudaSuccess && (rc = mdg_step(s, steps)) != MDG_OK) break;
-        if (ce == cudaSuccess) ce = cudaEventRecord(e1, s->stream);
-        if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
-        if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
-        if (ce != cudaSuccess) {
-          rc = fail(MDG_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(ce));
-          break;
-        }
-        const double per = ms / steps;
-        if (per < bestms) { bestms = per; bestc = c; }
+    // one trial: the state restored, a warm-up (and graph capture), then `steps` timed steps
+    auto trial = [&](const mdg_launch_config &c) -> int {
+      int r = mdg_set_launch_config(s, &c);
+      if (r == MDG_OK) r = restore();
+      if (r == MDG_OK) r = mdg_step(s, k > 0 ? k : 1);
+      if (r != MDG_OK) return r;
+      float ms = 0.f;
+      cudaError_t ce = cudaEventRecord(e0, s->stream);
+      if (ce == cudaSuccess && (r = mdg_step(s, steps)) != MDG_OK) return r;
+      if (ce == cudaSuccess) ce = cudaEventRecord(e1, s->stream);
+      if (ce == cudaSuccess) ce = cudaEventSynchronize(e1);
+      if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+      if (ce != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("autotune timing: ") + cudaGetErrorString(ce));
+      const double per = ms / steps;
+      if (per < bestms) { bestms = per; bestc = c; }
+      return MDG_OK;
+    };
+    for (size_t ci = 0; ci < cand.size() && rc == MDG_OK; ci++) rc = trial(cand[ci]);
+    // the mixed 1-D sweep: lanes with the best (threads, ctas_per_sm)
+    if (!dendritic) {
+      const mdg_launch_config shape = bestc;
+      for (int nl : {2, 4}) {
+        if (rc != MDG_OK) break;
+        mdg_launch_config c = shape;
+        c.lanes = nl;
+        rc = trial(c);
       }
     }
     if (rc == MDG_OK) rc = mdg_set_launch_config(s, &bestc);

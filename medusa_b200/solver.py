@@ -43,11 +43,11 @@ class MdgError(RuntimeError):
 class LaunchConfig(ctypes.Structure):
     """mdg_launch_config of include/medusa_b200.h."""
     _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("steps_per_graph", ctypes.c_int),
-                ("run_length", ctypes.c_int)]
+                ("run_length", ctypes.c_int), ("lanes", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {"threads": self.threads, "ctas_per_sm": self.ctas_per_sm, "steps_per_graph": self.steps_per_graph,
-                "run_length": self.run_length}
+                "run_length": self.run_length, "lanes": self.lanes}
 
 
 class ServerConfig(ctypes.Structure):
@@ -425,17 +425,18 @@ class Solver:
         return c.as_dict()
 
     def set_launch_config(self, threads: int = None, ctas_per_sm: int = None, steps_per_graph: int = None,
-                          run_length: int = None):
+                          run_length: int = None, lanes: int = None):
         cur = self.launch_config()
         c = LaunchConfig(cur["threads"] if threads is None else threads,
                          cur["ctas_per_sm"] if ctas_per_sm is None else ctas_per_sm,
                          cur["steps_per_graph"] if steps_per_graph is None else steps_per_graph,
-                         cur["run_length"] if run_length is None else run_length)
+                         cur["run_length"] if run_length is None else run_length,
+                         cur["lanes"] if lanes is None else lanes)
         _check(library().mdg_set_launch_config(self._h, ctypes.byref(c)), "mdg_set_launch_config")
 
     def autotune(self, trial_steps: int = 5):
-        """Pick the fastest launch shape (the mixed 1-D sweep's threads and persistent CTAs, a
-        dendritic sweep's run length); returns (config, ms per step)."""
+        """Pick the fastest launch shape (the mixed 1-D sweep's threads, persistent CTAs and
+        lanes, a dendritic sweep's run length); returns (config, ms per step)."""
         c = LaunchConfig()
         ms = ctypes.c_double()
         _check(library().mdg_autotune(self._h, int(trial_steps), ctypes.byref(c), ctypes.byref(ms)), "mdg_autotune")

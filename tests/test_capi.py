@@ -87,7 +87,7 @@ def test_unknown_precision_is_rejected():
 
 def test_launch_config_calls_reject_null_solver():
     L = S.library()
-    c = S.LaunchConfig(128, 0, 10, 16)
+    c = S.LaunchConfig(128, 0, 10, 16, 1)
     assert L.mdg_get_launch_config(None, ctypes.byref(c)) == 1
     assert L.mdg_set_launch_config(None, ctypes.byref(c)) == 1
     assert L.mdg_autotune(None, 3, None, None) == 1

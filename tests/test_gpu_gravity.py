@@ -189,6 +189,11 @@ def test_mixed_1d_monopole_matches_fp64(radius, floors, n1, nsteps):
     with Solver(batch_probs, precision=PREC_MIXED) as s:
         s.step(30)
         batch = [s.update_cpu(m) for m in range(3)]
+    with Solver(batch_probs, precision=PREC_MIXED) as s:
+        s.set_launch_config(lanes=3)   # each problem on a stream of its own
+        s.step(30)
+        for m in range(3):
+            assert np.array_equal(s.update_cpu(m), batch[m])
     for m, q in enumerate(batch_probs):
         with Solver(q, precision=PREC_MIXED) as s:
             s.step(30)

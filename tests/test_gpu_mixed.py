@@ -185,13 +185,13 @@ def test_mixed_closed_form_and_table_problems_batched_equal_alone():
     """Problems whose geometry is evaluated in closed form and problems that read the
     Romberg tables (SINH and LOG radii, SINH_MODIFIED + POLYTH) run in two launches per
     stage with their own work queues: each result is the same alone and in the batch, in
-    persistent and one-CTA-per-tile mode."""
+    persistent and one-CTA-per-tile mode, and with the problems split into lanes."""
     probs = [P.spherical_1d("sedov", 300, 1.4, p_ratio=1.0e4, r0=0.05),
              P.spherical_1d("sedov", 256, 1.4, p_ratio=1.0e4, r0=0.05, dr_min=2.0e-3),
              P.sod(257),
              P.spherical_1d("sedov", 160, 1.4, p_ratio=1.0e4, r0=0.02, coords="log", r_in=1.0e-3),
              P.spherical_1d("sod", 200, 1.4, rho_ratio=10.0, p_ratio=100.0, dr_min=1.0e-3, coords="default")]
-    for cfg in (dict(), dict(ctas_per_sm=0)):
+    for cfg in (dict(), dict(ctas_per_sm=0), dict(lanes=3)):
         batched, bt = _run(probs, PREC_MIXED, 25, **cfg)
         for m, pb in enumerate(probs):
             alone, at = _run([pb], PREC_MIXED, 25, **cfg)
@@ -201,7 +201,8 @@ def test_mixed_closed_form_and_table_problems_batched_equal_alone():
 
 @pytest.mark.parametrize("cfg", [dict(threads=64), dict(threads=256), dict(ctas_per_sm=2),
                                  dict(threads=64, ctas_per_sm=8), dict(steps_per_graph=0),
-                                 dict(steps_per_graph=7)])
+                                 dict(steps_per_graph=7), dict(lanes=2), dict(lanes=4, steps_per_graph=0),
+                                 dict(lanes=3, ctas_per_sm=0), dict(lanes=4, threads=256)])
 def test_mixed_launch_shapes_identical(cfg):
     ens = _small_ensemble()
     ref, rt = _run(ens, PREC_MIXED, 23)
@@ -225,7 +226,7 @@ def test_autotune_restores_state():
     with Solver(ens, precision=PREC_MIXED) as s:
         s.step(4)
         cfg, ms = s.autotune(trial_steps=3)
-        assert cfg["threads"] in (64, 128, 256) and cfg["ctas_per_sm"] >= 0 and ms > 0
+        assert cfg["threads"] in (64, 128, 256) and cfg["ctas_per_sm"] >= 0 and cfg["lanes"] in (1, 2, 4) and ms > 0
         assert s.launch_config() == cfg
         s.step(4)
         s.synchronize()
@@ -244,7 +245,7 @@ def test_autotune_rejected_for_fp64():
 def test_launch_config_validation():
     with Solver(P.sod(64), precision=PREC_MIXED) as s:
         for bad in (dict(threads=96), dict(ctas_per_sm=-1), dict(steps_per_graph=-3), dict(run_length=0),
-                    dict(run_length=65)):
+                    dict(run_length=65), dict(lanes=0), dict(lanes=5)):
             with pytest.raises(MdgError) as e:
                 s.set_launch_config(**bad)
             assert e.value.code == 1
