@@ -573,7 +573,8 @@ def run_ensemble(args, ctx):
         "config": ensemble_config(probs, ctx.world),
         "precision": "mixed: FP32 reconstruction/limiting/Riemann, FP64 state/fluxes/sources/update/dt",
         "launch": dict(tuned, autotune_ms_per_step=tune_ms),
-        "gpu_launches": 4 * K,
+        # per step and lane: dt, the two stage kernels, the time update
+        "gpu_launches": 4 * K * tuned.get("lanes", 1),
         "e2e": {"value": e2e, "unit": "zone-updates/s", "h2d_bytes_per_step": h2d / K,
                 "d2h_bytes_per_step": d2h / K,
                 "timed": "mdg_run_host: upload of all %d initial states (pinned H2D) + %d steps + download of "
