@@ -215,12 +215,19 @@ def timed_steps(ctx, solver, K, sample_clocks=False):
 
 
 def stage_times(solver, nsteps):
-    """Per-step device time of each RK stage from the library's event timers."""
+    """Per-step device time of each RK stage from the library's event timers, each stage
+    one launch over all problems (lanes set to 1 for the measurement: the roofline is the
+    kernel's, whatever the scheduling of the timed run)."""
+    cfg = solver.launch_config()
+    if cfg.get("lanes", 1) != 1:
+        solver.set_launch_config(lanes=1)
     solver.set_timing(True)
     solver.step(nsteps)
     solver.synchronize()
     tm = solver.timers()
     solver.set_timing(False)
+    if cfg.get("lanes", 1) != 1:
+        solver.set_launch_config(lanes=cfg["lanes"])
     return ({k: tm[k][0] / max(1, tm[k][1]) for k in ("stage0", "stage1", "estimate_dt", "finish")})
 
 
