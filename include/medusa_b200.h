@@ -217,6 +217,13 @@ const char *mdg_last_error_message(void);
 #define MDG_NTIMERS         4
 int mdg_set_timing(mdg_solver *s, int enable);
 int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
+/* Append the timers to the CSV file `path` in the columns of the reference's timing.csv
+ * (output_timers, io.c:51-108: timer, time, step, ncycle, max, min, avg; seconds; the
+ * header row when the file is new), with t and the step count of problem `prob`.  Timer
+ * names: estimate_dt, step_stage0, step_stage1, step_finish.  (The reference's
+ * single-process path writes the first timer's total in every row; here each row has its
+ * own timer's.) */
+int mdg_write_timers(mdg_solver *s, int prob, const char *path);
 
 /*
  * No counterpart in the reference (its launch shapes are compile-time constants).

@@ -1452,6 +1452,29 @@ int mdg_get_timers(mdg_solver *s, double *ms, long long *calls)
   return MDG_OK;
 }
 
+int mdg_write_timers(mdg_solver *s, int prob, const char *path)
+{
+  if (!s || !path) return fail(MDG_ERR_INVALID, "solver/path");
+  double t = 0.0;
+  int istep = 0;
+  int rc = mdg_get_time(s, prob, &t, nullptr, &istep);
+  if (rc != MDG_OK) return rc;
+  static const char *names[MDG_NTIMERS] = {"estimate_dt", "step_stage0", "step_stage1", "step_finish"};
+  const bool fresh = std::fopen(path, "r") == nullptr ? true : false;
+  FILE *f = std::fopen(path, "a");
+  if (!f) return fail(MDG_ERR_IO, std::string("cannot open ") + path);
+  bool ok = true;
+  if (fresh) ok = std::fprintf(f, "timer,time,step,ncycle,max,min,avg\n") > 0;
+  for (int k = 0; k < MDG_NTIMERS && ok; k++) {
+    // one process: the maximum, minimum and mean over ranks are its own total, in seconds
+    const double sec = s->tms[k] * 1.0e-3;
+    ok = std::fprintf(f, "%s,%f,%d,%lu,%f,%f,%f\n", names[k], t, istep, (unsigned long)s->tcalls[k], sec, sec,
+                      sec) > 0;
+  }
+  if (std::fclose(f) != 0 || !ok) return fail(MDG_ERR_IO, std::string("cannot write ") + path);
+  return MDG_OK;
+}
+
 int mdg_destroy(mdg_solver *s)
 {
   if (!s) return MDG_OK;

@@ -135,6 +135,7 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_get_time.argtypes = [vp, i, ctypes.POINTER(d), ctypes.POINTER(d), ctypes.POINTER(i)]
     L.mdg_get_stream.argtypes = [vp, ctypes.POINTER(vp)]
     L.mdg_set_time.argtypes = [vp, i, d, i]
+    L.mdg_write_timers.argtypes = [vp, i, ctypes.c_char_p]
     L.mdg_restart_write.argtypes = [vp, i, ctypes.c_char_p]
     L.mdg_restart_read.argtypes = [vp, i, ctypes.c_char_p]
     L.mdg_synchronize.argtypes = [vp]
@@ -417,6 +418,10 @@ class Solver:
         calls = np.zeros(4, dtype=np.int64)
         _check(library().mdg_get_timers(self._h, ms.ctypes.data, calls.ctypes.data), "mdg_get_timers")
         return {n: (float(ms[k]), int(calls[k])) for k, n in enumerate(self.TIMER_NAMES)}
+
+    def write_timers(self, path: str, m: int = 0):
+        """Append the timers to a CSV file in the reference's timing.csv columns."""
+        _check(library().mdg_write_timers(self._h, int(m), os.fsencode(path)), "mdg_write_timers")
 
     # --- launch shape, autotuning and conservation diagnostics
     def launch_config(self) -> dict:

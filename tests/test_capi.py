@@ -95,6 +95,7 @@ def test_launch_config_calls_reject_null_solver():
     assert L.mdg_set_time(None, 0, 0.0, 0) == 1
     assert L.mdg_restart_write(None, 0, b"x") == 1
     assert L.mdg_restart_read(None, 0, b"x") == 1
+    assert L.mdg_write_timers(None, 0, b"x") == 1
 
 
 @pytest.mark.parametrize("field,value", [("precision", 7), ("max_problems", 0), ("max_zones", 2),

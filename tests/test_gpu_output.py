@@ -144,3 +144,27 @@ def test_restart_of_a_dendritic_grid_and_wrong_file(tmp_path):
         with pytest.raises(MdgError) as e:
             s.restart_read(str(tmp_path / "restart.bin"), 0)
         assert e.value.code == 1
+
+
+def test_write_timers_in_the_reference_timing_csv_columns(tmp_path):
+    """timing.csv as output_timers (io.c:51-108) lays it out: a header row when the file is
+    new, then per timer its name, t, step, cycle count and max/min/avg seconds; a second
+    call appends."""
+    import csv
+    path = str(tmp_path / "timing.csv")
+    with Solver(P.spherical_1d("sedov", 300, 1.4, p_ratio=1.0e4, r0=0.05)) as s:
+        s.set_timing(True)
+        s.step(5)
+        s.write_timers(path)
+        s.step(3)
+        s.write_timers(path)
+        t, _, ist = s.time(0)
+    rows = list(csv.reader(open(path)))
+    assert rows[0] == ["timer", "time", "step", "ncycle", "max", "min", "avg"]
+    assert len(rows) == 1 + 2 * 4
+    names = [r[0] for r in rows[1:5]]
+    assert names == ["estimate_dt", "step_stage0", "step_stage1", "step_finish"]
+    assert all(int(r[3]) == 5 for r in rows[1:5]) and all(int(r[3]) == 8 for r in rows[5:])
+    assert all(int(r[2]) == 5 for r in rows[1:5]) and all(int(r[2]) == ist for r in rows[5:])
+    assert abs(float(rows[5][1]) - t) <= 1.0e-6 * max(t, 1e-30) + 1e-6
+    assert all(float(r[4]) > 0.0 and r[4] == r[5] == r[6] for r in rows[1:])
