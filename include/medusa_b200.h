@@ -288,7 +288,9 @@ int mdg_conserved_totals(mdg_solver *s, double *mass, double *energy);
  * (about 4.4 MB, held by every GPU that loads this library until exit).  Rules:
  *   - n1 > MDG_NOALLOC_MAX_ZONES is rejected with MDG_ERR_OUTOFMEM (does not fit);
  *   - the first call on a device performs the device set-up (it looks up the array's
- *     device address); make that first call before any stream capture;
+ *     device address);
+ *   - no call can be captured into a CUDA graph: each waits on its stream before it
+ *     returns (the host tables must outlive their copies);
  *   - all calls share the array: calls whose work overlaps on the GPU race;
  *   - the array keeps the last call's contents; each call re-initialises what it uses;
  *   - the tables are built in one process-wide host buffer under a lock, so calls from
