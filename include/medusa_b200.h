@@ -220,7 +220,7 @@ int mdg_get_timers(mdg_solver *s, double *ms, long long *calls);
 /* Append the timers to the CSV file `path` in the columns of the reference's timing.csv
  * (output_timers, io.c:51-108: timer, time, step, ncycle, max, min, avg; seconds; the
  * header row when the file is new), with t and the step count of problem `prob`.  Timer
- * names: estimate_dt, step_stage0, step_stage1, step_finish.  (The reference's
+ * names: estimate_dt, stage0, stage1, finish (as Solver.timers).  (The reference's
  * single-process path writes the first timer's total in every row; here each row has its
  * own timer's.) */
 int mdg_write_timers(mdg_solver *s, int prob, const char *path);
@@ -240,7 +240,14 @@ int mdg_write_timers(mdg_solver *s, int prob, const char *path);
  *   lanes            mixed 1-D sweep: the problems split into 1..4 groups of about equal
  *                    zone count, each group's steps queued on a stream of its own, so that
  *                    one group's short kernels and kernel tails overlap another's stage
- *                    kernels (default 1); the results do not depend on it.
+ *                    kernels (default 1); the results do not depend on it;
+ *   resident         plain FP64 1-D solvers without monopole gravity whose problems have at
+ *                    most 16 tiles (2016 zones): 1 (default) = mdg_step runs the whole
+ *                    step sequence -- dt rules, both RK stages, time update -- in one launch
+ *                    per 256 steps, one thread-block cluster of CTAs per problem (the
+ *                    per-phase path launches four dependent kernels per step); 0 = the
+ *                    per-phase launches.  Other solvers ignore it; the results do not
+ *                    depend on it.  mdg_resident_cluster reports whether it applies.
  */
 #define MDG_MAX_LANES 4
 typedef struct mdg_launch_config {
@@ -249,9 +256,15 @@ typedef struct mdg_launch_config {
   int steps_per_graph;
   int run_length;
   int lanes;
+  int resident;
 } mdg_launch_config;
 int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg);
 int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg);
+/* CTAs per problem of the resident stepper (mdg_launch_config::resident) for this solver,
+ * 0 when mdg_step cannot use it (other solvers, a problem of more than 16 tiles, or such
+ * a cluster does not fit the device).  With resident = 1 and *ctas > 0, mdg_step(s, n)
+ * queues ceil(n / 256) kernel launches. */
+int mdg_resident_cluster(mdg_solver *s, int *ctas);
 
 /* Time every admissible launch shape over trial_steps steps of the solver's own
  * problems, keep the fastest and restore the state, times and error flag as they were:

@@ -83,7 +83,10 @@ struct mdg_solver {
   cudaEvent_t lane_ev[MDG_MAX_LANES] = {};
   cudaEvent_t ev_fork = nullptr;
   int num_sms = 0;
-  mdg_launch_config cfg{128, 0, 10, 16, 1};
+  mdg_launch_config cfg{128, 0, 10, 16, 1, 1};
+  // plain FP64 1-D solvers without monopole gravity whose problems have at most
+  // RESIDENT1D_MAX_TILES tiles: CTAs per problem of the resident stepper (0: none)
+  int res_cs = 0;
   // CUDA graph of cfg.steps_per_graph steps (rebuilt when the launch shape changes)
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -701,6 +704,11 @@ int mdg_create(const mdg_problem_desc *descs, int nprob, int precision, int devi
     int rc = build_mixed_tiles(s, s->cfg.threads, s->cfg.lanes);
     if (rc != MDG_OK) { free_all(s); delete s; return rc; }
   }
+  if (precision == MDG_PREC_FP64 && ndim == 1 && !s->any_mono) {
+    int max_tiles = 0;
+    for (const ProbDev &P : s->hprobs) max_tiles = std::max(max_tiles, (P.n1 + TILE1 - 1) / TILE1);
+    s->res_cs = resident1d_cluster_size(max_tiles);
+  }
   *out = s;
   return MDG_OK;
 }
@@ -934,11 +942,25 @@ static void drop_graph(mdg_solver *s)
   s->graph_steps = 0;
 }
 
+// mdg_step advances the solver with the resident stepper (launches of at most
+// RESIDENT_STEPS steps each) rather than the per-phase launches
+static bool uses_resident(const mdg_solver *s)
+{
+  return s->res_cs > 0 && s->cfg.resident && !s->timing;
+}
+constexpr int RESIDENT_STEPS = 256;
+
 int mdg_step(mdg_solver *s, int nsteps)
 {
   if (!s) return fail(MDG_ERR_INVALID, "solver");
   if (nsteps < 0) return fail(MDG_ERR_INVALID, "nsteps < 0");
   CK(cudaSetDevice(s->device));
+  if (uses_resident(s)) {
+    for (int left = nsteps; left > 0; left -= RESIDENT_STEPS)
+      CK(launch_resident1d(s->res_cs, s->nprob, s->d_probs, s->d_times, s->tb, s->P, s->PH,
+                           std::min(left, RESIDENT_STEPS), s->d_err, s->stream));
+    return MDG_OK;
+  }
   const int k = s->cfg.steps_per_graph;
   if (s->timing || k <= 0 || nsteps < k) return queue_steps(s, nsteps);
   int rc = ensure_graph(s);
@@ -963,7 +985,9 @@ int mdg_run_host(mdg_solver *const *solvers, int n, const double *const *h_in, d
     mdg_solver *s = solvers[i];
     int rc = stage_all(s);
     if (rc != MDG_OK) return rc;
-    if (s->cfg.steps_per_graph > 0 && nsteps >= s->cfg.steps_per_graph && (rc = ensure_graph(s)) != MDG_OK) return rc;
+    if (!uses_resident(s) && s->cfg.steps_per_graph > 0 && nsteps >= s->cfg.steps_per_graph &&
+        (rc = ensure_graph(s)) != MDG_OK)
+      return rc;
   }
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> done(n, nullptr);
@@ -1030,6 +1054,13 @@ int mdg_get_launch_config(mdg_solver *s, mdg_launch_config *cfg)
   return MDG_OK;
 }
 
+int mdg_resident_cluster(mdg_solver *s, int *ctas)
+{
+  if (!s || !ctas) return fail(MDG_ERR_INVALID, "solver/ctas");
+  *ctas = s->res_cs;
+  return MDG_OK;
+}
+
 int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
 {
   if (!s || !cfg) return fail(MDG_ERR_INVALID, "solver/cfg");
@@ -1040,6 +1071,7 @@ int mdg_set_launch_config(mdg_solver *s, const mdg_launch_config *cfg)
     return fail(MDG_ERR_INVALID, "steps_per_graph out of [0, 10000]");
   if (cfg->run_length < 1 || cfg->run_length > 64) return fail(MDG_ERR_INVALID, "run_length out of [1, 64]");
   if (cfg->lanes < 1 || cfg->lanes > MDG_MAX_LANES) return fail(MDG_ERR_INVALID, "lanes out of [1, 4]");
+  if (cfg->resident != 0 && cfg->resident != 1) return fail(MDG_ERR_INVALID, "resident must be 0 or 1");
   CK(cudaSetDevice(s->device));
   CK(cudaStreamSynchronize(s->stream));
   if (s->ndim == 3 && cfg->run_length != s->cfg.run_length) {
@@ -1104,12 +1136,13 @@ int mdg_autotune(mdg_solver *s, int trial_steps, mdg_launch_config *best, double
     std::vector<mdg_launch_config> cand;
     const int k = orig.steps_per_graph;
     if (dendritic) {
-      for (int len : {4, 8, 16, 32}) cand.push_back(mdg_launch_config{orig.threads, orig.ctas_per_sm, k, len, 1});
+      for (int len : {4, 8, 16, 32})
+        cand.push_back(mdg_launch_config{orig.threads, orig.ctas_per_sm, k, len, 1, orig.resident});
     } else {
       for (int nt : {64, 128, 256}) {
         const int occ = mixed_max_ctas_per_sm(nt);
         for (int c : {0, 1, 2, 3, 4, 6, 8, 12, 16})
-          if (c <= occ) cand.push_back(mdg_launch_config{nt, c, k, orig.run_length, 1});
+          if (c <= occ) cand.push_back(mdg_launch_config{nt, c, k, orig.run_length, 1, orig.resident});
       }
     }
     const int steps = (k > 0) ? ((trial_steps + k - 1) / k) * k : trial_steps;
@@ -1459,8 +1492,10 @@ int mdg_write_timers(mdg_solver *s, int prob, const char *path)
   int istep = 0;
   int rc = mdg_get_time(s, prob, &t, nullptr, &istep);
   if (rc != MDG_OK) return rc;
-  static const char *names[MDG_NTIMERS] = {"estimate_dt", "step_stage0", "step_stage1", "step_finish"};
-  const bool fresh = std::fopen(path, "r") == nullptr ? true : false;
+  static const char *names[MDG_NTIMERS] = {"estimate_dt", "stage0", "stage1", "finish"};
+  FILE *probe = std::fopen(path, "r");
+  const bool fresh = probe == nullptr;
+  if (probe) std::fclose(probe);
   FILE *f = std::fopen(path, "a");
   if (!f) return fail(MDG_ERR_IO, std::string("cannot open ") + path);
   bool ok = true;

@@ -54,6 +54,14 @@ constexpr int TJY2 = NTY2 - 2;
 constexpr int TIY2 = MDG_TIY2;    // rows per direction-1 tile
 
 struct TmaTables1d;
+// The resident 1-D stepper (plain FP64): CTAs per problem for problems of at most
+// max_tiles tiles (a power of two), or 0 when it cannot run (more than
+// RESIDENT1D_MAX_TILES tiles, or such a cluster does not fit this device); the launch of
+// nsteps steps of nprob problems with that cluster size.
+constexpr int RESIDENT1D_MAX_TILES = 16;
+int resident1d_cluster_size(int max_tiles);
+cudaError_t launch_resident1d(int cs, int nprob, const ProbDev *probs, ProbTime *times, const Tables &tb,
+                              StateSoA p, StateSoA ph, int nsteps, int *err, cudaStream_t st);
 // One RK stage of the plain FP64 1-D sweep; tm (may be NULL): tensor maps of tb's rc0 and
 // geo tables, with which each tile's tables are staged into shared memory by TMA.
 void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,

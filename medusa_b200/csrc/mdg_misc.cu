@@ -2,49 +2,17 @@
 // bookkeeping, the first estimate before step 0, and AoS <-> SoA staging of the state.
 #include "mdg_hydro.cuh"
 #include "mdg_kernels.cuh"
+#include "mdg_timeloop.cuh"
 
 namespace mdg {
 
-// estimate_dt() (step.c:192-198) applied to the accumulated minimum, then the safety,
-// growth and end-time rules of main.c:239-251.  One thread per problem.
+// estimate_dt() + the main.c dt rules (dt_finalize_one), one thread per problem.
 __global__ void dt_finalize_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, int nprob,
                                    int *err)
 {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= nprob) return;
-  ProbTime T = times[m];
-  if (T.dt_ready) return;
-  const ProbDev &P = probs[m];
-  // the reference's time loop runs while t < tmax (main.c:206); past it nothing changes
-  // (an empty slot of a solve server has tmax = 0 and is done from the start)
-  if (!(T.t < P.tmax)) {
-    T.done = 1;
-    T.dt_ready = 1;
-    times[m] = T;
-    return;
-  }
-  double min_dt = ord_to_dbl(T.minacc);
-  if (T.istep == 0) min_dt = tmin(min_dt, P.initial_dt);
-  min_dt = tmin(min_dt, P.dtmax);
-  min_dt *= P.cfl;
-  // main.c:229-238 aborts the run when the estimate drops below dtmin; here the
-  // condition is recorded for the host (mdg_synchronize returns MDG_ERR_NONFINITE)
-  if (!(min_dt >= P.dtmin)) {
-    atomicExch(err, MDG_ERR_NONFINITE);
-    T.err = MDG_ERR_NONFINITE;
-  }
-  double dt = min_dt;
-  if (T.istep == 0) dt *= P.dt_init_safety;
-  else dt = tmin(T.dtold * P.dt_grow_safety, dt);
-  T.dtold = dt;
-  if (T.t + 1 * dt > P.tmax) dt = 1.000000001 * (P.tmax - T.t) / 1;
-  if (dt < P.dtmin) dt = P.dtmin;
-  T.dt = dt;
-  T.t_bc1 = T.t + dt;                  // reset_boundaries_gpu: t += dt (bc.c:721)
-  T.t_next = (T.t_bc1 - dt) + dt;      // ... t -= dt (bc.c:1418), then main.c:263 t += dt
-  T.minacc = dbl_to_ord(1.0e100);      // step.c:49
-  T.dt_ready = 1;
-  times[m] = T;
+  dt_finalize_one(probs[m], times + m, err);
 }
 
 // estimate_dt() (step.c:192-198) alone: what it leaves in the reference's global dt.
@@ -94,11 +62,7 @@ __global__ void finish_kernel(ProbTime *__restrict__ times, int nprob)
 {
   const int m = blockIdx.x * blockDim.x + threadIdx.x;
   if (m >= nprob) return;
-  if (!times[m].done) {
-    times[m].t = times[m].t_next;
-    times[m].istep += 1;
-  }
-  times[m].dt_ready = 0;
+  finish_one(times + m);
 }
 
 // monopole_gravity_start/finish (gravity.c:145-425, GR_MONOPOLE=FALSE) of a 1-D problem,

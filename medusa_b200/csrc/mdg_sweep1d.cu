@@ -12,6 +12,12 @@
 //
 // Many problems of different sizes are advanced by one launch: the grid is a list of
 // (problem, tile) work items.
+//
+// Small problems (at most 16 tiles, 2016 zones) can instead be advanced by the resident
+// stepper: one thread-block cluster per problem, one CTA per tile, runs the whole step
+// sequence of many steps in one launch -- the dt rules, both RK stages and the time
+// update, separated by cluster barriers -- where the per-phase path pays four dependent
+// launches per step.  It runs the same tile code, so the two paths agree bit for bit.
 // The FP64 reconstruction is called out of line here (one copy of para_recon in the
 // kernel instead of six): the kernel is bound by instruction fetch and load latency, and
 // the smaller code ran the 2048-problem ensemble 18 % faster on a B200 (same results).
@@ -20,6 +26,8 @@
 #include "mdg_kernels.cuh"
 #include "mdg_load1d.cuh"
 #include "mdg_tma.cuh"
+#include "mdg_timeloop.cuh"
+#include <cooperative_groups.h>
 
 namespace mdg {
 
@@ -27,11 +35,12 @@ namespace mdg {
 // (GF_TMA_ROWS rows) arrive in shared memory by two tensor loads issued at the start,
 // which overlap the state loads; otherwise every field is read from the tables in HBM
 // when used.  The results are the same.
+// One RK stage of one tile (run by the NT1 threads of a CTA).  tm: the tensor maps of
+// the tables (a __grid_constant__ kernel parameter; not read without TMA).
 template <int STAGE, bool TMA>
-__global__ void __launch_bounds__(NT1)
-stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
-               const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA sn, StateSoA out,
-               const __grid_constant__ TmaTables1d tm)
+__device__ __forceinline__ void stage1d_tile(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+                                             const Tile tile, const Tables &tb, const StateSoA &sst,
+                                             const StateSoA &sn, const StateSoA &out, const TmaTables1d &tm)
 {
   __shared__ double sv[6][NT1 + 2];     // stage-state pencil: 5 primitives + pressure
   __shared__ double sred[32];
@@ -46,7 +55,6 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   double (*sar)[NT1] = TMA ? reinterpret_cast<double(*)[NT1]>(&s_rc[0][0]) : sar_own;
   double (*sfl)[NT1] = TMA ? reinterpret_cast<double(*)[NT1]>(&s_rc[0][0] + 6 * NT1) : sfl_own;
 
-  const Tile tile = tiles[blockIdx.x];
   if (times[tile.prob].done) return;   // past tmax: the time loop has ended (CTA-uniform)
   const ProbDev &P = probs[tile.prob];
   const double dt = times[tile.prob].dt;
@@ -210,6 +218,90 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
   lmin = tmin(lmin, src_dt_from_numerator(nmin));
   if (STAGE == 1) lmin = tmin(lmin, 1.0 / lmax);
   block_min_to(lmin, &times[tile.prob].minacc, sred);
+}
+
+template <int STAGE, bool TMA>
+__global__ void __launch_bounds__(NT1)
+stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
+               const Tile *__restrict__ tiles, Tables tb, StateSoA sst, StateSoA sn, StateSoA out,
+               const __grid_constant__ TmaTables1d tm)
+{
+  stage1d_tile<STAGE, TMA>(probs, times, tiles[blockIdx.x], tb, sst, sn, out, tm);
+}
+
+// The resident stepper: nsteps steps of every problem, cluster c advancing problem c with
+// CTA r on the tile of zones [126 r, 126 r + 126) (CTAs past the last zone only take part
+// in the barriers).  Each step: the dt rules (one thread), stage 0 (p -> ph), stage 1
+// (ph, p -> p), the time update (one thread); a cluster barrier after the dt rules and
+// after each stage orders the state, the time record and the CFL accumulator between the
+// CTAs (release/acquire at cluster scope).  Every CTA runs the same nsteps iterations and
+// the same barriers; a problem past its end time skips the stage work inside them.
+__global__ void __launch_bounds__(NT1)
+resident1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, Tables tb, StateSoA p,
+                  StateSoA ph, int nsteps, int *err, const __grid_constant__ TmaTables1d none)
+{
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  const int m = (int)(blockIdx.x / cl.num_blocks());
+  const Tile tile{m, rank * TILE1, 0, 0};
+  const bool active = tile.i0 < probs[m].n1;
+  const bool lead = rank == 0 && threadIdx.x == 0;
+  for (int k = 0; k < nsteps; k++) {
+    if (lead) dt_finalize_one(probs[m], times + m, err);
+    cl.sync();
+    if (active) stage1d_tile<0, false>(probs, times, tile, tb, p, p, ph, none);
+    cl.sync();
+    if (active) stage1d_tile<1, false>(probs, times, tile, tb, ph, p, p, none);
+    cl.sync();
+    if (lead) finish_one(times + m);
+  }
+}
+
+static cudaLaunchConfig_t resident1d_config(int cs, int nprob, cudaStream_t st, cudaLaunchAttribute *attr)
+{
+  cudaLaunchConfig_t c = {};
+  c.gridDim = dim3((unsigned)(cs * nprob), 1, 1);
+  c.blockDim = dim3(NT1, 1, 1);
+  c.dynamicSmemBytes = 0;
+  c.stream = st;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  c.attrs = attr;
+  c.numAttrs = 1;
+  return c;
+}
+
+int resident1d_cluster_size(int max_tiles)
+{
+  if (max_tiles < 1 || max_tiles > RESIDENT1D_MAX_TILES) return 0;
+  int cs = 1;
+  while (cs < max_tiles) cs <<= 1;
+  if (cs > 8 && cudaFuncSetAttribute(resident1d_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                    cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchAttribute attr[1];
+  const cudaLaunchConfig_t c = resident1d_config(cs, 1, nullptr, attr);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (const void *)resident1d_kernel, &c) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n >= 1 ? cs : 0;
+}
+
+cudaError_t launch_resident1d(int cs, int nprob, const ProbDev *probs, ProbTime *times, const Tables &tb,
+                              StateSoA p, StateSoA ph, int nsteps, int *err, cudaStream_t st)
+{
+  if (nsteps <= 0 || nprob <= 0) return cudaSuccess;
+  cudaLaunchAttribute attr[1];
+  const cudaLaunchConfig_t c = resident1d_config(cs, nprob, st, attr);
+  static const TmaTables1d none{};
+  return cudaLaunchKernelEx(&c, resident1d_kernel, probs, times, tb, p, ph, nsteps, err, none);
 }
 
 void launch_stage1d(int stage, const ProbDev *probs, ProbTime *times, const Tile *tiles, int ntiles,

@@ -43,11 +43,11 @@ class MdgError(RuntimeError):
 class LaunchConfig(ctypes.Structure):
     """mdg_launch_config of include/medusa_b200.h."""
     _fields_ = [("threads", ctypes.c_int), ("ctas_per_sm", ctypes.c_int), ("steps_per_graph", ctypes.c_int),
-                ("run_length", ctypes.c_int), ("lanes", ctypes.c_int)]
+                ("run_length", ctypes.c_int), ("lanes", ctypes.c_int), ("resident", ctypes.c_int)]
 
     def as_dict(self) -> dict:
         return {"threads": self.threads, "ctas_per_sm": self.ctas_per_sm, "steps_per_graph": self.steps_per_graph,
-                "run_length": self.run_length, "lanes": self.lanes}
+                "run_length": self.run_length, "lanes": self.lanes, "resident": self.resident}
 
 
 class ServerConfig(ctypes.Structure):
@@ -148,6 +148,7 @@ def library(path: str = _LIB_PATH) -> ctypes.CDLL:
     L.mdg_get_timers.argtypes = [vp, vp, vp]
     L.mdg_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     L.mdg_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.mdg_resident_cluster.argtypes = [vp, ctypes.POINTER(i)]
     L.mdg_autotune.argtypes = [vp, i, ctypes.POINTER(LaunchConfig), ctypes.POINTER(d)]
     L.mdg_conserved_totals.argtypes = [vp, vp, vp]
     L.mdg_upload_all.argtypes = [vp, vp]
@@ -430,14 +431,21 @@ class Solver:
         return c.as_dict()
 
     def set_launch_config(self, threads: int = None, ctas_per_sm: int = None, steps_per_graph: int = None,
-                          run_length: int = None, lanes: int = None):
+                          run_length: int = None, lanes: int = None, resident: int = None):
         cur = self.launch_config()
         c = LaunchConfig(cur["threads"] if threads is None else threads,
                          cur["ctas_per_sm"] if ctas_per_sm is None else ctas_per_sm,
                          cur["steps_per_graph"] if steps_per_graph is None else steps_per_graph,
                          cur["run_length"] if run_length is None else run_length,
-                         cur["lanes"] if lanes is None else lanes)
+                         cur["lanes"] if lanes is None else lanes,
+                         cur["resident"] if resident is None else resident)
         _check(library().mdg_set_launch_config(self._h, ctypes.byref(c)), "mdg_set_launch_config")
+
+    def resident_cluster(self) -> int:
+        """CTAs per problem of the resident stepper, 0 when mdg_step cannot use it."""
+        n = ctypes.c_int()
+        _check(library().mdg_resident_cluster(self._h, ctypes.byref(n)), "mdg_resident_cluster")
+        return n.value
 
     def autotune(self, trial_steps: int = 5):
         """Pick the fastest launch shape (the mixed 1-D sweep's threads, persistent CTAs and

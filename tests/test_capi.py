@@ -87,7 +87,7 @@ def test_unknown_precision_is_rejected():
 
 def test_launch_config_calls_reject_null_solver():
     L = S.library()
-    c = S.LaunchConfig(128, 0, 10, 16, 1)
+    c = S.LaunchConfig(128, 0, 10, 16, 1, 1)
     assert L.mdg_get_launch_config(None, ctypes.byref(c)) == 1
     assert L.mdg_set_launch_config(None, ctypes.byref(c)) == 1
     assert L.mdg_autotune(None, 3, None, None) == 1
@@ -96,6 +96,8 @@ def test_launch_config_calls_reject_null_solver():
     assert L.mdg_restart_write(None, 0, b"x") == 1
     assert L.mdg_restart_read(None, 0, b"x") == 1
     assert L.mdg_write_timers(None, 0, b"x") == 1
+    n = ctypes.c_int()
+    assert L.mdg_resident_cluster(None, ctypes.byref(n)) == 1
 
 
 @pytest.mark.parametrize("field,value", [("precision", 7), ("max_problems", 0), ("max_zones", 2),

@@ -163,7 +163,7 @@ def test_write_timers_in_the_reference_timing_csv_columns(tmp_path):
     assert rows[0] == ["timer", "time", "step", "ncycle", "max", "min", "avg"]
     assert len(rows) == 1 + 2 * 4
     names = [r[0] for r in rows[1:5]]
-    assert names == ["estimate_dt", "step_stage0", "step_stage1", "step_finish"]
+    assert names == ["estimate_dt", "stage0", "stage1", "finish"]
     assert all(int(r[3]) == 5 for r in rows[1:5]) and all(int(r[3]) == 8 for r in rows[5:])
     assert all(int(r[2]) == 5 for r in rows[1:5]) and all(int(r[2]) == ist for r in rows[5:])
     assert abs(float(rows[5][1]) - t) <= 1.0e-6 * max(t, 1e-30) + 1e-6
