@@ -234,8 +234,11 @@ stage1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times,
 // in the barriers).  Each step: the dt rules (one thread), stage 0 (p -> ph), stage 1
 // (ph, p -> p), the time update (one thread); a cluster barrier after the dt rules and
 // after each stage orders the state, the time record and the CFL accumulator between the
-// CTAs (release/acquire at cluster scope).  Every CTA runs the same nsteps iterations and
-// the same barriers; a problem past its end time skips the stage work inside them.
+// CTAs (release/acquire at cluster scope).  Every CTA of a cluster takes the same
+// barriers: the loop runs nsteps iterations unless the problem's loop has ended (t >=
+// tmax), which every CTA reads from the time record after the same barrier -- the next
+// write of that flag comes two barriers later -- so all leave together; the lead then
+// closes the step as the time update would (a step past the end changes nothing else).
 __global__ void __launch_bounds__(NT1)
 resident1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ times, Tables tb, StateSoA p,
                   StateSoA ph, int nsteps, int *err, const __grid_constant__ TmaTables1d none)
@@ -250,6 +253,10 @@ resident1d_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ time
   for (int k = 0; k < nsteps; k++) {
     if (lead) dt_finalize_one(probs[m], times + m, err);
     cl.sync();
+    if (times[m].done) {
+      if (lead) finish_one(times + m);
+      break;
+    }
     if (active) stage1d_tile<0, false>(probs, times, tile, tb, p, p, ph, none);
     cl.sync();
     if (active) stage1d_tile<1, false>(probs, times, tile, tb, ph, p, p, none);
