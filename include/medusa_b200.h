@@ -154,7 +154,9 @@ int mdg_run_host(mdg_solver *const *solvers, int n, const double *const *h_in, d
 int mdg_estimate_dt(mdg_solver *s, double *dt_out);
 
 /* Advance every problem by nsteps passes of the main.c time loop.  Asynchronous with
- * respect to the host (work is queued on the solver's stream). */
+ * respect to the host (work is queued on the solver's stream): the per-phase launches
+ * (replayed from CUDA graphs of mdg_launch_config::steps_per_graph steps), or for small
+ * plain-FP64 1-D problems the resident stepper (mdg_launch_config::resident). */
 int mdg_step(mdg_solver *s, int nsteps);
 
 /* For a host that runs the main.c time loop itself (its own dump/pdump/tmax clipping of
