@@ -373,7 +373,8 @@ typedef struct mdg_server_stats {
 } mdg_server_stats;
 
 int mdg_server_create(const mdg_server_config *cfg, mdg_server **out);
-/* Queue a 1-D or 2-D request (thread-safe); *id identifies it in the calls below. */
+/* Queue a 1-D, 2-D Cartesian or dendritic (3-D, 2-D spherical) request (thread-safe);
+ * *id identifies it in the calls below. */
 int mdg_server_submit(mdg_server *s, const mdg_problem_desc *desc, const double *prim, long long *id);
 /* Run `rounds` scheduling rounds in the calling thread (rounds <= 0: until nothing is
  * queued or running); *active = problems resident after the last round. */
