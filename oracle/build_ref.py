@@ -153,6 +153,10 @@ def log_metric_source(ref_root, cdir):
             f.write(src)
     return out
 
+# configurations also built with the reference's timers on (DO_TIMING=TRUE, its Makefile
+# flags): reftime_<cfg> writes timing.csv for the phase split of the CPU baseline
+TIMING_CONFIGS = ("cart1d", "cart2d", "sph1d", "sph3d_sinh")
+
 PARITY_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]
 FAST_FLAGS = ["-O3", "-ffast-math", "-ftree-vectorize", "-fpeel-loops"]
 
@@ -174,10 +178,12 @@ def write_build_h(path, defs):
         f.write(text)
 
 
-def build_config(name, cfg, ref_root, force=False):
+def build_config(name, cfg, ref_root, force=False, timing=False):
     defs = dict(BASE_DEFS)
     defs.update(cfg)
-    cdir = os.path.join(OUT, name)
+    if timing:
+        defs["DO_TIMING"] = "TRUE"
+    cdir = os.path.join(OUT, name + ("_timing" if timing else ""))
     os.makedirs(cdir, exist_ok=True)
     write_build_h(os.path.join(cdir, "build.h"), defs)
     srcs = [os.path.join(ref_root, s) for s in REF_SOURCES]
@@ -192,7 +198,9 @@ def build_config(name, cfg, ref_root, force=False):
     srcs += [os.path.join(SHIM, "ref_harness.c"), os.path.join(SHIM, "ref_main.c")]
     deps = srcs + [os.path.join(cdir, "build.h"), os.path.abspath(__file__)]
     built = []
-    for exe, flags in (("ref_" + name, PARITY_FLAGS), ("reffast_" + name, FAST_FLAGS)):
+    exes = (("reftime_" + name, FAST_FLAGS),) if timing else (("ref_" + name, PARITY_FLAGS),
+                                                               ("reffast_" + name, FAST_FLAGS))
+    for exe, flags in exes:
         target = os.path.join(OUT, exe)
         if (not force and os.path.exists(target)
                 and os.path.getmtime(target) >= max(os.path.getmtime(d) for d in deps)):
@@ -275,6 +283,8 @@ def build(ref_root=DEFAULT_REF_ROOT, force=False, dropin=True):
     out = []
     for name, cfg in CONFIGS.items():
         out += build_config(name, cfg, ref_root, force)
+    for name in TIMING_CONFIGS:
+        out += build_config(name, CONFIGS[name], ref_root, force, timing=True)
     if dropin and os.path.exists(os.path.join(LIBDIR, "libmedusa_b200.so")):
         for name in DROPIN:
             out += build_dropin(name, ref_root, force)

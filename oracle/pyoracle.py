@@ -7,7 +7,8 @@
 - :func:`run_reference` runs the reference itself (built unmodified by
   oracle/build_ref.py into oracle/_ref/) on the same problem in a subprocess.
 
-Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module.
+Only tests/, __graft_entry__.smoke(), bench.py's CPU-baseline leg and
+oracle/reference_phases.py (the timer split of that baseline) use this module.
 """
 from __future__ import annotations
 
@@ -252,6 +253,32 @@ def reference_geometry(pb):
     scale[0..NDIM][3], conn[27]) of zone (i, j, 0) for every row of reference_grid, in
     the same order."""
     return np.frombuffer(_ref_dump(pb, "geom"), dtype=np.float64).reshape(-1, 64).copy()
+
+
+def time_reference_phases(pb, warmup: int, steps: int) -> dict:
+    """The reference's own timers (TIMER_START/TIMER_STOP around step, estimate_dt,
+    prim_to_fluxes1/2/3, push, reset_boundaries, ...) over `steps` steps after `warmup`,
+    from the reftime_<cfg> build (its Makefile flags with DO_TIMING=TRUE) and the
+    timing.csv it writes (io.c:51-108 columns).  Returns {"zone_updates_per_s", "seconds",
+    "steps", "cells", "timers": {name: (total seconds, cycles)}}."""
+    exe = os.path.join(REF_DIR, "reftime_" + ref_config(pb))
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        _write_input(pb, fin)
+        r = subprocess.run([exe, "time", fin, str(warmup), str(steps)], check=True, cwd=td,
+                           capture_output=True, text=True)
+        rows = open(os.path.join(td, "timing.csv")).read().strip().splitlines()
+    out = {}
+    for tok in r.stdout.split():
+        k, v = tok.split("=")
+        out[k] = float(v)
+    if rows[0].split(",") != ["timer", "time", "step", "ncycle", "max", "min", "avg"]:
+        raise RuntimeError("unexpected timing.csv header: %r" % rows[0])
+    out["timers"] = {}
+    for row in rows[1:]:
+        f = row.split(",")
+        out["timers"][f[0]] = (float(f[4]), int(f[3]))
+    return out
 
 
 def time_reference(pb, warmup: int, steps: int, fast: bool = True) -> dict:

@@ -18,7 +18,8 @@
  *     caller (the problem files problems/init_sod.c, init_kh.c, init_sedov.c and
  *     init_spherical_noh.c are restated on the Python side), prob_bounds restates
  *     problems/init_spherical_noh.c:63-79;
- *   - the io.c entry points that the hot path references are no-ops.
+ *   - output_timers restates io.c:51-108 (timing.csv) for builds with DO_TIMING=TRUE;
+ *     the other io.c entry points that the hot path references are no-ops.
  */
 #include "decs.h"
 #include "defs.h"
@@ -58,7 +59,29 @@ static double g_dtold = 1.0e100;
 /* ---------------- io.c entry points referenced by the hot path ---------------- */
 void parse_input(char *name) { (void)name; }
 void run_log() {}
-void output_timers() {}
+/* io.c:51-108: append the reference's timers (TIMER_START/TIMER_STOP, decs.h:717-746)
+ * to timing.csv in the working directory, with the header row when the file is new.
+ * One process: max, min and avg are the timer's own total (the reference's serial path
+ * writes the first timer's total in every row). */
+void output_timers()
+{
+#if DO_TIMING==TRUE
+  const char *fname = "timing.csv";
+  FILE *probe = fopen(fname, "r");
+  const int fresh = probe == NULL;
+  if (probe) fclose(probe);
+  FILE *fp = fopen(fname, "a");
+  if (!fp) return;
+  if (fresh) fprintf(fp, "timer,time,step,ncycle,max,min,avg\n");
+  for (int k = 0; k < ntimers; ++k) {
+    Timer *timer = get_timer(k);
+    double total = 0.0;
+    timer_get_total(timer, &total);
+    fprintf(fp, "%s,%f,%d,%lu,%f,%f,%f\n", timer->name, t, istep, timer->ncycles, total, total, total);
+  }
+  fclose(fp);
+#endif
+}
 void dump1() {}
 void dump2() {}
 void dump3() {}
@@ -282,6 +305,14 @@ REF_API void ref_step_with_dt(double dtin)
   istep++;
 }
 
+/* the timers of a DO_TIMING=TRUE build: zeroed (after warm-up steps) and written */
+REF_API void ref_timers_reset(void)
+{
+#if DO_TIMING==TRUE
+  for (int k = 0; k < ntimers; ++k) timer_reset(get_timer(k));
+#endif
+}
+REF_API void ref_timers_write(void) { output_timers(); }
 REF_API double ref_get_t(void) { return t; }
 REF_API double ref_get_min_dt(void) { return min_dt; }
 REF_API int ref_get_istep(void) { return istep; }

@@ -10,7 +10,9 @@
  *       output: for the initial state and every snap_every-th step:
  *               [istep, t, dt_used, min_dt] + interior prims [ncell][5] (all double)
  *   ref_<cfg> time  <input.bin> <warmup> <steps>
- *       prints one line: "zone_updates_per_s=<v> seconds=<s> steps=<n> cells=<c>"
+ *       prints one line: "zone_updates_per_s=<v> seconds=<s> steps=<n> cells=<c>"; a
+ *       DO_TIMING=TRUE build (reftime_<cfg>) also writes the reference's timers of the
+ *       timed steps to timing.csv in the working directory
  *   ref_<cfg> grid  <input.bin> <output.bin>
  *       output: int32 nj[n1+2NG], then int32 nk for every row (i, j) of ref_get_grid
  *   ref_<cfg> geom  <input.bin> <output.bin>
@@ -50,6 +52,8 @@ int ref_init(const ref_params *prm, const double *ic);
 double ref_advance_one(void);
 double ref_get_t(void);
 double ref_get_min_dt(void);
+void ref_timers_reset(void);
+void ref_timers_write(void);
 int ref_get_istep(void);
 int ref_cell_count(void);
 void ref_get_interior(double *prim, double *eos);
@@ -116,9 +120,11 @@ int main(int argc, char **argv)
     int warm = atoi(argv[3]);
     int steps = atoi(argv[4]);
     for (int s=0; s<warm; s++) ref_advance_one();
+    ref_timers_reset();
     double t0 = now_s();
     for (int s=0; s<steps; s++) ref_advance_one();
     double el = now_s() - t0;
+    ref_timers_write();
     printf("zone_updates_per_s=%.6e seconds=%.6f steps=%d cells=%d\n",
            (double)ncell*steps/el, el, steps, ncell);
   } else if (strcmp(argv[1], "grid") == 0 || strcmp(argv[1], "geom") == 0) {
