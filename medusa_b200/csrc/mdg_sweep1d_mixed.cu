@@ -253,7 +253,10 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
                      Tables tb, StateSoA sst, StateSoA sn, StateSoA out)
 {
   __shared__ double sv[6][NT + 2];     // stage-state pencil: 5 primitives + pressure
-  __shared__ double sar[6][NT];        // right face values of each reconstructed zone
+  // FP32 right-face offset of each reconstructed zone (face value = zone average + offset,
+  // formed in FP64 by the reader: half the shared memory of storing the FP64 face values,
+  // which leaves more of the SM's L1 to the register spills)
+  __shared__ float sdr[6][NT];
   __shared__ double sfl[NPRIM][NT];    // face fluxes
   __shared__ double sred[32];
   __shared__ int s_item;
@@ -320,7 +323,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
         float dl, dr;
         mixed_recon((float)(a - sv[v][t]), (float)(sv[v][t + 2] - a), w, dl, dr);
         al[v] = a + (double)dl;
-        sar[v][t] = a + (double)dr;
+        sdr[v][t] = dr;
       }
     }
     __syncthreads();
@@ -331,7 +334,7 @@ stage1d_mixed_kernel(const ProbDev *__restrict__ probs, ProbTime *__restrict__ t
       double pl[6], flux[NPRIM];
       float sig;
 #pragma unroll
-      for (int v = 0; v < 6; v++) pl[v] = sar[v][t - 1];
+      for (int v = 0; v < 6; v++) pl[v] = sv[v][t] + (double)sdr[v][t - 1];   // zone z-1: average sv[v][t]
       const int zf = z < 0 ? 0 : (z > n1 ? n1 : z);
       const FaceGeom<double> fg = TAB ? face_geom_tab(tb.geo, gs, P.geo_off + zf + NG) : face_geom_1d(P, zf);
       const GamConst<float> gc = gam_const<float>((float)P.gam);
