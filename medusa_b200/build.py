@@ -15,6 +15,8 @@ import os
 import shutil
 import subprocess
 import sys
+import time
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -49,12 +51,15 @@ def _newer(target, deps):
     return all(os.path.getmtime(d) <= t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, report: bool = False) -> str:
+    """Compile the translation units that are out of date (all with force), in parallel,
+    and link the library; with report, one line on stderr says what was compiled."""
+    t0 = time.time()
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(LIBDIR, "obj")
     os.makedirs(objdir, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "medusa_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for src in SOURCES:
         sp = os.path.join(CSRC, src)
         obj = os.path.join(objdir, src + ".o")
@@ -66,21 +71,37 @@ def build(force: bool = False, verbose: bool = False) -> str:
                "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-I", INCLUDE] + ARCH
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        r = subprocess.run(cmd, capture_output=True, text=True)
-        if verbose or r.returncode != 0:
-            sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc failed on %s" % src)
+        jobs.append((src, cmd))
+
+    def compile_one(job):
+        return job, subprocess.run(job[1], capture_output=True, text=True)
+
+    failed = []
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for (src, cmd), r in ex.map(compile_one, jobs):
+            if verbose or r.returncode != 0:
+                sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+            if r.returncode != 0:
+                failed.append(src)
+    if failed:
+        raise RuntimeError("nvcc failed on %s" % ", ".join(failed))
     mapfile = os.path.join(objdir, "exports.map")
-    with open(mapfile, "w") as f:
-        f.write("{ global: mdg_*; local: *; };\n")
+    if not (os.path.exists(mapfile) and open(mapfile).read() == "{ global: mdg_*; local: *; };\n"):
+        with open(mapfile, "w") as f:
+            f.write("{ global: mdg_*; local: *; };\n")
+    linked = False
     if force or not _newer(LIB, objs + [mapfile]):
+        linked = True
         cmd = [nvcc(), "-shared", "-o", LIB] + objs + ARCH + [
             "-Xlinker", "--version-script=" + mapfile, "-cudart", "static"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
             raise RuntimeError("link of libmedusa_b200.so failed")
+    if report:
+        sys.stderr.write("medusa_b200: compiled %d of %d translation units for sm_100a%s, %s libmedusa_b200.so "
+                         "(%.0f s)\n" % (len(jobs), len(SOURCES), " (forced)" if force else "",
+                                         "linked" if linked else "kept", time.time() - t0))
     return LIB
 
 
@@ -89,4 +110,4 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     a = ap.parse_args()
-    print(build(a.force, a.verbose))
+    print(build(a.force, a.verbose, report=True))
