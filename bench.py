@@ -426,6 +426,18 @@ def run_reference_arm(args, ctx):
         cb = cpu_baseline_ensemble(probs, steps=args.steps)
         config = {"workload": server_workload_name(args), "requests": len(probs)}
         dtype = "f64"
+    elif args.workload == "eos":
+        cb = cpu_baseline_eos()
+        config = {"workload": "tabulated_eos_given_rex_%dM_zones_table_16x50x300x300" % (EOS_ZONES >> 20),
+                  "global_batch": 1, "seq_len": EOS_ZONES, "parallelism": "replicas"}
+        line = {"metric": "zone EOS updates/s", "value": cb["value"], "unit": "zone EOS updates/s",
+                "n_gpus": ctx.world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": config, "cpu_baseline": cb,
+                "e2e": {"value": cb["value"], "unit": "zone EOS updates/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
     else:
         probs = P.ensemble_1d(args.ensemble_count, seed=ENSEMBLE_SEED)
         cb = cpu_baseline_ensemble(probs, steps=args.steps)
@@ -932,6 +944,114 @@ def sedov3d_full_run(ctx, pb, t_end, chunk=2000):
     return out
 
 
+EOS_ZONES = 8 * 1024 * 1024
+EOS_BYTES_PER_ZONE = 72      # rho, u, Ye, T read; T, p, cs, s, Gamma_1 written (FP64)
+
+
+def cpu_baseline_eos(n=1 << 20):
+    """The reference's own tabulated-EOS zone update (eos/burrows/eos_stuff.c:768-902,
+    oracle/_ref/refeos) on one core over n seeded zones of the synthetic table at the
+    reference's sizes, from the temperatures of a first pass (the warm start that the GPU
+    leg's timed launches have too); the second pass's loop alone is timed."""
+    import subprocess
+    import tempfile
+    import numpy as np
+    from medusa_b200 import eos_table as ET
+    from oracle import pyoracle
+    exe = os.path.join(pyoracle.REF_DIR, "refeos")
+    if not os.path.exists(exe):
+        return {"value": None, "unit": "zone EOS updates/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/refeos was not built"}
+    g = ET.REFERENCE_GRID
+    tab = ET.synthetic_table(g)
+    rho, u, ye, tg = ET.synthetic_zones(g, n, seed=32, table=tab)
+    with tempfile.TemporaryDirectory() as td:
+        ft, fz, fo = (os.path.join(td, x) for x in ("table.bin", "zones.bin", "out.bin"))
+        tab.tofile(ft)
+        for _ in range(2):
+            with open(fz, "wb") as f:
+                f.write(np.int64(n).tobytes())
+                f.write(np.ascontiguousarray(np.stack([rho, u, ye, tg], axis=1)).tobytes())
+            r = subprocess.run([exe, ft, fz, fo], check=True, capture_output=True, text=True)
+            tg = np.fromfile(fo, dtype=np.float64).reshape(-1, 5)[:, 2].copy()
+    kv = dict(tok.split("=") for tok in r.stdout.split())
+    sec = float(kv["seconds"])
+    return {"value": n / sec, "unit": "zone EOS updates/s", "cores": 1, "kind": "reference",
+            "sample": "%d zones, temperature guesses from a first pass, the reference's eos_given_rex_per_zone "
+                      "built with -O2 -fno-fast-math, 1 core, %.3f s" % (n, sec)}
+
+
+def run_eos(args, ctx):
+    """The tabulated nuclear EOS zone update (eos_given_rex_per_zone) over EOS_ZONES zones
+    of the synthetic table at the reference's sizes (16 x 50 x 300 x 300); each launch
+    starts from the previous launch's temperatures, as successive calls of the reference
+    do (eos[TEMP] is the guess)."""
+    import numpy as np
+    import torch
+    from medusa_b200 import eos_table as ET
+    g = ET.REFERENCE_GRID
+    tab = ET.synthetic_table(g)
+    n = EOS_ZONES
+    rho, u, ye, tg = ET.synthetic_zones(g, n, seed=31, table=tab)
+    dev = ctx.local
+    with ET.EosTable(tab, g, device=dev) as t:
+        ins = [torch.tensor(a, dtype=torch.float64, device="cuda:%d" % dev) for a in (rho, u, ye, tg)]
+        outs = [torch.empty(n, dtype=torch.float64, device="cuda:%d" % dev) for _ in range(4)]
+        stream = torch.cuda.current_stream(dev)
+        ptrs = [x.data_ptr() for x in ins] + [o.data_ptr() for o in outs]
+
+        def launch():
+            t.given_rex_device(n, *ptrs, stream=stream.cuda_stream)
+        for _ in range(args.warmup):
+            launch()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        sampler = ClockSampler(dev)
+        sampler.start()
+        ctx.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            launch()
+        e1.record(stream)
+        e1.synchronize()
+        ms = ctx.max_ms(e0.elapsed_time(e1)) / args.steps
+        clocks = sampler.stop()
+        # end to end through the host entry point: host arrays, copies in and out included
+        h0 = time.perf_counter()
+        k_e2e = 3
+        for _ in range(k_e2e):
+            t.given_rex(rho, u, ye, tg)
+        e2e_ms = (time.perf_counter() - h0) * 1e3 / k_e2e
+    value = ctx.world * n / (ms / 1e3)
+    if ctx.rank != 0:
+        return
+    peak, peak_kind = read_peaks()
+    achieved = EOS_BYTES_PER_ZONE * n / (ms / 1e3) / 1e9
+    line = {
+        "metric": "zone EOS updates/s", "value": value, "unit": "zone EOS updates/s", "n_gpus": ctx.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "tabulated_eos_given_rex_%dM_zones_table_16x50x300x300" % (n >> 20),
+                   "global_batch": ctx.world, "seq_len": n,
+                   "parallelism": "replicas" if ctx.world > 1 else "single",
+                   "l2": "inputs and outputs (600 MB) and table (180 MB on the device) larger than L2"},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "e2e": {"value": ctx.world * n / (e2e_ms / 1e3), "unit": "zone EOS updates/s",
+                "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 40 * n,
+                "timed": "mdg_eos_given_rex_host: pageable host arrays, copies in and out, wall clock"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "eos_rex_kernel",
+                     "algorithmic_bytes_per_zone": EOS_BYTES_PER_ZONE,
+                     "note": "streamed zone bytes only; each zone also gathers 4 x 64 B of interpolated "
+                             "records and 32 B per energy-scan step from the table",
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)"},
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_eos()
+    print(json.dumps(line), flush=True)
+
+
 def run_sod1d(args, ctx):
     """Config C1: the Sod tube of problems/init_sod.c, 1024 zones, CFL 0.8, run to t = 0.2
     in plain FP64, timed as a whole (device time from t = 0 to the end: the resident
@@ -1099,7 +1219,8 @@ def main():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="ensemble", choices=["ensemble", "kh2048", "server", "sedov3d", "sod1d"])
+    ap.add_argument("--workload", default="ensemble",
+                    choices=["ensemble", "kh2048", "server", "sedov3d", "sod1d", "eos"])
     ap.add_argument("--server-requests", type=int, default=6000)
     ap.add_argument("--server-rates", default="1000,4000,16000,inf",
                     help="server: Poisson arrival rates (requests/s) swept; inf = all at once")
@@ -1147,6 +1268,8 @@ def main():
             run_sedov3d(args, ctx)
         elif args.workload == "sod1d":
             run_sod1d(args, ctx)
+        elif args.workload == "eos":
+            run_eos(args, ctx)
         else:
             run_kh(args, ctx)
     finally:

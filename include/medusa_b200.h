@@ -431,6 +431,42 @@ int mdg_dump_ascii1(mdg_solver *s, int prob, const char *path);
 int mdg_grid3d_counts(const mdg_problem_desc *desc, int *nj, int *nk, long long *ncell);
 int mdg_grid3d_geometry(const mdg_problem_desc *desc, double *rows, long long *nrows);
 
+/*
+ * Tabulated (nuclear) EOS: the zone update of the reference's production EOS,
+ * eos_given_rex_per_zone (eos/burrows/eos_stuff.c:768-902, called per zone by
+ * eos_given_rex_tianshu, :507-640): from density, internal energy density, Ye and a
+ * temperature guess to temperature, pressure, sound speed, entropy and Gamma_1.
+ *
+ * mdg_eos_grid holds what the reference fixes in DEFINE_EOSCONST_1 (eos_stuff.c:8-21:
+ * nrec = 16 records of ny = 50 x nr = 300 x nt = 300, log10 rho in [1, 15.5], log10 T
+ * (MeV) in [-2, 2], Ye in [0.035, 0.56]) and const_hack (0 there).  mdg_eos_table_create
+ * copies a table in the reference's layout (TAB_ELEM, eos_stuff.c:7: [nrec][ny][nr][nt],
+ * jt fastest; records 1, 2, 3 and 12 -- energy, log pressure, entropy, Gamma_1 -- are
+ * used, so nrec >= 12) to the device, rearranged for the gathers (the four records
+ * interleaved per grid point, 32 B: 144 MB at the reference's sizes).  Results agree with the reference's to a few
+ * ulps (CUDA's log10, exp and pow; everything else in the reference's operation order).
+ * Indices the reference would take outside the table (inputs outside its range) are
+ * clamped to it.
+ */
+typedef struct mdg_eos_grid {
+  int nrec, ny, nr, nt;
+  double r1, r2;            /* log10 rho range */
+  double t1, t2;            /* log10 T (MeV) range */
+  double y1, y2;            /* Ye range */
+  double const_hack;        /* subtracted from the specific energy (eos_stuff.c:784) */
+} mdg_eos_grid;
+typedef struct mdg_eos_table mdg_eos_table;   /* opaque */
+int mdg_eos_table_create(const mdg_eos_grid *grid, const double *table, int device, mdg_eos_table **out);
+int mdg_eos_table_destroy(mdg_eos_table *t);
+/* n zones, DEVICE pointers: rho, u (internal energy density), ye in; temp in (the guess,
+ * eos[TEMP] before the call) and out; press, cs, ent, gam1 out.  Queued on `stream` (a
+ * cudaStream_t, 0 for the legacy default stream). */
+int mdg_eos_given_rex(mdg_eos_table *t, long long n, const double *rho, const double *u, const double *ye,
+                      double *temp, double *press, double *cs, double *ent, double *gam1, void *stream);
+/* The same from HOST buffers: copies in, the update, copies out; returns when done. */
+int mdg_eos_given_rex_host(mdg_eos_table *t, long long n, const double *rho, const double *u, const double *ye,
+                           double *temp, double *press, double *cs, double *ent, double *gam1);
+
 /* Library version as major*10000 + minor*100 + patch. */
 int mdg_version(void);
 

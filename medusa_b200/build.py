@@ -26,7 +26,8 @@ LIB = os.path.join(LIBDIR, "libmedusa_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 SOURCES = ["mdg_capi.cu", "mdg_sweep1d.cu", "mdg_sweep1d_mixed.cu", "mdg_sweep2d.cu", "mdg_misc.cu",
-           "mdg_geometry.cpp", "mdg_noalloc.cu", "mdg_server.cu", "mdg_tables.cu", "mdg_sweep3d.cu", "mdg_tma.cu"]
+           "mdg_geometry.cpp", "mdg_noalloc.cu", "mdg_server.cu", "mdg_tables.cu", "mdg_sweep3d.cu", "mdg_tma.cu",
+           "mdg_eos_table.cu"]
 HEADERS = ["mdg_internal.h", "mdg_hydro.cuh", "mdg_kernels.cuh", "mdg_load1d.cuh", "mdg_tables.cuh",
            "mdg_grid3d.cuh", "mdg_mixed.cuh", "mdg_tma.cuh",
            "mdg_timeloop.cuh"]

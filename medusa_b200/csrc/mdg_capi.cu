@@ -1510,6 +1510,113 @@ int mdg_write_timers(mdg_solver *s, int prob, const char *path)
   return MDG_OK;
 }
 
+struct mdg_eos_table {
+  int device = 0;
+  int num_sms = 0;
+  mdg_eos_grid g{};
+  double2 *d_f = nullptr;
+  cudaStream_t stream = nullptr;
+  EosTableDev dev() const
+  {
+    return EosTableDev{d_f, g.ny, g.nr, g.nt, g.r1, g.r2, g.t1, g.t2, g.y1, g.y2, g.const_hack};
+  }
+};
+
+int mdg_eos_table_destroy(mdg_eos_table *t)
+{
+  if (!t) return MDG_OK;
+  cudaSetDevice(t->device);
+  if (t->stream) cudaStreamSynchronize(t->stream);
+  cudaFree(t->d_f);
+  if (t->stream) cudaStreamDestroy(t->stream);
+  delete t;
+  return MDG_OK;
+}
+
+int mdg_eos_table_create(const mdg_eos_grid *grid, const double *table, int device, mdg_eos_table **out)
+{
+  if (!grid || !table || !out) return fail(MDG_ERR_INVALID, "grid/table/out");
+  *out = nullptr;
+  const mdg_eos_grid &g = *grid;
+  if (g.nrec < 12 || g.ny < 2 || g.nr < 2 || g.nt < 2)
+    return fail(MDG_ERR_INVALID, "the table needs nrec >= 12 and at least 2 points per axis");
+  if (!(g.r2 > g.r1) || !(g.t2 > g.t1) || !(g.y2 > g.y1) || !std::isfinite(g.const_hack))
+    return fail(MDG_ERR_INVALID, "table bounds must be finite and increasing");
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) return fail(MDG_ERR_INVALID, "device ordinal out of range");
+  CK(cudaSetDevice(device));
+  const size_t npt = (size_t)g.ny * g.nr * g.nt;
+  // records 1, 2, 3, 12 (energy, log pressure, entropy, Gamma_1) interleaved per grid point
+  std::vector<double> hf(4 * npt);
+  const double *e = table, *lp = table + 1 * npt, *en = table + 2 * npt, *g1 = table + 11 * npt;
+  for (size_t k = 0; k < npt; k++) {
+    hf[4 * k + 0] = e[k];
+    hf[4 * k + 1] = lp[k];
+    hf[4 * k + 2] = en[k];
+    hf[4 * k + 3] = g1[k];
+  }
+  mdg_eos_table *t = new mdg_eos_table();
+  t->device = device;
+  t->g = g;
+  auto bail = [&](cudaError_t e) {
+    mdg_eos_table_destroy(t);
+    if (e == cudaErrorMemoryAllocation) return fail(MDG_ERR_OUTOFMEM, "no device memory for the EOS table");
+    return fail(MDG_ERR_CUDA, std::string("EOS table: ") + cudaGetErrorString(e));
+  };
+  cudaError_t ce = cudaDeviceGetAttribute(&t->num_sms, cudaDevAttrMultiProcessorCount, device);
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaMalloc(&t->d_f, sizeof(double) * 4 * npt);
+  if (ce == cudaSuccess) ce = cudaMemcpy(t->d_f, hf.data(), sizeof(double) * 4 * npt, cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) return bail(ce);
+  *out = t;
+  return MDG_OK;
+}
+
+int mdg_eos_given_rex(mdg_eos_table *t, long long n, const double *rho, const double *u, const double *ye,
+                      double *temp, double *press, double *cs, double *ent, double *gam1, void *stream)
+{
+  if (!t) return fail(MDG_ERR_INVALID, "table");
+  if (n < 0) return fail(MDG_ERR_INVALID, "n < 0");
+  if (n > 0 && (!rho || !u || !ye || !temp || !press || !cs || !ent || !gam1))
+    return fail(MDG_ERR_INVALID, "null zone array");
+  CK(cudaSetDevice(t->device));
+  launch_eos_rex(t->dev(), n, rho, u, ye, temp, press, cs, ent, gam1, t->num_sms, (cudaStream_t)stream);
+  CK(cudaGetLastError());
+  return MDG_OK;
+}
+
+int mdg_eos_given_rex_host(mdg_eos_table *t, long long n, const double *rho, const double *u, const double *ye,
+                           double *temp, double *press, double *cs, double *ent, double *gam1)
+{
+  if (!t) return fail(MDG_ERR_INVALID, "table");
+  if (n < 0) return fail(MDG_ERR_INVALID, "n < 0");
+  if (n == 0) return MDG_OK;
+  if (!rho || !u || !ye || !temp || !press || !cs || !ent || !gam1) return fail(MDG_ERR_INVALID, "null zone array");
+  CK(cudaSetDevice(t->device));
+  const size_t b = sizeof(double) * (size_t)n;
+  double *d = nullptr;
+  CK(cudaMalloc(&d, 8 * b));
+  double *dz[8];
+  for (int k = 0; k < 8; k++) dz[k] = d + (size_t)k * (size_t)n;
+  const double *hin[4] = {rho, u, ye, temp};
+  double *hout[5] = {temp, press, cs, ent, gam1};
+  cudaError_t e = cudaSuccess;
+  for (int k = 0; k < 4 && e == cudaSuccess; k++)
+    e = cudaMemcpyAsync(dz[k], hin[k], b, cudaMemcpyHostToDevice, t->stream);
+  if (e == cudaSuccess) {
+    launch_eos_rex(t->dev(), n, dz[0], dz[1], dz[2], dz[3], dz[4], dz[5], dz[6], dz[7], t->num_sms, t->stream);
+    e = cudaGetLastError();
+  }
+  double *dout[5] = {dz[3], dz[4], dz[5], dz[6], dz[7]};
+  for (int k = 0; k < 5 && e == cudaSuccess; k++)
+    e = cudaMemcpyAsync(hout[k], dout[k], b, cudaMemcpyDeviceToHost, t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(MDG_ERR_CUDA, std::string("mdg_eos_given_rex_host: ") + cudaGetErrorString(e));
+  return MDG_OK;
+}
+
 int mdg_destroy(mdg_solver *s)
 {
   if (!s) return MDG_OK;

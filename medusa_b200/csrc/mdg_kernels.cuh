@@ -54,6 +54,17 @@ constexpr int TJY2 = NTY2 - 2;
 constexpr int TIY2 = MDG_TIY2;    // rows per direction-1 tile
 
 struct TmaTables1d;
+// Tabulated EOS on the device (mdg_eos_table.cu): the records f[jy][jr][jt] = {e, log p,
+// s, Gamma_1} as two double2 per grid point; grid sizes and bounds as the reference's
+// DEFINE_EOSCONST_1.
+struct EosTableDev {
+  const double2 *f;
+  int ny, nr, nt;
+  double r1, r2, t1, t2, y1, y2, const_hack;
+};
+void launch_eos_rex(const EosTableDev &d, long long n, const double *rho, const double *u, const double *ye,
+                    double *temp, double *press, double *cs, double *ent, double *gam1, int num_sms,
+                    cudaStream_t st);
 // The resident 1-D stepper (plain FP64): CTAs per problem for problems of at most
 // max_tiles tiles (a power of two), or 0 when it cannot run (more than
 // RESIDENT1D_MAX_TILES tiles, or such a cluster does not fit this device); the launch of

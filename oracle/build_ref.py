@@ -274,6 +274,30 @@ def build_dropin(name, ref_root, force=False):
     return built
 
 
+def build_eos(ref_root, force=False):
+    """oracle/_ref/refeos: the reference's tabulated-EOS zone update
+    (eos/burrows/eos_stuff.c, unmodified) driven by oracle/refshim/eos_ref_harness.c, with
+    the parity flags and the build switches of the 1-D spherical configuration."""
+    defs = dict(BASE_DEFS)
+    defs.update(CONFIGS["sph1d"])
+    cdir = os.path.join(OUT, "eos")
+    os.makedirs(cdir, exist_ok=True)
+    write_build_h(os.path.join(cdir, "build.h"), defs)
+    srcs = [os.path.join(ref_root, "eos", "burrows", "eos_stuff.c"), os.path.join(SHIM, "eos_ref_harness.c")]
+    target = os.path.join(OUT, "refeos")
+    deps = srcs + [os.path.join(cdir, "build.h"), os.path.abspath(__file__)]
+    if (not force and os.path.exists(target)
+            and os.path.getmtime(target) >= max(os.path.getmtime(d) for d in deps)):
+        return [target]
+    cmd = (["gcc", "-std=gnu99", "-w"] + PARITY_FLAGS + ["-I" + cdir, "-I" + ref_root, "-include", "limits.h",
+                                                        "-o", target] + srcs + ["-lm"])
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("oracle/_ref build failed for refeos")
+    return [target]
+
+
 def build(ref_root=DEFAULT_REF_ROOT, force=False, dropin=True):
     """Build every configuration (and, when libmedusa_b200.so is built, the drop-in
     runs); returns the list of binaries.  Needs the reference tree."""
@@ -285,6 +309,7 @@ def build(ref_root=DEFAULT_REF_ROOT, force=False, dropin=True):
         out += build_config(name, cfg, ref_root, force)
     for name in TIMING_CONFIGS:
         out += build_config(name, CONFIGS[name], ref_root, force, timing=True)
+    out += build_eos(ref_root, force)
     if dropin and os.path.exists(os.path.join(LIBDIR, "libmedusa_b200.so")):
         for name in DROPIN:
             out += build_dropin(name, ref_root, force)

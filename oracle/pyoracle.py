@@ -24,6 +24,7 @@ BUILD_DIR = os.path.join(HERE, "_build")
 LIB_PATH = os.path.join(BUILD_DIR, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 SRC = os.path.join(HERE, "hydro_oracle.c")
+EOS_SRC = os.path.join(HERE, "eos_table_oracle.c")
 ORACLE_FLAGS = ["-O2", "-fno-fast-math", "-ffp-contract=off"]
 
 
@@ -77,9 +78,9 @@ def params_of(pb) -> Params:
 def build_oracle(force: bool = False) -> str:
     os.makedirs(BUILD_DIR, exist_ok=True)
     if (not force and os.path.exists(LIB_PATH)
-            and os.path.getmtime(LIB_PATH) >= os.path.getmtime(SRC)):
+            and os.path.getmtime(LIB_PATH) >= max(os.path.getmtime(SRC), os.path.getmtime(EOS_SRC))):
         return LIB_PATH
-    cmd = ["gcc", "-std=gnu99", "-shared", "-fPIC"] + ORACLE_FLAGS + ["-o", LIB_PATH, SRC, "-lm"]
+    cmd = ["gcc", "-std=gnu99", "-shared", "-fPIC"] + ORACLE_FLAGS + ["-o", LIB_PATH, SRC, EOS_SRC, "-lm"]
     subprocess.run(cmd, check=True)
     return LIB_PATH
 
@@ -111,8 +112,29 @@ def lib():
         L.orc_restart.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.orc_get_moments0.argtypes = [ctypes.c_void_p] * 4
         L.orc_get_geom.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+        L.orc_eos_given_rex_n.argtypes = [ctypes.c_void_p, ctypes.POINTER(EosGrid), ctypes.c_int] + [ctypes.c_void_p] * 5
         _lib = L
     return _lib
+
+
+class EosGrid(ctypes.Structure):
+    """orc_eos_grid of oracle/eos_table_oracle.c: table sizes and grid bounds."""
+    _fields_ = [("nrec", ctypes.c_int), ("ny", ctypes.c_int), ("nr", ctypes.c_int), ("nt", ctypes.c_int),
+                ("r1", ctypes.c_double), ("r2", ctypes.c_double), ("t1", ctypes.c_double),
+                ("t2", ctypes.c_double), ("y1", ctypes.c_double), ("y2", ctypes.c_double),
+                ("const_hack", ctypes.c_double)]
+
+
+def eos_given_rex(table, grid: EosGrid, rho, u, ye, temp_guess):
+    """The tabulated EOS update of eos_given_rex_per_zone (eos/burrows/eos_stuff.c:768-902)
+    for every zone: returns [n][5] = pressure, sound speed, temperature, entropy, Gamma_1."""
+    table = np.ascontiguousarray(table, dtype=np.float64)
+    cols = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, u, ye, temp_guess)]
+    n = cols[0].size
+    out = np.zeros((n, 5))
+    lib().orc_eos_given_rex_n(table.ctypes.data, ctypes.byref(grid), n, *[c.ctypes.data for c in cols],
+                              out.ctypes.data)
+    return out
 
 
 class Oracle:
