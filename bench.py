@@ -1,7 +1,7 @@
 """Benchmark of the hydro sweep: zone-updates/s, batched mixed precision vs plain FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ensemble|kh2048] [--no-cpu-baseline]
+                    [--workload ensemble|kh2048|server|sedov3d|sod1d|eos] [--no-cpu-baseline]
 
 A step is one full RK2 step of the reference time loop (estimate_dt + both stages +
 t += dt) of every problem of the workload; the metric is zone-updates/s (zones x steps /
@@ -23,6 +23,10 @@ replayed from a CUDA graph.  Beside it, measured in the same run:
     sensitivity floor (the same FP64 run with its CFL number scaled by 1 + 1e-7) and, for
     the Noh problems, the FP64 path's L1 error against the analytic solution.
 Workload "kh2048": 2-D Kelvin-Helmholtz 2048 x 2048, plain FP64, gamma 5/3, CFL 0.8.
+Workloads "server" (the solve server under seeded request streams), "sedov3d" (3-D Sedov
+on the dendritic grid), "sod1d" (the 1024-zone Sod job, timed whole) and "eos" (the
+tabulated nuclear EOS zone update over 8 M zones of a synthetic table of the reference's
+sizes; metric zone EOS updates/s) are described at their functions.
 
 - value:  device time of K steps with the state resident in HBM, CUDA events on the
           solver's stream, barrier + synchronize on both sides, max over ranks.  The
