@@ -75,3 +75,25 @@ def test_abi_checks_before_device_work():
     assert L.mdg_eos_given_rex(None, 1, *([None] * 9)) == 1
     assert L.mdg_eos_given_rex_host(None, 1, *([None] * 8)) == 1
     assert L.mdg_eos_table_destroy(None) == 0
+
+
+def test_top_row_guess_is_the_reference_result(ref_table):
+    """A temperature guess on the table's last row makes the reference start its scan at
+    jt = nt; the restatement (and the device kernel) start one row lower.  Where the zone's
+    energy lies inside the table the scan goes down in both and brackets the same rows:
+    the results are the same bits."""
+    if not os.path.exists(REFEOS):
+        pytest.skip("oracle/_ref/refeos absent (python oracle/build_ref.py)")
+    g = ET.REFERENCE_GRID
+    rho, u, ye, _ = ET.synthetic_zones(g, 64, seed=41, table=ref_table)
+    tg = np.full(rho.size, 10.0 ** g.t2)
+    with tempfile.TemporaryDirectory() as td:
+        ft, fz, fo = (os.path.join(td, x) for x in ("table.bin", "zones.bin", "out.bin"))
+        ref_table.tofile(ft)
+        with open(fz, "wb") as fh:
+            fh.write(np.int64(rho.size).tobytes())
+            fh.write(np.ascontiguousarray(np.stack([rho, u, ye, tg], axis=1)).tobytes())
+        subprocess.run([REFEOS, ft, fz, fo], check=True, stdout=subprocess.DEVNULL)
+        ref = np.fromfile(fo, dtype=np.float64).reshape(-1, 5)
+    assert np.array_equal(pyoracle.eos_given_rex(ref_table, _grid(g), rho, u, ye, tg), ref)
+
